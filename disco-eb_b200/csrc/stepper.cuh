@@ -1,0 +1,477 @@
+// Rodas5 step with structured linear algebra, and the adaptive solve of one k-mode.
+//
+// The method is the 8-stage Rosenbrock scheme of Di Marzo (1993), as used by the
+// reference's Rodas5Transformed (src/discoeb/ode_integrators_stiff.py:680-892); step
+// control is diffrax's PIDController rule (perturbations.py:913-914) restated from its
+// documentation.  Differences from the reference, all of them documented: steps end
+// exactly on every output time and approximation switch time (no linear interpolation
+// between accepted steps), and the approximation regime is held fixed within a step.
+//
+// W = I/(gamma h) - J is never formed densely.  With the model in coefficient form
+// (model.cuh), J = [[j00, 0], [c0, S + U G]] plus the leaf row 1:
+//   * x_0 from the 1x1 row of the scale factor,
+//   * A = I/(gamma h) - S is a set of independent banded chains, factored without pivoting
+//     (all chain pivots are >= 1/(gamma h) > 0 for these free-streaming / Thomson blocks),
+//     one chain per lane,
+//   * the rank-3 coupling U G (metric h', eta', polarisation sum) by the Woodbury identity,
+//   * x_1 (a h', read by no equation) last.
+// Work per step: O(n) instead of the (2/3) n^3 of a dense LU.
+#pragma once
+
+#include "model.cuh"
+#include "team.cuh"
+
+namespace dscb {
+
+struct Rodas5Tab {
+    double gamma;
+    double a[6][5];
+    double C[8][7];
+    double c[6];
+    double d[5];
+};
+
+#if defined(__CUDACC__)
+__constant__ __device__
+#endif
+static const Rodas5Tab kR5 = {
+    0.19,
+    {{0, 0, 0, 0, 0},
+     {2.0, 0, 0, 0, 0},
+     {3.040894194418781, 1.041747909077569, 0, 0, 0},
+     {2.576417536461461, 1.622083060776640, -0.9089668560264532, 0, 0},
+     {2.760842080225597, 1.446624659844071, -0.3036980084553738, 0.2877498600325443, 0},
+     {-14.09640773051259, 6.925207756232704, -41.47510893210728, 2.343771018586405, 24.13215229196062}},
+    {{0, 0, 0, 0, 0, 0, 0},
+     {-10.31323885133993, 0, 0, 0, 0, 0, 0},
+     {-21.04823117650003, -7.234992135176716, 0, 0, 0, 0, 0},
+     {32.22751541853323, -4.943732386540191, 19.44922031041879, 0, 0, 0, 0},
+     {-20.69865579590063, -8.816374604402768, 1.260436877740897, -0.7495647613787146, 0, 0, 0},
+     {-46.22004352711257, -17.49534862857472, -289.6389582892057, 93.60855400400906, 318.3822534212147, 0, 0},
+     {34.20013733472935, -14.15535402717690, 57.82335640988400, 25.83362985412365, 1.408950972071624,
+      -6.551835421242162, 0},
+     {42.57076742291101, -13.80770672017997, 93.98938432427124, 18.77919633714503, -31.58359187223370,
+      -6.685968952921985, -5.810979938412932}},
+    {0.0, 0.38, 0.3878509998321533, 0.4839718937873840, 0.4570477008819580, 1.0},
+    {0.19, -0.1823079225333714636, -0.319231832186874912, 0.3449828624725343, -0.377417564392089818}};
+
+// ---- chain table ----
+struct Chain {
+    int start, len, stride, kl, ku;
+};
+
+DHD int n_chains(const Dims& D) { return 5 + D.nq; }
+
+DHD Chain chain_of(const Dims& D, int c)
+{
+    Chain ch;
+    ch.stride = 1;
+    ch.kl = 1;
+    ch.ku = 1;
+    if (c == 0) { ch.start = 5; ch.len = D.lmaxg + 3; ch.kl = 2; ch.ku = 2; }
+    else if (c == 1) { ch.start = D.idxgp; ch.len = D.lmaxgp + 1; }
+    else if (c == 2) { ch.start = D.idxr; ch.len = D.lmaxr + 1; }
+    else if (c < 3 + D.nq) { ch.start = D.iq0 + (c - 3); ch.len = D.lmaxnu + 1; ch.stride = D.nq; }
+    else if (c == 3 + D.nq) { ch.start = 3; ch.len = 2; }
+    else { ch.start = D.n - 2; ch.len = 2; }
+    return ch;
+}
+
+// number of doubles of per-mode workspace
+DHD int mode_mem_doubles(const Dims& D) { return 27 * D.n + 32; }
+
+struct ModeMem {
+    double *y, *u, *f, *dT, *col0, *F1, *K, *A, *G, *Z, *sc;
+};
+
+DHD ModeMem carve(double* base, const Dims& D)
+{
+    const int n = D.n;
+    ModeMem m;
+    m.y = base;
+    m.u = m.y + n;
+    m.f = m.u + n;
+    m.dT = m.f + n;
+    m.col0 = m.dT + n;
+    m.F1 = m.col0 + n;
+    m.K = m.F1 + n;      // 8n
+    m.A = m.K + 8 * n;   // 7n
+    m.G = m.A + 7 * n;   // 3n
+    m.Z = m.G + 3 * n;   // 3n
+    m.sc = m.Z + 3 * n;  // 32 scalars
+    return m;
+}
+// scalar slots
+enum { SC_W00 = 0, SC_ETAC = 1, SC_CINV = 2, SC_F1Z = 11, SC_F1U = 14, SC_GH = 17 };
+
+DHD double dual_with(double x, double) { return x; }
+DHD Dual dual_with(const Dual& x, double d) { return Dual(x.v, d); }
+
+// ---- RHS f(tau, y) (all entries), T = double or Dual in a ----
+template <class TM, class T>
+DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau,
+                  const double* y, double* f, double* dfda)
+{
+    const int n = D.n;
+    T g0 = 0.0, g1 = 0.0, g2 = 0.0, s1 = 0.0;
+    for (int j = tm.lane; j < n; j += tm.nl) {
+        T gc[3];
+        gcol(P, D, b, k, j, gc);
+        const double yj = y[j];
+        g0 = g0 + gc[0] * yj;
+        g1 = g1 + gc[1] * yj;
+        g2 = g2 + gc[2] * yj;
+        s1 = s1 + f1col(P, D, b, k, j) * yj;
+    }
+    T g[3];
+    g[0] = T(tm.sum(val(g0)));
+    g[1] = T(tm.sum(val(g1)));
+    g[2] = T(tm.sum(val(g2)));
+    T f1s = T(tm.sum(val(s1)));
+    if (dfda) {  // derivative parts of the reductions
+        g[0] = dual_with(g[0], tm.sum(der(g0)));
+        g[1] = dual_with(g[1], tm.sum(der(g1)));
+        g[2] = dual_with(g[2], tm.sum(der(g2)));
+        f1s = dual_with(f1s, tm.sum(der(s1)));
+    }
+    for (int i = tm.lane; i < n; i += tm.nl) {
+        T fi;
+        if (i == 0) {
+            fi = b.aH * b.a;
+        } else if (i == 1) {
+            T u[3];
+            f1u(P, b, k, u);
+            fi = f1s + u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
+        } else {
+            T band[7], etac, u[3];
+            rowc(P, D, b, k, tau, i, band, etac, u);
+            const int s = row_stride(D, i);
+            fi = etac * y[2] + u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
+            for (int m = -3; m <= 3; ++m) {
+                const int jj = i + m * s;
+                if (jj >= 0 && jj < n) fi = fi + band[m + 3] * y[jj];
+            }
+        }
+        f[i] = val(fi);
+        if (dfda) dfda[i] = der(fi);
+    }
+}
+
+// ---- chain LU (no pivoting) and solves ----
+DHD double& bandA(double* A, int i, int m) { return A[7 * i + m + 3]; }
+
+DDV bool factor_chain(double* A, const Chain& ch)
+{
+    bool ok = true;
+    for (int p = 0; p < ch.len; ++p) {
+        const int i = ch.start + p * ch.stride;
+        const double piv = bandA(A, i, 0);
+        if (!(fabs(piv) > 0.0) || !xfinite(piv)) ok = false;
+        const double rp = 1.0 / piv;
+        bandA(A, i, 0) = rp;
+        for (int d = 1; d <= ch.kl && p + d < ch.len; ++d) {
+            const int r = i + d * ch.stride;
+            const double l = bandA(A, r, -d) * rp;
+            bandA(A, r, -d) = l;
+            if (l != 0.0)
+                for (int m = 1; m <= ch.ku && p + m < ch.len; ++m) bandA(A, r, m - d) -= l * bandA(A, i, m);
+        }
+    }
+    return ok;
+}
+
+DDV void solve_chain(const double* A, const Chain& ch, double* z)
+{
+    for (int p = 1; p < ch.len; ++p) {
+        const int i = ch.start + p * ch.stride;
+        double s = z[i];
+        for (int d = 1; d <= ch.kl && p - d >= 0; ++d) s -= A[7 * i + 3 - d] * z[i - d * ch.stride];
+        z[i] = s;
+    }
+    for (int p = ch.len - 1; p >= 0; --p) {
+        const int i = ch.start + p * ch.stride;
+        double s = z[i];
+        for (int m = 1; m <= ch.ku && p + m < ch.len; ++m) s -= A[7 * i + 3 + m] * z[i + m * ch.stride];
+        z[i] = s * A[7 * i + 3];
+    }
+}
+
+// A z = r for rows >= 2 (in place); gh = gamma*h
+template <class TM> DDV void solve_A(const TM& tm, const Dims& D, const ModeMem& M, double gh, double* z)
+{
+    if (tm.leader()) z[2] *= gh;
+    tm.sync();
+    const int nc = n_chains(D);
+    const double etac = M.sc[SC_ETAC];
+    for (int c = tm.lane; c < nc; c += tm.nl) {
+        const Chain ch = chain_of(D, c);
+        if (c == 0) z[6] += etac * z[2];
+        solve_chain(M.A, ch, z);
+    }
+    tm.sync();
+}
+
+// Assemble and factor W at (t, y) for step size h.  Needs M.col0 (d f/d a) already set.
+template <class TM>
+DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<double>& b, double k, double tau,
+                  double h, const ModeMem& M)
+{
+    const int n = D.n;
+    const double gh = kR5.gamma * h;
+    const double igh = 1.0 / gh;
+    for (int i = tm.lane; i < n; i += tm.nl) {
+        double band[7], etac, u[3];
+        if (i >= 2) {
+            rowc(P, D, b, k, tau, i, band, etac, u);
+        } else {
+            for (int m = 0; m < 7; ++m) band[m] = 0.0;
+            etac = 0.0; u[0] = u[1] = u[2] = 0.0;
+        }
+        for (int m = 0; m < 7; ++m) M.A[7 * i + m] = -band[m];
+        M.A[7 * i + 3] += igh;
+        if (i == 6) M.sc[SC_ETAC] = etac;
+        M.Z[i] = u[0];
+        M.Z[n + i] = u[1];
+        M.Z[2 * n + i] = u[2];
+        double gc[3];
+        gcol(P, D, b, k, i, gc);
+        M.G[i] = gc[0];
+        M.G[n + i] = gc[1];
+        M.G[2 * n + i] = gc[2];
+        M.F1[i] = (i >= 2) ? f1col(P, D, b, k, i) : 0.0;
+    }
+    if (tm.leader()) {
+        M.sc[SC_W00] = igh - M.col0[0];
+        double u[3];
+        f1u(P, b, k, u);
+        M.sc[SC_F1U] = u[0];
+        M.sc[SC_F1U + 1] = u[1];
+        M.sc[SC_F1U + 2] = u[2];
+    }
+    tm.sync();
+    bool ok = true;
+    const int nc = n_chains(D);
+    for (int c = tm.lane; c < nc; c += tm.nl) ok = factor_chain(M.A, chain_of(D, c)) && ok;
+    tm.sync();
+    // Z = A^{-1} U
+    for (int r = 0; r < 3; ++r) solve_A(tm, D, M, gh, M.Z + r * n);
+    // C = I - G Z, F1Z = F1 . Z
+    double acc[12];
+    for (int q = 0; q < 12; ++q) acc[q] = 0.0;
+    for (int j = tm.lane; j < n; j += tm.nl) {
+        if (j < 2) continue;
+        for (int r = 0; r < 3; ++r)
+            for (int s = 0; s < 3; ++s) acc[3 * r + s] += M.G[r * n + j] * M.Z[s * n + j];
+        for (int s = 0; s < 3; ++s) acc[9 + s] += M.F1[j] * M.Z[s * n + j];
+    }
+    double C[9];
+    for (int q = 0; q < 9; ++q) C[q] = ((q % 4) == 0 ? 1.0 : 0.0) - tm.sum(acc[q]);
+    double F1Z[3];
+    for (int s = 0; s < 3; ++s) F1Z[s] = tm.sum(acc[9 + s]);
+    // 3x3 inverse by cofactors
+    const double c00 = C[4] * C[8] - C[5] * C[7];
+    const double c01 = C[5] * C[6] - C[3] * C[8];
+    const double c02 = C[3] * C[7] - C[4] * C[6];
+    const double det = C[0] * c00 + C[1] * c01 + C[2] * c02;
+    const double id = 1.0 / det;
+    double Ci[9];
+    Ci[0] = c00 * id;
+    Ci[1] = (C[2] * C[7] - C[1] * C[8]) * id;
+    Ci[2] = (C[1] * C[5] - C[2] * C[4]) * id;
+    Ci[3] = c01 * id;
+    Ci[4] = (C[0] * C[8] - C[2] * C[6]) * id;
+    Ci[5] = (C[2] * C[3] - C[0] * C[5]) * id;
+    Ci[6] = c02 * id;
+    Ci[7] = (C[1] * C[6] - C[0] * C[7]) * id;
+    Ci[8] = (C[0] * C[4] - C[1] * C[3]) * id;
+    if (tm.leader()) {
+        for (int q = 0; q < 9; ++q) M.sc[SC_CINV + q] = Ci[q];
+        for (int s = 0; s < 3; ++s) M.sc[SC_F1Z + s] = F1Z[s];
+    }
+    tm.sync();
+    return ok && xfinite(det) && det != 0.0;
+}
+
+// x = W^{-1} r, in place in v
+template <class TM> DDV void solve_W(const TM& tm, const Dims& D, const ModeMem& M, double h, double* v)
+{
+    const int n = D.n;
+    const double gh = kR5.gamma * h;
+    const double x0 = v[0] / M.sc[SC_W00];
+    tm.sync();
+    for (int i = tm.lane; i < n; i += tm.nl)
+        if (i >= 1) v[i] += M.col0[i] * x0;
+    tm.sync();
+    solve_A(tm, D, M, gh, v);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    for (int j = tm.lane; j < n; j += tm.nl) {
+        if (j < 2) continue;
+        const double zj = v[j];
+        a0 += M.G[j] * zj;
+        a1 += M.G[n + j] * zj;
+        a2 += M.G[2 * n + j] * zj;
+        a3 += M.F1[j] * zj;
+    }
+    const double gz0 = tm.sum(a0), gz1 = tm.sum(a1), gz2 = tm.sum(a2), f1z = tm.sum(a3);
+    const double* Ci = M.sc + SC_CINV;
+    const double c0 = Ci[0] * gz0 + Ci[1] * gz1 + Ci[2] * gz2;
+    const double c1 = Ci[3] * gz0 + Ci[4] * gz1 + Ci[5] * gz2;
+    const double c2 = Ci[6] * gz0 + Ci[7] * gz1 + Ci[8] * gz2;
+    const double r1 = v[1];
+    tm.sync();
+    for (int i = tm.lane; i < n; i += tm.nl)
+        if (i >= 2) v[i] += M.Z[i] * c0 + M.Z[n + i] * c1 + M.Z[2 * n + i] * c2;
+    if (tm.leader()) {
+        const double* F1Z = M.sc + SC_F1Z;
+        const double* F1U = M.sc + SC_F1U;
+        v[1] = gh * (r1 + f1z + (F1Z[0] + F1U[0]) * c0 + (F1Z[1] + F1U[1]) * c1 + (F1Z[2] + F1U[2]) * c2);
+        v[0] = x0;
+    }
+    tm.sync();
+}
+
+DHD int regime_at(const DiscoebCosmo& P, double t, const double* sw)
+{
+    const bool rsa = P.use_rsa && t >= sw[0];
+    const bool ufa = !rsa && P.use_ufa && t >= sw[1];
+    const bool tca = !rsa && P.use_tca && t < sw[2];
+    return (rsa ? 1 : 0) | (ufa ? 2 : 0) | (tca ? 4 : 0);
+}
+
+struct SolveResult {
+    int status, steps, accepted;
+};
+
+// One Rodas5 step from (t, y) with size h: on return M.u + M.K[7] is the candidate and
+// M.K[7] the error estimate.  Returns false on a non-finite factorisation.
+template <class TM>
+DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
+                     const ModeMem& M)
+{
+    const int n = D.n;
+    // Jacobian column d f/d a and f(y) in one dual pass
+    Bg<Dual> bd;
+    bg_eval(P, Dual(M.y[0], 1.0), t, k, regime, bd);
+    rhs_team(tm, P, D, bd, k, t, M.y, M.f, M.col0);
+    Bg<double> b;
+    bg_eval(P, M.y[0], t, k, regime, b);
+    for (int i = tm.lane; i < n; i += tm.nl) M.dT[i] = dtau_row(D, b, t, i, M.y);
+    tm.sync();
+    const bool ok = factor_W(tm, P, D, b, k, t, h, M);
+    const double ih = 1.0 / h;
+    for (int s = 0; s < 8; ++s) {
+        double* Ks = M.K + s * n;
+        if (s > 0) {
+            for (int i = tm.lane; i < n; i += tm.nl) {
+                double v;
+                if (s <= 5) {
+                    v = M.y[i];
+                    for (int j = 0; j < s; ++j) v += kR5.a[s][j] * M.K[j * n + i];
+                } else {
+                    v = M.u[i] + M.K[(s - 1) * n + i];
+                }
+                M.u[i] = v;
+            }
+            tm.sync();
+            const double ts = (s <= 5) ? t + kR5.c[s] * h : t + h;
+            Bg<double> bs;
+            bg_eval(P, M.u[0], ts, k, regime, bs);
+            rhs_team(tm, P, D, bs, k, ts, M.u, M.f, (double*)nullptr);
+            tm.sync();
+        }
+        for (int i = tm.lane; i < n; i += tm.nl) {
+            double r = M.f[i];
+            if (s < 5) r += h * kR5.d[s] * M.dT[i];
+            for (int j = 0; j < s; ++j) r += kR5.C[s][j] * ih * M.K[j * n + i];
+            Ks[i] = r;
+        }
+        tm.sync();
+        solve_W(tm, D, M, h, Ks);
+    }
+    return ok;
+}
+
+// Adaptive solve of one mode: y(t0) in M.y -> outputs at every tout[j] written to
+// yout[j*n ...] (raw state).  sw[3]: RSA start, UFA start, TCA end.
+template <class TM>
+DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, const DiscoebControl& C, double k,
+                           double t0, const double* sw, int nout, const double* tout, const ModeMem& M,
+                           double* yout)
+{
+    const int n = D.n;
+    SolveResult R = {DISCOEB_OK, 0, 0};
+    double t1 = tout[0];
+    for (int j = 1; j < nout; ++j) t1 = tout[j] > t1 ? tout[j] : t1;
+    const double eo = 6.0;  // error order of a 5th-order method
+    const double c1 = (C.icoeff + C.pcoeff + C.dcoeff) / eo;
+    const double c2 = -(C.pcoeff + 2.0 * C.dcoeff) / eo;
+    const double c3 = C.dcoeff / eo;
+    double prev_inv = 1.0, prev_prev_inv = 1.0;
+    double t = t0;
+    double dt = fmin(t0 / 4.0, 0.5 * (t1 - t0));
+    int iout = 0;
+    const int idx[6] = {0, 2, 3, 5, 6, 7};
+    const double w6[6] = {1.0, k * k, 1.0, 1.0, 1.0 / (k * k), 1.0};
+    while (t < t1) {
+        if (R.steps >= C.max_steps) { R.status = DISCOEB_MAX_STEPS; break; }
+        double tev = t1;
+        if (iout < nout && tout[iout] < tev) tev = tout[iout];
+        for (int q = 0; q < 3; ++q)
+            if (sw[q] > t && sw[q] < tev) tev = sw[q];
+        const double dt_try = dt;
+        double tn = t + dt;
+        bool clipped = false;
+        if (tn >= tev - 1e-12 * fabs(tev)) { clipped = tn > tev; tn = tev; }
+        const double h = tn - t;
+        if (!(h > 1e-14 * fabs(t))) { R.status = DISCOEB_DT_UNDERFLOW; break; }
+        const int regime = regime_at(P, t, sw);
+        const bool ok = rodas5_step(tm, P, D, k, t, h, regime, M);
+        R.steps++;
+        // error norm (perturbations.py:855-878 with the weights of :913)
+        double sumsq = 0.0;
+        bool finite = ok;
+        for (int q = 0; q < 6; ++q) {
+            const int i = idx[q];
+            const double y1 = M.u[i] + M.K[7 * n + i];
+            const double sc = fmax(fabs(M.y[i]), fabs(y1));
+            const double e = M.K[7 * n + i] / (C.atol + C.rtol * sc) * w6[q];
+            sumsq += e * e;
+            if (!xfinite(y1)) finite = false;
+        }
+        double lf = 0.0;
+        for (int i = tm.lane; i < n; i += tm.nl) lf += xfinite(M.u[i] + M.K[7 * n + i]) ? 0.0 : 1.0;
+        if (tm.sum(lf) > 0.0) finite = false;
+        const double err = finite ? sqrt(sumsq / 6.0) : INFINITY;
+        const bool keep = err < 1.0;
+        double inv = 1.0 / err;
+        const double f1 = pow(inv, c1);
+        const double f2 = (c2 == 0.0) ? 1.0 : pow(prev_inv, c2);
+        const double f3 = (c3 == 0.0) ? 1.0 : pow(prev_prev_inv, c3);
+        const double fmn = keep ? 1.0 : C.factormin;
+        double factor = 0.9 * f1 * f2 * f3;
+        if (!(factor == factor)) factor = fmn;
+        factor = fmin(fmax(factor, fmn), C.factormax);
+        if (inv == 0.0 || !xfinite(inv)) inv = 1.0;
+        double dtn = h * factor;
+        tm.sync();
+        if (keep) {
+            R.accepted++;
+            for (int i = tm.lane; i < n; i += tm.nl) M.y[i] = M.u[i] + M.K[7 * n + i];
+            tm.sync();
+            t = tn;
+            while (iout < nout && tout[iout] <= t) {
+                for (int i = tm.lane; i < n; i += tm.nl) yout[(size_t)iout * n + i] = M.y[i];
+                iout++;
+            }
+            if (clipped && dt_try > dtn) dtn = dt_try;
+            prev_prev_inv = prev_inv;
+            prev_inv = inv;
+        }
+        dt = dtn;
+        tm.sync();
+    }
+    if (R.status == DISCOEB_OK && iout < nout) R.status = DISCOEB_MAX_STEPS;
+    return R;
+}
+
+}  // namespace dscb

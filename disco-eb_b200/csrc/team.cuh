@@ -1,0 +1,34 @@
+// A "team" is the group of threads that owns one k-mode: one warp on the GPU.  The same
+// stepper source also compiles for a single host thread (HostTeam) so that its algebra
+// can be unit-tested on a CPU against the oracle.  Loops over state entries are written
+// as `for (i = T.lane; i < n; i += T.nl)`, with T.sync() between phases.
+#pragma once
+
+#include "dual.cuh"
+
+namespace dscb {
+
+#if defined(__CUDACC__)
+struct WarpTeam {
+    int lane;
+    static constexpr int nl = 32;
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    __device__ __forceinline__ double sum(double x) const
+    {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        return x;
+    }
+    __device__ __forceinline__ bool leader() const { return lane == 0; }
+};
+#endif
+
+struct HostTeam {
+    int lane = 0;
+    static constexpr int nl = 1;
+    DHD void sync() const {}
+    DHD double sum(double x) const { return x; }
+    DHD bool leader() const { return true; }
+};
+
+}  // namespace dscb

@@ -1,0 +1,152 @@
+"""ctypes mirror of ``include/discoeb.h`` and the loader of the CUDA library.
+
+The shared library ``libdiscoeb_b200.so`` is built in-tree by ``build.py``.  There is
+no CPU fallback: if the library (or a GPU) is missing, the entry points raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+MAX_NQ = 16
+ABI_VERSION = 1
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_NAME = "libdiscoeb_b200.so"
+LIB_PATH = os.path.join(HERE, LIB_NAME)
+
+METHOD_RODAS5_STRUCTURED = 0
+METHOD_RODAS5_DENSE = 1
+METHOD_RODAS5_DENSE_MIXED = 2
+
+STATUS_NAMES = {0: "ok", 1: "max_steps exceeded", 2: "non-finite state", 3: "step size underflow", 4: "singular"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class DiscoebSpline(ctypes.Structure):
+    _fields_ = [("n_knots", ctypes.c_int32), ("uniform", ctypes.c_int32),
+                ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("S", ctypes.c_void_p)]
+
+
+class DiscoebCosmo(ctypes.Structure):
+    _fields_ = ([(f, ctypes.c_int32) for f in ("lmaxg", "lmaxgp", "lmaxr", "lmaxnu", "nqmax",
+                                                "use_tca", "use_rsa", "use_ufa")]
+                + [(f, ctypes.c_double) for f in ("tca_tau_c_over_tau_h", "tca_tau_c_over_tau_k",
+                                                   "rsa_tau_c_over_tau", "rsa_tau_over_tau_k", "ufa_tau_over_tau_k",
+                                                   "grhom", "grhog", "grhor", "Omegam", "Omegab", "OmegaDE", "Omegak",
+                                                   "Neff", "Nmnu", "amnu", "w0", "wa", "cs2_DE", "YHe", "H0",
+                                                   "de_guard_eps")]
+                + [("q", ctypes.c_double * MAX_NQ), ("wq", ctypes.c_double * MAX_NQ)]
+                + [(f, DiscoebSpline) for f in ("xe_loga", "cs2a_loga", "logrhonu_loga", "logpnu_loga")])
+
+
+class DiscoebControl(ctypes.Structure):
+    _fields_ = ([(f, ctypes.c_double) for f in ("rtol", "atol", "pcoeff", "icoeff", "dcoeff", "factormax", "factormin")]
+                + [(f, ctypes.c_int32) for f in ("max_steps", "method", "warps_per_block", "reserved")])
+
+
+def nvar(lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax):
+    return 7 + (lmaxg + 1) + (lmaxgp + 1) + (lmaxr + 1) + nqmax * (lmaxnu + 1) + 2
+
+
+def approximation_settings(param):
+    """Defaults of get_approximation_settings (src/discoeb/approximations.py:9-20)."""
+    return {
+        "use_tca": bool(param.get("use_tca", False)),
+        "tca_tau_c_over_tau_h_trigger": float(param.get("tca_tau_c_over_tau_h_trigger", 0.015)),
+        "tca_tau_c_over_tau_k_trigger": float(param.get("tca_tau_c_over_tau_k_trigger", 0.010)),
+        "use_rsa": bool(param.get("use_rsa", True)),
+        "tau_c_over_tau_trigger": float(param.get("rsa_tau_c_over_tau_trigger", 10.0)),
+        "tau_over_tau_k_trigger": float(param.get("rsa_tau_over_tau_k_trigger", 80.0)),
+        "use_ur_fluid": bool(param.get("use_ur_fluid", True)),
+        "ur_fluid_tau_over_tau_k_trigger": float(param.get("ur_fluid_tau_over_tau_k_trigger", 120.0)),
+    }
+
+
+def make_cosmo(param, *, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, de_guard_eps, table_ptrs):
+    """Fill a DiscoebCosmo from a background ``param`` dict.
+
+    ``table_ptrs`` maps spline keys to (n, uniform, x_ptr, y_ptr, S_ptr) with pointers
+    valid where the struct is consumed (device pointers for the CUDA library).
+    """
+    from .background import get_neutrino_momentum_bins
+    if nqmax > MAX_NQ:
+        raise ValueError(f"nqmax={nqmax} exceeds the supported maximum {MAX_NQ}")
+    if min(lmaxg, lmaxgp, lmaxr, lmaxnu) < 3:
+        raise ValueError("lmaxg, lmaxgp, lmaxr and lmaxnu must be >= 3")
+    s = approximation_settings(param)
+    c = DiscoebCosmo()
+    c.lmaxg, c.lmaxgp, c.lmaxr, c.lmaxnu, c.nqmax = lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax
+    c.use_tca = int(s["use_tca"])
+    c.use_rsa = int(s["use_rsa"])
+    c.use_ufa = int(s["use_ur_fluid"])
+    c.tca_tau_c_over_tau_h = s["tca_tau_c_over_tau_h_trigger"]
+    c.tca_tau_c_over_tau_k = s["tca_tau_c_over_tau_k_trigger"]
+    c.rsa_tau_c_over_tau = s["tau_c_over_tau_trigger"]
+    c.rsa_tau_over_tau_k = s["tau_over_tau_k_trigger"]
+    c.ufa_tau_over_tau_k = s["ur_fluid_tau_over_tau_k_trigger"]
+    for f in ("grhom", "grhog", "grhor", "Omegam", "Omegab", "OmegaDE", "Omegak", "Neff", "Nmnu", "amnu",
+              "cs2_DE", "YHe", "H0"):
+        setattr(c, f, float(param[f]))
+    c.w0 = float(param["w_DE_0"])
+    c.wa = float(param["w_DE_a"])
+    c.de_guard_eps = float(de_guard_eps)
+    q, w = get_neutrino_momentum_bins(nqmax)
+    for i in range(nqmax):
+        c.q[i] = float(q[i])
+        c.wq[i] = float(w[i])
+    for name, key in (("xe_loga", "xe_of_loga_spline"), ("cs2a_loga", "cs2a_of_loga_spline"),
+                      ("logrhonu_loga", "logrhonu_of_loga_spline"), ("logpnu_loga", "logpnu_of_loga_spline")):
+        n, uni, xp, yp, sp = table_ptrs[key]
+        setattr(c, name, DiscoebSpline(n, uni, xp, yp, sp))
+    return c
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_NAME} not found at {LIB_PATH}: build it with disco-eb_b200/build.py "
+                               "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.discoeb_abi_version.restype = ctypes.c_int32
+        L.discoeb_nvar.argtypes = [ctypes.POINTER(DiscoebCosmo)]
+        L.discoeb_nvar.restype = ctypes.c_int32
+        vp = ctypes.c_void_p
+        L.discoeb_fwd.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, ctypes.POINTER(DiscoebControl),
+                                  ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp, vp]
+        L.discoeb_fwd.restype = ctypes.c_int32
+        L.discoeb_rhs.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, vp, vp, vp, ctypes.c_int32, vp, vp]
+        L.discoeb_rhs.restype = ctypes.c_int32
+        if L.discoeb_abi_version() != ABI_VERSION:
+            raise RuntimeError("libdiscoeb_b200.so ABI version mismatch; rebuild it")
+        _lib = L
+    return _lib
+
+
+def host_table_ptrs(param, keep):
+    """Table pointers into host numpy arrays (for the CPU model test harness)."""
+    out = {}
+    for key in ("xe_of_loga_spline", "cs2a_of_loga_spline", "logrhonu_of_loga_spline", "logpnu_of_loga_spline"):
+        s = param[key]
+        arrs = [np.ascontiguousarray(s.x, dtype=np.float64), np.ascontiguousarray(s.y, dtype=np.float64),
+                np.ascontiguousarray(s.S, dtype=np.float64)]
+        keep.extend(arrs)
+        out[key] = (s.n, int(s.uniform), arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data)
+    # xe and cs2*a are tabulated on the same knots: share the x pointer so the kernel does one search
+    xe, cs = param["xe_of_loga_spline"], param["cs2a_of_loga_spline"]
+    if xe.n == cs.n and np.array_equal(xe.x, cs.x):
+        n, u, _, yp, sp = out["cs2a_of_loga_spline"]
+        out["cs2a_of_loga_spline"] = (n, u, out["xe_of_loga_spline"][2], yp, sp)
+    rn, rp = param["logrhonu_of_loga_spline"], param["logpnu_of_loga_spline"]
+    if rn.n == rp.n and np.array_equal(rn.x, rp.x):
+        n, u, _, yp, sp = out["logpnu_of_loga_spline"]
+        out["logpnu_of_loga_spline"] = (n, u, out["logrhonu_of_loga_spline"][2], yp, sp)
+    return out

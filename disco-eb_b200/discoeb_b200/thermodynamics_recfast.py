@@ -1,0 +1,440 @@
+"""Recfast recombination history (host side, float64 numpy).
+
+Restates ``src/discoeb/thermodynamics_recfast.py`` of the reference: the three-variable
+Recfast ODE (x_H, x_He, T_mat) of Seager, Sasselov & Scott (1999, 2000) with the
+Wong, Moss & Scott (2008) fudges, integrated interval by interval on the adaptive
+a-grid with the Kaps-Rentrop GRK4A Rosenbrock method and a PI step controller,
+plus the Saha HeII correction.  This is the producer of the ``xe`` and ``c_s^2``
+tables that the perturbation kernels read; it is not on the device path.
+
+The Jacobian of the GRK4A step is taken by complex-step differentiation, which gives
+the exact derivative to rounding, as the reference's forward-mode ``jacfwd`` does.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .romberg import romb
+
+# physical constants (thermodynamics_recfast.py:38-53)
+const_G = 6.67430e-11
+const_mH = 1.67353284e-27
+const_me = 9.1093837015e-31
+const_mHe_mH = 3.97146570884
+const_c = 2.99792458e08
+const_h = 6.62607015e-34
+const_kB = 1.380649e-23
+const_sigma = 6.6524587321e-29
+const_arad = 4 * 5.670374419e-8 / const_c
+bigH = 3.2407792902755102e-18
+const_dens_fac = 11.223810928601939
+const_c2ok = 1.62581581e4
+const_c_Mpc_s = 9.71561189e-15
+const_EionHe12s = 6.314878282674e5
+
+# atomic data (thermodynamics_recfast.py:57-122)
+Lambda = 8.2245809
+Lambda_He = 51.3
+L_H_ion = 1.096787737e7
+L_H_alpha = 8.225916453e6
+L_He1_ion = 1.98310772e7
+L_He2_ion = 4.389088863e7
+L_He_2s = 1.66277434e7
+L_He_2p = 1.71134891e7
+A2P_s = 1.798287e9
+A2P_t = 177.58
+L_He_2Pt = 1.690871466e7
+L_He_2St = 1.5985597526e7
+L_He2St_ion = 3.8454693845e6
+sigma_He_2Ps = 1.436289e-22
+sigma_He_2Pt = 1.484872e-22
+AGauss1 = -0.14
+AGauss2 = 0.05
+zGauss1 = 7.28
+zGauss2 = 6.75
+wGauss1 = 0.18
+wGauss2 = 0.33
+H_frac = 1.0e-3
+
+Lalpha = 1.0 / L_H_alpha
+Lalpha_He = 1.0 / L_He_2p
+DeltaB = const_h * const_c * (L_H_ion - L_H_alpha)
+CDB = DeltaB / const_kB
+DeltaB_He = const_h * const_c * (L_He1_ion - L_He_2s)
+CDB_He = DeltaB_He / const_kB
+CB1 = const_h * const_c * L_H_ion / const_kB
+CB1_He1 = const_h * const_c * L_He1_ion / const_kB
+CB1_He2 = const_h * const_c * L_He2_ion / const_kB
+CR = 2.0 * math.pi * (const_me / const_h) * (const_kB / const_h)
+CK = Lalpha**3 / (8.0 * math.pi)
+CK_He = Lalpha_He**3 / (8.0 * math.pi)
+CL = const_c * const_h / (const_kB * Lalpha)
+CL_He = const_c * const_h / (const_kB / L_He_2s)
+CT = (8.0 / 3.0) * (const_sigma / (const_me * const_c)) * const_arad
+Bfact = const_h * const_c * (L_He_2p - L_He_2s) / const_kB
+CL_PSt = const_h * const_c * (L_He_2Pt - L_He_2St) / const_kB
+const_h_c_L_He_2St_kB = const_h * const_c * L_He_2St / const_kB
+
+a_PPB = 4.309
+b_PPB = -0.6166
+c_PPB = 0.6703
+d_PPB = 0.5300
+a_VF = 10.0 ** (-16.744)
+b_VF = 0.711
+T_0 = 10 ** 0.477121
+T_1 = 10 ** 5.114
+a_trip = 10.0 ** (-16.306)
+b_trip = 0.761
+
+
+def _re(x):
+    return np.real(x)
+
+
+def ionization(a, y, param, aprimeoa):
+    """d(x_H, x_He, T_mat)/da (thermodynamics_recfast.py:124-281).
+
+    ``y`` may be complex (complex-step Jacobian) and may carry trailing batch axes;
+    comparisons use the real part.  ``aprimeoa`` is the conformal Hubble rate at
+    ``a`` (``get_aprimeoa``), passed in because it only depends on ``a``.
+    """
+    with np.errstate(all="ignore"):
+        return _ionization(a, y, param, aprimeoa)
+
+
+def _ionization(a, y, param, aprimeoa):
+    z = 1.0 / a - 1.0
+    H = param["H0"] / 100.0
+    HO = H * bigH
+    fu = 1.105
+    mu_H = 1.0 / (1.0 - param["YHe"])
+    fHe = param["YHe"] / (const_mHe_mH * (1.0 - param["YHe"]))
+    Nnow = const_dens_fac * H * H * param["Omegab"] / mu_H
+
+    x_H = y[0]
+    x_He = y[1]
+    x = x_H + fHe * x_He
+    Tmat = np.where(_re(y[2]) >= 0, y[2], -y[2])
+
+    n = Nnow * (1 + z) ** 3
+    n_He = fHe * n
+    Trad = param["Tcmb"] * (1 + z)
+    z_term = 1 + z
+    Hz = (1e-5 * aprimeoa) / a * const_c * bigH
+
+    Tmat_1e4 = Tmat / 1e4
+    CR_Tmat_15 = (CR * Tmat) ** 1.5
+    Rdown = 1e-19 * a_PPB * Tmat_1e4**b_PPB / (1 + c_PPB * Tmat_1e4**d_PPB)
+    Rup = Rdown * CR_Tmat_15 * np.exp(-CDB / Tmat)
+
+    sq_0 = np.sqrt(Tmat / T_0)
+    sq_1 = np.sqrt(Tmat / T_1)
+    sq_0_term = 1 + sq_0
+    sq_1_term = 1 + sq_1
+    Rdown_He = a_VF / (sq_0 * sq_0_term ** (1 - b_VF) * sq_1_term ** (1 + b_VF))
+    Rup_He = 4 * Rdown_He * CR_Tmat_15 * np.exp(-CDB_He / Tmat)
+
+    bt = Bfact / Tmat
+    He_Boltz = np.exp(np.where(_re(bt) < 680.0, bt, 680.0))
+
+    Rdown_trip = a_trip / (sq_0 * sq_0_term ** (1 - b_trip) * sq_1_term ** (1 + b_trip))
+    Rup_trip = Rdown_trip * np.exp(-const_h * const_c * L_He2St_ion / (const_kB * Tmat)) * CR_Tmat_15 * (4 / 3)
+
+    lz = math.log(z_term)
+    K_gaussian = 1 + AGauss1 * math.exp(-(((lz - zGauss1) / wGauss1) ** 2)) + AGauss2 * math.exp(-(((lz - zGauss2) / wGauss2) ** 2))
+    K = CK / Hz * K_gaussian
+
+    one_minus_x_He = 1 - x_He
+    one_minus_x_H = 1 - x_H
+    n_He_1_minus_x_He = n_He * one_minus_x_He
+
+    tauHe_s = A2P_s * CK_He * 3 * n_He_1_minus_x_He / Hz
+    pHe_s = (1 - np.exp(-tauHe_s)) / tauHe_s
+
+    Doppler_term = np.sqrt(2 * const_kB * Tmat / (const_mH * const_mHe_mH * const_c**2))
+    Doppler_2p = const_c * L_He_2p * Doppler_term
+    Doppler_2Pt = const_c * L_He_2Pt * Doppler_term
+
+    gamma_2Ps_term = 3 * A2P_s * fHe * one_minus_x_He * const_c**2
+    gamma_2Ps_denom = math.sqrt(math.pi) * sigma_He_2Ps * 8 * math.pi * Doppler_2p * one_minus_x_H * (const_c * L_He_2p) ** 2
+    gamma_2Ps = gamma_2Ps_term / gamma_2Ps_denom
+
+    pb = 0.36
+    qb = 0.86
+    AHcon = A2P_s / (1 + pb * (gamma_2Ps**qb))
+
+    K_He_cond1 = (_re(x_He) < 5e-9) | (_re(x_He) > 0.98)
+    K_He_cond2 = _re(x_H) < 0.9999999
+    K_He_default = CK_He / Hz
+    K_He_case1 = 1.0 / ((A2P_s * pHe_s + AHcon) * 3.0 * n_He_1_minus_x_He)
+    K_He_case2 = 1.0 / (A2P_s * pHe_s * 3.0 * n_He_1_minus_x_He)
+    K_He = np.where(K_He_cond1, K_He_default, np.where(K_He_cond2, K_He_case1, K_He_case2))
+
+    tauHe_t = A2P_t * n_He_1_minus_x_He * 3 / (8 * math.pi * Hz * L_He_2Pt**3)
+    pHe_t = (1 - np.exp(-tauHe_t)) / tauHe_t
+    gamma_2Pt_term = 3 * A2P_t * fHe * one_minus_x_He * const_c**2
+    gamma_2Pt_denom = math.sqrt(math.pi) * sigma_He_2Pt * 8 * math.pi * Doppler_2Pt * one_minus_x_H * (const_c * L_He_2Pt) ** 2
+    gamma_2Pt = gamma_2Pt_term / gamma_2Pt_denom
+    pb_t = 0.66
+    qb_t = 0.9
+    AHcon_t = A2P_t / (1 + pb_t * gamma_2Pt**qb_t) / 3
+
+    exp_CL_PSt = np.exp(-CL_PSt / Tmat)
+    CfHe_t_case1 = A2P_t * pHe_t * exp_CL_PSt
+    CfHe_t_case2 = (A2P_t * pHe_t + AHcon_t) * exp_CL_PSt
+    CfHe_t = np.where(_re(x_H) > 0.99999, CfHe_t_case1, CfHe_t_case2)
+    CfHe_t = CfHe_t / (Rup_trip + CfHe_t)
+
+    timeTh = (1 / (CT * Trad**4)) * (1 + x + fHe) / x
+    timeH = 2 / (3 * HO * z_term**1.5)
+
+    Hz_z_term = Hz * z_term
+    x_x_H_n_Rdown = x * x_H * n * Rdown
+    Rup_1_minus_x_H_exp_CL = Rup * one_minus_x_H * np.exp(-CL / Tmat)
+    rate_diff = x_x_H_n_Rdown - Rup_1_minus_x_H_exp_CL
+    K_Lambda_n_1_minus_x_H = K * Lambda * n * one_minus_x_H
+    denom_term = 1 / fu + K_Lambda_n_1_minus_x_H / fu + K * Rup * n * one_minus_x_H
+    f0_case2 = rate_diff / Hz_z_term
+    f0_case3 = (rate_diff * (1 + K_Lambda_n_1_minus_x_H)) / (Hz_z_term * denom_term)
+    f0 = np.where(_re(x_H) > 0.99, 0.0 * x_H, np.where(_re(x_H) > 0.985, f0_case2, f0_case3))
+
+    x_x_He_n_Rdown_He = x * x_He * n * Rdown_He
+    Rup_He_term = Rup_He * one_minus_x_He * np.exp(-CL_He / Tmat)
+    rate_diff_He = x_x_He_n_Rdown_He - Rup_He_term
+    K_He_LHe = K_He * Lambda_He * n_He_1_minus_x_He * He_Boltz
+    He_denom_term = 1 + K_He * (Lambda_He + Rup_He) * n_He_1_minus_x_He * He_Boltz
+    f1_main = (rate_diff_He * (1 + K_He_LHe)) / (Hz_z_term * He_denom_term)
+    trip_rate_diff = x * x_He * n * Rdown_trip - one_minus_x_He * 3 * Rup_trip * np.exp(-const_h_c_L_He_2St_kB / Tmat)
+    trip_contrib = trip_rate_diff * CfHe_t / Hz_z_term
+    trip_cond = (_re(x_He) < 5e-9) | (_re(x_He) > 0.98)
+    f1 = np.where(_re(x_He) < 1e-8, 0.0 * x_He, f1_main + np.where(trip_cond, 0.0 * x_He, trip_contrib))
+
+    f2_case1 = Tmat / z_term
+    f2_case2 = CT * (Trad**4) * x / (1 + x + fHe) * (Tmat - Trad) / Hz_z_term + 2 * Tmat / z_term
+    f2 = np.where(_re(timeTh) < H_frac * timeH, f2_case1, f2_case2)
+
+    dzda = -1.0 / a**2
+    return np.stack([f0 * dzda, f1 * dzda, f2 * dzda])
+
+
+# Kaps & Rentrop (1979) GRK4A coefficients (thermodynamics via ode_integrators_stiff.py:176-196)
+_G = dict(gamma=0.395, gamma21=-0.767672395484, gamma31=-0.851675323742, gamma32=0.522967289188,
+          gamma41=0.288463109545, gamma42=0.880214273381e-1, gamma43=-0.337389840627,
+          alpha21=0.438, alpha31=0.796920457938, alpha32=0.730795420615e-1,
+          chat1=0.346325833758, chat2=0.285693175712, chat3=0.367980990530,
+          c1=0.199293275701, c2=0.482645235674, c3=0.680614886256e-1, c4=0.25)
+
+
+def _lu3(A):
+    """No-pivot 3x3 LU (ode_integrators_stiff.py:77-96)."""
+    u00, u01, u02 = A[0, 0], A[0, 1], A[0, 2]
+    l10 = A[1, 0] / u00
+    u11 = A[1, 1] - l10 * u01
+    u12 = A[1, 2] - l10 * u02
+    l20 = A[2, 0] / u00
+    r21 = A[2, 1] - l20 * u01
+    r22 = A[2, 2] - l20 * u02
+    l21 = r21 / u11
+    u22 = r22 - l21 * u12
+    return (u00, u01, u02, l10, u11, u12, l20, l21, u22)
+
+
+def _lu3_solve(f, b):
+    u00, u01, u02, l10, u11, u12, l20, l21, u22 = f
+    y0 = b[0]
+    y1 = b[1] - l10 * y0
+    y2 = b[2] - l20 * y0 - l21 * y1
+    x2 = y2 / u22
+    x1 = (y1 - u12 * x2) / u11
+    x0 = (y0 - u01 * x1 - u02 * x2) / u00
+    return np.array([x0, x1, x2])
+
+
+def _grk4a_step(fun, t0, t1, y0):
+    """One GRK4A step (ode_integrators_stiff.py:157-254); all stages at t0 as the reference."""
+    g = _G
+    dt = t1 - t0
+    h = 1e-40
+    # J = d(dt*f)/dy by complex step (three columns at once)
+    Y = y0[:, None] + 1j * h * np.eye(3)
+    J = np.imag(fun(t0, Y)) / h * dt
+    A = np.eye(3) - g["gamma"] * J
+    lu = _lu3(A)
+    b1 = dt * fun(t0, y0)
+    k1 = _lu3_solve(lu, b1)
+    y1 = y0 + g["alpha21"] * k1
+    f1 = dt * fun(t0, y1)
+    Jk1 = J @ k1
+    k2 = _lu3_solve(lu, f1 + g["gamma21"] * Jk1)
+    y2 = y0 + g["alpha31"] * k1 + g["alpha32"] * k2
+    f2 = dt * fun(t0, y2)
+    Jk2 = J @ k2
+    k3 = _lu3_solve(lu, f2 + g["gamma31"] * Jk1 + g["gamma32"] * Jk2)
+    Jk3 = J @ k3
+    k4 = _lu3_solve(lu, f2 + g["gamma41"] * Jk1 + g["gamma42"] * Jk2 + g["gamma43"] * Jk3)
+    y_new = y0 + g["c1"] * k1 + g["c2"] * k2 + g["c3"] * k3 + g["c4"] * k4
+    y_err = (g["c1"] - g["chat1"]) * k1 + (g["c2"] - g["chat2"]) * k2 + (g["c3"] - g["chat3"]) * k3 + g["c4"] * k4
+    return y_new, y_err
+
+
+def _clip_to_end(tprev, tnext, t1, keep):
+    tol = 1e-10 * abs(tnext)
+    if tnext > t1 - tol:
+        return t1 if keep else tprev + 0.5 * (t1 - tprev)
+    return tnext
+
+
+def solve_pid_grk4a(fun, t0, t1, y0, dt0, rtol, atol, max_steps):
+    """Adaptive GRK4A solve with an integral controller (diffrax ``PIDController``
+    defaults: icoeff=1, pcoeff=dcoeff=0, safety 0.9, factor in [0.2, 10],
+    RMS norm, error order 3).  Returns y(t1) (``throw=False``: the last accepted
+    state is returned when ``max_steps`` is exhausted)."""
+    t = t0
+    y = np.array(y0, dtype=np.float64)
+    tn = _clip_to_end(t0, t0 + dt0, t1, True)
+    for _ in range(max_steps):
+        if not (t < t1):
+            break
+        y1, yerr = _grk4a_step(fun, t, tn, y)
+        sc = yerr / (atol + rtol * np.maximum(np.abs(y), np.abs(y1)))
+        err = math.sqrt(float(np.mean(sc * sc)))
+        keep = err < 1.0
+        inv = 1.0 / err if err > 0 else math.inf
+        factor = 0.9 * inv ** (1.0 / 3.0) if math.isfinite(inv) else 10.0
+        fmin = 1.0 if keep else 0.2
+        factor = min(max(factor, fmin), 10.0)
+        dt = (tn - t) * factor
+        if keep:
+            t, y = tn, y1
+        tn = _clip_to_end(t, t + dt, t1, keep)
+    return y
+
+
+def Saha_HeII(a, param):
+    """Saha HeII electron fraction (thermodynamics_recfast.py:303-322); ``a`` may be complex."""
+    const_Hfac = 1 / (1.0e06 * 3.0856775807e13)
+    mu_H = 1 / (1 - param["YHe"])
+    rho_c = 3 * (param["H0"] * const_Hfac) ** 2 / (8 * math.pi * const_G)
+    NH = rho_c * param["Omegab"] / (const_mH * mu_H) / a**3
+    T = param["Tcmb"] / a
+    betaE = const_EionHe12s / T
+    fHe = param["fHe"]
+    A = 1 + fHe
+    B = 1 + 2 * fHe
+    R = (2 * math.pi * const_me * const_kB / const_h**2 * T) ** 1.5 / NH * np.exp(-betaE)
+    with np.errstate(all="ignore"):
+        big = fHe * (1 - B / R + (1 + 5 * fHe + 6 * fHe**2) / R**2)
+        small = -(R - A) / 2 + np.sqrt((R - A) ** 2 / 4 + R * B) - A
+    return np.where(np.real(R) > 1e5, big, small)
+
+
+def _get_adaptive_sampling(a0, a1, N):
+    """Four geometric segments concentrated on recombination (thermodynamics_recfast.py:325-361)."""
+    n_very_early = max(8, int(N * 0.05))
+    n_pre = max(8, int(N * 0.10))
+    n_rec = int(N * 0.50)
+    n_post = N - n_very_early - n_pre - n_rec
+    ab1 = max(1.0 / (1.0 + 10000), a0)
+    ab2 = 1.0 / (1.0 + 1400)
+    ab3 = 1.0 / (1.0 + 600)
+    return np.concatenate([
+        np.geomspace(a0, ab1, n_very_early, endpoint=False),
+        np.geomspace(ab1, ab2, n_pre, endpoint=False),
+        np.geomspace(ab2, ab3, n_rec, endpoint=False),
+        np.geomspace(ab3, a1, n_post),
+    ])
+
+
+def compute_thermal_history(*, a0, a1, N, param, aprimeoa_fn, rtol=1e-3, atol=1e-6):
+    """Interval-by-interval ionisation history (thermodynamics_recfast.py:363-453).
+
+    Returns ``y[6, N]`` = (x_H, x_He, T_m, dx_H/da, dx_He/da, dT_m/da) at ``a[1:]``.
+    """
+    a = _get_adaptive_sampling(a0, a1, N + 1)
+    y = np.zeros((6, N))
+    H = param["H0"] / 100.0
+    HO = H * bigH
+    mu_H = 1.0 / (1.0 - param["YHe"])
+    Nnow = 3.0 * HO * HO * param["Omegab"] / (8.0 * math.pi * const_G * mu_H * const_mH)
+    fHe = param["YHe"] / (const_mHe_mH * (1.0 - param["YHe"]))
+    Tcmb = param["Tcmb"]
+    Tcmb3 = Tcmb**3
+
+    def fun(t, yy):
+        return ionization(t, yy, param, aprimeoa_fn(t))
+
+    for i in range(N):
+        astart = a[i]
+        zstart = 1.0 / astart - 1.0
+        aend = a[i + 1]
+        zend = 1.0 / aend - 1.0
+        dzda = -1.0 / aend**2
+        if i > 0:
+            y_prev = y[:, i - 1].copy()
+        else:
+            y_prev = np.array([1.0, 1.0, Tcmb * (1.0 + zstart), 0.0, 0.0, -Tcmb * (1.0 + zstart)])
+        if zend > 3500.0:
+            new = np.array([1.0, 1.0, Tcmb * (1.0 + zend), 0.0, 0.0, -Tcmb * (1.0 + zend)])
+        elif i > 0 and y_prev[1] > 0.99:
+            rhs = (math.exp(1.5 * math.log(CR * Tcmb / (1.0 + zend)) - CB1_He1 / (Tcmb * (1.0 + zend))) / Nnow) * 4.0
+            x_He0 = 0.5 * (math.sqrt((rhs - 1.0) ** 2 + 4.0 * (1.0 + fHe) * rhs) - (rhs - 1.0))
+            q = -((CB1_He1 - CR * Tcmb**2) / (Tcmb * (1 + zend)))
+            dxHeIdz = ((-3 * (-(CB1_He1 / Tcmb) + CR * Tcmb) ** 1.5 * (Nnow + 2 * fHe * Nnow + 4 * q**1.5
+                        - math.sqrt(Nnow**2 + (16 * (-CB1_He1 + CR * Tcmb**2) ** 3) / (Tcmb3 * (1 + zend) ** 3)
+                                    + 8 * (1 + 2 * fHe) * Nnow * q**1.5)))
+                       / (Nnow * (1 + zend) ** 2.5 * math.sqrt(Nnow**2 + (16 * (-CB1_He1 + CR * Tcmb**2) ** 3)
+                                                                / (Tcmb**3 * (1 + zend) ** 3)
+                                                                + 8 * (1 + 2 * fHe) * Nnow
+                                                                * (-((CB1_He1 - CR * Tcmb**2) / (Tcmb + Tcmb * zend))) ** 1.5)))
+            new = np.array([1.0, (x_He0 - 1.0) / fHe, Tcmb * (1.0 + zend), 0.0, dxHeIdz * dzda, -Tcmb * (1.0 + zend)])
+        elif i > 0 and y_prev[0] > 0.99:
+            rhs = math.exp(1.5 * math.log(CR * Tcmb / (1.0 + zend)) - CB1 / (Tcmb * (1.0 + zend))) / Nnow
+            x_H0 = 0.5 * (math.sqrt(rhs**2 + 4.0 * rhs) - rhs)
+            q = -((CB1 - CR * Tcmb**2) / (Tcmb * (1 + zend)))
+            dxHdz = ((3 * ((2 * q**1.5) / (1 + zend)
+                           + ((CB1 - CR * Tcmb**2) * (2 * CB1**2 - 4 * CB1 * CR * Tcmb**2 + Tcmb**2
+                                                      * (2 * CR**2 * Tcmb**2 + Nnow * (1 + zend) ** 2 * math.sqrt(q))))
+                           / (Tcmb**1.5 * (1 + zend) ** 2.5 * math.sqrt((-CB1 + CR * Tcmb**2)
+                              * (CB1**2 - 2 * CB1 * CR * Tcmb**2 + Tcmb**2 * (CR**2 * Tcmb**2 + Nnow * (1 + zend) ** 2
+                                                                          * math.sqrt(q)))))))
+                     / (2.0 * Nnow))
+            new = _solve_ionization(fun, astart, aend, y_prev, rtol, atol)
+            new[0] = x_H0
+            new[3] = dxHdz * dzda
+        else:
+            new = _solve_ionization(fun, astart, aend, y_prev, rtol, atol)
+        y[:, i] = new
+    return y, a[1:]
+
+
+def _solve_ionization(fun, astart, aend, ystart, rtol, atol, max_steps=128):
+    """thermodynamics_recfast.py:283-301: state at ``aend`` and its derivative."""
+    y_end = solve_pid_grk4a(fun, astart, aend, ystart[:3], abs(astart * 1e-3), rtol, atol, max_steps)
+    dyda = np.real(fun(aend, y_end))
+    return np.array([y_end[0], y_end[1], y_end[2], dyda[0], dyda[1], dyda[2]])
+
+
+def evaluate_thermo(*, param, num_thermo, aprimeoa_fn, dadtau_fn, dtauda_fn):
+    """Thermal history tables on the Recfast a-grid (thermodynamics_recfast.py:456-492)."""
+    param["fHe"] = param["YHe"] / (const_mHe_mH * (1.0 - param["YHe"]))
+    y, a = compute_thermal_history(a0=param["amin"], a1=param["amax"], N=num_thermo, param=param,
+                                   aprimeoa_fn=aprimeoa_fn)
+    xeHI = y[0]
+    xeHeI = y[1]
+    xeHeII = Saha_HeII(a, param)
+    xe = xeHI + param["fHe"] * xeHeI + xeHeII
+    mu = 1 / (1 + (1 / const_mHe_mH - 1) * param["YHe"] + (1 - param["YHe"]) * xe)
+    Tm = y[2]
+    dxeHIda = y[3]
+    dxeHeIda = y[4]
+    hc = 1e-30 * a
+    dxHeIIda = np.imag(Saha_HeII(a + 1j * hc, param)) / hc
+    dTmda = y[5]
+    daTmda = Tm + a * dTmda
+    cs2 = const_kB / const_mH / const_c**2 / mu * Tm * (4 - daTmda / Tm) / 3
+    dxedtau = (dxeHIda + param["fHe"] * dxeHeIda + dxHeIIda) * dadtau_fn(a)
+    inc = np.array([romb(dtauda_fn, lo, hi) for lo, hi in zip(a[:-1], a[1:])])
+    tau = param["taumin"] + np.concatenate([[0.0], np.cumsum(inc)])
+    return param, tau, a, cs2, Tm, mu, xe, xeHI, xeHeI, xeHeII, dxedtau

@@ -1,0 +1,120 @@
+/*
+ * discoeb_b200 C ABI: the drop-in boundary of the per-k-mode linear perturbation solve.
+ *
+ * Plain C types only.  All array pointers passed to discoeb_fwd / discoeb_los are DEVICE
+ * pointers owned by the caller (torch tensors, XLA FFI buffers, cudaMalloc'd memory);
+ * `stream` is a cudaStream_t passed as void*.  Calls are stream-ordered and re-entrant;
+ * the library keeps no per-call state.
+ *
+ * Interfaces replaced (paths relative to the reference project, lawrenceberry/DISCO-EB):
+ *   discoeb_fwd    -> evolve_one_mode / evolve_perturbations / evolve_perturbations_batched
+ *                     (src/discoeb/perturbations.py:882-949, :1124-1226, :1229-1337):
+ *                     the diffrax solve with Rodas5 + PIDController + SaveAt(ts),
+ *                     the RSA output projection (src/discoeb/approximations.py:84-176)
+ *                     and convert_to_output_variables (src/discoeb/perturbations.py:528-677).
+ *                     Start times and adiabatic initial conditions
+ *                     (perturbations.py:680-835) stay in the caller's host code so that
+ *                     automatic differentiation can flow through them.
+ *   discoeb_rhs    -> model_synchronous (src/discoeb/perturbations.py:88-525) evaluated at
+ *                     given states, i.e. compute_time_derivatives (perturbations.py:1339-1406).
+ */
+#ifndef DISCOEB_B200_H
+#define DISCOEB_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DISCOEB_MAX_NQ 16
+#define DISCOEB_ABI_VERSION 1
+
+/* Natural cubic spline table (x, y, S = y'' at the knots), the format of the reference's
+ * spline_interpolation (src/discoeb/spline_interpolation.py:6-116).  Device pointers. */
+typedef struct {
+    int32_t n_knots;
+    int32_t uniform; /* 1: knots equally spaced, index = floor((x - x0)/dx) */
+    const double* x;
+    const double* y;
+    const double* S;
+} DiscoebSpline;
+
+/* One cosmology: scalar parameters of the param dict (background.py:141-189), the
+ * neutrino momentum quadrature (background.py:14-45) and the four tables the RHS reads. */
+typedef struct {
+    int32_t lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax;
+    int32_t use_tca, use_rsa, use_ufa;
+    double tca_tau_c_over_tau_h, tca_tau_c_over_tau_k;
+    double rsa_tau_c_over_tau, rsa_tau_over_tau_k, ufa_tau_over_tau_k;
+    double grhom, grhog, grhor, Omegam, Omegab, OmegaDE, Omegak, Neff, Nmnu, amnu;
+    double w0, wa, cs2_DE, YHe, H0;
+    /* 0: reference equations (NaN at w = -1 exactly); > 0: dark-energy perturbations are
+     * held constant where |1 + w(a)| < de_guard_eps (the cosmological-constant limit). */
+    double de_guard_eps;
+    double q[DISCOEB_MAX_NQ], wq[DISCOEB_MAX_NQ];
+    DiscoebSpline xe_loga, cs2a_loga, logrhonu_loga, logpnu_loga;
+} DiscoebCosmo;
+
+/* Step control: diffrax PIDController fields (perturbations.py:913-914, :1124-1128). */
+typedef struct {
+    double rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin;
+    int32_t max_steps;
+    int32_t method;       /* DISCOEB_METHOD_* */
+    int32_t warps_per_block;
+    int32_t reserved;
+} DiscoebControl;
+
+#define DISCOEB_METHOD_RODAS5_STRUCTURED 0 /* default: banded-chain + rank-3 LU, FP64 */
+#define DISCOEB_METHOD_RODAS5_DENSE 1      /* dense partial-pivot LU per mode, FP64 */
+#define DISCOEB_METHOD_RODAS5_DENSE_MIXED 2/* dense FP32 LU + FP64 residual refinement */
+
+/* per-mode status codes */
+#define DISCOEB_OK 0
+#define DISCOEB_MAX_STEPS 1
+#define DISCOEB_NONFINITE 2
+#define DISCOEB_DT_UNDERFLOW 3
+#define DISCOEB_SINGULAR 4
+
+/* return codes of the entry points */
+#define DISCOEB_SUCCESS 0
+#define DISCOEB_EINVAL -1
+#define DISCOEB_ECUDA -2
+#define DISCOEB_EUNSUPPORTED -3
+
+int32_t discoeb_abi_version(void);
+
+/* Number of state variables per mode: 7 + (lmaxg+1) + (lmaxgp+1) + (lmaxr+1)
+ * + nqmax*(lmaxnu+1) + 2 (perturbations.py:893). */
+int32_t discoeb_nvar(const DiscoebCosmo* cosmo);
+
+/* Forward solve of n_modes k-modes.
+ *   cosmos[n_cosmo]        device array of DiscoebCosmo (tables inside are device pointers)
+ *   mode_cosmo[n_modes]    cosmology index per mode (NULL: all 0)
+ *   kmodes, tau_start      [n_modes]
+ *   y0                     [n_modes, nvar]   initial states (adiabatic ICs)
+ *   switch_tau             [n_modes, 3]      times where RSA starts, UFA starts, TCA ends
+ *                                            (+inf when never); steps end exactly there
+ *   tau_out                [n_out] increasing output times (shared by all modes)
+ *   y_full                 [n_modes, n_out, nvar] state at tau_out after the RSA projection
+ *                          (may be NULL)
+ *   y_out20                [n_modes, n_out, 20] output fields (may be NULL)
+ *   status, nsteps         [n_modes] per-mode status code and number of step attempts
+ * All modes of all cosmologies run in one launch. */
+int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                    const DiscoebControl* ctrl, int32_t n_modes, const int32_t* mode_cosmo,
+                    const double* kmodes, const double* tau_start, const double* y0,
+                    const double* switch_tau, int32_t n_out, const double* tau_out,
+                    double* y_full, double* y_out20, int32_t* status, int32_t* nsteps, void* stream);
+
+/* RHS f(tau_i, y_i; k_i) of n_points states (compute_time_derivatives):
+ *   y, f [n_points, nvar]; tau, kmodes [n_points]; regime < 0: approximation switches
+ *   evaluated from (tau, a) as the reference does, else bitmask 1=RSA 2=UFA 4=TCA. */
+int32_t discoeb_rhs(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_points,
+                    const double* tau, const double* kmodes, const double* y, int32_t regime, double* f,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

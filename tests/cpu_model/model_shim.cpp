@@ -1,0 +1,93 @@
+// Test harness: compiles the device model and stepper sources for one host thread so that
+// their algebra can be compared with the oracle on a CPU.  Test infrastructure only; the
+// library that ships is the CUDA build of the same headers.
+#include <cstring>
+#include <vector>
+
+#include "stepper.cuh"
+
+using namespace dscb;
+
+extern "C" {
+
+int shim_nvar(const DiscoebCosmo* P) { return make_dims(*P).n; }
+
+void shim_rhs(const DiscoebCosmo* P, double tau, const double* y, double k, int regime, double* f, double* col0)
+{
+    const Dims D = make_dims(*P);
+    HostTeam tm;
+    Bg<Dual> b;
+    bg_eval(*P, Dual(y[0], 1.0), tau, k, regime, b);
+    rhs_team(tm, *P, D, b, k, tau, y, f, col0);
+}
+
+// dense expansion of the structured Jacobian J = [[j00,0],[c0, S + U G]] (+ row 1) and dT
+void shim_jacobian(const DiscoebCosmo* P, double tau, const double* y, double k, int regime, double* J, double* dT)
+{
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    std::vector<double> f(n), col0(n);
+    shim_rhs(P, tau, y, k, regime, f.data(), col0.data());
+    Bg<double> b;
+    bg_eval(*P, y[0], tau, k, regime, b);
+    std::vector<double> G(3 * n);
+    for (int j = 0; j < n; ++j) {
+        double g[3];
+        gcol(*P, D, b, k, j, g);
+        for (int r = 0; r < 3; ++r) G[r * n + j] = g[r];
+    }
+    std::memset(J, 0, sizeof(double) * n * n);
+    for (int i = 0; i < n; ++i) J[i * n] = col0[i];
+    double fu[3];
+    f1u(*P, b, k, fu);
+    for (int j = 2; j < n; ++j) J[n + j] = f1col(*P, D, b, k, j) + fu[0] * G[j] + fu[1] * G[n + j] + fu[2] * G[2 * n + j];
+    for (int i = 2; i < n; ++i) {
+        double band[7], etac, u[3];
+        rowc(*P, D, b, k, tau, i, band, etac, u);
+        const int s = row_stride(D, i);
+        for (int m = -3; m <= 3; ++m) {
+            int jj = i + m * s;
+            if (jj >= 0 && jj < n) J[i * n + jj] += band[m + 3];
+        }
+        J[i * n + 2] += etac;
+        for (int j = 1; j < n; ++j) J[i * n + j] += u[0] * G[j] + u[1] * G[n + j] + u[2] * G[2 * n + j];
+    }
+    for (int i = 0; i < n; ++i) dT[i] = dtau_row(D, b, tau, i, y);
+}
+
+// x = W^{-1} r with W = I/(gamma h) - J(t, y), through the structured factorisation
+int shim_wsolve(const DiscoebCosmo* P, double tau, const double* y, double k, int regime, double h, const double* r,
+                double* x)
+{
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    std::vector<double> mem(mode_mem_doubles(D));
+    ModeMem M = carve(mem.data(), D);
+    HostTeam tm;
+    std::memcpy(M.y, y, sizeof(double) * n);
+    Bg<Dual> bd;
+    bg_eval(*P, Dual(y[0], 1.0), tau, k, regime, bd);
+    rhs_team(tm, *P, D, bd, k, tau, M.y, M.f, M.col0);
+    Bg<double> b;
+    bg_eval(*P, y[0], tau, k, regime, b);
+    bool ok = factor_W(tm, *P, D, b, k, tau, h, M);
+    std::memcpy(x, r, sizeof(double) * n);
+    solve_W(tm, D, M, h, x);
+    return ok ? 0 : 1;
+}
+
+int shim_solve_mode(const DiscoebCosmo* P, const DiscoebControl* C, double k, double t0, const double* y0,
+                    const double* sw, int nout, const double* tout, double* yout, int* stats)
+{
+    const Dims D = make_dims(*P);
+    std::vector<double> mem(mode_mem_doubles(D));
+    ModeMem M = carve(mem.data(), D);
+    std::memcpy(M.y, y0, sizeof(double) * D.n);
+    HostTeam tm;
+    SolveResult R = solve_mode(tm, *P, D, *C, k, t0, sw, nout, tout, M, yout);
+    stats[0] = R.status;
+    stats[1] = R.steps;
+    stats[2] = R.accepted;
+    return R.status;
+}
+}
