@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the per-k-mode perturbation solve (one JSON line on stdout, rank 0).
+
+Workload (default): flat LCDM + one 0.06 eV neutrino (5 momentum bins, l_max 12/12/17/17,
+143 state variables per mode), 512 log-spaced k-modes in [1e-4, 10] /Mpc, outputs at
+z = 2, 1, 0.5, 0, rtol 1e-5 / atol 1e-8.  One "step" = one complete forward solve of all
+512 modes of one cosmology.  Under torchrun every rank solves its own replica of the
+cosmology (weak scaling, no collective on the data path).
+
+  value : k-mode solves/s, inputs resident in HBM, CUDA events around each solve
+  e2e   : the same metric through the public API evolve_perturbations (numpy in, numpy out,
+          host prologue + H2D + kernel + D2H inside the timed region)
+  --impl reference : the oracle's CPU restatement of the reference algorithm (dense LU Rodas5)
+          timed on all host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+import warnings
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "disco-eb_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "fwd+adjoint k-mode solves/s at ≤1e-4 rel err vs FP64 oracle; ms per cosmology"
+UNIT = "k-mode solves/s"
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def _background(w):
+    from discoeb_b200.background import evolve_background
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        return evolve_background(param=w["param"])
+
+
+def _sample_modes(w, count):
+    k = np.geomspace(w["kmin"], w["kmax"], w["num_k"])
+    idx = np.unique(np.linspace(0, len(k) - 1, count).round().astype(int))
+    return k[idx]
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of the reference algorithm (oracle port) on all host threads."""
+    if rank != 0:
+        return
+    from discoeb_b200.workloads import workload
+    from oracle import pyoracle as O
+    w = workload(args.workload)
+    bg = _background(w)
+    L = {k: w[k] for k in ("lmaxg", "lmaxgp", "lmaxr", "lmaxnu", "nqmax")}
+    ks = _sample_modes(w, args.ref_sample)
+    threads = os.cpu_count() or 1
+
+    def one():
+        t = time.perf_counter()
+        y, _, st = O.evolve_perturbations(param=bg, aexp_out=w["aexp_out"], kmin=0, kmax=0, num_k=0, rtol=w["rtol"],
+                                          atol=w["atol"], kmodes=ks, mode="reference", de_guard_eps=1e-9,
+                                          max_steps=100000, threads=threads, **L)
+        return time.perf_counter() - t
+
+    for _ in range(args.warmup):
+        one()
+    times = [one() for _ in range(args.steps)]
+    ms = 1e3 * statistics.mean(times)
+    value = len(ks) / (ms / 1e3)
+    sample = (f"{len(ks)} of the {w['num_k']} modes (k evenly spread in log over [{w['kmin']:g}, {w['kmax']:g}]), "
+              f"dense-LU Rodas5 with diffrax controller semantics, {threads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cosmology, no dataset)",
+            "config": {"workload": args.workload, "mode": "forward", "modes_per_step": len(ks)},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.tmp,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.tmp.flush()
+        try:
+            rows = [r.split(",") for r in open(self.tmp.name).read().strip().splitlines() if r.strip()]
+        except OSError:
+            rows = []
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def fp64_peak_tflops(torch, device):
+    """Measured FP64 peak on this GPU: cuBLAS DGEMM 8192^3, best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * n**3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pk_lcdm_mnu_k512_z4")
+    ap.add_argument("--ref-sample", type=int, default=24)
+    ap.add_argument("--cpu-sample", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import ctypes
+
+    import torch
+
+    from discoeb_b200 import _abi
+    from discoeb_b200 import perturbations as pert
+    from discoeb_b200.workloads import workload
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+    w = workload(args.workload)
+    bg = _background(w)
+    L = {k: w[k] for k in ("lmaxg", "lmaxgp", "lmaxr", "lmaxnu", "nqmax")}
+    n = pert.nvar_of(**L)
+    kmodes = np.geomspace(w["kmin"], w["kmax"], w["num_k"])
+    K = kmodes.shape[0]
+    aout = np.asarray(w["aexp_out"], dtype=np.float64)
+    tau_out = bg["tau_of_a_spline"].evaluate(aout)
+    nout = tau_out.shape[0]
+
+    # ---- device-resident inputs for the kernel-only measurement ----
+    tau_s = pert.determine_starting_time(param=bg, k=kmodes)
+    tau_start = 0.99 * np.minimum(tau_out.min(), tau_s)
+    y0 = pert.adiabatic_ics(tau=tau_start, param=bg, kmode=kmodes, **L)
+    sw = pert.approximation_switch_times(bg, kmodes)
+    order = np.argsort(-kmodes, kind="stable")
+    dc = pert.DeviceCosmo(bg, de_guard_eps=1e-9, device=device, **L)
+    f64 = dict(dtype=torch.float64, device=device)
+    d_k = torch.tensor(kmodes[order], **f64)
+    d_ts = torch.tensor(tau_start[order], **f64)
+    d_y0 = torch.tensor(y0[order], **f64).contiguous()
+    d_sw = torch.tensor(sw[order], **f64).contiguous()
+    d_tout = torch.tensor(tau_out, **f64)
+    d_out = torch.empty((K, nout, 20), **f64)
+    d_stat = torch.empty((2, K), dtype=torch.int32, device=device)
+    ctrl = _abi.DiscoebControl(w["rtol"], w["atol"], 0.25, 0.80, 0.0, 20.0, 0.3, 100000,
+                               _abi.METHOD_RODAS5_STRUCTURED, 0, 0)
+    lib = _abi.lib()
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)  # > 126 MB L2
+
+    def solve():
+        rc = lib.discoeb_fwd(dc.struct.data_ptr(), ctypes.byref(dc.host), 1, ctypes.byref(ctrl), K, None,
+                             d_k.data_ptr(), d_ts.data_ptr(), d_y0.data_ptr(), d_sw.data_ptr(), nout,
+                             d_tout.data_ptr(), None, d_out.data_ptr(), d_stat[0].data_ptr(), d_stat[1].data_ptr(),
+                             stream.cuda_stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_fwd returned {rc}")
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    stat = d_stat.cpu().numpy()
+    if (stat[0] != 0).any():
+        raise RuntimeError(f"{int((stat[0] != 0).sum())} modes failed")
+    total_steps = int(stat[1].sum())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier()
+        for i in range(args.steps):
+            flush.zero_()  # evict L2 between timed solves (outside the events)
+            starts[i].record(stream)
+            solve()
+            ends[i].record(stream)
+        barrier()
+    times_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    clocks = clk.summary()
+    ms = statistics.mean(times_ms)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * K / (ms / 1e3)
+
+    # ---- end to end through the public API (host arrays in, host arrays out) ----
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        y, k, _ = pert.evolve_perturbations(param=dict(bg), aexp_out=aout, kmin=w["kmin"], kmax=w["kmax"],
+                                            num_k=w["num_k"], rtol=w["rtol"], atol=w["atol"], max_steps=100000,
+                                            k_sampling_method="log", **L)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e = statistics.mean(e2e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+    h2d = 8 * (2 * K + K * n + 3 * K + nout) + sum(t.numel() * 8 for t in dc.tensors) + ctypes.sizeof(dc.host)
+    d2h = 8 * K * nout * 20 + 8 * K
+
+    # ---- roofline: FP64 work of the structured Rodas5 step against a measured FP64 peak ----
+    flops_per_step = 850.0 * n + 1650.0  # structured step, counted from stepper.cuh
+    dense_per_step = (2.0 / 3.0) * n**3 + 16.0 * n**2 + 45.0 * n * n  # reference algorithm: LU + 8 solves + jacfwd
+    achieved = total_steps * flops_per_step / (ms / 1e3) / 1e12
+    peak = fp64_peak_tflops(torch, device) if rank == 0 else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+        ks = _sample_modes(w, args.cpu_sample)
+        th = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.evolve_perturbations(param=bg, aexp_out=aout, kmin=0, kmax=0, num_k=0, rtol=w["rtol"], atol=w["atol"],
+                               kmodes=ks, mode="reference", de_guard_eps=1e-9, max_steps=100000, threads=th, **L)
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(ks) / dt, "unit": UNIT, "cores": th, "kind": "port",
+               "sample": f"{len(ks)} modes spread over the workload's k range, oracle dense-LU Rodas5, {dt:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cosmology, no dataset)",
+            "config": {"workload": args.workload, "mode": "forward", "num_k": K, "nvar": n, "n_out": nout,
+                       "rtol": w["rtol"], "atol": w["atol"], "method": "rodas5-structured",
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "ms_per_cosmology": ms, "step_attempts": total_steps},
+            "e2e": {"value": world * K / (e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_cosmology": e2e},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if peak else None, "traffic": None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                         "dense_equivalent_tflops": total_steps * dense_per_step / (ms / 1e3) / 1e12},
+            "clocks": clocks,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,199 @@
+// Forward perturbation solve on sm_100a: kernels and the C ABI (include/discoeb.h).
+//
+// Layout: one warp owns one k-mode.  Its whole working set (state, eight Rodas5 stage
+// vectors, the banded chain factors and the Woodbury blocks, 27 n doubles) lives in
+// shared memory; the four background tables are read through the read-only cache.
+// All modes of all cosmologies run in one launch; each warp takes modes from a
+// grid-stride schedule ordered by the caller (longest first).  HBM traffic is only the
+// initial states and the outputs, so the kernel is bound by FP64 latency, not bandwidth.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include "discoeb.h"
+#include "stepper.cuh"
+
+using namespace dscb;
+
+namespace {
+
+constexpr int kCosmoDoubles = (sizeof(DiscoebCosmo) + 7) / 8;
+
+__device__ __forceinline__ void copy_cosmo(const WarpTeam& tm, const DiscoebCosmo* src, DiscoebCosmo* dst)
+{
+    const int* s = reinterpret_cast<const int*>(src);
+    int* d = reinterpret_cast<int*>(dst);
+    for (int i = tm.lane; i < (int)(sizeof(DiscoebCosmo) / 4); i += 32) d[i] = s[i];
+    tm.sync();
+}
+
+// write state / projected state / output fields of one output time (team-parallel)
+__device__ void emit_output(const WarpTeam& tm, const DiscoebCosmo& P, const Dims& D, double k, double tau,
+                            const double* y, double* yfull, double* y20, double* scratch20)
+{
+    const int n = D.n;
+    double fld[4];
+    const bool rsa = rsa_projection(P, D, tau, k, y, fld);  // all lanes, identical
+    // projected state into scratch (shared) then outputs
+    double* yp = scratch20;  // n doubles of shared scratch
+    for (int i = tm.lane; i < n; i += 32) {
+        double v = y[i];
+        if (rsa) {
+            const int s = rsa_slot(D, i);
+            if (s >= 0) v = fld[s];
+            else if (s == -1) v = 0.0;
+        }
+        yp[i] = v;
+        if (yfull) yfull[i] = v;
+    }
+    tm.sync();
+    if (y20 && tm.leader()) {
+        double o[20];
+        output_vars(P, D, k, yp, o);
+        for (int q = 0; q < 20; ++q) y20[q] = o[q];
+    }
+    tm.sync();
+}
+
+__global__ void __launch_bounds__(256) fwd_structured_kernel(
+    const DiscoebCosmo* __restrict__ cosmos, const int32_t* __restrict__ mode_cosmo, DiscoebControl ctrl, int n_modes,
+    const double* __restrict__ kmodes, const double* __restrict__ tau_start, const double* __restrict__ y0,
+    const double* __restrict__ sw, int n_out, const double* __restrict__ tau_out, int mem_doubles, double* y_full,
+    double* y_out20, int32_t* status, int32_t* nsteps)
+{
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5;
+    const WarpTeam tm{(int)(threadIdx.x & 31)};
+    const int wpb = blockDim.x >> 5;
+    double* base = smem + (size_t)warp * (kCosmoDoubles + mem_doubles);
+    DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(base);
+    double* wmem = base + kCosmoDoubles;
+    const int total_warps = gridDim.x * wpb;
+    int cur_cosmo = -1;
+    for (int mode = blockIdx.x * wpb + warp; mode < n_modes; mode += total_warps) {
+        const int ci = mode_cosmo ? mode_cosmo[mode] : 0;
+        if (ci != cur_cosmo) {
+            copy_cosmo(tm, cosmos + ci, P);
+            cur_cosmo = ci;
+        }
+        const Dims D = make_dims(*P);
+        const int n = D.n;
+        ModeMem M = carve(wmem, D);
+        const double k = kmodes[mode];
+        for (int i = tm.lane; i < n; i += 32) M.y[i] = y0[(size_t)mode * n + i];
+        double swm[3] = {sw[3 * mode], sw[3 * mode + 1], sw[3 * mode + 2]};
+        tm.sync();
+        const size_t obase = (size_t)mode * n_out;
+        auto emit = [&](int j, const double* y) {
+            const size_t o = obase + j;
+            emit_output(tm, *P, D, k, tau_out[j], y, y_full ? y_full + o * n : nullptr,
+                        y_out20 ? y_out20 + o * 20 : nullptr, M.f);
+        };
+        const SolveResult R = solve_mode(tm, *P, D, ctrl, k, tau_start[mode], swm, n_out, tau_out, M, emit);
+        const int st = R.status, steps = R.steps;
+        // outputs never reached are filled with NaN so that they cannot pass for data
+        const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+        for (int j = R.outputs; j < n_out; ++j) {
+            const size_t o = obase + j;
+            if (y_full) for (int i = tm.lane; i < n; i += 32) y_full[o * n + i] = qnan;
+            if (y_out20) for (int i = tm.lane; i < 20; i += 32) y_out20[o * 20 + i] = qnan;
+        }
+        if (tm.leader()) {
+            status[mode] = st;
+            nsteps[mode] = steps;
+        }
+        tm.sync();
+    }
+}
+
+__global__ void rhs_kernel(const DiscoebCosmo* __restrict__ cosmo, int n_points, const double* __restrict__ tau,
+                           const double* __restrict__ kmodes, const double* __restrict__ y, int regime, double* f)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= n_points) return;
+    const WarpTeam tm{(int)(threadIdx.x & 31)};
+    const DiscoebCosmo& P = *cosmo;
+    const Dims D = make_dims(P);
+    const double* yy = y + (size_t)warp * D.n;
+    Bg<double> b;
+    bg_eval(P, yy[0], tau[warp], kmodes[warp], regime, b);
+    rhs_team(tm, P, D, b, kmodes[warp], tau[warp], yy, f + (size_t)warp * D.n, (double*)nullptr);
+}
+
+int validate_cosmo(const DiscoebCosmo* c)
+{
+    if (!c) return DISCOEB_EINVAL;
+    if (c->nqmax < 0 || c->nqmax > DISCOEB_MAX_NQ) return DISCOEB_EINVAL;
+    if (c->lmaxg < 3 || c->lmaxgp < 3 || c->lmaxr < 3 || c->lmaxnu < 3) return DISCOEB_EINVAL;
+    if (c->use_tca) return DISCOEB_EUNSUPPORTED;
+    return DISCOEB_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t discoeb_abi_version(void) { return DISCOEB_ABI_VERSION; }
+
+int32_t discoeb_nvar(const DiscoebCosmo* cosmo)
+{
+    if (!cosmo) return DISCOEB_EINVAL;
+    return make_dims(*cosmo).n;
+}
+
+int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                    const DiscoebControl* ctrl, int32_t n_modes, const int32_t* mode_cosmo, const double* kmodes,
+                    const double* tau_start, const double* y0, const double* switch_tau, int32_t n_out,
+                    const double* tau_out, double* y_full, double* y_out20, int32_t* status, int32_t* nsteps,
+                    void* stream)
+{
+    int rc = validate_cosmo(cosmo0_host);
+    if (rc) return rc;
+    if (!cosmos_dev || !ctrl || n_cosmo < 1 || n_modes < 0 || n_out < 1) return DISCOEB_EINVAL;
+    if (n_modes == 0) return DISCOEB_SUCCESS;
+    if (!kmodes || !tau_start || !y0 || !switch_tau || !tau_out || !status || !nsteps) return DISCOEB_EINVAL;
+    if (!y_full && !y_out20) return DISCOEB_EINVAL;
+    if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED) return DISCOEB_EUNSUPPORTED;
+    if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
+    const Dims D = make_dims(*cosmo0_host);
+    const int mem = mode_mem_doubles(D);
+    const size_t per_warp = (size_t)(kCosmoDoubles + mem) * sizeof(double);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
+    int max_optin = 0, n_sm = 0;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    int wpb = ctrl->warps_per_block > 0 ? ctrl->warps_per_block : 2;
+    if (wpb > 8) wpb = 8;
+    while (wpb > 1 && per_warp * wpb > (size_t)max_optin) --wpb;
+    if (per_warp > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
+    const size_t smem = per_warp * wpb;
+    if (cudaFuncSetAttribute(fwd_structured_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return DISCOEB_ECUDA;
+    int blocks = (n_modes + wpb - 1) / wpb;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    fwd_structured_kernel<<<blocks, 32 * wpb, smem, s>>>(cosmos_dev, mode_cosmo, *ctrl, n_modes, kmodes, tau_start,
+                                                          y0, switch_tau, n_out, tau_out, mem, y_full, y_out20, status,
+                                                          nsteps);
+    (void)n_sm;
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int32_t discoeb_rhs(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_points,
+                    const double* tau, const double* kmodes, const double* y, int32_t regime, double* f, void* stream)
+{
+    int rc = validate_cosmo(cosmo_host);
+    if (rc) return rc;
+    if (!cosmo_dev || n_points < 0) return DISCOEB_EINVAL;
+    if (n_points == 0) return DISCOEB_SUCCESS;
+    if (!tau || !kmodes || !y || !f) return DISCOEB_EINVAL;
+    const int threads = 128;
+    const long long blocks = ((long long)n_points * 32 + threads - 1) / threads;
+    rhs_kernel<<<(unsigned)blocks, threads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(cosmo_dev, n_points, tau,
+                                                                                          kmodes, y, regime, f);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+}  // extern "C"

@@ -368,3 +368,105 @@ DHD double dtau_row(const Dims& D, const Bg<T>& b, double tau, int i, const doub
 }
 
 }  // namespace dscb
+
+namespace dscb {
+
+// ---- RSA output projection (approximations.py:84-176): the fields that replace the
+// photon and massless-neutrino moments at an output time.  Returns true when the RSA
+// condition holds there (evaluated from (tau, a) as the reference does).
+DHD bool rsa_projection(const DiscoebCosmo& P, const Dims& D, double tau, double k, const double* y, double out[4])
+{
+    const double a = y[0], loga = log(a), eta = y[2], deltab = y[5], thetab = y[6];
+    const double aH = aprimeoa_of(P, a, loga);
+    const int ix = spline_index(P.xe_loga, loga);
+    const double xe = spline_eval_at(P.xe_loga, ix, loga);
+    const double xeprime = spline_deriv_at(P.xe_loga, ix, loga) * aH;
+    const double cs2 = spline_eval(P.cs2a_loga, loga) / a;
+    const double akthom = 2.3038921003709498e-9 * (1.0 - P.YHe) * P.Omegab * P.H0 * P.H0;
+    const double opac = xe * akthom / (a * a);
+    const double tau_c = 1.0 / (opac > 1e-30 ? opac : 1e-30);
+    const double tau_c_prime = tau_c * (2.0 * aH - xeprime / (xe > 1e-30 ? xe : 1e-30));
+    const double Omegac = P.Omegam - P.Omegab;
+    double drhonu = 0.0;
+    for (int q = 0; q < D.nq; ++q) {
+        const double aq = a * P.amnu / P.q[q];
+        drhonu += P.wq[q] * y[D.iq0 + q] * sqrt(1.0 + aq * aq);
+    }
+    const double rho_Q = pow(a, -3.0 * (1.0 + P.w0 + P.wa)) * exp(3.0 * (a - 1.0) * P.wa);
+    const double dgrho_wo_rel = P.grhom * (Omegac * y[3] + P.Omegab * deltab) / a + P.grhor * P.Nmnu * drhonu / (a * a) +
+                                P.grhom * P.OmegaDE * y[D.n - 2] * rho_Q * a * a;
+    const double k2 = k * k;
+    const double hprime = (2.0 * k2 * eta + dgrho_wo_rel) / (aH > 1e-30 ? aH : 1e-30);
+    const double sk2 = k2 > 1e-30 ? k2 : 1e-30, stc = tau_c > 1e-30 ? tau_c : 1e-30;
+    out[0] = 4.0 / sk2 * (aH * hprime - sk2 * eta) + 4.0 / (sk2 * stc) * (thetab + 0.5 * hprime);
+    out[1] = -0.5 * hprime + 3.0 / (sk2 * stc) *
+             (-tau_c_prime / stc * (thetab + 0.5 * hprime) + (-aH * thetab + cs2 * sk2 * deltab + sk2 * eta));
+    out[2] = 4.0 / sk2 * (aH * hprime - sk2 * eta);
+    out[3] = -0.5 * hprime;
+    return P.use_rsa && (tau_c / (tau > 1e-30 ? tau : 1e-30) > P.rsa_tau_c_over_tau) && (tau * k > P.rsa_tau_over_tau_k);
+}
+
+// is index i one of the moments the RSA projection overwrites?  (value slot or -1 for zero)
+DHD int rsa_slot(const Dims& D, int i)
+{
+    if (i == 7) return 0;
+    if (i == 8) return 1;
+    if (i > 8 && i <= D.idxgp + D.lmaxgp) return -1;  // shear, l >= 3 and all polarisation
+    if (i == D.idxr) return 2;
+    if (i == D.idxr + 1) return 3;
+    if (i > D.idxr + 1 && i <= D.idxr + D.lmaxr) return -1;
+    return -2;  // untouched
+}
+
+// ---- convert_to_output_variables (perturbations.py:528-677) ----
+DHD void output_vars(const DiscoebCosmo& P, const Dims& D, double k, const double* y, double* o)
+{
+    const double Omegac = P.Omegam - P.Omegab;
+    const int n = D.n, nq = D.nq, iq0 = D.iq0, iq1 = iq0 + nq;
+    const double a = y[0], eta = y[2], deltac = y[3], thetac = y[4], deltab = y[5], thetab = y[6];
+    const double deltag = y[7], thetag = y[8], deltar = y[D.idxr], thetar = y[D.idxr + 1];
+    const double loga = log(a);
+    const int inu = spline_index(P.logrhonu_loga, loga);
+    const double rhonu = exp(spline_eval_at(P.logrhonu_loga, inu, loga));
+    const int ip = (P.logpnu_loga.x == P.logrhonu_loga.x) ? inu : spline_index(P.logpnu_loga, loga);
+    const double pnu = exp(spline_eval_at(P.logpnu_loga, ip, loga));
+    double drhonu = 0.0, fnu = 0.0;
+    for (int q = 0; q < nq; ++q) {
+        const double aq = a * P.amnu / P.q[q];
+        drhonu += P.wq[q] * y[iq0 + q] * sqrt(1.0 + aq * aq);
+        fnu += P.wq[q] * y[iq1 + q];
+    }
+    const double deltanu = drhonu / rhonu, thetanu = k * fnu / (rhonu + pnu);
+    const double deltaq = y[n - 2], thetaq = y[n - 1];
+    const double w_Q = P.w0 + P.wa * (1.0 - a);
+    const double rho_Q = pow(a, -3.0 * (1.0 + P.w0 + P.wa)) * exp(3.0 * (a - 1.0) * P.wa);
+    const double rpt = (1.0 + w_Q) * rho_Q * P.grhom * P.OmegaDE * thetaq * a * a;
+    const double a2 = a * a;
+    const double grho = P.grhom * P.Omegam / a + (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / a2 +
+                        P.grhom * P.OmegaDE * rho_Q * a2 + P.grhom * P.Omegak;
+    const double aH = sqrt(grho / 3.0);
+    const double dgrho = P.grhom * (Omegac * deltac + P.Omegab * deltab) / a +
+                         (P.grhog * deltag + P.grhor * (P.Neff * deltar + P.Nmnu * drhonu)) / a2 +
+                         P.grhom * P.OmegaDE * deltaq * rho_Q * a2;
+    const double dgtheta = P.grhom * (Omegac * thetac + P.Omegab * thetab) / a +
+                           4.0 / 3.0 * (P.grhog * thetag + P.Neff * P.grhor * thetar) / a2 +
+                           P.Nmnu * P.grhor * k * fnu / a2 + rpt;
+    const double k2 = k * k;
+    const double hprime = (2.0 * k2 * eta + dgrho) / aH;
+    const double etaprime = 0.5 * dgtheta / k2;
+    const double alpha = (hprime + 6.0 * etaprime) / 2.0 / k2;
+    const double mden = P.grhom * P.Omegam / a + P.grhor * P.Nmnu * rhonu / a2;
+    const double deltam = (P.grhom * (Omegac * deltac + P.Omegab * deltab) / a + P.grhor * P.Nmnu * drhonu / a2) / mden;
+    double thetam = (P.grhom * (Omegac * thetac + P.Omegab * thetab) / a + P.Nmnu * P.grhor * k * fnu / a2) / (3.0 * mden);
+    const double deltabc = (P.grhom * (Omegac * deltac + P.Omegab * deltab) / a) / (P.grhom * P.Omegam / a);
+    double thetabc = (P.grhom * (Omegac * thetac + P.Omegab * thetab) / a) / (3.0 * (P.grhom * P.Omegam / a) / a2);
+    thetam += alpha * k2;
+    thetabc += alpha * k2;
+    o[0] = eta; o[1] = etaprime; o[2] = hprime; o[3] = alpha;
+    o[4] = deltam; o[5] = thetam / aH; o[6] = deltabc; o[7] = thetabc / aH;
+    o[8] = deltac; o[9] = thetac / aH; o[10] = deltab; o[11] = thetab / aH;
+    o[12] = deltag; o[13] = thetag / aH; o[14] = deltar; o[15] = thetar / aH;
+    o[16] = deltanu; o[17] = thetanu / aH; o[18] = deltaq; o[19] = thetaq / aH;
+}
+
+}  // namespace dscb

@@ -339,7 +339,7 @@ DHD int regime_at(const DiscoebCosmo& P, double t, const double* sw)
 }
 
 struct SolveResult {
-    int status, steps, accepted;
+    int status, steps, accepted, outputs;
 };
 
 // One Rodas5 step from (t, y) with size h: on return M.u + M.K[7] is the candidate and
@@ -391,24 +391,23 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
     return ok;
 }
 
-// Adaptive solve of one mode: y(t0) in M.y -> outputs at every tout[j] written to
-// yout[j*n ...] (raw state).  sw[3]: RSA start, UFA start, TCA end.
-template <class TM>
+// Adaptive solve of one mode from y(t0) in M.y.  At every output time the team calls
+// emit(j, y) with the state exactly at tout[j].  sw[3]: RSA start, UFA start, TCA end.
+template <class TM, class Emit>
 DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, const DiscoebControl& C, double k,
-                           double t0, const double* sw, int nout, const double* tout, const ModeMem& M,
-                           double* yout)
+                           double t0, const double* sw, int nout, const double* tout, const ModeMem& M, Emit& emit)
 {
     const int n = D.n;
-    SolveResult R = {DISCOEB_OK, 0, 0};
+    SolveResult R = {DISCOEB_OK, 0, 0, 0};
     double t1 = tout[0];
     for (int j = 1; j < nout; ++j) t1 = tout[j] > t1 ? tout[j] : t1;
-    const double eo = 6.0;  // error order of a 5th-order method
+    const double eo = 6.0;  // diffrax error order of a 5th-order method: order + 1
     const double c1 = (C.icoeff + C.pcoeff + C.dcoeff) / eo;
     const double c2 = -(C.pcoeff + 2.0 * C.dcoeff) / eo;
     const double c3 = C.dcoeff / eo;
     double prev_inv = 1.0, prev_prev_inv = 1.0;
     double t = t0;
-    double dt = fmin(t0 / 4.0, 0.5 * (t1 - t0));
+    double dt = fmin(t0 / 4.0, 0.5 * (t1 - t0));  // dt0 of perturbations.py:910
     int iout = 0;
     const int idx[6] = {0, 2, 3, 5, 6, 7};
     const double w6[6] = {1.0, k * k, 1.0, 1.0, 1.0 / (k * k), 1.0};
@@ -427,20 +426,19 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
         const int regime = regime_at(P, t, sw);
         const bool ok = rodas5_step(tm, P, D, k, t, h, regime, M);
         R.steps++;
-        // error norm (perturbations.py:855-878 with the weights of :913)
+        // weighted RMS error over (a, eta, delta_c, delta_b, theta_b, delta_gamma)
+        // (perturbations.py:855-878 with the weights of :913)
         double sumsq = 0.0;
-        bool finite = ok;
         for (int q = 0; q < 6; ++q) {
             const int i = idx[q];
             const double y1 = M.u[i] + M.K[7 * n + i];
             const double sc = fmax(fabs(M.y[i]), fabs(y1));
             const double e = M.K[7 * n + i] / (C.atol + C.rtol * sc) * w6[q];
             sumsq += e * e;
-            if (!xfinite(y1)) finite = false;
         }
         double lf = 0.0;
         for (int i = tm.lane; i < n; i += tm.nl) lf += xfinite(M.u[i] + M.K[7 * n + i]) ? 0.0 : 1.0;
-        if (tm.sum(lf) > 0.0) finite = false;
+        const bool finite = ok && tm.sum(lf) == 0.0;
         const double err = finite ? sqrt(sumsq / 6.0) : INFINITY;
         const bool keep = err < 1.0;
         double inv = 1.0 / err;
@@ -460,7 +458,7 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
             tm.sync();
             t = tn;
             while (iout < nout && tout[iout] <= t) {
-                for (int i = tm.lane; i < n; i += tm.nl) yout[(size_t)iout * n + i] = M.y[i];
+                emit(iout, M.y);
                 iout++;
             }
             if (clipped && dt_try > dtn) dtn = dt_try;
@@ -471,6 +469,7 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
         tm.sync();
     }
     if (R.status == DISCOEB_OK && iout < nout) R.status = DISCOEB_MAX_STEPS;
+    R.outputs = iout;
     return R;
 }
 

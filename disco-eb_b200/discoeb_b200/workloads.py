@@ -1,0 +1,56 @@
+"""Named workloads: cosmologies and solver settings of the measured problems.
+
+Cosmological parameters are given as (h, omega_b, omega_c, A_s, n_s, ...) and mapped to
+the reference's parameter dict: H0 = 100 h, Omegab = omega_b/h^2,
+Omegam = (omega_b + omega_c)/h^2 (massive neutrinos are not part of Omegam,
+background.py:170-178), YHe = 0.248 and cs2_DE = 1 as in the reference's tests.  The
+reference has no reionisation, so tau_reio has no counterpart and is not used.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def cosmo_params(*, h=0.674, omega_b=0.0224, omega_c=0.120, A_s=2.1e-9, n_s=0.965, Tcmb=2.7255, Neff=3.046,
+                 m_nu=0.0, w0=-1.0, wa=0.0, YHe=0.248, cs2_DE=1.0, k_p=0.05):
+    """Reference param dict; ``m_nu > 0`` adds one massive species and moves one unit of
+    N_eff from the massless to the massive sector (the reference tests' convention)."""
+    massive = m_nu > 0.0
+    return {
+        "Omegam": (omega_b + omega_c) / h**2,
+        "Omegab": omega_b / h**2,
+        "H0": 100.0 * h,
+        "n_s": n_s,
+        "A_s": A_s,
+        "mnu": float(m_nu),
+        "Tcmb": Tcmb,
+        "YHe": YHe,
+        "Neff": Neff - 1.0 if massive else Neff,
+        "Nmnu": 1 if massive else 0,
+        "w_DE_0": w0,
+        "w_DE_a": wa,
+        "cs2_DE": cs2_DE,
+        "Omegak": 0.0,
+        "k_p": k_p,
+    }
+
+
+# z in {2, 1, 0.5, 0} as increasing scale factors
+A_OUT_4Z = np.array([1.0 / 3.0, 0.5, 2.0 / 3.0, 1.0])
+
+WORKLOADS = {
+    # flat LCDM, massless neutrinos only, P(k, z=0) on 128 log-spaced modes
+    "pk_lcdm_massless_k128": dict(
+        cosmo=dict(), kmin=1e-4, kmax=1.0, num_k=128, aexp_out=np.array([1.0]),
+        lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=3, nqmax=3, rtol=1e-5, atol=1e-8),
+    # + one 0.06 eV neutrino (5 momentum bins, l_max 17): 512 modes to k = 10/Mpc, P(k) at z = 0, 0.5, 1, 2
+    "pk_lcdm_mnu_k512_z4": dict(
+        cosmo=dict(m_nu=0.06), kmin=1e-4, kmax=10.0, num_k=512, aexp_out=A_OUT_4Z,
+        lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5, rtol=1e-5, atol=1e-8),
+}
+
+
+def workload(name):
+    w = dict(WORKLOADS[name])
+    w["param"] = cosmo_params(**w.pop("cosmo"))
+    return w

@@ -1,0 +1,46 @@
+import os
+import sys
+import warnings
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "disco-eb_b200"))
+sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (run with -m gpu)")
+
+
+@pytest.fixture(scope="session")
+def golden():
+    return dict(np.load(os.path.join(GOLDEN, "reference_golden.npz")))
+
+
+_BG = {}
+
+
+def background(name, num_thermo):
+    """Cached evolve_background of a named cosmology."""
+    from discoeb_b200.background import evolve_background
+    from discoeb_b200.workloads import cosmo_params
+    key = (name, num_thermo)
+    if key not in _BG:
+        if name == "disco_notebook":
+            p = {"Omegam": 0.3099, "Omegab": 0.0488911, "H0": 67.742, "n_s": 0.96822, "A_s": 2.1064e-09,
+                 "mnu": 0.06, "Tcmb": 2.7255, "YHe": 0.248, "Neff": 2.046, "Nmnu": 1, "w_DE_0": -0.99,
+                 "w_DE_a": 0.0, "cs2_DE": 1.0, "Omegak": 0.0, "k_p": 0.05}
+        elif name == "lcdm_massless":
+            p = cosmo_params()
+        elif name == "lcdm_mnu":
+            p = cosmo_params(m_nu=0.06)
+        else:
+            raise KeyError(name)
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            _BG[key] = evolve_background(param=p, num_thermo=num_thermo)
+    return _BG[key]

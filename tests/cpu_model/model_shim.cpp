@@ -84,7 +84,9 @@ int shim_solve_mode(const DiscoebCosmo* P, const DiscoebControl* C, double k, do
     ModeMem M = carve(mem.data(), D);
     std::memcpy(M.y, y0, sizeof(double) * D.n);
     HostTeam tm;
-    SolveResult R = solve_mode(tm, *P, D, *C, k, t0, sw, nout, tout, M, yout);
+    const int n = D.n;
+    auto emit = [&](int j, const double* y) { std::memcpy(yout + (size_t)j * n, y, sizeof(double) * n); };
+    SolveResult R = solve_mode(tm, *P, D, *C, k, t0, sw, nout, tout, M, emit);
     stats[0] = R.status;
     stats[1] = R.steps;
     stats[2] = R.accepted;

@@ -1,0 +1,97 @@
+"""Host-side logic of the package and the C ABI library surface (CPU, no GPU calls)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, background
+from discoeb_b200 import _abi
+from discoeb_b200 import perturbations as pert
+from oracle import pyoracle as O
+
+L = dict(lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5)
+
+
+def test_start_times_and_ics_match_oracle():
+    bg = background("disco_notebook", 512)
+    OP = O.OracleProblem(bg, **L)
+    ks = np.geomspace(1e-5, 10.0, 23)
+    ts = pert.determine_starting_time(param=bg, k=ks)
+    np.testing.assert_allclose(ts, [OP.start_time(k) for k in ks], rtol=1e-12)
+    y = pert.adiabatic_ics(tau=ts, param=bg, kmode=ks, **L)
+    yo = np.stack([OP.ics(t, k) for t, k in zip(ts, ks)])
+    np.testing.assert_allclose(y, yo, rtol=1e-12, atol=0)
+
+
+def test_switch_times_match_oracle():
+    bg = background("disco_notebook", 512)
+    OP = O.OracleProblem(bg, **L)
+    ks = np.geomspace(1e-4, 10.0, 17)
+    sw = pert.approximation_switch_times(bg, ks)
+    so = np.stack([OP.switch_times(k) for k in ks])
+    np.testing.assert_allclose(sw[:, :2], so[:, :2], rtol=1e-9)
+    assert np.isinf(sw[:, 2]).all()
+
+
+def test_k_sampling_and_errors():
+    bg = background("disco_notebook", 256)
+    k = pert.k_sampling(bg, 1e-4, 1.0, 64, "camb")
+    assert k.shape == (64,) and np.all(np.diff(k) > 0)
+    with pytest.raises(ValueError):
+        pert.k_sampling(bg, 1e-4, 1.0, 64, "nope")
+    with pytest.raises(ValueError):
+        pert.k_sampling({}, 1e-4, 1.0, 64, "camb")
+    with pytest.raises(ValueError):
+        pert.evolve_perturbations_batched(param=bg, aexp_out=[1.0], kmin=1e-4, kmax=1.0, num_k=10, batch_size=4)
+
+
+def test_get_power_formula():
+    p = {"A_s": 2.1e-9, "n_s": 0.965, "k_p": 0.05}
+    k = np.array([0.01, 0.1])
+    y = np.zeros((2, 1, 20))
+    y[:, 0, 4] = [3.0, 4.0]
+    P = pert.get_power(k=k, y=y[:, -1, :], idx=4, param=p)
+    np.testing.assert_allclose(P, 2 * np.pi**2 * 2.1e-9 * (k / 0.05) ** -0.035 * k ** -3 * np.array([9.0, 16.0]))
+
+
+def test_library_exports_every_declared_symbol():
+    path = os.path.join(ROOT, "disco-eb_b200", "discoeb_b200", _abi.LIB_NAME)
+    if not os.path.exists(path):
+        subprocess.run(["python", os.path.join(ROOT, "disco-eb_b200", "build.py")], check=True)
+    declared = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", h)).read()
+            declared |= set(re.findall(r"^\s*(?:int32_t|void|double)\s+(discoeb_\w+)\s*\(", txt, re.M))
+    assert {"discoeb_fwd", "discoeb_rhs", "discoeb_nvar", "discoeb_abi_version"} <= declared
+    lib = ctypes.CDLL(path)
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert lib.discoeb_abi_version() == _abi.ABI_VERSION
+    c = _abi.DiscoebCosmo()
+    c.lmaxg, c.lmaxgp, c.lmaxr, c.lmaxnu, c.nqmax = 12, 12, 17, 17, 5
+    lib.discoeb_nvar.restype = ctypes.c_int32
+    assert lib.discoeb_nvar(ctypes.byref(c)) == 143
+
+
+def test_struct_layout_matches_header():
+    # the ctypes mirror must have the C layout: compile a tiny probe of offsetof/sizeof
+    import tempfile
+    src = r'''
+#include <stddef.h>
+#include <stdio.h>
+#include "discoeb.h"
+int main(void){printf("%zu %zu %zu %zu %zu\n", sizeof(DiscoebCosmo), offsetof(DiscoebCosmo, q),
+ offsetof(DiscoebCosmo, xe_loga), sizeof(DiscoebControl), offsetof(DiscoebControl, max_steps));return 0;}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        open(os.path.join(d, "p.c"), "w").write(src)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", os.path.join(d, "p"), os.path.join(d, "p.c")],
+                       check=True)
+        out = subprocess.run([os.path.join(d, "p")], capture_output=True, text=True, check=True).stdout.split()
+    C, K = _abi.DiscoebCosmo, _abi.DiscoebControl
+    assert [int(v) for v in out] == [ctypes.sizeof(C), C.q.offset, C.xe_loga.offset, ctypes.sizeof(K),
+                                     K.max_steps.offset]
