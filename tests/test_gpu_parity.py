@@ -40,9 +40,10 @@ def test_gpu_rhs_matches_oracle(torch_cuda):
             np.testing.assert_allclose(f[i, j], fo, rtol=0, atol=1e-12 * np.abs(fo).max())
 
 
-def _oracle_outputs(bg, ks, aout, L, rtol, atol, guard=1e-9):
+def _oracle_outputs(bg, ks, aout, L, rtol, atol, guard=1e-9, full=False):
     y, _, st = O.evolve_perturbations(param=bg, aexp_out=aout, kmin=0, kmax=0, num_k=0, rtol=rtol, atol=atol,
-                                      max_steps=200000, kmodes=ks, mode="clip", de_guard_eps=guard, **L)
+                                      max_steps=200000, kmodes=ks, mode="clip", de_guard_eps=guard, return_full=full,
+                                      **L)
     assert all(s[3] == 0 for s in st)
     return y
 
@@ -86,7 +87,8 @@ def test_gpu_full_state_and_projection(torch_cuda):
     y, k, p = evolve_perturbations(param=dict(bg), aexp_out=aout, kmin=1e-3, kmax=1.0, num_k=6, rtol=1e-5, atol=1e-8,
                                    return_full=True, k_sampling_method="log", max_steps=4096)
     assert y.shape == (6, 7, 72) and p["nout"] == 7
-    yo = _oracle_outputs(bg, k, aout, dict(lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3), 1e-5, 1e-8, 0.0)
+    yo = _oracle_outputs(bg, k, aout, dict(lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3), 1e-5, 1e-8, 0.0,
+                         full=True)
     np.testing.assert_allclose(y[:, :, 3], yo[:, :, 3], rtol=1e-6)
     np.testing.assert_allclose(y[:, :, 7], yo[:, :, 7], rtol=1e-5, atol=1e-9 * np.abs(yo[:, :, 7]).max())
 
