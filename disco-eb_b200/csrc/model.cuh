@@ -18,6 +18,7 @@
 
 #include "dual.cuh"
 #include "discoeb.h"
+#include "team.cuh"
 
 #if defined(__CUDACC__) && defined(__CUDA_ARCH__)
 #define DLDG(p) __ldg(p)
@@ -95,10 +96,33 @@ template <class T> DHD T spline_eval(const DiscoebSpline& s, T xn) { return spli
 
 // ---- background quantities at (a, tau) ----
 template <class T> struct Bg {
-    T a, a2, aH, opac, tauc, taucprime, cs2, pb43, rho_Q, w_Q, ca2_Q, pnu, aprimeprimeoa;
-    T v[DISCOEB_MAX_NQ];
+    T a, ia, a2, ia2, aH, iaHG, opac, po, tauc, taucprime, cs2, pb43, rho_Q, w_Q, opw, iopw, ca2_Q, pnu;
+    T rsa_fac, rsa_tcs;  // 3/(k^2 tau_c), tau_c'/tau_c (RSA fields)
+    T aprimeprimeoa;
+    double itau;
     bool rsa, ufa, tca, de_frozen;
 };
+
+DHD double rcp(double x)
+{
+#if defined(__CUDA_ARCH__)
+    return __drcp_rn(x);
+#else
+    return 1.0 / x;
+#endif
+}
+DHD Dual rcp(const Dual& x)
+{
+    const double r = rcp(x.v);
+    return Dual(r, -r * r * x.d);
+}
+
+// velocity of momentum bin q: v = 1/sqrt(1 + (a m/q)^2), and its inverse
+template <class T> DHD T inv_vq(const DiscoebCosmo& P, const Bg<T>& b, int q)
+{
+    const T aq = b.a * (P.amnu / P.q[q]);
+    return xsqrt(1.0 + aq * aq);
+}
 
 template <class T> DHD T aprimeoa_of(const DiscoebCosmo& P, T a, T loga)
 {
@@ -109,44 +133,108 @@ template <class T> DHD T aprimeoa_of(const DiscoebCosmo& P, T a, T loga)
     return xsqrt(grho / 3.0);
 }
 
+// index of a non-uniform spline searched from a hint (the previous index): same result
+// as spline_index (count of knots below xn, minus one, clipped) in O(|step|) loads
+DHD int spline_index_from(const DiscoebSpline& s, double xn, int& hint)
+{
+    if (s.uniform) return spline_index(s, xn);
+    const int n = s.n_knots;
+    int i = hint < 0 ? 0 : (hint > n - 2 ? n - 2 : hint);
+    while (i > 0 && !(DLDG(s.x + i) < xn)) --i;
+    while (i < n - 2 && DLDG(s.x + i + 1) < xn) ++i;
+    hint = i;
+    return i;
+}
+
+// The six table-derived quantities at log a: xe, dxe/dloga, cs2*a, rho_nu, p_nu, rho_Q.
+// Table slot t (0..4) is computed by one lane of a team (t % nl), with the same
+// instruction stream on every lane, and broadcast.
+template <class T> struct BgTables {
+    T xe, xep, cs2a, rhonu, pnu, rho_Q;
+};
+
+template <class T>
+DHD T table_slot_value(const DiscoebCosmo& P, int t, T a, T loga, int& hint, T& deriv)
+{
+    // t: 0 xe (and its derivative), 1 cs2*a, 2 log rho_nu, 3 log p_nu, 4 log rho_Q
+    if (t == 4) {
+        deriv = 0.0;
+        return -3.0 * (1.0 + P.w0 + P.wa) * loga + 3.0 * (a - 1.0) * P.wa;
+    }
+    const DiscoebSpline& s = t == 0 ? P.xe_loga : (t == 1 ? P.cs2a_loga : (t == 2 ? P.logrhonu_loga : P.logpnu_loga));
+    int h = hint;
+    const int i = spline_index_from(s, val(loga), h);
+    if (t == 0) hint = h;
+    deriv = spline_deriv_at(s, i, loga);
+    return spline_eval_at(s, i, loga);
+}
+
+template <class TM, class T>
+DHD BgTables<T> bg_tables(const TM& tm, const DiscoebCosmo& P, T a, int& hint)
+{
+    const T loga = xlog(a);
+    BgTables<T> r;
+    if (tm.nl == 1) {
+        T d;
+        int h = hint;
+        r.xe = table_slot_value(P, 0, a, loga, h, r.xep);
+        r.cs2a = table_slot_value(P, 1, a, loga, hint, d);
+        r.rhonu = xexp(table_slot_value(P, 2, a, loga, hint, d));
+        r.pnu = xexp(table_slot_value(P, 3, a, loga, hint, d));
+        r.rho_Q = xexp(table_slot_value(P, 4, a, loga, hint, d));
+        hint = h;
+        return r;
+    }
+    // lanes 0..4 each evaluate one table slot with the same instruction stream, then broadcast
+    T v = 0.0, d = 0.0;
+    int h = hint;
+    if (tm.lane < 5) {
+        v = table_slot_value(P, tm.lane, a, loga, h, d);
+        if (tm.lane >= 2) v = xexp(v);
+    }
+    r.xe = tm.bcast(v, 0);
+    r.xep = tm.bcast(d, 0);
+    r.cs2a = tm.bcast(v, 1);
+    r.rhonu = tm.bcast(v, 2);
+    r.pnu = tm.bcast(v, 3);
+    r.rho_Q = tm.bcast(v, 4);
+    hint = (int)tm.bcast((double)h, 0);
+    return r;
+}
+
 // regime < 0: switches from (tau, a) exactly as model_synchronous evaluates them;
 // otherwise bitmask 1 = RSA, 2 = UFA, 4 = TCA.
-template <class T> DHD void bg_eval(const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b)
+template <class T>
+DHD void bg_finish(const DiscoebCosmo& P, T a, const BgTables<T>& tb, double tau, double k, int regime, Bg<T>& b)
 {
     b.a = a;
+    b.ia = rcp(a);
     b.a2 = a * a;
-    T loga = xlog(a);
-    // xe and cs2*a share the knot grid (both tabulated on log of the Recfast a-grid)
-    int ix = spline_index(P.xe_loga, val(loga));
-    T xe = spline_eval_at(P.xe_loga, ix, loga);
-    T xep = spline_deriv_at(P.xe_loga, ix, loga);
-    int ic = (P.cs2a_loga.x == P.xe_loga.x) ? ix : spline_index(P.cs2a_loga, val(loga));
-    b.cs2 = spline_eval_at(P.cs2a_loga, ic, loga) / a;
-    int inu = spline_index(P.logrhonu_loga, val(loga));
-    T rhonu = xexp(spline_eval_at(P.logrhonu_loga, inu, loga));
-    int ip = (P.logpnu_loga.x == P.logrhonu_loga.x) ? inu : spline_index(P.logpnu_loga, val(loga));
-    b.pnu = xexp(spline_eval_at(P.logpnu_loga, ip, loga));
-    T photbar = P.grhog / (P.grhom * P.Omegab * a);
-    b.pb43 = 4.0 / 3.0 * photbar;
+    b.ia2 = b.ia * b.ia;
+    b.itau = rcp(tau);
+    const T& xe = tb.xe;
+    b.cs2 = tb.cs2a * b.ia;
+    b.pnu = tb.pnu;
+    b.pb43 = (4.0 / 3.0) * P.grhog / (P.grhom * P.Omegab) * b.ia;
     b.w_Q = P.w0 + P.wa * (1.0 - a);
-    b.rho_Q = xpow(a, -3.0 * (1.0 + P.w0 + P.wa)) * xexp(3.0 * (a - 1.0) * P.wa);
-    T grho = P.grhom * P.Omegam / a + (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / b.a2 +
+    b.opw = 1.0 + b.w_Q;
+    b.iopw = rcp(b.opw);
+    b.rho_Q = tb.rho_Q;
+    T grho = P.grhom * P.Omegam * b.ia + (P.grhog + P.grhor * (P.Neff + P.Nmnu * tb.rhonu)) * b.ia2 +
              P.grhom * P.OmegaDE * b.rho_Q * b.a2 + P.grhom * P.Omegak;
-    b.aH = xsqrt(grho / 3.0);
-    T xeprime = xep * b.aH;
-    T gpres = ((P.grhog + P.grhor * P.Neff) / 3.0 + P.grhor * P.Nmnu * b.pnu) / b.a2 +
+    b.aH = xsqrt(grho * (1.0 / 3.0));
+    const T iaH = rcp(b.aH);
+    T xeprime = tb.xep * b.aH;
+    T gpres = ((P.grhog + P.grhor * P.Neff) * (1.0 / 3.0) + P.grhor * P.Nmnu * b.pnu) * b.ia2 +
               b.w_Q * P.grhom * P.OmegaDE * b.rho_Q * b.a2;
     b.aprimeprimeoa = 0.5 * (b.aH * b.aH - gpres);
     T w_Q_prime = -P.wa * b.aH * a;
-    b.ca2_Q = b.w_Q - w_Q_prime / 3.0 / ((1.0 + b.w_Q) + 1e-6) / b.aH;
+    b.ca2_Q = b.w_Q - w_Q_prime * (1.0 / 3.0) / ((1.0 + b.w_Q) + 1e-6) * iaH;
     const double akthom = 2.3038921003709498e-9 * (1.0 - P.YHe) * P.Omegab * P.H0 * P.H0;
-    b.opac = xe * akthom / b.a2;
-    b.tauc = 1.0 / xmaxc(b.opac, 1e-30);
+    b.opac = xe * akthom * b.ia2;
+    b.po = b.pb43 * b.opac;
+    b.tauc = rcp(xmaxc(b.opac, 1e-30));
     b.taucprime = b.tauc * (2.0 * b.aH - xeprime / xmaxc(xe, 1e-30));
-    for (int q = 0; q < P.nqmax; ++q) {
-        T aq = a * (P.amnu / P.q[q]);
-        b.v[q] = 1.0 / xsqrt(1.0 + aq * aq);
-    }
     if (regime < 0) {
         double tcr = val(b.tauc), thr = 1.0 / (val(b.aH) > 1e-30 ? val(b.aH) : 1e-30);
         double tk = 1.0 / (k > 1e-30 ? k : 1e-30);
@@ -160,10 +248,57 @@ template <class T> DHD void bg_eval(const DiscoebCosmo& P, T a, double tau, doub
         b.ufa = !b.rsa && (regime & 2) != 0;
         b.tca = !b.rsa && (regime & 4) != 0;
     }
+    b.iaHG = b.rsa ? rcp(xmaxc(b.aH, 1e-30)) : iaH;
+    if (b.rsa) {
+        const double k2 = k * k, sk2 = k2 > 1e-30 ? k2 : 1e-30;
+        const T stc = xmaxc(b.tauc, 1e-30);
+        const T istc = rcp(stc);
+        b.rsa_fac = (3.0 / sk2) * istc;
+        b.rsa_tcs = b.taucprime * istc;
+    } else {
+        b.rsa_fac = 0.0;
+        b.rsa_tcs = 0.0;
+    }
     b.de_frozen = P.de_guard_eps > 0.0 && fabs(val(1.0 + b.w_Q)) < P.de_guard_eps;
 }
 
+template <class TM, class T>
+DHD void bg_eval_team(const TM& tm, const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b, int& hint)
+{
+    const BgTables<T> tb = bg_tables(tm, P, a, hint);
+    bg_finish(P, a, tb, tau, k, regime, b);
+}
+
+template <class T>
+DHD void bg_eval(const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b, int& hint)
+{
+    bg_eval_team(HostTeam(), P, a, tau, k, regime, b, hint);
+}
+
+template <class T> DHD void bg_eval(const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b)
+{
+    int hint = P.xe_loga.n_knots / 2;
+    bg_eval(P, a, tau, k, regime, b, hint);
+}
+
 DHD double dlfdlq_of(double q) { return -q / (1.0 + exp(-q)); }
+
+// 1/(2l+1)
+DHD double inv_odd(int l) { return rcp(2.0 * l + 1.0); }
+
+// ---- slots: the state indices read by the functionals G and the leaf row F1 ----
+DHD int n_slots(const Dims& D) { return 14 + 2 * D.nq; }
+DHD int slot_index(const Dims& D, int s)
+{
+    if (s < 8) return 2 + s;
+    if (s == 8) return D.idxgp;
+    if (s == 9) return D.idxgp + 2;
+    if (s == 10) return D.idxr;
+    if (s == 11) return D.idxr + 1;
+    if (s < 12 + D.nq) return D.iq0 + (s - 12);
+    if (s < 12 + 2 * D.nq) return D.iq0 + D.nq + (s - 12 - D.nq);
+    return s == 12 + 2 * D.nq ? D.n - 2 : D.n - 1;
+}
 
 // ---- G: column j of the three functionals (h', eta', polter) ----
 template <class T>
@@ -172,35 +307,35 @@ DHD void gcol(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, in
     g[0] = 0.0; g[1] = 0.0; g[2] = 0.0;
     const double k2 = k * k;
     const double Omegac = P.Omegam - P.Omegab;
-    const T a = b.a, a2 = b.a2;
-    const T invaH = 1.0 / (b.rsa ? xmaxc(b.aH, 1e-30) : b.aH);
+    const T& ia = b.ia;
+    const T& ia2 = b.ia2;
+    const T& invaH = b.iaHG;
     const double hE = 0.5 / k2;
     const int nq = D.nq;
     // h' = (2 k^2 eta + dgrho) / (a'/a)   (perturbations.py:294-306, :346)
     if (j == 2) g[0] = 2.0 * k2 * invaH;
-    else if (j == 3) g[0] = P.grhom * Omegac / a * invaH;
-    else if (j == 5) g[0] = P.grhom * P.Omegab / a * invaH;
-    else if (j == 7) { if (!b.rsa) g[0] = P.grhog / a2 * invaH; }
-    else if (j == D.idxr) { if (!b.rsa) g[0] = P.grhor * P.Neff / a2 * invaH; }
-    else if (j >= D.iq0 && j < D.iq0 + nq) { int q = j - D.iq0; g[0] = P.grhor * P.Nmnu * P.wq[q] / b.v[q] / a2 * invaH; }
-    else if (j == D.n - 2) g[0] = P.grhom * P.OmegaDE * b.rho_Q * a2 * invaH;
+    else if (j == 3) g[0] = P.grhom * Omegac * ia * invaH;
+    else if (j == 5) g[0] = P.grhom * P.Omegab * ia * invaH;
+    else if (j == 7) { if (!b.rsa) g[0] = P.grhog * ia2 * invaH; }
+    else if (j == D.idxr) { if (!b.rsa) g[0] = P.grhor * P.Neff * ia2 * invaH; }
+    else if (j >= D.iq0 && j < D.iq0 + nq) { int q = j - D.iq0; g[0] = P.grhor * P.Nmnu * P.wq[q] * inv_vq(P, b, q) * ia2 * invaH; }
+    else if (j == D.n - 2) g[0] = P.grhom * P.OmegaDE * b.rho_Q * b.a2 * invaH;
     // eta' = dgtheta / (2 k^2)   (perturbations.py:330-335, :349)
-    if (j == 4) g[1] = hE * P.grhom * Omegac / a;
-    else if (j == 6) g[1] = hE * P.grhom * P.Omegab / a;
-    else if (j == 8) { if (!b.rsa) g[1] = hE * (4.0 / 3.0) * P.grhog / a2; }
-    else if (j == D.idxr + 1) { if (!b.rsa) g[1] = hE * (4.0 / 3.0) * P.Neff * P.grhor / a2; }
-    else if (j >= D.iq0 + nq && j < D.iq0 + 2 * nq) { int q = j - D.iq0 - nq; g[1] = hE * P.Nmnu * P.grhor * k * P.wq[q] / a2; }
-    else if (j == D.n - 1) g[1] = hE * (1.0 + b.w_Q) * b.rho_Q * P.grhom * P.OmegaDE * a2;
+    if (j == 4) g[1] = hE * P.grhom * Omegac * ia;
+    else if (j == 6) g[1] = hE * P.grhom * P.Omegab * ia;
+    else if (j == 8) { if (!b.rsa) g[1] = hE * (4.0 / 3.0) * P.grhog * ia2; }
+    else if (j == D.idxr + 1) { if (!b.rsa) g[1] = hE * (4.0 / 3.0) * P.Neff * P.grhor * ia2; }
+    else if (j >= D.iq0 + nq && j < D.iq0 + 2 * nq) { int q = j - D.iq0 - nq; g[1] = hE * P.Nmnu * P.grhor * k * P.wq[q] * ia2; }
+    else if (j == D.n - 1) g[1] = hE * b.opw * b.rho_Q * P.grhom * P.OmegaDE * b.a2;
     if (b.rsa) {
         // theta_gamma and theta_r replaced by the RSA fields (approximations.py:28-47)
         const double sk2 = k2 > 1e-30 ? k2 : 1e-30;
-        const T stc = xmaxc(b.tauc, 1e-30);
-        const T cg = hE * (4.0 / 3.0) * P.grhog / a2;
-        const T fac = 3.0 / (sk2 * stc);
-        if (j == 6) g[1] = g[1] + cg * fac * (-b.taucprime / stc - b.aH);
+        const T cg = hE * (4.0 / 3.0) * P.grhog * ia2;
+        const T& fac = b.rsa_fac;
+        if (j == 6) g[1] = g[1] + cg * fac * (-b.rsa_tcs - b.aH);
         else if (j == 5) g[1] = g[1] + cg * fac * (b.cs2 * sk2);
         else if (j == 2) g[1] = g[1] + cg * fac * sk2;
-        const T eH = cg * (-0.5 - 0.5 * fac * b.taucprime / stc) + hE * (4.0 / 3.0) * P.Neff * P.grhor / a2 * (-0.5);
+        const T eH = cg * (-0.5 - 0.5 * fac * b.rsa_tcs) + hE * (4.0 / 3.0) * P.Neff * P.grhor * ia2 * (-0.5);
         g[1] = g[1] + eH * g[0];
     } else if (!b.tca) {
         if (j == 9 || j == D.idxgp || j == D.idxgp + 2) g[2] = 1.0;
@@ -215,24 +350,21 @@ DHD void rowc(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, do
     etac = 0.0;
     u[0] = 0.0; u[1] = 0.0; u[2] = 0.0;
     const double k2 = k * k;
-    if (i == 2) { u[1] = 1.0; return; }
-    if (i == 3) { band[4] = -1.0; u[0] = -0.5; return; }
-    if (i == 4) { band[3] = -b.aH; return; }
-    if (i == 5) { band[4] = -1.0; u[0] = -0.5; return; }
-    if (i == 6) {
-        const T po = b.pb43 * b.opac;
-        if (!b.rsa) {
+    if (i < 7) {
+        if (i == 2) { u[1] = 1.0; }
+        else if (i == 3 || i == 5) { band[4] = -1.0; u[0] = -0.5; }
+        else if (i == 4) { band[3] = -b.aH; }
+        else if (!b.rsa) {  // i == 6: baryon velocity
             band[2] = k2 * b.cs2;
-            band[3] = -b.aH - po;
-            band[5] = po;
+            band[3] = -b.aH - b.po;
+            band[5] = b.po;
         } else {
             const double sk2 = k2 > 1e-30 ? k2 : 1e-30;
-            const T stc = xmaxc(b.tauc, 1e-30);
-            const T fac = 3.0 / (sk2 * stc);
-            band[2] = k2 * b.cs2 + po * fac * (b.cs2 * sk2);
-            band[3] = -b.aH - po + po * fac * (-b.taucprime / stc - b.aH);
-            etac = po * fac * sk2;
-            u[0] = po * (-0.5 - 0.5 * fac * b.taucprime / stc);
+            const T pf = b.po * b.rsa_fac;
+            band[2] = k2 * b.cs2 + pf * (b.cs2 * sk2);
+            band[3] = -b.aH - b.po + pf * (-b.rsa_tcs - b.aH);
+            etac = pf * sk2;
+            u[0] = b.po * (-0.5 - 0.5 * b.rsa_fac * b.rsa_tcs);
         }
         return;
     }
@@ -245,9 +377,10 @@ DHD void rowc(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, do
             band[2] = 8.0 / 15.0; band[3] = -b.opac; band[4] = -0.6 * k;
             u[0] = 4.0 / 15.0; u[1] = 8.0 / 5.0; u[2] = 0.1 * b.opac;
         } else if (l < L) {
-            band[2] = k * l / (2.0 * l + 1.0); band[3] = -b.opac; band[4] = -k * (l + 1.0) / (2.0 * l + 1.0);
+            const double ki = k * inv_odd(l);
+            band[2] = ki * l; band[3] = -b.opac; band[4] = -ki * (l + 1.0);
         } else {
-            band[2] = k; band[3] = -(L + 1.0) / tau - b.opac;
+            band[2] = k; band[3] = -(L + 1.0) * b.itau - b.opac;
         }
         return;
     }
@@ -255,13 +388,14 @@ DHD void rowc(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, do
         if (b.rsa || b.tca) return;
         const int l = i - D.idxgp, L = D.lmaxgp;
         if (l < L) {
-            if (l > 0) band[2] = k * l / (2.0 * l + 1.0);
+            const double ki = k * inv_odd(l);
+            band[2] = ki * l;
             band[3] = -b.opac;
-            band[4] = -k * (l + 1.0) / (2.0 * l + 1.0);
+            band[4] = -ki * (l + 1.0);
             if (l == 0) u[2] = 0.5 * b.opac;
             if (l == 2) u[2] = 0.1 * b.opac;
         } else {
-            band[2] = k; band[3] = -(L + 1.0) / tau - b.opac;
+            band[2] = k; band[3] = -(L + 1.0) * b.itau - b.opac;
         }
         return;
     }
@@ -273,37 +407,36 @@ DHD void rowc(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, do
         else if (l == 2) {
             if (b.ufa) {
                 band[2] = 4.0 / 15.0;
-                band[3] = -1.5 / (tau > 1e-30 ? tau : 1e-30);
+                band[3] = -1.5 * (tau > 1e-30 ? b.itau : 1e30);
                 u[0] = 2.0 / 15.0;
             } else {
                 band[2] = 8.0 / 15.0; band[4] = -0.6 * k; u[0] = 4.0 / 15.0; u[1] = 8.0 / 5.0;
             }
         } else if (!b.ufa) {
-            if (l < L) { band[2] = k * l / (2.0 * l + 1.0); band[4] = -k * (l + 1.0) / (2.0 * l + 1.0); }
-            else { band[2] = k; band[3] = -(L + 1.0) / tau; }
+            if (l < L) { const double ki = k * inv_odd(l); band[2] = ki * l; band[4] = -ki * (l + 1.0); }
+            else { band[2] = k; band[3] = -(L + 1.0) * b.itau; }
         }
         return;
     }
     if (i < D.n - 2) {  // massive neutrinos, l-major blocks of nq bins
         const int r = i - D.iq0, l = r / D.nq, q = r - l * D.nq, L = D.lmaxnu;
-        const T kv = k * b.v[q];
+        const T kv = k * rcp(inv_vq(P, b, q));
         const double dl = dlfdlq_of(P.q[q]);
-        if (l == 0) { band[4] = -kv; u[0] = dl / 6.0; }
-        else if (l == 1) { band[2] = kv / 3.0; band[4] = -2.0 * kv / 3.0; }
-        else if (l == 2 && L > 2) { band[2] = 2.0 * kv / 5.0; band[4] = -3.0 * kv / 5.0; u[0] = -dl / 15.0; u[1] = -0.4 * dl; }
-        else if (l < L) { band[2] = kv * (double)l / (2.0 * l + 1.0); band[4] = -kv * (l + 1.0) / (2.0 * l + 1.0); }
-        else { band[2] = kv; band[3] = -(L + 1.0) / tau; }
+        if (l == 0) { band[4] = -kv; u[0] = dl * (1.0 / 6.0); }
+        else if (l == 1) { band[2] = kv * (1.0 / 3.0); band[4] = -2.0 * kv * (1.0 / 3.0); }
+        else if (l == 2 && L > 2) { band[2] = 2.0 * kv * 0.2; band[4] = -3.0 * kv * 0.2; u[0] = -dl * (1.0 / 15.0); u[1] = -0.4 * dl; }
+        else if (l < L) { const double io = inv_odd(l); band[2] = kv * ((double)l * io); band[4] = -kv * ((l + 1.0) * io); }
+        else { band[2] = kv; band[3] = -(L + 1.0) * b.itau; }
         return;
     }
     if (b.de_frozen) return;
     const double cs2Q = P.cs2_DE;
-    const T opw = 1.0 + b.w_Q;
     if (i == D.n - 2) {
         band[3] = -3.0 * (cs2Q - b.w_Q) * b.aH;
-        band[4] = -opw - 9.0 * opw * (cs2Q - b.ca2_Q) * b.aH * b.aH / k2;
-        u[0] = -0.5 * opw;
+        band[4] = -b.opw - 9.0 * b.opw * (cs2Q - b.ca2_Q) * b.aH * b.aH * (1.0 / k2);
+        u[0] = -0.5 * b.opw;
     } else {
-        band[2] = cs2Q / opw * k2;
+        band[2] = cs2Q * b.iopw * k2;
         band[3] = -(1.0 - 3.0 * cs2Q) * b.aH;
     }
 }
@@ -314,30 +447,31 @@ DHD T f1col(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, int 
 {
     const double k2 = k * k;
     const double Omegac = P.Omegam - P.Omegab;
-    const T a = b.a, a2 = b.a2;
+    const T& ia = b.ia;
+    const T& ia2 = b.ia2;
     const int nq = D.nq;
     T rho = 0.0, pres = 0.0;  // coefficients of y_j in dgrho and dgpres
-    if (j == 3) rho = P.grhom * Omegac / a;
-    else if (j == 5) rho = P.grhom * P.Omegab / a;
-    else if (j == 7) { rho = P.grhog / a2; if (!b.rsa) pres = P.grhog / a2 / 3.0; }
-    else if (j == D.idxr) { rho = P.grhor * P.Neff / a2; if (!b.rsa) pres = P.grhor * P.Neff / a2 / 3.0; }
+    if (j == 3) rho = P.grhom * Omegac * ia;
+    else if (j == 5) rho = P.grhom * P.Omegab * ia;
+    else if (j == 7) { rho = P.grhog * ia2; if (!b.rsa) pres = P.grhog * ia2 * (1.0 / 3.0); }
+    else if (j == D.idxr) { rho = P.grhor * P.Neff * ia2; if (!b.rsa) pres = P.grhor * P.Neff * ia2 * (1.0 / 3.0); }
     else if (j >= D.iq0 && j < D.iq0 + nq) {
-        int q = j - D.iq0;
-        rho = P.grhor * P.Nmnu * P.wq[q] / b.v[q] / a2;
-        pres = P.grhor * P.Nmnu / a2 * P.wq[q] * b.v[q] / 3.0;
+        const int q = j - D.iq0;
+        const T iv = inv_vq(P, b, q);
+        rho = P.grhor * P.Nmnu * P.wq[q] * iv * ia2;
+        pres = P.grhor * P.Nmnu * ia2 * P.wq[q] * rcp(iv) * (1.0 / 3.0);
     } else if (j == D.n - 2) {
-        rho = P.grhom * P.OmegaDE * b.rho_Q * a2;
-        pres = P.cs2_DE * P.grhom * P.OmegaDE * b.rho_Q * a2;
+        rho = P.grhom * P.OmegaDE * b.rho_Q * b.a2;
+        pres = P.cs2_DE * P.grhom * P.OmegaDE * b.rho_Q * b.a2;
     } else if (j == D.n - 1) {
-        pres = (P.cs2_DE - b.ca2_Q) * (3.0 * b.aH * (1.0 + b.w_Q) * b.rho_Q * P.grhom * P.OmegaDE * a2 / k2);
+        pres = (P.cs2_DE - b.ca2_Q) * (3.0 * b.aH * b.opw * b.rho_Q * P.grhom * P.OmegaDE * b.a2 * (1.0 / k2));
     }
     if (b.rsa) {
         const double sk2 = k2 > 1e-30 ? k2 : 1e-30;
-        const T stc = xmaxc(b.tauc, 1e-30);
-        if (j == 2) pres = pres + (P.grhog + P.grhor * P.Neff) / a2 / 3.0 * (-4.0);
-        else if (j == 6) pres = pres + P.grhog / a2 / 3.0 * (4.0 / (sk2 * stc));
+        if (j == 2) pres = pres + (P.grhog + P.grhor * P.Neff) * ia2 * (1.0 / 3.0) * (-4.0);
+        else if (j == 6) pres = pres + P.grhog * ia2 * (1.0 / 3.0) * (4.0 / sk2) * (b.rsa_fac * (sk2 / 3.0));
     }
-    return -a * (rho + 3.0 * pres);
+    return -b.a * (rho + 3.0 * pres);
 }
 
 template <class T>
@@ -346,9 +480,9 @@ DHD void f1u(const DiscoebCosmo& P, const Bg<T>& b, double k, T u[3])
     u[0] = 0.0; u[1] = 0.0; u[2] = 0.0;
     if (b.rsa) {
         const double k2 = k * k, sk2 = k2 > 1e-30 ? k2 : 1e-30;
-        const T stc = xmaxc(b.tauc, 1e-30);
-        const T a2 = b.a2;
-        T presH = P.grhog / a2 / 3.0 * (4.0 * b.aH / sk2 + 2.0 / (sk2 * stc)) + P.grhor * P.Neff / a2 / 3.0 * (4.0 * b.aH / sk2);
+        const T itc = b.rsa_fac * (sk2 / 3.0);  // 1 / max(tau_c, 1e-30)
+        T presH = P.grhog * b.ia2 * (1.0 / 3.0) * (4.0 * b.aH / sk2 + 2.0 / sk2 * itc) +
+                  P.grhor * P.Neff * b.ia2 * (1.0 / 3.0) * (4.0 * b.aH / sk2);
         u[0] = -b.a * 3.0 * presH;
     }
 }

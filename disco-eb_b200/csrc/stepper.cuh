@@ -78,10 +78,11 @@ DHD Chain chain_of(const Dims& D, int c)
 }
 
 // number of doubles of per-mode workspace
-DHD int mode_mem_doubles(const Dims& D) { return 27 * D.n + 32; }
+constexpr int kMaxSlots = 48;  // >= 14 + 2 * DISCOEB_MAX_NQ
+DHD int mode_mem_doubles(const Dims& D) { return 23 * D.n + 4 * kMaxSlots + 32; }
 
 struct ModeMem {
-    double *y, *u, *f, *dT, *col0, *F1, *K, *A, *G, *Z, *sc;
+    double *y, *u, *f, *dT, *col0, *K, *A, *Z, *Gs, *F1s, *sc;
 };
 
 DHD ModeMem carve(double* base, const Dims& D)
@@ -93,16 +94,16 @@ DHD ModeMem carve(double* base, const Dims& D)
     m.f = m.u + n;
     m.dT = m.f + n;
     m.col0 = m.dT + n;
-    m.F1 = m.col0 + n;
-    m.K = m.F1 + n;      // 8n
-    m.A = m.K + 8 * n;   // 7n
-    m.G = m.A + 7 * n;   // 3n
-    m.Z = m.G + 3 * n;   // 3n
-    m.sc = m.Z + 3 * n;  // 32 scalars
+    m.K = m.col0 + n;          // 8n stage vectors
+    m.A = m.K + 8 * n;         // 7n banded chain factors
+    m.Z = m.A + 7 * n;         // 3n  A^{-1} U
+    m.Gs = m.Z + 3 * n;        // 3 x kMaxSlots functional rows on the slot list
+    m.F1s = m.Gs + 3 * kMaxSlots;
+    m.sc = m.F1s + kMaxSlots;  // 32 scalars
     return m;
 }
 // scalar slots
-enum { SC_W00 = 0, SC_ETAC = 1, SC_CINV = 2, SC_F1Z = 11, SC_F1U = 14, SC_GH = 17 };
+enum { SC_W00 = 0, SC_ETAC = 1, SC_CINV = 2, SC_F1Z = 11, SC_F1U = 14 };
 
 DHD double dual_with(double x, double) { return x; }
 DHD Dual dual_with(const Dual& x, double d) { return Dual(x.v, d); }
@@ -113,8 +114,10 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
                   const double* y, double* f, double* dfda)
 {
     const int n = D.n;
+    const int ns = n_slots(D);
     T g0 = 0.0, g1 = 0.0, g2 = 0.0, s1 = 0.0;
-    for (int j = tm.lane; j < n; j += tm.nl) {
+    for (int sl = tm.lane; sl < ns; sl += tm.nl) {
+        const int j = slot_index(D, sl);
         T gc[3];
         gcol(P, D, b, k, j, gc);
         const double yj = y[j];
@@ -233,12 +236,16 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
         M.Z[i] = u[0];
         M.Z[n + i] = u[1];
         M.Z[2 * n + i] = u[2];
+    }
+    const int ns = n_slots(D);
+    for (int sl = tm.lane; sl < ns; sl += tm.nl) {
+        const int j = slot_index(D, sl);
         double gc[3];
-        gcol(P, D, b, k, i, gc);
-        M.G[i] = gc[0];
-        M.G[n + i] = gc[1];
-        M.G[2 * n + i] = gc[2];
-        M.F1[i] = (i >= 2) ? f1col(P, D, b, k, i) : 0.0;
+        gcol(P, D, b, k, j, gc);
+        M.Gs[sl] = gc[0];
+        M.Gs[kMaxSlots + sl] = gc[1];
+        M.Gs[2 * kMaxSlots + sl] = gc[2];
+        M.F1s[sl] = f1col(P, D, b, k, j);
     }
     if (tm.leader()) {
         M.sc[SC_W00] = igh - M.col0[0];
@@ -258,11 +265,11 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
     // C = I - G Z, F1Z = F1 . Z
     double acc[12];
     for (int q = 0; q < 12; ++q) acc[q] = 0.0;
-    for (int j = tm.lane; j < n; j += tm.nl) {
-        if (j < 2) continue;
+    for (int sl = tm.lane; sl < ns; sl += tm.nl) {
+        const int j = slot_index(D, sl);
         for (int r = 0; r < 3; ++r)
-            for (int s = 0; s < 3; ++s) acc[3 * r + s] += M.G[r * n + j] * M.Z[s * n + j];
-        for (int s = 0; s < 3; ++s) acc[9 + s] += M.F1[j] * M.Z[s * n + j];
+            for (int s = 0; s < 3; ++s) acc[3 * r + s] += M.Gs[r * kMaxSlots + sl] * M.Z[s * n + j];
+        for (int s = 0; s < 3; ++s) acc[9 + s] += M.F1s[sl] * M.Z[s * n + j];
     }
     double C[9];
     for (int q = 0; q < 9; ++q) C[q] = ((q % 4) == 0 ? 1.0 : 0.0) - tm.sum(acc[q]);
@@ -304,13 +311,13 @@ template <class TM> DDV void solve_W(const TM& tm, const Dims& D, const ModeMem&
     tm.sync();
     solve_A(tm, D, M, gh, v);
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    for (int j = tm.lane; j < n; j += tm.nl) {
-        if (j < 2) continue;
-        const double zj = v[j];
-        a0 += M.G[j] * zj;
-        a1 += M.G[n + j] * zj;
-        a2 += M.G[2 * n + j] * zj;
-        a3 += M.F1[j] * zj;
+    const int ns = n_slots(D);
+    for (int sl = tm.lane; sl < ns; sl += tm.nl) {
+        const double zj = v[slot_index(D, sl)];
+        a0 += M.Gs[sl] * zj;
+        a1 += M.Gs[kMaxSlots + sl] * zj;
+        a2 += M.Gs[2 * kMaxSlots + sl] * zj;
+        a3 += M.F1s[sl] * zj;
     }
     const double gz0 = tm.sum(a0), gz1 = tm.sum(a1), gz2 = tm.sum(a2), f1z = tm.sum(a3);
     const double* Ci = M.sc + SC_CINV;
@@ -346,15 +353,15 @@ struct SolveResult {
 // M.K[7] the error estimate.  Returns false on a non-finite factorisation.
 template <class TM>
 DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
-                     const ModeMem& M)
+                     const ModeMem& M, int& hint)
 {
     const int n = D.n;
     // Jacobian column d f/d a and f(y) in one dual pass
     Bg<Dual> bd;
-    bg_eval(P, Dual(M.y[0], 1.0), t, k, regime, bd);
+    bg_eval_team(tm, P, Dual(M.y[0], 1.0), t, k, regime, bd, hint);
     rhs_team(tm, P, D, bd, k, t, M.y, M.f, M.col0);
     Bg<double> b;
-    bg_eval(P, M.y[0], t, k, regime, b);
+    bg_eval_team(tm, P, M.y[0], t, k, regime, b, hint);
     for (int i = tm.lane; i < n; i += tm.nl) M.dT[i] = dtau_row(D, b, t, i, M.y);
     tm.sync();
     const bool ok = factor_W(tm, P, D, b, k, t, h, M);
@@ -375,7 +382,7 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
             tm.sync();
             const double ts = (s <= 5) ? t + kR5.c[s] * h : t + h;
             Bg<double> bs;
-            bg_eval(P, M.u[0], ts, k, regime, bs);
+            bg_eval_team(tm, P, M.u[0], ts, k, regime, bs, hint);
             rhs_team(tm, P, D, bs, k, ts, M.u, M.f, (double*)nullptr);
             tm.sync();
         }
@@ -411,6 +418,7 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
     int iout = 0;
     const int idx[6] = {0, 2, 3, 5, 6, 7};
     const double w6[6] = {1.0, k * k, 1.0, 1.0, 1.0 / (k * k), 1.0};
+    int hint = P.xe_loga.n_knots / 2;
     while (t < t1) {
         if (R.steps >= C.max_steps) { R.status = DISCOEB_MAX_STEPS; break; }
         double tev = t1;
@@ -424,7 +432,7 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
         const double h = tn - t;
         if (!(h > 1e-14 * fabs(t))) { R.status = DISCOEB_DT_UNDERFLOW; break; }
         const int regime = regime_at(P, t, sw);
-        const bool ok = rodas5_step(tm, P, D, k, t, h, regime, M);
+        const bool ok = rodas5_step(tm, P, D, k, t, h, regime, M, hint);
         R.steps++;
         // weighted RMS error over (a, eta, delta_c, delta_b, theta_b, delta_gamma)
         // (perturbations.py:855-878 with the weights of :913)

@@ -20,6 +20,11 @@ struct WarpTeam {
         return x;
     }
     __device__ __forceinline__ bool leader() const { return lane == 0; }
+    __device__ __forceinline__ double bcast(double x, int src) const { return __shfl_sync(0xffffffffu, x, src); }
+    __device__ __forceinline__ Dual bcast(const Dual& x, int src) const
+    {
+        return Dual(__shfl_sync(0xffffffffu, x.v, src), __shfl_sync(0xffffffffu, x.d, src));
+    }
 };
 #endif
 
@@ -29,6 +34,8 @@ struct HostTeam {
     DHD void sync() const {}
     DHD double sum(double x) const { return x; }
     DHD bool leader() const { return true; }
+    DHD double bcast(double x, int) const { return x; }
+    DHD Dual bcast(const Dual& x, int) const { return x; }
 };
 
 }  // namespace dscb
