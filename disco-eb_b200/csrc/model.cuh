@@ -441,6 +441,65 @@ DHD void rowc(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, do
     }
 }
 
+// ---- row classes ----
+// Hierarchy rows (photon temperature l >= 3, photon polarisation, massless neutrinos l >= 3,
+// massive neutrinos) are tridiagonal with coefficients that depend on (species, l) through a
+// few selects; evaluating them as one class keeps all lanes of a warp on the same path.
+// The remaining "special" rows (a, a h', eta, CDM, baryons, photon l <= 2, massless l <= 2,
+// dark energy) go through rowc.
+DHD int n_hier_rows(const Dims& D) { return (D.lmaxg - 2) + (D.lmaxgp + 1) + (D.lmaxr - 2) + D.nq * (D.lmaxnu + 1); }
+DHD int hier_row(const Dims& D, int h)
+{
+    const int nT = D.lmaxg - 2;
+    if (h < nT) return 10 + h;
+    h -= nT;
+    const int nP = D.lmaxgp + 1;
+    if (h < nP) return D.idxgp + h;
+    h -= nP;
+    const int nR = D.lmaxr - 2;
+    if (h < nR) return D.idxr + 3 + h;
+    return D.iq0 + (h - nR);
+}
+DHD int n_special_rows() { return 15; }
+DHD int special_row(const Dims& D, int s)
+{
+    if (s < 10) return s;
+    if (s < 13) return D.idxr + (s - 10);
+    return s == 13 ? D.n - 2 : D.n - 1;
+}
+// momentum bin of a massive-neutrino row (0 for other rows)
+DHD int hier_bin(const Dims& D, int i) { return i >= D.iq0 ? (i - D.iq0) % D.nq : 0; }
+
+// tridiagonal coefficients of hierarchy row i: f_i = lo*y[i-s] + di*y[i] + up*y[i+s] + u.g;
+// vq = velocity of the row's momentum bin (ignored for massless species)
+template <class T>
+DHD void hier_coef(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, int i, const T& vq, T& lo, T& di,
+                   T& up, T u[3], int& stride, bool& trunc)
+{
+    int l, L, species;
+    if (i <= 7 + D.lmaxg) { l = i - 7; L = D.lmaxg; species = 0; }
+    else if (i <= D.idxgp + D.lmaxgp) { l = i - D.idxgp; L = D.lmaxgp; species = 1; }
+    else if (i <= D.idxr + D.lmaxr) { l = i - D.idxr; L = D.lmaxr; species = 2; }
+    else { l = (i - D.iq0) / D.nq; L = D.lmaxnu; species = 3; }
+    const bool massive = species == 3;
+    const T scale = massive ? T(k) * vq : T(k);
+    trunc = (l == L);
+    const double io = inv_odd(l);
+    lo = trunc ? scale : scale * ((double)l * io);
+    up = trunc ? T(0.0) : -scale * ((l + 1.0) * io);
+    di = (species <= 1 ? -b.opac : T(0.0)) - (trunc ? T((L + 1.0) * b.itau) : T(0.0));
+    u[0] = 0.0; u[1] = 0.0; u[2] = 0.0;
+    if (species == 1) u[2] = l == 0 ? 0.5 * b.opac : (l == 2 ? 0.1 * b.opac : T(0.0));
+    if (massive) {
+        const double dl = dlfdlq_of(P.q[(i - D.iq0) - l * D.nq]);
+        u[0] = l == 0 ? T(dl * (1.0 / 6.0)) : (l == 2 ? T(-dl * (1.0 / 15.0)) : T(0.0));
+        u[1] = l == 2 ? T(-0.4 * dl) : T(0.0);
+    }
+    const bool frozen = (species <= 2 && b.rsa) || (species == 2 && b.ufa) || (species == 1 && b.tca);
+    if (frozen) { lo = 0.0; di = 0.0; up = 0.0; u[2] = 0.0; }
+    stride = massive ? D.nq : 1;
+}
+
 // ---- row 1 (a h'), read by no other equation: f_1 = sum_j F1_j y_j + F1U . g ----
 template <class T>
 DHD T f1col(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, int j)

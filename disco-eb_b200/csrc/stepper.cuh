@@ -137,7 +137,24 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
         g[2] = dual_with(g[2], tm.sum(der(g2)));
         f1s = dual_with(f1s, tm.sum(der(s1)));
     }
-    for (int i = tm.lane; i < n; i += tm.nl) {
+    // velocities of the momentum bins: lane q holds bin q (a single-lane team computes per row)
+    T vlane = 1.0;
+    if (tm.full() && tm.lane < D.nq) vlane = rcp(inv_vq(P, b, tm.lane));
+    const int nh = n_hier_rows(D);
+    for (int hh = tm.lane; hh < nh; hh += tm.nl) {
+        const int i = hier_row(D, hh);
+        const int q = hier_bin(D, i);
+        const T vq = tm.full() ? tm.bcast(vlane, q) : rcp(inv_vq(P, b, q));
+        T lo, di, up, u[3];
+        int st;
+        bool trunc;
+        hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
+        const T fi = lo * y[i - st] + di * y[i] + up * y[trunc ? i : i + st] + u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
+        f[i] = val(fi);
+        if (dfda) dfda[i] = der(fi);
+    }
+    for (int ss = tm.lane; ss < n_special_rows(); ss += tm.nl) {
+        const int i = special_row(D, ss);
         T fi;
         if (i == 0) {
             fi = b.aH * b.a;
@@ -185,17 +202,46 @@ DDV bool factor_chain(double* A, const Chain& ch)
 
 DDV void solve_chain(const double* A, const Chain& ch, double* z)
 {
-    for (int p = 1; p < ch.len; ++p) {
-        const int i = ch.start + p * ch.stride;
-        double s = z[i];
-        for (int d = 1; d <= ch.kl && p - d >= 0; ++d) s -= A[7 * i + 3 - d] * z[i - d * ch.stride];
-        z[i] = s;
+    const int st = ch.stride;
+    if (ch.kl == 1 && ch.ku == 1) {
+        // tridiagonal: carry the neighbour in a register
+        int i = ch.start;
+        double prev = z[i];
+        for (int p = 1; p < ch.len; ++p) {
+            i += st;
+            prev = z[i] - A[7 * i + 2] * prev;
+            z[i] = prev;
+        }
+        double next = prev * A[7 * i + 3];
+        z[i] = next;
+        for (int p = ch.len - 2; p >= 0; --p) {
+            i -= st;
+            next = (z[i] - A[7 * i + 4] * next) * A[7 * i + 3];
+            z[i] = next;
+        }
+        return;
     }
-    for (int p = ch.len - 1; p >= 0; --p) {
-        const int i = ch.start + p * ch.stride;
-        double s = z[i];
-        for (int m = 1; m <= ch.ku && p + m < ch.len; ++m) s -= A[7 * i + 3 + m] * z[i + m * ch.stride];
-        z[i] = s * A[7 * i + 3];
+    // pentadiagonal (kl = ku = 2)
+    int i = ch.start;
+    double p1 = z[i], p2 = 0.0;
+    for (int p = 1; p < ch.len; ++p) {
+        i += st;
+        double v = z[i] - A[7 * i + 2] * p1;
+        if (p >= 2) v -= A[7 * i + 1] * p2;
+        z[i] = v;
+        p2 = p1;
+        p1 = v;
+    }
+    double n1 = p1 * A[7 * i + 3], n2 = 0.0;
+    z[i] = n1;
+    for (int p = ch.len - 2; p >= 0; --p) {
+        i -= st;
+        double v = z[i] - A[7 * i + 4] * n1;
+        if (p + 2 < ch.len) v -= A[7 * i + 5] * n2;
+        v *= A[7 * i + 3];
+        z[i] = v;
+        n2 = n1;
+        n1 = v;
     }
 }
 
@@ -222,7 +268,25 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
     const int n = D.n;
     const double gh = kR5.gamma * h;
     const double igh = 1.0 / gh;
-    for (int i = tm.lane; i < n; i += tm.nl) {
+    double vlane = 1.0;
+    if (tm.full() && tm.lane < D.nq) vlane = rcp(inv_vq(P, b, tm.lane));
+    const int nh = n_hier_rows(D);
+    for (int hh = tm.lane; hh < nh; hh += tm.nl) {
+        const int i = hier_row(D, hh);
+        const int q = hier_bin(D, i);
+        const double vq = tm.full() ? tm.bcast(vlane, q) : rcp(inv_vq(P, b, q));
+        double lo, di, up, u[3];
+        int st;
+        bool trunc;
+        hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
+        double* Ai = M.A + 7 * i;
+        Ai[0] = 0.0; Ai[1] = 0.0; Ai[2] = -lo; Ai[3] = igh - di; Ai[4] = -up; Ai[5] = 0.0; Ai[6] = 0.0;
+        M.Z[i] = u[0];
+        M.Z[n + i] = u[1];
+        M.Z[2 * n + i] = u[2];
+    }
+    for (int ss = tm.lane; ss < n_special_rows(); ss += tm.nl) {
+        const int i = special_row(D, ss);
         double band[7], etac, u[3];
         if (i >= 2) {
             rowc(P, D, b, k, tau, i, band, etac, u);

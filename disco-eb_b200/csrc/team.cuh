@@ -25,6 +25,7 @@ struct WarpTeam {
     {
         return Dual(__shfl_sync(0xffffffffu, x.v, src), __shfl_sync(0xffffffffu, x.d, src));
     }
+    __device__ __forceinline__ bool full() const { return true; }
 };
 #endif
 
@@ -36,6 +37,7 @@ struct HostTeam {
     DHD bool leader() const { return true; }
     DHD double bcast(double x, int) const { return x; }
     DHD Dual bcast(const Dual& x, int) const { return x; }
+    DHD bool full() const { return false; }
 };
 
 }  // namespace dscb
