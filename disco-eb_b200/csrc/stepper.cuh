@@ -109,69 +109,116 @@ DHD double dual_with(double x, double) { return x; }
 DHD Dual dual_with(const Dual& x, double d) { return Dual(x.v, d); }
 
 // ---- RHS f(tau, y) (all entries), T = double or Dual in a ----
+// The metric functionals and the 15 "special" rows are computed in straight-line code by every
+// lane (no divergence, no reductions); the hierarchy rows are spread over the lanes as one
+// uniform class.  Same equations as model_synchronous (perturbations.py:88-525).
 template <class TM, class T>
 DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau,
                   const double* y, double* f, double* dfda)
 {
-    const int n = D.n;
-    const int ns = n_slots(D);
-    T g0 = 0.0, g1 = 0.0, g2 = 0.0, s1 = 0.0;
-    for (int sl = tm.lane; sl < ns; sl += tm.nl) {
-        const int j = slot_index(D, sl);
-        T gc[3];
-        gcol(P, D, b, k, j, gc);
-        const double yj = y[j];
-        g0 = g0 + gc[0] * yj;
-        g1 = g1 + gc[1] * yj;
-        g2 = g2 + gc[2] * yj;
-        s1 = s1 + f1col(P, D, b, k, j) * yj;
+    const int n = D.n, nq = D.nq, iq0 = D.iq0, idxr = D.idxr;
+    const double k2 = k * k;
+    const double Omegac = P.Omegam - P.Omegab;
+    // 1/v of momentum bin q on lane q
+    T ivl = 1.0;
+    if (tm.full() && tm.lane < nq) ivl = inv_vq(P, b, tm.lane);
+    const T vl = rcp(ivl);
+    T drho = 0.0, dp = 0.0, fnu = 0.0;
+#pragma unroll
+    for (int q = 0; q < DISCOEB_MAX_NQ; ++q) {
+        if (q < nq) {
+            const T iv = tm.full() ? tm.bcast(ivl, q) : inv_vq(P, b, q);
+            const T v = tm.full() ? tm.bcast(vl, q) : rcp(iv);
+            const double w = P.wq[q];
+            drho = drho + (w * y[iq0 + q]) * iv;
+            dp = dp + (w * y[iq0 + q]) * v;
+            fnu = fnu + w * y[iq0 + nq + q];
+        }
     }
-    T g[3];
-    g[0] = T(tm.sum(val(g0)));
-    g[1] = T(tm.sum(val(g1)));
-    g[2] = T(tm.sum(val(g2)));
-    T f1s = T(tm.sum(val(s1)));
-    if (dfda) {  // derivative parts of the reductions
-        g[0] = dual_with(g[0], tm.sum(der(g0)));
-        g[1] = dual_with(g[1], tm.sum(der(g1)));
-        g[2] = dual_with(g[2], tm.sum(der(g2)));
-        f1s = dual_with(f1s, tm.sum(der(s1)));
+    dp = dp * (1.0 / 3.0);
+    const double eta = y[2], deltac = y[3], thetac = y[4], deltab = y[5], thetab = y[6];
+    const double deltag = y[7], thetag = y[8], y9 = y[9];
+    const double deltar = y[idxr], thetar = y[idxr + 1], yr2 = y[idxr + 2];
+    const double deltaq = y[n - 2], thetaq = y[n - 1];
+    const T rQa2 = b.rho_Q * b.a2;
+    const T dgm = P.grhom * (Omegac * deltac + P.Omegab * deltab) * b.ia;
+    const T dgnu = P.grhor * P.Nmnu * drho * b.ia2;
+    const T dgq = P.grhom * P.OmegaDE * deltaq * rQa2;
+    const T dgrho = dgm + (P.grhog * deltag + P.grhor * P.Neff * deltar) * b.ia2 + dgnu + dgq;
+    const T dgrho_wo_rel = dgm + dgnu + dgq;
+    T H, thg, thr, dge, dre;
+    if (b.rsa) {
+        const double sk2 = k2 > 1e-30 ? k2 : 1e-30;
+        H = (2.0 * k2 * eta + dgrho_wo_rel) * b.iaHG;
+        dre = (4.0 / sk2) * (b.aH * H - sk2 * eta);
+        dge = dre + (4.0 / 3.0) * b.rsa_fac * (thetab + 0.5 * H);
+        thg = -0.5 * H + b.rsa_fac * (-b.rsa_tcs * (thetab + 0.5 * H) + (-b.aH * thetab + b.cs2 * sk2 * deltab + sk2 * eta));
+        thr = -0.5 * H;
+    } else {
+        H = (2.0 * k2 * eta + dgrho) * b.iaHG;
+        dge = T(deltag);
+        dre = T(deltar);
+        thg = T(thetag);
+        thr = T(thetar);
     }
-    // velocities of the momentum bins: lane q holds bin q (a single-lane team computes per row)
-    T vlane = 1.0;
-    if (tm.full() && tm.lane < D.nq) vlane = rcp(inv_vq(P, b, tm.lane));
+    const T rptq = b.opw * P.grhom * P.OmegaDE * thetaq * rQa2;
+    const T dgtheta = P.grhom * (Omegac * thetac + P.Omegab * thetab) * b.ia +
+                      (4.0 / 3.0) * (P.grhog * thg + P.Neff * P.grhor * thr) * b.ia2 + P.Nmnu * P.grhor * k * fnu * b.ia2 +
+                      rptq;
+    const T E = (0.5 / k2) * dgtheta;
+    const double cs2Q = P.cs2_DE;
+    const T dgpres = (P.grhog * dge + P.grhor * P.Neff * dre) * b.ia2 * (1.0 / 3.0) + P.grhor * P.Nmnu * dp * b.ia2 +
+                     (cs2Q * P.grhom * P.OmegaDE * deltaq * rQa2 + (cs2Q - b.ca2_Q) * (3.0 * b.aH * rptq * (1.0 / k2)));
+    const bool hier_photons = !b.rsa && !b.tca;
+    const T polter = hier_photons ? T(y9 + y[D.idxgp] + y[D.idxgp + 2]) : T(0.0);
+    const T alpha = (H + 6.0 * E) * (0.5 / k2);
+    // special rows
+    T sp[15];
+    sp[0] = b.aH * b.a;
+    sp[1] = -(dgrho + 3.0 * dgpres) * b.a;
+    sp[2] = E;
+    sp[3] = -thetac - 0.5 * H;
+    sp[4] = -b.aH * thetac;
+    sp[5] = -thetab - 0.5 * H;
+    sp[6] = -b.aH * thetab + k2 * b.cs2 * deltab + b.po * (thg - thetab);
+    if (!b.rsa) {
+        sp[7] = (4.0 / 3.0) * (-thg - 0.5 * H);
+        sp[8] = k2 * (0.25 * dge - 0.5 * y9) - b.opac * (thg - thetab);
+        sp[9] = (8.0 / 15.0) * (thg + k2 * alpha) - 0.6 * k * y[10] - b.opac * (y9 - 0.1 * polter);
+        sp[10] = (4.0 / 3.0) * (-thr - 0.5 * H);
+        sp[11] = k2 * (0.25 * dre - 0.5 * yr2);
+        sp[12] = b.ufa ? -1.5 * (tau > 1e-30 ? b.itau : 1e30) * yr2 + (4.0 / 15.0) * (thr + 0.5 * H)
+                       : (8.0 / 15.0) * (thr + k2 * alpha) - 0.6 * k * y[idxr + 3];
+    } else {
+        for (int q = 7; q < 13; ++q) sp[q] = 0.0;
+    }
+    if (b.de_frozen) {
+        sp[13] = 0.0;
+        sp[14] = 0.0;
+    } else {
+        sp[13] = -b.opw * (thetaq + 0.5 * H) - 3.0 * (cs2Q - b.w_Q) * b.aH * deltaq -
+                 9.0 * b.opw * (cs2Q - b.ca2_Q) * b.aH * b.aH * (1.0 / k2) * thetaq;
+        sp[14] = -(1.0 - 3.0 * cs2Q) * b.aH * thetaq + cs2Q * b.iopw * k2 * deltaq;
+    }
+    if (tm.leader()) {
+#pragma unroll
+        for (int ss = 0; ss < 15; ++ss) {
+            const int i = special_row(D, ss);
+            f[i] = val(sp[ss]);
+            if (dfda) dfda[i] = der(sp[ss]);
+        }
+    }
+    const T g0 = H, g1 = E, g2 = polter;
     const int nh = n_hier_rows(D);
     for (int hh = tm.lane; hh < nh; hh += tm.nl) {
         const int i = hier_row(D, hh);
         const int q = hier_bin(D, i);
-        const T vq = tm.full() ? tm.bcast(vlane, q) : rcp(inv_vq(P, b, q));
+        const T vq = tm.full() ? tm.bcast(vl, q) : rcp(inv_vq(P, b, q));
         T lo, di, up, u[3];
         int st;
         bool trunc;
         hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
-        const T fi = lo * y[i - st] + di * y[i] + up * y[trunc ? i : i + st] + u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
-        f[i] = val(fi);
-        if (dfda) dfda[i] = der(fi);
-    }
-    for (int ss = tm.lane; ss < n_special_rows(); ss += tm.nl) {
-        const int i = special_row(D, ss);
-        T fi;
-        if (i == 0) {
-            fi = b.aH * b.a;
-        } else if (i == 1) {
-            T u[3];
-            f1u(P, b, k, u);
-            fi = f1s + u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
-        } else {
-            T band[7], etac, u[3];
-            rowc(P, D, b, k, tau, i, band, etac, u);
-            const int s = row_stride(D, i);
-            fi = etac * y[2] + u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
-            for (int m = -3; m <= 3; ++m) {
-                const int jj = i + m * s;
-                if (jj >= 0 && jj < n) fi = fi + band[m + 3] * y[jj];
-            }
-        }
+        const T fi = lo * y[i - st] + di * y[i] + up * y[trunc ? i : i + st] + u[0] * g0 + u[1] * g1 + u[2] * g2;
         f[i] = val(fi);
         if (dfda) dfda[i] = der(fi);
     }
