@@ -114,7 +114,7 @@ DHD Dual dual_with(const Dual& x, double d) { return Dual(x.v, d); }
 // uniform class.  Same equations as model_synchronous (perturbations.py:88-525).
 template <class TM, class T>
 DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau,
-                  const double* __restrict__ y, double* __restrict__ f, double* __restrict__ dfda)
+                  const double* y, double* f, double* dfda)
 {
     const int n = D.n, nq = D.nq, iq0 = D.iq0, idxr = D.idxr;
     const double k2 = k * k;
@@ -210,24 +210,17 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
     }
     const T g0 = H, g1 = E, g2 = polter;
     const int nh = n_hier_rows(D);
-    // independent rows, unrolled so that their latency chains overlap
-    for (int base = 0; base < nh; base += tm.nl * 4) {
-#pragma unroll
-        for (int uu = 0; uu < 4; ++uu) {
-            const int hh = base + uu * tm.nl + tm.lane;
-            const int q = hh < nh ? hier_bin(D, hier_row(D, hh)) : 0;
-            const T vq = tm.full() ? tm.bcast(vl, q) : rcp(inv_vq(P, b, q));
-            if (hh < nh) {
-                const int i = hier_row(D, hh);
-                T lo, di, up, u[3];
-                int st;
-                bool trunc;
-                hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
-                const T fi = lo * y[i - st] + di * y[i] + up * y[trunc ? i : i + st] + u[0] * g0 + u[1] * g1 + u[2] * g2;
-                f[i] = val(fi);
-                if (dfda) dfda[i] = der(fi);
-            }
-        }
+    for (int hh = tm.lane; hh < nh; hh += tm.nl) {
+        const int i = hier_row(D, hh);
+        const int q = hier_bin(D, i);
+        const T vq = tm.full() ? tm.bcast(vl, q) : rcp(inv_vq(P, b, q));
+        T lo, di, up, u[3];
+        int st;
+        bool trunc;
+        hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
+        const T fi = lo * y[i - st] + di * y[i] + up * y[trunc ? i : i + st] + u[0] * g0 + u[1] * g1 + u[2] * g2;
+        f[i] = val(fi);
+        if (dfda) dfda[i] = der(fi);
     }
 }
 
@@ -325,29 +318,21 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
     double vlane = 1.0;
     if (tm.full() && tm.lane < D.nq) vlane = rcp(inv_vq(P, b, tm.lane));
     const int nh = n_hier_rows(D);
-    for (int base = 0; base < nh; base += tm.nl * 4) {
-#pragma unroll
-        for (int uu = 0; uu < 4; ++uu) {
-            const int hh = base + uu * tm.nl + tm.lane;
-            const int q = hh < nh ? hier_bin(D, hier_row(D, hh)) : 0;
-            const double vq = tm.full() ? tm.bcast(vlane, q) : rcp(inv_vq(P, b, q));
-            if (hh < nh) {
-                const int i = hier_row(D, hh);
-                double lo, di, up, u[3];
-                int st;
-                bool trunc;
-                hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
-                double* Ai = M.A + 7 * i;
-                Ai[0] = 0.0; Ai[1] = 0.0; Ai[2] = -lo; Ai[3] = igh - di; Ai[4] = -up; Ai[5] = 0.0; Ai[6] = 0.0;
-                M.Z[i] = u[0];
-                M.Z[n + i] = u[1];
-                M.Z[2 * n + i] = u[2];
-            }
-        }
+    for (int hh = tm.lane; hh < nh; hh += tm.nl) {
+        const int i = hier_row(D, hh);
+        const int q = hier_bin(D, i);
+        const double vq = tm.full() ? tm.bcast(vlane, q) : rcp(inv_vq(P, b, q));
+        double lo, di, up, u[3];
+        int st;
+        bool trunc;
+        hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
+        double* Ai = M.A + 7 * i;
+        Ai[0] = 0.0; Ai[1] = 0.0; Ai[2] = -lo; Ai[3] = igh - di; Ai[4] = -up; Ai[5] = 0.0; Ai[6] = 0.0;
+        M.Z[i] = u[0];
+        M.Z[n + i] = u[1];
+        M.Z[2 * n + i] = u[2];
     }
-    // special rows: every lane evaluates each row (uniform control flow), one lane stores it
-#pragma unroll
-    for (int ss = 0; ss < 15; ++ss) {
+    for (int ss = tm.lane; ss < n_special_rows(); ss += tm.nl) {
         const int i = special_row(D, ss);
         double band[7], etac, u[3];
         if (i >= 2) {
@@ -356,14 +341,12 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
             for (int m = 0; m < 7; ++m) band[m] = 0.0;
             etac = 0.0; u[0] = u[1] = u[2] = 0.0;
         }
-        if (tm.lane == ss % tm.nl) {
-            for (int m = 0; m < 7; ++m) M.A[7 * i + m] = -band[m];
-            M.A[7 * i + 3] += igh;
-            if (i == 6) M.sc[SC_ETAC] = etac;
-            M.Z[i] = u[0];
-            M.Z[n + i] = u[1];
-            M.Z[2 * n + i] = u[2];
-        }
+        for (int m = 0; m < 7; ++m) M.A[7 * i + m] = -band[m];
+        M.A[7 * i + 3] += igh;
+        if (i == 6) M.sc[SC_ETAC] = etac;
+        M.Z[i] = u[0];
+        M.Z[n + i] = u[1];
+        M.Z[2 * n + i] = u[2];
     }
     const int ns = n_slots(D);
     for (int sl = tm.lane; sl < ns; sl += tm.nl) {
