@@ -34,7 +34,7 @@ __device__ void emit_output(const WarpTeam& tm, const DiscoebCosmo& P, const Dim
 {
     const int n = D.n;
     double fld[4];
-    const bool rsa = rsa_projection(P, D, tau, k, y, fld);  // all lanes, identical
+    const bool rsa = rsa_projection<double>(P, nullptr, D, tau, k, y, nullptr, fld);  // all lanes, identical
     // projected state into scratch (shared) then outputs
     double* yp = scratch20;  // n doubles of shared scratch
     for (int i = tm.lane; i < n; i += 32) {
@@ -50,7 +50,7 @@ __device__ void emit_output(const WarpTeam& tm, const DiscoebCosmo& P, const Dim
     tm.sync();
     if (y20 && tm.leader()) {
         double o[20];
-        output_vars(P, D, k, yp, o);
+        output_vars<double>(P, nullptr, D, k, yp, nullptr, o);
         for (int q = 0; q < 20; ++q) y20[q] = o[q];
     }
     tm.sync();

@@ -1,7 +1,10 @@
-// Forward-mode dual numbers (value + derivative in one direction) and math wrappers
-// shared by double and Dual code paths.  The derivative direction used by the solver
-// is the scale factor a = y[0]: the Jacobian column d f / d a comes out of one RHS
-// evaluation with a seeded as Dual{a, 1}.
+// Forward-mode dual numbers and the math wrappers shared by the double and dual code paths.
+//
+// DualT<B> carries a value and one directional derivative, both of type B.  Dual =
+// DualT<double> is used for the Jacobian column d f / d a (direction: the scale factor) and
+// for tangents of the whole solve (direction: a parameter); HDual = DualT<Dual> carries two
+// directions and their mixed second derivative, which the tangent of the Rosenbrock step
+// needs (the derivative of J k along a parameter direction).
 #pragma once
 
 #include <cmath>
@@ -16,63 +19,76 @@
 
 namespace dscb {
 
-struct Dual {
-    double v, d;
-    DHD Dual() : v(0.0), d(0.0) {}
-    DHD Dual(double x) : v(x), d(0.0) {}
-    DHD Dual(double x, double dx) : v(x), d(dx) {}
+template <class B> struct DualT {
+    B v, d;
+    DHD DualT() : v(0.0), d(0.0) {}
+    DHD DualT(double x) : v(x), d(0.0) {}
+    DHD DualT(const B& x, const B& dx) : v(x), d(dx) {}
 };
+using Dual = DualT<double>;
+using HDual = DualT<Dual>;
 
-DHD Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
-DHD Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
-DHD Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
-DHD Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
-DHD Dual operator/(Dual a, Dual b)
+template <class B> DHD DualT<B> operator+(const DualT<B>& a, const DualT<B>& b) { return DualT<B>(a.v + b.v, a.d + b.d); }
+template <class B> DHD DualT<B> operator-(const DualT<B>& a, const DualT<B>& b) { return DualT<B>(a.v - b.v, a.d - b.d); }
+template <class B> DHD DualT<B> operator-(const DualT<B>& a) { return DualT<B>(-a.v, -a.d); }
+template <class B> DHD DualT<B> operator*(const DualT<B>& a, const DualT<B>& b)
 {
-    double r = 1.0 / b.v;
-    double q = a.v * r;
-    return Dual(q, (a.d - q * b.d) * r);
+    return DualT<B>(a.v * b.v, a.d * b.v + a.v * b.d);
 }
-DHD Dual operator+(Dual a, double b) { return Dual(a.v + b, a.d); }
-DHD Dual operator+(double a, Dual b) { return Dual(a + b.v, b.d); }
-DHD Dual operator-(Dual a, double b) { return Dual(a.v - b, a.d); }
-DHD Dual operator-(double a, Dual b) { return Dual(a - b.v, -b.d); }
-DHD Dual operator*(Dual a, double b) { return Dual(a.v * b, a.d * b); }
-DHD Dual operator*(double a, Dual b) { return Dual(a * b.v, a * b.d); }
-DHD Dual operator/(Dual a, double b) { return Dual(a.v / b, a.d / b); }
-DHD Dual operator/(double a, Dual b)
-{
-    double q = a / b.v;
-    return Dual(q, -q * b.d / b.v);
-}
-DHD Dual& operator+=(Dual& a, Dual b) { a.v += b.v; a.d += b.d; return a; }
-DHD Dual& operator-=(Dual& a, Dual b) { a.v -= b.v; a.d -= b.d; return a; }
+template <class B> DHD DualT<B> rcp(const DualT<B>& x);
+template <class B> DHD DualT<B> operator/(const DualT<B>& a, const DualT<B>& b) { return a * rcp(b); }
+template <class B> DHD DualT<B> operator+(const DualT<B>& a, double b) { return DualT<B>(a.v + b, a.d); }
+template <class B> DHD DualT<B> operator+(double a, const DualT<B>& b) { return DualT<B>(a + b.v, b.d); }
+template <class B> DHD DualT<B> operator-(const DualT<B>& a, double b) { return DualT<B>(a.v - b, a.d); }
+template <class B> DHD DualT<B> operator-(double a, const DualT<B>& b) { return DualT<B>(a - b.v, -b.d); }
+template <class B> DHD DualT<B> operator*(const DualT<B>& a, double b) { return DualT<B>(a.v * b, a.d * b); }
+template <class B> DHD DualT<B> operator*(double a, const DualT<B>& b) { return DualT<B>(a * b.v, a * b.d); }
+template <class B> DHD DualT<B> operator/(const DualT<B>& a, double b) { return DualT<B>(a.v / b, a.d / b); }
+template <class B> DHD DualT<B> operator/(double a, const DualT<B>& b) { return a * rcp(b); }
+template <class B> DHD DualT<B>& operator+=(DualT<B>& a, const DualT<B>& b) { a.v += b.v; a.d += b.d; return a; }
+template <class B> DHD DualT<B>& operator-=(DualT<B>& a, const DualT<B>& b) { a.v -= b.v; a.d -= b.d; return a; }
 
+// innermost value (all comparisons and table indices use it)
 DHD double val(double x) { return x; }
-DHD double val(const Dual& x) { return x.v; }
+template <class B> DHD double val(const DualT<B>& x) { return val(x.v); }
+// first-level derivative part
 DHD double der(double) { return 0.0; }
 DHD double der(const Dual& x) { return x.d; }
+
+DHD double rcp(double x)
+{
+#if defined(__CUDA_ARCH__)
+    return __drcp_rn(x);
+#else
+    return 1.0 / x;
+#endif
+}
+template <class B> DHD DualT<B> rcp(const DualT<B>& x)
+{
+    const B r = rcp(x.v);
+    return DualT<B>(r, -(r * r) * x.d);
+}
 
 DHD double xexp(double x) { return exp(x); }
 DHD double xlog(double x) { return log(x); }
 DHD double xsqrt(double x) { return sqrt(x); }
 DHD double xpow(double x, double p) { return pow(x, p); }
 
-DHD Dual xexp(Dual x)
+template <class B> DHD DualT<B> xexp(const DualT<B>& x)
 {
-    double e = exp(x.v);
-    return Dual(e, e * x.d);
+    const B e = xexp(x.v);
+    return DualT<B>(e, e * x.d);
 }
-DHD Dual xlog(Dual x) { return Dual(log(x.v), x.d / x.v); }
-DHD Dual xsqrt(Dual x)
+template <class B> DHD DualT<B> xlog(const DualT<B>& x) { return DualT<B>(xlog(x.v), x.d * rcp(x.v)); }
+template <class B> DHD DualT<B> xsqrt(const DualT<B>& x)
 {
-    double s = sqrt(x.v);
-    return Dual(s, 0.5 * x.d / s);
+    const B s = xsqrt(x.v);
+    return DualT<B>(s, (0.5 * x.d) * rcp(s));
 }
-DHD Dual xpow(Dual x, double p)
+template <class B> DHD DualT<B> xpow(const DualT<B>& x, double p)
 {
-    double r = pow(x.v, p);
-    return Dual(r, p * r / x.v * x.d);
+    const B r = xpow(x.v, p);
+    return DualT<B>(r, (p * r) * rcp(x.v) * x.d);
 }
 
 DHD bool xfinite(double x)
@@ -85,6 +101,14 @@ DHD bool xfinite(double x)
 }
 
 // max(x, lo) selecting on the value, as jnp.maximum does for the primal
-template <class T> DHD T xmaxc(T x, double lo) { return val(x) > lo ? x : T(lo); }
+template <class T> DHD T xmaxc(const T& x, double lo) { return val(x) > lo ? x : T(lo); }
+
+// a value with first-direction part e (the "tangent" slot): double drops it, Dual stores it,
+// HDual stores it in the inner dual of the value part
+DHD double seed(double v, double) { return v; }
+DHD Dual seed_as(const Dual*, double v, double e) { return Dual(v, e); }
+DHD HDual seed_as(const HDual*, double v, double e) { return HDual(Dual(v, e), Dual(0.0)); }
+DHD double seed_as(const double*, double v, double) { return v; }
+template <class T> DHD T seed_t(double v, double e) { return seed_as((const T*)nullptr, v, e); }
 
 }  // namespace dscb

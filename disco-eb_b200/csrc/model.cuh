@@ -70,32 +70,65 @@ DHD int spline_index(const DiscoebSpline& s, double xn)
     return i;
 }
 
-template <class T> DHD T spline_eval_at(const DiscoebSpline& s, int i, T xn)
+// knot values, with tangent arrays (may be null) seeded into the first-derivative slot
+template <class T> DHD T knot(const double* a, const double* ad, int i)
 {
-    double xi = DLDG(s.x + i), xj = DLDG(s.x + i + 1);
-    double h = xj - xi;
-    T t = (xn - xi) / h;
-    T A = 1.0 - t, B = t;
-    return A * DLDG(s.y + i) + B * DLDG(s.y + i + 1) +
-           ((A * A * A - A) * DLDG(s.S + i) + (B * B * B - B) * DLDG(s.S + i + 1)) * (h * h / 6.0);
+    return seed_t<T>(DLDG(a + i), ad ? DLDG(ad + i) : 0.0);
 }
 
-template <class T> DHD T spline_deriv_at(const DiscoebSpline& s, int i, T xn)
+template <class T>
+DHD T spline_eval_at(const DiscoebSpline& s, int i, T xn, const double* yd = nullptr, const double* Sd = nullptr)
 {
     double xi = DLDG(s.x + i), xj = DLDG(s.x + i + 1);
     double h = xj - xi;
-    double yi = DLDG(s.y + i), yj = DLDG(s.y + i + 1), Si = DLDG(s.S + i), Sj = DLDG(s.S + i + 1);
+    T t = (xn - xi) * (1.0 / h);
+    T A = 1.0 - t, B = t;
+    return A * knot<T>(s.y, yd, i) + B * knot<T>(s.y, yd, i + 1) +
+           ((A * A * A - A) * knot<T>(s.S, Sd, i) + (B * B * B - B) * knot<T>(s.S, Sd, i + 1)) * (h * h / 6.0);
+}
+
+template <class T>
+DHD T spline_deriv_at(const DiscoebSpline& s, int i, T xn, const double* yd = nullptr, const double* Sd = nullptr)
+{
+    double xi = DLDG(s.x + i), xj = DLDG(s.x + i + 1);
+    double h = xj - xi;
+    const T yi = knot<T>(s.y, yd, i), yj = knot<T>(s.y, yd, i + 1), Si = knot<T>(s.S, Sd, i), Sj = knot<T>(s.S, Sd, i + 1);
     T d = xn - xi;
-    double b = (yj - yi) / h - h * (Sj + 2.0 * Si) / 6.0;
-    double c = Si / 2.0;
-    double dd = (Sj - Si) / (6.0 * h);
+    T b = (yj - yi) * (1.0 / h) - h * (Sj + 2.0 * Si) * (1.0 / 6.0);
+    T c = Si * 0.5;
+    T dd = (Sj - Si) * (1.0 / (6.0 * h));
     return b + 2.0 * c * d + 3.0 * dd * d * d;
 }
 
 template <class T> DHD T spline_eval(const DiscoebSpline& s, T xn) { return spline_eval_at(s, spline_index(s, val(xn)), xn); }
 
+// ---- parameters that depend on the cosmological parameters (typed, so that tangents flow) ----
+template <class T> struct Par {
+    T grhom, Omegam, Omegab, OmegaDE, amnu, w0, wa, akthom;
+};
+
+// parameter values, with their derivatives along a tangent direction seeded into the
+// first-derivative slot of T (tn == nullptr: no tangent)
+template <class T> DHD Par<T> make_par(const DiscoebCosmo& P, const DiscoebTangent* tn)
+{
+    Par<T> r;
+    const double z = 0.0;
+    r.grhom = seed_t<T>(P.grhom, tn ? tn->grhom : z);
+    r.Omegam = seed_t<T>(P.Omegam, tn ? tn->Omegam : z);
+    r.Omegab = seed_t<T>(P.Omegab, tn ? tn->Omegab : z);
+    r.OmegaDE = seed_t<T>(P.OmegaDE, tn ? tn->OmegaDE : z);
+    r.amnu = seed_t<T>(P.amnu, tn ? tn->amnu : z);
+    r.w0 = seed_t<T>(P.w0, tn ? tn->w0 : z);
+    r.wa = seed_t<T>(P.wa, tn ? tn->wa : z);
+    const double c = 2.3038921003709498e-9 * (1.0 - P.YHe);
+    const T H0 = seed_t<T>(P.H0, tn ? tn->H0 : z);
+    r.akthom = c * r.Omegab * H0 * H0;
+    return r;
+}
+
 // ---- background quantities at (a, tau) ----
 template <class T> struct Bg {
+    Par<T> par;
     T a, ia, a2, ia2, aH, iaHG, opac, po, tauc, taucprime, cs2, pb43, rho_Q, w_Q, opw, iopw, ca2_Q, pnu;
     T rsa_fac, rsa_tcs;  // 3/(k^2 tau_c), tau_c'/tau_c (RSA fields)
     T aprimeprimeoa;
@@ -103,34 +136,21 @@ template <class T> struct Bg {
     bool rsa, ufa, tca, de_frozen;
 };
 
-DHD double rcp(double x)
-{
-#if defined(__CUDA_ARCH__)
-    return __drcp_rn(x);
-#else
-    return 1.0 / x;
-#endif
-}
-DHD Dual rcp(const Dual& x)
-{
-    const double r = rcp(x.v);
-    return Dual(r, -r * r * x.d);
-}
-
 // velocity of momentum bin q: v = 1/sqrt(1 + (a m/q)^2), and its inverse
 template <class T> DHD T inv_vq(const DiscoebCosmo& P, const Bg<T>& b, int q)
 {
-    const T aq = b.a * (P.amnu / P.q[q]);
+    const T aq = b.a * b.par.amnu * (1.0 / P.q[q]);
     return xsqrt(1.0 + aq * aq);
 }
 
-template <class T> DHD T aprimeoa_of(const DiscoebCosmo& P, T a, T loga)
+template <class T> DHD T aprimeoa_of(const DiscoebCosmo& P, const Par<T>& par, const DiscoebTangent* tn, T a, T loga)
 {
-    T rhonu = xexp(spline_eval(P.logrhonu_loga, loga));
-    T rho_Q = xpow(a, -3.0 * (1.0 + P.w0 + P.wa)) * xexp(3.0 * (a - 1.0) * P.wa);
-    T grho = P.grhom * P.Omegam / a + (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / (a * a) +
-             P.grhom * P.OmegaDE * rho_Q * a * a + P.grhom * P.Omegak;
-    return xsqrt(grho / 3.0);
+    const int i = spline_index(P.logrhonu_loga, val(loga));
+    T rhonu = xexp(spline_eval_at(P.logrhonu_loga, i, loga, tn ? tn->logrhonu_y : nullptr, tn ? tn->logrhonu_S : nullptr));
+    T rho_Q = xexp(-3.0 * (1.0 + par.w0 + par.wa) * loga + 3.0 * (a - 1.0) * par.wa);
+    T grho = par.grhom * par.Omegam / a + (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / (a * a) +
+             par.grhom * par.OmegaDE * rho_Q * a * a + par.grhom * P.Omegak;
+    return xsqrt(grho * (1.0 / 3.0));
 }
 
 // index of a non-uniform spline searched from a hint (the previous index): same result
@@ -154,34 +174,42 @@ template <class T> struct BgTables {
 };
 
 template <class T>
-DHD T table_slot_value(const DiscoebCosmo& P, int t, T a, T loga, int& hint, T& deriv)
+DHD T table_slot_value(const DiscoebCosmo& P, const Par<T>& par, const DiscoebTangent* tn, int t, T a, T loga,
+                       int& hint, T& deriv)
 {
     // t: 0 xe (and its derivative), 1 cs2*a, 2 log rho_nu, 3 log p_nu, 4 log rho_Q
     if (t == 4) {
         deriv = 0.0;
-        return -3.0 * (1.0 + P.w0 + P.wa) * loga + 3.0 * (a - 1.0) * P.wa;
+        return -3.0 * (1.0 + par.w0 + par.wa) * loga + 3.0 * (a - 1.0) * par.wa;
     }
     const DiscoebSpline& s = t == 0 ? P.xe_loga : (t == 1 ? P.cs2a_loga : (t == 2 ? P.logrhonu_loga : P.logpnu_loga));
+    const double* yd = nullptr;
+    const double* Sd = nullptr;
+    if (tn) {
+        yd = t == 0 ? tn->xe_y : (t == 1 ? tn->cs2a_y : (t == 2 ? tn->logrhonu_y : tn->logpnu_y));
+        Sd = t == 0 ? tn->xe_S : (t == 1 ? tn->cs2a_S : (t == 2 ? tn->logrhonu_S : tn->logpnu_S));
+    }
     int h = hint;
     const int i = spline_index_from(s, val(loga), h);
     if (t == 0) hint = h;
-    deriv = spline_deriv_at(s, i, loga);
-    return spline_eval_at(s, i, loga);
+    deriv = spline_deriv_at(s, i, loga, yd, Sd);
+    return spline_eval_at(s, i, loga, yd, Sd);
 }
 
 template <class TM, class T>
-DHD BgTables<T> bg_tables(const TM& tm, const DiscoebCosmo& P, T a, int& hint)
+DHD BgTables<T> bg_tables(const TM& tm, const DiscoebCosmo& P, const Par<T>& par, const DiscoebTangent* tn, T a,
+                          int& hint)
 {
     const T loga = xlog(a);
     BgTables<T> r;
     if (tm.nl == 1) {
         T d;
         int h = hint;
-        r.xe = table_slot_value(P, 0, a, loga, h, r.xep);
-        r.cs2a = table_slot_value(P, 1, a, loga, hint, d);
-        r.rhonu = xexp(table_slot_value(P, 2, a, loga, hint, d));
-        r.pnu = xexp(table_slot_value(P, 3, a, loga, hint, d));
-        r.rho_Q = xexp(table_slot_value(P, 4, a, loga, hint, d));
+        r.xe = table_slot_value(P, par, tn, 0, a, loga, h, r.xep);
+        r.cs2a = table_slot_value(P, par, tn, 1, a, loga, hint, d);
+        r.rhonu = xexp(table_slot_value(P, par, tn, 2, a, loga, hint, d));
+        r.pnu = xexp(table_slot_value(P, par, tn, 3, a, loga, hint, d));
+        r.rho_Q = xexp(table_slot_value(P, par, tn, 4, a, loga, hint, d));
         hint = h;
         return r;
     }
@@ -189,7 +217,7 @@ DHD BgTables<T> bg_tables(const TM& tm, const DiscoebCosmo& P, T a, int& hint)
     T v = 0.0, d = 0.0;
     int h = hint;
     if (tm.lane < 5) {
-        v = table_slot_value(P, tm.lane, a, loga, h, d);
+        v = table_slot_value(P, par, tn, tm.lane, a, loga, h, d);
         if (tm.lane >= 2) v = xexp(v);
     }
     r.xe = tm.bcast(v, 0);
@@ -205,8 +233,10 @@ DHD BgTables<T> bg_tables(const TM& tm, const DiscoebCosmo& P, T a, int& hint)
 // regime < 0: switches from (tau, a) exactly as model_synchronous evaluates them;
 // otherwise bitmask 1 = RSA, 2 = UFA, 4 = TCA.
 template <class T>
-DHD void bg_finish(const DiscoebCosmo& P, T a, const BgTables<T>& tb, double tau, double k, int regime, Bg<T>& b)
+DHD void bg_finish(const DiscoebCosmo& P, const Par<T>& par, T a, const BgTables<T>& tb, double tau, double k,
+                   int regime, Bg<T>& b)
 {
+    b.par = par;
     b.a = a;
     b.ia = rcp(a);
     b.a2 = a * a;
@@ -215,23 +245,22 @@ DHD void bg_finish(const DiscoebCosmo& P, T a, const BgTables<T>& tb, double tau
     const T& xe = tb.xe;
     b.cs2 = tb.cs2a * b.ia;
     b.pnu = tb.pnu;
-    b.pb43 = (4.0 / 3.0) * P.grhog / (P.grhom * P.Omegab) * b.ia;
-    b.w_Q = P.w0 + P.wa * (1.0 - a);
+    b.pb43 = (4.0 / 3.0) * P.grhog * rcp(par.grhom * par.Omegab) * b.ia;
+    b.w_Q = par.w0 + par.wa * (1.0 - a);
     b.opw = 1.0 + b.w_Q;
     b.iopw = rcp(b.opw);
     b.rho_Q = tb.rho_Q;
-    T grho = P.grhom * P.Omegam * b.ia + (P.grhog + P.grhor * (P.Neff + P.Nmnu * tb.rhonu)) * b.ia2 +
-             P.grhom * P.OmegaDE * b.rho_Q * b.a2 + P.grhom * P.Omegak;
+    T grho = par.grhom * par.Omegam * b.ia + (P.grhog + P.grhor * (P.Neff + P.Nmnu * tb.rhonu)) * b.ia2 +
+             par.grhom * par.OmegaDE * b.rho_Q * b.a2 + par.grhom * P.Omegak;
     b.aH = xsqrt(grho * (1.0 / 3.0));
     const T iaH = rcp(b.aH);
     T xeprime = tb.xep * b.aH;
     T gpres = ((P.grhog + P.grhor * P.Neff) * (1.0 / 3.0) + P.grhor * P.Nmnu * b.pnu) * b.ia2 +
-              b.w_Q * P.grhom * P.OmegaDE * b.rho_Q * b.a2;
+              b.w_Q * par.grhom * par.OmegaDE * b.rho_Q * b.a2;
     b.aprimeprimeoa = 0.5 * (b.aH * b.aH - gpres);
-    T w_Q_prime = -P.wa * b.aH * a;
+    T w_Q_prime = -par.wa * b.aH * a;
     b.ca2_Q = b.w_Q - w_Q_prime * (1.0 / 3.0) / ((1.0 + b.w_Q) + 1e-6) * iaH;
-    const double akthom = 2.3038921003709498e-9 * (1.0 - P.YHe) * P.Omegab * P.H0 * P.H0;
-    b.opac = xe * akthom * b.ia2;
+    b.opac = xe * par.akthom * b.ia2;
     b.po = b.pb43 * b.opac;
     b.tauc = rcp(xmaxc(b.opac, 1e-30));
     b.taucprime = b.tauc * (2.0 * b.aH - xeprime / xmaxc(xe, 1e-30));
@@ -263,16 +292,19 @@ DHD void bg_finish(const DiscoebCosmo& P, T a, const BgTables<T>& tb, double tau
 }
 
 template <class TM, class T>
-DHD void bg_eval_team(const TM& tm, const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b, int& hint)
+DHD void bg_eval_team(const TM& tm, const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b, int& hint,
+                      const DiscoebTangent* tn = nullptr)
 {
-    const BgTables<T> tb = bg_tables(tm, P, a, hint);
-    bg_finish(P, a, tb, tau, k, regime, b);
+    const Par<T> par = make_par<T>(P, tn);
+    const BgTables<T> tb = bg_tables(tm, P, par, tn, a, hint);
+    bg_finish(P, par, a, tb, tau, k, regime, b);
 }
 
 template <class T>
-DHD void bg_eval(const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b, int& hint)
+DHD void bg_eval(const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b, int& hint,
+                 const DiscoebTangent* tn = nullptr)
 {
-    bg_eval_team(HostTeam(), P, a, tau, k, regime, b, hint);
+    bg_eval_team(HostTeam(), P, a, tau, k, regime, b, hint, tn);
 }
 
 template <class T> DHD void bg_eval(const DiscoebCosmo& P, T a, double tau, double k, int regime, Bg<T>& b)
@@ -306,7 +338,7 @@ DHD void gcol(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, in
 {
     g[0] = 0.0; g[1] = 0.0; g[2] = 0.0;
     const double k2 = k * k;
-    const double Omegac = P.Omegam - P.Omegab;
+    const T Omegac = b.par.Omegam - b.par.Omegab;
     const T& ia = b.ia;
     const T& ia2 = b.ia2;
     const T& invaH = b.iaHG;
@@ -314,19 +346,19 @@ DHD void gcol(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, in
     const int nq = D.nq;
     // h' = (2 k^2 eta + dgrho) / (a'/a)   (perturbations.py:294-306, :346)
     if (j == 2) g[0] = 2.0 * k2 * invaH;
-    else if (j == 3) g[0] = P.grhom * Omegac * ia * invaH;
-    else if (j == 5) g[0] = P.grhom * P.Omegab * ia * invaH;
+    else if (j == 3) g[0] = b.par.grhom * Omegac * ia * invaH;
+    else if (j == 5) g[0] = b.par.grhom * b.par.Omegab * ia * invaH;
     else if (j == 7) { if (!b.rsa) g[0] = P.grhog * ia2 * invaH; }
     else if (j == D.idxr) { if (!b.rsa) g[0] = P.grhor * P.Neff * ia2 * invaH; }
     else if (j >= D.iq0 && j < D.iq0 + nq) { int q = j - D.iq0; g[0] = P.grhor * P.Nmnu * P.wq[q] * inv_vq(P, b, q) * ia2 * invaH; }
-    else if (j == D.n - 2) g[0] = P.grhom * P.OmegaDE * b.rho_Q * b.a2 * invaH;
+    else if (j == D.n - 2) g[0] = b.par.grhom * b.par.OmegaDE * b.rho_Q * b.a2 * invaH;
     // eta' = dgtheta / (2 k^2)   (perturbations.py:330-335, :349)
-    if (j == 4) g[1] = hE * P.grhom * Omegac * ia;
-    else if (j == 6) g[1] = hE * P.grhom * P.Omegab * ia;
+    if (j == 4) g[1] = hE * b.par.grhom * Omegac * ia;
+    else if (j == 6) g[1] = hE * b.par.grhom * b.par.Omegab * ia;
     else if (j == 8) { if (!b.rsa) g[1] = hE * (4.0 / 3.0) * P.grhog * ia2; }
     else if (j == D.idxr + 1) { if (!b.rsa) g[1] = hE * (4.0 / 3.0) * P.Neff * P.grhor * ia2; }
     else if (j >= D.iq0 + nq && j < D.iq0 + 2 * nq) { int q = j - D.iq0 - nq; g[1] = hE * P.Nmnu * P.grhor * k * P.wq[q] * ia2; }
-    else if (j == D.n - 1) g[1] = hE * b.opw * b.rho_Q * P.grhom * P.OmegaDE * b.a2;
+    else if (j == D.n - 1) g[1] = hE * b.opw * b.rho_Q * b.par.grhom * b.par.OmegaDE * b.a2;
     if (b.rsa) {
         // theta_gamma and theta_r replaced by the RSA fields (approximations.py:28-47)
         const double sk2 = k2 > 1e-30 ? k2 : 1e-30;
@@ -505,13 +537,13 @@ template <class T>
 DHD T f1col(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, int j)
 {
     const double k2 = k * k;
-    const double Omegac = P.Omegam - P.Omegab;
+    const T Omegac = b.par.Omegam - b.par.Omegab;
     const T& ia = b.ia;
     const T& ia2 = b.ia2;
     const int nq = D.nq;
     T rho = 0.0, pres = 0.0;  // coefficients of y_j in dgrho and dgpres
-    if (j == 3) rho = P.grhom * Omegac * ia;
-    else if (j == 5) rho = P.grhom * P.Omegab * ia;
+    if (j == 3) rho = b.par.grhom * Omegac * ia;
+    else if (j == 5) rho = b.par.grhom * b.par.Omegab * ia;
     else if (j == 7) { rho = P.grhog * ia2; if (!b.rsa) pres = P.grhog * ia2 * (1.0 / 3.0); }
     else if (j == D.idxr) { rho = P.grhor * P.Neff * ia2; if (!b.rsa) pres = P.grhor * P.Neff * ia2 * (1.0 / 3.0); }
     else if (j >= D.iq0 && j < D.iq0 + nq) {
@@ -520,10 +552,10 @@ DHD T f1col(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, int 
         rho = P.grhor * P.Nmnu * P.wq[q] * iv * ia2;
         pres = P.grhor * P.Nmnu * ia2 * P.wq[q] * rcp(iv) * (1.0 / 3.0);
     } else if (j == D.n - 2) {
-        rho = P.grhom * P.OmegaDE * b.rho_Q * b.a2;
-        pres = P.cs2_DE * P.grhom * P.OmegaDE * b.rho_Q * b.a2;
+        rho = b.par.grhom * b.par.OmegaDE * b.rho_Q * b.a2;
+        pres = P.cs2_DE * b.par.grhom * b.par.OmegaDE * b.rho_Q * b.a2;
     } else if (j == D.n - 1) {
-        pres = (P.cs2_DE - b.ca2_Q) * (3.0 * b.aH * b.opw * b.rho_Q * P.grhom * P.OmegaDE * b.a2 * (1.0 / k2));
+        pres = (P.cs2_DE - b.ca2_Q) * (3.0 * b.aH * b.opw * b.rho_Q * b.par.grhom * b.par.OmegaDE * b.a2 * (1.0 / k2));
     }
     if (b.rsa) {
         const double sk2 = k2 > 1e-30 ? k2 : 1e-30;
@@ -566,37 +598,44 @@ namespace dscb {
 
 // ---- RSA output projection (approximations.py:84-176): the fields that replace the
 // photon and massless-neutrino moments at an output time.  Returns true when the RSA
-// condition holds there (evaluated from (tau, a) as the reference does).
-DHD bool rsa_projection(const DiscoebCosmo& P, const Dims& D, double tau, double k, const double* y, double out[4])
+// condition holds there (evaluated from (tau, a) as the reference does).  y with tangent yd
+// (may be null) and parameter tangent tn (may be null).
+template <class T>
+DHD bool rsa_projection(const DiscoebCosmo& P, const DiscoebTangent* tn, const Dims& D, double tau, double k,
+                        const double* y, const double* yd, T out[4])
 {
-    const double a = y[0], loga = log(a), eta = y[2], deltab = y[5], thetab = y[6];
-    const double aH = aprimeoa_of(P, a, loga);
-    const int ix = spline_index(P.xe_loga, loga);
-    const double xe = spline_eval_at(P.xe_loga, ix, loga);
-    const double xeprime = spline_deriv_at(P.xe_loga, ix, loga) * aH;
-    const double cs2 = spline_eval(P.cs2a_loga, loga) / a;
-    const double akthom = 2.3038921003709498e-9 * (1.0 - P.YHe) * P.Omegab * P.H0 * P.H0;
-    const double opac = xe * akthom / (a * a);
-    const double tau_c = 1.0 / (opac > 1e-30 ? opac : 1e-30);
-    const double tau_c_prime = tau_c * (2.0 * aH - xeprime / (xe > 1e-30 ? xe : 1e-30));
-    const double Omegac = P.Omegam - P.Omegab;
-    double drhonu = 0.0;
+    const Par<T> par = make_par<T>(P, tn);
+    auto Y = [&](int i) { return seed_t<T>(y[i], yd ? yd[i] : 0.0); };
+    const T a = Y(0), loga = xlog(a), eta = Y(2), deltab = Y(5), thetab = Y(6);
+    const T aH = aprimeoa_of(P, par, tn, a, loga);
+    const int ix = spline_index(P.xe_loga, val(loga));
+    const T xe = spline_eval_at(P.xe_loga, ix, loga, tn ? tn->xe_y : nullptr, tn ? tn->xe_S : nullptr);
+    const T xeprime = spline_deriv_at(P.xe_loga, ix, loga, tn ? tn->xe_y : nullptr, tn ? tn->xe_S : nullptr) * aH;
+    const int ic = spline_index(P.cs2a_loga, val(loga));
+    const T cs2 = spline_eval_at(P.cs2a_loga, ic, loga, tn ? tn->cs2a_y : nullptr, tn ? tn->cs2a_S : nullptr) / a;
+    const T opac = xe * par.akthom / (a * a);
+    const T tau_c = rcp(xmaxc(opac, 1e-30));
+    const T tau_c_prime = tau_c * (2.0 * aH - xeprime / xmaxc(xe, 1e-30));
+    const T Omegac = par.Omegam - par.Omegab;
+    T drhonu = 0.0;
     for (int q = 0; q < D.nq; ++q) {
-        const double aq = a * P.amnu / P.q[q];
-        drhonu += P.wq[q] * y[D.iq0 + q] * sqrt(1.0 + aq * aq);
+        const T aq = a * par.amnu * (1.0 / P.q[q]);
+        drhonu = drhonu + P.wq[q] * Y(D.iq0 + q) * xsqrt(1.0 + aq * aq);
     }
-    const double rho_Q = pow(a, -3.0 * (1.0 + P.w0 + P.wa)) * exp(3.0 * (a - 1.0) * P.wa);
-    const double dgrho_wo_rel = P.grhom * (Omegac * y[3] + P.Omegab * deltab) / a + P.grhor * P.Nmnu * drhonu / (a * a) +
-                                P.grhom * P.OmegaDE * y[D.n - 2] * rho_Q * a * a;
+    const T rho_Q = xexp(-3.0 * (1.0 + par.w0 + par.wa) * loga + 3.0 * (a - 1.0) * par.wa);
+    const T dgrho_wo_rel = par.grhom * (Omegac * Y(3) + par.Omegab * deltab) / a + P.grhor * P.Nmnu * drhonu / (a * a) +
+                           par.grhom * par.OmegaDE * Y(D.n - 2) * rho_Q * a * a;
     const double k2 = k * k;
-    const double hprime = (2.0 * k2 * eta + dgrho_wo_rel) / (aH > 1e-30 ? aH : 1e-30);
-    const double sk2 = k2 > 1e-30 ? k2 : 1e-30, stc = tau_c > 1e-30 ? tau_c : 1e-30;
-    out[0] = 4.0 / sk2 * (aH * hprime - sk2 * eta) + 4.0 / (sk2 * stc) * (thetab + 0.5 * hprime);
+    const T hprime = (2.0 * k2 * eta + dgrho_wo_rel) / xmaxc(aH, 1e-30);
+    const double sk2 = k2 > 1e-30 ? k2 : 1e-30;
+    const T stc = xmaxc(tau_c, 1e-30);
+    out[0] = (4.0 / sk2) * (aH * hprime - sk2 * eta) + 4.0 / (sk2 * stc) * (thetab + 0.5 * hprime);
     out[1] = -0.5 * hprime + 3.0 / (sk2 * stc) *
              (-tau_c_prime / stc * (thetab + 0.5 * hprime) + (-aH * thetab + cs2 * sk2 * deltab + sk2 * eta));
-    out[2] = 4.0 / sk2 * (aH * hprime - sk2 * eta);
+    out[2] = (4.0 / sk2) * (aH * hprime - sk2 * eta);
     out[3] = -0.5 * hprime;
-    return P.use_rsa && (tau_c / (tau > 1e-30 ? tau : 1e-30) > P.rsa_tau_c_over_tau) && (tau * k > P.rsa_tau_over_tau_k);
+    const double tcr = val(tau_c);
+    return P.use_rsa && (tcr / (tau > 1e-30 ? tau : 1e-30) > P.rsa_tau_c_over_tau) && (tau * k > P.rsa_tau_over_tau_k);
 }
 
 // is index i one of the moments the RSA projection overwrites?  (value slot or -1 for zero)
@@ -611,55 +650,61 @@ DHD int rsa_slot(const Dims& D, int i)
     return -2;  // untouched
 }
 
-// ---- convert_to_output_variables (perturbations.py:528-677) ----
-DHD void output_vars(const DiscoebCosmo& P, const Dims& D, double k, const double* y, double* o)
+// ---- convert_to_output_variables (perturbations.py:528-677), state y with tangent yd ----
+template <class T>
+DHD void output_vars(const DiscoebCosmo& P, const DiscoebTangent* tn, const Dims& D, double k, const double* y,
+                     const double* yd, T* o)
 {
-    const double Omegac = P.Omegam - P.Omegab;
+    const Par<T> par = make_par<T>(P, tn);
+    auto Y = [&](int i) { return seed_t<T>(y[i], yd ? yd[i] : 0.0); };
+    const T Omegac = par.Omegam - par.Omegab;
     const int n = D.n, nq = D.nq, iq0 = D.iq0, iq1 = iq0 + nq;
-    const double a = y[0], eta = y[2], deltac = y[3], thetac = y[4], deltab = y[5], thetab = y[6];
-    const double deltag = y[7], thetag = y[8], deltar = y[D.idxr], thetar = y[D.idxr + 1];
-    const double loga = log(a);
-    const int inu = spline_index(P.logrhonu_loga, loga);
-    const double rhonu = exp(spline_eval_at(P.logrhonu_loga, inu, loga));
-    const int ip = (P.logpnu_loga.x == P.logrhonu_loga.x) ? inu : spline_index(P.logpnu_loga, loga);
-    const double pnu = exp(spline_eval_at(P.logpnu_loga, ip, loga));
-    double drhonu = 0.0, fnu = 0.0;
+    const T a = Y(0), eta = Y(2), deltac = Y(3), thetac = Y(4), deltab = Y(5), thetab = Y(6);
+    const T deltag = Y(7), thetag = Y(8), deltar = Y(D.idxr), thetar = Y(D.idxr + 1);
+    const T loga = xlog(a);
+    const int inu = spline_index(P.logrhonu_loga, val(loga));
+    const T rhonu = xexp(spline_eval_at(P.logrhonu_loga, inu, loga, tn ? tn->logrhonu_y : nullptr,
+                                        tn ? tn->logrhonu_S : nullptr));
+    const int ip = spline_index(P.logpnu_loga, val(loga));
+    const T pnu = xexp(spline_eval_at(P.logpnu_loga, ip, loga, tn ? tn->logpnu_y : nullptr, tn ? tn->logpnu_S : nullptr));
+    T drhonu = 0.0, fnu = 0.0;
     for (int q = 0; q < nq; ++q) {
-        const double aq = a * P.amnu / P.q[q];
-        drhonu += P.wq[q] * y[iq0 + q] * sqrt(1.0 + aq * aq);
-        fnu += P.wq[q] * y[iq1 + q];
+        const T aq = a * par.amnu * (1.0 / P.q[q]);
+        drhonu = drhonu + P.wq[q] * Y(iq0 + q) * xsqrt(1.0 + aq * aq);
+        fnu = fnu + P.wq[q] * Y(iq1 + q);
     }
-    const double deltanu = drhonu / rhonu, thetanu = k * fnu / (rhonu + pnu);
-    const double deltaq = y[n - 2], thetaq = y[n - 1];
-    const double w_Q = P.w0 + P.wa * (1.0 - a);
-    const double rho_Q = pow(a, -3.0 * (1.0 + P.w0 + P.wa)) * exp(3.0 * (a - 1.0) * P.wa);
-    const double rpt = (1.0 + w_Q) * rho_Q * P.grhom * P.OmegaDE * thetaq * a * a;
-    const double a2 = a * a;
-    const double grho = P.grhom * P.Omegam / a + (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / a2 +
-                        P.grhom * P.OmegaDE * rho_Q * a2 + P.grhom * P.Omegak;
-    const double aH = sqrt(grho / 3.0);
-    const double dgrho = P.grhom * (Omegac * deltac + P.Omegab * deltab) / a +
-                         (P.grhog * deltag + P.grhor * (P.Neff * deltar + P.Nmnu * drhonu)) / a2 +
-                         P.grhom * P.OmegaDE * deltaq * rho_Q * a2;
-    const double dgtheta = P.grhom * (Omegac * thetac + P.Omegab * thetab) / a +
-                           4.0 / 3.0 * (P.grhog * thetag + P.Neff * P.grhor * thetar) / a2 +
-                           P.Nmnu * P.grhor * k * fnu / a2 + rpt;
+    const T deltanu = drhonu / rhonu, thetanu = k * fnu / (rhonu + pnu);
+    const T deltaq = Y(n - 2), thetaq = Y(n - 1);
+    const T w_Q = par.w0 + par.wa * (1.0 - a);
+    const T rho_Q = xexp(-3.0 * (1.0 + par.w0 + par.wa) * loga + 3.0 * (a - 1.0) * par.wa);
+    const T rpt = (1.0 + w_Q) * rho_Q * par.grhom * par.OmegaDE * thetaq * a * a;
+    const T a2 = a * a;
+    const T grho = par.grhom * par.Omegam / a + (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / a2 +
+                   par.grhom * par.OmegaDE * rho_Q * a2 + par.grhom * P.Omegak;
+    const T aH = xsqrt(grho * (1.0 / 3.0));
+    const T dgrho = par.grhom * (Omegac * deltac + par.Omegab * deltab) / a +
+                    (P.grhog * deltag + P.grhor * (P.Neff * deltar + P.Nmnu * drhonu)) / a2 +
+                    par.grhom * par.OmegaDE * deltaq * rho_Q * a2;
+    const T dgtheta = par.grhom * (Omegac * thetac + par.Omegab * thetab) / a +
+                      (4.0 / 3.0) * (P.grhog * thetag + P.Neff * P.grhor * thetar) / a2 +
+                      P.Nmnu * P.grhor * k * fnu / a2 + rpt;
     const double k2 = k * k;
-    const double hprime = (2.0 * k2 * eta + dgrho) / aH;
-    const double etaprime = 0.5 * dgtheta / k2;
-    const double alpha = (hprime + 6.0 * etaprime) / 2.0 / k2;
-    const double mden = P.grhom * P.Omegam / a + P.grhor * P.Nmnu * rhonu / a2;
-    const double deltam = (P.grhom * (Omegac * deltac + P.Omegab * deltab) / a + P.grhor * P.Nmnu * drhonu / a2) / mden;
-    double thetam = (P.grhom * (Omegac * thetac + P.Omegab * thetab) / a + P.Nmnu * P.grhor * k * fnu / a2) / (3.0 * mden);
-    const double deltabc = (P.grhom * (Omegac * deltac + P.Omegab * deltab) / a) / (P.grhom * P.Omegam / a);
-    double thetabc = (P.grhom * (Omegac * thetac + P.Omegab * thetab) / a) / (3.0 * (P.grhom * P.Omegam / a) / a2);
-    thetam += alpha * k2;
-    thetabc += alpha * k2;
+    const T hprime = (2.0 * k2 * eta + dgrho) / aH;
+    const T etaprime = 0.5 * dgtheta / k2;
+    const T alpha = (hprime + 6.0 * etaprime) / 2.0 / k2;
+    const T mden = par.grhom * par.Omegam / a + P.grhor * P.Nmnu * rhonu / a2;
+    const T deltam = (par.grhom * (Omegac * deltac + par.Omegab * deltab) / a + P.grhor * P.Nmnu * drhonu / a2) / mden;
+    T thetam = (par.grhom * (Omegac * thetac + par.Omegab * thetab) / a + P.Nmnu * P.grhor * k * fnu / a2) / (3.0 * mden);
+    const T deltabc = (par.grhom * (Omegac * deltac + par.Omegab * deltab) / a) / (par.grhom * par.Omegam / a);
+    T thetabc = (par.grhom * (Omegac * thetac + par.Omegab * thetab) / a) / (3.0 * (par.grhom * par.Omegam / a) / a2);
+    thetam = thetam + alpha * k2;
+    thetabc = thetabc + alpha * k2;
+    const T iaH = rcp(aH);
     o[0] = eta; o[1] = etaprime; o[2] = hprime; o[3] = alpha;
-    o[4] = deltam; o[5] = thetam / aH; o[6] = deltabc; o[7] = thetabc / aH;
-    o[8] = deltac; o[9] = thetac / aH; o[10] = deltab; o[11] = thetab / aH;
-    o[12] = deltag; o[13] = thetag / aH; o[14] = deltar; o[15] = thetar / aH;
-    o[16] = deltanu; o[17] = thetanu / aH; o[18] = deltaq; o[19] = thetaq / aH;
+    o[4] = deltam; o[5] = thetam * iaH; o[6] = deltabc; o[7] = thetabc * iaH;
+    o[8] = deltac; o[9] = thetac * iaH; o[10] = deltab; o[11] = thetab * iaH;
+    o[12] = deltag; o[13] = thetag * iaH; o[14] = deltar; o[15] = thetar * iaH;
+    o[16] = deltanu; o[17] = thetanu * iaH; o[18] = deltaq; o[19] = thetaq * iaH;
 }
 
 }  // namespace dscb

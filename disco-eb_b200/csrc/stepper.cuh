@@ -118,7 +118,7 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
 {
     const int n = D.n, nq = D.nq, iq0 = D.iq0, idxr = D.idxr;
     const double k2 = k * k;
-    const double Omegac = P.Omegam - P.Omegab;
+    const T Omegac = b.par.Omegam - b.par.Omegab;
     // 1/v of momentum bin q on lane q
     T ivl = 1.0;
     if (tm.full() && tm.lane < nq) ivl = inv_vq(P, b, tm.lane);
@@ -141,9 +141,9 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
     const double deltar = y[idxr], thetar = y[idxr + 1], yr2 = y[idxr + 2];
     const double deltaq = y[n - 2], thetaq = y[n - 1];
     const T rQa2 = b.rho_Q * b.a2;
-    const T dgm = P.grhom * (Omegac * deltac + P.Omegab * deltab) * b.ia;
+    const T dgm = b.par.grhom * (Omegac * deltac + b.par.Omegab * deltab) * b.ia;
     const T dgnu = P.grhor * P.Nmnu * drho * b.ia2;
-    const T dgq = P.grhom * P.OmegaDE * deltaq * rQa2;
+    const T dgq = b.par.grhom * b.par.OmegaDE * deltaq * rQa2;
     const T dgrho = dgm + (P.grhog * deltag + P.grhor * P.Neff * deltar) * b.ia2 + dgnu + dgq;
     const T dgrho_wo_rel = dgm + dgnu + dgq;
     T H, thg, thr, dge, dre;
@@ -161,14 +161,14 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
         thg = T(thetag);
         thr = T(thetar);
     }
-    const T rptq = b.opw * P.grhom * P.OmegaDE * thetaq * rQa2;
-    const T dgtheta = P.grhom * (Omegac * thetac + P.Omegab * thetab) * b.ia +
+    const T rptq = b.opw * b.par.grhom * b.par.OmegaDE * thetaq * rQa2;
+    const T dgtheta = b.par.grhom * (Omegac * thetac + b.par.Omegab * thetab) * b.ia +
                       (4.0 / 3.0) * (P.grhog * thg + P.Neff * P.grhor * thr) * b.ia2 + P.Nmnu * P.grhor * k * fnu * b.ia2 +
                       rptq;
     const T E = (0.5 / k2) * dgtheta;
     const double cs2Q = P.cs2_DE;
     const T dgpres = (P.grhog * dge + P.grhor * P.Neff * dre) * b.ia2 * (1.0 / 3.0) + P.grhor * P.Nmnu * dp * b.ia2 +
-                     (cs2Q * P.grhom * P.OmegaDE * deltaq * rQa2 + (cs2Q - b.ca2_Q) * (3.0 * b.aH * rptq * (1.0 / k2)));
+                     (cs2Q * b.par.grhom * b.par.OmegaDE * deltaq * rQa2 + (cs2Q - b.ca2_Q) * (3.0 * b.aH * rptq * (1.0 / k2)));
     const bool hier_photons = !b.rsa && !b.tca;
     const T polter = hier_photons ? T(y9 + y[D.idxgp] + y[D.idxgp + 2]) : T(0.0);
     const T alpha = (H + 6.0 * E) * (0.5 / k2);

@@ -56,6 +56,14 @@ typedef struct {
     DiscoebSpline xe_loga, cs2a_loga, logrhonu_loga, logpnu_loga;
 } DiscoebCosmo;
 
+/* Tangent of one cosmology along one parameter direction: the derivatives of the scalar
+ * parameters the solve reads and of the (y, S) arrays of the four spline tables (the knots do
+ * not depend on the parameters).  Device pointers; NULL arrays mean zero. */
+typedef struct {
+    double grhom, Omegam, Omegab, OmegaDE, amnu, w0, wa, H0;
+    const double *xe_y, *xe_S, *cs2a_y, *cs2a_S, *logrhonu_y, *logrhonu_S, *logpnu_y, *logpnu_S;
+} DiscoebTangent;
+
 /* Step control: diffrax PIDController fields (perturbations.py:913-914, :1124-1128). */
 typedef struct {
     double rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin;
