@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(256) fwd_structured_kernel(
         double swm[3] = {sw[3 * mode], sw[3 * mode + 1], sw[3 * mode + 2]};
         tm.sync();
         const size_t obase = (size_t)mode * n_out;
-        auto emit = [&](int j, const double* y) {
+        auto emit = [&](int j, const double* y, int) {
             const size_t o = obase + j;
             emit_output(tm, *P, D, k, tau_out[j], y, y_full ? y_full + o * n : nullptr,
                         y_out20 ? y_out20 + o * 20 : nullptr, M.f);
@@ -102,6 +102,98 @@ __global__ void __launch_bounds__(256) fwd_structured_kernel(
         if (tm.leader()) {
             status[mode] = st;
             nsteps[mode] = steps;
+        }
+        tm.sync();
+    }
+}
+
+constexpr int kTanDoubles = (sizeof(DiscoebTangent) + 7) / 8;
+
+// Forward solve + tangent along one parameter direction per warp: warp w handles
+// (mode w / n_dir, direction w % n_dir).  The step sequence is chosen on the forward state
+// only, so the tangent is the derivative of the discrete solution with the accepted steps
+// held fixed (what forward-mode AD through the reference's diffrax loop computes).
+__global__ void __launch_bounds__(256) jvp_kernel(
+    const DiscoebCosmo* __restrict__ cosmo, const DiscoebTangent* __restrict__ tangents, int n_dir,
+    DiscoebControl ctrl, int n_modes, const double* __restrict__ kmodes, const double* __restrict__ tau_start,
+    const double* __restrict__ y0, const double* __restrict__ y0_dot, const double* __restrict__ sw, int n_out,
+    const double* __restrict__ tau_out, const double* __restrict__ tau_out_dot, int mem_doubles, int tan_doubles,
+    double* y_out20, double* y_out20_dot, int32_t* status, int32_t* nsteps)
+{
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5;
+    const WarpTeam tm{(int)(threadIdx.x & 31)};
+    const int wpb = blockDim.x >> 5;
+    double* base = smem + (size_t)warp * (kCosmoDoubles + kTanDoubles + mem_doubles + tan_doubles);
+    DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(base);
+    DiscoebTangent* TN = reinterpret_cast<DiscoebTangent*>(base + kCosmoDoubles);
+    double* wmem = base + kCosmoDoubles + kTanDoubles;
+    double* tmem = wmem + mem_doubles;
+    copy_cosmo(tm, cosmo, P);
+    const int total = n_modes * n_dir;
+    for (int w = blockIdx.x * wpb + warp; w < total; w += gridDim.x * wpb) {
+        const int mode = w / n_dir, dir = w - mode * n_dir;
+        {
+            const int* s = reinterpret_cast<const int*>(tangents + dir);
+            int* d = reinterpret_cast<int*>(TN);
+            for (int i = tm.lane; i < (int)(sizeof(DiscoebTangent) / 4); i += 32) d[i] = s[i];
+        }
+        const Dims D = make_dims(*P);
+        const int n = D.n;
+        ModeMem M = carve(wmem, D);
+        TanMem TT = carve_tan(tmem, D);
+        const double k = kmodes[mode];
+        for (int i = tm.lane; i < n; i += 32) {
+            M.y[i] = y0[(size_t)mode * n + i];
+            TT.yd[i] = y0_dot[((size_t)dir * n_modes + mode) * n + i];
+        }
+        double swm[3] = {sw[3 * mode], sw[3 * mode + 1], sw[3 * mode + 2]};
+        tm.sync();
+        auto emit = [&](int j, const double* y, int regime) {
+            // f at the output time (left limit of the last step's regime), for the moving output time
+            int hint = P->xe_loga.n_knots / 2;
+            Bg<double> b;
+            bg_eval_team(tm, *P, y[0], tau_out[j], k, regime, b, hint);
+            rhs_team(tm, *P, D, b, k, tau_out[j], y, TT.fd, (double*)nullptr);
+            tm.sync();
+            const double td = tau_out_dot[(size_t)dir * n_out + j];
+            for (int i = tm.lane; i < n; i += 32) TT.jk[i] = TT.yd[i] + TT.fd[i] * td;
+            tm.sync();
+            Dual fld[4];
+            const bool rsa = rsa_projection<Dual>(*P, TN, D, tau_out[j], k, y, TT.jk, fld);
+            for (int i = tm.lane; i < n; i += 32) {
+                double v = y[i], vd = TT.jk[i];
+                if (rsa) {
+                    const int sl = rsa_slot(D, i);
+                    if (sl >= 0) { v = fld[sl].v; vd = fld[sl].d; }
+                    else if (sl == -1) { v = 0.0; vd = 0.0; }
+                }
+                M.f[i] = v;
+                TT.fd[i] = vd;
+            }
+            tm.sync();
+            if (tm.leader()) {
+                Dual o[20];
+                output_vars<Dual>(*P, TN, D, k, M.f, TT.fd, o);
+                const size_t oo = (size_t)mode * n_out + j;
+                for (int q = 0; q < 20; ++q) y_out20_dot[((size_t)dir * n_modes * n_out + oo) * 20 + q] = o[q].d;
+                if (dir == 0 && y_out20)
+                    for (int q = 0; q < 20; ++q) y_out20[oo * 20 + q] = o[q].v;
+            }
+            tm.sync();
+        };
+        const SolveResult R = solve_mode(tm, *P, D, ctrl, k, tau_start[mode], swm, n_out, tau_out, M, emit, TN, &TT);
+        const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+        for (int j = R.outputs; j < n_out; ++j) {
+            const size_t oo = (size_t)mode * n_out + j;
+            for (int i = tm.lane; i < 20; i += 32) {
+                y_out20_dot[((size_t)dir * n_modes * n_out + oo) * 20 + i] = qnan;
+                if (dir == 0 && y_out20) y_out20[oo * 20 + i] = qnan;
+            }
+        }
+        if (tm.leader() && dir == 0) {
+            status[mode] = R.status;
+            nsteps[mode] = R.steps;
         }
         tm.sync();
     }
@@ -178,6 +270,43 @@ int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
                                                           y0, switch_tau, n_out, tau_out, mem, y_full, y_out20, status,
                                                           nsteps);
     (void)n_sm;
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int32_t discoeb_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, const DiscoebTangent* tangents_dev,
+                    int32_t n_dir, const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes,
+                    const double* tau_start, const double* y0, const double* y0_dot, const double* switch_tau,
+                    int32_t n_out, const double* tau_out, const double* tau_out_dot, double* y_out20,
+                    double* y_out20_dot, int32_t* status, int32_t* nsteps, void* stream)
+{
+    int rc = validate_cosmo(cosmo_host);
+    if (rc) return rc;
+    if (!cosmo_dev || !ctrl || !tangents_dev || n_dir < 1 || n_modes < 0 || n_out < 1) return DISCOEB_EINVAL;
+    if (n_modes == 0) return DISCOEB_SUCCESS;
+    if (!kmodes || !tau_start || !y0 || !y0_dot || !switch_tau || !tau_out || !tau_out_dot || !y_out20_dot ||
+        !status || !nsteps)
+        return DISCOEB_EINVAL;
+    if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED) return DISCOEB_EUNSUPPORTED;
+    if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
+    const Dims D = make_dims(*cosmo_host);
+    const int mem = mode_mem_doubles(D), tmem = tan_mem_doubles(D);
+    const size_t per_warp = (size_t)(kCosmoDoubles + kTanDoubles + mem + tmem) * sizeof(double);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
+    int max_optin = 0;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    int wpb = ctrl->warps_per_block > 0 ? ctrl->warps_per_block : 2;
+    if (wpb > 8) wpb = 8;
+    while (wpb > 1 && per_warp * wpb > (size_t)max_optin) --wpb;
+    if (per_warp > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
+    const size_t smem = per_warp * wpb;
+    if (cudaFuncSetAttribute(jvp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return DISCOEB_ECUDA;
+    const long long total = (long long)n_modes * n_dir;
+    const int blocks = (int)((total + wpb - 1) / wpb);
+    jvp_kernel<<<blocks, 32 * wpb, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        cosmo_dev, tangents_dev, n_dir, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot, switch_tau, n_out, tau_out,
+        tau_out_dot, mem, tmem, y_out20, y_out20_dot, status, nsteps);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 

@@ -105,8 +105,39 @@ DHD ModeMem carve(double* base, const Dims& D)
 // scalar slots
 enum { SC_W00 = 0, SC_ETAC = 1, SC_CINV = 2, SC_F1Z = 11, SC_F1U = 14 };
 
+// tangent workspace: y', the stage state tangent u', two n-vector scratches and the 8 stage
+// tangents K'
+struct TanMem {
+    double *yd, *ud, *fd, *jk, *Kd;
+};
+DHD int tan_mem_doubles(const Dims& D) { return 12 * D.n; }
+DHD TanMem carve_tan(double* base, const Dims& D)
+{
+    const int n = D.n;
+    TanMem t;
+    t.yd = base;
+    t.ud = t.yd + n;
+    t.fd = t.ud + n;
+    t.jk = t.fd + n;
+    t.Kd = t.jk + n;
+    return t;
+}
+
 DHD double dual_with(double x, double) { return x; }
 DHD Dual dual_with(const Dual& x, double d) { return Dual(x.v, d); }
+
+// state entry with its first-direction part yd and second-direction part yk (null = 0)
+DHD double mk_state(const double*, double y, double, double) { return y; }
+DHD Dual mk_state(const Dual*, double y, double yd, double) { return Dual(y, yd); }
+DHD HDual mk_state(const HDual*, double y, double yd, double yk) { return HDual(Dual(y, yd), Dual(yk, 0.0)); }
+template <class T> DHD T state_at(const double* y, const double* yd, const double* yk, int j)
+{
+    return mk_state((const T*)nullptr, y[j], yd ? yd[j] : 0.0, yk ? yk[j] : 0.0);
+}
+// component c of a value: 0 value, 1 first direction, 2 second direction, 3 mixed
+DHD double comp(double x, int c) { return c == 0 ? x : 0.0; }
+DHD double comp(const Dual& x, int c) { return c == 0 ? x.v : (c == 1 ? x.d : 0.0); }
+DHD double comp(const HDual& x, int c) { return c == 0 ? x.v.v : (c == 1 ? x.v.d : (c == 2 ? x.d.v : x.d.d)); }
 
 // ---- RHS f(tau, y) (all entries), T = double or Dual in a ----
 // The metric functionals and the 15 "special" rows are computed in straight-line code by every
@@ -114,8 +145,10 @@ DHD Dual dual_with(const Dual& x, double d) { return Dual(x.v, d); }
 // uniform class.  Same equations as model_synchronous (perturbations.py:88-525).
 template <class TM, class T>
 DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau,
-                  const double* y, double* f, double* dfda)
+                  const double* y, double* f, double* dfda, const double* yd = nullptr, const double* yk = nullptr,
+                  int fcomp = 0, int dcomp = 1)
 {
+    auto Y = [&](int j) { return state_at<T>(y, yd, yk, j); };
     const int n = D.n, nq = D.nq, iq0 = D.iq0, idxr = D.idxr;
     const double k2 = k * k;
     const T Omegac = b.par.Omegam - b.par.Omegab;
@@ -130,16 +163,16 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
             const T iv = tm.full() ? tm.bcast(ivl, q) : inv_vq(P, b, q);
             const T v = tm.full() ? tm.bcast(vl, q) : rcp(iv);
             const double w = P.wq[q];
-            drho = drho + (w * y[iq0 + q]) * iv;
-            dp = dp + (w * y[iq0 + q]) * v;
-            fnu = fnu + w * y[iq0 + nq + q];
+            drho = drho + (w * Y(iq0 + q)) * iv;
+            dp = dp + (w * Y(iq0 + q)) * v;
+            fnu = fnu + w * Y(iq0 + nq + q);
         }
     }
     dp = dp * (1.0 / 3.0);
-    const double eta = y[2], deltac = y[3], thetac = y[4], deltab = y[5], thetab = y[6];
-    const double deltag = y[7], thetag = y[8], y9 = y[9];
-    const double deltar = y[idxr], thetar = y[idxr + 1], yr2 = y[idxr + 2];
-    const double deltaq = y[n - 2], thetaq = y[n - 1];
+    const T eta = Y(2), deltac = Y(3), thetac = Y(4), deltab = Y(5), thetab = Y(6);
+    const T deltag = Y(7), thetag = Y(8), y9 = Y(9);
+    const T deltar = Y(idxr), thetar = Y(idxr + 1), yr2 = Y(idxr + 2);
+    const T deltaq = Y(n - 2), thetaq = Y(n - 1);
     const T rQa2 = b.rho_Q * b.a2;
     const T dgm = b.par.grhom * (Omegac * deltac + b.par.Omegab * deltab) * b.ia;
     const T dgnu = P.grhor * P.Nmnu * drho * b.ia2;
@@ -156,10 +189,10 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
         thr = -0.5 * H;
     } else {
         H = (2.0 * k2 * eta + dgrho) * b.iaHG;
-        dge = T(deltag);
-        dre = T(deltar);
-        thg = T(thetag);
-        thr = T(thetar);
+        dge = deltag;
+        dre = deltar;
+        thg = thetag;
+        thr = thetar;
     }
     const T rptq = b.opw * b.par.grhom * b.par.OmegaDE * thetaq * rQa2;
     const T dgtheta = b.par.grhom * (Omegac * thetac + b.par.Omegab * thetab) * b.ia +
@@ -170,7 +203,7 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
     const T dgpres = (P.grhog * dge + P.grhor * P.Neff * dre) * b.ia2 * (1.0 / 3.0) + P.grhor * P.Nmnu * dp * b.ia2 +
                      (cs2Q * b.par.grhom * b.par.OmegaDE * deltaq * rQa2 + (cs2Q - b.ca2_Q) * (3.0 * b.aH * rptq * (1.0 / k2)));
     const bool hier_photons = !b.rsa && !b.tca;
-    const T polter = hier_photons ? T(y9 + y[D.idxgp] + y[D.idxgp + 2]) : T(0.0);
+    const T polter = hier_photons ? y9 + Y(D.idxgp) + Y(D.idxgp + 2) : T(0.0);
     const T alpha = (H + 6.0 * E) * (0.5 / k2);
     // special rows
     T sp[15];
@@ -184,11 +217,11 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
     if (!b.rsa) {
         sp[7] = (4.0 / 3.0) * (-thg - 0.5 * H);
         sp[8] = k2 * (0.25 * dge - 0.5 * y9) - b.opac * (thg - thetab);
-        sp[9] = (8.0 / 15.0) * (thg + k2 * alpha) - 0.6 * k * y[10] - b.opac * (y9 - 0.1 * polter);
+        sp[9] = (8.0 / 15.0) * (thg + k2 * alpha) - 0.6 * k * Y(10) - b.opac * (y9 - 0.1 * polter);
         sp[10] = (4.0 / 3.0) * (-thr - 0.5 * H);
         sp[11] = k2 * (0.25 * dre - 0.5 * yr2);
         sp[12] = b.ufa ? -1.5 * (tau > 1e-30 ? b.itau : 1e30) * yr2 + (4.0 / 15.0) * (thr + 0.5 * H)
-                       : (8.0 / 15.0) * (thr + k2 * alpha) - 0.6 * k * y[idxr + 3];
+                       : (8.0 / 15.0) * (thr + k2 * alpha) - 0.6 * k * Y(idxr + 3);
     } else {
         for (int q = 7; q < 13; ++q) sp[q] = 0.0;
     }
@@ -204,8 +237,8 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
 #pragma unroll
         for (int ss = 0; ss < 15; ++ss) {
             const int i = special_row(D, ss);
-            f[i] = val(sp[ss]);
-            if (dfda) dfda[i] = der(sp[ss]);
+            f[i] = comp(sp[ss], fcomp);
+            if (dfda) dfda[i] = comp(sp[ss], dcomp);
         }
     }
     const T g0 = H, g1 = E, g2 = polter;
@@ -218,9 +251,9 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
         int st;
         bool trunc;
         hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
-        const T fi = lo * y[i - st] + di * y[i] + up * y[trunc ? i : i + st] + u[0] * g0 + u[1] * g1 + u[2] * g2;
-        f[i] = val(fi);
-        if (dfda) dfda[i] = der(fi);
+        const T fi = lo * Y(i - st) + di * Y(i) + up * Y(trunc ? i : i + st) + u[0] * g0 + u[1] * g1 + u[2] * g2;
+        f[i] = comp(fi, fcomp);
+        if (dfda) dfda[i] = comp(fi, dcomp);
     }
 }
 
@@ -460,11 +493,64 @@ struct SolveResult {
     int status, steps, accepted, outputs;
 };
 
+// Tangent of stage s of the Rosenbrock step along one parameter direction: with
+// k_s = W^{-1} r_s, the derivative is k_s' = W^{-1} (r_s' + J' k_s), where r_s' holds the
+// directional derivative of f at the stage state (state tangent u_s' and the parameter /
+// table tangents tn) and J' k_s = d/de [J(y_n + e y_n', p + e p') k_s] is one hyper-dual RHS
+// evaluation.  The step sizes are the forward solve's (the derivative of the discrete scheme
+// with the accepted step sequence held fixed).
+template <class TM>
+DDV void tangent_stage(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
+                       const ModeMem& M, const TanMem& TT, const DiscoebTangent* tn, int s, int& hint)
+{
+    const int n = D.n;
+    const double* us = (s == 0) ? M.y : M.u;
+    for (int i = tm.lane; i < n; i += tm.nl) {
+        double v;
+        if (s == 0) v = TT.yd[i];
+        else if (s <= 5) {
+            v = TT.yd[i];
+            for (int j = 0; j < s; ++j) v += kR5.a[s][j] * TT.Kd[j * n + i];
+        } else {
+            v = TT.ud[i] + TT.Kd[(s - 1) * n + i];
+        }
+        TT.ud[i] = v;
+    }
+    tm.sync();
+    const double ts = (s == 0) ? t : ((s <= 5) ? t + kR5.c[s] * h : t + h);
+    {
+        Bg<Dual> bt;
+        bg_eval_team(tm, P, Dual(us[0], TT.ud[0]), ts, k, regime, bt, hint, tn);
+        rhs_team(tm, P, D, bt, k, ts, us, TT.fd, (double*)nullptr, TT.ud, (const double*)nullptr, 1, 1);
+    }
+    const double* Ks = M.K + s * n;
+    {
+        Bg<HDual> bh;
+        bg_eval_team(tm, P, HDual(Dual(M.y[0], TT.yd[0]), Dual(Ks[0], 0.0)), t, k, regime, bh, hint, tn);
+        rhs_team(tm, P, D, bh, k, t, M.y, TT.jk, (double*)nullptr, TT.yd, Ks, 3, 3);
+    }
+    tm.sync();
+    Bg<double> b0;
+    b0.rsa = (regime & 1) != 0;
+    b0.ufa = !b0.rsa && (regime & 2) != 0;
+    b0.tca = !b0.rsa && (regime & 4) != 0;
+    double* Kds = TT.Kd + s * n;
+    const double ih = 1.0 / h;
+    for (int i = tm.lane; i < n; i += tm.nl) {
+        double r = TT.fd[i] + TT.jk[i];
+        if (s < 5) r += h * kR5.d[s] * dtau_row(D, b0, t, i, TT.yd);
+        for (int j = 0; j < s; ++j) r += kR5.C[s][j] * ih * TT.Kd[j * n + i];
+        Kds[i] = r;
+    }
+    tm.sync();
+    solve_W(tm, D, M, h, Kds);
+}
+
 // One Rodas5 step from (t, y) with size h: on return M.u + M.K[7] is the candidate and
 // M.K[7] the error estimate.  Returns false on a non-finite factorisation.
 template <class TM>
 DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
-                     const ModeMem& M, int& hint)
+                     const ModeMem& M, int& hint, const DiscoebTangent* tn = nullptr, const TanMem* TT = nullptr)
 {
     const int n = D.n;
     // Jacobian column d f/d a and f(y) in one dual pass
@@ -505,6 +591,7 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
         }
         tm.sync();
         solve_W(tm, D, M, h, Ks);
+        if (TT) tangent_stage(tm, P, D, k, t, h, regime, M, *TT, tn, s, hint);
     }
     return ok;
 }
@@ -513,7 +600,9 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
 // emit(j, y) with the state exactly at tout[j].  sw[3]: RSA start, UFA start, TCA end.
 template <class TM, class Emit>
 DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, const DiscoebControl& C, double k,
-                           double t0, const double* sw, int nout, const double* tout, const ModeMem& M, Emit& emit)
+                           double t0, const double* sw, int nout, const double* tout, const ModeMem& M, Emit& emit,
+                           const DiscoebTangent* tn = nullptr, const TanMem* TT = nullptr, double* tlog = nullptr,
+                           int tlog_cap = 0)
 {
     const int n = D.n;
     SolveResult R = {DISCOEB_OK, 0, 0, 0};
@@ -537,13 +626,13 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
         for (int q = 0; q < 3; ++q)
             if (sw[q] > t && sw[q] < tev) tev = sw[q];
         const double dt_try = dt;
-        double tn = t + dt;
+        double tnext = t + dt;
         bool clipped = false;
-        if (tn >= tev - 1e-12 * fabs(tev)) { clipped = tn > tev; tn = tev; }
-        const double h = tn - t;
+        if (tnext >= tev - 1e-12 * fabs(tev)) { clipped = tnext > tev; tnext = tev; }
+        const double h = tnext - t;
         if (!(h > 1e-14 * fabs(t))) { R.status = DISCOEB_DT_UNDERFLOW; break; }
         const int regime = regime_at(P, t, sw);
-        const bool ok = rodas5_step(tm, P, D, k, t, h, regime, M, hint);
+        const bool ok = rodas5_step(tm, P, D, k, t, h, regime, M, hint, tn, TT);
         R.steps++;
         // weighted RMS error over (a, eta, delta_c, delta_b, theta_b, delta_gamma)
         // (perturbations.py:855-878 with the weights of :913)
@@ -574,10 +663,13 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
         if (keep) {
             R.accepted++;
             for (int i = tm.lane; i < n; i += tm.nl) M.y[i] = M.u[i] + M.K[7 * n + i];
+            if (TT)
+                for (int i = tm.lane; i < n; i += tm.nl) TT->yd[i] = TT->ud[i] + TT->Kd[7 * n + i];
             tm.sync();
-            t = tn;
+            if (tlog && R.accepted <= tlog_cap) tlog[R.accepted - 1] = tnext;
+            t = tnext;
             while (iout < nout && tout[iout] <= t) {
-                emit(iout, M.y);
+                emit(iout, M.y, regime);
                 iout++;
             }
             if (clipped && dt_try > dtn) dtn = dt_try;

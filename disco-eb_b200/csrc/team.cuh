@@ -21,9 +21,9 @@ struct WarpTeam {
     }
     __device__ __forceinline__ bool leader() const { return lane == 0; }
     __device__ __forceinline__ double bcast(double x, int src) const { return __shfl_sync(0xffffffffu, x, src); }
-    __device__ __forceinline__ Dual bcast(const Dual& x, int src) const
+    template <class B> __device__ __forceinline__ DualT<B> bcast(const DualT<B>& x, int src) const
     {
-        return Dual(__shfl_sync(0xffffffffu, x.v, src), __shfl_sync(0xffffffffu, x.d, src));
+        return DualT<B>(bcast(x.v, src), bcast(x.d, src));
     }
     __device__ __forceinline__ bool full() const { return true; }
 };
@@ -36,7 +36,7 @@ struct HostTeam {
     DHD double sum(double x) const { return x; }
     DHD bool leader() const { return true; }
     DHD double bcast(double x, int) const { return x; }
-    DHD Dual bcast(const Dual& x, int) const { return x; }
+    template <class B> DHD DualT<B> bcast(const DualT<B>& x, int) const { return x; }
     DHD bool full() const { return false; }
 };
 

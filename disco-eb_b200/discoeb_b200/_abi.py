@@ -43,6 +43,12 @@ class DiscoebCosmo(ctypes.Structure):
                 + [(f, DiscoebSpline) for f in ("xe_loga", "cs2a_loga", "logrhonu_loga", "logpnu_loga")])
 
 
+class DiscoebTangent(ctypes.Structure):
+    _fields_ = ([(f, ctypes.c_double) for f in ("grhom", "Omegam", "Omegab", "OmegaDE", "amnu", "w0", "wa", "H0")]
+                + [(f, ctypes.c_void_p) for f in ("xe_y", "xe_S", "cs2a_y", "cs2a_S", "logrhonu_y", "logrhonu_S",
+                                                   "logpnu_y", "logpnu_S")])
+
+
 class DiscoebControl(ctypes.Structure):
     _fields_ = ([(f, ctypes.c_double) for f in ("rtol", "atol", "pcoeff", "icoeff", "dcoeff", "factormax", "factormin")]
                 + [(f, ctypes.c_int32) for f in ("max_steps", "method", "warps_per_block", "reserved")])
@@ -124,6 +130,9 @@ def lib():
                                   ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp, vp]
         L.discoeb_fwd.restype = ctypes.c_int32
         L.discoeb_rhs.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, vp, vp, vp, ctypes.c_int32, vp, vp]
+        L.discoeb_jvp.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), vp, ctypes.c_int32, ctypes.POINTER(DiscoebControl),
+                                  ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp, vp, vp]
+        L.discoeb_jvp.restype = ctypes.c_int32
         L.discoeb_rhs.restype = ctypes.c_int32
         if L.discoeb_abi_version() != ABI_VERSION:
             raise RuntimeError("libdiscoeb_b200.so ABI version mismatch; rebuild it")

@@ -112,7 +112,7 @@ def setup_background_evolution(*, amin, amax, param):
     param["logrhonu_of_loga_spline"] = spline_interpolation(loga, np.log(rhonu_), uniform=True)
     param["logpnu_of_loga_spline"] = spline_interpolation(loga, np.log(pnu_), uniform=True)
     param["logppseudonu_of_loga_spline"] = spline_interpolation(loga, np.log(ppnu_), uniform=True)
-    rhonu0 = float(np.exp(param["logrhonu_of_loga_spline"].evaluate(0.0)))
+    rhonu0 = np.exp(param["logrhonu_of_loga_spline"].evaluate(0.0))
     param["Omegamnu"] = param["grhor"] * rhonu0 / param["grhom"]
     Omegar = (param["Neff"] + param["Nmnu"] * rhonu0) * param["grhor"] / param["grhom"]
     Omegag = param["grhog"] / param["grhom"]
@@ -123,11 +123,13 @@ def setup_background_evolution(*, amin, amax, param):
 
 
 def evolve_background(*, param, thermo_module="RECFAST", num_thermo: int = 256, rtol: float = 1e-5,
-                      atol: float = 1e-7, order: int = 5, class_thermo=None):
+                      atol: float = 1e-7, order: int = 5, class_thermo=None, trace=None, replay=None):
     """Background + Recfast thermal history + visibility (background.py:191-345).
 
     Returns a new dict (the caller's dict is not modified, as under the
     reference's ``jax.jit``).  Only ``thermo_module='RECFAST'`` is provided.
+    ``trace``/``replay``: record / repeat the Recfast step sequence (see
+    thermodynamics_recfast.solve_pid_grk4a), for derivatives with respect to parameters.
     """
     if thermo_module != "RECFAST":
         raise ValueError(f"thermo_module {thermo_module!r} is not provided; use 'RECFAST'")
@@ -137,9 +139,9 @@ def evolve_background(*, param, thermo_module="RECFAST", num_thermo: int = 256, 
     param = setup_background_evolution(amin=amin, amax=amax, param=param)
     param, tau, aexp, cs2, Tm, mu, xe, xeHI, xeHeI, xeHeII, xeprime_recfast = _recfast.evaluate_thermo(
         param=param, num_thermo=num_thermo,
-        aprimeoa_fn=lambda a: float(get_aprimeoa(param=param, aexp=a)),
+        aprimeoa_fn=lambda a: get_aprimeoa(param=param, aexp=a)[()],
         dadtau_fn=lambda a: dadtau(a, param),
-        dtauda_fn=lambda a: dtauda(a, param))
+        dtauda_fn=lambda a: dtauda(a, param), trace=trace, replay=replay)
     param["aexp"] = aexp
     param["tau"] = tau
     param["xe"] = xe
@@ -173,8 +175,8 @@ def evolve_background(*, param, thermo_module="RECFAST", num_thermo: int = 256, 
     param["gvis"] = vis
     param["gvisprime"] = (opacprime + opac**2) * expmmu
     param["gvispprime"] = (opacpprime + 3 * opac * opacprime + opac**3) * expmmu
-    param["tau0"] = float(param["tau_of_a_spline"].evaluate(1.0))
-    param["tau_maxvis"] = float(param["tau"][int(np.argmax(param["gvis"]))])
+    param["tau0"] = param["tau_of_a_spline"].evaluate(1.0)[()]
+    param["tau_maxvis"] = np.real(param["tau"][int(np.argmax(np.real(param["gvis"])))])[()]
     param["xeprime_recf"] = xeprime_recfast
     param["xeprime"] = xeprime
     return param

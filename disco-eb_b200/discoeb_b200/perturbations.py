@@ -105,8 +105,8 @@ def adiabatic_ics(*, tau, param, kmode, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax):
     tau, k = np.broadcast_arrays(tau, k)
     n = nvar_of(lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax)
     iq0 = 10 + lmaxg + lmaxgp + lmaxr
-    y = np.zeros(tau.shape + (n,))
     a = param["a_of_tau_spline"].evaluate(tau)
+    y = np.zeros(tau.shape + (n,), dtype=np.result_type(a.dtype, np.asarray(param["grhom"]).dtype, np.float64))
     rhonu_bg = np.exp(param["logrhonu_of_loga_spline"].evaluate(np.log(a)))
     rhom = param["grhom"] * param["Omegam"] / a**3
     rhor = (param["grhog"] + param["grhor"] * (param["Neff"] + param["Nmnu"] * rhonu_bg)) / a**4

@@ -19,14 +19,16 @@ class spline_interpolation:
     """Natural cubic spline through ``(xin, yin)`` (reference class of the same name)."""
 
     def __init__(self, xin, yin, integrate_from_start: bool = True, uniform: bool = False):
-        x = np.array(xin, dtype=np.float64).ravel()
-        y = np.array(yin, dtype=np.float64).ravel()
+        x = np.array(xin).ravel()
+        x = x.astype(np.result_type(x.dtype, np.float64))
+        y = np.array(yin).ravel()
+        y = y.astype(np.result_type(y.dtype, np.float64))
         n = y.shape[0]
         if n < 2:
             raise ValueError("There must be at least two data points.")
         # forward-fill NaNs (spline_interpolation.py:33-40): y repeats the last
         # finite value, x grows geometrically by 1.01
-        if np.isnan(y).any() or np.isnan(x).any():
+        if np.isnan(np.real(y)).any() or np.isnan(np.real(x)).any():
             for i in range(n):
                 prev_y = y[i - 1] if i > 0 else y[0]
                 prev_x = x[i - 1] if i > 0 else x[0]
@@ -36,21 +38,21 @@ class spline_interpolation:
                     x[i] = prev_x * 1.01
         h = x[1:] - x[:-1]
         m = n - 2
-        S = np.zeros(n)
+        S = np.zeros(n, dtype=np.result_type(x.dtype, y.dtype))
         if m > 0:
             a = h[:-1]
             b = 2.0 * (h[:-1] + h[1:])
             c = h[1:]
             d = 6.0 * ((y[2:] - y[1:-1]) / h[1:] - (y[1:-1] - y[:-2]) / h[:-1])
-            cp = np.zeros(m)
-            dp = np.zeros(m)
+            cp = np.zeros(m, dtype=S.dtype)
+            dp = np.zeros(m, dtype=S.dtype)
             cp[0] = c[0] / b[0]
             dp[0] = d[0] / b[0]
             for i in range(1, m):
                 denom = b[i] - a[i] * cp[i - 1]
                 cp[i] = c[i] / denom if i < m - 1 else 0.0
                 dp[i] = (d[i] - a[i] * dp[i - 1]) / denom
-            Si = np.zeros(m)
+            Si = np.zeros(m, dtype=S.dtype)
             Si[m - 1] = dp[m - 1]
             for idx in range(m - 2, -1, -1):
                 Si[idx] = dp[idx] - cp[idx] * Si[idx + 1]
@@ -73,7 +75,7 @@ class spline_interpolation:
 
     # -- index lookup -----------------------------------------------------------------
     def _find_index(self, x_new):
-        x_new = np.asarray(x_new, dtype=np.float64)
+        x_new = np.real(np.asarray(x_new))
         if self.uniform:
             idx = np.floor((x_new - self.x0) * self.dx_inv).astype(np.int64)
         else:
@@ -82,7 +84,7 @@ class spline_interpolation:
         return np.clip(idx, 0, self.n - 2)
 
     def _local(self, x_new):
-        x_new = np.asarray(x_new, dtype=np.float64)
+        x_new = np.asarray(x_new)
         idx = self._find_index(x_new)
         x, y, S = self.x, self.y, self.S
         h = x[idx + 1] - x[idx]

@@ -256,10 +256,17 @@ def _grk4a_step(fun, t0, t1, y0):
     """One GRK4A step (ode_integrators_stiff.py:157-254); all stages at t0 as the reference."""
     g = _G
     dt = t1 - t0
-    h = 1e-40
-    # J = d(dt*f)/dy by complex step (three columns at once)
-    Y = y0[:, None] + 1j * h * np.eye(3)
-    J = np.imag(fun(t0, Y)) / h * dt
+    if np.iscomplexobj(y0) or np.iscomplexobj(fun(t0, y0)):
+        # parameters carry a complex-step perturbation: the Jacobian by central differences
+        # of the (complex) RHS, relative step 1e-7
+        hv = 1e-7 * np.maximum(np.abs(np.real(y0)), 1e-10)
+        J = np.stack([(fun(t0, y0 + hv[j] * np.eye(3)[j]) - fun(t0, y0 - hv[j] * np.eye(3)[j])) / (2 * hv[j])
+                      for j in range(3)], axis=1) * dt
+    else:
+        # J = d(dt*f)/dy by complex step (three columns at once)
+        h = 1e-40
+        Y = y0[:, None] + 1j * h * np.eye(3)
+        J = np.imag(fun(t0, Y)) / h * dt
     A = np.eye(3) - g["gamma"] * J
     lu = _lu3(A)
     b1 = dt * fun(t0, y0)
@@ -286,13 +293,24 @@ def _clip_to_end(tprev, tnext, t1, keep):
     return tnext
 
 
-def solve_pid_grk4a(fun, t0, t1, y0, dt0, rtol, atol, max_steps):
+def solve_pid_grk4a(fun, t0, t1, y0, dt0, rtol, atol, max_steps, steps=None, replay=None):
     """Adaptive GRK4A solve with an integral controller (diffrax ``PIDController``
     defaults: icoeff=1, pcoeff=dcoeff=0, safety 0.9, factor in [0.2, 10],
     RMS norm, error order 3).  Returns y(t1) (``throw=False``: the last accepted
-    state is returned when ``max_steps`` is exhausted)."""
+    state is returned when ``max_steps`` is exhausted).
+
+    ``steps`` (a list) receives the accepted step end times; ``replay`` (such a list)
+    repeats them without error control, which makes the result a smooth function of the
+    parameters (used for derivatives with the step sequence held fixed, as forward-mode
+    AD through the reference's diffrax loop does)."""
+    y = np.array(y0, dtype=np.result_type(np.asarray(y0).dtype, np.float64))
+    if replay is not None:
+        t = t0
+        for tn in replay:
+            y, _ = _grk4a_step(fun, t, tn, y)
+            t = tn
+        return y
     t = t0
-    y = np.array(y0, dtype=np.float64)
     tn = _clip_to_end(t0, t0 + dt0, t1, True)
     for _ in range(max_steps):
         if not (t < t1):
@@ -308,6 +326,8 @@ def solve_pid_grk4a(fun, t0, t1, y0, dt0, rtol, atol, max_steps):
         dt = (tn - t) * factor
         if keep:
             t, y = tn, y1
+            if steps is not None:
+                steps.append(tn)
         tn = _clip_to_end(t, t + dt, t1, keep)
     return y
 
@@ -347,13 +367,18 @@ def _get_adaptive_sampling(a0, a1, N):
     ])
 
 
-def compute_thermal_history(*, a0, a1, N, param, aprimeoa_fn, rtol=1e-3, atol=1e-6):
+def compute_thermal_history(*, a0, a1, N, param, aprimeoa_fn, rtol=1e-3, atol=1e-6, trace=None, replay=None):
     """Interval-by-interval ionisation history (thermodynamics_recfast.py:363-453).
 
     Returns ``y[6, N]`` = (x_H, x_He, T_m, dx_H/da, dx_He/da, dT_m/da) at ``a[1:]``.
+    ``trace`` (a dict) records the branch taken and the accepted steps of every interval;
+    ``replay`` (such a dict) repeats them.
     """
+    if trace is not None:
+        trace["case"], trace["steps"] = [], []
     a = _get_adaptive_sampling(a0, a1, N + 1)
-    y = np.zeros((6, N))
+    cplx = any(np.iscomplexobj(param[k]) for k in ("H0", "Omegab", "Omegam", "OmegaDE", "amnu", "w_DE_0", "w_DE_a"))
+    y = np.zeros((6, N), dtype=complex if cplx else np.float64)
     H = param["H0"] / 100.0
     HO = H * bigH
     mu_H = 1.0 / (1.0 - param["YHe"])
@@ -374,53 +399,64 @@ def compute_thermal_history(*, a0, a1, N, param, aprimeoa_fn, rtol=1e-3, atol=1e
         if i > 0:
             y_prev = y[:, i - 1].copy()
         else:
-            y_prev = np.array([1.0, 1.0, Tcmb * (1.0 + zstart), 0.0, 0.0, -Tcmb * (1.0 + zstart)])
-        if zend > 3500.0:
+            y_prev = np.array([1.0, 1.0, Tcmb * (1.0 + zstart), 0.0, 0.0, -Tcmb * (1.0 + zstart)], dtype=y.dtype)
+        if replay is not None:
+            case = replay["case"][i]
+        else:
+            case = 1 if zend > 3500.0 else (2 if (i > 0 and np.real(y_prev[1]) > 0.99) else
+                                            (3 if (i > 0 and np.real(y_prev[0]) > 0.99) else 4))
+        steps = [] if trace is not None else None
+        rsteps = replay["steps"][i] if replay is not None else None
+        if trace is not None:
+            trace["case"].append(case)
+            trace["steps"].append(steps)
+        if case == 1:
             new = np.array([1.0, 1.0, Tcmb * (1.0 + zend), 0.0, 0.0, -Tcmb * (1.0 + zend)])
-        elif i > 0 and y_prev[1] > 0.99:
-            rhs = (math.exp(1.5 * math.log(CR * Tcmb / (1.0 + zend)) - CB1_He1 / (Tcmb * (1.0 + zend))) / Nnow) * 4.0
-            x_He0 = 0.5 * (math.sqrt((rhs - 1.0) ** 2 + 4.0 * (1.0 + fHe) * rhs) - (rhs - 1.0))
+        elif case == 2:
+            rhs = (np.exp(1.5 * np.log(CR * Tcmb / (1.0 + zend)) - CB1_He1 / (Tcmb * (1.0 + zend))) / Nnow) * 4.0
+            x_He0 = 0.5 * (np.sqrt((rhs - 1.0) ** 2 + 4.0 * (1.0 + fHe) * rhs) - (rhs - 1.0))
             q = -((CB1_He1 - CR * Tcmb**2) / (Tcmb * (1 + zend)))
             dxHeIdz = ((-3 * (-(CB1_He1 / Tcmb) + CR * Tcmb) ** 1.5 * (Nnow + 2 * fHe * Nnow + 4 * q**1.5
-                        - math.sqrt(Nnow**2 + (16 * (-CB1_He1 + CR * Tcmb**2) ** 3) / (Tcmb3 * (1 + zend) ** 3)
+                        - np.sqrt(Nnow**2 + (16 * (-CB1_He1 + CR * Tcmb**2) ** 3) / (Tcmb3 * (1 + zend) ** 3)
                                     + 8 * (1 + 2 * fHe) * Nnow * q**1.5)))
-                       / (Nnow * (1 + zend) ** 2.5 * math.sqrt(Nnow**2 + (16 * (-CB1_He1 + CR * Tcmb**2) ** 3)
+                       / (Nnow * (1 + zend) ** 2.5 * np.sqrt(Nnow**2 + (16 * (-CB1_He1 + CR * Tcmb**2) ** 3)
                                                                 / (Tcmb**3 * (1 + zend) ** 3)
                                                                 + 8 * (1 + 2 * fHe) * Nnow
                                                                 * (-((CB1_He1 - CR * Tcmb**2) / (Tcmb + Tcmb * zend))) ** 1.5)))
             new = np.array([1.0, (x_He0 - 1.0) / fHe, Tcmb * (1.0 + zend), 0.0, dxHeIdz * dzda, -Tcmb * (1.0 + zend)])
-        elif i > 0 and y_prev[0] > 0.99:
-            rhs = math.exp(1.5 * math.log(CR * Tcmb / (1.0 + zend)) - CB1 / (Tcmb * (1.0 + zend))) / Nnow
-            x_H0 = 0.5 * (math.sqrt(rhs**2 + 4.0 * rhs) - rhs)
+        elif case == 3:
+            rhs = np.exp(1.5 * np.log(CR * Tcmb / (1.0 + zend)) - CB1 / (Tcmb * (1.0 + zend))) / Nnow
+            x_H0 = 0.5 * (np.sqrt(rhs**2 + 4.0 * rhs) - rhs)
             q = -((CB1 - CR * Tcmb**2) / (Tcmb * (1 + zend)))
             dxHdz = ((3 * ((2 * q**1.5) / (1 + zend)
                            + ((CB1 - CR * Tcmb**2) * (2 * CB1**2 - 4 * CB1 * CR * Tcmb**2 + Tcmb**2
-                                                      * (2 * CR**2 * Tcmb**2 + Nnow * (1 + zend) ** 2 * math.sqrt(q))))
-                           / (Tcmb**1.5 * (1 + zend) ** 2.5 * math.sqrt((-CB1 + CR * Tcmb**2)
+                                                      * (2 * CR**2 * Tcmb**2 + Nnow * (1 + zend) ** 2 * np.sqrt(q))))
+                           / (Tcmb**1.5 * (1 + zend) ** 2.5 * np.sqrt((-CB1 + CR * Tcmb**2)
                               * (CB1**2 - 2 * CB1 * CR * Tcmb**2 + Tcmb**2 * (CR**2 * Tcmb**2 + Nnow * (1 + zend) ** 2
-                                                                          * math.sqrt(q)))))))
+                                                                          * np.sqrt(q)))))))
                      / (2.0 * Nnow))
-            new = _solve_ionization(fun, astart, aend, y_prev, rtol, atol)
+            new = _solve_ionization(fun, astart, aend, y_prev, rtol, atol, steps=steps, replay=rsteps)
             new[0] = x_H0
             new[3] = dxHdz * dzda
         else:
-            new = _solve_ionization(fun, astart, aend, y_prev, rtol, atol)
+            new = _solve_ionization(fun, astart, aend, y_prev, rtol, atol, steps=steps, replay=rsteps)
         y[:, i] = new
     return y, a[1:]
 
 
-def _solve_ionization(fun, astart, aend, ystart, rtol, atol, max_steps=128):
+def _solve_ionization(fun, astart, aend, ystart, rtol, atol, max_steps=128, steps=None, replay=None):
     """thermodynamics_recfast.py:283-301: state at ``aend`` and its derivative."""
-    y_end = solve_pid_grk4a(fun, astart, aend, ystart[:3], abs(astart * 1e-3), rtol, atol, max_steps)
-    dyda = np.real(fun(aend, y_end))
+    y_end = solve_pid_grk4a(fun, astart, aend, ystart[:3], abs(astart * 1e-3), rtol, atol, max_steps, steps=steps,
+                            replay=replay)
+    dyda = fun(aend, y_end)
     return np.array([y_end[0], y_end[1], y_end[2], dyda[0], dyda[1], dyda[2]])
 
 
-def evaluate_thermo(*, param, num_thermo, aprimeoa_fn, dadtau_fn, dtauda_fn):
+def evaluate_thermo(*, param, num_thermo, aprimeoa_fn, dadtau_fn, dtauda_fn, trace=None, replay=None):
     """Thermal history tables on the Recfast a-grid (thermodynamics_recfast.py:456-492)."""
     param["fHe"] = param["YHe"] / (const_mHe_mH * (1.0 - param["YHe"]))
     y, a = compute_thermal_history(a0=param["amin"], a1=param["amax"], N=num_thermo, param=param,
-                                   aprimeoa_fn=aprimeoa_fn)
+                                   aprimeoa_fn=aprimeoa_fn, trace=trace, replay=replay)
     xeHI = y[0]
     xeHeI = y[1]
     xeHeII = Saha_HeII(a, param)
@@ -429,8 +465,12 @@ def evaluate_thermo(*, param, num_thermo, aprimeoa_fn, dadtau_fn, dtauda_fn):
     Tm = y[2]
     dxeHIda = y[3]
     dxeHeIda = y[4]
-    hc = 1e-30 * a
-    dxHeIIda = np.imag(Saha_HeII(a + 1j * hc, param)) / hc
+    if np.iscomplexobj(param["H0"]) or np.iscomplexobj(param["Omegab"]):
+        hc = 1e-6 * a
+        dxHeIIda = (Saha_HeII(a + hc, param) - Saha_HeII(a - hc, param)) / (2 * hc)
+    else:
+        hc = 1e-30 * a
+        dxHeIIda = np.imag(Saha_HeII(a + 1j * hc, param)) / hc
     dTmda = y[5]
     daTmda = Tm + a * dTmda
     cs2 = const_kB / const_mH / const_c**2 / mu * Tm * (4 - daTmda / Tm) / 3

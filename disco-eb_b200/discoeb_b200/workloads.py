@@ -15,14 +15,14 @@ def cosmo_params(*, h=0.674, omega_b=0.0224, omega_c=0.120, A_s=2.1e-9, n_s=0.96
                  m_nu=0.0, w0=-1.0, wa=0.0, YHe=0.248, cs2_DE=1.0, k_p=0.05):
     """Reference param dict; ``m_nu > 0`` adds one massive species and moves one unit of
     N_eff from the massless to the massive sector (the reference tests' convention)."""
-    massive = m_nu > 0.0
+    massive = bool(np.real(m_nu) > 0.0)
     return {
         "Omegam": (omega_b + omega_c) / h**2,
         "Omegab": omega_b / h**2,
         "H0": 100.0 * h,
         "n_s": n_s,
         "A_s": A_s,
-        "mnu": float(m_nu),
+        "mnu": m_nu,
         "Tcmb": Tcmb,
         "YHe": YHe,
         "Neff": Neff - 1.0 if massive else Neff,

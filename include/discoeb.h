@@ -115,6 +115,22 @@ int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
                     const double* switch_tau, int32_t n_out, const double* tau_out,
                     double* y_full, double* y_out20, int32_t* status, int32_t* nsteps, void* stream);
 
+/* Forward solve plus tangents along n_dir parameter directions, for gradients with respect to
+ * cosmological parameters (replaces jax.jacfwd through diffeqsolve with DirectAdjoint,
+ * perturbations.py:904-925, as used in the reference's gradient notebooks).  The tangent is the
+ * exact derivative of the discrete Rodas5 solution with the accepted step sequence held fixed.
+ *   tangents[n_dir]          device array: d(parameters, tables)/d(theta_d)
+ *   y0_dot [n_dir, n_modes, nvar]   d(initial state)/d(theta_d) at fixed start times
+ *   tau_out_dot [n_dir, n_out]      d(output times)/d(theta_d)
+ *   y_out20 [n_modes, n_out, 20]    output fields (may be NULL)
+ *   y_out20_dot [n_dir, n_modes, n_out, 20]  their derivatives
+ * One warp per (mode, direction); one launch. */
+int32_t discoeb_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, const DiscoebTangent* tangents_dev,
+                    int32_t n_dir, const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes,
+                    const double* tau_start, const double* y0, const double* y0_dot, const double* switch_tau,
+                    int32_t n_out, const double* tau_out, const double* tau_out_dot, double* y_out20,
+                    double* y_out20_dot, int32_t* status, int32_t* nsteps, void* stream);
+
 /* RHS f(tau_i, y_i; k_i) of n_points states (compute_time_derivatives):
  *   y, f [n_points, nvar]; tau, kmodes [n_points]; regime < 0: approximation switches
  *   evaluated from (tau, a) as the reference does, else bitmask 1=RSA 2=UFA 4=TCA. */

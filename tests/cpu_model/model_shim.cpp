@@ -76,6 +76,53 @@ int shim_wsolve(const DiscoebCosmo* P, double tau, const double* y, double k, in
     return ok ? 0 : 1;
 }
 
+// forward + tangent solve: raw state and its tangent at the output times (fixed output times)
+int shim_solve_mode_tangent(const DiscoebCosmo* P, const DiscoebTangent* tn, const DiscoebControl* C, double k,
+                            double t0, const double* y0, const double* yd0, const double* sw, int nout,
+                            const double* tout, double* yout, double* ydout, int* stats, double* tlog, int tlog_cap)
+{
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    std::vector<double> mem(mode_mem_doubles(D)), tmem(tan_mem_doubles(D));
+    ModeMem M = carve(mem.data(), D);
+    TanMem TT = carve_tan(tmem.data(), D);
+    std::memcpy(M.y, y0, sizeof(double) * n);
+    std::memcpy(TT.yd, yd0, sizeof(double) * n);
+    HostTeam tm;
+    auto emit = [&](int j, const double* y, int) {
+        std::memcpy(yout + (size_t)j * n, y, sizeof(double) * n);
+        std::memcpy(ydout + (size_t)j * n, TT.yd, sizeof(double) * n);
+    };
+    SolveResult R = solve_mode(tm, *P, D, *C, k, t0, sw, nout, tout, M, emit, tn, &TT, tlog, tlog_cap);
+    stats[0] = R.status;
+    stats[1] = R.steps;
+    stats[2] = R.accepted;
+    return R.status;
+}
+
+// forward solve replaying a given sequence of step end times (no error control)
+int shim_replay(const DiscoebCosmo* P, double k, double t0, const double* y0, const double* sw, int nsteps,
+                const double* tsteps, double* yend)
+{
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    std::vector<double> mem(mode_mem_doubles(D));
+    ModeMem M = carve(mem.data(), D);
+    std::memcpy(M.y, y0, sizeof(double) * n);
+    HostTeam tm;
+    int hint = P->xe_loga.n_knots / 2;
+    double t = t0;
+    for (int s = 0; s < nsteps; ++s) {
+        const double h = tsteps[s] - t;
+        const int regime = regime_at(*P, t, sw);
+        rodas5_step(tm, *P, D, k, t, h, regime, M, hint);
+        for (int i = 0; i < n; ++i) M.y[i] = M.u[i] + M.K[7 * n + i];
+        t = tsteps[s];
+    }
+    std::memcpy(yend, M.y, sizeof(double) * n);
+    return 0;
+}
+
 int shim_solve_mode(const DiscoebCosmo* P, const DiscoebControl* C, double k, double t0, const double* y0,
                     const double* sw, int nout, const double* tout, double* yout, int* stats)
 {
@@ -85,7 +132,7 @@ int shim_solve_mode(const DiscoebCosmo* P, const DiscoebControl* C, double k, do
     std::memcpy(M.y, y0, sizeof(double) * D.n);
     HostTeam tm;
     const int n = D.n;
-    auto emit = [&](int j, const double* y) { std::memcpy(yout + (size_t)j * n, y, sizeof(double) * n); };
+    auto emit = [&](int j, const double* y, int) { std::memcpy(yout + (size_t)j * n, y, sizeof(double) * n); };
     SolveResult R = solve_mode(tm, *P, D, *C, k, t0, sw, nout, tout, M, emit);
     stats[0] = R.status;
     stats[1] = R.steps;
