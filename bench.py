@@ -3,15 +3,20 @@
 
 Workload (default): flat LCDM + one 0.06 eV neutrino (5 momentum bins, l_max 12/12/17/17,
 143 state variables per mode), 512 log-spaced k-modes in [1e-4, 10] /Mpc, outputs at
-z = 2, 1, 0.5, 0, rtol 1e-5 / atol 1e-8.  One "step" = one complete forward solve of all
-512 modes of one cosmology.  Under torchrun every rank solves its own replica of the
-cosmology (weak scaling, no collective on the data path).
+z = 2, 1, 0.5, 0, rtol 1e-5 / atol 1e-8.  One "step" = one cosmology: P(k) of all 512 modes
+and its Jacobian with respect to theta = (omega_c, omega_b, h, n_s, ln 10^10 A_s, w0, wa,
+m_nu) at the four redshifts (``--mode fwd+grad``, one discoeb_jvp launch: 6 tangent
+directions through the solver, n_s and A_s analytic), or the forward solve alone
+(``--mode forward``, one discoeb_fwd launch).  Under torchrun every rank solves its own
+replica of the cosmology (weak scaling, no collective on the data path).
 
-  value : k-mode solves/s, inputs resident in HBM, CUDA events around each solve
-  e2e   : the same metric through the public API evolve_perturbations (numpy in, numpy out,
-          host prologue + H2D + kernel + D2H inside the timed region)
+  value : k-modes/s (forward + gradient of each mode), inputs resident in HBM, CUDA events
+          around each launch
+  e2e   : the same metric through the public API (gradients.power_spectrum_jacobian or
+          evolve_perturbations: host prologue + H2D + kernel + D2H inside the timed region)
   --impl reference : the oracle's CPU restatement of the reference algorithm (dense LU Rodas5)
-          timed on all host cores on a bounded sample of the same workload.
+          timed on all host cores on a bounded sample of the same workload; for fwd+grad the
+          Jacobian of the sample comes from central differences (1 + 2 x 6 solves per mode).
 """
 from __future__ import annotations
 
@@ -55,6 +60,21 @@ def _sample_modes(w, count):
     return k[idx]
 
 
+def _shifted_backgrounds(w):
+    """Backgrounds at theta +- 1e-4 |theta_i| along the 6 solver directions (central differences)."""
+    from discoeb_b200.background import evolve_background
+    from discoeb_b200.gradients import ODE_DIRECTIONS, theta_to_params
+    out = []
+    for name in ODE_DIRECTIONS:
+        for sgn in (1, -1):
+            th = dict(w["theta"])
+            th[name] += sgn * 1e-4 * max(abs(th[name]), 1e-3)
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore")
+                out.append(evolve_background(param=theta_to_params(th)))
+    return out
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the reference algorithm (oracle port) on all host threads."""
     if rank != 0:
@@ -67,11 +87,15 @@ def run_reference(args, rank, world):
     ks = _sample_modes(w, args.ref_sample)
     threads = os.cpu_count() or 1
 
+    grad = args.mode == "fwd+grad"
+    bgs = [bg] + (_shifted_backgrounds(w) if grad else [])
+
     def one():
         t = time.perf_counter()
-        y, _, st = O.evolve_perturbations(param=bg, aexp_out=w["aexp_out"], kmin=0, kmax=0, num_k=0, rtol=w["rtol"],
-                                          atol=w["atol"], kmodes=ks, mode="reference", de_guard_eps=1e-9,
-                                          max_steps=100000, threads=threads, **L)
+        for b in bgs:
+            O.evolve_perturbations(param=b, aexp_out=w["aexp_out"], kmin=0, kmax=0, num_k=0, rtol=w["rtol"],
+                                   atol=w["atol"], kmodes=ks, mode="reference", de_guard_eps=1e-9,
+                                   max_steps=100000, threads=threads, **L)
         return time.perf_counter() - t
 
     for _ in range(args.warmup):
@@ -80,11 +104,12 @@ def run_reference(args, rank, world):
     ms = 1e3 * statistics.mean(times)
     value = len(ks) / (ms / 1e3)
     sample = (f"{len(ks)} of the {w['num_k']} modes (k evenly spread in log over [{w['kmin']:g}, {w['kmax']:g}]), "
-              f"dense-LU Rodas5 with diffrax controller semantics, {threads} threads")
+              f"dense-LU Rodas5 with diffrax controller semantics, {threads} threads"
+              + (", forward + central-difference Jacobian (13 solves per mode)" if grad else ""))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cosmology, no dataset)",
-            "config": {"workload": args.workload, "mode": "forward", "modes_per_step": len(ks)},
+            "config": {"workload": args.workload, "mode": args.mode, "modes_per_step": len(ks)},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -164,6 +189,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pk_lcdm_mnu_k512_z4")
+    ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward"])
     ap.add_argument("--ref-sample", type=int, default=24)
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -223,7 +249,7 @@ def main():
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)  # > 126 MB L2
 
-    def solve():
+    def forward():
         rc = lib.discoeb_fwd(dc.struct.data_ptr(), ctypes.byref(dc.host), 1, ctypes.byref(ctrl), K, None,
                              d_k.data_ptr(), d_ts.data_ptr(), d_y0.data_ptr(), d_sw.data_ptr(), nout,
                              d_tout.data_ptr(), None, d_out.data_ptr(), d_stat[0].data_ptr(), d_stat[1].data_ptr(),
@@ -231,13 +257,24 @@ def main():
         if rc != 0:
             raise RuntimeError(f"discoeb_fwd returned {rc}")
 
+    grad = args.mode == "fwd+grad"
+    if grad:
+        from discoeb_b200.gradients import JacobianProblem, power_spectrum_jacobian
+        prob = JacobianProblem(w["theta"], aexp_out=aout, kmodes=kmodes, rtol=w["rtol"], atol=w["atol"],
+                               max_steps=100000, device=device, **L)
+        n_dir = len(prob.dirs)
+        solve, stat_of = prob.launch, (lambda: prob.d_stat)
+    else:
+        n_dir = 0
+        solve, stat_of = forward, (lambda: d_stat)
+
     for _ in range(args.warmup):
         solve()
     torch.cuda.synchronize()
-    stat = d_stat.cpu().numpy()
+    stat = stat_of().cpu().numpy()
     if (stat[0] != 0).any():
         raise RuntimeError(f"{int((stat[0] != 0).sum())} modes failed")
-    total_steps = int(stat[1].sum())
+    step_attempts = int(stat[1].sum())  # per mode (every direction of a mode takes the same steps)
 
     def barrier():
         if dist is not None:
@@ -263,15 +300,34 @@ def main():
         ms = float(t.item())
     value = world * K / (ms / 1e3)
 
+    fwd_ms = None
+    if grad:  # the forward solve alone, for comparison (same events and L2 flush)
+        for _ in range(args.warmup):
+            forward()
+        fwd_times = []
+        for i in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            forward()
+            e1.record(stream)
+            e1.synchronize()
+            fwd_times.append(e0.elapsed_time(e1))
+        fwd_ms = statistics.mean(fwd_times)
+
     # ---- end to end through the public API (host arrays in, host arrays out) ----
     e2e_ms = []
     for i in range(0 if args.kernel_only else args.warmup + args.steps):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        y, k, _ = pert.evolve_perturbations(param=dict(bg), aexp_out=aout, kmin=w["kmin"], kmax=w["kmax"],
-                                            num_k=w["num_k"], rtol=w["rtol"], atol=w["atol"], max_steps=100000,
-                                            k_sampling_method="log", **L)
+        if grad:
+            power_spectrum_jacobian(w["theta"], aexp_out=aout, kmin=w["kmin"], kmax=w["kmax"], num_k=w["num_k"],
+                                    rtol=w["rtol"], atol=w["atol"], max_steps=100000, k_sampling_method="log", **L)
+        else:
+            pert.evolve_perturbations(param=dict(bg), aexp_out=aout, kmin=w["kmin"], kmax=w["kmax"],
+                                      num_k=w["num_k"], rtol=w["rtol"], atol=w["atol"], max_steps=100000,
+                                      k_sampling_method="log", **L)
         e1.record(stream)
         e1.synchronize()
         if i >= args.warmup:
@@ -283,11 +339,20 @@ def main():
         e2e = float(t.item())
     h2d = 8 * (2 * K + K * n + 3 * K + nout) + sum(t.numel() * 8 for t in dc.tensors) + ctypes.sizeof(dc.host)
     d2h = 8 * K * nout * 20 + 8 * K
+    if grad:  # + tangent tables, tangent structs, initial-state and output-time tangents; + output tangents
+        h2d += sum(t.numel() * 8 for t in prob._keep) + prob.d_tan.numel() + 8 * n_dir * (K * n + nout)
+        d2h += 8 * n_dir * K * nout * 20
 
     # ---- roofline: FP64 work of the structured Rodas5 step against a measured FP64 peak ----
-    flops_per_step = 850.0 * n + 1650.0  # structured step, counted from stepper.cuh
+    flops_per_step = 850.0 * n + 1650.0  # forward structured step, counted from stepper.cuh
+    # one tangent direction's extra work per step, estimated from the operation mix of tangent_stage
+    # (stepper.cuh): 8 stages x (a dual and a hyper-dual RHS pass ~ 6 real RHS passes of ~10 n + 300
+    # flops, one W solve ~30 n, stage sums ~14 n)
+    tangent_per_step = 8.0 * (6.0 * (10.0 * n + 300.0) + 44.0 * n)
     dense_per_step = (2.0 / 3.0) * n**3 + 16.0 * n**2 + 45.0 * n * n  # reference algorithm: LU + 8 solves + jacfwd
-    achieved = total_steps * flops_per_step / (ms / 1e3) / 1e12
+    work = step_attempts * (flops_per_step + tangent_per_step) * n_dir if grad else step_attempts * flops_per_step
+    dense_work = step_attempts * dense_per_step * (1 + n_dir)
+    achieved = work / (ms / 1e3) / 1e12
     peak = fp64_peak_tflops(torch, device) if rank == 0 and not args.kernel_only else None
 
     cpu = None
@@ -295,31 +360,39 @@ def main():
         from oracle import pyoracle as O
         ks = _sample_modes(w, args.cpu_sample)
         th = os.cpu_count() or 1
+        bgs = [bg] + (_shifted_backgrounds(w) if grad else [])
         t0 = time.perf_counter()
-        O.evolve_perturbations(param=bg, aexp_out=aout, kmin=0, kmax=0, num_k=0, rtol=w["rtol"], atol=w["atol"],
-                               kmodes=ks, mode="reference", de_guard_eps=1e-9, max_steps=100000, threads=th, **L)
+        for b in bgs:
+            O.evolve_perturbations(param=b, aexp_out=aout, kmin=0, kmax=0, num_k=0, rtol=w["rtol"], atol=w["atol"],
+                                   kmodes=ks, mode="reference", de_guard_eps=1e-9, max_steps=100000, threads=th, **L)
         dt = time.perf_counter() - t0
+        how = ", forward + central-difference Jacobian (13 solves per mode)" if grad else ""
         cpu = {"value": len(ks) / dt, "unit": UNIT, "cores": th, "kind": "port",
-               "sample": f"{len(ks)} modes spread over the workload's k range, oracle dense-LU Rodas5, {dt:.1f} s"}
+               "sample": f"{len(ks)} modes spread over the workload's k range, oracle dense-LU Rodas5{how}, "
+                         f"{dt:.1f} s"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cosmology, no dataset)",
-            "config": {"workload": args.workload, "mode": "forward", "num_k": K, "nvar": n, "n_out": nout,
+            "config": {"workload": args.workload, "mode": args.mode, "num_k": K, "nvar": n, "n_out": nout,
+                       "tangent_directions": n_dir, "gradient_of": "P(k) at every output w.r.t. omega_c, omega_b, h, "
+                       "n_s, ln10As, w0, wa, m_nu" if grad else None,
                        "rtol": w["rtol"], "atol": w["atol"], "method": "rodas5-structured",
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "ms_per_cosmology": ms, "step_attempts": total_steps},
+                       "ms_per_cosmology": ms, "step_attempts_per_mode_sum": step_attempts},
             "e2e": {"value": world * K / (e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_cosmology": e2e},
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if peak else None, "traffic": None,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-                         "dense_equivalent_tflops": total_steps * dense_per_step / (ms / 1e3) / 1e12},
+                         "dense_equivalent_tflops": dense_work / (ms / 1e3) / 1e12},
             "clocks": clocks,
         }
+        if fwd_ms is not None:
+            line["forward_only"] = {"value": world * K / (fwd_ms / 1e3), "unit": UNIT, "ms_per_cosmology": fwd_ms}
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)

@@ -20,7 +20,6 @@ analytically.
 from __future__ import annotations
 
 import ctypes
-import math
 
 import numpy as np
 
@@ -66,84 +65,119 @@ def background_tangents(theta, bg, trace, directions, *, aexp_out, tau_start, km
     return out
 
 
-def power_spectrum_jacobian(theta, *, aexp_out=(1.0,), kmin=1e-4, kmax=1.0, num_k=64, lmaxg=12, lmaxgp=12, lmaxr=17,
-                            lmaxnu=17, nqmax=5, rtol=1e-5, atol=1e-8, pcoeff=0.25, icoeff=0.80, dcoeff=0.0,
-                            factormax=20.0, factormin=0.3, max_steps=100000, k_sampling_method="log", idx=4,
-                            num_thermo=256, de_guard_eps=1e-9, device=None, warps_per_block=0, on_failure="raise",
-                            return_stats=False):
+class JacobianProblem:
+    """Everything one discoeb_jvp launch needs for P(k) and dP/dtheta of one cosmology.
+
+    The host prologue (background, its tangents, start times, initial states and their
+    tangents) runs in the constructor and leaves the inputs resident on the device;
+    ``launch`` enqueues the kernel on the current stream and ``result`` reads it back.
+    """
+
+    def __init__(self, theta, *, aexp_out=(1.0,), kmin=1e-4, kmax=1.0, num_k=64, kmodes=None, lmaxg=12, lmaxgp=12,
+                 lmaxr=17, lmaxnu=17, nqmax=5, rtol=1e-5, atol=1e-8, pcoeff=0.25, icoeff=0.80, dcoeff=0.0,
+                 factormax=20.0, factormin=0.3, max_steps=100000, k_sampling_method="log", idx=4, num_thermo=256,
+                 de_guard_eps=1e-9, device=None, warps_per_block=0):
+        import torch
+        if device is None:
+            if not torch.cuda.is_available():
+                raise RuntimeError("discoeb_b200 needs a CUDA device (there is no CPU path)")
+            device = torch.device("cuda", torch.cuda.current_device())
+        self.torch, self.device, self.idx = torch, device, idx
+        self.lib = _abi.lib()
+        L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
+        trace = {}
+        bg = evolve_background(param=theta_to_params(theta), trace=trace, num_thermo=num_thermo)
+        self.bg = bg
+        if kmodes is None:
+            kmodes = k_sampling(bg, kmin, kmax, num_k, k_sampling_method)
+        kmodes = np.ascontiguousarray(kmodes, dtype=np.float64)
+        aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
+        tau_out = bg["tau_of_a_spline"].evaluate(aexp_out)
+        if np.any(np.diff(tau_out) <= 0):
+            raise ValueError("aexp_out must map to strictly increasing output times")
+        K, nout = kmodes.shape[0], tau_out.shape[0]
+        self.kmodes, self.K, self.nout, self.n = kmodes, K, nout, nvar_of(**L)
+        tau_s = determine_starting_time(param=bg, k=kmodes)
+        tau_start = 0.99 * np.minimum(tau_out.min(), tau_s)
+        y0 = adiabatic_ics(tau=tau_start, param=bg, kmode=kmodes, **L)
+        sw = approximation_switch_times(bg, kmodes)
+        self.dirs = ODE_DIRECTIONS
+        tans = background_tangents(theta, bg, trace, self.dirs, aexp_out=aexp_out, tau_start=tau_start,
+                                   kmodes=kmodes, L=L)
+        # longest modes (largest k) first so that the tail of the launch is short
+        order = np.argsort(-kmodes, kind="stable")
+        self.inv = np.empty_like(order)
+        self.inv[order] = np.arange(K)
+        self.dc = DeviceCosmo(bg, de_guard_eps=de_guard_eps, device=device, **L)
+        f64 = dict(dtype=torch.float64, device=device)
+        self._keep = []
+        tstructs = []
+        for d in tans:
+            t = _abi.DiscoebTangent()
+            for f, v in d["scalars"].items():
+                setattr(t, f, v)
+            for short, (yy, SS) in d["tables"].items():
+                ty = torch.from_numpy(yy).to(device)
+                tS = torch.from_numpy(SS).to(device)
+                self._keep += [ty, tS]
+                setattr(t, short + "_y", ty.data_ptr())
+                setattr(t, short + "_S", tS.data_ptr())
+            tstructs.append(t)
+        tan_arr = (_abi.DiscoebTangent * len(tstructs))(*tstructs)
+        self.d_tan = torch.frombuffer(bytearray(bytes(tan_arr)), dtype=torch.uint8).to(device)
+        self.d_k = torch.tensor(kmodes[order], **f64)
+        self.d_ts = torch.tensor(tau_start[order], **f64)
+        self.d_y0 = torch.tensor(y0[order], **f64).contiguous()
+        self.d_y0d = torch.tensor(np.stack([d["y0"][order] for d in tans]), **f64).contiguous()
+        self.d_sw = torch.tensor(sw[order], **f64).contiguous()
+        self.d_tout = torch.tensor(tau_out, **f64)
+        self.d_toutd = torch.tensor(np.stack([d["tau_out"] for d in tans]), **f64).contiguous()
+        self.d_out = torch.empty((K, nout, 20), **f64)
+        self.d_outd = torch.empty((len(self.dirs), K, nout, 20), **f64)
+        self.d_stat = torch.empty((2, K), dtype=torch.int32, device=device)
+        self.ctrl = _abi.DiscoebControl(rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin, int(max_steps),
+                                        _abi.METHOD_RODAS5_STRUCTURED, int(warps_per_block), 0)
+
+    def launch(self):
+        stream = self.torch.cuda.current_stream(self.device).cuda_stream
+        rc = self.lib.discoeb_jvp(self.dc.struct.data_ptr(), ctypes.byref(self.dc.host), self.d_tan.data_ptr(),
+                                  len(self.dirs), ctypes.byref(self.ctrl), self.K, self.d_k.data_ptr(),
+                                  self.d_ts.data_ptr(), self.d_y0.data_ptr(), self.d_y0d.data_ptr(),
+                                  self.d_sw.data_ptr(), self.nout, self.d_tout.data_ptr(), self.d_toutd.data_ptr(),
+                                  self.d_out.data_ptr(), self.d_outd.data_ptr(), self.d_stat[0].data_ptr(),
+                                  self.d_stat[1].data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_jvp failed with code {rc}")
+
+    def result(self, on_failure="raise"):
+        """(P[K, nout], J[8, K, nout], status[K], nsteps[K]) in the caller's k order."""
+        inv, bg, kmodes, idx = self.inv, self.bg, self.kmodes, self.idx
+        y = self.d_out.cpu().numpy()[inv]
+        yd = self.d_outd.cpu().numpy()[:, inv]
+        stat = self.d_stat.cpu().numpy()[:, inv]
+        status, nsteps = stat[0], stat[1]
+        _check_status(status, nsteps, kmodes, on_failure)
+        delta = y[..., idx]
+        P = 2 * np.pi**2 * bg["A_s"] * (kmodes[:, None] / bg["k_p"]) ** (bg["n_s"] - 1) * kmodes[:, None] ** -3 \
+            * delta**2
+        J = np.zeros((len(THETA_NAMES), self.K, self.nout))
+        for di, name in enumerate(self.dirs):
+            J[THETA_NAMES.index(name)] = 2.0 * P * yd[di, ..., idx] / delta
+        J[THETA_NAMES.index("n_s")] = P * np.log(kmodes[:, None] / bg["k_p"])
+        J[THETA_NAMES.index("ln10As")] = P
+        return P, J, status, nsteps
+
+
+def power_spectrum_jacobian(theta, *, on_failure="raise", return_stats=False, **options):
     """P(k, a_out) of field ``idx`` (4: total matter) and its Jacobian with respect to theta.
 
-    theta: dict with keys THETA_NAMES.  Returns (k, P[K, nout], J[8, K, nout]) with the rows
-    of J in THETA_NAMES order.
+    theta: dict with keys THETA_NAMES.  Options as JacobianProblem.  Returns
+    (k, P[K, nout], J[8, K, nout]) with the rows of J in THETA_NAMES order (with
+    ``return_stats`` also the per-mode status and step-attempt counts).
     """
-    import torch
-    if device is None:
-        device = torch.device("cuda", torch.cuda.current_device())
-    L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
-    lib = _abi.lib()
-    trace = {}
-    bg = evolve_background(param=theta_to_params(theta), trace=trace, num_thermo=num_thermo)
-    kmodes = k_sampling(bg, kmin, kmax, num_k, k_sampling_method)
-    aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
-    tau_out = bg["tau_of_a_spline"].evaluate(aexp_out)
-    K, nout, n = kmodes.shape[0], tau_out.shape[0], nvar_of(**L)
-    tau_s = determine_starting_time(param=bg, k=kmodes)
-    tau_start = 0.99 * np.minimum(tau_out.min(), tau_s)
-    y0 = adiabatic_ics(tau=tau_start, param=bg, kmode=kmodes, **L)
-    sw = approximation_switch_times(bg, kmodes)
-    dirs = ODE_DIRECTIONS
-    tans = background_tangents(theta, bg, trace, dirs, aexp_out=aexp_out, tau_start=tau_start, kmodes=kmodes, L=L)
-    order = np.argsort(-kmodes, kind="stable")
-    dc = DeviceCosmo(bg, de_guard_eps=de_guard_eps, device=device, **L)
-    f64 = dict(dtype=torch.float64, device=device)
-    keep = []
-    tstructs = []
-    for d in tans:
-        t = _abi.DiscoebTangent()
-        for f, v in d["scalars"].items():
-            setattr(t, f, v)
-        for short, (yy, SS) in d["tables"].items():
-            ty = torch.from_numpy(yy).to(device)
-            tS = torch.from_numpy(SS).to(device)
-            keep += [ty, tS]
-            setattr(t, short + "_y", ty.data_ptr())
-            setattr(t, short + "_S", tS.data_ptr())
-        tstructs.append(t)
-    tan_arr = (_abi.DiscoebTangent * len(tstructs))(*tstructs)
-    d_tan = torch.frombuffer(bytearray(bytes(tan_arr)), dtype=torch.uint8).to(device)
-    d_k = torch.tensor(kmodes[order], **f64)
-    d_ts = torch.tensor(tau_start[order], **f64)
-    d_y0 = torch.tensor(y0[order], **f64).contiguous()
-    d_y0d = torch.tensor(np.stack([d["y0"][order] for d in tans]), **f64).contiguous()
-    d_sw = torch.tensor(sw[order], **f64).contiguous()
-    d_tout = torch.tensor(tau_out, **f64)
-    d_toutd = torch.tensor(np.stack([d["tau_out"] for d in tans]), **f64).contiguous()
-    d_out = torch.empty((K, nout, 20), **f64)
-    d_outd = torch.empty((len(dirs), K, nout, 20), **f64)
-    d_stat = torch.empty((2, K), dtype=torch.int32, device=device)
-    ctrl = _abi.DiscoebControl(rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin, int(max_steps),
-                               _abi.METHOD_RODAS5_STRUCTURED, int(warps_per_block), 0)
-    stream = torch.cuda.current_stream(device).cuda_stream
-    rc = lib.discoeb_jvp(dc.struct.data_ptr(), ctypes.byref(dc.host), d_tan.data_ptr(), len(dirs), ctypes.byref(ctrl),
-                         K, d_k.data_ptr(), d_ts.data_ptr(), d_y0.data_ptr(), d_y0d.data_ptr(), d_sw.data_ptr(), nout,
-                         d_tout.data_ptr(), d_toutd.data_ptr(), d_out.data_ptr(), d_outd.data_ptr(),
-                         d_stat[0].data_ptr(), d_stat[1].data_ptr(), stream)
-    if rc != 0:
-        raise RuntimeError(f"discoeb_jvp failed with code {rc}")
-    inv = np.empty_like(order)
-    inv[order] = np.arange(K)
-    y = d_out.cpu().numpy()[inv]
-    yd = d_outd.cpu().numpy()[:, inv]
-    stat = d_stat.cpu().numpy()
-    status, nsteps = stat[0][inv], stat[1][inv]
-    _check_status(status, nsteps, kmodes, on_failure)
-    delta = y[..., idx]
-    P = 2 * np.pi**2 * bg["A_s"] * (kmodes[:, None] / bg["k_p"]) ** (bg["n_s"] - 1) * kmodes[:, None] ** -3 * delta**2
-    J = np.zeros((len(THETA_NAMES), K, nout))
-    for di, name in enumerate(dirs):
-        J[THETA_NAMES.index(name)] = 2.0 * P * yd[di, ..., idx] / delta
-    J[THETA_NAMES.index("n_s")] = P * np.log(kmodes[:, None] / bg["k_p"])
-    J[THETA_NAMES.index("ln10As")] = P
+    prob = JacobianProblem(theta, **options)
+    prob.launch()
+    P, J, status, nsteps = prob.result(on_failure)
     if return_stats:
-        return kmodes, P, J, status, nsteps
-    return kmodes, P, J
+        return prob.kmodes, P, J, status, nsteps
+    return prob.kmodes, P, J

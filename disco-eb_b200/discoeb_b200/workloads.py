@@ -41,16 +41,21 @@ A_OUT_4Z = np.array([1.0 / 3.0, 0.5, 2.0 / 3.0, 1.0])
 WORKLOADS = {
     # flat LCDM, massless neutrinos only, P(k, z=0) on 128 log-spaced modes
     "pk_lcdm_massless_k128": dict(
-        cosmo=dict(), kmin=1e-4, kmax=1.0, num_k=128, aexp_out=np.array([1.0]),
+        cosmo=dict(), theta=dict(m_nu=0.0, w0=-1.0, wa=0.0), kmin=1e-4, kmax=1.0, num_k=128, aexp_out=np.array([1.0]),
         lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=3, nqmax=3, rtol=1e-5, atol=1e-8),
     # + one 0.06 eV neutrino (5 momentum bins, l_max 17): 512 modes to k = 10/Mpc, P(k) at z = 0, 0.5, 1, 2
     "pk_lcdm_mnu_k512_z4": dict(
-        cosmo=dict(m_nu=0.06), kmin=1e-4, kmax=10.0, num_k=512, aexp_out=A_OUT_4Z,
+        cosmo=dict(m_nu=0.06), theta=dict(m_nu=0.06, w0=-1.0, wa=0.0), kmin=1e-4, kmax=10.0, num_k=512, aexp_out=A_OUT_4Z,
         lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5, rtol=1e-5, atol=1e-8),
 }
+
+
+# the LCDM point of both workloads as theta = (omega_c, omega_b, h, n_s, ln(10^10 A_s), w0, wa, m_nu)
+_THETA_LCDM = dict(omega_c=0.120, omega_b=0.0224, h=0.674, n_s=0.965, ln10As=float(np.log(2.1e-9 * 1e10)))
 
 
 def workload(name):
     w = dict(WORKLOADS[name])
     w["param"] = cosmo_params(**w.pop("cosmo"))
+    w["theta"] = dict(_THETA_LCDM, **w["theta"])
     return w

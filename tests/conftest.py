@@ -1,4 +1,6 @@
+import ctypes
 import os
+import subprocess
 import sys
 import warnings
 
@@ -44,3 +46,26 @@ def background(name, num_thermo):
             warnings.simplefilter("ignore")
             _BG[key] = evolve_background(param=p, num_thermo=num_thermo)
     return _BG[key]
+
+
+@pytest.fixture(scope="session")
+def shim(tmp_path_factory):
+    """The device model and stepper headers compiled for one host thread (tests/cpu_model)."""
+    from discoeb_b200 import _abi
+    out = str(tmp_path_factory.mktemp("shim") / "model_shim.so")
+    subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    "-I", os.path.join(ROOT, "disco-eb_b200", "csrc"), "-o", out,
+                    os.path.join(ROOT, "tests", "cpu_model", "model_shim.cpp")], check=True)
+    S = ctypes.CDLL(out)
+    dp = ctypes.POINTER(ctypes.c_double)
+    CP = ctypes.POINTER(_abi.DiscoebCosmo)
+    CT = ctypes.POINTER(_abi.DiscoebControl)
+    ip = ctypes.POINTER(ctypes.c_int)
+    S.shim_rhs.argtypes = [CP, ctypes.c_double, dp, ctypes.c_double, ctypes.c_int, dp, dp]
+    S.shim_jacobian.argtypes = [CP, ctypes.c_double, dp, ctypes.c_double, ctypes.c_int, dp, dp]
+    S.shim_wsolve.argtypes = [CP, ctypes.c_double, dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, dp]
+    S.shim_solve_mode.argtypes = [CP, CT, ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_int, dp, dp, ip]
+    S.shim_solve_mode_tangent.argtypes = [CP, ctypes.c_void_p, CT, ctypes.c_double, ctypes.c_double, dp, dp, dp,
+                                          ctypes.c_int, dp, dp, dp, ip, dp, ctypes.c_int]
+    S.shim_replay.argtypes = [CP, ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_int, dp, dp]
+    return S

@@ -5,13 +5,11 @@ checks their algebra (RHS, Jacobian, structured W solve, full adaptive solve) be
 GPU run.
 """
 import ctypes
-import os
-import subprocess
 
 import numpy as np
 import pytest
 
-from conftest import ROOT, background
+from conftest import background
 from discoeb_b200 import _abi
 from oracle import pyoracle as O
 
@@ -22,21 +20,6 @@ L = dict(lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5)
 
 def ptr(a):
     return a.ctypes.data_as(dp)
-
-
-@pytest.fixture(scope="module")
-def shim(tmp_path_factory):
-    out = str(tmp_path_factory.mktemp("shim") / "model_shim.so")
-    subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-I", os.path.join(ROOT, "include"),
-                    "-I", os.path.join(ROOT, "disco-eb_b200", "csrc"), "-o", out,
-                    os.path.join(ROOT, "tests", "cpu_model", "model_shim.cpp")], check=True)
-    S = ctypes.CDLL(out)
-    S.shim_rhs.argtypes = [CP, ctypes.c_double, dp, ctypes.c_double, ctypes.c_int, dp, dp]
-    S.shim_jacobian.argtypes = [CP, ctypes.c_double, dp, ctypes.c_double, ctypes.c_int, dp, dp]
-    S.shim_wsolve.argtypes = [CP, ctypes.c_double, dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, dp]
-    S.shim_solve_mode.argtypes = [CP, ctypes.POINTER(_abi.DiscoebControl), ctypes.c_double, ctypes.c_double, dp, dp,
-                                  ctypes.c_int, dp, dp, ctypes.POINTER(ctypes.c_int)]
-    return S
 
 
 @pytest.fixture(scope="module")
