@@ -194,6 +194,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel-only", action="store_true", help="skip the e2e loop and the FP64 peak (profiling)")
+    ap.add_argument("--num-k", type=int, default=0, help="override the workload's mode count (small profiling case)")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
@@ -219,6 +220,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
     w = workload(args.workload)
+    if args.num_k > 0:
+        w["num_k"] = args.num_k
     bg = _background(w)
     L = {k: w[k] for k in ("lmaxg", "lmaxgp", "lmaxr", "lmaxnu", "nqmax")}
     n = pert.nvar_of(**L)

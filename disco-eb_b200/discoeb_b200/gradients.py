@@ -181,3 +181,32 @@ def power_spectrum_jacobian(theta, *, on_failure="raise", return_stats=False, **
     if return_stats:
         return prob.kmodes, P, J, status, nsteps
     return prob.kmodes, P, J
+
+
+def power_spectrum_function(**options):
+    """A ``torch.autograd.Function`` mapping theta (float64[8], THETA_NAMES order) to
+    P(k, a_out) (float64[K, nout]).
+
+    The forward pass runs ``discoeb_jvp`` (P and its full Jacobian in one launch) and keeps the
+    Jacobian; the backward pass contracts it with the incoming gradient, so ``torch.autograd``
+    (grad, vjp, jacrev, jacfwd through it) sees the exact discrete derivative.  ``options``
+    are those of JacobianProblem (k range, output scale factors, l_max, tolerances).
+    """
+    import torch
+
+    class PowerSpectrum(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, theta):
+            if theta.shape != (len(THETA_NAMES),):
+                raise ValueError(f"theta must have shape ({len(THETA_NAMES)},) in the order {THETA_NAMES}")
+            th = dict(zip(THETA_NAMES, theta.detach().to("cpu", torch.float64).tolist()))
+            _, P, J = power_spectrum_jacobian(th, **options)
+            ctx.save_for_backward(torch.from_numpy(J).to(theta.device))
+            return torch.from_numpy(P).to(theta.device)
+
+        @staticmethod
+        def backward(ctx, grad_P):
+            (J,) = ctx.saved_tensors
+            return torch.einsum("dkn,kn->d", J, grad_P.to(J.dtype))
+
+    return PowerSpectrum

@@ -236,11 +236,13 @@ def _check_status(status, nsteps, kmodes, on_failure):
 
 def solve_modes(*, param, kmodes, tau_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, rtol, atol, pcoeff, icoeff, dcoeff,
                 factormax, factormin, max_steps, return_full, de_guard_eps=1e-9, device=None, warps_per_block=0,
-                on_failure="raise", sort_modes=True, return_stats=False):
+                on_failure="raise", sort_modes=True, return_stats=False, tau_start=None, switch_tau=None):
     """Integrate the given modes of one cosmology to ``tau_out`` on the GPU.
 
     Returns numpy ``y`` (``[K, nout, 20]`` or ``[K, nout, nvar]``); with
-    ``return_stats`` also ``(status, nsteps)``.
+    ``return_stats`` also ``(status, nsteps)``.  ``tau_start`` [K] and ``switch_tau`` [K, 3]
+    override the start times and approximation switch times derived from ``param`` (to hold
+    these numerical choices fixed while parameters move, as forward-mode AD does).
     """
     import torch
     if device is None:
@@ -255,11 +257,14 @@ def solve_modes(*, param, kmodes, tau_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, 
     K = kmodes.shape[0]
     n = nvar_of(lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax)
     nout = tau_out.shape[0]
-    tau_s = determine_starting_time(param=param, k=kmodes)
-    tau_start = 0.99 * np.minimum(tau_out.min(), tau_s)
+    if tau_start is None:
+        tau_s = determine_starting_time(param=param, k=kmodes)
+        tau_start = 0.99 * np.minimum(tau_out.min(), tau_s)
+    tau_start = np.ascontiguousarray(tau_start, dtype=np.float64)
     y0 = adiabatic_ics(tau=tau_start, param=param, kmode=kmodes, lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr,
                        lmaxnu=lmaxnu, nqmax=nqmax)
-    sw = approximation_switch_times(param, kmodes)
+    sw = approximation_switch_times(param, kmodes) if switch_tau is None else \
+        np.ascontiguousarray(switch_tau, dtype=np.float64)
     # longest modes (largest k) first so that the tail of the launch is short
     order = np.argsort(-kmodes, kind="stable") if sort_modes else np.arange(K)
     dc = DeviceCosmo(param, lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax,

@@ -139,4 +139,17 @@ int shim_solve_mode(const DiscoebCosmo* P, const DiscoebControl* C, double k, do
     stats[2] = R.accepted;
     return R.status;
 }
+
+// the 20 output fields and their tangents (output_vars with dual numbers), and the RSA
+// projection fields; tn may be null (state tangent only)
+void shim_output_tangent(const DiscoebCosmo* P, const DiscoebTangent* tn, double k, double tau, const double* y,
+                         const double* yd, double* o, double* od, double* rsa, double* rsad)
+{
+    const Dims D = make_dims(*P);
+    Dual out[20], f[4];
+    output_vars<Dual>(*P, tn, D, k, y, yd, out);
+    for (int q = 0; q < 20; ++q) { o[q] = out[q].v; od[q] = out[q].d; }
+    rsa_projection<Dual>(*P, tn, D, tau, k, y, yd, f);
+    for (int q = 0; q < 4; ++q) { rsa[q] = f[q].v; rsad[q] = f[q].d; }
+}
 }

@@ -108,6 +108,56 @@ def test_tangent_is_derivative_of_discrete_solve(shim, prob, k, case):
         assert abs(ydo[0][v] - fd[v]) <= 1e-5 * abs(fd[v]) + noise, (v, ydo[0][v], fd[v], noise)
 
 
+@pytest.mark.parametrize("case", ["y", "grhom", "Omegam", "Omegab", "OmegaDE", "amnu", "w0", "wa", "H0", "logrhonu",
+                                  "logpnu", "xe", "cs2a"])
+def test_output_and_projection_tangents(shim, prob, case):
+    """output_vars and the RSA projection in dual numbers against central differences."""
+    bg, OP = prob
+    n = OP.n
+    keep = []
+    rng = np.random.default_rng(3)
+    k = 0.3
+    tau = bg["tau_of_a_spline"].evaluate(0.5)
+    ts = 0.99 * OP.start_time(k)
+    ys, _ = OP.solve([k], ts, OP.ics(ts, k), np.array([tau]), rtol=1e-6, atol=1e-9, max_steps=100000)
+    y = ys[0][0]
+    tn = _abi.DiscoebTangent()
+    yd = np.zeros(n)
+    dtab = None
+    if case == "y":
+        yd = y * rng.standard_normal(n)
+    elif case in TABLES:
+        yt = bg[TABLES[case]].y
+        dtab = rng.standard_normal(yt.size) * np.abs(yt)
+        keep.append(dtab)
+        setattr(tn, case + "_y", dtab.ctypes.data)
+    else:
+        setattr(tn, case, 1.0)
+    C = _cosmo(bg, keep)
+    o, od, r, rd = np.zeros(20), np.zeros(20), np.zeros(4), np.zeros(4)
+    shim.shim_output_tangent(ctypes.byref(C), ctypes.byref(tn), k, tau, ptr(y), ptr(yd), ptr(o), ptr(od), ptr(r),
+                             ptr(rd))
+
+    def at(eps):
+        if case == "y":
+            Cx, yy = C, y + eps * yd
+        elif case in TABLES:
+            Cx, yy = _cosmo(bg, keep, table=case, eps=eps, dtab=dtab), y
+        else:
+            Cx, yy = _cosmo(bg, keep, scalar=case, eps=eps), y
+        oo, ood, rr, rrd = np.zeros(20), np.zeros(20), np.zeros(4), np.zeros(4)
+        shim.shim_output_tangent(ctypes.byref(Cx), None, k, tau, ptr(yy.copy()), ptr(np.zeros(n)), ptr(oo),
+                                 ptr(ood), ptr(rr), ptr(rrd))
+        return np.concatenate([oo, rr])
+
+    eps = 1e-6 if case == "y" or case in TABLES else 1e-6 * (abs(getattr(C, case)) or 1.0)
+    fd = (at(eps) - at(-eps)) / (2 * eps)
+    got = np.concatenate([od, rd])
+    val = np.concatenate([o, r])
+    tol = 1e-6 * np.abs(fd) + 1e-12 * np.abs(val) / eps  # truncation + round-off
+    assert np.all(np.abs(got - fd) <= tol + 1e-12 * np.abs(fd).max()), np.abs(got - fd) / (np.abs(fd) + 1e-300)
+
+
 def _fd_background(theta, name, trace, eps):
     side = []
     for sgn in (1, -1):
