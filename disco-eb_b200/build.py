@@ -33,7 +33,7 @@ def build(force: bool = False, verbose: bool = False):
     if not force and up_to_date():
         return OUT
     cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-o", OUT, *sources(), "-lcudart"]
+           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-o", OUT, *sources(), "-lcudart", "-lcufft", "-lcublas"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

@@ -1,0 +1,635 @@
+// CMB source functions and the line-of-sight integral on sm_100a (include/discoeb.h).
+//
+// discoeb_sources: one warp per (mode, output time).  The warp re-evaluates the right-hand
+//   side at the stored (RSA-projected) state, as compute_time_derivatives does
+//   (perturbations.py:1339-1406), keeps y' in shared memory, and its leader assembles the
+//   massive-neutrino moments, the Einstein-equation metric terms, the polarisation terms and
+//   the Sachs-Wolfe, Doppler and polarisation sources of cmb.py:165-633 from them and from the
+//   per-time background table.  y' never goes to HBM.  A second kernel (one thread per mode)
+//   differentiates eta + alpha' along tau with a natural cubic spline (the ISW term) and sums S.
+// discoeb_los: compute_theta_ell (cmb.py:680-835): optional spline resampling to a dense
+//   log-k grid, spline resampling of every row onto the FFTLog log-chi grid with the bias
+//   factor, a batched real-to-complex FFT in place (cuFFT), the coefficient table
+//   M_l(p_n) = 2^(p-1) sqrt(pi) Gamma((1+l+p)/2) / Gamma((2+l-p)/2), and the contraction over
+//   the frequencies as one FP64 GEMM on interleaved (re, im) pairs (cuBLAS): the complex sum
+//   sum_n w_n Re(c_n k^-(p_n+1) M_l(p_n)) becomes a real dot product of length 2 n_freq.
+// discoeb_cell: compute_Cell (cmb.py:838-873), trapezoid in ln k, one thread per l.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <cstdint>
+#include <mutex>
+
+#include "discoeb.h"
+#include "stepper.cuh"
+
+using namespace dscb;
+
+namespace {
+
+constexpr double kBias = -1.1;   // FFTLog bias (cmb.py:761)
+constexpr double kPad = 2.0;     // padding of the log-chi range (cmb.py:738)
+
+// ------------------------------------------------------------------------------------------
+// sources
+
+__global__ void __launch_bounds__(128) sources_kernel(const DiscoebCosmo* __restrict__ cosmo, int n_modes,
+                                                      const double* __restrict__ kmodes, int n_tau,
+                                                      const double* __restrict__ tau, const double* __restrict__ bt,
+                                                      const double* __restrict__ y_full, double* fields)
+{
+    extern __shared__ double smem[];
+    const int wib = threadIdx.x >> 5;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long n_points = (long long)n_modes * n_tau;
+    if (warp >= n_points) return;
+    const WarpTeam tm{(int)(threadIdx.x & 31)};
+    const DiscoebCosmo& P = *cosmo;
+    const Dims D = make_dims(P);
+    const int n = D.n;
+    const int im = (int)(warp / n_tau), j = (int)(warp - (long long)im * n_tau);
+    const double k = kmodes[im], t = tau[j];
+    const double* y = y_full + (size_t)warp * n;
+    double* yp = smem + (size_t)wib * n;
+    Bg<double> b;
+    bg_eval(P, y[0], t, k, -1, b);
+    rhs_team(tm, P, D, b, k, t, y, yp, (double*)nullptr);
+    tm.sync();
+    if (!tm.leader()) return;
+
+    const double a = bt[DISCOEB_BG_A * n_tau + j], aH = bt[DISCOEB_BG_APRIMEOA * n_tau + j];
+    const double rhonu = bt[DISCOEB_BG_RHONU * n_tau + j], rho_Q = bt[DISCOEB_BG_RHO_Q * n_tau + j];
+    const double w_Q = bt[DISCOEB_BG_W_Q * n_tau + j];
+    const double opac = bt[DISCOEB_BG_OPAC * n_tau + j], opacprime = bt[DISCOEB_BG_OPACPRIME * n_tau + j];
+    const double gvis = bt[DISCOEB_BG_GVIS * n_tau + j], gvisprime = bt[DISCOEB_BG_GVISPRIME * n_tau + j];
+    const double gvispprime = bt[DISCOEB_BG_GVISPPRIME * n_tau + j];
+    // massive neutrinos (nu_perturb, nu_perturb_prime: perturbations.py:29-85; the derivative
+    // of the speed is written as the reference writes it)
+    double drhonu = 0.0, dpnu = 0.0, fnu = 0.0, shearnu = 0.0, rnp = 0.0, snp = 0.0;
+    const int nq = D.nq, i0 = D.iq0, i1 = i0 + nq, i2 = i1 + nq;
+    for (int q = 0; q < nq; ++q) {
+        const double aq = a * P.amnu / P.q[q];
+        const double v = 1.0 / sqrt(1.0 + aq * aq);
+        const double vp = -0.5 * aq * aH * v * v * v;
+        const double w = P.wq[q];
+        drhonu += w * y[i0 + q] / v;
+        dpnu += w * y[i0 + q] * v;
+        fnu += w * y[i1 + q];
+        shearnu += w * y[i2 + q] * v;
+        rnp += w * (yp[i0 + q] / v - y[i0 + q] / (v * v) * vp);
+        snp += w * (yp[i2 + q] * v + y[i2 + q] * vp);
+    }
+    dpnu /= 3.0;
+    shearnu *= 2.0 / 3.0;
+    snp *= 2.0 / 3.0;
+    // metric (cmb.py:241-338)
+    const int ig = 7, igp = D.idxgp, ir = D.idxr;
+    const double eta = y[2], deltac = y[3], thetac = y[4], deltab = y[5], thetab = y[6];
+    const double deltag = y[ig], thetag = y[ig + 1], shearg = 0.5 * y[ig + 2];
+    const double deltar = y[ir], thetar = y[ir + 1], shearr = 0.5 * y[ir + 2];
+    const double deltaq = y[n - 2], thetaq = y[n - 1];
+    const double thetabprime = yp[6], thetagprime = yp[ig + 1], sheargprime = 0.5 * yp[ig + 2];
+    const double shearrprime = 0.5 * yp[ir + 2];
+    const double a2 = a * a, k2 = k * k;
+    const double Omegac = P.Omegam - P.Omegab;
+    const double rpt = (1.0 + w_Q) * rho_Q * P.grhom * P.OmegaDE * thetaq * a2;
+    const double grhoprime =
+        (-P.grhom * P.Omegam / a - 2.0 * (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / a2 +
+         P.grhom * P.OmegaDE * (-3.0 * (1.0 + P.w0 + (1.0 - a) * P.wa) * rho_Q * a2 + 2.0 * rho_Q * a2)) * aH +
+        P.grhor * P.Nmnu * rnp / a2;
+    const double aHprime = grhoprime / (6.0 * aH);
+    const double dgrho = P.grhom * (Omegac * deltac + P.Omegab * deltab) / a +
+                         (P.grhog * deltag + P.grhor * (P.Neff * deltar + P.Nmnu * drhonu)) / a2 +
+                         P.grhom * P.OmegaDE * deltaq * rho_Q * a2;
+    const double dgtheta = P.grhom * (Omegac * thetac + P.Omegab * thetab) / a +
+                           4.0 / 3.0 * (P.grhog * thetag + P.Neff * P.grhor * thetar) / a2 +
+                           P.Nmnu * P.grhor * k * fnu / a2 + rpt;
+    const double dgshear = 4.0 / 3.0 * (P.grhog * shearg + P.Neff * P.grhor * shearr) / a2 +
+                           P.Nmnu * P.grhor * shearnu / a2;
+    const double dgshearprime = 4.0 / 3.0 * (P.grhog * sheargprime + P.Neff * P.grhor * shearrprime) / a2 +
+                                P.Nmnu * P.grhor * snp / a2 - 2.0 * aH * dgshear;
+    const double hprime = (2.0 * k2 * eta + dgrho) / aH;
+    const double etaprime = 0.5 * dgtheta / k2;
+    const double alpha = (hprime + 6.0 * etaprime) / 2.0 / k2;
+    const double alphaprime = -3.0 * dgshear / (2.0 * k2) + eta - 2.0 * aH * alpha;
+    const double alphapprime = -3.0 * dgshearprime / (2.0 * k2) + etaprime - 2.0 * (aHprime * alpha + aH * alphaprime);
+    // polarisation (cmb.py:341-389)
+    const double couplprime = 8.0 * (thetagprime + k2 * alphaprime) / 15.0 -
+                              k * 0.6 * (yp[ig + 3] + yp[igp + 1] + yp[igp + 3]);
+    const double pol = y[ig + 2] + y[igp] + y[igp + 2];
+    const double polp = yp[ig + 2] + yp[igp] + yp[igp + 2];
+    const double polpp = couplprime - 0.3 * (opacprime * pol + opac * polp);
+    // sources (cmb.py:456-582); S1 needs d/dtau along the mode, see isw_kernel
+    const double S2 = gvis * (0.25 * deltag + 2.0 * alphaprime + pol / 16.0 + (thetabprime + 3.0 / 16.0 * polpp) / k2);
+    const double S3 = gvisprime * (alpha + (thetab + 3.0 / 8.0 * polp) / k2);
+    const double S4 = gvispprime * 3.0 / 16.0 * pol / k2;
+    const size_t stride = (size_t)n_points, o = (size_t)warp;
+    fields[DISCOEB_SRC_S2 * stride + o] = S2;
+    fields[DISCOEB_SRC_S3 * stride + o] = S3;
+    fields[DISCOEB_SRC_S4 * stride + o] = S4;
+    fields[DISCOEB_SRC_POTENTIAL * stride + o] = eta + alphaprime;
+    fields[DISCOEB_SRC_ALPHA * stride + o] = alpha;
+    fields[DISCOEB_SRC_ALPHAPRIME * stride + o] = alphaprime;
+    fields[DISCOEB_SRC_ALPHAPPRIME * stride + o] = alphapprime;
+    fields[DISCOEB_SRC_HPRIME * stride + o] = hprime;
+    fields[DISCOEB_SRC_ETAPRIME * stride + o] = etaprime;
+    fields[DISCOEB_SRC_APRIMEOAPRIME * stride + o] = aHprime;
+    fields[DISCOEB_SRC_POL * stride + o] = pol;
+    fields[DISCOEB_SRC_POLPRIME * stride + o] = polp;
+    fields[DISCOEB_SRC_POLPPRIME * stride + o] = polpp;
+    fields[DISCOEB_SRC_DRHONU * stride + o] = drhonu;
+    fields[DISCOEB_SRC_DPNU * stride + o] = dpnu;
+    fields[DISCOEB_SRC_FNU * stride + o] = fnu;
+    fields[DISCOEB_SRC_SHEARNU * stride + o] = shearnu;
+    fields[DISCOEB_SRC_RHONUPRIME * stride + o] = rnp;
+    fields[DISCOEB_SRC_SHEARNUPRIME * stride + o] = snp;
+    fields[DISCOEB_SRC_THETABPRIME * stride + o] = thetabprime;
+}
+
+// Natural cubic spline second derivatives through (x[i], y[i*ys]) for i < n (the Thomas
+// recurrence of spline_interpolation.py:19-75), written to S[i*ys]; cp is scratch of n
+// doubles with stride cs.
+__device__ void spline_second(int n, const double* x, int xs, const double* y, long long ys, double* S, double* cp,
+                              long long cs)
+{
+    S[0] = 0.0;
+    S[(long long)(n - 1) * ys] = 0.0;
+    const int m = n - 2;
+    if (m <= 0) return;
+    auto X = [&](int i) { return x[(long long)i * xs]; };
+    auto Y = [&](int i) { return y[(long long)i * ys]; };
+    // forward sweep: cp in cp[], dp in S[1..]
+    double dprev = 0.0, cprev = 0.0;
+    for (int i = 0; i < m; ++i) {
+        const double h0 = X(i + 1) - X(i), h1 = X(i + 2) - X(i + 1);
+        const double a = h0, bb = 2.0 * (h0 + h1), c = h1;
+        const double d = 6.0 * ((Y(i + 2) - Y(i + 1)) / h1 - (Y(i + 1) - Y(i)) / h0);
+        double cc, dd;
+        if (i == 0) {
+            cc = c / bb;
+            dd = d / bb;
+        } else {
+            const double den = bb - a * cprev;
+            cc = (i < m - 1) ? c / den : 0.0;
+            dd = (d - a * dprev) / den;
+        }
+        cp[(long long)i * cs] = cc;
+        S[(long long)(i + 1) * ys] = dd;
+        cprev = cc;
+        dprev = dd;
+    }
+    for (int i = m - 2; i >= 0; --i)
+        S[(long long)(i + 1) * ys] = S[(long long)(i + 1) * ys] - cp[(long long)i * cs] * S[(long long)(i + 2) * ys];
+}
+
+// interval index of the reference: count(x < xn) - 1, clipped to [0, n-2]
+__device__ int spline_interval(const double* x, int xs, int n, double xn)
+{
+    int lo = 0, hi = n;  // first index with x >= xn
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (x[(long long)mid * xs] < xn) lo = mid + 1;
+        else hi = mid;
+    }
+    int i = lo - 1;
+    if (i < 0) i = 0;
+    if (i > n - 2) i = n - 2;
+    return i;
+}
+
+__device__ double spline_value(double x0, double x1, double y0, double y1, double S0, double S1, double xn)
+{
+    const double h = x1 - x0, t = (xn - x0) / h, A = 1.0 - t, B = t;
+    return A * y0 + B * y1 + ((A * A * A - A) * S0 + (B * B * B - B) * S1) * (h * h) / 6.0;
+}
+
+__device__ double spline_slope(double x0, double x1, double y0, double y1, double S0, double S1, double xn)
+{
+    const double h = x1 - x0, d = xn - x0;
+    const double b = (y1 - y0) / h - h * (S1 + 2.0 * S0) / 6.0, c = S0 / 2.0, dd = (S1 - S0) / (6.0 * h);
+    return b + 2.0 * c * d + 3.0 * dd * d * d;
+}
+
+// S1 = exp(-optical depth) d(eta + alpha')/dtau with a natural spline along tau per mode
+// (compute_source_term_isw, cmb.py:392-453), S = S1 + S2 + S3 + S4.  One thread per mode.
+__global__ void isw_kernel(int n_modes, int n_tau, const double* __restrict__ tau, const double* __restrict__ bt,
+                           double* fields, double* scratch)
+{
+    const int im = blockIdx.x * blockDim.x + threadIdx.x;
+    if (im >= n_modes) return;
+    const size_t stride = (size_t)n_modes * n_tau, row = (size_t)im * n_tau;
+    const double* pot = fields + DISCOEB_SRC_POTENTIAL * stride + row;
+    double* S1 = fields + DISCOEB_SRC_S1 * stride + row;  // holds the second derivatives first
+    double* cp = scratch + row;
+    spline_second(n_tau, tau, 1, pot, 1, S1, cp, 1);
+    for (int j = 0; j < n_tau; ++j) {
+        const int i = spline_interval(tau, 1, n_tau, tau[j]);
+        cp[j] = spline_slope(tau[i], tau[i + 1], pot[i], pot[i + 1], S1[i], S1[i + 1], tau[j]);
+    }
+    double* S = fields + DISCOEB_SRC_S * stride + row;
+    const double* S2 = fields + DISCOEB_SRC_S2 * stride + row;
+    const double* S3 = fields + DISCOEB_SRC_S3 * stride + row;
+    const double* S4 = fields + DISCOEB_SRC_S4 * stride + row;
+    for (int j = 0; j < n_tau; ++j) {
+        const double s1 = exp(-bt[DISCOEB_BG_OPTICAL_DEPTH * n_tau + j]) * cp[j];
+        S1[j] = s1;
+        S[j] = s1 + S2[j] + S3[j] + S4[j];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// line of sight
+
+// lo = ln chi_min - 2, dl = (ln chi_max + 2 - lo) / n_fft of compute_theta_ell (cmb.py:730-745)
+__global__ void geom_kernel(int n_tau, const double* __restrict__ tau, double tau0, int n_fft, double* g)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double chi_min = fmax(tau0 - tau[n_tau - 1], 1.0), chi_max = tau0 - tau[0];
+    const double lo = log(chi_min) - kPad, hi = log(chi_max) + kPad;
+    g[0] = lo;
+    g[1] = (hi - lo) / n_fft;
+}
+
+// spline second derivatives along ln k for every tau column (one thread per column)
+__global__ void k_spline_log_kernel(int n_modes, const double* __restrict__ lk, int n_tau, const double* S, double* S2k,
+                                    double* cp)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_tau) return;
+    spline_second(n_modes, lk, 1, S + j, n_tau, S2k + j, cp + j, n_tau);
+}
+
+__global__ void log_kernel(int n, const double* __restrict__ x, double* lx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) lx[i] = log(x[i]);
+}
+
+// S on the dense log-k grid: Sd[kd, j]; also the dense k values
+__global__ void k_dense_kernel(int n_modes, const double* __restrict__ lk, int n_tau, const double* __restrict__ S,
+                               const double* __restrict__ S2k, int n_dense, double* Sd, double* kd)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_dense * n_tau) return;
+    const int id = (int)(t / n_tau), j = (int)(t - (long long)id * n_tau);
+    const double lk0 = lk[0], lk1 = lk[n_modes - 1];
+    const double x = (id == n_dense - 1) ? lk1 : lk0 + id * ((lk1 - lk0) / (n_dense - 1));
+    const int i = spline_interval(lk, 1, n_modes, x);
+    const size_t r0 = (size_t)i * n_tau + j, r1 = r0 + n_tau;
+    Sd[t] = spline_value(lk[i], lk[i + 1], S[r0], S[r1], S2k[r0], S2k[r1], x);
+    if (j == 0) kd[id] = exp(x);
+}
+
+// per-row spline second derivatives along ln chi (chi = tau0 - tau, increasing), one thread per row
+__global__ void chi_spline_kernel(int n_rows, int n_tau, const double* __restrict__ lchi, const double* Srow,
+                                  double* S2c, double* cp)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    // row values in chi order: S[r, n_tau - 1 - m]
+    const double* y = Srow + (size_t)r * n_tau + (n_tau - 1);
+    spline_second(n_tau, lchi, 1, y, -1, S2c + (size_t)r * n_tau + (n_tau - 1), cp + (size_t)r * n_tau, 1);
+}
+
+// ln chi of the knots, chi = tau0 - tau in increasing order (cmb.py:724-752)
+__global__ void lchi_kernel(int n_tau, const double* __restrict__ tau, double tau0, double* lchi)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_tau) lchi[t] = log(fmax(tau0 - tau[n_tau - 1 - t], 1e-10));
+}
+
+// per FFTLog point: interval index among the knots, abscissa ln chi_m, and chi_m^-bias
+__global__ void fgrid_kernel(int n_tau, const double* __restrict__ lchi, int n_fft, const double* __restrict__ g,
+                             int* fidx, double* fx, double* fbias)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_fft) return;
+    const double cf = exp(g[0] + t * g[1]);
+    const double x = log(cf);
+    fidx[t] = spline_interval(lchi, 1, n_tau, x);
+    fx[t] = x;
+    fbias[t] = pow(cf, -kBias);
+}
+
+// biased source on the FFTLog grid into the in-place FFT buffer (row pitch `pitch` doubles)
+__global__ void chi_eval_kernel(int n_rows, int n_tau, const double* __restrict__ lchi, const double* __restrict__ Srow,
+                                const double* __restrict__ S2c, int n_fft, const int* __restrict__ fidx,
+                                const double* __restrict__ fx, const double* __restrict__ fbias, long long pitch,
+                                double* F)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_rows * n_fft) return;
+    const int r = (int)(t / n_fft), m = (int)(t - (long long)r * n_fft);
+    const int i = fidx[m];
+    const size_t base = (size_t)r * n_tau + (n_tau - 1);
+    const double y0 = Srow[base - i], y1 = Srow[base - i - 1];
+    const double s0 = S2c[base - i], s1 = S2c[base - i - 1];
+    F[(size_t)r * pitch + m] = spline_value(lchi[i], lchi[i + 1], y0, y1, s0, s1, fx[m]) * fbias[m];
+}
+
+// c_n k^-(p_n+1) with the rfft normalisation and the interval phase, times the weight of the
+// real reconstruction (1 for n = 0 and the Nyquist term, 2 otherwise), in place
+__global__ void ck_kernel(int n_rows, const double* __restrict__ krow, int n_fft, int n_freq,
+                          const double* __restrict__ g, long long pitch, double* F)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_rows * n_freq) return;
+    const double lo = g[0], dl = g[1];
+    const int r = (int)(t / n_freq), q = (int)(t - (long long)r * n_freq);
+    const double eta = 2.0 * M_PI * q / (n_fft * dl);
+    const double lk = log(krow[r]);
+    double w = 2.0;
+    if (q == 0 || ((n_fft % 2 == 0) && q == n_freq - 1)) w = 1.0;
+    const double mag = w * exp(-(kBias + 1.0) * lk) / n_fft;
+    double sn, cs;
+    sincos(-eta * (lo + lk), &sn, &cs);
+    double* c = F + (size_t)r * pitch + 2 * q;
+    const double re = c[0], im = c[1];
+    c[0] = mag * (re * cs - im * sn);
+    c[1] = mag * (re * sn + im * cs);
+}
+
+struct Cx {
+    double re, im;
+};
+__device__ Cx cx(double r, double i) { return Cx{r, i}; }
+__device__ Cx operator+(Cx a, Cx b) { return cx(a.re + b.re, a.im + b.im); }
+__device__ Cx operator-(Cx a, Cx b) { return cx(a.re - b.re, a.im - b.im); }
+__device__ Cx operator*(Cx a, Cx b) { return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+__device__ Cx cx_log(Cx z) { return cx(log(hypot(z.re, z.im)), atan2(z.im, z.re)); }
+
+// log Gamma(z) for Re z > 0.5: Lanczos g = 7 with 9 terms (Lanczos, SIAM J. Numer. Anal. B 1
+// (1964) 86; the coefficient set of util.py:26-36)
+__device__ Cx lngamma_lanczos(Cx z)
+{
+    const double c[9] = {0.99999999999980993227684700473478, 676.520368121885098567009190444019,
+                         -1259.13921672240287047156078755283, 771.3234287776530788486528258894,
+                         -176.61502916214059906584551354, 12.507343278686904814458936853,
+                         -0.13857109526572011689554707, 9.984369578019570859563e-6, 1.50563273514931155834e-7};
+    z = cx(z.re - 1.0, z.im);
+    Cx A = cx(c[0], 0.0);
+    for (int j = 1; j < 9; ++j) {
+        const double re = z.re + j, im = z.im;
+        const double s = c[j] / (re * re + im * im);
+        A = A + cx(s * re, -s * im);
+    }
+    const Cx zh = cx(z.re + 0.5, z.im), zg = cx(z.re + 7.5, z.im);
+    return zh * cx_log(zg) - zg + cx(0.9189385332046727418, 0.0) + cx_log(A);
+}
+
+// log sin(pi z), stable for large |Im z| (sin(pi z) = (e^{i pi z} - e^{-i pi z}) / 2i)
+__device__ Cx log_sin_pi(Cx z)
+{
+    const double x = M_PI * z.re, y = M_PI * z.im;
+    if (fabs(y) < 20.0) {
+        double sx, cxv;
+        sincos(x, &sx, &cxv);
+        return cx_log(cx(sx * cosh(y), cxv * sinh(y)));
+    }
+    // |y| large: sin(pi z) = e^{|y|} e^{-i s x} (1 - e^{-2|y|} e^{2 i s x}) / (2 i s), s = sign(y)
+    const double s = y > 0 ? 1.0 : -1.0, ay = fabs(y);
+    double sn, cs;
+    sincos(2.0 * s * x, &sn, &cs);
+    const double e = exp(-2.0 * ay);
+    const Cx corr = cx_log(cx(1.0 - e * cs, -e * sn));
+    // log(1 / (2 i s)) = -log 2 - i s pi/2
+    return cx(ay - M_LN2, -s * x - s * M_PI_2) + corr;
+}
+
+__device__ Cx lngamma_c(Cx z)
+{
+    if (z.re <= 0.5) {  // reflection
+        const Cx l = lngamma_lanczos(cx(1.0 - z.re, -z.im));
+        const Cx ls = log_sin_pi(z);
+        return cx(1.14472988584940017414342735135, 0.0) - ls - l;
+    }
+    return lngamma_lanczos(z);
+}
+
+// B[l, 2q] = Re M_l(p_q), B[l, 2q + 1] = -Im M_l(p_q) (cmb.py:636-677)
+__global__ void mcoef_kernel(int n_ell, int n_freq, int n_fft, const double* __restrict__ g, double* B)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_ell * n_freq) return;
+    const double dl = g[1];
+    const int l = (int)(t / n_freq), q = (int)(t - (long long)l * n_freq);
+    const double eta = 2.0 * M_PI * q / (n_fft * dl);
+    const Cx p = cx(kBias, eta);
+    const Cx a1 = cx((1.0 + l + p.re) / 2.0, p.im / 2.0), a2 = cx((2.0 + l - p.re) / 2.0, -p.im / 2.0);
+    const Cx lc = cx((p.re - 1.0) * M_LN2 + 0.5 * log(M_PI), p.im * M_LN2) + lngamma_c(a1) - lngamma_c(a2);
+    const double mag = exp(lc.re);
+    double sn, cs;
+    sincos(lc.im, &sn, &cs);
+    double* b = B + (size_t)l * (2 * (size_t)n_freq) + 2 * q;
+    b[0] = mag * cs;
+    b[1] = -mag * sn;
+}
+
+__global__ void cell_kernel(int n_modes, const double* __restrict__ kmodes, int n_ell, const double* __restrict__ theta,
+                            double n_s, double k_p, double* cell)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n_ell) return;
+    double acc = 0.0, fprev = 0.0, lkprev = 0.0;
+    for (int i = 0; i < n_modes; ++i) {
+        const double k = kmodes[i], th = theta[(size_t)i * n_ell + l];
+        const double f = pow(k / k_p, n_s - 1.0) * th * th, lk = log(k);
+        if (i > 0) acc += 0.5 * (f + fprev) * (lk - lkprev);
+        fprev = f;
+        lkprev = lk;
+    }
+    cell[l] = acc;
+}
+
+// ------------------------------------------------------------------------------------------
+// workspace layout of discoeb_los (byte offsets, 256-byte aligned)
+
+struct LosLayout {
+    size_t sd, s2k, lk, cpk, kd, s2c, cpc, lchi, fidx, fx, fbias, geom, fft, B, cufft, cublas, total;
+    long long pitch;
+    int n_rows, n_freq;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+constexpr size_t kCublasWorkspace = 32u << 20;
+
+LosLayout los_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n_dense, size_t cufft_bytes)
+{
+    LosLayout L;
+    L.n_rows = n_dense > 0 ? n_dense : n_modes;
+    L.n_freq = n_fft / 2 + 1;
+    L.pitch = 2LL * L.n_freq;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { const size_t at = o; o = align256(o + bytes); return at; };
+    L.sd = take(n_dense > 0 ? sizeof(double) * (size_t)n_dense * n_tau : 0);
+    L.s2k = take(n_dense > 0 ? sizeof(double) * (size_t)n_modes * n_tau : 0);
+    L.lk = take(sizeof(double) * (size_t)n_modes);
+    L.cpk = take(n_dense > 0 ? sizeof(double) * (size_t)n_modes * n_tau : 0);
+    L.kd = take(sizeof(double) * (size_t)L.n_rows);
+    L.s2c = take(sizeof(double) * (size_t)L.n_rows * n_tau);
+    L.cpc = take(sizeof(double) * (size_t)L.n_rows * n_tau);
+    L.lchi = take(sizeof(double) * (size_t)n_tau);
+    L.fidx = take(sizeof(int) * (size_t)n_fft);
+    L.fx = take(sizeof(double) * (size_t)n_fft);
+    L.fbias = take(sizeof(double) * (size_t)n_fft);
+    L.geom = take(sizeof(double) * 2);
+    L.fft = take(sizeof(double) * (size_t)L.n_rows * L.pitch);
+    L.B = take(sizeof(double) * (size_t)(ellmax + 1) * L.pitch);
+    L.cufft = take(cufft_bytes);
+    L.cublas = take(kCublasWorkspace);
+    L.total = o;
+    return L;
+}
+
+int make_fft_plan(cufftHandle* plan, int n_fft, int n_rows, long long pitch, size_t* work)
+{
+    if (cufftCreate(plan) != CUFFT_SUCCESS) return DISCOEB_ECUDA;
+    cufftSetAutoAllocation(*plan, 0);
+    long long nn[1] = {n_fft};
+    long long inembed[1] = {pitch}, onembed[1] = {pitch / 2};
+    size_t ws = 0;
+    if (cufftMakePlanMany64(*plan, 1, nn, inembed, 1, pitch, onembed, 1, pitch / 2, CUFFT_D2Z, n_rows, &ws) !=
+        CUFFT_SUCCESS) {
+        cufftDestroy(*plan);
+        return DISCOEB_ECUDA;
+    }
+    *work = ws;
+    return DISCOEB_SUCCESS;
+}
+
+std::mutex g_blas_mu;
+cublasHandle_t g_blas[64] = {};
+
+cublasHandle_t blas_handle(int dev)
+{
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!g_blas[dev] && cublasCreate(&g_blas[dev]) != CUBLAS_STATUS_SUCCESS) g_blas[dev] = nullptr;
+    return g_blas[dev];
+}
+
+inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace
+
+extern "C" {
+
+int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_modes,
+                        const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
+                        const double* y_full, double* fields, double* scratch, void* stream)
+{
+    if (!cosmo_host || !cosmo_dev || n_modes < 0 || n_tau < 0) return DISCOEB_EINVAL;
+    if (cosmo_host->use_tca) return DISCOEB_EUNSUPPORTED;
+    if (n_modes == 0 || n_tau == 0) return DISCOEB_SUCCESS;
+    if (n_tau < 3 || !kmodes || !tau || !bgtab || !y_full || !fields || !scratch) return DISCOEB_EINVAL;
+    const Dims D = make_dims(*cosmo_host);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const long long points = (long long)n_modes * n_tau;
+    const int threads = 128;
+    const size_t smem = sizeof(double) * (size_t)D.n * (threads / 32);
+    sources_kernel<<<blocks_for(points * 32, threads), threads, smem, s>>>(cosmo_dev, n_modes, kmodes, n_tau, tau,
+                                                                            bgtab, y_full, fields);
+    isw_kernel<<<blocks_for(n_modes, 64), 64, 0, s>>>(n_modes, n_tau, tau, bgtab, fields, scratch);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int64_t discoeb_los_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
+                                    int32_t n_k_dense)
+{
+    if (n_modes < 2 || n_tau < 3 || ellmax < 0 || n_fftlog < 2 || n_k_dense < 0 || n_k_dense == 1)
+        return DISCOEB_EINVAL;
+    const int rows = n_k_dense > 0 ? n_k_dense : n_modes;
+    cufftHandle plan;
+    size_t work = 0;
+    if (make_fft_plan(&plan, n_fftlog, rows, 2LL * (n_fftlog / 2 + 1), &work) != DISCOEB_SUCCESS) return DISCOEB_ECUDA;
+    cufftDestroy(plan);
+    return (int64_t)los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work).total;
+}
+
+int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S,
+                    double tau0, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, void* workspace,
+                    int64_t workspace_bytes, double* theta, double* kmodes_out, void* stream)
+{
+    if (n_modes < 2 || n_tau < 3 || ellmax < 0 || n_fftlog < 2 || n_k_dense < 0 || n_k_dense == 1)
+        return DISCOEB_EINVAL;
+    if (!kmodes || !tau || !S || !workspace || !theta || !kmodes_out) return DISCOEB_EINVAL;
+    if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return DISCOEB_EINVAL;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int rows = n_k_dense > 0 ? n_k_dense : n_modes;
+    cufftHandle plan;
+    size_t work = 0;
+    int rc = make_fft_plan(&plan, n_fftlog, rows, 2LL * (n_fftlog / 2 + 1), &work);
+    if (rc) return rc;
+    const LosLayout L = los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work);
+    if ((uint64_t)workspace_bytes < L.total) {
+        cufftDestroy(plan);
+        return DISCOEB_EINVAL;
+    }
+    char* ws = static_cast<char*>(workspace);
+    auto D = [&](size_t off) { return reinterpret_cast<double*>(ws + off); };
+    const int T = 256;
+    // 1. rows of S on the k grid used for the integral
+    const double* Srow = S;
+    const double* krow = kmodes;
+    log_kernel<<<blocks_for(n_modes, T), T, 0, s>>>(n_modes, kmodes, D(L.lk));
+    if (n_k_dense > 0) {
+        k_spline_log_kernel<<<blocks_for(n_tau, 64), 64, 0, s>>>(n_modes, D(L.lk), n_tau, S, D(L.s2k), D(L.cpk));
+        k_dense_kernel<<<blocks_for((long long)n_k_dense * n_tau, T), T, 0, s>>>(n_modes, D(L.lk), n_tau, S, D(L.s2k),
+                                                                                  n_k_dense, D(L.sd), D(L.kd));
+        Srow = D(L.sd);
+        krow = D(L.kd);
+    } else {
+        cudaMemcpyAsync(D(L.kd), kmodes, sizeof(double) * n_modes, cudaMemcpyDeviceToDevice, s);
+        krow = D(L.kd);
+    }
+    cudaMemcpyAsync(kmodes_out, krow, sizeof(double) * rows, cudaMemcpyDeviceToDevice, s);
+    // 2. the FFTLog grid and the biased source on it
+    geom_kernel<<<1, 32, 0, s>>>(n_tau, tau, tau0, n_fftlog, D(L.geom));
+    lchi_kernel<<<blocks_for(n_tau, T), T, 0, s>>>(n_tau, tau, tau0, D(L.lchi));
+    fgrid_kernel<<<blocks_for(n_fftlog, T), T, 0, s>>>(n_tau, D(L.lchi), n_fftlog, D(L.geom),
+                                                       reinterpret_cast<int*>(ws + L.fidx), D(L.fx), D(L.fbias));
+    chi_spline_kernel<<<blocks_for(rows, 64), 64, 0, s>>>(rows, n_tau, D(L.lchi), Srow, D(L.s2c), D(L.cpc));
+    chi_eval_kernel<<<blocks_for((long long)rows * n_fftlog, T), T, 0, s>>>(
+        rows, n_tau, D(L.lchi), Srow, D(L.s2c), n_fftlog, reinterpret_cast<const int*>(ws + L.fidx), D(L.fx),
+        D(L.fbias), L.pitch, D(L.fft));
+    // 3. rfft of every row, in place
+    cufftSetWorkArea(plan, ws + L.cufft);
+    cufftSetStream(plan, s);
+    const cufftResult fr = cufftExecD2Z(plan, D(L.fft), reinterpret_cast<cufftDoubleComplex*>(D(L.fft)));
+    cufftDestroy(plan);
+    if (fr != CUFFT_SUCCESS) return DISCOEB_ECUDA;
+    // 4. ck in place, and the M table
+    ck_kernel<<<blocks_for((long long)rows * L.n_freq, T), T, 0, s>>>(rows, krow, n_fftlog, L.n_freq, D(L.geom),
+                                                                      L.pitch, D(L.fft));
+    mcoef_kernel<<<blocks_for((long long)(ellmax + 1) * L.n_freq, T), T, 0, s>>>(ellmax + 1, L.n_freq, n_fftlog,
+                                                                                 D(L.geom), D(L.B));
+    if (cudaGetLastError() != cudaSuccess) return DISCOEB_ECUDA;
+    // 5. theta[r, l] = sum_j A[r, j] B[l, j] over the interleaved (re, im) pairs: one DGEMM
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
+    std::lock_guard<std::mutex> lock(g_blas_mu);
+    cublasHandle_t h = blas_handle(dev);
+    if (!h) return DISCOEB_ECUDA;
+    cublasSetStream(h, s);
+    cublasSetWorkspace(h, ws + L.cublas, kCublasWorkspace);
+    const double one = 1.0, zero = 0.0;
+    const cublasStatus_t st =
+        cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ellmax + 1, rows, (int)L.pitch, &one, D(L.B), (int)L.pitch, D(L.fft),
+                    (int)L.pitch, &zero, theta, ellmax + 1);
+    cublasSetWorkspace(h, nullptr, 0);
+    if (st != CUBLAS_STATUS_SUCCESS) return DISCOEB_ECUDA;
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta, double n_s, double k_p,
+                     double* cell, void* stream)
+{
+    if (n_modes < 2 || n_ell < 1 || !kmodes || !theta || !cell) return DISCOEB_EINVAL;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    cell_kernel<<<blocks_for(n_ell, 128), 128, 0, s>>>(n_modes, kmodes, n_ell, theta, n_s, k_p, cell);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+}  // extern "C"

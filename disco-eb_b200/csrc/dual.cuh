@@ -11,7 +11,7 @@
 
 #if defined(__CUDACC__)
 #define DHD __host__ __device__ __forceinline__
-#define DDV __device__
+#define DDV __device__ inline
 #else
 #define DHD inline
 #define DDV inline

@@ -134,6 +134,16 @@ def lib():
                                   ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp, vp, vp]
         L.discoeb_jvp.restype = ctypes.c_int32
         L.discoeb_rhs.restype = ctypes.c_int32
+        L.discoeb_sources.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, vp, ctypes.c_int32, vp, vp, vp,
+                                      vp, vp, vp]
+        L.discoeb_sources.restype = ctypes.c_int32
+        L.discoeb_los_workspace_bytes.argtypes = [ctypes.c_int32] * 5
+        L.discoeb_los_workspace_bytes.restype = ctypes.c_int64
+        L.discoeb_los.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, vp, ctypes.c_double, ctypes.c_int32,
+                                  ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int64, vp, vp, vp]
+        L.discoeb_los.restype = ctypes.c_int32
+        L.discoeb_cell.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, ctypes.c_double, ctypes.c_double, vp, vp]
+        L.discoeb_cell.restype = ctypes.c_int32
         if L.discoeb_abi_version() != ABI_VERSION:
             raise RuntimeError("libdiscoeb_b200.so ABI version mismatch; rebuild it")
         _lib = L

@@ -1,0 +1,198 @@
+"""CMB temperature source functions, line-of-sight multipoles and C_l on the GPU.
+
+Mirrors the call surface of the reference's ``src/discoeb/cmb.py``:
+``compute_visibility_functions`` (host, 1-D tables), ``compute_source_function`` ->
+``discoeb_sources``, ``compute_theta_ell`` -> ``discoeb_los`` (FFTLog: cuFFT + one FP64 GEMM),
+``compute_Cell`` -> ``discoeb_cell``, ``compute_Dell`` (unit conversion) and
+``compute_Cell_spectrum_from_cosmo_params`` (the whole chain with every large array resident on
+the device).  The per-stage intermediates of the reference (metric, polarisation and neutrino
+terms) are fields of the same source kernel, returned by ``compute_sources``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _abi
+from .background import compute_background_quantities, evolve_background, get_aprimeoa, get_neutrino_momentum_bins
+from .perturbations import DeviceCosmo, solve_modes, k_sampling
+from .spline import spline_interpolation
+
+BG_FIELDS = ("a", "aprimeoa", "rhonu", "rho_Q", "w_Q", "opac", "opacprime", "gvis", "gvisprime", "gvispprime",
+             "optical_depth")
+SRC_FIELDS = ("S", "S1", "S2", "S3", "S4", "potential", "alpha", "alphaprime", "alphapprime", "hprime", "etaprime",
+              "aprimeoaprime", "polarization_term", "polarization_termprime", "polarization_termpprime", "drhonu",
+              "dpnu", "fnu", "shearnu", "rho_nu_prime", "shear_nu_prime", "thetabprime")
+
+
+def _device(device):
+    import torch
+    if device is None:
+        if not torch.cuda.is_available():
+            raise RuntimeError("discoeb_b200 needs a CUDA device (there is no CPU path)")
+        device = torch.device("cuda", torch.cuda.current_device())
+    return torch, device
+
+
+def compute_visibility_functions(tau, param):
+    """Opacity, visibility g and its derivatives, optical depth at ``tau`` (cmb.py:95-163):
+    natural cubic splines in ln(tau) of the thermal-history arrays of ``evolve_background``."""
+    tau = np.asarray(tau, dtype=np.float64)
+    lt, ltn = np.log(param["tau"]), np.log(tau)
+    op = spline_interpolation(lt, param["opac"])
+    od = spline_interpolation(lt, np.log(np.maximum(param["optical_depth"], 1e-10)))
+    return {
+        "opac": op.evaluate(ltn),
+        "opacprime": op.derivative(ltn) / tau,
+        "gvis": spline_interpolation(lt, param["gvis"]).evaluate(ltn),
+        "gvisprime": spline_interpolation(lt, param["gvisprime"]).evaluate(ltn),
+        "gvispprime": spline_interpolation(lt, param["gvispprime"]).evaluate(ltn),
+        "optical_depth": np.exp(od.evaluate(ltn)),
+    }
+
+
+def background_table(aexp_out, tau, param):
+    """``float64[DISCOEB_BG_NFIELDS, n_tau]``: the per-output-time inputs of discoeb_sources."""
+    aexp_out = np.asarray(aexp_out, dtype=np.float64)
+    bq = compute_background_quantities(aexp_out, param)
+    vis = compute_visibility_functions(tau, param)
+    rows = {"a": aexp_out, "aprimeoa": get_aprimeoa(param=param, aexp=aexp_out), **bq, **vis}
+    return np.ascontiguousarray(np.stack([np.broadcast_to(rows[f], aexp_out.shape) for f in BG_FIELDS]))
+
+
+def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, de_guard_eps=1e-9,
+                    device=None):
+    """All source fields of compute_source_function and its intermediates (cmb.py:17-633).
+
+    ``yout``: the RSA-projected full states ``[K, n_tau, nvar]`` at ``tau(aexp_out)`` (numpy or
+    a device tensor).  Returns a dict of device tensors ``[K, n_tau]`` keyed by SRC_FIELDS.
+    """
+    torch, device = _device(device)
+    lib = _abi.lib()
+    aexp_out = np.asarray(aexp_out, dtype=np.float64)
+    tau = param["tau_of_a_spline"].evaluate(aexp_out)
+    kmodes = np.ascontiguousarray(kmodes, dtype=np.float64)
+    K, T = kmodes.shape[0], tau.shape[0]
+    dc = DeviceCosmo(param, lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax,
+                     de_guard_eps=de_guard_eps, device=device)
+    f64 = dict(dtype=torch.float64, device=device)
+    y = yout if isinstance(yout, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(yout))
+    y = y.to(**f64).contiguous()
+    if y.shape[:2] != (K, T):
+        raise ValueError(f"yout must have shape [{K}, {T}, nvar], got {tuple(y.shape)}")
+    d_k = torch.from_numpy(kmodes).to(device)
+    d_tau = torch.from_numpy(np.ascontiguousarray(tau)).to(device)
+    d_bt = torch.from_numpy(background_table(aexp_out, tau, param)).to(device)
+    fields = torch.empty((len(SRC_FIELDS), K, T), **f64)
+    scratch = torch.empty((K, T), **f64)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    rc = lib.discoeb_sources(dc.struct.data_ptr(), ctypes.byref(dc.host), K, d_k.data_ptr(), T, d_tau.data_ptr(),
+                             d_bt.data_ptr(), y.data_ptr(), fields.data_ptr(), scratch.data_ptr(), stream)
+    if rc != 0:
+        raise RuntimeError(f"discoeb_sources failed with code {rc}")
+    return {name: fields[i] for i, name in enumerate(SRC_FIELDS)}
+
+
+def compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0, device=None):
+    """Theta_l(k) by FFTLog line-of-sight integration (cmb.py:680-835).
+
+    Returns ``(theta [K', ellmax+1], kmodes [K'])`` as device tensors (K' = n_k_dense if > 0).
+    """
+    torch, device = _device(device)
+    lib = _abi.lib()
+    f64 = dict(dtype=torch.float64, device=device)
+    d_k = torch.as_tensor(np.asarray(kmodes, dtype=np.float64) if not isinstance(kmodes, torch.Tensor) else kmodes)
+    d_k = d_k.to(**f64).contiguous()
+    d_tau = torch.as_tensor(np.asarray(tau, dtype=np.float64) if not isinstance(tau, torch.Tensor) else tau)
+    d_tau = d_tau.to(**f64).contiguous()
+    d_S = S if isinstance(S, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(S, dtype=np.float64))
+    d_S = d_S.to(**f64).contiguous()
+    K, T = d_S.shape
+    if d_k.shape[0] != K or d_tau.shape[0] != T:
+        raise ValueError("S must have shape [len(kmodes), len(tau)]")
+    nb = lib.discoeb_los_workspace_bytes(K, T, int(ellmax), int(n_fftlog), int(n_k_dense))
+    if nb < 0:
+        raise ValueError(f"invalid sizes for the line-of-sight integral (code {nb})")
+    ws = torch.empty(int(nb) // 8 + 32, dtype=torch.float64, device=device)
+    rows = int(n_k_dense) if n_k_dense > 0 else K
+    theta = torch.empty((rows, int(ellmax) + 1), **f64)
+    k_out = torch.empty(rows, **f64)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    base = ws.data_ptr()
+    aligned = (base + 255) // 256 * 256
+    rc = lib.discoeb_los(K, d_k.data_ptr(), T, d_tau.data_ptr(), d_S.data_ptr(), float(tau0), int(ellmax),
+                         int(n_fftlog), int(n_k_dense), aligned, int(nb), theta.data_ptr(), k_out.data_ptr(), stream)
+    if rc != 0:
+        raise RuntimeError(f"discoeb_los failed with code {rc}")
+    return theta, k_out
+
+
+def compute_Cell(theta_ell, kmodes, n_s, k_p, device=None):
+    """C_l = int d ln k (k/k_p)^(n_s-1) Theta_l^2, trapezoid (cmb.py:838-873); device tensor."""
+    torch, device = _device(device)
+    lib = _abi.lib()
+    f64 = dict(dtype=torch.float64, device=device)
+    th = theta_ell if isinstance(theta_ell, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(theta_ell))
+    th = th.to(**f64).contiguous()
+    kk = kmodes if isinstance(kmodes, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(kmodes))
+    kk = kk.to(**f64).contiguous()
+    K, L = th.shape
+    cell = torch.empty(L, **f64)
+    rc = lib.discoeb_cell(K, kk.data_ptr(), L, th.data_ptr(), float(n_s), float(k_p), cell.data_ptr(),
+                          torch.cuda.current_stream(device).cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"discoeb_cell failed with code {rc}")
+    return cell
+
+
+def compute_Dell(Cell, A_s, Tcmb, ellmax=None):
+    """D_l = l(l+1) C_l A_s 2 T_cmb^2 1e12 for l >= 2 (the reference's convention, cmb.py:876-927)."""
+    C = Cell.detach().cpu().numpy() if hasattr(Cell, "detach") else np.asarray(Cell)
+    if ellmax is None:
+        ellmax = C.shape[0] - 1
+    ell = np.arange(ellmax + 1)
+    return ell[2:], ell[2:] * (ell[2:] + 1) * C[2:ellmax + 1] * A_s * 2 * Tcmb**2 * 1e12
+
+
+def cmb_aexp_out(n_early=32, n_pre_recomb=64, n_recomb=128, n_post=96):
+    """Output scale factors of compute_Cell_spectrum_from_cosmo_params (cmb.py:1006-1022)."""
+    a_b1, a_b2, a_b3 = 1.0 / 3001.0, 1.0 / 1401.0, 1.0 / 601.0
+    return np.concatenate([np.geomspace(1e-4, a_b1, n_early, endpoint=False),
+                           np.geomspace(a_b1, a_b2, n_pre_recomb, endpoint=False),
+                           np.geomspace(a_b2, a_b3, n_recomb, endpoint=False), np.geomspace(a_b3, 1.0, n_post)])
+
+
+def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0, n_k_dense=8192,
+                                            n_fftlog=16384, lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3,
+                                            num_thermo=1024, rtol=1e-4, atol=1e-4, max_steps=2048,
+                                            k_sampling_method="camb", aexp_out=None, device=None,
+                                            return_intermediates=False):
+    """C_l^TT of a cosmology (cmb.py:931-1090): background (host), full perturbation solve,
+    sources, FFTLog line of sight and C_l on the GPU, large arrays never leaving the device.
+
+    Returns ``(Cell [ellmax+1] numpy, param)`` like the reference.
+    """
+    torch, device = _device(device)
+    param = evolve_background(param=dict(param_dict), thermo_module="RECFAST", num_thermo=num_thermo)
+    aexp_out = cmb_aexp_out() if aexp_out is None else np.asarray(aexp_out, dtype=np.float64)
+    kmodes = k_sampling(param, kmin, kmax, nmodes, k_sampling_method)
+    tau = param["tau_of_a_spline"].evaluate(aexp_out)
+    L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
+    y = solve_modes(param=param, kmodes=kmodes, tau_out=tau, rtol=rtol, atol=atol, pcoeff=0.25, icoeff=0.80,
+                    dcoeff=0.0, factormax=20.0, factormin=0.3, max_steps=max_steps, return_full=True,
+                    device=device, as_tensor=True, **L)
+    src = compute_sources(param=param, yout=y, kmodes=kmodes, aexp_out=aexp_out, device=device, **L)
+    tau0 = float(param["tau_of_a_spline"].evaluate(1.0))
+    theta, kk = compute_theta_ell(ellmax, kmodes, tau, src["S"], tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                  device=device)
+    cell = compute_Cell(theta, kk, param["n_s"], param["k_p"], device=device)
+    for key, v in (("lmaxg", lmaxg), ("lmaxgp", lmaxgp), ("lmaxr", lmaxr), ("lmaxnu", lmaxnu), ("nqmax", nqmax),
+                   ("nout", aexp_out.shape[0]), ("tau_out", tau)):
+        param[key] = v
+    out = cell.cpu().numpy()
+    if return_intermediates:
+        return out, param, {"kmodes": kmodes, "aexp_out": aexp_out, "tau": tau, "y": y, "sources": src,
+                            "theta": theta, "kmodes_los": kk}
+    return out, param

@@ -236,13 +236,15 @@ def _check_status(status, nsteps, kmodes, on_failure):
 
 def solve_modes(*, param, kmodes, tau_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, rtol, atol, pcoeff, icoeff, dcoeff,
                 factormax, factormin, max_steps, return_full, de_guard_eps=1e-9, device=None, warps_per_block=0,
-                on_failure="raise", sort_modes=True, return_stats=False, tau_start=None, switch_tau=None):
+                on_failure="raise", sort_modes=True, return_stats=False, tau_start=None, switch_tau=None,
+                as_tensor=False):
     """Integrate the given modes of one cosmology to ``tau_out`` on the GPU.
 
     Returns numpy ``y`` (``[K, nout, 20]`` or ``[K, nout, nvar]``); with
     ``return_stats`` also ``(status, nsteps)``.  ``tau_start`` [K] and ``switch_tau`` [K, 3]
     override the start times and approximation switch times derived from ``param`` (to hold
     these numerical choices fixed while parameters move, as forward-mode AD does).
+    ``as_tensor``: return ``y`` as a device tensor (the caller's mode order) instead of numpy.
     """
     import torch
     if device is None:
@@ -294,11 +296,13 @@ def solve_modes(*, param, kmodes, tau_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, 
     if rc != 0:
         raise RuntimeError(f"discoeb_fwd failed with code {rc}")
     out_dev = d_full if return_full else d_out20
-    y_sorted = out_dev.cpu().numpy()
-    stat = d_stat.cpu().numpy()
     inv = np.empty_like(order)
     inv[order] = np.arange(K)
-    y = y_sorted[inv]
+    if as_tensor:
+        y = out_dev.index_select(0, torch.from_numpy(inv).to(device))
+    else:
+        y = out_dev.cpu().numpy()[inv]
+    stat = d_stat.cpu().numpy()
     status, nsteps = stat[0][inv], stat[1][inv]
     _check_status(status, nsteps, kmodes, on_failure)
     if return_stats:

@@ -138,6 +138,81 @@ int32_t discoeb_rhs(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_hos
                     const double* tau, const double* kmodes, const double* y, int32_t regime, double* f,
                     void* stream);
 
+/* ---- CMB sources and line-of-sight integral (src/discoeb/cmb.py) ---- */
+
+/* Per-output-time background table bgtab[DISCOEB_BG_NFIELDS, n_tau] (row f = field f):
+ * a(tau_out), a'/a (get_aprimeoa), rho_nu, rho_Q, w_Q (compute_background_quantities,
+ * background.py:348-406), and the visibility functions of compute_visibility_functions
+ * (cmb.py:95-163): opacity, its tau derivative, g, g', g'', optical depth. */
+#define DISCOEB_BG_A 0
+#define DISCOEB_BG_APRIMEOA 1
+#define DISCOEB_BG_RHONU 2
+#define DISCOEB_BG_RHO_Q 3
+#define DISCOEB_BG_W_Q 4
+#define DISCOEB_BG_OPAC 5
+#define DISCOEB_BG_OPACPRIME 6
+#define DISCOEB_BG_GVIS 7
+#define DISCOEB_BG_GVISPRIME 8
+#define DISCOEB_BG_GVISPPRIME 9
+#define DISCOEB_BG_OPTICAL_DEPTH 10
+#define DISCOEB_BG_NFIELDS 11
+
+/* Output fields of discoeb_sources, fields[DISCOEB_SRC_NFIELDS, n_modes, n_tau]. */
+#define DISCOEB_SRC_S 0             /* S = S1 + S2 + S3 + S4 (compute_source_function) */
+#define DISCOEB_SRC_S1 1            /* ISW, compute_source_term_isw */
+#define DISCOEB_SRC_S2 2            /* Sachs-Wolfe */
+#define DISCOEB_SRC_S3 3            /* Doppler */
+#define DISCOEB_SRC_S4 4            /* polarisation */
+#define DISCOEB_SRC_POTENTIAL 5     /* eta + alpha' (differentiated for S1) */
+#define DISCOEB_SRC_ALPHA 6         /* compute_metric_perturbations: alpha, alpha', alpha'', h', eta', (a'/a)' */
+#define DISCOEB_SRC_ALPHAPRIME 7
+#define DISCOEB_SRC_ALPHAPPRIME 8
+#define DISCOEB_SRC_HPRIME 9
+#define DISCOEB_SRC_ETAPRIME 10
+#define DISCOEB_SRC_APRIMEOAPRIME 11
+#define DISCOEB_SRC_POL 12          /* compute_polarization_terms: Pi, Pi', Pi'' */
+#define DISCOEB_SRC_POLPRIME 13
+#define DISCOEB_SRC_POLPPRIME 14
+#define DISCOEB_SRC_DRHONU 15       /* compute_neutrino_perturbations */
+#define DISCOEB_SRC_DPNU 16
+#define DISCOEB_SRC_FNU 17
+#define DISCOEB_SRC_SHEARNU 18
+#define DISCOEB_SRC_RHONUPRIME 19
+#define DISCOEB_SRC_SHEARNUPRIME 20
+#define DISCOEB_SRC_THETABPRIME 21  /* theta_b' of compute_time_derivatives */
+#define DISCOEB_SRC_NFIELDS 22
+
+/* CMB source function at the output times of a full solve: replaces
+ * compute_time_derivatives + extract_perturbations + compute_neutrino_perturbations +
+ * compute_metric_perturbations + compute_polarization_terms + compute_source_term_* +
+ * compute_source_function (perturbations.py:1339-1406, cmb.py:17-633).
+ *   y_full [n_modes, n_tau, nvar]  RSA-projected states (discoeb_fwd's y_full), device
+ *   tau [n_tau] increasing, kmodes [n_modes], bgtab [DISCOEB_BG_NFIELDS, n_tau], device
+ *   fields [DISCOEB_SRC_NFIELDS, n_modes, n_tau] out; scratch [n_modes, n_tau] doubles. */
+int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_modes,
+                        const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
+                        const double* y_full, double* fields, double* scratch, void* stream);
+
+/* Workspace bytes of discoeb_los for these sizes (< 0: invalid sizes or a cuFFT error). */
+int64_t discoeb_los_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
+                                    int32_t n_k_dense);
+
+/* Line-of-sight multipoles Theta_l(k) = int S(k, tau) j_l(k (tau0 - tau)) dtau by the
+ * reference's FFTLog method: replaces compute_theta_ell (cmb.py:680-835).
+ *   S [n_modes, n_tau] device; kmodes [n_modes] increasing; tau [n_tau] increasing.
+ *   n_k_dense > 0: S is first spline-resampled onto n_k_dense log-spaced modes.
+ *   theta [K', ellmax + 1] and kmodes_out [K'] out, K' = n_k_dense or n_modes.
+ *   workspace: >= discoeb_los_workspace_bytes(...) bytes of device memory, 256-byte aligned
+ *   (the FFT buffer, the coefficient table and the cuFFT / cuBLAS work areas live there). */
+int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S,
+                    double tau0, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, void* workspace,
+                    int64_t workspace_bytes, double* theta, double* kmodes_out, void* stream);
+
+/* C_l = trapezoid over ln k of (k/k_p)^(n_s-1) Theta_l(k)^2: replaces compute_Cell
+ * (cmb.py:838-873).  theta [n_modes, n_ell], cell [n_ell], device. */
+int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta, double n_s,
+                     double k_p, double* cell, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

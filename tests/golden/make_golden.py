@@ -5,6 +5,12 @@ Reads (as text) the committed fixtures of the reference project:
   tests/test_cmb/test_benchmark_evolve_perturbations_batched.csv (full states of 3 modes, 320 outputs)
   tests/resources/CLASS_data.json                            (CLASS P_bc(k) at a = 0.01)
   tests/resources/RECFAST_DISCO_EB_data.json                 (x_e(a) of DISCO-EB v0.1.0)
+and, into reference_cmb_golden.npz, the CMB chain's fixtures (DISCO-Notebook cosmology, 1024-point
+thermal history, 128 camb-sampled modes, 320 output times, lmax 11/11/11/8/3, rtol = atol = 1e-4):
+  tests/test_cmb/test_benchmark_compute_{time_derivatives, visibility_functions,
+  background_quantities, neutrino_perturbations, metric_perturbations, polarization_terms,
+  source_term_sachs_wolfe, source_term_doppler, source_term_polarization, theta_ell, Cell,
+  Dell}.csv and test_benchmark_extract_perturbations.csv
 Usage: python tests/golden/make_golden.py /path/to/reference
 """
 import csv
@@ -53,3 +59,27 @@ data = {
 }
 np.savez_compressed(out, **data)
 print(out, os.path.getsize(out), "bytes")
+
+cmb = {}
+d = os.path.join(ref, "tests/test_cmb")
+for stem in ("compute_visibility_functions", "compute_background_quantities", "extract_perturbations",
+             "compute_neutrino_perturbations", "compute_metric_perturbations", "compute_polarization_terms",
+             "compute_source_term_sachs_wolfe", "compute_source_term_doppler", "compute_source_term_polarization",
+             "compute_theta_ell", "compute_Cell", "compute_Dell"):
+    for key, v in read_csv(os.path.join(d, f"test_benchmark_{stem}.csv")).items():
+        cmb[f"{stem}:{key}"] = v
+td = read_csv(os.path.join(d, "test_benchmark_compute_time_derivatives.csv"))
+for key, v in td.items():  # [320, 72] per mode; every 4th output time plus the last
+    cmb[f"compute_time_derivatives:{key}"] = v.reshape(320, 72)[sel]
+cmb["compute_time_derivatives:out_index"] = sel
+# the reference's C_l^TT accuracy record against CAMB (|D_disco - D_camb| / D_camb per l = 2..2500)
+# and the CAMB spectrum it was measured against
+acc = read_csv(os.path.join(d, "test_cmb_vs_camb_DISCO_Notebook_.csv"))
+cmb["camb:disco_relative_error"] = acc["relative_error"]
+with open(os.path.join(ref, "tests/resources/camb_benchmarks/DISCO-Notebook.csv")) as fh:
+    cb = np.array([[float(v) for v in r] for r in list(csv.reader(fh))[1:]])  # columns ell, D_ell
+cmb["camb:ell"] = cb[:, 0]
+cmb["camb:D_ell"] = cb[:, 1]
+out2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_cmb_golden.npz")
+np.savez_compressed(out2, **cmb)
+print(out2, os.path.getsize(out2), "bytes")
