@@ -243,10 +243,14 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
     }
     const T g0 = H, g1 = E, g2 = polter;
     const int nh = n_hier_rows(D);
-    for (int hh = tm.lane; hh < nh; hh += tm.nl) {
-        const int i = hier_row(D, hh);
+    // every lane runs the same number of iterations: the shuffle in the loop needs all lanes
+    for (int h0 = 0; h0 < nh; h0 += tm.nl) {
+        const int hh = h0 + tm.lane;
+        const bool act = hh < nh;
+        const int i = hier_row(D, act ? hh : 0);
         const int q = hier_bin(D, i);
         const T vq = tm.full() ? tm.bcast(vl, q) : rcp(inv_vq(P, b, q));
+        if (!act) continue;
         T lo, di, up, u[3];
         int st;
         bool trunc;
@@ -351,10 +355,14 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
     double vlane = 1.0;
     if (tm.full() && tm.lane < D.nq) vlane = rcp(inv_vq(P, b, tm.lane));
     const int nh = n_hier_rows(D);
-    for (int hh = tm.lane; hh < nh; hh += tm.nl) {
-        const int i = hier_row(D, hh);
+    // every lane runs the same number of iterations: the shuffle in the loop needs all lanes
+    for (int h0 = 0; h0 < nh; h0 += tm.nl) {
+        const int hh = h0 + tm.lane;
+        const bool act = hh < nh;
+        const int i = hier_row(D, act ? hh : 0);
         const int q = hier_bin(D, i);
         const double vq = tm.full() ? tm.bcast(vlane, q) : rcp(inv_vq(P, b, q));
+        if (!act) continue;
         double lo, di, up, u[3];
         int st;
         bool trunc;
