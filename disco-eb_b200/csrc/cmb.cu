@@ -388,6 +388,14 @@ __device__ Cx log_sin_pi(Cx z)
         sincos(x, &sx, &cxv);
         return cx_log(cx(sx * cosh(y), cxv * sinh(y)));
     }
+    // Where sin(x) cosh(y) or cos(x) sinh(y) exceeds DBL_MAX the reference's complex sin
+    // overflows to infinity, its log is +inf, and the coefficient it feeds comes out as exactly
+    // zero: keep that behaviour (709.782712893384 = ln DBL_MAX).
+    {
+        double sx, cxv;
+        sincos(x, &sx, &cxv);
+        if (fabs(y) - M_LN2 + log(fmax(fabs(sx), fabs(cxv))) > 709.782712893384) return cx(INFINITY, 0.0);
+    }
     // |y| large: sin(pi z) = e^{|y|} e^{-i s x} (1 - e^{-2|y|} e^{2 i s x}) / (2 i s), s = sign(y)
     const double s = y > 0 ? 1.0 : -1.0, ay = fabs(y);
     double sn, cs;
@@ -419,10 +427,15 @@ __global__ void mcoef_kernel(int n_ell, int n_freq, int n_fft, const double* __r
     const Cx p = cx(kBias, eta);
     const Cx a1 = cx((1.0 + l + p.re) / 2.0, p.im / 2.0), a2 = cx((2.0 + l - p.re) / 2.0, -p.im / 2.0);
     const Cx lc = cx((p.re - 1.0) * M_LN2 + 0.5 * log(M_PI), p.im * M_LN2) + lngamma_c(a1) - lngamma_c(a2);
+    double* b = B + (size_t)l * (2 * (size_t)n_freq) + 2 * q;
+    if (lc.re == -INFINITY) {
+        b[0] = 0.0;
+        b[1] = 0.0;
+        return;
+    }
     const double mag = exp(lc.re);
     double sn, cs;
     sincos(lc.im, &sn, &cs);
-    double* b = B + (size_t)l * (2 * (size_t)n_freq) + 2 * q;
     b[0] = mag * cs;
     b[1] = -mag * sn;
 }
