@@ -396,14 +396,14 @@ __device__ Cx log_sin_pi(Cx z)
         sincos(x, &sx, &cxv);
         if (fabs(y) - M_LN2 + log(fmax(fabs(sx), fabs(cxv))) > 709.782712893384) return cx(INFINITY, 0.0);
     }
-    // |y| large: sin(pi z) = e^{|y|} e^{-i s x} (1 - e^{-2|y|} e^{2 i s x}) / (2 i s), s = sign(y)
+    // |y| large: sin(pi z) = (i s / 2) e^{|y|} e^{-i s x} (1 - e^{-2|y|} e^{2 i s x}), s = sign(y)
     const double s = y > 0 ? 1.0 : -1.0, ay = fabs(y);
     double sn, cs;
     sincos(2.0 * s * x, &sn, &cs);
     const double e = exp(-2.0 * ay);
     const Cx corr = cx_log(cx(1.0 - e * cs, -e * sn));
-    // log(1 / (2 i s)) = -log 2 - i s pi/2
-    return cx(ay - M_LN2, -s * x - s * M_PI_2) + corr;
+    // log of the prefactor: log(i s / 2) = -log 2 + i s pi/2
+    return cx(ay - M_LN2, -s * x + s * M_PI_2) + corr;
 }
 
 __device__ Cx lngamma_c(Cx z)
