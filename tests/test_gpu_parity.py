@@ -90,7 +90,7 @@ def test_gpu_full_state_and_projection(torch_cuda):
     yo = _oracle_outputs(bg, k, aout, dict(lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3), 1e-5, 1e-8, 0.0,
                          full=True)
     np.testing.assert_allclose(y[:, :, 3], yo[:, :, 3], rtol=2e-5)  # same algorithm; rare accept flips
-    np.testing.assert_allclose(y[:, :, 7], yo[:, :, 7], rtol=1e-5, atol=1e-9 * np.abs(yo[:, :, 7]).max())
+    np.testing.assert_allclose(y[:, :, 7], yo[:, :, 7], rtol=3e-5, atol=1e-9 * np.abs(yo[:, :, 7]).max())
 
 
 def test_gpu_edge_cases(torch_cuda):
