@@ -525,6 +525,27 @@ cublasHandle_t blas_handle(int dev)
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+// Scratch of discoeb_sources_noalloc: one module-static device array per device (8 MiB), so that
+// the call makes no allocation.  It holds the per-mode spline recurrence of the ISW term, which is
+// written before it is read, so nothing has to be cleared between calls.
+constexpr long long kNoAllocScratchDoubles = 1LL << 20;
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {};
+
+// device address of g_noalloc_scratch on the current device, looked up once per device
+double* noalloc_scratch(int dev)
+{
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return nullptr;
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
 }  // namespace
 
 extern "C" {
@@ -546,6 +567,21 @@ int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo
                                                                             bgtab, y_full, fields);
     isw_kernel<<<blocks_for(n_modes, 64), 64, 0, s>>>(n_modes, n_tau, tau, bgtab, fields, scratch);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int32_t discoeb_sources_noalloc(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_modes,
+                                const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
+                                const double* y_full, double* fields, void* stream)
+{
+    if (n_modes < 0 || n_tau < 0) return DISCOEB_EINVAL;
+    if ((long long)n_modes * n_tau > kNoAllocScratchDoubles) return DISCOEB_EINVAL;
+    if (n_modes == 0 || n_tau == 0) return discoeb_sources(cosmo_dev, cosmo_host, n_modes, kmodes, n_tau, tau, bgtab,
+                                                           y_full, fields, nullptr, stream);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
+    double* scratch = noalloc_scratch(dev);
+    if (!scratch) return DISCOEB_ECUDA;
+    return discoeb_sources(cosmo_dev, cosmo_host, n_modes, kmodes, n_tau, tau, bgtab, y_full, fields, scratch, stream);
 }
 
 int64_t discoeb_los_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,

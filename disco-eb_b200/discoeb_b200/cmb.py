@@ -63,11 +63,13 @@ def background_table(aexp_out, tau, param):
 
 
 def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, de_guard_eps=1e-9,
-                    device=None):
+                    device=None, no_alloc=False):
     """All source fields of compute_source_function and its intermediates (cmb.py:17-633).
 
     ``yout``: the RSA-projected full states ``[K, n_tau, nvar]`` at ``tau(aexp_out)`` (numpy or
     a device tensor).  Returns a dict of device tensors ``[K, n_tau]`` keyed by SRC_FIELDS.
+    ``no_alloc``: use discoeb_sources_noalloc (library-static scratch, K * n_tau <= 2^20; calls
+    must not overlap in time on one device).
     """
     torch, device = _device(device)
     lib = _abi.lib()
@@ -86,10 +88,14 @@ def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmax
     d_tau = torch.from_numpy(np.ascontiguousarray(tau)).to(device)
     d_bt = torch.from_numpy(background_table(aexp_out, tau, param)).to(device)
     fields = torch.empty((len(SRC_FIELDS), K, T), **f64)
-    scratch = torch.empty((K, T), **f64)
     stream = torch.cuda.current_stream(device).cuda_stream
-    rc = lib.discoeb_sources(dc.struct.data_ptr(), ctypes.byref(dc.host), K, d_k.data_ptr(), T, d_tau.data_ptr(),
-                             d_bt.data_ptr(), y.data_ptr(), fields.data_ptr(), scratch.data_ptr(), stream)
+    if no_alloc:
+        rc = lib.discoeb_sources_noalloc(dc.struct.data_ptr(), ctypes.byref(dc.host), K, d_k.data_ptr(), T,
+                                         d_tau.data_ptr(), d_bt.data_ptr(), y.data_ptr(), fields.data_ptr(), stream)
+    else:
+        scratch = torch.empty((K, T), **f64)
+        rc = lib.discoeb_sources(dc.struct.data_ptr(), ctypes.byref(dc.host), K, d_k.data_ptr(), T, d_tau.data_ptr(),
+                                 d_bt.data_ptr(), y.data_ptr(), fields.data_ptr(), scratch.data_ptr(), stream)
     if rc != 0:
         raise RuntimeError(f"discoeb_sources failed with code {rc}")
     return {name: fields[i] for i, name in enumerate(SRC_FIELDS)}

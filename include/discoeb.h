@@ -193,6 +193,15 @@ int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo
                         const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
                         const double* y_full, double* fields, double* scratch, void* stream);
 
+/* discoeb_sources without a caller scratch buffer and without any allocation: the scratch is a
+ * module-static device array of 2^20 doubles (8 MiB) per device, so n_modes * n_tau must be
+ * <= 1048576 (else DISCOEB_EINVAL).  Calls that overlap in time on one device (two streams, two
+ * host threads) race on that array: serialise them.  No counterpart in the reference (it is a
+ * no-allocation variant for callers that cannot provide workspace). */
+int32_t discoeb_sources_noalloc(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_modes,
+                                const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
+                                const double* y_full, double* fields, void* stream);
+
 /* Workspace bytes of discoeb_los for these sizes (< 0: invalid sizes or a cuFFT error). */
 int64_t discoeb_los_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
                                     int32_t n_k_dense);

@@ -1,0 +1,49 @@
+"""discoeb_sources_noalloc (library-static scratch) against discoeb_sources (caller scratch).
+
+Collected last so that it also runs after every other GPU test in the same process; it passes
+alone as well.  Two calls in a row through the no-allocation entry must both reproduce the
+caller-scratch entry exactly (same kernels, the static scratch is fully written before read).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import background
+
+pytestmark = pytest.mark.gpu
+
+L11 = dict(lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3)
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.fail("no CUDA device: the -m gpu tests need a GPU")
+    return torch
+
+
+def test_noalloc_sources_equal_caller_scratch_twice(torch_cuda):
+    from discoeb_b200.cmb import cmb_aexp_out, compute_sources
+    from discoeb_b200.perturbations import solve_modes
+    bg = background("disco_notebook", 1024)
+    a = cmb_aexp_out()
+    tau = bg["tau_of_a_spline"].evaluate(a)
+    ks = np.geomspace(1e-3, 0.3, 10)
+    y = solve_modes(param=bg, kmodes=ks, tau_out=tau, rtol=1e-4, atol=1e-4, pcoeff=0.25, icoeff=0.8, dcoeff=0.0,
+                    factormax=20.0, factormin=0.3, max_steps=4096, return_full=True, as_tensor=True, **L11)
+    ref = compute_sources(param=bg, yout=y, kmodes=ks, aexp_out=a, **L11)
+    for _ in range(2):
+        got = compute_sources(param=bg, yout=y, kmodes=ks, aexp_out=a, no_alloc=True, **L11)
+        for name in ("S", "S1", "S2", "alphaprime", "polarization_term"):
+            np.testing.assert_array_equal(got[name].cpu().numpy(), ref[name].cpu().numpy())
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch(torch_cuda):
+    from discoeb_b200 import _abi
+    lib = _abi.lib()
+    c = _abi.DiscoebCosmo()
+    # 2^20 + 1 points: rejected before any device work (null pointers are never touched)
+    rc = lib.discoeb_sources_noalloc(None, ctypes.byref(c), 1025, None, 1024, None, None, None, None, None)
+    assert rc == -1
