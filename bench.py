@@ -182,6 +182,77 @@ def fp64_peak_tflops(torch, device):
     return best
 
 
+def run_cmb(args, rank, world, local):
+    """C_l^TT of one cosmology at the reference's compute_Cell_spectrum_from_cosmo_params defaults
+    (128 camb-sampled modes, lmax 11/11/11/8/3, 320 output times, rtol = atol = 1e-4, 8192 dense k,
+    16384 FFTLog points, l <= 2500), DISCO-Notebook cosmology.  Device stages timed with CUDA events
+    (full solve, sources, line of sight, C_l); e2e = the public call with the host background."""
+    import torch
+
+    from discoeb_b200 import cmb
+    from discoeb_b200.perturbations import solve_modes, k_sampling
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    p = {"Omegam": 0.3099, "Omegab": 0.0488911, "H0": 67.742, "n_s": 0.96822, "A_s": 2.1064e-09, "mnu": 0.06,
+         "Tcmb": 2.7255, "YHe": 0.248, "Neff": 2.046, "Nmnu": 1, "w_DE_0": -0.99, "w_DE_a": 0.0, "cs2_DE": 1.0,
+         "Omegak": 0.0, "k_p": 0.05}
+    from discoeb_b200.background import evolve_background
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        bg = evolve_background(param=dict(p), num_thermo=1024)
+    L = dict(lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3)
+    a = cmb.cmb_aexp_out()
+    ks = k_sampling(bg, 1e-4, 1.0, 128, "camb")
+    tau = bg["tau_of_a_spline"].evaluate(a)
+    tau0 = float(bg["tau_of_a_spline"].evaluate(1.0))
+    stream = torch.cuda.current_stream(device)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def stages():
+        e = [ev() for _ in range(5)]
+        e[0].record(stream)
+        y = solve_modes(param=bg, kmodes=ks, tau_out=tau, rtol=1e-4, atol=1e-4, pcoeff=0.25, icoeff=0.8,
+                        dcoeff=0.0, factormax=20.0, factormin=0.3, max_steps=2048, return_full=True, as_tensor=True,
+                        device=device, **L)
+        e[1].record(stream)
+        src = cmb.compute_sources(param=bg, yout=y, kmodes=ks, aexp_out=a, device=device, **L)
+        e[2].record(stream)
+        th, kk = cmb.compute_theta_ell(2500, ks, tau, src["S"], tau0, n_fftlog=16384, n_k_dense=8192, device=device)
+        e[3].record(stream)
+        cmb.compute_Cell(th, kk, bg["n_s"], bg["k_p"], device=device)
+        e[4].record(stream)
+        e[4].synchronize()
+        return [e[i].elapsed_time(e[i + 1]) for i in range(4)]
+
+    for _ in range(args.warmup):
+        stages()
+    with ClockSampler(local) as clk:
+        times = [stages() for _ in range(args.steps)]
+    per = np.mean(np.array(times), axis=0)
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            cmb.compute_Cell_spectrum_from_cosmo_params(dict(p), device=device)
+        if i >= args.warmup:
+            e2e.append(time.perf_counter() - t0)
+    if rank == 0:
+        ms = float(per.sum())
+        print(json.dumps({
+            "metric": "C_l^TT pipeline of one cosmology (compute_Cell_spectrum_from_cosmo_params defaults)",
+            "value": 1e3 / ms, "unit": "spectra/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "dtype": "f64", "data": "synthetic (DISCO-Notebook cosmology)",
+            "config": {"workload": "cmb_tt_disco_notebook_k128_l2500", "num_k": 128, "n_tau": 320, "n_k_dense": 8192,
+                       "n_fftlog": 16384, "ellmax": 2500},
+            "stages_ms": {"full_solve": per[0], "sources": per[1], "line_of_sight": per[2], "cell": per[3]},
+            "e2e": {"value": 1.0 / statistics.mean(e2e), "unit": "spectra/s", "ms_per_cosmology":
+                    1e3 * statistics.mean(e2e)},
+            "clocks": clk.summary(),
+        }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -189,7 +260,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pk_lcdm_mnu_k512_z4")
-    ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward"])
+    ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward", "cmb"])
     ap.add_argument("--ref-sample", type=int, default=24)
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -201,6 +272,9 @@ def main():
     local = _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.mode == "cmb":
+        run_cmb(args, rank, world, local)
         return
 
     import ctypes
