@@ -57,7 +57,8 @@ __device__ void emit_output(const WarpTeam& tm, const DiscoebCosmo& P, const Dim
 }
 
 __global__ void __launch_bounds__(256) fwd_structured_kernel(
-    const DiscoebCosmo* __restrict__ cosmos, const int32_t* __restrict__ mode_cosmo, DiscoebControl ctrl, int n_modes,
+    const DiscoebCosmo* __restrict__ cosmos, int n_cosmo, const int32_t* __restrict__ mode_cosmo, DiscoebControl ctrl,
+    int n_modes,
     const double* __restrict__ kmodes, const double* __restrict__ tau_start, const double* __restrict__ y0,
     const double* __restrict__ sw, int n_out, const double* __restrict__ tau_out, int mem_doubles, double* y_full,
     double* y_out20, int32_t* status, int32_t* nsteps)
@@ -70,35 +71,56 @@ __global__ void __launch_bounds__(256) fwd_structured_kernel(
     DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(base);
     double* wmem = base + kCosmoDoubles;
     const int total_warps = gridDim.x * wpb;
+    const int n0 = (mem_doubles - 4 * kMaxSlots - 32) / 23;  // state size of the launch (mode_mem_doubles)
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+    // outputs never reached are filled with NaN so that they cannot pass for data
+    auto fill_nan = [&](int mode, int from) {
+        for (int j = from; j < n_out; ++j) {
+            const size_t o = (size_t)mode * n_out + j;
+            if (y_full) for (int i = tm.lane; i < n0; i += 32) y_full[o * n0 + i] = qnan;
+            if (y_out20) for (int i = tm.lane; i < 20; i += 32) y_out20[o * 20 + i] = qnan;
+        }
+    };
     int cur_cosmo = -1;
     for (int mode = blockIdx.x * wpb + warp; mode < n_modes; mode += total_warps) {
         const int ci = mode_cosmo ? mode_cosmo[mode] : 0;
+        if (ci < 0 || ci >= n_cosmo) {  // invalid cosmology index: report, solve nothing
+            fill_nan(mode, 0);
+            if (tm.leader()) {
+                status[mode] = DISCOEB_BAD_INDEX;
+                nsteps[mode] = 0;
+            }
+            continue;
+        }
         if (ci != cur_cosmo) {
             copy_cosmo(tm, cosmos + ci, P);
             cur_cosmo = ci;
         }
         const Dims D = make_dims(*P);
         const int n = D.n;
+        if (mode_mem_doubles(D) != mem_doubles) {  // every cosmology must have the sizes of the first
+            fill_nan(mode, 0);
+            if (tm.leader()) {
+                status[mode] = DISCOEB_BAD_INDEX;
+                nsteps[mode] = 0;
+            }
+            continue;
+        }
         ModeMem M = carve(wmem, D);
         const double k = kmodes[mode];
         for (int i = tm.lane; i < n; i += 32) M.y[i] = y0[(size_t)mode * n + i];
         double swm[3] = {sw[3 * mode], sw[3 * mode + 1], sw[3 * mode + 2]};
         tm.sync();
         const size_t obase = (size_t)mode * n_out;
+        const double* tout = tau_out + (size_t)ci * n_out;  // this cosmology's output times
         auto emit = [&](int j, const double* y, int) {
             const size_t o = obase + j;
-            emit_output(tm, *P, D, k, tau_out[j], y, y_full ? y_full + o * n : nullptr,
+            emit_output(tm, *P, D, k, tout[j], y, y_full ? y_full + o * n : nullptr,
                         y_out20 ? y_out20 + o * 20 : nullptr, M.f);
         };
-        const SolveResult R = solve_mode(tm, *P, D, ctrl, k, tau_start[mode], swm, n_out, tau_out, M, emit);
+        const SolveResult R = solve_mode(tm, *P, D, ctrl, k, tau_start[mode], swm, n_out, tout, M, emit);
         const int st = R.status, steps = R.steps;
-        // outputs never reached are filled with NaN so that they cannot pass for data
-        const double qnan = __longlong_as_double(0x7ff8000000000000LL);
-        for (int j = R.outputs; j < n_out; ++j) {
-            const size_t o = obase + j;
-            if (y_full) for (int i = tm.lane; i < n; i += 32) y_full[o * n + i] = qnan;
-            if (y_out20) for (int i = tm.lane; i < 20; i += 32) y_out20[o * 20 + i] = qnan;
-        }
+        fill_nan(mode, R.outputs);
         if (tm.leader()) {
             status[mode] = st;
             nsteps[mode] = steps;
@@ -266,9 +288,9 @@ int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
         return DISCOEB_ECUDA;
     int blocks = (n_modes + wpb - 1) / wpb;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    fwd_structured_kernel<<<blocks, 32 * wpb, smem, s>>>(cosmos_dev, mode_cosmo, *ctrl, n_modes, kmodes, tau_start,
-                                                          y0, switch_tau, n_out, tau_out, mem, y_full, y_out20, status,
-                                                          nsteps);
+    fwd_structured_kernel<<<blocks, 32 * wpb, smem, s>>>(cosmos_dev, n_cosmo, mode_cosmo, *ctrl, n_modes, kmodes,
+                                                          tau_start, y0, switch_tau, n_out, tau_out, mem, y_full,
+                                                          y_out20, status, nsteps);
     (void)n_sm;
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }

@@ -20,7 +20,8 @@ METHOD_RODAS5_STRUCTURED = 0
 METHOD_RODAS5_DENSE = 1
 METHOD_RODAS5_DENSE_MIXED = 2
 
-STATUS_NAMES = {0: "ok", 1: "max_steps exceeded", 2: "non-finite state", 3: "step size underflow", 4: "singular"}
+STATUS_NAMES = {0: "ok", 1: "max_steps exceeded", 2: "non-finite state", 3: "step size underflow", 4: "singular",
+                5: "cosmology index out of range"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)

@@ -390,3 +390,119 @@ def compute_time_derivatives(yout, tau, kmodes, param, lmaxg, lmaxgp, lmaxr, lma
     if rc != 0:
         raise RuntimeError(f"discoeb_rhs failed with code {rc}")
     return d_f.cpu().numpy().reshape(K, T, n)
+
+
+class CosmologyBatch:
+    """Device-resident inputs of one discoeb_fwd launch over several cosmologies (the prologue of
+    solve_cosmologies); ``launch`` enqueues the kernel, ``result`` reads it back."""
+
+    def __init__(self, *, params, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, rtol, atol, pcoeff=0.25,
+                 icoeff=0.80, dcoeff=0.0, factormax=20.0, factormin=0.3, max_steps=100000, return_full=False,
+                 de_guard_eps=1e-9, device=None, warps_per_block=0):
+        import torch
+        if device is None:
+            if not torch.cuda.is_available():
+                raise RuntimeError("discoeb_b200 needs a CUDA device (there is no CPU path)")
+            device = torch.device("cuda", torch.cuda.current_device())
+        self.torch, self.device, self.lib = torch, device, _abi.lib()
+        C = len(params)
+        if C < 1:
+            raise ValueError("params must hold at least one cosmology")
+        aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
+        km = np.asarray(kmodes, dtype=np.float64)
+        km = np.broadcast_to(km, (C, km.shape[-1])) if km.ndim == 1 else km
+        K, nout, n = km.shape[1], aexp_out.shape[0], nvar_of(lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax)
+        L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
+        touts, ts, y0s, sws, self.dcs = [], [], [], [], []
+        for c, p in enumerate(params):
+            tout = p["tau_of_a_spline"].evaluate(aexp_out)
+            if np.any(np.diff(tout) <= 0):
+                raise ValueError("aexp_out must map to strictly increasing output times")
+            t0 = 0.99 * np.minimum(tout.min(), determine_starting_time(param=p, k=km[c]))
+            touts.append(tout)
+            ts.append(t0)
+            y0s.append(adiabatic_ics(tau=t0, param=p, kmode=km[c], **L))
+            sws.append(approximation_switch_times(p, km[c]))
+            self.dcs.append(DeviceCosmo(p, de_guard_eps=de_guard_eps, device=device, **L))
+        self.C, self.K, self.nout, self.n, self.return_full = C, K, nout, n, return_full
+        self.flat_k = km.reshape(-1)
+        cidx = np.repeat(np.arange(C, dtype=np.int32), K)
+        order = np.argsort(-self.flat_k, kind="stable")  # longest modes first across all cosmologies
+        self.inv = np.empty_like(order)
+        self.inv[order] = np.arange(C * K)
+        raw = b"".join(bytes(ctypes.string_at(ctypes.addressof(d.host), ctypes.sizeof(d.host))) for d in self.dcs)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+        self.d_cosmos = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(device)
+        self.d_k, self.d_mc = t(self.flat_k[order]), t(cidx[order])
+        self.d_ts, self.d_y0 = t(np.concatenate(ts)[order]), t(np.concatenate(y0s)[order])
+        self.d_sw, self.d_tout = t(np.concatenate(sws)[order]), t(np.stack(touts))
+        f64 = dict(dtype=torch.float64, device=device)
+        M = C * K
+        self.d_full = torch.empty((M, nout, n), **f64) if return_full else None
+        self.d_out20 = None if return_full else torch.empty((M, nout, 20), **f64)
+        self.d_stat = torch.empty((2, M), dtype=torch.int32, device=device)
+        self.ctrl = _abi.DiscoebControl(rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin, int(max_steps),
+                                        _abi.METHOD_RODAS5_STRUCTURED, int(warps_per_block), 0)
+        self.h2d_bytes = sum(x.numel() * x.element_size() for x in (self.d_cosmos, self.d_k, self.d_mc, self.d_ts,
+                                                                   self.d_y0, self.d_sw, self.d_tout))
+        self.h2d_bytes += sum(sum(x.numel() * 8 for x in d.tensors) for d in self.dcs)
+
+    def launch(self):
+        f = self.d_full, self.d_out20
+        rc = self.lib.discoeb_fwd(self.d_cosmos.data_ptr(), ctypes.byref(self.dcs[0].host), self.C,
+                                  ctypes.byref(self.ctrl), self.C * self.K, self.d_mc.data_ptr(), self.d_k.data_ptr(),
+                                  self.d_ts.data_ptr(), self.d_y0.data_ptr(), self.d_sw.data_ptr(), self.nout,
+                                  self.d_tout.data_ptr(), f[0].data_ptr() if f[0] is not None else None,
+                                  f[1].data_ptr() if f[1] is not None else None, self.d_stat[0].data_ptr(),
+                                  self.d_stat[1].data_ptr(), self.torch.cuda.current_stream(self.device).cuda_stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_fwd failed with code {rc}")
+
+    def result(self, on_failure="raise"):
+        out = (self.d_full if self.return_full else self.d_out20).cpu().numpy()[self.inv]
+        stat = self.d_stat.cpu().numpy()[:, self.inv]
+        _check_status(stat[0], stat[1], self.flat_k, on_failure)
+        return out.reshape(self.C, self.K, self.nout, -1), stat[0].reshape(self.C, self.K), \
+            stat[1].reshape(self.C, self.K)
+
+
+def solve_cosmologies(*, params, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, rtol, atol, pcoeff=0.25,
+                      icoeff=0.80, dcoeff=0.0, factormax=20.0, factormin=0.3, max_steps=100000, return_full=False,
+                      de_guard_eps=1e-9, device=None, warps_per_block=0, on_failure="raise", return_stats=False):
+    """Forward solve of the k-modes of several cosmologies in ONE launch (what ``jax.vmap`` over
+    cosmologies of the reference's ``evolve_perturbations`` computes).
+
+    ``params``: list of C background dicts (``evolve_background`` outputs) with the same l_max /
+    nqmax; ``kmodes``: ``[K]`` shared or ``[C, K]``; ``aexp_out``: ``[nout]`` scale factors (each
+    cosmology's own output times).  Returns ``y [C, K, nout, 20]`` (or ``[C, K, nout, nvar]``).
+    """
+    b = CosmologyBatch(params=params, kmodes=kmodes, aexp_out=aexp_out, lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr,
+                       lmaxnu=lmaxnu, nqmax=nqmax, rtol=rtol, atol=atol, pcoeff=pcoeff, icoeff=icoeff, dcoeff=dcoeff,
+                       factormax=factormax, factormin=factormin, max_steps=max_steps, return_full=return_full,
+                       de_guard_eps=de_guard_eps, device=device, warps_per_block=warps_per_block)
+    b.launch()
+    y, status, nsteps = b.result(on_failure)
+    if return_stats:
+        return y, status, nsteps
+    return y
+
+
+def _background_worker(p):
+    import warnings
+    from .background import evolve_background
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        return evolve_background(param=p)
+
+
+def backgrounds(param_dicts, processes=None):
+    """evolve_background of many cosmologies on the host, in a process pool (spawned, so that
+    it is safe to call after CUDA is initialised) when there is more than one."""
+    param_dicts = list(param_dicts)
+    if len(param_dicts) <= 1 or processes == 1:
+        return [_background_worker(p) for p in param_dicts]
+    import multiprocessing as mp
+    import os
+    nproc = processes or min(len(param_dicts), os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(nproc) as pool:
+        return pool.map(_background_worker, param_dicts)

@@ -59,3 +59,23 @@ def workload(name):
     w["param"] = cosmo_params(**w.pop("cosmo"))
     w["theta"] = dict(_THETA_LCDM, **w["theta"])
     return w
+
+
+# the uneven-batch box: theta ranges of the many-cosmology workload
+THETA_BOX = {"omega_c": (0.10, 0.14), "omega_b": (0.020, 0.025), "h": (0.60, 0.76), "n_s": (0.92, 1.00),
+             "ln10As": (2.9, 3.2), "w0": (-1.3, -0.7), "wa": (-0.5, 0.5), "m_nu": (0.02, 0.3)}
+
+
+def sample_thetas(n, seed=0):
+    """n cosmologies drawn uniformly from THETA_BOX with numpy's default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    names = list(THETA_BOX)
+    u = rng.uniform(size=(n, len(names)))
+    return [{nm: THETA_BOX[nm][0] + (THETA_BOX[nm][1] - THETA_BOX[nm][0]) * u[i, j] for j, nm in enumerate(names)}
+            for i in range(n)]
+
+
+def crosses_phantom_divide(theta):
+    """Whether w(a) = w0 + wa (1 - a) equals -1 for some a in (0, 1]."""
+    w_early, w_today = theta["w0"] + theta["wa"], theta["w0"]
+    return (w_early + 1.0) * (w_today + 1.0) <= 0.0

@@ -83,6 +83,8 @@ typedef struct {
 #define DISCOEB_NONFINITE 2
 #define DISCOEB_DT_UNDERFLOW 3
 #define DISCOEB_SINGULAR 4
+#define DISCOEB_BAD_INDEX 5 /* mode_cosmo[mode] outside [0, n_cosmo), or that cosmology's l_max / nq
+                              * differ from cosmos[0]'s: the mode was not solved */
 
 /* return codes of the entry points */
 #define DISCOEB_SUCCESS 0
@@ -97,18 +99,21 @@ int32_t discoeb_abi_version(void);
 int32_t discoeb_nvar(const DiscoebCosmo* cosmo);
 
 /* Forward solve of n_modes k-modes.
- *   cosmos[n_cosmo]        device array of DiscoebCosmo (tables inside are device pointers)
+ *   cosmos[n_cosmo]        device array of DiscoebCosmo (tables inside are device pointers); all
+ *                          with the l_max / nqmax of cosmo0_host (a host copy of cosmos[0])
  *   mode_cosmo[n_modes]    cosmology index per mode (NULL: all 0)
  *   kmodes, tau_start      [n_modes]
  *   y0                     [n_modes, nvar]   initial states (adiabatic ICs)
  *   switch_tau             [n_modes, 3]      times where RSA starts, UFA starts, TCA ends
  *                                            (+inf when never); steps end exactly there
- *   tau_out                [n_out] increasing output times (shared by all modes)
+ *   tau_out                [n_cosmo, n_out] increasing output times of each cosmology (a row per
+ *                          cosmology: the same scale factors map to different times)
  *   y_full                 [n_modes, n_out, nvar] state at tau_out after the RSA projection
  *                          (may be NULL)
  *   y_out20                [n_modes, n_out, 20] output fields (may be NULL)
  *   status, nsteps         [n_modes] per-mode status code and number of step attempts
- * All modes of all cosmologies run in one launch. */
+ * All modes of all cosmologies run in one launch (jax.vmap over cosmologies of the reference's
+ * evolve_perturbations maps onto n_cosmo / mode_cosmo). */
 int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
                     const DiscoebControl* ctrl, int32_t n_modes, const int32_t* mode_cosmo,
                     const double* kmodes, const double* tau_start, const double* y0,
