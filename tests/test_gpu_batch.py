@@ -60,10 +60,11 @@ def test_gpu_bad_cosmology_index_is_reported(torch_cuda):
     stat = torch.zeros((2, 2), dtype=torch.int32, device="cuda")
     mc = f(np.array([0, 7], dtype=np.int32))  # the second mode names a cosmology that does not exist
     ctrl = _abi.DiscoebControl(1e-5, 1e-8, 0.25, 0.8, 0.0, 20.0, 0.3, 100000, 0, 0, 0)
+    # keep every device input referenced until the kernel has finished
+    d_k, d_t0, d_sw, d_tout = f(ks), f(t0), f(approximation_switch_times(bg, ks)), f(tout)
     rc = _abi.lib().discoeb_fwd(dc.struct.data_ptr(), ctypes.byref(dc.host), 1, ctypes.byref(ctrl), 2, mc.data_ptr(),
-                                f(ks).data_ptr(), f(t0).data_ptr(), y0.data_ptr(),
-                                f(approximation_switch_times(bg, ks)).data_ptr(), 1, f(tout).data_ptr(), None,
-                                out.data_ptr(), stat[0].data_ptr(), stat[1].data_ptr(),
+                                d_k.data_ptr(), d_t0.data_ptr(), y0.data_ptr(), d_sw.data_ptr(), 1,
+                                d_tout.data_ptr(), None, out.data_ptr(), stat[0].data_ptr(), stat[1].data_ptr(),
                                 torch.cuda.current_stream().cuda_stream)
     assert rc == 0
     s = stat.cpu().numpy()
