@@ -525,15 +525,19 @@ cublasHandle_t blas_handle(int dev)
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
-// Scratch of discoeb_sources_noalloc: one module-static device array per device (8 MiB), so that
-// the call makes no allocation.  It holds the per-mode spline recurrence of the ISW term, which is
-// written before it is read, so nothing has to be cleared between calls.
+// Scratch of discoeb_sources_noalloc, for callers that cannot allocate device memory: one
+// file-scope device array (8 MiB) that every GPU loading the library holds until exit, so the
+// call itself allocates nothing.  It holds the per-mode spline recurrence of the ISW term, which
+// is written before it is read, so nothing has to be cleared between calls; calls overlapping on
+// the GPU share it and race.  Host code must not pass the symbol itself to a kernel (on the host
+// it names a stand-in, not device memory): noalloc_scratch() looks up the device address.
 constexpr long long kNoAllocScratchDoubles = 1LL << 20;
-__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[64] = {};
 
-// device address of g_noalloc_scratch on the current device, looked up once per device
+// device address of g_noalloc_scratch on the current device, looked up once per device (on the
+// first no-allocation call made with that device current)
 double* noalloc_scratch(int dev)
 {
     if (dev < 0 || dev >= 64) return nullptr;

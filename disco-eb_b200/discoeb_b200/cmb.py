@@ -68,8 +68,9 @@ def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmax
 
     ``yout``: the RSA-projected full states ``[K, n_tau, nvar]`` at ``tau(aexp_out)`` (numpy or
     a device tensor).  Returns a dict of device tensors ``[K, n_tau]`` keyed by SRC_FIELDS.
-    ``no_alloc``: use discoeb_sources_noalloc (library-static scratch, K * n_tau <= 2^20; calls
-    must not overlap in time on one device).
+    ``no_alloc``: use discoeb_sources_noalloc, which needs no scratch buffer from the caller (for
+    callers that cannot allocate device memory; the library's own 8 MiB array limits
+    K * n_tau to 2^20, and calls must not overlap on one device).
     """
     torch, device = _device(device)
     lib = _abi.lib()
@@ -84,6 +85,8 @@ def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmax
     y = y.to(**f64).contiguous()
     if y.shape[:2] != (K, T):
         raise ValueError(f"yout must have shape [{K}, {T}, nvar], got {tuple(y.shape)}")
+    if no_alloc and K * T > (1 << 20):
+        raise ValueError(f"no_alloc: {K} modes x {T} times exceeds the 2^20 points of the library's scratch")
     d_k = torch.from_numpy(kmodes).to(device)
     d_tau = torch.from_numpy(np.ascontiguousarray(tau)).to(device)
     d_bt = torch.from_numpy(background_table(aexp_out, tau, param)).to(device)

@@ -198,11 +198,18 @@ int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo
                         const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
                         const double* y_full, double* fields, double* scratch, void* stream);
 
-/* discoeb_sources without a caller scratch buffer and without any allocation: the scratch is a
- * module-static device array of 2^20 doubles (8 MiB) per device, so n_modes * n_tau must be
- * <= 1048576 (else DISCOEB_EINVAL).  Calls that overlap in time on one device (two streams, two
- * host threads) race on that array: serialise them.  No counterpart in the reference (it is a
- * no-allocation variant for callers that cannot provide workspace). */
+/* discoeb_sources for callers that cannot allocate device memory: code running where another
+ * framework owns the GPU's memory (XLA preallocates most of it, so an FFI handler that was given
+ * no workspace buffer has nothing to pass as scratch and must not cudaMalloc behind the
+ * framework's back), or a real-time host loop where allocation is not allowed.  It takes the
+ * arguments of discoeb_sources without `scratch` and allocates nothing: its scratch is a
+ * file-scope device array of 2^20 doubles (8 MiB) that the library holds on every GPU that loads
+ * it, until the process exits.  Limit: n_modes * n_tau <= 1048576, else DISCOEB_EINVAL and no
+ * work.  The first call on a device looks up the array's device address (cudaGetSymbolAddress,
+ * with that device current); make that first call before any stream capture.  Every call shares
+ * the array, so calls that overlap on the GPU (two streams, two host threads) race: serialise
+ * them.  Nothing in the array has to start at zero (it is written before it is read).  No
+ * counterpart in the reference. */
 int32_t discoeb_sources_noalloc(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_modes,
                                 const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
                                 const double* y_full, double* fields, void* stream);

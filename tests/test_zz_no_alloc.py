@@ -1,8 +1,12 @@
-"""discoeb_sources_noalloc (library-static scratch) against discoeb_sources (caller scratch).
+"""discoeb_sources_noalloc against discoeb_sources.
 
-Collected last so that it also runs after every other GPU test in the same process; it passes
-alone as well.  Two calls in a row through the no-allocation entry must both reproduce the
-caller-scratch entry exactly (same kernels, the static scratch is fully written before read).
+The no-allocation entry serves callers that cannot allocate device memory (a framework that
+owns the GPU's memory, a host loop where allocation is not allowed): it keeps its scratch in an
+array the library holds on the GPU instead of a buffer from the caller.  Two calls in a row
+through it, via the C ABI, must both reproduce the caller-scratch entry exactly (same kernels;
+the shared array is written before it is read, so the first call leaves nothing that changes
+the second).  Collected last, so that a run stopping at the first failure has run every other
+test; it passes alone in a fresh process as well.
 """
 import ctypes
 
