@@ -315,6 +315,7 @@ def main():
     ap.add_argument("--workload", default="pk_lcdm_mnu_k512_z4")
     ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward", "cmb", "batch"])
     ap.add_argument("--n-cosmo", type=int, default=64, help="cosmologies per launch in --mode batch")
+    ap.add_argument("--wpb", type=int, default=0, help="warps (modes) per block; 0 = the library default")
     ap.add_argument("--ref-sample", type=int, default=24)
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -378,7 +379,7 @@ def main():
     d_out = torch.empty((K, nout, 20), **f64)
     d_stat = torch.empty((2, K), dtype=torch.int32, device=device)
     ctrl = _abi.DiscoebControl(w["rtol"], w["atol"], 0.25, 0.80, 0.0, 20.0, 0.3, 100000,
-                               _abi.METHOD_RODAS5_STRUCTURED, 0, 0)
+                               _abi.METHOD_RODAS5_STRUCTURED, args.wpb, 0)
     lib = _abi.lib()
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)  # > 126 MB L2
@@ -395,7 +396,7 @@ def main():
     if grad:
         from discoeb_b200.gradients import JacobianProblem, power_spectrum_jacobian
         prob = JacobianProblem(w["theta"], aexp_out=aout, kmodes=kmodes, rtol=w["rtol"], atol=w["atol"],
-                               max_steps=100000, device=device, **L)
+                               max_steps=100000, device=device, warps_per_block=args.wpb, **L)
         n_dir = len(prob.dirs)
         solve, stat_of = prob.launch, (lambda: prob.d_stat)
     else:
@@ -515,7 +516,8 @@ def main():
                        "n_s, ln10As, w0, wa, m_nu" if grad else None,
                        "rtol": w["rtol"], "atol": w["atol"], "method": "rodas5-structured",
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "ms_per_cosmology": ms, "step_attempts_per_mode_sum": step_attempts},
+                       "ms_per_cosmology": ms, "step_attempts_per_mode_sum": step_attempts,
+                       "warps_per_block": args.wpb or "default"},
             "e2e": {"value": world * K / (e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_cosmology": e2e},
             "gpu_launches": args.steps,
