@@ -278,7 +278,7 @@ int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
     int max_optin = 0, n_sm = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    int wpb = ctrl->warps_per_block > 0 ? ctrl->warps_per_block : 2;
+    int wpb = ctrl->warps_per_block > 0 ? ctrl->warps_per_block : 1;  // one mode per block: the most resident warps
     if (wpb > 8) wpb = 8;
     while (wpb > 1 && per_warp * wpb > (size_t)max_optin) --wpb;
     if (per_warp > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
@@ -317,7 +317,7 @@ int32_t discoeb_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_hos
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
     int max_optin = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    int wpb = ctrl->warps_per_block > 0 ? ctrl->warps_per_block : 2;
+    int wpb = ctrl->warps_per_block > 0 ? ctrl->warps_per_block : 1;  // one mode per block: the most resident warps
     if (wpb > 8) wpb = 8;
     while (wpb > 1 && per_warp * wpb > (size_t)max_optin) --wpb;
     if (per_warp > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;

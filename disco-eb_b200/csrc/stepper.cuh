@@ -105,12 +105,12 @@ DHD ModeMem carve(double* base, const Dims& D)
 // scalar slots
 enum { SC_W00 = 0, SC_ETAC = 1, SC_CINV = 2, SC_F1Z = 11, SC_F1U = 14 };
 
-// tangent workspace: y', the stage state tangent u', two n-vector scratches and the 8 stage
-// tangents K'
+// tangent workspace: y', the stage state tangent u', two n-vector scratches, d/de of the
+// Jacobian column d f/d a, and the 8 stage tangents K'
 struct TanMem {
-    double *yd, *ud, *fd, *jk, *Kd;
+    double *yd, *ud, *fd, *jk, *c0d, *Kd;
 };
-DHD int tan_mem_doubles(const Dims& D) { return 12 * D.n; }
+DHD int tan_mem_doubles(const Dims& D) { return 13 * D.n; }
 DHD TanMem carve_tan(double* base, const Dims& D)
 {
     const int n = D.n;
@@ -119,7 +119,8 @@ DHD TanMem carve_tan(double* base, const Dims& D)
     t.ud = t.yd + n;
     t.fd = t.ud + n;
     t.jk = t.fd + n;
-    t.Kd = t.jk + n;
+    t.c0d = t.jk + n;
+    t.Kd = t.c0d + n;
     return t;
 }
 
@@ -504,12 +505,16 @@ struct SolveResult {
 // Tangent of stage s of the Rosenbrock step along one parameter direction: with
 // k_s = W^{-1} r_s, the derivative is k_s' = W^{-1} (r_s' + J' k_s), where r_s' holds the
 // directional derivative of f at the stage state (state tangent u_s' and the parameter /
-// table tangents tn) and J' k_s = d/de [J(y_n + e y_n', p + e p') k_s] is one hyper-dual RHS
-// evaluation.  The step sizes are the forward solve's (the derivative of the discrete scheme
-// with the accepted step sequence held fixed).
+// table tangents tn) and J' k_s = d/de [J(y_n + e y_n', p + e p') k_s].  Rows >= 1 of f are
+// linear and homogeneous in y[1:] with coefficients that depend on a (through the background)
+// and the parameters, so the columns >= 1 of J' applied to k_s are the e-part of f evaluated at
+// the state k_s with the dual background bj of the step start; column 0 contributes
+// k_s[0] d/de(d f/d a), computed once per step into c0d.  The step sizes are the forward solve's
+// (the derivative of the discrete scheme with the accepted step sequence held fixed).
 template <class TM>
 DDV void tangent_stage(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
-                       const ModeMem& M, const TanMem& TT, const DiscoebTangent* tn, int s, int& hint)
+                       const ModeMem& M, const TanMem& TT, const DiscoebTangent* tn, const Bg<Dual>& bj, int s,
+                       int& hint)
 {
     const int n = D.n;
     const double* us = (s == 0) ? M.y : M.u;
@@ -532,10 +537,11 @@ DDV void tangent_stage(const TM& tm, const DiscoebCosmo& P, const Dims& D, doubl
         rhs_team(tm, P, D, bt, k, ts, us, TT.fd, (double*)nullptr, TT.ud, (const double*)nullptr, 1, 1);
     }
     const double* Ks = M.K + s * n;
+    rhs_team(tm, P, D, bj, k, t, Ks, TT.jk, (double*)nullptr, (const double*)nullptr, (const double*)nullptr, 1, 1);
+    tm.sync();
     {
-        Bg<HDual> bh;
-        bg_eval_team(tm, P, HDual(Dual(M.y[0], TT.yd[0]), Dual(Ks[0], 0.0)), t, k, regime, bh, hint, tn);
-        rhs_team(tm, P, D, bh, k, t, M.y, TT.jk, (double*)nullptr, TT.yd, Ks, 3, 3);
+        const double k0 = Ks[0];
+        for (int i = tm.lane; i < n; i += tm.nl) TT.jk[i] = (i == 0 ? 0.0 : TT.jk[i]) + k0 * TT.c0d[i];
     }
     tm.sync();
     Bg<double> b0;
@@ -565,11 +571,20 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
     Bg<Dual> bd;
     bg_eval_team(tm, P, Dual(M.y[0], 1.0), t, k, regime, bd, hint);
     rhs_team(tm, P, D, bd, k, t, M.y, M.f, M.col0);
-    Bg<double> b;
-    bg_eval_team(tm, P, M.y[0], t, k, regime, b, hint);
+    const Bg<double> b = bg_value(bd);
     for (int i = tm.lane; i < n; i += tm.nl) M.dT[i] = dtau_row(D, b, t, i, M.y);
     tm.sync();
     const bool ok = factor_W(tm, P, D, b, k, t, h, M);
+    // tangent, once per step: the background at the step start with its derivative along the
+    // direction, and d/de of the Jacobian column d f / d a (see tangent_stage)
+    Bg<Dual> bj;
+    if (TT) {
+        bg_eval_team(tm, P, Dual(M.y[0], TT->yd[0]), t, k, regime, bj, hint, tn);
+        Bg<HDual> bh;
+        bg_eval_team(tm, P, HDual(Dual(M.y[0], TT->yd[0]), Dual(1.0, 0.0)), t, k, regime, bh, hint, tn);
+        rhs_team(tm, P, D, bh, k, t, M.y, TT->c0d, (double*)nullptr, TT->yd, (const double*)nullptr, 3, 3);
+        tm.sync();
+    }
     const double ih = 1.0 / h;
     for (int s = 0; s < 8; ++s) {
         double* Ks = M.K + s * n;
@@ -599,7 +614,7 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
         }
         tm.sync();
         solve_W(tm, D, M, h, Ks);
-        if (TT) tangent_stage(tm, P, D, k, t, h, regime, M, *TT, tn, s, hint);
+        if (TT) tangent_stage(tm, P, D, k, t, h, regime, M, *TT, tn, bj, s, hint);
     }
     return ok;
 }
