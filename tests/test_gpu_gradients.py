@@ -43,8 +43,11 @@ def test_gpu_jvp_values_match_forward_solve(torch_cuda):
     P, J, status, nsteps = prob.result()
     assert (status == 0).all()
     P_fwd, _ = _power(THETA, prob.kmodes, A4, rtol=1e-5, atol=1e-8, max_steps=100000)
-    # same algorithm and step sequence: the value part of the tangent solve is the forward solve
-    np.testing.assert_allclose(P, P_fwd, rtol=1e-9)
+    # same algorithm: the value part of the tangent solve is the forward solve.  The two kernels
+    # are compiled separately (their fused multiply-adds may differ in the last bit), and the
+    # step-size control can turn such a difference into a different accept decision, which moves
+    # the result by up to the solver tolerance (rtol 1e-5)
+    np.testing.assert_allclose(P, P_fwd, rtol=2e-5)
     assert np.isfinite(J).all()
 
 
@@ -71,7 +74,7 @@ def test_gpu_jacobian_matches_central_differences(torch_cuda):
     from discoeb_b200.perturbations import approximation_switch_times, determine_starting_time
     trace = {}
     P0, bg = _power(THETA, k, (0.5, 1.0), trace=trace, **solver)
-    np.testing.assert_allclose(P, P0, rtol=1e-9)
+    np.testing.assert_allclose(P, P0, rtol=1e-8)  # same algorithm, solver tolerance 1e-10
     tau_out = bg["tau_of_a_spline"].evaluate(np.array([0.5, 1.0]))
     fixed = dict(tau_start=0.99 * np.minimum(tau_out.min(), determine_starting_time(param=bg, k=k)),
                  switch_tau=approximation_switch_times(bg, k))
