@@ -130,13 +130,82 @@ __global__ void __launch_bounds__(256) fwd_structured_kernel(
 }
 
 constexpr int kTanDoubles = (sizeof(DiscoebTangent) + 7) / 8;
+constexpr int kMaxDirsPerBlock = 6;
 
-// Forward solve + tangent along one parameter direction per warp: warp w handles
-// (mode w / n_dir, direction w % n_dir).  The step sequence is chosen on the forward state
-// only, so the tangent is the derivative of the discrete solution with the accepted steps
-// held fixed (what forward-mode AD through the reference's diffrax loop computes).
-__global__ void __launch_bounds__(256) jvp_kernel(
-    const DiscoebCosmo* __restrict__ cosmo, const DiscoebTangent* __restrict__ tangents, int n_dir,
+// Output fields and their tangents at output time j of one (mode, direction): the tangent of
+// the state at the moving output time is y' + f tau_out', then the RSA projection and the
+// output conversion in dual numbers.  y: the forward state at tau_out[j]; pf: n doubles of
+// scratch; TT.fd / TT.jk are used as scratch.
+__device__ void emit_tangent_output(const WarpTeam& tm, const DiscoebCosmo& P, const DiscoebTangent* TN, const Dims& D,
+                                    double k, int mode, int dir, int n_modes, int n_out, int j, const double* tau_out,
+                                    const double* tau_out_dot, const double* y, int regime, const TanMem& TT,
+                                    double* pf, double* y_out20, double* y_out20_dot)
+{
+    const int n = D.n;
+    // f at the output time (left limit of the last step's regime), for the moving output time
+    int hint = P.xe_loga.n_knots / 2;
+    Bg<double> b;
+    bg_eval_team(tm, P, y[0], tau_out[j], k, regime, b, hint);
+    rhs_team(tm, P, D, b, k, tau_out[j], y, TT.fd, (double*)nullptr);
+    tm.sync();
+    const double td = tau_out_dot[(size_t)dir * n_out + j];
+    for (int i = tm.lane; i < n; i += 32) TT.jk[i] = TT.yd[i] + TT.fd[i] * td;
+    tm.sync();
+    Dual fld[4];
+    const bool rsa = rsa_projection<Dual>(P, TN, D, tau_out[j], k, y, TT.jk, fld);
+    for (int i = tm.lane; i < n; i += 32) {
+        double v = y[i], vd = TT.jk[i];
+        if (rsa) {
+            const int sl = rsa_slot(D, i);
+            if (sl >= 0) { v = fld[sl].v; vd = fld[sl].d; }
+            else if (sl == -1) { v = 0.0; vd = 0.0; }
+        }
+        pf[i] = v;
+        TT.fd[i] = vd;
+    }
+    tm.sync();
+    if (tm.leader()) {
+        Dual o[20];
+        output_vars<Dual>(P, TN, D, k, pf, TT.fd, o);
+        const size_t oo = (size_t)mode * n_out + j;
+        for (int q = 0; q < 20; ++q) y_out20_dot[((size_t)dir * n_modes * n_out + oo) * 20 + q] = o[q].d;
+        if (dir == 0 && y_out20)
+            for (int q = 0; q < 20; ++q) y_out20[oo * 20 + q] = o[q].v;
+    }
+    tm.sync();
+}
+
+// Bounded wait of one warp on a shared-memory counter: lane 0 polls until *flag >= target (or
+// the block's abort flag is set, or the poll budget runs out, after which it sets the abort
+// flag itself); returns true when the target was reached.  No wait can last forever.
+constexpr long long kMaxPolls = 1LL << 24;  // ~2 s with the back-off below; a step takes < 1 ms
+__device__ bool wait_at_least(const WarpTeam& tm, volatile int* flag, int target, volatile int* abort_flag)
+{
+    int ok = 0;
+    if (tm.leader()) {
+        long long polls = 0;
+        while (true) {
+            if (*flag >= target) { ok = 1; break; }
+            if (*abort_flag) break;
+            if (++polls > kMaxPolls) { *abort_flag = 1; break; }
+            __nanosleep(100);
+        }
+        __threadfence_block();
+    }
+    return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+// discoeb_jvp: one block per (mode, group of directions).  Warp 0 runs the adaptive forward
+// solve and publishes every accepted step (start state, the 8 stages and the factorisation of
+// W) into one of two shared-memory record slots; warps 1..nd each carry the tangent of one
+// direction through the published steps (tangent_step) and write its outputs.  The forward
+// is solved once per block instead of once per direction, and it runs ahead of the tangents
+// by up to two steps.  Steps are handed over with counters in shared memory (published /
+// consumed), every wait bounded (wait_at_least); if a wait gives up, the whole block stops and
+// reports DISCOEB_ABORTED.  The step sequence is the forward's only, so the tangent is the
+// derivative of the discrete solution with the accepted steps held fixed.
+__global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
+    const DiscoebCosmo* __restrict__ cosmo, const DiscoebTangent* __restrict__ tangents, int n_dir, int dpb,
     DiscoebControl ctrl, int n_modes, const double* __restrict__ kmodes, const double* __restrict__ tau_start,
     const double* __restrict__ y0, const double* __restrict__ y0_dot, const double* __restrict__ sw, int n_out,
     const double* __restrict__ tau_out, const double* __restrict__ tau_out_dot, int mem_doubles, int tan_doubles,
@@ -145,80 +214,139 @@ __global__ void __launch_bounds__(256) jvp_kernel(
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5;
     const WarpTeam tm{(int)(threadIdx.x & 31)};
-    const int wpb = blockDim.x >> 5;
-    double* base = smem + (size_t)warp * (kCosmoDoubles + kTanDoubles + mem_doubles + tan_doubles);
-    DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(base);
-    DiscoebTangent* TN = reinterpret_cast<DiscoebTangent*>(base + kCosmoDoubles);
-    double* wmem = base + kCosmoDoubles + kTanDoubles;
-    double* tmem = wmem + mem_doubles;
-    copy_cosmo(tm, cosmo, P);
-    const int total = n_modes * n_dir;
-    for (int w = blockIdx.x * wpb + warp; w < total; w += gridDim.x * wpb) {
-        const int mode = w / n_dir, dir = w - mode * n_dir;
-        {
-            const int* s = reinterpret_cast<const int*>(tangents + dir);
-            int* d = reinterpret_cast<int*>(TN);
-            for (int i = tm.lane; i < (int)(sizeof(DiscoebTangent) / 4); i += 32) d[i] = s[i];
+    const int groups = (n_dir + dpb - 1) / dpb;
+    const int mode = blockIdx.x / groups, grp = blockIdx.x - mode * groups;
+    const int d0 = grp * dpb, nd = min(dpb, n_dir - d0);
+    // shared layout: cosmology, tangents, forward workspace, two step records (+4 scalars
+    // each: t, h, t_next, regime), per tangent warp its workspace + 3 n doubles, flags
+    DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(smem);
+    DiscoebTangent* TNs = reinterpret_cast<DiscoebTangent*>(smem + kCosmoDoubles);
+    double* fmem = smem + kCosmoDoubles + dpb * kTanDoubles;
+    double* slot0 = fmem + mem_doubles;
+    const int rec = mem_doubles + 4;
+    const int n0 = (mem_doubles - 4 * kMaxSlots - 32) / 23;  // state size (mode_mem_doubles)
+    const int per_tan = tan_doubles + 3 * n0;
+    double* twork = slot0 + 2 * rec;
+    int* flags = reinterpret_cast<int*>(twork + (size_t)dpb * per_tan);
+    // flags: [0,1] published count per slot (step m + 1), [2,3] consumptions per slot,
+    //        [4] forward finished, [5] published steps in total, [6] abort
+    volatile int* vf = flags;
+    {
+        const int* s = reinterpret_cast<const int*>(cosmo);
+        int* d = reinterpret_cast<int*>(P);
+        for (int i = threadIdx.x; i < (int)(sizeof(DiscoebCosmo) / 4); i += blockDim.x) d[i] = s[i];
+        for (int dd = 0; dd < nd; ++dd) {
+            const int* ts = reinterpret_cast<const int*>(tangents + d0 + dd);
+            int* td = reinterpret_cast<int*>(TNs + dd);
+            for (int i = threadIdx.x; i < (int)(sizeof(DiscoebTangent) / 4); i += blockDim.x) td[i] = ts[i];
         }
-        const Dims D = make_dims(*P);
-        const int n = D.n;
-        ModeMem M = carve(wmem, D);
-        TanMem TT = carve_tan(tmem, D);
-        const double k = kmodes[mode];
-        for (int i = tm.lane; i < n; i += 32) {
-            M.y[i] = y0[(size_t)mode * n + i];
-            TT.yd[i] = y0_dot[((size_t)dir * n_modes + mode) * n + i];
-        }
+        if (threadIdx.x < 8) flags[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    if (warp > nd) return;  // surplus warps of the last group
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    const double k = kmodes[mode];
+    const double* tout = tau_out;
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+
+    if (warp == 0) {
+        // ---- forward: solve, publish every accepted step ----
+        ModeMem M = carve(fmem, D);
+        for (int i = tm.lane; i < n; i += 32) M.y[i] = y0[(size_t)mode * n + i];
         double swm[3] = {sw[3 * mode], sw[3 * mode + 1], sw[3 * mode + 2]};
         tm.sync();
-        auto emit = [&](int j, const double* y, int regime) {
-            // f at the output time (left limit of the last step's regime), for the moving output time
-            int hint = P->xe_loga.n_knots / 2;
-            Bg<double> b;
-            bg_eval_team(tm, *P, y[0], tau_out[j], k, regime, b, hint);
-            rhs_team(tm, *P, D, b, k, tau_out[j], y, TT.fd, (double*)nullptr);
-            tm.sync();
-            const double td = tau_out_dot[(size_t)dir * n_out + j];
-            for (int i = tm.lane; i < n; i += 32) TT.jk[i] = TT.yd[i] + TT.fd[i] * td;
-            tm.sync();
-            Dual fld[4];
-            const bool rsa = rsa_projection<Dual>(*P, TN, D, tau_out[j], k, y, TT.jk, fld);
-            for (int i = tm.lane; i < n; i += 32) {
-                double v = y[i], vd = TT.jk[i];
-                if (rsa) {
-                    const int sl = rsa_slot(D, i);
-                    if (sl >= 0) { v = fld[sl].v; vd = fld[sl].d; }
-                    else if (sl == -1) { v = 0.0; vd = 0.0; }
-                }
-                M.f[i] = v;
-                TT.fd[i] = vd;
+        int m = 0;
+        auto accept = [&](double t, double h, double tnext, int regime) -> bool {
+            const int sl = m & 1;
+            if (m >= 2 && !wait_at_least(tm, vf + 2 + sl, nd * (m / 2), vf + 6)) return false;
+            double* dst = slot0 + sl * rec;
+            for (int i = tm.lane; i < mem_doubles; i += 32) dst[i] = fmem[i];
+            if (tm.leader()) {
+                dst[mem_doubles] = t;
+                dst[mem_doubles + 1] = h;
+                dst[mem_doubles + 2] = tnext;
+                dst[mem_doubles + 3] = (double)regime;
             }
             tm.sync();
             if (tm.leader()) {
-                Dual o[20];
-                output_vars<Dual>(*P, TN, D, k, M.f, TT.fd, o);
-                const size_t oo = (size_t)mode * n_out + j;
-                for (int q = 0; q < 20; ++q) y_out20_dot[((size_t)dir * n_modes * n_out + oo) * 20 + q] = o[q].d;
-                if (dir == 0 && y_out20)
-                    for (int q = 0; q < 20; ++q) y_out20[oo * 20 + q] = o[q].v;
+                __threadfence_block();
+                vf[sl] = m + 1;
             }
             tm.sync();
+            ++m;
+            return true;
         };
-        const SolveResult R = solve_mode(tm, *P, D, ctrl, k, tau_start[mode], swm, n_out, tau_out, M, emit, TN, &TT);
-        const double qnan = __longlong_as_double(0x7ff8000000000000LL);
-        for (int j = R.outputs; j < n_out; ++j) {
-            const size_t oo = (size_t)mode * n_out + j;
-            for (int i = tm.lane; i < 20; i += 32) {
-                y_out20_dot[((size_t)dir * n_modes * n_out + oo) * 20 + i] = qnan;
-                if (dir == 0 && y_out20) y_out20[oo * 20 + i] = qnan;
+        auto no_emit = [&](int, const double*, int) {};
+        const SolveResult R = solve_mode(tm, *P, D, ctrl, k, tau_start[mode], swm, n_out, tout, M, no_emit,
+                                         (const DiscoebTangent*)nullptr, (const TanMem*)nullptr, (double*)nullptr, 0,
+                                         &accept);
+        if (tm.leader()) {
+            vf[5] = m;
+            __threadfence_block();
+            vf[4] = 1;
+            if (grp == 0) {
+                status[mode] = R.status;
+                nsteps[mode] = R.steps;
             }
         }
-        if (tm.leader() && dir == 0) {
-            status[mode] = R.status;
-            nsteps[mode] = R.steps;
+        return;
+    }
+
+    // ---- tangent of direction d0 + warp - 1 ----
+    const int dl = warp - 1, dir = d0 + dl;
+    const DiscoebTangent* TN = TNs + dl;
+    double* mine = twork + (size_t)dl * per_tan;
+    const TanMem TT = carve_tan(mine, D);
+    double* ubuf = mine + tan_doubles;
+    double* yend = ubuf + n;
+    double* pf = yend + n;
+    for (int i = tm.lane; i < n; i += 32) TT.yd[i] = y0_dot[((size_t)dir * n_modes + mode) * n + i];
+    tm.sync();
+    int hint = P->xe_loga.n_knots / 2, iout = 0;
+    for (int m = 0;; ++m) {
+        const int sl = m & 1;
+        // the next step, unless the forward has finished with fewer steps
+        int have = 0;
+        if (tm.leader()) {
+            long long polls = 0;
+            while (true) {
+                if (vf[sl] == m + 1) { have = 1; break; }
+                if (vf[4] && vf[5] <= m) break;
+                if (vf[6]) break;
+                if (++polls > kMaxPolls) { vf[6] = 1; break; }
+                __nanosleep(100);
+            }
+            __threadfence_block();
+        }
+        if (!__shfl_sync(0xffffffffu, have, 0)) break;
+        const double* r = slot0 + sl * rec;
+        ModeMem Mr = carve(const_cast<double*>(r), D);
+        Mr.u = ubuf;
+        const double t = r[mem_doubles], h = r[mem_doubles + 1], tnext = r[mem_doubles + 2];
+        const int regime = (int)r[mem_doubles + 3];
+        tangent_step(tm, *P, D, k, t, h, regime, Mr, TT, TN, hint);
+        for (int i = tm.lane; i < n; i += 32) yend[i] = ubuf[i] + Mr.K[7 * n + i];
+        tm.sync();
+        if (tm.leader()) {
+            __threadfence_block();
+            atomicAdd(flags + 2 + sl, 1);  // the record may be overwritten from here on
         }
         tm.sync();
+        while (iout < n_out && tout[iout] <= tnext) {
+            emit_tangent_output(tm, *P, TN, D, k, mode, dir, n_modes, n_out, iout, tout, tau_out_dot, yend, regime, TT,
+                                pf, y_out20, y_out20_dot);
+            ++iout;
+        }
     }
+    for (int j = iout; j < n_out; ++j) {
+        const size_t oo = (size_t)mode * n_out + j;
+        for (int i = tm.lane; i < 20; i += 32) {
+            y_out20_dot[((size_t)dir * n_modes * n_out + oo) * 20 + i] = qnan;
+            if (dir == 0 && y_out20) y_out20[oo * 20 + i] = qnan;
+        }
+    }
+    tm.sync();
 }
 
 __global__ void rhs_kernel(const DiscoebCosmo* __restrict__ cosmo, int n_points, const double* __restrict__ tau,
@@ -312,22 +440,25 @@ int32_t discoeb_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_hos
     if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
     const Dims D = make_dims(*cosmo_host);
     const int mem = mode_mem_doubles(D), tmem = tan_mem_doubles(D);
-    const size_t per_warp = (size_t)(kCosmoDoubles + kTanDoubles + mem + tmem) * sizeof(double);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
     int max_optin = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    int wpb = ctrl->warps_per_block > 0 ? ctrl->warps_per_block : 1;  // one mode per block: the most resident warps
-    if (wpb > 8) wpb = 8;
-    while (wpb > 1 && per_warp * wpb > (size_t)max_optin) --wpb;
-    if (per_warp > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
-    const size_t smem = per_warp * wpb;
-    if (cudaFuncSetAttribute(jvp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    // directions per block: as many as fit (at most kMaxDirsPerBlock), the forward is shared
+    auto block_bytes = [&](int d) {
+        return (size_t)(kCosmoDoubles + d * kTanDoubles + 3 * mem + 8 + d * (tmem + 3 * D.n)) * sizeof(double) +
+               8 * sizeof(int);
+    };
+    int dpb = n_dir < kMaxDirsPerBlock ? n_dir : kMaxDirsPerBlock;
+    while (dpb > 1 && block_bytes(dpb) > (size_t)max_optin) --dpb;
+    if (block_bytes(dpb) > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
+    const size_t smem = block_bytes(dpb);
+    if (cudaFuncSetAttribute(jvp_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return DISCOEB_ECUDA;
-    const long long total = (long long)n_modes * n_dir;
-    const int blocks = (int)((total + wpb - 1) / wpb);
-    jvp_kernel<<<blocks, 32 * wpb, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-        cosmo_dev, tangents_dev, n_dir, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot, switch_tau, n_out, tau_out,
+    const long long blocks = (long long)n_modes * ((n_dir + dpb - 1) / dpb);
+    if (blocks > 0x7fffffffLL) return DISCOEB_EINVAL;
+    jvp_block_kernel<<<(unsigned)blocks, 32 * (1 + dpb), smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        cosmo_dev, tangents_dev, n_dir, dpb, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot, switch_tau, n_out, tau_out,
         tau_out_dot, mem, tmem, y_out20, y_out20_dot, status, nsteps);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }

@@ -560,6 +560,43 @@ DDV void tangent_stage(const TM& tm, const DiscoebCosmo& P, const Dims& D, doubl
     solve_W(tm, D, M, h, Kds);
 }
 
+// Tangent of one accepted Rodas5 step from a record of the forward step: M.y (start state),
+// M.K (the 8 stages) and the factorisation of W (M.A, M.Z, M.Gs, M.F1s, M.sc, M.col0), with
+// M.u a buffer of this team's own where the stage states are rebuilt.  Same arithmetic as the
+// tangent part of rodas5_step; on return TT.yd holds the tangent at t + h.
+template <class TM>
+DDV void tangent_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
+                      const ModeMem& M, const TanMem& TT, const DiscoebTangent* tn, int& hint)
+{
+    const int n = D.n;
+    Bg<Dual> bj;
+    bg_eval_team(tm, P, Dual(M.y[0], TT.yd[0]), t, k, regime, bj, hint, tn);
+    {
+        Bg<HDual> bh;
+        bg_eval_team(tm, P, HDual(Dual(M.y[0], TT.yd[0]), Dual(1.0, 0.0)), t, k, regime, bh, hint, tn);
+        rhs_team(tm, P, D, bh, k, t, M.y, TT.c0d, (double*)nullptr, TT.yd, (const double*)nullptr, 3, 3);
+        tm.sync();
+    }
+    for (int s = 0; s < 8; ++s) {
+        if (s > 0) {
+            for (int i = tm.lane; i < n; i += tm.nl) {
+                double v;
+                if (s <= 5) {
+                    v = M.y[i];
+                    for (int j = 0; j < s; ++j) v += kR5.a[s][j] * M.K[j * n + i];
+                } else {
+                    v = M.u[i] + M.K[(s - 1) * n + i];
+                }
+                M.u[i] = v;
+            }
+            tm.sync();
+        }
+        tangent_stage(tm, P, D, k, t, h, regime, M, TT, tn, bj, s, hint);
+    }
+    for (int i = tm.lane; i < n; i += tm.nl) TT.yd[i] = TT.ud[i] + TT.Kd[7 * n + i];
+    tm.sync();
+}
+
 // One Rodas5 step from (t, y) with size h: on return M.u + M.K[7] is the candidate and
 // M.K[7] the error estimate.  Returns false on a non-finite factorisation.
 template <class TM>
@@ -621,11 +658,18 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
 
 // Adaptive solve of one mode from y(t0) in M.y.  At every output time the team calls
 // emit(j, y) with the state exactly at tout[j].  sw[3]: RSA start, UFA start, TCA end.
-template <class TM, class Emit>
+// called for every accepted step before the state advances, with (t, h, t + h as the solver
+// rounds it, regime) of the step and M still holding its start state, stages and
+// factorisation; returning false stops the solve (DISCOEB_ABORTED)
+struct NoAccept {
+    DHD bool operator()(double, double, double, int) const { return true; }
+};
+
+template <class TM, class Emit, class Accept = NoAccept>
 DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, const DiscoebControl& C, double k,
                            double t0, const double* sw, int nout, const double* tout, const ModeMem& M, Emit& emit,
                            const DiscoebTangent* tn = nullptr, const TanMem* TT = nullptr, double* tlog = nullptr,
-                           int tlog_cap = 0)
+                           int tlog_cap = 0, Accept* accept = nullptr)
 {
     const int n = D.n;
     SolveResult R = {DISCOEB_OK, 0, 0, 0};
@@ -684,6 +728,7 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
         double dtn = h * factor;
         tm.sync();
         if (keep) {
+            if (accept && !(*accept)(t, h, tnext, regime)) { R.status = DISCOEB_ABORTED; break; }
             R.accepted++;
             for (int i = tm.lane; i < n; i += tm.nl) M.y[i] = M.u[i] + M.K[7 * n + i];
             if (TT)

@@ -85,6 +85,7 @@ typedef struct {
 #define DISCOEB_SINGULAR 4
 #define DISCOEB_BAD_INDEX 5 /* mode_cosmo[mode] outside [0, n_cosmo), or that cosmology's l_max / nq
                               * differ from cosmos[0]'s: the mode was not solved */
+#define DISCOEB_ABORTED 6   /* the solve stopped because a cooperating warp of the same mode gave up */
 
 /* return codes of the entry points */
 #define DISCOEB_SUCCESS 0

@@ -68,5 +68,7 @@ def shim(tmp_path_factory):
     S.shim_solve_mode_tangent.argtypes = [CP, ctypes.c_void_p, CT, ctypes.c_double, ctypes.c_double, dp, dp, dp,
                                           ctypes.c_int, dp, dp, dp, ip, dp, ctypes.c_int]
     S.shim_replay.argtypes = [CP, ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_int, dp, dp]
+    S.shim_solve_mode_tangent_records.argtypes = [CP, ctypes.c_void_p, CT, ctypes.c_double, ctypes.c_double, dp, dp,
+                                                  dp, ctypes.c_int, dp, dp, ip]
     S.shim_output_tangent.argtypes = [CP, ctypes.c_void_p, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp, dp, dp]
     return S

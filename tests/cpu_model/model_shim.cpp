@@ -152,4 +152,50 @@ void shim_output_tangent(const DiscoebCosmo* P, const DiscoebTangent* tn, double
     rsa_projection<Dual>(*P, tn, D, tau, k, y, yd, f);
     for (int q = 0; q < 4; ++q) { rsa[q] = f[q].v; rsad[q] = f[q].d; }
 }
+
+// forward solve that records every accepted step, then the tangent replayed from the records
+// (the arithmetic of the per-mode block kernel of discoeb_jvp); tangents at the output times
+int shim_solve_mode_tangent_records(const DiscoebCosmo* P, const DiscoebTangent* tn, const DiscoebControl* C, double k,
+                                    double t0, const double* y0, const double* yd0, const double* sw, int nout,
+                                    const double* tout, double* ydout, int* stats)
+{
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    std::vector<double> mem(mode_mem_doubles(D));
+    ModeMem M = carve(mem.data(), D);
+    std::memcpy(M.y, y0, sizeof(double) * n);
+    HostTeam tm;
+    const int mem_n = mode_mem_doubles(D);
+    std::vector<std::vector<double>> recs;
+    std::vector<double> rt, rh, rtn;
+    std::vector<int> rr;
+    auto accept = [&](double t, double h, double tnext, int regime) {
+        recs.emplace_back(mem.begin(), mem.begin() + mem_n);
+        rt.push_back(t);
+        rh.push_back(h);
+        rtn.push_back(tnext);
+        rr.push_back(regime);
+        return true;
+    };
+    auto emit = [&](int, const double*, int) {};
+    SolveResult R = solve_mode(tm, *P, D, *C, k, t0, sw, nout, tout, M, emit, (const DiscoebTangent*)nullptr,
+                               (const TanMem*)nullptr, (double*)nullptr, 0, &accept);
+    stats[0] = R.status;
+    stats[1] = R.steps;
+    stats[2] = R.accepted;
+    std::vector<double> tmem(tan_mem_doubles(D));
+    TanMem TT = carve_tan(tmem.data(), D);
+    std::memcpy(TT.yd, yd0, sizeof(double) * n);
+    int hint = P->xe_loga.n_knots / 2, iout = 0;
+    for (size_t m = 0; m < recs.size(); ++m) {
+        ModeMem Mr = carve(recs[m].data(), D);
+        tangent_step(tm, *P, D, k, rt[m], rh[m], rr[m], Mr, TT, tn, hint);
+        const double tnew = rtn[m];
+        while (iout < nout && tout[iout] <= tnew) {
+            std::memcpy(ydout + (size_t)iout * n, TT.yd, sizeof(double) * n);
+            ++iout;
+        }
+    }
+    return R.status;
+}
 }

@@ -158,6 +158,33 @@ def test_output_and_projection_tangents(shim, prob, case):
     assert np.all(np.abs(got - fd) <= tol + 1e-12 * np.abs(fd).max()), np.abs(got - fd) / (np.abs(fd) + 1e-300)
 
 
+@pytest.mark.parametrize("k", [1e-3, 0.05, 1.0])
+def test_tangent_replayed_from_step_records_equals_combined_solve(shim, prob, k):
+    """The per-mode block kernel of discoeb_jvp solves the forward once, records every accepted
+    step (start state, stages, factorisation of W) and carries each direction's tangent through
+    the records afterwards: the same arithmetic as the tangent interleaved with the forward
+    stages, so the results agree exactly."""
+    bg, OP = prob
+    n = OP.n
+    keep = []
+    C = _cosmo(bg, keep)
+    ctrl = _abi.DiscoebControl(1e-5, 1e-8, 0.25, 0.8, 0.0, 20.0, 0.3, 100000, 0, 0, 0)
+    tout = bg["tau_of_a_spline"].evaluate(np.array([0.25, 0.5, 1.0]))
+    ts = 0.99 * min(tout.min(), OP.start_time(k))
+    y0, sw = OP.ics(ts, k), OP.switch_times(k)
+    yd0 = y0 * np.random.default_rng(5).standard_normal(n) * 0.1
+    tn = _abi.DiscoebTangent()
+    tn.Omegab, tn.amnu, tn.w0 = 1.0, 0.2, 0.5
+    ya, yda, yb_d = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
+    s1, s2 = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+    shim.shim_solve_mode_tangent(ctypes.byref(C), ctypes.byref(tn), ctypes.byref(ctrl), k, ts, ptr(y0.copy()),
+                                 ptr(yd0.copy()), ptr(sw), 3, ptr(tout), ptr(ya), ptr(yda), s1, ptr(np.zeros(1)), 0)
+    shim.shim_solve_mode_tangent_records(ctypes.byref(C), ctypes.byref(tn), ctypes.byref(ctrl), k, ts, ptr(y0.copy()),
+                                         ptr(yd0.copy()), ptr(sw), 3, ptr(tout), ptr(yb_d), s2)
+    assert s1[0] == s2[0] == 0 and s1[1] == s2[1] and s1[2] == s2[2]
+    np.testing.assert_array_equal(yb_d, yda)
+
+
 def _fd_background(theta, name, trace, eps):
     side = []
     for sgn in (1, -1):
