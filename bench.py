@@ -480,12 +480,15 @@ def main():
 
     # ---- roofline: FP64 work of the structured Rodas5 step against a measured FP64 peak ----
     flops_per_step = 850.0 * n + 1650.0  # forward structured step, counted from stepper.cuh
-    # one tangent direction's extra work per step, estimated from the operation mix of tangent_stage
-    # (stepper.cuh): 8 stages x (a dual and a hyper-dual RHS pass ~ 6 real RHS passes of ~10 n + 300
-    # flops, one W solve ~30 n, stage sums ~14 n)
-    tangent_per_step = 8.0 * (6.0 * (10.0 * n + 300.0) + 44.0 * n)
+    # one tangent direction's work per step, estimated from the operation mix of tangent_step
+    # (stepper.cuh): 8 stages x (two dual RHS passes ~ 4 real RHS passes of ~10 n + 300 flops, one
+    # W solve ~30 n, stage sums and the column-0 term ~16 n) + once per step a hyper-dual RHS pass
+    # (~4 real passes) and the stage-state rebuild (~24 n)
+    tangent_per_step = 8.0 * (4.0 * (10.0 * n + 300.0) + 46.0 * n) + 4.0 * (10.0 * n + 300.0) + 24.0 * n
     dense_per_step = (2.0 / 3.0) * n**3 + 16.0 * n**2 + 45.0 * n * n  # reference algorithm: LU + 8 solves + jacfwd
-    work = step_attempts * (flops_per_step + tangent_per_step) * n_dir if grad else step_attempts * flops_per_step
+    # forward once per mode, each direction's tangent on every step (counted on every attempt:
+    # an upper bound, the tangent runs on accepted steps only)
+    work = step_attempts * (flops_per_step + tangent_per_step * n_dir) if grad else step_attempts * flops_per_step
     dense_work = step_attempts * dense_per_step * (1 + n_dir)
     achieved = work / (ms / 1e3) / 1e12
     peak = fp64_peak_tflops(torch, device) if rank == 0 and not args.kernel_only else None
