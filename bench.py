@@ -12,8 +12,9 @@ replica of the cosmology (weak scaling, no collective on the data path).
 
   value : k-modes/s (forward + gradient of each mode), inputs resident in HBM, CUDA events
           around each launch
-  e2e   : the same metric through the public API (gradients.power_spectrum_jacobian or
-          evolve_perturbations: host prologue + H2D + kernel + D2H inside the timed region)
+  e2e   : the same metric through the public API (gradients.power_spectrum_jacobian with its
+          per-direction host tangents in a process pool, or evolve_perturbations: host prologue +
+          H2D + kernel + D2H inside the timed region)
   --impl reference : the oracle's CPU restatement of the reference algorithm (dense LU Rodas5)
           timed on all host cores on a bounded sample of the same workload; for fwd+grad the
           Jacobian of the sample comes from central differences (1 + 2 x 6 solves per mode).
@@ -458,7 +459,8 @@ def main():
         e0.record(stream)
         if grad:
             power_spectrum_jacobian(w["theta"], aexp_out=aout, kmin=w["kmin"], kmax=w["kmax"], num_k=w["num_k"],
-                                    rtol=w["rtol"], atol=w["atol"], max_steps=100000, k_sampling_method="log", **L)
+                                    rtol=w["rtol"], atol=w["atol"], max_steps=100000, k_sampling_method="log",
+                                    host_processes=0, **L)
         else:
             pert.evolve_perturbations(param=dict(bg), aexp_out=aout, kmin=w["kmin"], kmax=w["kmax"],
                                       num_k=w["num_k"], rtol=w["rtol"], atol=w["atol"], max_steps=100000,

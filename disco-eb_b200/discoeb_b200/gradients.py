@@ -43,26 +43,62 @@ def theta_to_params(theta, **extra):
                         n_s=t["n_s"], m_nu=t["m_nu"], w0=t["w0"], wa=t["wa"], **extra)
 
 
-def background_tangents(theta, bg, trace, directions, *, aexp_out, tau_start, kmodes, L):
-    """Host-side tangents along each direction: scalars, tables, output times, initial states."""
-    out = []
-    for name in directions:
-        tc = dict(theta)
-        tc[name] = tc[name] + 1j * _CSTEP
-        bgc = evolve_background(param=theta_to_params(tc), replay=trace)
-        d = {"scalars": {}, "tables": {}}
-        for key, field in (("grhom", "grhom"), ("Omegam", "Omegam"), ("Omegab", "Omegab"), ("OmegaDE", "OmegaDE"),
-                           ("amnu", "amnu"), ("w_DE_0", "w0"), ("w_DE_a", "wa"), ("H0", "H0")):
-            d["scalars"][field] = float(np.imag(bgc[key]) / _CSTEP)
-        for key, short in _TABLES:
-            s = bgc[key]
-            d["tables"][short] = (np.ascontiguousarray(np.imag(s.y) / _CSTEP),
-                                  np.ascontiguousarray(np.imag(s.S) / _CSTEP))
-        d["tau_out"] = np.imag(bgc["tau_of_a_spline"].evaluate(aexp_out)) / _CSTEP
-        y0c = adiabatic_ics(tau=tau_start, param=bgc, kmode=kmodes, **L)
-        d["y0"] = np.ascontiguousarray(np.imag(y0c) / _CSTEP)
-        out.append(d)
-    return out
+def _tangent_one(theta, name, trace, aexp_out, tau_start, kmodes, L, num_thermo=256):
+    """Complex-step tangent of the background along one direction (Recfast steps replayed)."""
+    import warnings
+    tc = dict(theta)
+    tc[name] = tc[name] + 1j * _CSTEP
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        bgc = evolve_background(param=theta_to_params(tc), replay=trace, num_thermo=num_thermo)
+    d = {"scalars": {}, "tables": {}}
+    for key, field in (("grhom", "grhom"), ("Omegam", "Omegam"), ("Omegab", "Omegab"), ("OmegaDE", "OmegaDE"),
+                       ("amnu", "amnu"), ("w_DE_0", "w0"), ("w_DE_a", "wa"), ("H0", "H0")):
+        d["scalars"][field] = float(np.imag(bgc[key]) / _CSTEP)
+    for key, short in _TABLES:
+        s = bgc[key]
+        d["tables"][short] = (np.ascontiguousarray(np.imag(s.y) / _CSTEP), np.ascontiguousarray(np.imag(s.S) / _CSTEP))
+    d["tau_out"] = np.imag(bgc["tau_of_a_spline"].evaluate(aexp_out)) / _CSTEP
+    y0c = adiabatic_ics(tau=tau_start, param=bgc, kmode=kmodes, **L)
+    d["y0"] = np.ascontiguousarray(np.imag(y0c) / _CSTEP)
+    return d
+
+
+def _tangent_task(args):
+    return _tangent_one(*args)
+
+
+_POOL = None
+
+
+def _pool(nproc):
+    """A persistent pool of spawned host processes (safe after CUDA is initialised), reused by
+    every gradient call so that its start-up is paid once."""
+    global _POOL
+    if _POOL is None or _POOL[1] < nproc:
+        import atexit
+        import multiprocessing as mp
+        if _POOL is not None:
+            _POOL[0].terminate()
+        _POOL = (mp.get_context("spawn").Pool(nproc), nproc)
+        atexit.register(_POOL[0].terminate)
+    return _POOL[0]
+
+
+def background_tangents(theta, bg, trace, directions, *, aexp_out, tau_start, kmodes, L, processes=1, num_thermo=256):
+    """Host-side tangents along each direction: scalars, tables, output times, initial states.
+
+    The directions are independent: with ``processes`` > 1 (0: one per direction, up to the
+    host's cores) they run in a persistent pool of spawned host processes (the calling script
+    must guard its top level with ``if __name__ == "__main__":``, as spawned processes import
+    it)."""
+    import os
+    directions = list(directions)
+    nproc = min(len(directions), os.cpu_count() or 1) if not processes else processes
+    args = [(dict(theta), name, trace, aexp_out, tau_start, kmodes, L, num_thermo) for name in directions]
+    if nproc <= 1 or len(directions) <= 1:
+        return [_tangent_task(a) for a in args]
+    return _pool(nproc).map(_tangent_task, args)
 
 
 class JacobianProblem:
@@ -71,12 +107,14 @@ class JacobianProblem:
     The host prologue (background, its tangents, start times, initial states and their
     tangents) runs in the constructor and leaves the inputs resident on the device;
     ``launch`` enqueues the kernel on the current stream and ``result`` reads it back.
+    ``host_processes``: host processes for the per-direction background tangents (1: serial;
+    0: one per direction; see background_tangents).
     """
 
     def __init__(self, theta, *, aexp_out=(1.0,), kmin=1e-4, kmax=1.0, num_k=64, kmodes=None, lmaxg=12, lmaxgp=12,
                  lmaxr=17, lmaxnu=17, nqmax=5, rtol=1e-5, atol=1e-8, pcoeff=0.25, icoeff=0.80, dcoeff=0.0,
                  factormax=20.0, factormin=0.3, max_steps=100000, k_sampling_method="log", idx=4, num_thermo=256,
-                 de_guard_eps=1e-9, device=None, warps_per_block=0):
+                 de_guard_eps=1e-9, device=None, warps_per_block=0, host_processes=1):
         import torch
         if device is None:
             if not torch.cuda.is_available():
@@ -103,7 +141,7 @@ class JacobianProblem:
         sw = approximation_switch_times(bg, kmodes)
         self.dirs = ODE_DIRECTIONS
         tans = background_tangents(theta, bg, trace, self.dirs, aexp_out=aexp_out, tau_start=tau_start,
-                                   kmodes=kmodes, L=L)
+                                   kmodes=kmodes, L=L, processes=host_processes, num_thermo=num_thermo)
         # longest modes (largest k) first so that the tail of the launch is short
         order = np.argsort(-kmodes, kind="stable")
         self.inv = np.empty_like(order)
