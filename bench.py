@@ -197,11 +197,19 @@ def run_batch(args, rank, world, local):
     device = torch.device("cuda", local)
     thetas = sample_thetas(args.n_cosmo, seed=0)
     t0 = time.perf_counter()
-    bgs = backgrounds([theta_to_params(t) for t in thetas])
+    bgs = [] if args.grad else backgrounds([theta_to_params(t) for t in thetas])
     host_s = time.perf_counter() - t0
     L = dict(lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5)
     ks = np.geomspace(1e-4, 5.0, 256)
-    batch = CosmologyBatch(params=bgs, kmodes=ks, aexp_out=np.array([1.0]), rtol=1e-5, atol=1e-8, device=device, **L)
+    if args.grad:
+        from discoeb_b200.gradients import JacobianBatch
+        t0 = time.perf_counter()
+        batch = JacobianBatch(thetas, kmodes=ks, aexp_out=np.array([1.0]), rtol=1e-5, atol=1e-8, device=device,
+                              host_processes=0, **L)
+        host_s = time.perf_counter() - t0
+    else:
+        batch = CosmologyBatch(params=bgs, kmodes=ks, aexp_out=np.array([1.0]), rtol=1e-5, atol=1e-8, device=device,
+                               **L)
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
     for _ in range(args.warmup):
@@ -217,17 +225,19 @@ def run_batch(args, rank, world, local):
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
-    _, status, nsteps = batch.result(on_failure="ignore")
+    status, nsteps = batch.result(on_failure="ignore")[-2:]
     ms = statistics.mean(times)
     cross = np.array([crosses_phantom_divide(t) for t in thetas])
     ok = status == 0
     if rank == 0:
         print(json.dumps({
-            "metric": "forward k-mode solves/s, many cosmologies per launch", "value": world * ok.size / (ms / 1e3),
+            "metric": ("fwd+adjoint" if args.grad else "forward") + " k-mode solves/s, many cosmologies per launch",
+            "value": world * ok.size / (ms / 1e3),
             "unit": "k-mode solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "dtype": "f64",
             "data": "synthetic (seeded uniform box of cosmologies)",
             "config": {"workload": f"box_{args.n_cosmo}x256", "n_cosmo": args.n_cosmo, "num_k": 256,
+                       "mode": "fwd+grad" if args.grad else "forward",
                        "ms_per_cosmology": ms / args.n_cosmo, "host_background_s": host_s,
                        "modes_ok": int(ok.sum()), "modes_failed": int((~ok).sum()),
                        "cosmologies_crossing_w_minus_1": int(cross.sum()),
@@ -316,6 +326,7 @@ def main():
     ap.add_argument("--workload", default="pk_lcdm_mnu_k512_z4")
     ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward", "cmb", "batch"])
     ap.add_argument("--n-cosmo", type=int, default=64, help="cosmologies per launch in --mode batch")
+    ap.add_argument("--grad", action="store_true", help="--mode batch: forward + gradient (discoeb_jvp)")
     ap.add_argument("--wpb", type=int, default=0, help="warps (modes) per block; 0 = the library default")
     ap.add_argument("--ref-sample", type=int, default=24)
     ap.add_argument("--cpu-sample", type=int, default=16)

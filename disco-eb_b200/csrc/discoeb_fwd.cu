@@ -205,7 +205,8 @@ __device__ bool wait_at_least(const WarpTeam& tm, volatile int* flag, int target
 // reports DISCOEB_ABORTED.  The step sequence is the forward's only, so the tangent is the
 // derivative of the discrete solution with the accepted steps held fixed.
 __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
-    const DiscoebCosmo* __restrict__ cosmo, const DiscoebTangent* __restrict__ tangents, int n_dir, int dpb,
+    const DiscoebCosmo* __restrict__ cosmos, int n_cosmo, const int32_t* __restrict__ mode_cosmo,
+    const DiscoebTangent* __restrict__ tangents, int n_dir, int dpb,
     DiscoebControl ctrl, int n_modes, const double* __restrict__ kmodes, const double* __restrict__ tau_start,
     const double* __restrict__ y0, const double* __restrict__ y0_dot, const double* __restrict__ sw, int n_out,
     const double* __restrict__ tau_out, const double* __restrict__ tau_out_dot, int mem_doubles, int tan_doubles,
@@ -217,6 +218,24 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     const int groups = (n_dir + dpb - 1) / dpb;
     const int mode = blockIdx.x / groups, grp = blockIdx.x - mode * groups;
     const int d0 = grp * dpb, nd = min(dpb, n_dir - d0);
+    const int ci = mode_cosmo ? mode_cosmo[mode] : 0;
+    if (ci < 0 || ci >= n_cosmo) {  // invalid cosmology index: report, solve nothing
+        const double qn = __longlong_as_double(0x7ff8000000000000LL);
+        if (threadIdx.x == 0 && grp == 0) {
+            status[mode] = DISCOEB_BAD_INDEX;
+            nsteps[mode] = 0;
+        }
+        for (int dd = 0; dd < nd; ++dd)
+            for (int i = threadIdx.x; i < n_out * 20; i += blockDim.x) {
+                y_out20_dot[((size_t)(d0 + dd) * n_modes + mode) * n_out * 20 + i] = qn;
+                if (d0 + dd == 0 && y_out20) y_out20[(size_t)mode * n_out * 20 + i] = qn;
+            }
+        return;
+    }
+    const DiscoebCosmo* cosmo = cosmos + ci;
+    tangents += (size_t)ci * n_dir;
+    tau_out += (size_t)ci * n_out;
+    tau_out_dot += (size_t)ci * n_dir * n_out;
     // shared layout: cosmology, tangents, forward workspace, two step records (+4 scalars
     // each: t, h, t_next, regime), per tangent warp its workspace + 3 n doubles, flags
     DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(smem);
@@ -246,6 +265,22 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     if (warp > nd) return;  // surplus warps of the last group
     const Dims D = make_dims(*P);
     const int n = D.n;
+    if (mode_mem_doubles(D) != mem_doubles) {  // every cosmology must have the sizes of the first
+        const double qn = __longlong_as_double(0x7ff8000000000000LL);
+        if (warp == 0) {
+            if (tm.leader() && grp == 0) {
+                status[mode] = DISCOEB_BAD_INDEX;
+                nsteps[mode] = 0;
+            }
+        } else {
+            const int dir = d0 + warp - 1;
+            for (int i = tm.lane; i < n_out * 20; i += 32) {
+                y_out20_dot[((size_t)dir * n_modes + mode) * n_out * 20 + i] = qn;
+                if (dir == 0 && y_out20) y_out20[(size_t)mode * n_out * 20 + i] = qn;
+            }
+        }
+        return;
+    }
     const double k = kmodes[mode];
     const double* tout = tau_out;
     const double qnan = __longlong_as_double(0x7ff8000000000000LL);
@@ -423,22 +458,24 @@ int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 
-int32_t discoeb_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, const DiscoebTangent* tangents_dev,
+int32_t discoeb_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                    const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev,
                     int32_t n_dir, const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes,
                     const double* tau_start, const double* y0, const double* y0_dot, const double* switch_tau,
                     int32_t n_out, const double* tau_out, const double* tau_out_dot, double* y_out20,
                     double* y_out20_dot, int32_t* status, int32_t* nsteps, void* stream)
 {
-    int rc = validate_cosmo(cosmo_host);
+    int rc = validate_cosmo(cosmo0_host);
     if (rc) return rc;
-    if (!cosmo_dev || !ctrl || !tangents_dev || n_dir < 1 || n_modes < 0 || n_out < 1) return DISCOEB_EINVAL;
+    if (!cosmos_dev || !ctrl || !tangents_dev || n_cosmo < 1 || n_dir < 1 || n_modes < 0 || n_out < 1)
+        return DISCOEB_EINVAL;
     if (n_modes == 0) return DISCOEB_SUCCESS;
     if (!kmodes || !tau_start || !y0 || !y0_dot || !switch_tau || !tau_out || !tau_out_dot || !y_out20_dot ||
         !status || !nsteps)
         return DISCOEB_EINVAL;
     if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED) return DISCOEB_EUNSUPPORTED;
     if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
-    const Dims D = make_dims(*cosmo_host);
+    const Dims D = make_dims(*cosmo0_host);
     const int mem = mode_mem_doubles(D), tmem = tan_mem_doubles(D);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
@@ -458,8 +495,8 @@ int32_t discoeb_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_hos
     const long long blocks = (long long)n_modes * ((n_dir + dpb - 1) / dpb);
     if (blocks > 0x7fffffffLL) return DISCOEB_EINVAL;
     jvp_block_kernel<<<(unsigned)blocks, 32 * (1 + dpb), smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-        cosmo_dev, tangents_dev, n_dir, dpb, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot, switch_tau, n_out, tau_out,
-        tau_out_dot, mem, tmem, y_out20, y_out20_dot, status, nsteps);
+        cosmos_dev, n_cosmo, mode_cosmo, tangents_dev, n_dir, dpb, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot,
+        switch_tau, n_out, tau_out, tau_out_dot, mem, tmem, y_out20, y_out20_dot, status, nsteps);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 

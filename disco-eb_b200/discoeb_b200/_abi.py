@@ -131,8 +131,9 @@ def lib():
                                   ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp, vp]
         L.discoeb_fwd.restype = ctypes.c_int32
         L.discoeb_rhs.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, vp, vp, vp, ctypes.c_int32, vp, vp]
-        L.discoeb_jvp.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), vp, ctypes.c_int32, ctypes.POINTER(DiscoebControl),
-                                  ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp, vp, vp]
+        L.discoeb_jvp.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, vp, vp, ctypes.c_int32,
+                                  ctypes.POINTER(DiscoebControl), ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32,
+                                  vp, vp, vp, vp, vp, vp, vp]
         L.discoeb_jvp.restype = ctypes.c_int32
         L.discoeb_rhs.restype = ctypes.c_int32
         L.discoeb_sources.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, vp, ctypes.c_int32, vp, vp, vp,

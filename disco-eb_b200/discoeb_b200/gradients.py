@@ -178,8 +178,9 @@ class JacobianProblem:
 
     def launch(self):
         stream = self.torch.cuda.current_stream(self.device).cuda_stream
-        rc = self.lib.discoeb_jvp(self.dc.struct.data_ptr(), ctypes.byref(self.dc.host), self.d_tan.data_ptr(),
-                                  len(self.dirs), ctypes.byref(self.ctrl), self.K, self.d_k.data_ptr(),
+        rc = self.lib.discoeb_jvp(self.dc.struct.data_ptr(), ctypes.byref(self.dc.host), 1, None,
+                                  self.d_tan.data_ptr(), len(self.dirs), ctypes.byref(self.ctrl), self.K,
+                                  self.d_k.data_ptr(),
                                   self.d_ts.data_ptr(), self.d_y0.data_ptr(), self.d_y0d.data_ptr(),
                                   self.d_sw.data_ptr(), self.nout, self.d_tout.data_ptr(), self.d_toutd.data_ptr(),
                                   self.d_out.data_ptr(), self.d_outd.data_ptr(), self.d_stat[0].data_ptr(),
@@ -248,3 +249,126 @@ def power_spectrum_function(**options):
             return torch.einsum("dkn,kn->d", J, grad_P.to(J.dtype))
 
     return PowerSpectrum
+
+
+def _cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo):
+    """Host prologue of one cosmology of a JacobianBatch: background (with its Recfast trace),
+    output and start times, initial states, switch times and the per-direction tangents."""
+    import warnings
+    trace = {}
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        bg = evolve_background(param=theta_to_params(theta), trace=trace, num_thermo=num_thermo)
+    tau_out = bg["tau_of_a_spline"].evaluate(aexp_out)
+    if np.any(np.diff(tau_out) <= 0):
+        raise ValueError("aexp_out must map to strictly increasing output times")
+    tau_start = 0.99 * np.minimum(tau_out.min(), determine_starting_time(param=bg, k=kmodes))
+    y0 = adiabatic_ics(tau=tau_start, param=bg, kmode=kmodes, **L)
+    sw = approximation_switch_times(bg, kmodes)
+    tans = background_tangents(theta, bg, trace, ODE_DIRECTIONS, aexp_out=aexp_out, tau_start=tau_start,
+                               kmodes=kmodes, L=L, processes=1, num_thermo=num_thermo)
+    return {"bg": bg, "tau_out": tau_out, "tau_start": tau_start, "y0": y0, "sw": sw, "tans": tans}
+
+
+def _prologue_task(args):
+    return _cosmology_prologue(*args)
+
+
+class JacobianBatch:
+    """P(k) and dP/dtheta of many cosmologies in ONE discoeb_jvp launch (what ``jax.vmap`` of
+    ``jax.jacfwd`` over cosmologies computes in the reference).
+
+    ``thetas``: list of C theta dicts; ``kmodes``: ``[K]`` shared by all cosmologies.  The host
+    prologue runs per cosmology, in a persistent process pool when ``host_processes`` != 1 (0:
+    up to the host's cores).  ``launch`` / ``result`` as JacobianProblem; result returns
+    ``(P [C, K, nout], J [C, 8, K, nout], status [C, K], nsteps [C, K])``.
+    """
+
+    def __init__(self, thetas, *, kmodes, aexp_out=(1.0,), lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5,
+                 rtol=1e-5, atol=1e-8, pcoeff=0.25, icoeff=0.80, dcoeff=0.0, factormax=20.0, factormin=0.3,
+                 max_steps=100000, idx=4, num_thermo=256, de_guard_eps=1e-9, device=None, host_processes=0):
+        import os
+
+        import torch
+        if device is None:
+            if not torch.cuda.is_available():
+                raise RuntimeError("discoeb_b200 needs a CUDA device (there is no CPU path)")
+            device = torch.device("cuda", torch.cuda.current_device())
+        self.torch, self.device, self.idx, self.lib = torch, device, idx, _abi.lib()
+        L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
+        kmodes = np.ascontiguousarray(kmodes, dtype=np.float64)
+        aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
+        args = [(dict(t), aexp_out, kmodes, L, num_thermo) for t in thetas]
+        nproc = (os.cpu_count() or 1) if not host_processes else host_processes
+        nproc = min(nproc, len(args))
+        pro = [_prologue_task(a) for a in args] if nproc <= 1 else _pool(nproc).map(_prologue_task, args)
+        C, K, nout, n = len(pro), kmodes.shape[0], aexp_out.shape[0], nvar_of(**L)
+        nd = len(ODE_DIRECTIONS)
+        self.C, self.K, self.nout, self.nd, self.kmodes = C, K, nout, nd, kmodes
+        self.bgs = [p["bg"] for p in pro]
+        flat_k = np.tile(kmodes, C)
+        cidx = np.repeat(np.arange(C, dtype=np.int32), K)
+        order = np.argsort(-flat_k, kind="stable")  # longest modes first across all cosmologies
+        self.inv = np.empty_like(order)
+        self.inv[order] = np.arange(C * K)
+        self.dcs = [DeviceCosmo(p["bg"], de_guard_eps=de_guard_eps, device=device, **L) for p in pro]
+        raw = b"".join(bytes(ctypes.string_at(ctypes.addressof(d.host), ctypes.sizeof(d.host))) for d in self.dcs)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+        self.d_cosmos = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(device)
+        self._keep, tstructs = [], []
+        for p in pro:
+            for d in p["tans"]:
+                ts = _abi.DiscoebTangent()
+                for f, v in d["scalars"].items():
+                    setattr(ts, f, v)
+                for short, (yy, SS) in d["tables"].items():
+                    ty, tS = t(yy), t(SS)
+                    self._keep += [ty, tS]
+                    setattr(ts, short + "_y", ty.data_ptr())
+                    setattr(ts, short + "_S", tS.data_ptr())
+                tstructs.append(ts)
+        arr = (_abi.DiscoebTangent * len(tstructs))(*tstructs)
+        self.d_tan = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).to(device)
+        self.d_k, self.d_mc = t(flat_k[order]), t(cidx[order])
+        self.d_ts = t(np.concatenate([p["tau_start"] for p in pro])[order])
+        self.d_y0 = t(np.concatenate([p["y0"] for p in pro])[order])
+        y0d = np.stack([np.concatenate([p["tans"][di]["y0"] for p in pro])[order] for di in range(nd)])
+        self.d_y0d = t(y0d)
+        self.d_sw = t(np.concatenate([p["sw"] for p in pro])[order])
+        self.d_tout = t(np.stack([p["tau_out"] for p in pro]))
+        self.d_toutd = t(np.stack([np.stack([d["tau_out"] for d in p["tans"]]) for p in pro]))
+        f64 = dict(dtype=torch.float64, device=device)
+        self.d_out = torch.empty((C * K, nout, 20), **f64)
+        self.d_outd = torch.empty((nd, C * K, nout, 20), **f64)
+        self.d_stat = torch.empty((2, C * K), dtype=torch.int32, device=device)
+        self.ctrl = _abi.DiscoebControl(rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin, int(max_steps),
+                                        _abi.METHOD_RODAS5_STRUCTURED, 0, 0)
+
+    def launch(self):
+        stream = self.torch.cuda.current_stream(self.device).cuda_stream
+        rc = self.lib.discoeb_jvp(self.d_cosmos.data_ptr(), ctypes.byref(self.dcs[0].host), self.C,
+                                  self.d_mc.data_ptr(), self.d_tan.data_ptr(), self.nd, ctypes.byref(self.ctrl),
+                                  self.C * self.K, self.d_k.data_ptr(), self.d_ts.data_ptr(), self.d_y0.data_ptr(),
+                                  self.d_y0d.data_ptr(), self.d_sw.data_ptr(), self.nout, self.d_tout.data_ptr(),
+                                  self.d_toutd.data_ptr(), self.d_out.data_ptr(), self.d_outd.data_ptr(),
+                                  self.d_stat[0].data_ptr(), self.d_stat[1].data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_jvp failed with code {rc}")
+
+    def result(self, on_failure="raise"):
+        C, K, nout, inv = self.C, self.K, self.nout, self.inv
+        y = self.d_out.cpu().numpy()[inv].reshape(C, K, nout, 20)
+        yd = self.d_outd.cpu().numpy()[:, inv].reshape(self.nd, C, K, nout, 20)
+        stat = self.d_stat.cpu().numpy()[:, inv]
+        _check_status(stat[0], stat[1], np.tile(self.kmodes, C), on_failure)
+        P = np.empty((C, K, nout))
+        J = np.zeros((C, len(THETA_NAMES), K, nout))
+        k = self.kmodes[:, None]
+        for c, bg in enumerate(self.bgs):
+            delta = y[c, ..., self.idx]
+            P[c] = 2 * np.pi**2 * bg["A_s"] * (k / bg["k_p"]) ** (bg["n_s"] - 1) * k**-3 * delta**2
+            for di, name in enumerate(ODE_DIRECTIONS):
+                J[c, THETA_NAMES.index(name)] = 2.0 * P[c] * yd[di, c, ..., self.idx] / delta
+            J[c, THETA_NAMES.index("n_s")] = P[c] * np.log(k / bg["k_p"])
+            J[c, THETA_NAMES.index("ln10As")] = P[c]
+        return P, J, stat[0].reshape(C, K), stat[1].reshape(C, K)

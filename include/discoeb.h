@@ -125,17 +125,21 @@ int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
  * cosmological parameters (replaces jax.jacfwd through diffeqsolve with DirectAdjoint,
  * perturbations.py:904-925, as used in the reference's gradient notebooks).  The tangent is the
  * exact derivative of the discrete Rodas5 solution with the accepted step sequence held fixed.
- *   tangents[n_dir]          device array: d(parameters, tables)/d(theta_d)
- *   y0_dot [n_dir, n_modes, nvar]   d(initial state)/d(theta_d) at fixed start times
- *   tau_out_dot [n_dir, n_out]      d(output times)/d(theta_d)
- *   y_out20 [n_modes, n_out, 20]    output fields (may be NULL)
+ *   cosmos[n_cosmo], mode_cosmo[n_modes]   as in discoeb_fwd (mode_cosmo may be NULL: all 0)
+ *   tangents [n_cosmo, n_dir]        device array: d(parameters, tables)/d(theta_d) per cosmology
+ *   y0_dot [n_dir, n_modes, nvar]    d(initial state)/d(theta_d) at fixed start times
+ *   tau_out [n_cosmo, n_out]         output times of each cosmology
+ *   tau_out_dot [n_cosmo, n_dir, n_out]  d(output times)/d(theta_d)
+ *   y_out20 [n_modes, n_out, 20]     output fields (may be NULL)
  *   y_out20_dot [n_dir, n_modes, n_out, 20]  their derivatives
- * One warp per (mode, direction); one launch. */
-int32_t discoeb_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, const DiscoebTangent* tangents_dev,
-                    int32_t n_dir, const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes,
-                    const double* tau_start, const double* y0, const double* y0_dot, const double* switch_tau,
-                    int32_t n_out, const double* tau_out, const double* tau_out_dot, double* y_out20,
-                    double* y_out20_dot, int32_t* status, int32_t* nsteps, void* stream);
+ * One block per mode (and group of up to 6 directions): one warp solves the forward once, the
+ * others carry the tangents through its published steps; one launch. */
+int32_t discoeb_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                    const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev, int32_t n_dir,
+                    const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
+                    const double* y0, const double* y0_dot, const double* switch_tau, int32_t n_out,
+                    const double* tau_out, const double* tau_out_dot, double* y_out20, double* y_out20_dot,
+                    int32_t* status, int32_t* nsteps, void* stream);
 
 /* RHS f(tau_i, y_i; k_i) of n_points states (compute_time_derivatives):
  *   y, f [n_points, nvar]; tau, kmodes [n_points]; regime < 0: approximation switches

@@ -71,3 +71,23 @@ def test_gpu_bad_cosmology_index_is_reported(torch_cuda):
     assert s[0, 0] == 0 and s[0, 1] == 5 and s[1, 1] == 0
     o = out.cpu().numpy()
     assert np.isfinite(o[0]).all() and np.isnan(o[1]).all()
+
+
+def test_gpu_jacobian_batch_equals_single_cosmology_launches(torch_cuda):
+    from discoeb_b200.gradients import JacobianBatch, JacobianProblem
+    from discoeb_b200.workloads import sample_thetas
+    thetas = sample_thetas(2, seed=11)
+    ks = np.geomspace(1e-3, 0.5, 5)
+    kw = dict(aexp_out=(0.5, 1.0), rtol=1e-5, atol=1e-8, **L65)
+    batch = JacobianBatch(thetas, kmodes=ks, host_processes=1, **kw)
+    batch.launch()
+    P, J, status, nsteps = batch.result(on_failure="ignore")
+    assert P.shape == (2, 5, 2) and J.shape == (2, 8, 5, 2)
+    for c, th in enumerate(thetas):
+        one = JacobianProblem(th, kmodes=ks, **kw)
+        one.launch()
+        P1, J1, s1, n1 = one.result(on_failure="ignore")
+        np.testing.assert_array_equal(status[c], s1)
+        np.testing.assert_array_equal(nsteps[c], n1)
+        np.testing.assert_array_equal(P[c], P1)  # same per-mode arithmetic in both launches
+        np.testing.assert_array_equal(J[c], J1)
