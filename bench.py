@@ -355,14 +355,11 @@ def main():
     from discoeb_b200 import perturbations as pert
     from discoeb_b200.workloads import workload
 
+    from discoeb_b200 import replicas
+
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+    rank, world, dist = replicas.init("nccl", device=device)
     w = workload(args.workload)
     if args.num_k > 0:
         w["num_k"] = args.num_k
@@ -424,8 +421,7 @@ def main():
     step_attempts = int(stat[1].sum())  # per mode (every direction of a mode takes the same steps)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        replicas.barrier(dist)
         torch.cuda.synchronize()
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -440,11 +436,7 @@ def main():
         barrier()
     times_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     clocks = clk.summary()
-    ms = statistics.mean(times_ms)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(statistics.mean(times_ms), dist, device)
     value = world * K / (ms / 1e3)
 
     fwd_ms = None
@@ -460,7 +452,7 @@ def main():
             e1.record(stream)
             e1.synchronize()
             fwd_times.append(e0.elapsed_time(e1))
-        fwd_ms = statistics.mean(fwd_times)
+        fwd_ms = replicas.max_over_ranks(statistics.mean(fwd_times), dist, device)
 
     # ---- end to end through the public API (host arrays in, host arrays out) ----
     e2e_ms = []
@@ -480,11 +472,7 @@ def main():
         e1.synchronize()
         if i >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
-    e2e = statistics.mean(e2e_ms) if e2e_ms else float("nan")
-    if dist is not None:
-        t = torch.tensor([e2e], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = float(t.item())
+    e2e = replicas.max_over_ranks(statistics.mean(e2e_ms) if e2e_ms else float("nan"), dist, device)
     h2d = 8 * (2 * K + K * n + 3 * K + nout) + sum(t.numel() * 8 for t in dc.tensors) + ctypes.sizeof(dc.host)
     d2h = 8 * K * nout * 20 + 8 * K
     if grad:  # + tangent tables, tangent structs, initial-state and output-time tangents; + output tangents
@@ -548,9 +536,7 @@ def main():
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
 
 
 if __name__ == "__main__":
