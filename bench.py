@@ -12,9 +12,9 @@ replica of the cosmology (weak scaling, no collective on the data path).
 
   value : k-modes/s (forward + gradient of each mode), inputs resident in HBM, CUDA events
           around each launch
-  e2e   : the same metric through the public API (gradients.power_spectrum_jacobian with its
-          per-direction host tangents in a process pool, or evolve_perturbations: host prologue +
-          H2D + kernel + D2H inside the timed region)
+  e2e   : the same metric through the public API (gradients.power_spectrum_jacobian: native
+          background + Recfast with forward-mode tangents, one host thread per direction; or
+          evolve_perturbations: host prologue + H2D + kernel + D2H inside the timed region)
   --impl reference : the oracle's CPU restatement of the reference algorithm (dense LU Rodas5)
           timed on all host cores on a bounded sample of the same workload; for fwd+grad the
           Jacobian of the sample comes from central differences (1 + 2 x 6 solves per mode).
@@ -205,7 +205,7 @@ def run_batch(args, rank, world, local):
         from discoeb_b200.gradients import JacobianBatch
         t0 = time.perf_counter()
         batch = JacobianBatch(thetas, kmodes=ks, aexp_out=np.array([1.0]), rtol=1e-5, atol=1e-8, device=device,
-                              host_processes=0, **L)
+                              **L)
         host_s = time.perf_counter() - t0
     else:
         batch = CosmologyBatch(params=bgs, kmodes=ks, aexp_out=np.array([1.0]), rtol=1e-5, atol=1e-8, device=device,
@@ -463,7 +463,7 @@ def main():
         if grad:
             power_spectrum_jacobian(w["theta"], aexp_out=aout, kmin=w["kmin"], kmax=w["kmax"], num_k=w["num_k"],
                                     rtol=w["rtol"], atol=w["atol"], max_steps=100000, k_sampling_method="log",
-                                    host_processes=0, **L)
+                                    host_threads=0, **L)
         else:
             pert.evolve_perturbations(param=dict(bg), aexp_out=aout, kmin=w["kmin"], kmax=w["kmax"],
                                       num_k=w["num_k"], rtol=w["rtol"], atol=w["atol"], max_steps=100000,

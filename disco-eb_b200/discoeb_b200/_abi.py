@@ -55,6 +55,37 @@ class DiscoebControl(ctypes.Structure):
                 + [(f, ctypes.c_int32) for f in ("max_steps", "method", "warps_per_block", "reserved")])
 
 
+class DiscoebCosmoParams(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_double) for f in ("H0", "Omegab", "Omegam", "mnu", "w_DE_0", "w_DE_a", "Tcmb", "YHe",
+                                                "Neff", "Nmnu", "cs2_DE", "Omegak")]
+
+
+# discoeb_background output layout (the DISCOEB_BGS_* / DISCOEB_BGN_* / DISCOEB_BGT_* enums)
+NU_KNOTS = 512
+BGS = ("amin", "amax", "grhom", "grhog", "grhor", "adotrad", "amnu", "Omegamnu", "OmegaDE", "taumin", "taumax", "fHe",
+       "tau0", "tau_maxvis", "H0", "Omegab", "Omegam", "mnu", "w_DE_0", "w_DE_a")
+BGN = ("a", "loga", "logrhonu_y", "logrhonu_S", "logpnu_y", "logpnu_S", "logppnu_y", "logppnu_S")
+BGT = ("aexp", "loga", "tau", "xe", "xeHI", "xeHeI", "xeHeII", "cs2", "Tm", "mu", "xeprime_recf", "cs2a", "tempba",
+       "tau_of_a_S", "a_of_tau_S", "xe_of_tau_S", "cs2a_of_tau_S", "tempba_of_tau_S", "xe_of_loga_S", "cs2a_of_loga_S",
+       "opac", "opac_S", "optical_depth", "gvis", "gvisprime", "gvispprime", "xeprime", "rec_case", "rec_steps")
+
+
+def background_layout(num_thermo):
+    """Split of one discoeb_background output buffer: {name: slice} for the scalars (``s:``),
+    the neutrino tables (``n:``) and the Recfast-grid tables (``t:``), and the total size."""
+    out, o = {}, 0
+    for nm in BGS:
+        out["s:" + nm] = o
+        o += 1
+    for nm in BGN:
+        out["n:" + nm] = slice(o, o + NU_KNOTS)
+        o += NU_KNOTS
+    for nm in BGT:
+        out["t:" + nm] = slice(o, o + num_thermo)
+        o += num_thermo
+    return out, o
+
+
 def nvar(lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax):
     return 7 + (lmaxg + 1) + (lmaxgp + 1) + (lmaxr + 1) + nqmax * (lmaxnu + 1) + 2
 
@@ -149,6 +180,11 @@ def lib():
         L.discoeb_los.restype = ctypes.c_int32
         L.discoeb_cell.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, ctypes.c_double, ctypes.c_double, vp, vp]
         L.discoeb_cell.restype = ctypes.c_int32
+        L.discoeb_background_size.argtypes = [ctypes.c_int32]
+        L.discoeb_background_size.restype = ctypes.c_int64
+        L.discoeb_background.argtypes = [ctypes.POINTER(DiscoebCosmoParams), vp, ctypes.c_int32, ctypes.c_int32, vp, vp,
+                                         ctypes.c_int32]
+        L.discoeb_background.restype = ctypes.c_int32
         if L.discoeb_abi_version() != ABI_VERSION:
             raise RuntimeError("libdiscoeb_b200.so ABI version mismatch; rebuild it")
         _lib = L

@@ -8,6 +8,7 @@ producer of the device kernels' inputs and runs on the host.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 
 import numpy as np
@@ -122,17 +123,92 @@ def setup_background_evolution(*, amin, amax, param):
     return param
 
 
+_PARAM_FIELDS = ("H0", "Omegab", "Omegam", "mnu", "w_DE_0", "w_DE_a", "Tcmb", "YHe", "Neff", "Nmnu", "cs2_DE", "Omegak")
+_DIFF_FIELDS = _PARAM_FIELDS[:6]
+
+
+def _is_complex(param):
+    return any(np.iscomplexobj(param.get(k, 0.0)) for k in _PARAM_FIELDS)
+
+
+def _params_struct(param, fields=_PARAM_FIELDS):
+    from . import _abi
+    c = _abi.DiscoebCosmoParams()
+    for f in fields:
+        setattr(c, f, float(np.real(param.get(f, 0.0))))
+    return c
+
+
+def native_background(param, num_thermo=256, param_dots=(), n_threads=0):
+    """``discoeb_background``: the values (one flat buffer, layout ``_abi.background_layout``) and,
+    for each entry of ``param_dots`` (dicts of d(H0, Omegab, Omegam, mnu, w_DE_0, w_DE_a)), the
+    exact tangent buffer (Recfast branches and steps held fixed)."""
+    from . import _abi
+    lib = _abi.lib()
+    _, size = _abi.background_layout(num_thermo)
+    out = np.empty(size)
+    nd = len(param_dots)
+    dots = (_abi.DiscoebCosmoParams * max(nd, 1))(*[_params_struct(d, _DIFF_FIELDS) for d in param_dots])
+    out_dot = np.empty((nd, size)) if nd else None
+    rc = lib.discoeb_background(ctypes.byref(_params_struct(param)), ctypes.cast(dots, ctypes.c_void_p) if nd else None,
+                                nd, int(num_thermo), out.ctypes.data, out_dot.ctypes.data if nd else None,
+                                int(n_threads))
+    if rc != 0:
+        raise ValueError(f"discoeb_background rejected its arguments (code {rc}; num_thermo >= 32 required)")
+    return out, out_dot
+
+
+def background_from_buffer(param, buf, num_thermo):
+    """The evolve_background dict of ``param`` from a discoeb_background value buffer."""
+    from . import _abi
+    lay, _ = _abi.background_layout(num_thermo)
+    S = lambda nm: buf[lay["s:" + nm]]  # noqa: E731
+    N = lambda nm: buf[lay["n:" + nm]]  # noqa: E731
+    T = lambda nm: buf[lay["t:" + nm]]  # noqa: E731
+    param = dict(param)
+    param.setdefault("Omegak", 0.0)
+    for nm in ("amin", "amax", "grhom", "grhog", "grhor", "adotrad", "amnu", "Omegamnu", "OmegaDE", "taumin", "taumax",
+               "fHe", "tau0", "tau_maxvis"):
+        param[nm] = float(S(nm))
+    param["a"] = N("a")
+    spl = spline_interpolation.from_table
+    param["logrhonu_of_loga_spline"] = spl(N("loga"), N("logrhonu_y"), N("logrhonu_S"), uniform=True)
+    param["logpnu_of_loga_spline"] = spl(N("loga"), N("logpnu_y"), N("logpnu_S"), uniform=True)
+    param["logppseudonu_of_loga_spline"] = spl(N("loga"), N("logppnu_y"), N("logppnu_S"), uniform=True)
+    aexp, tau = T("aexp"), T("tau")
+    for nm in ("aexp", "tau", "xe", "xeHI", "xeHeI", "xeHeII", "cs2", "Tm", "optical_depth", "opac", "gvis",
+               "gvisprime", "gvispprime", "xeprime_recf", "xeprime"):
+        param[nm] = T(nm)
+    param["tau_of_a_spline"] = spl(aexp, tau, T("tau_of_a_S"))
+    param["a_of_tau_spline"] = spl(tau, aexp, T("a_of_tau_S"))
+    param["xe_of_tau_spline"] = spl(tau, T("xe"), T("xe_of_tau_S"))
+    param["cs2a_of_tau_spline"] = spl(tau, T("cs2a"), T("cs2a_of_tau_S"))
+    param["tempba_of_tau_spline"] = spl(tau, T("tempba"), T("tempba_of_tau_S"))
+    param["xe_of_loga_spline"] = spl(T("loga"), T("xe"), T("xe_of_loga_S"))
+    param["cs2a_of_loga_spline"] = spl(T("loga"), T("cs2a"), T("cs2a_of_loga_S"))
+    return param
+
+
 def evolve_background(*, param, thermo_module="RECFAST", num_thermo: int = 256, rtol: float = 1e-5,
-                      atol: float = 1e-7, order: int = 5, class_thermo=None, trace=None, replay=None):
+                      atol: float = 1e-7, order: int = 5, class_thermo=None, trace=None, replay=None,
+                      backend="native"):
     """Background + Recfast thermal history + visibility (background.py:191-345).
 
     Returns a new dict (the caller's dict is not modified, as under the
     reference's ``jax.jit``).  Only ``thermo_module='RECFAST'`` is provided.
+    ``backend``: "native" (``discoeb_background``, C++ host code) or "numpy" (this module's
+    restatement, which also takes complex parameters for complex-step derivatives).  Complex
+    parameters, ``trace`` or ``replay`` select the numpy restatement.
     ``trace``/``replay``: record / repeat the Recfast step sequence (see
     thermodynamics_recfast.solve_pid_grk4a), for derivatives with respect to parameters.
     """
     if thermo_module != "RECFAST":
         raise ValueError(f"thermo_module {thermo_module!r} is not provided; use 'RECFAST'")
+    if backend not in ("native", "numpy"):
+        raise ValueError(f"unknown backend {backend!r}")
+    if backend == "native" and trace is None and replay is None and not _is_complex(param):
+        buf, _ = native_background(param, num_thermo)
+        return background_from_buffer(param, buf, num_thermo)
     param = dict(param)
     param.setdefault("Omegak", 0.0)
     amin, amax = 1e-9, 1.01

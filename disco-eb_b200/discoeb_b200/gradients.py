@@ -6,9 +6,12 @@ solve (``DirectAdjoint``, perturbations.py:919; the gradient notebooks
 Here the same forward-mode derivative is assembled from two exact pieces:
 
 * the background tables, scalar parameters, initial states and output times are
-  differentiated on the host by complex-step differentiation of the background restatement
-  with its Recfast step sequence replayed (so the derivative is that of the discrete
-  background, branch choices held, as forward-mode AD gives);
+  differentiated on the host: ``discoeb_background`` carries one forward-mode derivative per
+  parameter direction through the background and Recfast (C++, one host thread per direction;
+  the derivative of the discrete background with Recfast's branches and step sequence held, as
+  forward-mode AD gives), and the initial states by complex-step differentiation of
+  ``adiabatic_ics``.  ``host_backend="numpy"`` takes the complex-step derivative of the numpy
+  restatement with its Recfast steps replayed instead (same quantity, ~100x slower);
 * the perturbation solve is differentiated on the GPU by ``discoeb_jvp``: the tangent of the
   discrete Rodas5 solution with the accepted step sequence held fixed (the step-size
   controller is not differentiated, exactly as diffrax's stop-gradient on the step factor).
@@ -24,7 +27,8 @@ import ctypes
 import numpy as np
 
 from . import _abi
-from .background import evolve_background
+from .background import _DIFF_FIELDS, background_from_buffer, evolve_background, native_background
+from .spline import spline_interpolation
 from .perturbations import (DeviceCosmo, adiabatic_ics, approximation_switch_times, determine_starting_time, k_sampling,
                             nvar_of, _check_status)
 from .workloads import cosmo_params
@@ -101,20 +105,95 @@ def background_tangents(theta, bg, trace, directions, *, aexp_out, tau_start, km
     return _pool(nproc).map(_tangent_task, args)
 
 
+def param_dots(theta, directions):
+    """d(H0, Omegab, Omegam, mnu, w_DE_0, w_DE_a)/d(theta_d) for each direction (complex step of
+    theta_to_params: exact for these rational maps)."""
+    out = []
+    for name in directions:
+        tc = dict(theta)
+        tc[name] = tc[name] + 1j * _CSTEP
+        pc = theta_to_params(tc)
+        out.append({f: float(np.imag(pc[f]) / _CSTEP) for f in _DIFF_FIELDS})
+    return out
+
+
+def _tangent_from_buffers(bg, buf, dot, num_thermo, aexp_out, tau_start, kmodes, L):
+    """One direction's tangent record (as _tangent_one) from discoeb_background buffers."""
+    lay, _ = _abi.background_layout(num_thermo)
+    s = lambda nm: float(dot[lay["s:" + nm]])  # noqa: E731
+    d = {"scalars": {"grhom": s("grhom"), "Omegam": s("Omegam"), "Omegab": s("Omegab"), "OmegaDE": s("OmegaDE"),
+                     "amnu": s("amnu"), "w0": s("w_DE_0"), "wa": s("w_DE_a"), "H0": s("H0")}}
+    c = lambda key: np.ascontiguousarray(dot[lay[key]])  # noqa: E731
+    d["tables"] = {"xe": (c("t:xe"), c("t:xe_of_loga_S")), "cs2a": (c("t:cs2a"), c("t:cs2a_of_loga_S")),
+                   "logrhonu": (c("n:logrhonu_y"), c("n:logrhonu_S")), "logpnu": (c("n:logpnu_y"), c("n:logpnu_S"))}
+    # tau(a_out): the spline is linear in (y, S) at fixed knots
+    aexp = buf[lay["t:aexp"]]
+    d["tau_out"] = spline_interpolation.from_table(aexp, dot[lay["t:tau"]], dot[lay["t:tau_of_a_S"]]).evaluate(aexp_out)
+    # initial states at fixed start times: complex step of adiabatic_ics through the tables it reads
+    h = _CSTEP
+    cx = lambda key: buf[lay[key]] + 1j * h * dot[lay[key]]  # noqa: E731
+    bgc = {k: bg[k] for k in ("grhog", "grhor", "Neff", "Nmnu", "cs2_DE")}
+    for key, nm in (("grhom", "grhom"), ("Omegam", "Omegam"), ("Omegab", "Omegab"), ("amnu", "amnu"),
+                    ("w_DE_0", "w_DE_0"), ("w_DE_a", "w_DE_a")):
+        bgc[key] = bg[key] + 1j * h * dot[lay["s:" + nm]]
+    bgc["a_of_tau_spline"] = spline_interpolation.from_table(cx("t:tau"), aexp, cx("t:a_of_tau_S"))
+    bgc["logrhonu_of_loga_spline"] = spline_interpolation.from_table(buf[lay["n:loga"]], cx("n:logrhonu_y"),
+                                                                      cx("n:logrhonu_S"), uniform=True)
+    y0c = adiabatic_ics(tau=tau_start, param=bgc, kmode=kmodes, **L)
+    d["y0"] = np.ascontiguousarray(np.imag(y0c) / h)
+    return d
+
+
+def cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo=256, host_backend="native", host_threads=0):
+    """Host prologue of one cosmology's P(k) Jacobian: background, output and start times,
+    initial states, switch times and the per-direction tangents (ODE_DIRECTIONS).
+
+    ``host_backend``: "native" (discoeb_background with ``host_threads`` threads, 0: one per
+    direction) or "numpy" (complex step through the numpy restatement, Recfast steps replayed,
+    ``host_threads`` spawned processes)."""
+    import warnings
+    aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
+    kmodes = np.ascontiguousarray(kmodes, dtype=np.float64)
+    if host_backend == "native":
+        p = theta_to_params(theta)
+        buf, dots = native_background(p, num_thermo, param_dots(theta, ODE_DIRECTIONS), host_threads)
+        bg = background_from_buffer(p, buf, num_thermo)
+    elif host_backend == "numpy":
+        trace = {}
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            bg = evolve_background(param=theta_to_params(theta), trace=trace, num_thermo=num_thermo, backend="numpy")
+    else:
+        raise ValueError(f"unknown host_backend {host_backend!r}")
+    tau_out = bg["tau_of_a_spline"].evaluate(aexp_out)
+    if np.any(np.diff(tau_out) <= 0):
+        raise ValueError("aexp_out must map to strictly increasing output times")
+    tau_start = 0.99 * np.minimum(tau_out.min(), determine_starting_time(param=bg, k=kmodes))
+    y0 = adiabatic_ics(tau=tau_start, param=bg, kmode=kmodes, **L)
+    sw = approximation_switch_times(bg, kmodes)
+    if host_backend == "native":
+        tans = [_tangent_from_buffers(bg, buf, d, num_thermo, aexp_out, tau_start, kmodes, L) for d in dots]
+    else:
+        tans = background_tangents(theta, bg, trace, ODE_DIRECTIONS, aexp_out=aexp_out, tau_start=tau_start,
+                                   kmodes=kmodes, L=L, processes=max(host_threads, 1), num_thermo=num_thermo)
+    return {"bg": bg, "tau_out": tau_out, "tau_start": tau_start, "y0": y0, "sw": sw, "tans": tans}
+
+
 class JacobianProblem:
     """Everything one discoeb_jvp launch needs for P(k) and dP/dtheta of one cosmology.
 
     The host prologue (background, its tangents, start times, initial states and their
     tangents) runs in the constructor and leaves the inputs resident on the device;
     ``launch`` enqueues the kernel on the current stream and ``result`` reads it back.
-    ``host_processes``: host processes for the per-direction background tangents (1: serial;
-    0: one per direction; see background_tangents).
+    ``host_backend`` / ``host_threads``: see cosmology_prologue (``host_processes`` is the older
+    name of ``host_threads``).
     """
 
     def __init__(self, theta, *, aexp_out=(1.0,), kmin=1e-4, kmax=1.0, num_k=64, kmodes=None, lmaxg=12, lmaxgp=12,
                  lmaxr=17, lmaxnu=17, nqmax=5, rtol=1e-5, atol=1e-8, pcoeff=0.25, icoeff=0.80, dcoeff=0.0,
                  factormax=20.0, factormin=0.3, max_steps=100000, k_sampling_method="log", idx=4, num_thermo=256,
-                 de_guard_eps=1e-9, device=None, warps_per_block=0, host_processes=1):
+                 de_guard_eps=1e-9, device=None, warps_per_block=0, host_backend="native", host_threads=0,
+                 host_processes=None):
         import torch
         if device is None:
             if not torch.cuda.is_available():
@@ -123,25 +202,21 @@ class JacobianProblem:
         self.torch, self.device, self.idx = torch, device, idx
         self.lib = _abi.lib()
         L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
-        trace = {}
-        bg = evolve_background(param=theta_to_params(theta), trace=trace, num_thermo=num_thermo)
-        self.bg = bg
         if kmodes is None:
-            kmodes = k_sampling(bg, kmin, kmax, num_k, k_sampling_method)
+            kp = theta_to_params(theta)
+            if k_sampling_method == "camb":  # needs tau_maxvis of the background
+                kp = evolve_background(param=kp, num_thermo=num_thermo)
+            kmodes = k_sampling(kp, kmin, kmax, num_k, k_sampling_method)
         kmodes = np.ascontiguousarray(kmodes, dtype=np.float64)
         aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
-        tau_out = bg["tau_of_a_spline"].evaluate(aexp_out)
-        if np.any(np.diff(tau_out) <= 0):
-            raise ValueError("aexp_out must map to strictly increasing output times")
+        if host_processes is not None:
+            host_threads = host_processes
+        pro = cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo, host_backend, host_threads)
+        bg, tau_out, tau_start, y0, sw, tans = (pro[k] for k in ("bg", "tau_out", "tau_start", "y0", "sw", "tans"))
+        self.bg = bg
         K, nout = kmodes.shape[0], tau_out.shape[0]
         self.kmodes, self.K, self.nout, self.n = kmodes, K, nout, nvar_of(**L)
-        tau_s = determine_starting_time(param=bg, k=kmodes)
-        tau_start = 0.99 * np.minimum(tau_out.min(), tau_s)
-        y0 = adiabatic_ics(tau=tau_start, param=bg, kmode=kmodes, **L)
-        sw = approximation_switch_times(bg, kmodes)
         self.dirs = ODE_DIRECTIONS
-        tans = background_tangents(theta, bg, trace, self.dirs, aexp_out=aexp_out, tau_start=tau_start,
-                                   kmodes=kmodes, L=L, processes=host_processes, num_thermo=num_thermo)
         # longest modes (largest k) first so that the tail of the launch is short
         order = np.argsort(-kmodes, kind="stable")
         self.inv = np.empty_like(order)
@@ -251,27 +326,8 @@ def power_spectrum_function(**options):
     return PowerSpectrum
 
 
-def _cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo):
-    """Host prologue of one cosmology of a JacobianBatch: background (with its Recfast trace),
-    output and start times, initial states, switch times and the per-direction tangents."""
-    import warnings
-    trace = {}
-    with warnings.catch_warnings():
-        warnings.simplefilter("ignore")
-        bg = evolve_background(param=theta_to_params(theta), trace=trace, num_thermo=num_thermo)
-    tau_out = bg["tau_of_a_spline"].evaluate(aexp_out)
-    if np.any(np.diff(tau_out) <= 0):
-        raise ValueError("aexp_out must map to strictly increasing output times")
-    tau_start = 0.99 * np.minimum(tau_out.min(), determine_starting_time(param=bg, k=kmodes))
-    y0 = adiabatic_ics(tau=tau_start, param=bg, kmode=kmodes, **L)
-    sw = approximation_switch_times(bg, kmodes)
-    tans = background_tangents(theta, bg, trace, ODE_DIRECTIONS, aexp_out=aexp_out, tau_start=tau_start,
-                               kmodes=kmodes, L=L, processes=1, num_thermo=num_thermo)
-    return {"bg": bg, "tau_out": tau_out, "tau_start": tau_start, "y0": y0, "sw": sw, "tans": tans}
-
-
 def _prologue_task(args):
-    return _cosmology_prologue(*args)
+    return cosmology_prologue(*args)
 
 
 class JacobianBatch:
@@ -279,14 +335,16 @@ class JacobianBatch:
     ``jax.jacfwd`` over cosmologies computes in the reference).
 
     ``thetas``: list of C theta dicts; ``kmodes``: ``[K]`` shared by all cosmologies.  The host
-    prologue runs per cosmology, in a persistent process pool when ``host_processes`` != 1 (0:
-    up to the host's cores).  ``launch`` / ``result`` as JacobianProblem; result returns
-    ``(P [C, K, nout], J [C, 8, K, nout], status [C, K], nsteps [C, K])``.
+    prologue (cosmology_prologue) runs per cosmology: in the calling process when
+    ``host_processes`` is 1 (each with ``host_threads`` threads), else in a persistent pool of
+    spawned processes (0: up to the host's cores).  ``launch`` / ``result`` as JacobianProblem;
+    result returns ``(P [C, K, nout], J [C, 8, K, nout], status [C, K], nsteps [C, K])``.
     """
 
     def __init__(self, thetas, *, kmodes, aexp_out=(1.0,), lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5,
                  rtol=1e-5, atol=1e-8, pcoeff=0.25, icoeff=0.80, dcoeff=0.0, factormax=20.0, factormin=0.3,
-                 max_steps=100000, idx=4, num_thermo=256, de_guard_eps=1e-9, device=None, host_processes=0):
+                 max_steps=100000, idx=4, num_thermo=256, de_guard_eps=1e-9, device=None, host_backend="native",
+                 host_threads=0, host_processes=1):
         import os
 
         import torch
@@ -298,9 +356,10 @@ class JacobianBatch:
         L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
         kmodes = np.ascontiguousarray(kmodes, dtype=np.float64)
         aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
-        args = [(dict(t), aexp_out, kmodes, L, num_thermo) for t in thetas]
         nproc = (os.cpu_count() or 1) if not host_processes else host_processes
-        nproc = min(nproc, len(args))
+        nproc = min(nproc, len(thetas))
+        threads = host_threads if nproc <= 1 else max(host_threads, 1)
+        args = [(dict(t), aexp_out, kmodes, L, num_thermo, host_backend, threads) for t in thetas]
         pro = [_prologue_task(a) for a in args] if nproc <= 1 else _pool(nproc).map(_prologue_task, args)
         C, K, nout, n = len(pro), kmodes.shape[0], aexp_out.shape[0], nvar_of(**L)
         nd = len(ODE_DIRECTIONS)

@@ -495,9 +495,11 @@ def _background_worker(p):
         return evolve_background(param=p)
 
 
-def backgrounds(param_dicts, processes=None):
-    """evolve_background of many cosmologies on the host, in a process pool (spawned, so that
-    it is safe to call after CUDA is initialised) when there is more than one."""
+def backgrounds(param_dicts, processes=1):
+    """evolve_background of many cosmologies on the host.  The native background takes a few
+    milliseconds per cosmology, so they run in this process by default; ``processes`` > 1 (or 0:
+    the host's cores) spreads them over a pool of spawned processes (safe after CUDA is
+    initialised)."""
     param_dicts = list(param_dicts)
     if len(param_dicts) <= 1 or processes == 1:
         return [_background_worker(p) for p in param_dicts]

@@ -57,6 +57,23 @@ class spline_interpolation:
             for idx in range(m - 2, -1, -1):
                 Si[idx] = dp[idx] - cp[idx] * Si[idx + 1]
             S[1:-1] = Si
+        self._finish(x, y, S, integrate_from_start, uniform)
+
+    @classmethod
+    def from_table(cls, x, y, S, integrate_from_start: bool = True, uniform: bool = False):
+        """The spline with knots ``x``, values ``y`` and knot second derivatives ``S`` given
+        (tables computed elsewhere, e.g. by the native background)."""
+        obj = cls.__new__(cls)
+        x = np.asarray(x)
+        y = np.asarray(y)
+        S = np.asarray(S)
+        obj._finish(x.astype(np.result_type(x.dtype, np.float64)), y.astype(np.result_type(y.dtype, np.float64)),
+                    S.astype(np.result_type(S.dtype, np.float64)), integrate_from_start, uniform)
+        return obj
+
+    def _finish(self, x, y, S, integrate_from_start, uniform):
+        n = y.shape[0]
+        h = x[1:] - x[:-1]
         a_i = y[:-1]
         b_i = (y[1:] - y[:-1]) / h - h * (S[1:] + 2.0 * S[:-1]) / 6.0
         c_i = S[:-1] / 2.0

@@ -17,6 +17,10 @@
  *                     automatic differentiation can flow through them.
  *   discoeb_rhs    -> model_synchronous (src/discoeb/perturbations.py:88-525) evaluated at
  *                     given states, i.e. compute_time_derivatives (perturbations.py:1339-1406).
+ *   discoeb_background -> evolve_background (src/discoeb/background.py:191-345) with
+ *                     thermo_module='RECFAST' (src/discoeb/thermodynamics_recfast.py:124-492),
+ *                     and its parameter derivatives: host memory, host code (the producer of
+ *                     the solve's tables, not a device entry point).
  */
 #ifndef DISCOEB_B200_H
 #define DISCOEB_B200_H
@@ -238,6 +242,65 @@ int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
  * (cmb.py:838-873).  theta [n_modes, n_ell], cell [n_ell], device. */
 int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta, double n_s,
                      double k_p, double* cell, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Background and thermal history (host code): replaces evolve_background with RECFAST
+ * (background.py:141-345, thermodynamics_recfast.py:124-492) and, with tangents, jax.jacfwd
+ * through it.  The cosmological parameters of the reference's param dict; the first six carry
+ * derivatives. */
+typedef struct {
+    double H0, Omegab, Omegam, mnu, w_DE_0, w_DE_a;
+    double Tcmb, YHe, Neff, Nmnu, cs2_DE, Omegak;
+} DiscoebCosmoParams;
+
+/* Output layout: DISCOEB_BGS_COUNT scalars, then DISCOEB_BGN_COUNT arrays of DISCOEB_NU_KNOTS
+ * doubles (massive-neutrino tables on the log-a grid), then DISCOEB_BGT_COUNT arrays of
+ * num_thermo doubles (the Recfast a-grid tables); total discoeb_background_size(num_thermo). */
+#define DISCOEB_NU_KNOTS 512
+enum {
+    DISCOEB_BGS_AMIN, DISCOEB_BGS_AMAX, DISCOEB_BGS_GRHOM, DISCOEB_BGS_GRHOG, DISCOEB_BGS_GRHOR,
+    DISCOEB_BGS_ADOTRAD, DISCOEB_BGS_AMNU, DISCOEB_BGS_OMEGAMNU, DISCOEB_BGS_OMEGADE, DISCOEB_BGS_TAUMIN,
+    DISCOEB_BGS_TAUMAX, DISCOEB_BGS_FHE, DISCOEB_BGS_TAU0, DISCOEB_BGS_TAU_MAXVIS, DISCOEB_BGS_H0,
+    DISCOEB_BGS_OMEGAB, DISCOEB_BGS_OMEGAM, DISCOEB_BGS_MNU, DISCOEB_BGS_W0, DISCOEB_BGS_WA,
+    DISCOEB_BGS_COUNT
+};
+enum {
+    DISCOEB_BGN_A, DISCOEB_BGN_LOGA, DISCOEB_BGN_LOGRHONU_Y, DISCOEB_BGN_LOGRHONU_S, DISCOEB_BGN_LOGPNU_Y,
+    DISCOEB_BGN_LOGPNU_S, DISCOEB_BGN_LOGPPNU_Y, DISCOEB_BGN_LOGPPNU_S, DISCOEB_BGN_COUNT
+};
+/* *_S: second derivatives of the natural spline whose knots and values are the named arrays
+ * (tau_of_a: x = AEXP, y = TAU; a_of_tau: TAU, AEXP; xe_of_tau: TAU, XE; cs2a_of_tau: TAU, CS2A;
+ * tempba_of_tau: TAU, TEMPBA; xe_of_loga: LOGA, XE; cs2a_of_loga: LOGA, CS2A; opac: TAU, OPAC).
+ * REC_CASE: Recfast branch of each interval (1 early, 2 He Saha, 3 H Saha, 4 full ODE);
+ * REC_STEPS: accepted GRK4A steps of each interval (zero in the tangents). */
+enum {
+    DISCOEB_BGT_AEXP, DISCOEB_BGT_LOGA, DISCOEB_BGT_TAU, DISCOEB_BGT_XE, DISCOEB_BGT_XEHI, DISCOEB_BGT_XEHEI,
+    DISCOEB_BGT_XEHEII, DISCOEB_BGT_CS2, DISCOEB_BGT_TM, DISCOEB_BGT_MU, DISCOEB_BGT_XEPRIME_RECF,
+    DISCOEB_BGT_CS2A, DISCOEB_BGT_TEMPBA, DISCOEB_BGT_TAU_OF_A_S, DISCOEB_BGT_A_OF_TAU_S,
+    DISCOEB_BGT_XE_OF_TAU_S, DISCOEB_BGT_CS2A_OF_TAU_S, DISCOEB_BGT_TEMPBA_OF_TAU_S, DISCOEB_BGT_XE_OF_LOGA_S,
+    DISCOEB_BGT_CS2A_OF_LOGA_S, DISCOEB_BGT_OPAC, DISCOEB_BGT_OPAC_S, DISCOEB_BGT_OPTICAL_DEPTH,
+    DISCOEB_BGT_GVIS, DISCOEB_BGT_GVISPRIME, DISCOEB_BGT_GVISPPRIME, DISCOEB_BGT_XEPRIME,
+    DISCOEB_BGT_REC_CASE, DISCOEB_BGT_REC_STEPS, DISCOEB_BGT_COUNT
+};
+
+/* Number of doubles of one background output (values or one tangent). */
+int64_t discoeb_background_size(int32_t num_thermo);
+
+/* Background, Recfast history and visibility tables of one cosmology, and optionally their
+ * derivatives along n_dir parameter directions (the exact derivative of the discrete result with
+ * the Recfast branches and GRK4A step sequence held fixed, as forward-mode AD through the
+ * reference's loops gives).
+ *   par                     parameters
+ *   par_dot [n_dir]         d(par)/d(theta_d) (only the first six fields are read; may be NULL
+ *                           when n_dir = 0)
+ *   num_thermo              Recfast a-grid size (>= 32; the reference's default is 256)
+ *   out [size]              values (host memory)
+ *   out_dot [n_dir, size]   tangents (host memory; NULL when n_dir = 0)
+ *   n_threads               host threads for the directions (<= 0: one per direction)
+ * Host code: touches no device and allocates only host scratch.  Returns DISCOEB_SUCCESS or
+ * DISCOEB_EINVAL. */
+int32_t discoeb_background(const DiscoebCosmoParams* par, const DiscoebCosmoParams* par_dot, int32_t n_dir,
+                           int32_t num_thermo, double* out, double* out_dot, int32_t n_threads);
 
 #ifdef __cplusplus
 }

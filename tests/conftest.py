@@ -26,11 +26,11 @@ def golden():
 _BG = {}
 
 
-def background(name, num_thermo):
+def background(name, num_thermo, backend="native"):
     """Cached evolve_background of a named cosmology."""
     from discoeb_b200.background import evolve_background
     from discoeb_b200.workloads import cosmo_params
-    key = (name, num_thermo)
+    key = (name, num_thermo, backend)
     if key not in _BG:
         if name == "disco_notebook":
             p = {"Omegam": 0.3099, "Omegab": 0.0488911, "H0": 67.742, "n_s": 0.96822, "A_s": 2.1064e-09,
@@ -44,7 +44,7 @@ def background(name, num_thermo):
             raise KeyError(name)
         with warnings.catch_warnings():
             warnings.simplefilter("ignore")
-            _BG[key] = evolve_background(param=p, num_thermo=num_thermo)
+            _BG[key] = evolve_background(param=p, num_thermo=num_thermo, backend=backend)
     return _BG[key]
 
 

@@ -5,9 +5,10 @@ import pytest
 from conftest import background
 
 
-def test_background_matches_reference_golden(golden):
+@pytest.mark.parametrize("backend", ["native", "numpy"])
+def test_background_matches_reference_golden(golden, backend):
     # tests/test_cmb/test_benchmark_evolve_background.csv: DISCO-Notebook cosmology, 1024 thermo points
-    bg = background("disco_notebook", 1024)
+    bg = background("disco_notebook", 1024, backend)
     assert bg["grhom"] == pytest.approx(float(golden["bg_grhom"][0]), rel=1e-14)
     tau = bg["tau_of_a_spline"].evaluate(golden["bg_a"])
     np.testing.assert_allclose(tau, golden["bg_tau"], rtol=1e-10)

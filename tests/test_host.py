@@ -65,8 +65,9 @@ def test_library_exports_every_declared_symbol():
     for h in os.listdir(os.path.join(ROOT, "include")):
         if h.endswith(".h"):
             txt = open(os.path.join(ROOT, "include", h)).read()
-            declared |= set(re.findall(r"^\s*(?:int32_t|void|double)\s+(discoeb_\w+)\s*\(", txt, re.M))
-    assert {"discoeb_fwd", "discoeb_rhs", "discoeb_nvar", "discoeb_abi_version"} <= declared
+            declared |= set(re.findall(r"^\s*(?:int32_t|int64_t|void|double)\s+(discoeb_\w+)\s*\(", txt, re.M))
+    assert {"discoeb_fwd", "discoeb_rhs", "discoeb_nvar", "discoeb_abi_version", "discoeb_los_workspace_bytes",
+            "discoeb_background", "discoeb_background_size"} <= declared
     lib = ctypes.CDLL(path)
     for name in declared:
         assert hasattr(lib, name), name
@@ -84,8 +85,9 @@ def test_struct_layout_matches_header():
 #include <stddef.h>
 #include <stdio.h>
 #include "discoeb.h"
-int main(void){printf("%zu %zu %zu %zu %zu\n", sizeof(DiscoebCosmo), offsetof(DiscoebCosmo, q),
- offsetof(DiscoebCosmo, xe_loga), sizeof(DiscoebControl), offsetof(DiscoebControl, max_steps));return 0;}
+int main(void){printf("%zu %zu %zu %zu %zu %zu %d %d %d %d\n", sizeof(DiscoebCosmo), offsetof(DiscoebCosmo, q),
+ offsetof(DiscoebCosmo, xe_loga), sizeof(DiscoebControl), offsetof(DiscoebControl, max_steps),
+ sizeof(DiscoebCosmoParams), DISCOEB_BGS_COUNT, DISCOEB_BGN_COUNT, DISCOEB_BGT_COUNT, DISCOEB_NU_KNOTS);return 0;}
 '''
     with tempfile.TemporaryDirectory() as d:
         open(os.path.join(d, "p.c"), "w").write(src)
@@ -94,4 +96,5 @@ int main(void){printf("%zu %zu %zu %zu %zu\n", sizeof(DiscoebCosmo), offsetof(Di
         out = subprocess.run([os.path.join(d, "p")], capture_output=True, text=True, check=True).stdout.split()
     C, K = _abi.DiscoebCosmo, _abi.DiscoebControl
     assert [int(v) for v in out] == [ctypes.sizeof(C), C.q.offset, C.xe_loga.offset, ctypes.sizeof(K),
-                                     K.max_steps.offset]
+                                     K.max_steps.offset, ctypes.sizeof(_abi.DiscoebCosmoParams), len(_abi.BGS),
+                                     len(_abi.BGN), len(_abi.BGT), _abi.NU_KNOTS]
