@@ -440,20 +440,47 @@ __global__ void mcoef_kernel(int n_ell, int n_freq, int n_fft, const double* __r
     b[1] = -mag * sn;
 }
 
-__global__ void cell_kernel(int n_modes, const double* __restrict__ kmodes, int n_ell, const double* __restrict__ theta,
-                            double n_s, double k_p, double* cell)
+// C_l = trapezoid over ln k of (k/k_p)^(n_s-1) Theta_l(k)^2, written as sum_i w_i Theta_il^2 with
+// w_i = (k_i/k_p)^(n_s-1) (ln k_{i+1} - ln k_{i-1})/2 (one-sided at the ends).  A block owns 32
+// consecutive l (one coalesced 256-byte row segment per mode) and its 8 warps stride over the
+// modes; the weights of a chunk of modes are computed once per block into shared memory.
+constexpr int kCellChunk = 1024;
+
+__global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __restrict__ kmodes, int n_ell,
+                                                   const double* __restrict__ theta, double n_s, double k_p,
+                                                   double* cell)
 {
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= n_ell) return;
-    double acc = 0.0, fprev = 0.0, lkprev = 0.0;
-    for (int i = 0; i < n_modes; ++i) {
-        const double k = kmodes[i], th = theta[(size_t)i * n_ell + l];
-        const double f = pow(k / k_p, n_s - 1.0) * th * th, lk = log(k);
-        if (i > 0) acc += 0.5 * (f + fprev) * (lk - lkprev);
-        fprev = f;
-        lkprev = lk;
+    __shared__ double w[kCellChunk];
+    __shared__ double part[8][32];
+    const int lx = threadIdx.x & 31, wy = threadIdx.x >> 5;
+    const int l = blockIdx.x * 32 + lx;
+    double acc = 0.0;
+    for (int c0 = 0; c0 < n_modes; c0 += kCellChunk) {
+        const int cn = min(kCellChunk, n_modes - c0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < cn; j += blockDim.x) {
+            const int i = c0 + j;
+            const double lk = log(kmodes[i]);
+            const double lo = i > 0 ? log(kmodes[i - 1]) : lk;
+            const double hi = i + 1 < n_modes ? log(kmodes[i + 1]) : lk;
+            w[j] = pow(kmodes[i] / k_p, n_s - 1.0) * (0.5 * (hi - lo));
+        }
+        __syncthreads();
+        if (l < n_ell) {
+#pragma unroll 4
+            for (int j = wy; j < cn; j += 8) {
+                const double th = theta[(size_t)(c0 + j) * n_ell + l];
+                acc += w[j] * (th * th);
+            }
+        }
     }
-    cell[l] = acc;
+    part[wy][lx] = acc;
+    __syncthreads();
+    if (wy == 0 && l < n_ell) {
+        double sum = 0.0;
+        for (int q = 0; q < 8; ++q) sum += part[q][lx];
+        cell[l] = sum;
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -681,7 +708,7 @@ int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const
 {
     if (n_modes < 2 || n_ell < 1 || !kmodes || !theta || !cell) return DISCOEB_EINVAL;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    cell_kernel<<<blocks_for(n_ell, 128), 128, 0, s>>>(n_modes, kmodes, n_ell, theta, n_s, k_p, cell);
+    cell_kernel<<<(n_ell + 31) / 32, 256, 0, s>>>(n_modes, kmodes, n_ell, theta, n_s, k_p, cell);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 
