@@ -180,6 +180,17 @@ def lib():
         L.discoeb_los.restype = ctypes.c_int32
         L.discoeb_cell.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, ctypes.c_double, ctypes.c_double, vp, vp]
         L.discoeb_cell.restype = ctypes.c_int32
+        c32, c64, cd = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+        L.discoeb_power_amplitudes.argtypes = [c32, vp, vp, c32, c32, cd, cd, cd, c32, vp, vp]
+        L.discoeb_savgol_log_power.argtypes = [c32, vp, c32, vp, vp, vp]
+        L.discoeb_power_kaiser.argtypes = [c32, vp, vp, cd, c32, vp, vp, vp]
+        L.discoeb_power_multipoles.argtypes = [c32, vp, vp, cd, vp, vp, vp, vp]
+        L.discoeb_xi_workspace_bytes.argtypes = [c32]
+        L.discoeb_xi_workspace_bytes.restype = c64
+        L.discoeb_xi_from_power.argtypes = [c32, vp, vp, c32, vp, c64, vp, vp, vp]
+        for nm in ("discoeb_power_amplitudes", "discoeb_savgol_log_power", "discoeb_power_kaiser",
+                   "discoeb_power_multipoles", "discoeb_xi_from_power"):
+            getattr(L, nm).restype = c32
         L.discoeb_background_size.argtypes = [ctypes.c_int32]
         L.discoeb_background_size.restype = ctypes.c_int64
         L.discoeb_background.argtypes = [ctypes.POINTER(DiscoebCosmoParams), vp, ctypes.c_int32, ctypes.c_int32, vp, vp,

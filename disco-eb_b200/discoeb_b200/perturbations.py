@@ -508,3 +508,7 @@ def backgrounds(param_dicts, processes=1):
     nproc = processes or min(len(param_dicts), os.cpu_count() or 1)
     with mp.get_context("spawn").Pool(nproc) as pool:
         return pool.map(_background_worker, param_dicts)
+
+
+# the reference's perturbations module also holds the power-spectrum observables
+from .observables import get_power_smoothed, get_xi_from_P, power_Kaiser, power_multipoles  # noqa: E402,F401

@@ -244,6 +244,40 @@ int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const
                      double k_p, double* cell, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Observables of the linear power spectrum (device arrays, stream-ordered).
+ *
+ * squared = 0: amp[i] = sqrt(2 pi^2 A_s (k_i/k_p)^(n_s-1) k_i^-3) y[i * y_stride + idx], the field
+ * amplitudes that power_Kaiser and power_multipoles build from the output fields
+ * (perturbations.py:1515-1516, :1555-1556); squared = 1: the power spectrum of get_power
+ * (perturbations.py:1445-1468). */
+int32_t discoeb_power_amplitudes(int32_t n_k, const double* kmodes, const double* y, int32_t y_stride, int32_t idx,
+                                 double A_s, double n_s, double k_p, int32_t squared, double* amp, void* stream);
+
+/* Savitzky-Golay smoothing of log P as get_power_smoothed (perturbations.py:1471-1493, with
+ * savgol_filter of util.py:291-327): out = exp(convolve(log P, coeffs, 'same')), except the first
+ * window_length/2 and the last (window_length+1)/2 entries, which keep P.  coeffs
+ * [window_length] (odd) are the filter coefficients (a small least-squares solve the caller does). */
+int32_t discoeb_savgol_log_power(int32_t n_k, const double* P, int32_t window_length, const double* coeffs,
+                                 double* out, void* stream);
+
+/* Kaiser redshift-space spectrum P(k_i, mu_j) = (bias delta_i - mu_j^2 theta_i)^2 into pkmu
+ * [n_k, n_mu] (power_Kaiser, perturbations.py:1495-1524). */
+int32_t discoeb_power_kaiser(int32_t n_k, const double* delta, const double* theta, double bias, int32_t n_mu,
+                             const double* mu, double* pkmu, void* stream);
+
+/* Its multipoles l = 0, 2, 4 (power_multipoles, perturbations.py:1528-1564). */
+int32_t discoeb_power_multipoles(int32_t n_k, const double* delta, const double* theta, double b, double* P0,
+                                 double* P2, double* P4, void* stream);
+
+/* Correlation function multipole xi_l(r) from P(k) on log-spaced k by FFTLog (get_xi_from_P,
+ * perturbations.py:1409-1442): xi, r [n_k] in increasing r = 2 pi / k.  n_k even (the reference's
+ * inverse real FFT returns n_k - 1 points for odd n_k and fails).  workspace: at least
+ * discoeb_xi_workspace_bytes(n_k) bytes of 256-byte-aligned device memory. */
+int64_t discoeb_xi_workspace_bytes(int32_t n_k);
+int32_t discoeb_xi_from_power(int32_t n_k, const double* kmodes, const double* Pk, int32_t ell, void* workspace,
+                              int64_t workspace_bytes, double* xi, double* r, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * Background and thermal history (host code): replaces evolve_background with RECFAST
  * (background.py:141-345, thermodynamics_recfast.py:124-492) and, with tangents, jax.jacfwd
  * through it.  The cosmological parameters of the reference's param dict; the first six carry
