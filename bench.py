@@ -38,6 +38,11 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "fwd+adjoint k-mode solves/s at ≤1e-4 rel err vs FP64 oracle; ms per cosmology"
+# DRAM bytes of one launch per mode, from an ncu capture of a 48-mode case of the same kernel
+# (dram__bytes_read.sum + dram__bytes_write.sum: jvp_block_kernel 1.61 MB, fwd_structured_kernel
+# 0.369 MB), scaled by the number of modes: the initial states, their tangents and the outputs grow
+# with it, the tables are shared (so this slightly overstates a full launch)
+DRAM_BYTES_PER_MODE = {"fwd+grad": 1.61e6 / 48, "forward": 0.369e6 / 48}
 UNIT = "k-mode solves/s"
 
 
@@ -526,7 +531,9 @@ def main():
                     "d2h_bytes_per_step": d2h, "ms_per_cosmology": e2e},
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if peak else None, "traffic": None,
+                         "frac": (achieved / peak) if peak else None,
+                         "traffic": DRAM_BYTES_PER_MODE.get(args.mode, 0.0) * K or None,
+                         "traffic_source": "ncu capture of 48 modes of the same kernel, scaled by the mode count",
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                          "dense_equivalent_tflops": dense_work / (ms / 1e3) / 1e12},
             "clocks": clocks,

@@ -136,12 +136,13 @@ template <class T> struct Bg {
     bool rsa, ufa, tca, de_frozen;
 };
 
-// value part of a background evaluated in dual numbers (the same operations on the values)
-DHD Bg<double> bg_value(const Bg<Dual>& d)
+// value part of a background evaluated in dual numbers (the same operations on the values): a
+// Bg<Dual> gives the double background, a Bg<HDual> the Bg<Dual> of its first direction
+template <class B> DHD Bg<B> bg_value(const Bg<DualT<B>>& d)
 {
-    Bg<double> b;
-    b.par = Par<double>{d.par.grhom.v, d.par.Omegam.v, d.par.Omegab.v, d.par.OmegaDE.v, d.par.amnu.v, d.par.w0.v,
-                        d.par.wa.v, d.par.akthom.v};
+    Bg<B> b;
+    b.par = Par<B>{d.par.grhom.v, d.par.Omegam.v, d.par.Omegab.v, d.par.OmegaDE.v, d.par.amnu.v, d.par.w0.v,
+                   d.par.wa.v, d.par.akthom.v};
     b.a = d.a.v; b.ia = d.ia.v; b.a2 = d.a2.v; b.ia2 = d.ia2.v; b.aH = d.aH.v; b.iaHG = d.iaHG.v;
     b.opac = d.opac.v; b.po = d.po.v; b.tauc = d.tauc.v; b.taucprime = d.taucprime.v; b.cs2 = d.cs2.v;
     b.pb43 = d.pb43.v; b.rho_Q = d.rho_Q.v; b.w_Q = d.w_Q.v; b.opw = d.opw.v; b.iopw = d.iopw.v;

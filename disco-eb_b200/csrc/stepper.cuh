@@ -511,6 +511,8 @@ struct SolveResult {
 // the state k_s with the dual background bj of the step start; column 0 contributes
 // k_s[0] d/de(d f/d a), computed once per step into c0d.  The step sizes are the forward solve's
 // (the derivative of the discrete scheme with the accepted step sequence held fixed).
+// Stage 0's f' (the e-part of f at the step start) comes from the same once-per-step
+// hyper-dual pass as c0d and is in TT.fd on entry for s = 0.
 template <class TM>
 DDV void tangent_stage(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
                        const ModeMem& M, const TanMem& TT, const DiscoebTangent* tn, const Bg<Dual>& bj, int s,
@@ -530,8 +532,8 @@ DDV void tangent_stage(const TM& tm, const DiscoebCosmo& P, const Dims& D, doubl
         TT.ud[i] = v;
     }
     tm.sync();
-    const double ts = (s == 0) ? t : ((s <= 5) ? t + kR5.c[s] * h : t + h);
-    {
+    if (s > 0) {
+        const double ts = (s <= 5) ? t + kR5.c[s] * h : t + h;
         Bg<Dual> bt;
         bg_eval_team(tm, P, Dual(us[0], TT.ud[0]), ts, k, regime, bt, hint, tn);
         rhs_team(tm, P, D, bt, k, ts, us, TT.fd, (double*)nullptr, TT.ud, (const double*)nullptr, 1, 1);
@@ -569,12 +571,15 @@ DDV void tangent_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
                       const ModeMem& M, const TanMem& TT, const DiscoebTangent* tn, int& hint)
 {
     const int n = D.n;
+    // once per step: the background at the step start in hyper-dual numbers (direction e, and a);
+    // its e-part is the dual background bj, and one RHS pass gives d/de(d f/d a) (c0d) and
+    // stage 0's f' (fd)
     Bg<Dual> bj;
-    bg_eval_team(tm, P, Dual(M.y[0], TT.yd[0]), t, k, regime, bj, hint, tn);
     {
         Bg<HDual> bh;
         bg_eval_team(tm, P, HDual(Dual(M.y[0], TT.yd[0]), Dual(1.0, 0.0)), t, k, regime, bh, hint, tn);
-        rhs_team(tm, P, D, bh, k, t, M.y, TT.c0d, (double*)nullptr, TT.yd, (const double*)nullptr, 3, 3);
+        bj = bg_value(bh);
+        rhs_team(tm, P, D, bh, k, t, M.y, TT.c0d, TT.fd, TT.yd, (const double*)nullptr, 3, 1);
         tm.sync();
     }
     for (int s = 0; s < 8; ++s) {
@@ -616,10 +621,10 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
     // direction, and d/de of the Jacobian column d f / d a (see tangent_stage)
     Bg<Dual> bj;
     if (TT) {
-        bg_eval_team(tm, P, Dual(M.y[0], TT->yd[0]), t, k, regime, bj, hint, tn);
         Bg<HDual> bh;
         bg_eval_team(tm, P, HDual(Dual(M.y[0], TT->yd[0]), Dual(1.0, 0.0)), t, k, regime, bh, hint, tn);
-        rhs_team(tm, P, D, bh, k, t, M.y, TT->c0d, (double*)nullptr, TT->yd, (const double*)nullptr, 3, 3);
+        bj = bg_value(bh);
+        rhs_team(tm, P, D, bh, k, t, M.y, TT->c0d, TT->fd, TT->yd, (const double*)nullptr, 3, 1);
         tm.sync();
     }
     const double ih = 1.0 / h;
