@@ -517,19 +517,37 @@ DHD int special_row(const Dims& D, int s)
     return s == 13 ? D.n - 2 : D.n - 1;
 }
 // momentum bin of a massive-neutrino row (0 for other rows)
-DHD int hier_bin(const Dims& D, int i) { return i >= D.iq0 ? (i - D.iq0) % D.nq : 0; }
+// m / nq for 0 <= m < 2^16 and 1 <= nq <= 16.  On the device through a float reciprocal: with
+// m = l nq + r, (m + 1/2)/nq lies at least 1/(2 nq) >= 1/32 away from an integer and the two float
+// roundings move it by less than 2^-22 (m + 1/2) < 0.016, so the truncation is exact (an integer
+// division by a run-time value would cost some twenty instructions per row).
+DHD int div_nq(int m, int nq)
+{
+#if defined(__CUDA_ARCH__)
+    return __float2int_rz(((float)m + 0.5f) * __frcp_rn((float)nq));
+#else
+    return m / nq;
+#endif
+}
+DHD int hier_bin(const Dims& D, int i)
+{
+    if (i < D.iq0) return 0;
+    const int m = i - D.iq0;
+    return m - div_nq(m, D.nq) * D.nq;
+}
 
 // tridiagonal coefficients of hierarchy row i: f_i = lo*y[i-s] + di*y[i] + up*y[i+s] + u.g;
-// vq = velocity of the row's momentum bin (ignored for massless species)
+// vq = velocity of the row's momentum bin and dl = d ln f0 / d ln q of that bin (both ignored for
+// massless species)
 template <class T>
-DHD void hier_coef(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, int i, const T& vq, T& lo, T& di,
-                   T& up, T u[3], int& stride, bool& trunc)
+DHD void hier_coef(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, int i, const T& vq, double dl, T& lo,
+                   T& di, T& up, T u[3], int& stride, bool& trunc)
 {
     int l, L, species;
     if (i <= 7 + D.lmaxg) { l = i - 7; L = D.lmaxg; species = 0; }
     else if (i <= D.idxgp + D.lmaxgp) { l = i - D.idxgp; L = D.lmaxgp; species = 1; }
     else if (i <= D.idxr + D.lmaxr) { l = i - D.idxr; L = D.lmaxr; species = 2; }
-    else { l = (i - D.iq0) / D.nq; L = D.lmaxnu; species = 3; }
+    else { l = div_nq(i - D.iq0, D.nq); L = D.lmaxnu; species = 3; }
     const bool massive = species == 3;
     const T scale = massive ? T(k) * vq : T(k);
     trunc = (l == L);
@@ -540,7 +558,6 @@ DHD void hier_coef(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double 
     u[0] = 0.0; u[1] = 0.0; u[2] = 0.0;
     if (species == 1) u[2] = l == 0 ? 0.5 * b.opac : (l == 2 ? 0.1 * b.opac : T(0.0));
     if (massive) {
-        const double dl = dlfdlq_of(P.q[(i - D.iq0) - l * D.nq]);
         u[0] = l == 0 ? T(dl * (1.0 / 6.0)) : (l == 2 ? T(-dl * (1.0 / 15.0)) : T(0.0));
         u[1] = l == 2 ? T(-0.4 * dl) : T(0.0);
     }

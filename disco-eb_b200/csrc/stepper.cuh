@@ -157,6 +157,8 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
     T ivl = 1.0;
     if (tm.full() && tm.lane < nq) ivl = inv_vq(P, b, tm.lane);
     const T vl = rcp(ivl);
+    // d ln f0 / d ln q of bin q on lane q
+    const double dll = (tm.full() && tm.lane < nq) ? dlfdlq_of(P.q[tm.lane]) : 0.0;
     T drho = 0.0, dp = 0.0, fnu = 0.0;
 #pragma unroll
     for (int q = 0; q < DISCOEB_MAX_NQ; ++q) {
@@ -251,11 +253,12 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
         const int i = hier_row(D, act ? hh : 0);
         const int q = hier_bin(D, i);
         const T vq = tm.full() ? tm.bcast(vl, q) : rcp(inv_vq(P, b, q));
+        const double dlq = tm.full() ? tm.bcast(dll, q) : dlfdlq_of(P.q[q]);
         if (!act) continue;
         T lo, di, up, u[3];
         int st;
         bool trunc;
-        hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
+        hier_coef(P, D, b, k, i, vq, dlq, lo, di, up, u, st, trunc);
         const T fi = lo * Y(i - st) + di * Y(i) + up * Y(trunc ? i : i + st) + u[0] * g0 + u[1] * g1 + u[2] * g2;
         f[i] = comp(fi, fcomp);
         if (dfda) dfda[i] = comp(fi, dcomp);
@@ -355,6 +358,7 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
     const double igh = 1.0 / gh;
     double vlane = 1.0;
     if (tm.full() && tm.lane < D.nq) vlane = rcp(inv_vq(P, b, tm.lane));
+    const double dll = (tm.full() && tm.lane < D.nq) ? dlfdlq_of(P.q[tm.lane]) : 0.0;
     const int nh = n_hier_rows(D);
     // every lane runs the same number of iterations: the shuffle in the loop needs all lanes
     for (int h0 = 0; h0 < nh; h0 += tm.nl) {
@@ -363,11 +367,12 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
         const int i = hier_row(D, act ? hh : 0);
         const int q = hier_bin(D, i);
         const double vq = tm.full() ? tm.bcast(vlane, q) : rcp(inv_vq(P, b, q));
+        const double dlq = tm.full() ? tm.bcast(dll, q) : dlfdlq_of(P.q[q]);
         if (!act) continue;
         double lo, di, up, u[3];
         int st;
         bool trunc;
-        hier_coef(P, D, b, k, i, vq, lo, di, up, u, st, trunc);
+        hier_coef(P, D, b, k, i, vq, dlq, lo, di, up, u, st, trunc);
         double* Ai = M.A + 7 * i;
         Ai[0] = 0.0; Ai[1] = 0.0; Ai[2] = -lo; Ai[3] = igh - di; Ai[4] = -up; Ai[5] = 0.0; Ai[6] = 0.0;
         M.Z[i] = u[0];
