@@ -214,7 +214,8 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
 {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5;
-    const WarpTeam tm{(int)(threadIdx.x & 31)};
+    WarpTeamSeq tm;
+    tm.lane = (int)(threadIdx.x & 31);
     const int groups = (n_dir + dpb - 1) / dpb;
     const int mode = blockIdx.x / groups, grp = blockIdx.x - mode * groups;
     const int d0 = grp * dpb, nd = min(dpb, n_dir - d0);

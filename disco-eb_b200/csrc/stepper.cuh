@@ -275,7 +275,7 @@ DDV bool factor_chain(double* A, const Chain& ch)
         const int i = ch.start + p * ch.stride;
         const double piv = bandA(A, i, 0);
         if (!(fabs(piv) > 0.0) || !xfinite(piv)) ok = false;
-        const double rp = 1.0 / piv;
+        const double rp = rcp(piv);  // correctly rounded, as 1.0 / piv
         bandA(A, i, 0) = rp;
         for (int d = 1; d <= ch.kl && p + d < ch.len; ++d) {
             const int r = i + d * ch.stride;
@@ -288,21 +288,58 @@ DDV bool factor_chain(double* A, const Chain& ch)
     return ok;
 }
 
-DDV void solve_chain(const double* A, const Chain& ch, double* z)
+// Forward and back substitution along one chain.  With CH = 4 the sweeps run in chunks of four
+// elements whose loads are issued together before the dependent arithmetic (the loads do not
+// depend on the recurrence), so a chunk costs one shared-memory latency instead of four; CH = 1 is
+// the plain element-by-element sweep.  The arithmetic and its order are the same for both.
+template <int CH> DDV void solve_chain(const double* A, const Chain& ch, double* z)
 {
-    const int st = ch.stride;
+    const int st = ch.stride, len = ch.len;
     if (ch.kl == 1 && ch.ku == 1) {
         // tridiagonal: carry the neighbour in a register
         int i = ch.start;
         double prev = z[i];
-        for (int p = 1; p < ch.len; ++p) {
+        int p = 1;
+        for (; CH > 1 && p + 4 <= len; p += 4) {
+            double zz[4], a2[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = i + (q + 1) * st;
+                zz[q] = z[j];
+                a2[q] = A[7 * j + 2];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                prev = zz[q] - a2[q] * prev;
+                z[i + (q + 1) * st] = prev;
+            }
+            i += 4 * st;
+        }
+        for (; p < len; ++p) {
             i += st;
             prev = z[i] - A[7 * i + 2] * prev;
             z[i] = prev;
         }
         double next = prev * A[7 * i + 3];
         z[i] = next;
-        for (int p = ch.len - 2; p >= 0; --p) {
+        p = len - 2;
+        for (; CH > 1 && p >= 3; p -= 4) {
+            double zz[4], a4[4], a3[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = i - (q + 1) * st;
+                zz[q] = z[j];
+                a4[q] = A[7 * j + 4];
+                a3[q] = A[7 * j + 3];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                next = (zz[q] - a4[q] * next) * a3[q];
+                z[i - (q + 1) * st] = next;
+            }
+            i -= 4 * st;
+        }
+        for (; p >= 0; --p) {
             i -= st;
             next = (z[i] - A[7 * i + 4] * next) * A[7 * i + 3];
             z[i] = next;
@@ -312,20 +349,79 @@ DDV void solve_chain(const double* A, const Chain& ch, double* z)
     // pentadiagonal (kl = ku = 2)
     int i = ch.start;
     double p1 = z[i], p2 = 0.0;
-    for (int p = 1; p < ch.len; ++p) {
+    int p = 1;
+    if (len > 1) {  // the second element has one sub-diagonal neighbour
+        i += st;
+        const double v = z[i] - A[7 * i + 2] * p1;
+        z[i] = v;
+        p2 = p1;
+        p1 = v;
+        p = 2;
+    }
+    for (; CH > 1 && p + 4 <= len; p += 4) {
+        double zz[4], a2[4], a1[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = i + (q + 1) * st;
+            zz[q] = z[j];
+            a2[q] = A[7 * j + 2];
+            a1[q] = A[7 * j + 1];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double v = zz[q] - a2[q] * p1;
+            v -= a1[q] * p2;
+            z[i + (q + 1) * st] = v;
+            p2 = p1;
+            p1 = v;
+        }
+        i += 4 * st;
+    }
+    for (; p < len; ++p) {
         i += st;
         double v = z[i] - A[7 * i + 2] * p1;
-        if (p >= 2) v -= A[7 * i + 1] * p2;
+        v -= A[7 * i + 1] * p2;
         z[i] = v;
         p2 = p1;
         p1 = v;
     }
     double n1 = p1 * A[7 * i + 3], n2 = 0.0;
     z[i] = n1;
-    for (int p = ch.len - 2; p >= 0; --p) {
+    p = len - 2;
+    if (p >= 0) {  // the last-but-one element has one super-diagonal neighbour
         i -= st;
         double v = z[i] - A[7 * i + 4] * n1;
-        if (p + 2 < ch.len) v -= A[7 * i + 5] * n2;
+        v *= A[7 * i + 3];
+        z[i] = v;
+        n2 = n1;
+        n1 = v;
+        --p;
+    }
+    for (; CH > 1 && p >= 3; p -= 4) {
+        double zz[4], a4[4], a5[4], a3[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = i - (q + 1) * st;
+            zz[q] = z[j];
+            a4[q] = A[7 * j + 4];
+            a5[q] = A[7 * j + 5];
+            a3[q] = A[7 * j + 3];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double v = zz[q] - a4[q] * n1;
+            v -= a5[q] * n2;
+            v *= a3[q];
+            z[i - (q + 1) * st] = v;
+            n2 = n1;
+            n1 = v;
+        }
+        i -= 4 * st;
+    }
+    for (; p >= 0; --p) {
+        i -= st;
+        double v = z[i] - A[7 * i + 4] * n1;
+        v -= A[7 * i + 5] * n2;
         v *= A[7 * i + 3];
         z[i] = v;
         n2 = n1;
@@ -343,7 +439,7 @@ template <class TM> DDV void solve_A(const TM& tm, const Dims& D, const ModeMem&
     for (int c = tm.lane; c < nc; c += tm.nl) {
         const Chain ch = chain_of(D, c);
         if (c == 0) z[6] += etac * z[2];
-        solve_chain(M.A, ch, z);
+        solve_chain<TM::chunk>(M.A, ch, z);
     }
     tm.sync();
 }

@@ -12,6 +12,7 @@ namespace dscb {
 struct WarpTeam {
     int lane;
     static constexpr int nl = 32;
+    static constexpr int chunk = 4;  // elements per load batch in the chain substitutions
     __device__ __forceinline__ void sync() const { __syncwarp(); }
     __device__ __forceinline__ double sum(double x) const
     {
@@ -27,11 +28,18 @@ struct WarpTeam {
     }
     __device__ __forceinline__ bool full() const { return true; }
 };
+// The same warp team with element-by-element chain substitutions: the batched loads of
+// WarpTeam hold twelve more registers live, which a kernel already at the register limit (the
+// gradient block kernel, seven warps per block) pays for in spills and time.
+struct WarpTeamSeq : WarpTeam {
+    static constexpr int chunk = 1;
+};
 #endif
 
 struct HostTeam {
     int lane = 0;
     static constexpr int nl = 1;
+    static constexpr int chunk = 4;
     DHD void sync() const {}
     DHD double sum(double x) const { return x; }
     DHD bool leader() const { return true; }
