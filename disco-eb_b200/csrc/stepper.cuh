@@ -144,12 +144,15 @@ DHD double comp(const HDual& x, int c) { return c == 0 ? x.v.v : (c == 1 ? x.v.d
 // The metric functionals and the 15 "special" rows are computed in straight-line code by every
 // lane (no divergence, no reductions); the hierarchy rows are spread over the lanes as one
 // uniform class.  Same equations as model_synchronous (perturbations.py:88-525).
-template <class TM, class T>
+// S is the type of the state entries: T when the state carries derivative parts (yd, yk), or
+// double for a plain state under a dual background, where the products of coefficients and state
+// entries then cost the dual-times-double form.
+template <class TM, class T, class S = T>
 DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau,
                   const double* y, double* f, double* dfda, const double* yd = nullptr, const double* yk = nullptr,
                   int fcomp = 0, int dcomp = 1)
 {
-    auto Y = [&](int j) { return state_at<T>(y, yd, yk, j); };
+    auto Y = [&](int j) { return state_at<S>(y, yd, yk, j); };
     const int n = D.n, nq = D.nq, iq0 = D.iq0, idxr = D.idxr;
     const double k2 = k * k;
     const T Omegac = b.par.Omegam - b.par.Omegab;
@@ -172,10 +175,10 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
         }
     }
     dp = dp * (1.0 / 3.0);
-    const T eta = Y(2), deltac = Y(3), thetac = Y(4), deltab = Y(5), thetab = Y(6);
-    const T deltag = Y(7), thetag = Y(8), y9 = Y(9);
-    const T deltar = Y(idxr), thetar = Y(idxr + 1), yr2 = Y(idxr + 2);
-    const T deltaq = Y(n - 2), thetaq = Y(n - 1);
+    const S eta = Y(2), deltac = Y(3), thetac = Y(4), deltab = Y(5), thetab = Y(6);
+    const S deltag = Y(7), thetag = Y(8), y9 = Y(9);
+    const S deltar = Y(idxr), thetar = Y(idxr + 1), yr2 = Y(idxr + 2);
+    const S deltaq = Y(n - 2), thetaq = Y(n - 1);
     const T rQa2 = b.rho_Q * b.a2;
     const T dgm = b.par.grhom * (Omegac * deltac + b.par.Omegab * deltab) * b.ia;
     const T dgnu = P.grhor * P.Nmnu * drho * b.ia2;
@@ -206,7 +209,7 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
     const T dgpres = (P.grhog * dge + P.grhor * P.Neff * dre) * b.ia2 * (1.0 / 3.0) + P.grhor * P.Nmnu * dp * b.ia2 +
                      (cs2Q * b.par.grhom * b.par.OmegaDE * deltaq * rQa2 + (cs2Q - b.ca2_Q) * (3.0 * b.aH * rptq * (1.0 / k2)));
     const bool hier_photons = !b.rsa && !b.tca;
-    const T polter = hier_photons ? y9 + Y(D.idxgp) + Y(D.idxgp + 2) : T(0.0);
+    const T polter = hier_photons ? T(y9 + Y(D.idxgp) + Y(D.idxgp + 2)) : T(0.0);
     const T alpha = (H + 6.0 * E) * (0.5 / k2);
     // special rows
     T sp[15];
@@ -640,7 +643,8 @@ DDV void tangent_stage(const TM& tm, const DiscoebCosmo& P, const Dims& D, doubl
         rhs_team(tm, P, D, bt, k, ts, us, TT.fd, (double*)nullptr, TT.ud, (const double*)nullptr, 1, 1);
     }
     const double* Ks = M.K + s * n;
-    rhs_team(tm, P, D, bj, k, t, Ks, TT.jk, (double*)nullptr, (const double*)nullptr, (const double*)nullptr, 1, 1);
+    rhs_team<TM, Dual, double>(tm, P, D, bj, k, t, Ks, TT.jk, (double*)nullptr, (const double*)nullptr,
+                               (const double*)nullptr, 1, 1);
     tm.sync();
     {
         const double k0 = Ks[0];
@@ -713,7 +717,7 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
     // Jacobian column d f/d a and f(y) in one dual pass
     Bg<Dual> bd;
     bg_eval_team(tm, P, Dual(M.y[0], 1.0), t, k, regime, bd, hint);
-    rhs_team(tm, P, D, bd, k, t, M.y, M.f, M.col0);
+    rhs_team<TM, Dual, double>(tm, P, D, bd, k, t, M.y, M.f, M.col0);
     const Bg<double> b = bg_value(bd);
     for (int i = tm.lane; i < n; i += tm.nl) M.dT[i] = dtau_row(D, b, t, i, M.y);
     tm.sync();
