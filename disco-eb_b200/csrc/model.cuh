@@ -190,16 +190,47 @@ template <class T> struct BgTables {
     T xe, xep, cs2a, rhonu, pnu, rho_Q;
 };
 
-template <class T>
-DHD T table_slot_value(const DiscoebCosmo& P, const Par<T>& par, const DiscoebTangent* tn, int t, T a, T loga,
-                       int& hint, T& deriv)
+DHD const DiscoebSpline& table_slot_spline(const DiscoebCosmo& P, int t)
 {
-    // t: 0 xe (and its derivative), 1 cs2*a, 2 log rho_nu, 3 log p_nu, 4 log rho_Q
+    return t == 0 ? P.xe_loga : (t == 1 ? P.cs2a_loga : (t == 2 ? P.logrhonu_loga : P.logpnu_loga));
+}
+
+// interval index of table slot t (0..3) at log a; slot 0 (xe) moves the hint
+DHD int table_slot_index(const DiscoebCosmo& P, int t, double loga, int& hint)
+{
+    int h = hint;
+    const int i = spline_index_from(table_slot_spline(P, t), loga, h);
+    if (t == 0) hint = h;
+    return i;
+}
+
+// value of table slot t at log a in interval i (t: 0 xe with its derivative, 1 cs2*a,
+// 2 log rho_nu, 3 log p_nu, 4 log rho_Q, which needs no table)
+template <class T>
+DHD T table_slot_eval(const DiscoebCosmo& P, const Par<T>& par, const DiscoebTangent* tn, int t, int i, T a, T loga,
+                      T& deriv)
+{
     if (t == 4) {
         deriv = 0.0;
         return -3.0 * (1.0 + par.w0 + par.wa) * loga + 3.0 * (a - 1.0) * par.wa;
     }
-    const DiscoebSpline& s = t == 0 ? P.xe_loga : (t == 1 ? P.cs2a_loga : (t == 2 ? P.logrhonu_loga : P.logpnu_loga));
+    const DiscoebSpline& s = table_slot_spline(P, t);
+    const double* yd = nullptr;
+    const double* Sd = nullptr;
+    if (tn) {
+        yd = t == 0 ? tn->xe_y : (t == 1 ? tn->cs2a_y : (t == 2 ? tn->logrhonu_y : tn->logpnu_y));
+        Sd = t == 0 ? tn->xe_S : (t == 1 ? tn->cs2a_S : (t == 2 ? tn->logrhonu_S : tn->logpnu_S));
+    }
+    deriv = spline_deriv_at(s, i, loga, yd, Sd);
+    return spline_eval_at(s, i, loga, yd, Sd);
+}
+
+template <class T>
+DHD T table_slot_value(const DiscoebCosmo& P, const Par<T>& par, const DiscoebTangent* tn, int t, T a, T loga,
+                       int& hint, T& deriv)
+{
+    if (t == 4) return table_slot_eval(P, par, tn, 4, 0, a, loga, deriv);
+    const DiscoebSpline& s = table_slot_spline(P, t);
     const double* yd = nullptr;
     const double* Sd = nullptr;
     if (tn) {
@@ -230,12 +261,25 @@ DHD BgTables<T> bg_tables(const TM& tm, const DiscoebCosmo& P, const Par<T>& par
         hint = h;
         return r;
     }
-    // lanes 0..4 each evaluate one table slot with the same instruction stream, then broadcast
-    T v = 0.0, d = 0.0;
+    // lanes 0..4 each evaluate one table slot, then broadcast.  The lanes reach their interval
+    // index by different paths (uniform knots, a search from the hint, none for rho_Q).  With
+    // TM::reconverge the team reconverges after the index and again before the exponential, so
+    // that the evaluation and the exponential run once for all five lanes rather than once per
+    // path; otherwise each lane runs its slot in one piece.
     int h = hint;
-    if (tm.lane < 5) {
-        v = table_slot_value(P, par, tn, tm.lane, a, loga, h, d);
-        if (tm.lane >= 2) v = xexp(v);
+    T v = 0.0, d = 0.0;
+    if constexpr (TM::reconverge) {
+        int idx = 0;
+        if (tm.lane < 4) idx = table_slot_index(P, tm.lane, val(loga), h);
+        tm.sync();
+        if (tm.lane < 5) v = table_slot_eval(P, par, tn, tm.lane, idx, a, loga, d);
+        tm.sync();
+        if (tm.lane >= 2 && tm.lane < 5) v = xexp(v);
+    } else {
+        if (tm.lane < 5) {
+            v = table_slot_value(P, par, tn, tm.lane, a, loga, h, d);
+            if (tm.lane >= 2) v = xexp(v);
+        }
     }
     r.xe = tm.bcast(v, 0);
     r.xep = tm.bcast(d, 0);

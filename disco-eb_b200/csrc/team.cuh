@@ -12,7 +12,8 @@ namespace dscb {
 struct WarpTeam {
     int lane;
     static constexpr int nl = 32;
-    static constexpr int chunk = 4;  // elements per load batch in the chain substitutions
+    static constexpr int chunk = 4;         // elements per load batch in the chain substitutions
+    static constexpr bool reconverge = true;  // explicit reconvergence after divergent table lookups
     __device__ __forceinline__ void sync() const { __syncwarp(); }
     __device__ __forceinline__ double sum(double x) const
     {
@@ -28,11 +29,13 @@ struct WarpTeam {
     }
     __device__ __forceinline__ bool full() const { return true; }
 };
-// The same warp team with element-by-element chain substitutions: the batched loads of
-// WarpTeam hold twelve more registers live, which a kernel already at the register limit (the
-// gradient block kernel, seven warps per block) pays for in spills and time.
+// The same warp team with element-by-element chain substitutions and no extra reconvergence
+// points: measured on B200, both help a forward-solve warp (about 4 warps per SM) but slow the
+// gradient block kernel (seven warps per block at the register limit), where the batched loads
+// cost registers and the other warps of the block hide the divergence anyway.
 struct WarpTeamSeq : WarpTeam {
     static constexpr int chunk = 1;
+    static constexpr bool reconverge = false;
 };
 #endif
 
@@ -40,6 +43,7 @@ struct HostTeam {
     int lane = 0;
     static constexpr int nl = 1;
     static constexpr int chunk = 4;
+    static constexpr bool reconverge = false;
     DHD void sync() const {}
     DHD double sum(double x) const { return x; }
     DHD bool leader() const { return true; }
