@@ -202,7 +202,8 @@ def run_batch(args, rank, world, local):
     device = torch.device("cuda", local)
     thetas = sample_thetas(args.n_cosmo, seed=0)
     t0 = time.perf_counter()
-    bgs = [] if args.grad else backgrounds([theta_to_params(t) for t in thetas])
+    bgs = [] if args.grad else backgrounds([theta_to_params(t) for t in thetas],
+                                           device=device if args.host_backend == "device" else None)
     host_s = time.perf_counter() - t0
     L = dict(lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5)
     ks = np.geomspace(1e-4, 5.0, 256)
@@ -210,7 +211,7 @@ def run_batch(args, rank, world, local):
         from discoeb_b200.gradients import JacobianBatch
         t0 = time.perf_counter()
         batch = JacobianBatch(thetas, kmodes=ks, aexp_out=np.array([1.0]), rtol=1e-5, atol=1e-8, device=device,
-                              **L)
+                              host_backend=args.host_backend, **L)
         host_s = time.perf_counter() - t0
     else:
         batch = CosmologyBatch(params=bgs, kmodes=ks, aexp_out=np.array([1.0]), rtol=1e-5, atol=1e-8, device=device,
@@ -244,6 +245,7 @@ def run_batch(args, rank, world, local):
             "config": {"workload": f"box_{args.n_cosmo}x256", "n_cosmo": args.n_cosmo, "num_k": 256,
                        "mode": "fwd+grad" if args.grad else "forward",
                        "ms_per_cosmology": ms / args.n_cosmo, "host_background_s": host_s,
+                       "host_backend": args.host_backend,
                        "modes_ok": int(ok.sum()), "modes_failed": int((~ok).sum()),
                        "cosmologies_crossing_w_minus_1": int(cross.sum()),
                        "failed_in_crossing_cosmologies": int((~ok[cross]).sum()) if cross.any() else 0,
@@ -332,6 +334,8 @@ def main():
     ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward", "cmb", "batch"])
     ap.add_argument("--n-cosmo", type=int, default=64, help="cosmologies per launch in --mode batch")
     ap.add_argument("--grad", action="store_true", help="--mode batch: forward + gradient (discoeb_jvp)")
+    ap.add_argument("--host-backend", default="native", choices=["native", "device"],
+                    help="--mode batch: backgrounds on the host (native C++) or in one GPU launch")
     ap.add_argument("--wpb", type=int, default=0, help="warps (modes) per block; 0 = the library default")
     ap.add_argument("--ref-sample", type=int, default=24)
     ap.add_argument("--cpu-sample", type=int, default=16)

@@ -1,8 +1,12 @@
-// Host entry of the background and Recfast thermal history (discoeb_background): the double
+// Entries of the background and Recfast thermal history.  discoeb_background (host): the double
 // pass for the values, one forward-mode pass per parameter direction for the tangents, each
-// direction on its own host thread.
+// direction on its own host thread.  discoeb_background_batch (device): the same passes for many
+// cosmologies at once, one GPU thread per (cosmology, pass), each with its own workspace.
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "background.cuh"
@@ -13,7 +17,7 @@ namespace {
 using dscb::bgn::Fw;
 using dscb::bgn::Params;
 
-int64_t layout_size(int N)
+BGF int64_t layout_size(int N)
 {
     return (int64_t)DISCOEB_BGS_COUNT + (int64_t)DISCOEB_BGN_COUNT * DISCOEB_NU_KNOTS + (int64_t)DISCOEB_BGT_COUNT * N;
 }
@@ -29,7 +33,7 @@ template <class T> void run(const Params<T>& P, int N, std::vector<T>& buf)
     dscb::bgn::evolve_background_core(P, N, scal, nu, th, buf.data() + size, agrid.data());
 }
 
-Params<double> params_of(const DiscoebCosmoParams& c)
+BGF Params<double> params_of(const DiscoebCosmoParams& c)
 {
     Params<double> p;
     p.H0 = c.H0; p.Omegab = c.Omegab; p.Omegam = c.Omegam; p.mnu = c.mnu; p.w0 = c.w_DE_0; p.wa = c.w_DE_a;
@@ -37,7 +41,7 @@ Params<double> params_of(const DiscoebCosmoParams& c)
     return p;
 }
 
-Params<Fw<double>> params_dual(const DiscoebCosmoParams& c, const DiscoebCosmoParams& d)
+BGF Params<Fw<double>> params_dual(const DiscoebCosmoParams& c, const DiscoebCosmoParams& d)
 {
     Params<Fw<double>> p;
     p.H0 = Fw<double>(c.H0, d.H0);
@@ -50,7 +54,78 @@ Params<Fw<double>> params_dual(const DiscoebCosmoParams& c, const DiscoebCosmoPa
     return p;
 }
 
+// bytes of one device thread's workspace: the output image, the core's work arrays, the a-grid
+template <class T> size_t thread_bytes(int N)
+{
+    const size_t b = sizeof(T) * ((size_t)layout_size(N) + (size_t)dscb::bgn::bg_work_count(N)) +
+                     sizeof(double) * ((size_t)N + 1);
+    return (b + 255) & ~(size_t)255;
+}
+
+// one thread per (cosmology c, pass d): T = double gives the values (one pass per cosmology),
+// T = Fw<double> the values and the tangent along direction d
+template <class T>
+__global__ void __launch_bounds__(64) background_batch_kernel(const DiscoebCosmoParams* __restrict__ par,
+                                                              const DiscoebCosmoParams* __restrict__ dots,
+                                                              int n_cosmo, int n_pass, int N, unsigned char* ws,
+                                                              size_t per_thread, double* out, double* out_dot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_cosmo * n_pass) return;
+    const int c = t / n_pass, d = t - c * n_pass;
+    const int64_t size = layout_size(N);
+    T* buf = reinterpret_cast<T*>(ws + (size_t)t * per_thread);
+    double* agrid = reinterpret_cast<double*>(buf + size + dscb::bgn::bg_work_count(N));
+    T* scal = buf;
+    T* nu = scal + DISCOEB_BGS_COUNT;
+    T* th = nu + (size_t)DISCOEB_BGN_COUNT * DISCOEB_NU_KNOTS;
+    if constexpr (std::is_same<T, double>::value) {
+        dscb::bgn::evolve_background_core(params_of(par[c]), N, scal, nu, th, buf + size, agrid);
+        double* o = out + (size_t)c * size;
+        for (int64_t i = 0; i < size; ++i) o[i] = buf[i];
+    } else {
+        dscb::bgn::evolve_background_core(params_dual(par[c], dots[(size_t)c * n_pass + d]), N, scal, nu, th,
+                                          buf + size, agrid);
+        double* od = out_dot + ((size_t)c * n_pass + d) * size;
+        for (int64_t i = 0; i < size; ++i) od[i] = buf[i].d;
+        if (d == 0) {
+            double* o = out + (size_t)c * size;
+            for (int64_t i = 0; i < size; ++i) o[i] = buf[i].v;
+        }
+    }
+}
+
 }  // namespace
+
+extern "C" int64_t discoeb_background_batch_workspace_bytes(int32_t n_cosmo, int32_t n_dir, int32_t num_thermo)
+{
+    if (n_cosmo < 1 || n_dir < 0 || num_thermo < 32) return -1;
+    const size_t per = n_dir == 0 ? thread_bytes<double>(num_thermo) : thread_bytes<Fw<double>>(num_thermo);
+    return (int64_t)(per * (size_t)n_cosmo * (size_t)(n_dir == 0 ? 1 : n_dir));
+}
+
+extern "C" int32_t discoeb_background_batch(const DiscoebCosmoParams* par_dev, const DiscoebCosmoParams* par_dot_dev,
+                                            int32_t n_cosmo, int32_t n_dir, int32_t num_thermo, void* workspace,
+                                            int64_t workspace_bytes, double* out_dev, double* out_dot_dev, void* stream)
+{
+    if (!par_dev || !out_dev || !workspace || n_cosmo < 1 || n_dir < 0 || num_thermo < 32 ||
+        (n_dir > 0 && (!par_dot_dev || !out_dot_dev)))
+        return DISCOEB_EINVAL;
+    if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return DISCOEB_EINVAL;
+    if (workspace_bytes < discoeb_background_batch_workspace_bytes(n_cosmo, n_dir, num_thermo)) return DISCOEB_EINVAL;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    unsigned char* ws = static_cast<unsigned char*>(workspace);
+    const int n_pass = n_dir == 0 ? 1 : n_dir;
+    const int threads = n_cosmo * n_pass, block = 64, grid = (threads + block - 1) / block;
+    if (n_dir == 0)
+        background_batch_kernel<double><<<grid, block, 0, s>>>(par_dev, nullptr, n_cosmo, 1, num_thermo, ws,
+                                                               thread_bytes<double>(num_thermo), out_dev, nullptr);
+    else
+        background_batch_kernel<Fw<double>><<<grid, block, 0, s>>>(par_dev, par_dot_dev, n_cosmo, n_dir, num_thermo,
+                                                                   ws, thread_bytes<Fw<double>>(num_thermo), out_dev,
+                                                                   out_dot_dev);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
 
 extern "C" int64_t discoeb_background_size(int32_t num_thermo)
 {

@@ -196,6 +196,10 @@ def lib():
         L.discoeb_background.argtypes = [ctypes.POINTER(DiscoebCosmoParams), vp, ctypes.c_int32, ctypes.c_int32, vp, vp,
                                          ctypes.c_int32]
         L.discoeb_background.restype = ctypes.c_int32
+        L.discoeb_background_batch_workspace_bytes.argtypes = [c32, c32, c32]
+        L.discoeb_background_batch_workspace_bytes.restype = c64
+        L.discoeb_background_batch.argtypes = [vp, vp, c32, c32, c32, vp, c64, vp, vp, vp]
+        L.discoeb_background_batch.restype = c32
         if L.discoeb_abi_version() != ABI_VERSION:
             raise RuntimeError("libdiscoeb_b200.so ABI version mismatch; rebuild it")
         _lib = L

@@ -158,6 +158,43 @@ def native_background(param, num_thermo=256, param_dots=(), n_threads=0):
     return out, out_dot
 
 
+def native_backgrounds_device(params, num_thermo=256, param_dots=None, device=None):
+    """``discoeb_background_batch``: the backgrounds of many cosmologies (and, with ``param_dots``,
+    a list per cosmology of dicts of d(H0, Omegab, Omegam, mnu, w_DE_0, w_DE_a), the same number for
+    every cosmology) in one GPU launch.  Returns device tensors (values [C, size], tangents
+    [C, n_dir, size] or None)."""
+    import torch
+
+    from . import _abi
+    lib = _abi.lib()
+    if device is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    C = len(params)
+    nd = len(param_dots[0]) if param_dots else 0
+    if param_dots and any(len(d) != nd for d in param_dots):
+        raise ValueError("every cosmology needs the same number of tangent directions")
+    _, size = _abi.background_layout(num_thermo)
+    host = (_abi.DiscoebCosmoParams * C)(*[_params_struct(p) for p in params])
+    par = torch.frombuffer(bytearray(bytes(host)), dtype=torch.uint8).to(device)
+    dots = None
+    if nd:
+        hd = (_abi.DiscoebCosmoParams * (C * nd))(*[_params_struct(d, _DIFF_FIELDS) for ds in param_dots for d in ds])
+        dots = torch.frombuffer(bytearray(bytes(hd)), dtype=torch.uint8).to(device)
+    wsb = lib.discoeb_background_batch_workspace_bytes(C, nd, int(num_thermo))
+    if wsb < 0:
+        raise ValueError("discoeb_background_batch_workspace_bytes rejected its arguments (num_thermo >= 32)")
+    ws = torch.empty(int(wsb) + 256, dtype=torch.uint8, device=device)
+    base = (ws.data_ptr() + 255) & ~255
+    out = torch.empty((C, size), dtype=torch.float64, device=device)
+    out_dot = torch.empty((C, nd, size), dtype=torch.float64, device=device) if nd else None
+    rc = lib.discoeb_background_batch(par.data_ptr(), dots.data_ptr() if nd else None, C, nd, int(num_thermo), base,
+                                      int(wsb), out.data_ptr(), out_dot.data_ptr() if nd else None,
+                                      torch.cuda.current_stream(device).cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"discoeb_background_batch failed with code {rc}")
+    return out, out_dot
+
+
 def background_from_buffer(param, buf, num_thermo):
     """The evolve_background dict of ``param`` from a discoeb_background value buffer."""
     from . import _abi

@@ -144,17 +144,24 @@ def _tangent_from_buffers(bg, buf, dot, num_thermo, aexp_out, tau_start, kmodes,
     return d
 
 
-def cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo=256, host_backend="native", host_threads=0):
+def cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo=256, host_backend="native", host_threads=0,
+                       buffers=None):
     """Host prologue of one cosmology's P(k) Jacobian: background, output and start times,
     initial states, switch times and the per-direction tangents (ODE_DIRECTIONS).
 
     ``host_backend``: "native" (discoeb_background with ``host_threads`` threads, 0: one per
     direction) or "numpy" (complex step through the numpy restatement, Recfast steps replayed,
-    ``host_threads`` spawned processes)."""
+    ``host_threads`` spawned processes).  ``buffers``: the (values, tangents) buffers of this
+    cosmology's background when they were computed already (discoeb_background_batch)."""
     import warnings
     aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
     kmodes = np.ascontiguousarray(kmodes, dtype=np.float64)
-    if host_backend == "native":
+    if buffers is not None:
+        host_backend = "native"
+        p = theta_to_params(theta)
+        buf, dots = buffers
+        bg = background_from_buffer(p, buf, num_thermo)
+    elif host_backend == "native":
         p = theta_to_params(theta)
         buf, dots = native_background(p, num_thermo, param_dots(theta, ODE_DIRECTIONS), host_threads)
         bg = background_from_buffer(p, buf, num_thermo)
@@ -337,8 +344,10 @@ class JacobianBatch:
     ``thetas``: list of C theta dicts; ``kmodes``: ``[K]`` shared by all cosmologies.  The host
     prologue (cosmology_prologue) runs per cosmology: in the calling process when
     ``host_processes`` is 1 (each with ``host_threads`` threads), else in a persistent pool of
-    spawned processes (0: up to the host's cores).  ``launch`` / ``result`` as JacobianProblem;
-    result returns ``(P [C, K, nout], J [C, 8, K, nout], status [C, K], nsteps [C, K])``.
+    spawned processes (0: up to the host's cores).  ``host_backend="device"`` computes all the
+    backgrounds and their tangents in one GPU launch (discoeb_background_batch) first.
+    ``launch`` / ``result`` as JacobianProblem; result returns
+    ``(P [C, K, nout], J [C, 8, K, nout], status [C, K], nsteps [C, K])``.
     """
 
     def __init__(self, thetas, *, kmodes, aexp_out=(1.0,), lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5,
@@ -359,7 +368,14 @@ class JacobianBatch:
         nproc = (os.cpu_count() or 1) if not host_processes else host_processes
         nproc = min(nproc, len(thetas))
         threads = host_threads if nproc <= 1 else max(host_threads, 1)
-        args = [(dict(t), aexp_out, kmodes, L, num_thermo, host_backend, threads) for t in thetas]
+        bufs = [None] * len(thetas)
+        if host_backend == "device":
+            from .background import native_backgrounds_device
+            out, out_dot = native_backgrounds_device([theta_to_params(t) for t in thetas], num_thermo,
+                                                     [param_dots(t, ODE_DIRECTIONS) for t in thetas], device=device)
+            out, out_dot = out.cpu().numpy(), out_dot.cpu().numpy()
+            bufs = [(out[c], out_dot[c]) for c in range(len(thetas))]
+        args = [(dict(t), aexp_out, kmodes, L, num_thermo, host_backend, threads, b) for t, b in zip(thetas, bufs)]
         pro = [_prologue_task(a) for a in args] if nproc <= 1 else _pool(nproc).map(_prologue_task, args)
         C, K, nout, n = len(pro), kmodes.shape[0], aexp_out.shape[0], nvar_of(**L)
         nd = len(ODE_DIRECTIONS)

@@ -495,12 +495,17 @@ def _background_worker(p):
         return evolve_background(param=p)
 
 
-def backgrounds(param_dicts, processes=1):
-    """evolve_background of many cosmologies on the host.  The native background takes a few
-    milliseconds per cosmology, so they run in this process by default; ``processes`` > 1 (or 0:
-    the host's cores) spreads them over a pool of spawned processes (safe after CUDA is
-    initialised)."""
+def backgrounds(param_dicts, processes=1, device=None, num_thermo=256):
+    """evolve_background of many cosmologies.  The native background takes a few milliseconds per
+    cosmology, so they run in this process by default; ``processes`` > 1 (or 0: the host's cores)
+    spreads them over a pool of spawned processes (safe after CUDA is initialised); ``device``
+    (a CUDA device) computes them all in one GPU launch (discoeb_background_batch)."""
     param_dicts = list(param_dicts)
+    if device is not None:
+        from .background import background_from_buffer, native_backgrounds_device
+        out, _ = native_backgrounds_device(param_dicts, num_thermo, device=device)
+        out = out.cpu().numpy()
+        return [background_from_buffer(p, out[c], num_thermo) for c, p in enumerate(param_dicts)]
     if len(param_dicts) <= 1 or processes == 1:
         return [_background_worker(p) for p in param_dicts]
     import multiprocessing as mp

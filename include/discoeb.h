@@ -336,6 +336,18 @@ int64_t discoeb_background_size(int32_t num_thermo);
 int32_t discoeb_background(const DiscoebCosmoParams* par, const DiscoebCosmoParams* par_dot, int32_t n_dir,
                            int32_t num_thermo, double* out, double* out_dot, int32_t n_threads);
 
+/* The same for n_cosmo cosmologies on the GPU, batched over cosmologies (one device thread per
+ * cosmology and direction, each running the whole sequential background; stream-ordered):
+ *   par_dev [n_cosmo], par_dot_dev [n_cosmo, n_dir]      device arrays (par_dot_dev NULL if n_dir = 0)
+ *   out_dev [n_cosmo, size], out_dot_dev [n_cosmo, n_dir, size]   device, size = discoeb_background_size
+ *   workspace: discoeb_background_batch_workspace_bytes(...) bytes of 256-byte-aligned device memory
+ * Same layout as discoeb_background; the values agree with it up to the last bits of the device's
+ * exp/log/pow (amplified downstream of Recfast's Saha x_H formula, as between any two libms). */
+int64_t discoeb_background_batch_workspace_bytes(int32_t n_cosmo, int32_t n_dir, int32_t num_thermo);
+int32_t discoeb_background_batch(const DiscoebCosmoParams* par_dev, const DiscoebCosmoParams* par_dot_dev,
+                                 int32_t n_cosmo, int32_t n_dir, int32_t num_thermo, void* workspace,
+                                 int64_t workspace_bytes, double* out_dev, double* out_dot_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
