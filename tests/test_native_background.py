@@ -143,3 +143,24 @@ def test_native_tangents_match_central_differences_of_smooth_parts(name):
         np.testing.assert_allclose(d[lay[key]], fd[lay[key]], rtol=1e-6, atol=1e-9 * np.abs(fd[lay[key]]).max() + 1e-14)
     # tau at the Recfast knots: an integral of 1/(da/dtau) (smooth in the parameters)
     np.testing.assert_allclose(d[lay["t:tau"]], fd[lay["t:tau"]], rtol=1e-6, atol=1e-8 * np.abs(fd[lay["t:tau"]]).max())
+
+
+def test_background_batch_entry_validates_arguments():
+    """The device entry rejects bad sizes and workspaces before it touches a GPU (every call below
+    returns at its argument checks; the pointer values are never dereferenced)."""
+    lib = _abi.lib()
+    N = 256
+    _, size = _abi.background_layout(N)
+    work = 2 * max(N, _abi.NU_KNOTS) + 6 * N
+    per_fw = (16 * (size + work) + 8 * (N + 1) + 255) // 256 * 256
+    per_d = (8 * (size + work) + 8 * (N + 1) + 255) // 256 * 256
+    assert lib.discoeb_background_batch_workspace_bytes(4, 6, N) == 4 * 6 * per_fw
+    assert lib.discoeb_background_batch_workspace_bytes(4, 0, N) == 4 * per_d
+    for args in ((0, 6, N), (4, -1, N), (4, 6, 16)):
+        assert lib.discoeb_background_batch_workspace_bytes(*args) == -1
+    ws = lib.discoeb_background_batch_workspace_bytes(4, 0, N)
+    fake = 0x10000  # never dereferenced: each call fails its checks first
+    assert lib.discoeb_background_batch(None, None, 4, 0, N, fake, ws, fake, None, None) == -1
+    assert lib.discoeb_background_batch(fake, None, 4, 0, N, fake + 8, ws, fake, None, None) == -1  # misaligned
+    assert lib.discoeb_background_batch(fake, None, 4, 0, N, fake, ws - 1, fake, None, None) == -1  # too small
+    assert lib.discoeb_background_batch(fake, None, 4, 2, N, fake, ws, fake, None, None) == -1  # no tangent arrays
