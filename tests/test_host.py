@@ -98,3 +98,28 @@ int main(void){printf("%zu %zu %zu %zu %zu %zu %d %d %d %d\n", sizeof(DiscoebCos
     assert [int(v) for v in out] == [ctypes.sizeof(C), C.q.offset, C.xe_loga.offset, ctypes.sizeof(K),
                                      K.max_steps.offset, ctypes.sizeof(_abi.DiscoebCosmoParams), len(_abi.BGS),
                                      len(_abi.BGN), len(_abi.BGT), _abi.NU_KNOTS]
+
+
+def test_plain_c_caller_of_the_background_entry():
+    """The C ABI from C: a program that includes discoeb.h and links the library gets the same
+    background scalars and H0-derivatives as the Python layer (host entry; no GPU needed)."""
+    import tempfile
+
+    from discoeb_b200.background import native_background
+    from discoeb_b200.workloads import cosmo_params
+    libdir = os.path.join(ROOT, "disco-eb_b200", "discoeb_b200")
+    if not os.path.exists(os.path.join(libdir, _abi.LIB_NAME)):
+        subprocess.run(["python", os.path.join(ROOT, "disco-eb_b200", "build.py")], check=True)
+    p = cosmo_params(m_nu=0.06, w0=-0.95, wa=0.1)
+    with tempfile.TemporaryDirectory() as d:
+        exe = os.path.join(d, "bg")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", exe,
+                        os.path.join(ROOT, "tests", "c_abi", "background_from_c.c"), "-L", libdir,
+                        "-l:" + _abi.LIB_NAME, "-Wl,-rpath," + libdir], check=True)
+        args = [repr(float(p[k])) for k in ("H0", "Omegab", "Omegam", "mnu", "w_DE_0", "w_DE_a")]
+        txt = subprocess.run([exe, *args], capture_output=True, text=True, check=True).stdout.split()
+    got = np.array([float(v) for v in txt]).reshape(-1, 2)
+    buf, dots = native_background(p, 256, [{"H0": 1.0}])
+    assert got.shape == (len(_abi.BGS), 2)
+    np.testing.assert_array_equal(got[:, 0], buf[: len(_abi.BGS)])
+    np.testing.assert_array_equal(got[:, 1], dots[0][: len(_abi.BGS)])
