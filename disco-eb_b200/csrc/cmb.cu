@@ -23,6 +23,7 @@
 #include <mutex>
 
 #include "discoeb.h"
+#include "fft_plans.cuh"
 #include "lngamma.cuh"
 #include "stepper.cuh"
 
@@ -461,22 +462,6 @@ LosLayout los_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n_dense,
     return L;
 }
 
-int make_fft_plan(cufftHandle* plan, int n_fft, int n_rows, long long pitch, size_t* work)
-{
-    if (cufftCreate(plan) != CUFFT_SUCCESS) return DISCOEB_ECUDA;
-    cufftSetAutoAllocation(*plan, 0);
-    long long nn[1] = {n_fft};
-    long long inembed[1] = {pitch}, onembed[1] = {pitch / 2};
-    size_t ws = 0;
-    if (cufftMakePlanMany64(*plan, 1, nn, inembed, 1, pitch, onembed, 1, pitch / 2, CUFFT_D2Z, n_rows, &ws) !=
-        CUFFT_SUCCESS) {
-        cufftDestroy(*plan);
-        return DISCOEB_ECUDA;
-    }
-    *work = ws;
-    return DISCOEB_SUCCESS;
-}
-
 std::mutex g_blas_mu;
 cublasHandle_t g_blas[64] = {};
 
@@ -558,10 +543,11 @@ int64_t discoeb_los_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellm
     if (n_modes < 2 || n_tau < 3 || ellmax < 0 || n_fftlog < 2 || n_k_dense < 0 || n_k_dense == 1)
         return DISCOEB_EINVAL;
     const int rows = n_k_dense > 0 ? n_k_dense : n_modes;
+    const long long pitch = 2LL * (n_fftlog / 2 + 1);
     cufftHandle plan;
     size_t work = 0;
-    if (make_fft_plan(&plan, n_fftlog, rows, 2LL * (n_fftlog / 2 + 1), &work) != DISCOEB_SUCCESS) return DISCOEB_ECUDA;
-    cufftDestroy(plan);
+    std::lock_guard<std::mutex> lock(discoeb_fft::plan_mutex());
+    if (!discoeb_fft::cached_plan(CUFFT_D2Z, n_fftlog, rows, pitch, pitch / 2, &plan, &work)) return DISCOEB_ECUDA;
     return (int64_t)los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work).total;
 }
 
@@ -575,15 +561,13 @@ int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
     if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return DISCOEB_EINVAL;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int rows = n_k_dense > 0 ? n_k_dense : n_modes;
+    const long long pitch = 2LL * (n_fftlog / 2 + 1);
     cufftHandle plan;
     size_t work = 0;
-    int rc = make_fft_plan(&plan, n_fftlog, rows, 2LL * (n_fftlog / 2 + 1), &work);
-    if (rc) return rc;
+    std::unique_lock<std::mutex> fft_lock(discoeb_fft::plan_mutex());
+    if (!discoeb_fft::cached_plan(CUFFT_D2Z, n_fftlog, rows, pitch, pitch / 2, &plan, &work)) return DISCOEB_ECUDA;
     const LosLayout L = los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work);
-    if ((uint64_t)workspace_bytes < L.total) {
-        cufftDestroy(plan);
-        return DISCOEB_EINVAL;
-    }
+    if ((uint64_t)workspace_bytes < L.total) return DISCOEB_EINVAL;
     char* ws = static_cast<char*>(workspace);
     auto D = [&](size_t off) { return reinterpret_cast<double*>(ws + off); };
     const int T = 256;
@@ -611,11 +595,12 @@ int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
     chi_eval_kernel<<<blocks_for((long long)rows * n_fftlog, T), T, 0, s>>>(
         rows, n_tau, D(L.lchi), Srow, D(L.s2c), n_fftlog, reinterpret_cast<const int*>(ws + L.fidx), D(L.fx),
         D(L.fbias), L.pitch, D(L.fft));
-    // 3. rfft of every row, in place
+    // 3. rfft of every row, in place (the plan lock is held from the lookup to here, so no other
+    //    call can evict the plan or change its work area in between)
     cufftSetWorkArea(plan, ws + L.cufft);
     cufftSetStream(plan, s);
     const cufftResult fr = cufftExecD2Z(plan, D(L.fft), reinterpret_cast<cufftDoubleComplex*>(D(L.fft)));
-    cufftDestroy(plan);
+    fft_lock.unlock();
     if (fr != CUFFT_SUCCESS) return DISCOEB_ECUDA;
     // 4. ck in place, and the M table
     ck_kernel<<<blocks_for((long long)rows * L.n_freq, T), T, 0, s>>>(rows, krow, n_fftlog, L.n_freq, D(L.geom),

@@ -12,6 +12,7 @@
 #include <cstdint>
 
 #include "discoeb.h"
+#include "fft_plans.cuh"
 #include "lngamma.cuh"
 
 using namespace dscb::cplx;
@@ -124,22 +125,15 @@ struct XiLayout {
     size_t f, F, work, total, cufft_bytes;
 };
 
+// the cached forward (D2Z) and inverse (Z2D) plans of one length-n transform; the caller holds
+// discoeb_fft::plan_mutex()
 int xi_plans(int n, cufftHandle* fwd, cufftHandle* inv, size_t* work)
 {
     size_t w1 = 0, w2 = 0;
-    if (cufftCreate(fwd) != CUFFT_SUCCESS) return DISCOEB_ECUDA;
-    if (cufftCreate(inv) != CUFFT_SUCCESS) {
-        cufftDestroy(*fwd);
+    const long long nf = n / 2 + 1;
+    if (!discoeb_fft::cached_plan(CUFFT_D2Z, n, 1, n, nf, fwd, &w1) ||
+        !discoeb_fft::cached_plan(CUFFT_Z2D, n, 1, nf, n, inv, &w2))
         return DISCOEB_ECUDA;
-    }
-    cufftSetAutoAllocation(*fwd, 0);
-    cufftSetAutoAllocation(*inv, 0);
-    if (cufftMakePlan1d(*fwd, n, CUFFT_D2Z, 1, &w1) != CUFFT_SUCCESS ||
-        cufftMakePlan1d(*inv, n, CUFFT_Z2D, 1, &w2) != CUFFT_SUCCESS) {
-        cufftDestroy(*fwd);
-        cufftDestroy(*inv);
-        return DISCOEB_ECUDA;
-    }
     *work = w1 > w2 ? w1 : w2;
     return DISCOEB_SUCCESS;
 }
@@ -205,9 +199,8 @@ int64_t discoeb_xi_workspace_bytes(int32_t n_k)
     if (n_k < 2 || n_k % 2 != 0) return -1;
     cufftHandle a, b;
     size_t work = 0;
+    std::lock_guard<std::mutex> lock(discoeb_fft::plan_mutex());
     if (xi_plans(n_k, &a, &b, &work) != DISCOEB_SUCCESS) return -1;
-    cufftDestroy(a);
-    cufftDestroy(b);
     return (int64_t)xi_layout(n_k, work).total;
 }
 
@@ -218,13 +211,10 @@ int32_t discoeb_xi_from_power(int32_t n_k, const double* kmodes, const double* P
     if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return DISCOEB_EINVAL;
     cufftHandle fwd, inv;
     size_t work = 0;
+    std::lock_guard<std::mutex> lock(discoeb_fft::plan_mutex());
     if (xi_plans(n_k, &fwd, &inv, &work) != DISCOEB_SUCCESS) return DISCOEB_ECUDA;
     const XiLayout L = xi_layout(n_k, work);
-    if ((int64_t)L.total > workspace_bytes) {
-        cufftDestroy(fwd);
-        cufftDestroy(inv);
-        return DISCOEB_EINVAL;
-    }
+    if ((int64_t)L.total > workspace_bytes) return DISCOEB_EINVAL;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     char* ws = static_cast<char*>(workspace);
     double* f = reinterpret_cast<double*>(ws + L.f);
@@ -245,8 +235,6 @@ int32_t discoeb_xi_from_power(int32_t n_k, const double* kmodes, const double* P
     }
     if (rc == DISCOEB_SUCCESS) xi_out_kernel<<<blocks_for(n_k, 128), 128, 0, s>>>(n_k, kmodes, f, sign, xi, r);
     if (cudaGetLastError() != cudaSuccess) rc = DISCOEB_ECUDA;
-    cufftDestroy(fwd);
-    cufftDestroy(inv);
     return rc;
 }
 
