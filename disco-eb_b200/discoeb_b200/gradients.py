@@ -23,6 +23,7 @@ analytically.
 from __future__ import annotations
 
 import ctypes
+import threading
 
 import numpy as np
 
@@ -144,6 +145,28 @@ def _tangent_from_buffers(bg, buf, dot, num_thermo, aexp_out, tau_start, kmodes,
     return d
 
 
+def _native_tangents_in_background(param, num_thermo, dots, n_threads):
+    """Start discoeb_background's tangent passes on a helper thread (the C++ passes hold no GIL);
+    the returned function waits for them and returns the tangent buffers."""
+    box = {}
+
+    def run():
+        try:
+            box["dots"] = native_background(param, num_thermo, dots, n_threads)[1]
+        except BaseException as e:  # re-raised in the caller's thread
+            box["error"] = e
+
+    t = threading.Thread(target=run, daemon=True)
+    t.start()
+
+    def wait():
+        t.join()
+        if "error" in box:
+            raise box["error"]
+        return box["dots"]
+    return wait
+
+
 def cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo=256, host_backend="native", host_threads=0,
                        buffers=None):
     """Host prologue of one cosmology's P(k) Jacobian: background, output and start times,
@@ -162,8 +185,11 @@ def cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo=256, host_backend=
         buf, dots = buffers
         bg = background_from_buffer(p, buf, num_thermo)
     elif host_backend == "native":
+        # the tangent passes run while this thread takes the values alone (the same bits as the
+        # value part of the tangent passes) and the start times, initial states and switch times
         p = theta_to_params(theta)
-        buf, dots = native_background(p, num_thermo, param_dots(theta, ODE_DIRECTIONS), host_threads)
+        wait_dots = _native_tangents_in_background(p, num_thermo, param_dots(theta, ODE_DIRECTIONS), host_threads)
+        buf = native_background(p, num_thermo)[0]
         bg = background_from_buffer(p, buf, num_thermo)
     elif host_backend == "numpy":
         trace = {}
@@ -179,6 +205,8 @@ def cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo=256, host_backend=
     y0 = adiabatic_ics(tau=tau_start, param=bg, kmode=kmodes, **L)
     sw = approximation_switch_times(bg, kmodes)
     if host_backend == "native":
+        if buffers is None:
+            dots = wait_dots()
         tans = [_tangent_from_buffers(bg, buf, d, num_thermo, aexp_out, tau_start, kmodes, L) for d in dots]
     else:
         tans = background_tangents(theta, bg, trace, ODE_DIRECTIONS, aexp_out=aexp_out, tau_start=tau_start,

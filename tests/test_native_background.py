@@ -121,6 +121,26 @@ def test_native_tangents_match_complex_step_of_numpy_restatement():
         assert np.all(np.abs(a["y0"] - b["y0"]) <= 1e-9 * y0_scale + 1e-9 * np.abs(b["y0"])), name
 
 
+def test_overlapped_prologue_equals_one_background_call():
+    """The native prologue takes the values from a value-only call while the tangent passes run
+    on a helper thread: the result equals the prologue built from one call's buffers, bit for bit."""
+    theta = dict(omega_c=0.118, omega_b=0.0221, h=0.69, n_s=0.965, ln10As=np.log(21.0), w0=-0.95, wa=-0.1, m_nu=0.1)
+    ks, aout = np.geomspace(1e-4, 5.0, 24), np.array([0.5, 1.0])
+    p = theta_to_params(theta)
+    one = native_background(p, 256, param_dots(theta, ODE_DIRECTIONS))
+    a = cosmology_prologue(theta, aout, ks, L)
+    b = cosmology_prologue(theta, aout, ks, L, buffers=one)
+    for k in ("tau_out", "tau_start", "y0", "sw"):
+        np.testing.assert_array_equal(a[k], b[k])
+    for ta, tb in zip(a["tans"], b["tans"]):
+        assert ta["scalars"] == tb["scalars"]
+        np.testing.assert_array_equal(ta["tau_out"], tb["tau_out"])
+        np.testing.assert_array_equal(ta["y0"], tb["y0"])
+        for short, (yy, SS) in tb["tables"].items():
+            np.testing.assert_array_equal(ta["tables"][short][0], yy)
+            np.testing.assert_array_equal(ta["tables"][short][1], SS)
+
+
 @pytest.mark.parametrize("name", ["h", "w0", "m_nu"])
 def test_native_tangents_match_central_differences_of_smooth_parts(name):
     """Scalars, conformal times and the neutrino tables do not go through Recfast's branches:
