@@ -168,6 +168,34 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def fp64_fma_tflops(torch, device):
+    """Measured FP64 FMA throughput on this GPU (discoeb_fma_rate: 8 independent FMA chains per
+    thread, 4 x 256 threads per SM, 65536 iterations), best of 5 launches."""
+    import ctypes
+    from discoeb_b200 import _abi
+    lib = _abi.lib()
+    n = int(lib.discoeb_fma_rate_threads())
+    if n <= 0:
+        raise RuntimeError(f"discoeb_fma_rate_threads failed with code {n}")
+    out = torch.empty(n, dtype=torch.float64, device=device)
+    stream = torch.cuda.current_stream(device)
+    flops = ctypes.c_double(0.0)
+    best = 0.0
+    for i in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = lib.discoeb_fma_rate(65536, out.data_ptr(), n, ctypes.byref(flops), stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        if rc != 0:
+            raise RuntimeError(f"discoeb_fma_rate failed with code {rc}")
+        if i > 0:
+            best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    if not bool(torch.isfinite(out).all()):
+        raise RuntimeError("discoeb_fma_rate produced non-finite values")
+    return best
+
+
 def fp64_peak_tflops(torch, device):
     """Measured FP64 peak on this GPU: cuBLAS DGEMM 8192^3, best of 5."""
     n = 8192
@@ -501,7 +529,8 @@ def main():
     work = step_attempts * (flops_per_step + tangent_per_step * n_dir) if grad else step_attempts * flops_per_step
     dense_work = step_attempts * dense_per_step * (1 + n_dir)
     achieved = work / (ms / 1e3) / 1e12
-    peak = fp64_peak_tflops(torch, device) if rank == 0 and not args.kernel_only else None
+    peak = fp64_fma_tflops(torch, device) if rank == 0 and not args.kernel_only else None
+    dgemm = fp64_peak_tflops(torch, device) if rank == 0 and not args.kernel_only else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.kernel_only:
@@ -538,7 +567,8 @@ def main():
                          "frac": (achieved / peak) if peak else None,
                          "traffic": DRAM_BYTES_PER_MODE.get(args.mode, 0.0) * K or None,
                          "traffic_source": "ncu capture of 48 modes of the same kernel, scaled by the mode count",
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                         "peak_source": "FP64 FMA throughput measured in this run (discoeb_fma_rate)",
+                         "fp64_dgemm_tflops": dgemm,
                          "dense_equivalent_tflops": dense_work / (ms / 1e3) / 1e12},
             "clocks": clocks,
         }

@@ -200,6 +200,10 @@ def lib():
         L.discoeb_background_batch_workspace_bytes.restype = c64
         L.discoeb_background_batch.argtypes = [vp, vp, c32, c32, c32, vp, c64, vp, vp, vp]
         L.discoeb_background_batch.restype = c32
+        L.discoeb_fma_rate_threads.argtypes = []
+        L.discoeb_fma_rate_threads.restype = c64
+        L.discoeb_fma_rate.argtypes = [c64, vp, c64, ctypes.POINTER(ctypes.c_double), vp]
+        L.discoeb_fma_rate.restype = c32
         if L.discoeb_abi_version() != ABI_VERSION:
             raise RuntimeError("libdiscoeb_b200.so ABI version mismatch; rebuild it")
         _lib = L

@@ -348,6 +348,16 @@ int32_t discoeb_background_batch(const DiscoebCosmoParams* par_dev, const Discoe
                                  int32_t n_cosmo, int32_t n_dir, int32_t num_thermo, void* workspace,
                                  int64_t workspace_bytes, double* out_dev, double* out_dot_dev, void* stream);
 
+/* Measurement utility, no counterpart in the reference: the FP64 fused-multiply-add throughput of
+ * the current GPU, the roofline denominator of the solver kernels (their arithmetic is FP64 FMA
+ * work).  discoeb_fma_rate_threads() returns the thread count of one launch (4 blocks of 256 per
+ * SM; negative on a CUDA error).  discoeb_fma_rate enqueues one launch on `stream` in which every
+ * thread runs 8 independent FMA chains for `iters` iterations, writes one double per thread to
+ * `out` (device, n_out >= discoeb_fma_rate_threads()) and stores the launch's flop count
+ * (2 per FMA) in *flops (host); the caller times the launch. */
+int64_t discoeb_fma_rate_threads(void);
+int32_t discoeb_fma_rate(int64_t iters, double* out, int64_t n_out, double* flops, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

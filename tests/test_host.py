@@ -67,7 +67,7 @@ def test_library_exports_every_declared_symbol():
             txt = open(os.path.join(ROOT, "include", h)).read()
             declared |= set(re.findall(r"^\s*(?:int32_t|int64_t|void|double)\s+(discoeb_\w+)\s*\(", txt, re.M))
     assert {"discoeb_fwd", "discoeb_rhs", "discoeb_nvar", "discoeb_abi_version", "discoeb_los_workspace_bytes",
-            "discoeb_background", "discoeb_background_size"} <= declared
+            "discoeb_background", "discoeb_background_size", "discoeb_fma_rate", "discoeb_fma_rate_threads"} <= declared
     lib = ctypes.CDLL(path)
     for name in declared:
         assert hasattr(lib, name), name
@@ -76,6 +76,16 @@ def test_library_exports_every_declared_symbol():
     c.lmaxg, c.lmaxgp, c.lmaxr, c.lmaxnu, c.nqmax = 12, 12, 17, 17, 5
     lib.discoeb_nvar.restype = ctypes.c_int32
     assert lib.discoeb_nvar(ctypes.byref(c)) == 143
+
+
+def test_fma_rate_entry_rejects_bad_arguments_before_any_launch():
+    lib = _abi.lib()
+    flops = ctypes.c_double(-1.0)
+    # checked before the device is touched, so these run without a GPU
+    assert lib.discoeb_fma_rate(0, 256, 1 << 20, ctypes.byref(flops), None) == -1
+    assert lib.discoeb_fma_rate(10, None, 1 << 20, ctypes.byref(flops), None) == -1
+    assert lib.discoeb_fma_rate(10, 256, 1 << 20, None, None) == -1
+    assert flops.value == -1.0
 
 
 def test_struct_layout_matches_header():
