@@ -135,7 +135,9 @@ constexpr int kMaxDirsPerBlock = 6;
 // Output fields and their tangents at output time j of one (mode, direction): the tangent of
 // the state at the moving output time is y' + f tau_out', then the RSA projection and the
 // output conversion in dual numbers.  y: the forward state at tau_out[j]; pf: n doubles of
-// scratch; TT.fd / TT.jk are used as scratch.
+// scratch; TT.fd / TT.jk are used as scratch.  Full: the RSA-projected state and its tangent
+// (n values per output) are written instead of the 20 output fields.
+template <bool Full>
 __device__ void emit_tangent_output(const WarpTeam& tm, const DiscoebCosmo& P, const DiscoebTangent* TN, const Dims& D,
                                     double k, int mode, int dir, int n_modes, int n_out, int j, const double* tau_out,
                                     const double* tau_out_dot, const double* y, int regime, const TanMem& TT,
@@ -160,10 +162,17 @@ __device__ void emit_tangent_output(const WarpTeam& tm, const DiscoebCosmo& P, c
             if (sl >= 0) { v = fld[sl].v; vd = fld[sl].d; }
             else if (sl == -1) { v = 0.0; vd = 0.0; }
         }
-        pf[i] = v;
-        TT.fd[i] = vd;
+        if constexpr (Full) {
+            const size_t oo = (size_t)mode * n_out + j;
+            y_out20_dot[((size_t)dir * n_modes * n_out + oo) * n + i] = vd;
+            if (dir == 0 && y_out20) y_out20[oo * n + i] = v;
+        } else {
+            pf[i] = v;
+            TT.fd[i] = vd;
+        }
     }
     tm.sync();
+    if constexpr (Full) return;
     if (tm.leader()) {
         Dual o[20];
         output_vars<Dual>(P, TN, D, k, pf, TT.fd, o);
@@ -204,6 +213,7 @@ __device__ bool wait_at_least(const WarpTeam& tm, volatile int* flag, int target
 // consumed), every wait bounded (wait_at_least); if a wait gives up, the whole block stops and
 // reports DISCOEB_ABORTED.  The step sequence is the forward's only, so the tangent is the
 // derivative of the discrete solution with the accepted steps held fixed.
+template <bool Full>
 __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     const DiscoebCosmo* __restrict__ cosmos, int n_cosmo, const int32_t* __restrict__ mode_cosmo,
     const DiscoebTangent* __restrict__ tangents, int n_dir, int dpb,
@@ -226,10 +236,12 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
             status[mode] = DISCOEB_BAD_INDEX;
             nsteps[mode] = 0;
         }
+        // outputs of width 20 (fields) or, for Full, the state size of the first cosmology
+        const int W = Full ? make_dims(cosmos[0]).n : 20;
         for (int dd = 0; dd < nd; ++dd)
-            for (int i = threadIdx.x; i < n_out * 20; i += blockDim.x) {
-                y_out20_dot[((size_t)(d0 + dd) * n_modes + mode) * n_out * 20 + i] = qn;
-                if (d0 + dd == 0 && y_out20) y_out20[(size_t)mode * n_out * 20 + i] = qn;
+            for (int i = threadIdx.x; i < n_out * W; i += blockDim.x) {
+                y_out20_dot[((size_t)(d0 + dd) * n_modes + mode) * n_out * W + i] = qn;
+                if (d0 + dd == 0 && y_out20) y_out20[(size_t)mode * n_out * W + i] = qn;
             }
         return;
     }
@@ -275,9 +287,10 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
             }
         } else {
             const int dir = d0 + warp - 1;
-            for (int i = tm.lane; i < n_out * 20; i += 32) {
-                y_out20_dot[((size_t)dir * n_modes + mode) * n_out * 20 + i] = qn;
-                if (dir == 0 && y_out20) y_out20[(size_t)mode * n_out * 20 + i] = qn;
+            const int W = Full ? make_dims(cosmos[0]).n : 20;
+            for (int i = tm.lane; i < n_out * W; i += 32) {
+                y_out20_dot[((size_t)dir * n_modes + mode) * n_out * W + i] = qn;
+                if (dir == 0 && y_out20) y_out20[(size_t)mode * n_out * W + i] = qn;
             }
         }
         return;
@@ -370,16 +383,18 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
         }
         tm.sync();
         while (iout < n_out && tout[iout] <= tnext) {
-            emit_tangent_output(tm, *P, TN, D, k, mode, dir, n_modes, n_out, iout, tout, tau_out_dot, yend, regime, TT,
-                                pf, y_out20, y_out20_dot);
+            emit_tangent_output<Full>(tm, *P, TN, D, k, mode, dir, n_modes, n_out, iout, tout, tau_out_dot, yend,
+                                      regime, TT, pf, y_out20, y_out20_dot);
             ++iout;
         }
     }
+    constexpr int W20 = 20;
+    const int W = Full ? n : W20;
     for (int j = iout; j < n_out; ++j) {
         const size_t oo = (size_t)mode * n_out + j;
-        for (int i = tm.lane; i < 20; i += 32) {
-            y_out20_dot[((size_t)dir * n_modes * n_out + oo) * 20 + i] = qnan;
-            if (dir == 0 && y_out20) y_out20[oo * 20 + i] = qnan;
+        for (int i = tm.lane; i < W; i += 32) {
+            y_out20_dot[((size_t)dir * n_modes * n_out + oo) * W + i] = qnan;
+            if (dir == 0 && y_out20) y_out20[oo * W + i] = qnan;
         }
     }
     tm.sync();
@@ -406,6 +421,50 @@ int validate_cosmo(const DiscoebCosmo* c)
     if (c->lmaxg < 3 || c->lmaxgp < 3 || c->lmaxr < 3 || c->lmaxnu < 3) return DISCOEB_EINVAL;
     if (c->use_tca) return DISCOEB_EUNSUPPORTED;
     return DISCOEB_SUCCESS;
+}
+
+template <bool Full>
+int32_t launch_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                   const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev, int32_t n_dir,
+                   const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
+                   const double* y0, const double* y0_dot, const double* switch_tau, int32_t n_out,
+                   const double* tau_out, const double* tau_out_dot, double* y_out, double* y_out_dot,
+                   int32_t* status, int32_t* nsteps, void* stream)
+{
+    int rc = validate_cosmo(cosmo0_host);
+    if (rc) return rc;
+    if (!cosmos_dev || !ctrl || !tangents_dev || n_cosmo < 1 || n_dir < 1 || n_modes < 0 || n_out < 1)
+        return DISCOEB_EINVAL;
+    if (n_modes == 0) return DISCOEB_SUCCESS;
+    if (!kmodes || !tau_start || !y0 || !y0_dot || !switch_tau || !tau_out || !tau_out_dot || !y_out_dot ||
+        !status || !nsteps)
+        return DISCOEB_EINVAL;
+    if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED) return DISCOEB_EUNSUPPORTED;
+    if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
+    const Dims D = make_dims(*cosmo0_host);
+    const int mem = mode_mem_doubles(D), tmem = tan_mem_doubles(D);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
+    int max_optin = 0;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    // directions per block: as many as fit (at most kMaxDirsPerBlock), the forward is shared
+    auto block_bytes = [&](int d) {
+        return (size_t)(kCosmoDoubles + d * kTanDoubles + 3 * mem + 8 + d * (tmem + 3 * D.n)) * sizeof(double) +
+               8 * sizeof(int);
+    };
+    int dpb = n_dir < kMaxDirsPerBlock ? n_dir : kMaxDirsPerBlock;
+    while (dpb > 1 && block_bytes(dpb) > (size_t)max_optin) --dpb;
+    if (block_bytes(dpb) > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
+    const size_t smem = block_bytes(dpb);
+    if (cudaFuncSetAttribute(jvp_block_kernel<Full>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return DISCOEB_ECUDA;
+    const long long blocks = (long long)n_modes * ((n_dir + dpb - 1) / dpb);
+    if (blocks > 0x7fffffffLL) return DISCOEB_EINVAL;
+    jvp_block_kernel<Full><<<(unsigned)blocks, 32 * (1 + dpb), smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        cosmos_dev, n_cosmo, mode_cosmo, tangents_dev, n_dir, dpb, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot,
+        switch_tau, n_out, tau_out, tau_out_dot, mem, tmem, y_out, y_out_dot, status, nsteps);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 
 }  // namespace
@@ -466,39 +525,21 @@ int32_t discoeb_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
                     int32_t n_out, const double* tau_out, const double* tau_out_dot, double* y_out20,
                     double* y_out20_dot, int32_t* status, int32_t* nsteps, void* stream)
 {
-    int rc = validate_cosmo(cosmo0_host);
-    if (rc) return rc;
-    if (!cosmos_dev || !ctrl || !tangents_dev || n_cosmo < 1 || n_dir < 1 || n_modes < 0 || n_out < 1)
-        return DISCOEB_EINVAL;
-    if (n_modes == 0) return DISCOEB_SUCCESS;
-    if (!kmodes || !tau_start || !y0 || !y0_dot || !switch_tau || !tau_out || !tau_out_dot || !y_out20_dot ||
-        !status || !nsteps)
-        return DISCOEB_EINVAL;
-    if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED) return DISCOEB_EUNSUPPORTED;
-    if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
-    const Dims D = make_dims(*cosmo0_host);
-    const int mem = mode_mem_doubles(D), tmem = tan_mem_doubles(D);
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
-    int max_optin = 0;
-    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    // directions per block: as many as fit (at most kMaxDirsPerBlock), the forward is shared
-    auto block_bytes = [&](int d) {
-        return (size_t)(kCosmoDoubles + d * kTanDoubles + 3 * mem + 8 + d * (tmem + 3 * D.n)) * sizeof(double) +
-               8 * sizeof(int);
-    };
-    int dpb = n_dir < kMaxDirsPerBlock ? n_dir : kMaxDirsPerBlock;
-    while (dpb > 1 && block_bytes(dpb) > (size_t)max_optin) --dpb;
-    if (block_bytes(dpb) > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
-    const size_t smem = block_bytes(dpb);
-    if (cudaFuncSetAttribute(jvp_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return DISCOEB_ECUDA;
-    const long long blocks = (long long)n_modes * ((n_dir + dpb - 1) / dpb);
-    if (blocks > 0x7fffffffLL) return DISCOEB_EINVAL;
-    jvp_block_kernel<<<(unsigned)blocks, 32 * (1 + dpb), smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-        cosmos_dev, n_cosmo, mode_cosmo, tangents_dev, n_dir, dpb, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot,
-        switch_tau, n_out, tau_out, tau_out_dot, mem, tmem, y_out20, y_out20_dot, status, nsteps);
-    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+    return launch_jvp<false>(cosmos_dev, cosmo0_host, n_cosmo, mode_cosmo, tangents_dev, n_dir, ctrl, n_modes, kmodes,
+                             tau_start, y0, y0_dot, switch_tau, n_out, tau_out, tau_out_dot, y_out20, y_out20_dot,
+                             status, nsteps, stream);
+}
+
+int32_t discoeb_jvp_full(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                         const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev, int32_t n_dir,
+                         const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
+                         const double* y0, const double* y0_dot, const double* switch_tau, int32_t n_out,
+                         const double* tau_out, const double* tau_out_dot, double* y_full, double* y_full_dot,
+                         int32_t* status, int32_t* nsteps, void* stream)
+{
+    return launch_jvp<true>(cosmos_dev, cosmo0_host, n_cosmo, mode_cosmo, tangents_dev, n_dir, ctrl, n_modes, kmodes,
+                            tau_start, y0, y0_dot, switch_tau, n_out, tau_out, tau_out_dot, y_full, y_full_dot,
+                            status, nsteps, stream);
 }
 
 int32_t discoeb_rhs(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_points,

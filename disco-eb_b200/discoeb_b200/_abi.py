@@ -166,6 +166,8 @@ def lib():
                                   ctypes.POINTER(DiscoebControl), ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32,
                                   vp, vp, vp, vp, vp, vp, vp]
         L.discoeb_jvp.restype = ctypes.c_int32
+        L.discoeb_jvp_full.argtypes = L.discoeb_jvp.argtypes
+        L.discoeb_jvp_full.restype = ctypes.c_int32
         L.discoeb_rhs.restype = ctypes.c_int32
         L.discoeb_sources.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, vp, ctypes.c_int32, vp, vp, vp,
                                       vp, vp, vp]

@@ -205,3 +205,77 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
         return out, param, {"kmodes": kmodes, "aexp_out": aexp_out, "tau": tau, "y": y, "sources": src,
                             "theta": theta, "kmodes_los": kk}
     return out, param
+
+
+def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0, n_k_dense=8192, n_fftlog=16384,
+                          lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3, num_thermo=1024, rtol=1e-4, atol=1e-4,
+                          max_steps=2048, k_sampling_method="camb", aexp_out=None, de_guard_eps=1e-9, device=None,
+                          rel_step=1e-4):
+    """C_l^TT and dC_l/dtheta for theta = (omega_c, omega_b, h, n_s, ln10As, w0, wa, m_nu)
+    (``gradients.THETA_NAMES``), what ``jax.jacfwd`` of the reference's
+    compute_Cell_spectrum_from_cosmo_params (cmb.py:931-1090) gives.
+
+    The background and its six parameter tangents come from discoeb_background (forward mode,
+    Recfast steps held), the perturbation states at every output time and their tangents from one
+    discoeb_jvp_full launch (forward mode, accepted steps held).  The stages after the solve
+    (sources, line of sight, C_l) involve no adaptive choice: along each direction their
+    derivative is the fourth-order central difference of the same device stages with every input
+    (states, output times, background tables and scalars) moved by -2h, -h, h, 2h times its exact
+    tangent, h = ``rel_step`` max(|theta_d|, 0.01): the error is O(h^4) of a smooth function plus
+    their rounding (a few 1e-12 of C_l at low l, where the FFTLog sum cancels) over h.  n_s enters
+    through the primordial weight of C_l alone (a fourth-order difference of compute_Cell); C_l
+    does not depend on A_s (D_l carries it).  The k
+    sampling, start times and approximation switch times are held at the base point (the camb
+    sampling's dependence on tau_maxvis is not differentiated).
+
+    Returns ``(Cell [ellmax+1], J [8, ellmax+1], param)`` (numpy; param as
+    compute_Cell_spectrum_from_cosmo_params returns it).
+    """
+    from .background import _DIFF_FIELDS, background_from_buffer, native_background
+    from .gradients import ODE_DIRECTIONS, THETA_NAMES, JacobianProblem, param_dots, theta_to_params
+    torch, device = _device(device)
+    L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
+    aexp_out = cmb_aexp_out() if aexp_out is None else np.asarray(aexp_out, dtype=np.float64)
+    p = theta_to_params(theta)
+    pdots = param_dots(theta, ODE_DIRECTIONS)
+    buf, bdots = native_background(p, num_thermo, pdots)
+    bg = background_from_buffer(p, buf, num_thermo)
+    kmodes = k_sampling(bg, kmin, kmax, nmodes, k_sampling_method)
+    prob = JacobianProblem(theta, aexp_out=aexp_out, kmodes=kmodes, rtol=rtol, atol=atol, max_steps=max_steps,
+                           num_thermo=num_thermo, de_guard_eps=de_guard_eps, device=device, full_state=True,
+                           buffers=(buf, bdots), **L)
+    prob.launch()
+    y, ydot = prob.states()
+
+    def spectrum(param, states, n_s):
+        src = compute_sources(param=param, yout=states, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
+                              device=device, **L)
+        tau = param["tau_of_a_spline"].evaluate(aexp_out)
+        tau0 = float(param["tau_of_a_spline"].evaluate(1.0))
+        th, kk = compute_theta_ell(ellmax, kmodes, tau, src["S"], tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                   device=device)
+        return th, kk, compute_Cell(th, kk, n_s, param["k_p"], device=device).cpu().numpy()
+
+    th, kk, cell = spectrum(bg, y, bg["n_s"])
+    J = np.zeros((len(THETA_NAMES), ellmax + 1))
+    stencil = ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0))
+    for di, name in enumerate(ODE_DIRECTIONS):
+        h = rel_step * max(abs(float(theta[name])), 1e-2)
+        acc = np.zeros(ellmax + 1)
+        for m, wgt in stencil:
+            ps = dict(p)
+            for f in _DIFF_FIELDS:
+                ps[f] = p[f] + m * h * pdots[di][f]
+            bgs = background_from_buffer(ps, buf + m * h * bdots[di], num_thermo)
+            acc += wgt * spectrum(bgs, y + (m * h) * ydot[di], bg["n_s"])[2]
+        J[THETA_NAMES.index(name)] = acc / h
+    h = rel_step * max(abs(float(bg["n_s"])), 1e-2)
+    acc = np.zeros(ellmax + 1)
+    for m, wgt in stencil:
+        acc += wgt * compute_Cell(th, kk, bg["n_s"] + m * h, bg["k_p"], device=device).cpu().numpy()
+    J[THETA_NAMES.index("n_s")] = acc / h
+    param = dict(bg)
+    for key, v in (("lmaxg", lmaxg), ("lmaxgp", lmaxgp), ("lmaxr", lmaxr), ("lmaxnu", lmaxnu), ("nqmax", nqmax),
+                   ("nout", aexp_out.shape[0]), ("tau_out", bg["tau_of_a_spline"].evaluate(aexp_out))):
+        param[key] = v
+    return cell, J, param

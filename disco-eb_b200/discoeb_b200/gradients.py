@@ -220,15 +220,16 @@ class JacobianProblem:
     The host prologue (background, its tangents, start times, initial states and their
     tangents) runs in the constructor and leaves the inputs resident on the device;
     ``launch`` enqueues the kernel on the current stream and ``result`` reads it back.
-    ``host_backend`` / ``host_threads``: see cosmology_prologue (``host_processes`` is the older
-    name of ``host_threads``).
+    ``host_backend`` / ``host_threads`` / ``buffers``: see cosmology_prologue (``host_processes``
+    is the older name of ``host_threads``).  ``full_state``: launch discoeb_jvp_full, whose
+    states and state tangents ``states`` returns, instead of the P(k) fields.
     """
 
     def __init__(self, theta, *, aexp_out=(1.0,), kmin=1e-4, kmax=1.0, num_k=64, kmodes=None, lmaxg=12, lmaxgp=12,
                  lmaxr=17, lmaxnu=17, nqmax=5, rtol=1e-5, atol=1e-8, pcoeff=0.25, icoeff=0.80, dcoeff=0.0,
                  factormax=20.0, factormin=0.3, max_steps=100000, k_sampling_method="log", idx=4, num_thermo=256,
                  de_guard_eps=1e-9, device=None, warps_per_block=0, host_backend="native", host_threads=0,
-                 host_processes=None):
+                 host_processes=None, full_state=False, buffers=None):
         import torch
         if device is None:
             if not torch.cuda.is_available():
@@ -246,7 +247,7 @@ class JacobianProblem:
         aexp_out = np.atleast_1d(np.asarray(aexp_out, dtype=np.float64))
         if host_processes is not None:
             host_threads = host_processes
-        pro = cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo, host_backend, host_threads)
+        pro = cosmology_prologue(theta, aexp_out, kmodes, L, num_thermo, host_backend, host_threads, buffers)
         bg, tau_out, tau_start, y0, sw, tans = (pro[k] for k in ("bg", "tau_out", "tau_start", "y0", "sw", "tans"))
         self.bg = bg
         K, nout = kmodes.shape[0], tau_out.shape[0]
@@ -280,15 +281,18 @@ class JacobianProblem:
         self.d_sw = torch.tensor(sw[order], **f64).contiguous()
         self.d_tout = torch.tensor(tau_out, **f64)
         self.d_toutd = torch.tensor(np.stack([d["tau_out"] for d in tans]), **f64).contiguous()
-        self.d_out = torch.empty((K, nout, 20), **f64)
-        self.d_outd = torch.empty((len(self.dirs), K, nout, 20), **f64)
+        self.full_state = bool(full_state)
+        width = self.n if self.full_state else 20
+        self.d_out = torch.empty((K, nout, width), **f64)
+        self.d_outd = torch.empty((len(self.dirs), K, nout, width), **f64)
         self.d_stat = torch.empty((2, K), dtype=torch.int32, device=device)
         self.ctrl = _abi.DiscoebControl(rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin, int(max_steps),
                                         _abi.METHOD_RODAS5_STRUCTURED, int(warps_per_block), 0)
 
     def launch(self):
         stream = self.torch.cuda.current_stream(self.device).cuda_stream
-        rc = self.lib.discoeb_jvp(self.dc.struct.data_ptr(), ctypes.byref(self.dc.host), 1, None,
+        entry = self.lib.discoeb_jvp_full if self.full_state else self.lib.discoeb_jvp
+        rc = entry(self.dc.struct.data_ptr(), ctypes.byref(self.dc.host), 1, None,
                                   self.d_tan.data_ptr(), len(self.dirs), ctypes.byref(self.ctrl), self.K,
                                   self.d_k.data_ptr(),
                                   self.d_ts.data_ptr(), self.d_y0.data_ptr(), self.d_y0d.data_ptr(),
@@ -298,8 +302,21 @@ class JacobianProblem:
         if rc != 0:
             raise RuntimeError(f"discoeb_jvp failed with code {rc}")
 
+    def states(self, on_failure="raise"):
+        """(y[K, nout, n], y_dot[6, K, nout, n]) as device tensors in the caller's k order (a
+        ``full_state`` problem): the RSA-projected states at the output times and their
+        derivatives along ODE_DIRECTIONS (output times moving with the parameters)."""
+        if not self.full_state:
+            raise ValueError("states() needs a JacobianProblem made with full_state=True")
+        stat = self.d_stat.cpu().numpy()[:, self.inv]
+        _check_status(stat[0], stat[1], self.kmodes, on_failure)
+        inv = self.torch.as_tensor(self.inv, device=self.device)
+        return self.d_out[inv], self.d_outd[:, inv]
+
     def result(self, on_failure="raise"):
         """(P[K, nout], J[8, K, nout], status[K], nsteps[K]) in the caller's k order."""
+        if self.full_state:
+            raise ValueError("a full_state problem returns its states (states()), not P(k)")
         inv, bg, kmodes, idx = self.inv, self.bg, self.kmodes, self.idx
         y = self.d_out.cpu().numpy()[inv]
         yd = self.d_outd.cpu().numpy()[:, inv]

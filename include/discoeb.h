@@ -145,6 +145,20 @@ int32_t discoeb_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
                     const double* tau_out, const double* tau_out_dot, double* y_out20, double* y_out20_dot,
                     int32_t* status, int32_t* nsteps, void* stream);
 
+/* discoeb_jvp with whole states out instead of the 20 output fields: the RSA-projected state at
+ * every output time and its derivative along each direction (the inputs of the CMB source
+ * functions, whose gradients jax.jacfwd through the reference's
+ * compute_Cell_spectrum_from_cosmo_params, cmb.py:931-1090, pushes through the solve):
+ *   y_full [n_modes, n_out, nvar]             states (may be NULL)
+ *   y_full_dot [n_dir, n_modes, n_out, nvar]  d(state at the moving output time)/d(theta_d)
+ * Other arguments, launch and status codes as discoeb_jvp. */
+int32_t discoeb_jvp_full(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                         const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev, int32_t n_dir,
+                         const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
+                         const double* y0, const double* y0_dot, const double* switch_tau, int32_t n_out,
+                         const double* tau_out, const double* tau_out_dot, double* y_full, double* y_full_dot,
+                         int32_t* status, int32_t* nsteps, void* stream);
+
 /* RHS f(tau_i, y_i; k_i) of n_points states (compute_time_derivatives):
  *   y, f [n_points, nvar]; tau, kmodes [n_points]; regime < 0: approximation switches
  *   evaluated from (tau, a) as the reference does, else bitmask 1=RSA 2=UFA 4=TCA. */

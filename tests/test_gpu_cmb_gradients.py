@@ -1,0 +1,113 @@
+"""dC_l/dtheta (cmb.compute_Cell_jacobian: discoeb_jvp_full plus directional differences of the
+deterministic stages after the solve) against the forward chain and against central finite
+differences of the whole chain (GPU)."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+THETA = dict(omega_c=0.120, omega_b=0.0224, h=0.674, n_s=0.965, ln10As=math.log(21.0), w0=-0.95, wa=0.05, m_nu=0.06)
+# a reduced chain: 32 camb-sampled modes, l <= 600, 1024 dense modes, 4096 FFTLog points
+SMALL = dict(ellmax=600, nmodes=32, n_k_dense=1024, n_fftlog=4096)
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.fail("no CUDA device: the -m gpu tests need a GPU")
+    return torch
+
+
+def _chain(bg, kmodes, solver, fixed):
+    """C_l of the forward chain (full solve, sources, line of sight, C_l) on the background dict
+    ``bg`` at fixed k sampling, start times and switch times."""
+    from discoeb_b200 import cmb
+    from discoeb_b200.perturbations import solve_modes
+    a = cmb.cmb_aexp_out()
+    tau = bg["tau_of_a_spline"].evaluate(a)
+    L = dict(lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3)
+    y = solve_modes(param=bg, kmodes=kmodes, tau_out=tau, pcoeff=0.25, icoeff=0.8, dcoeff=0.0, factormax=20.0,
+                    factormin=0.3, return_full=True, as_tensor=True, **fixed, **solver, **L)
+    src = cmb.compute_sources(param=bg, yout=y, kmodes=kmodes, aexp_out=a, **L)
+    th, kk = cmb.compute_theta_ell(SMALL["ellmax"], kmodes, tau, src["S"], float(bg["tau_of_a_spline"].evaluate(1.0)),
+                                   n_fftlog=SMALL["n_fftlog"], n_k_dense=SMALL["n_k_dense"])
+    return cmb.compute_Cell(th, kk, bg["n_s"], bg["k_p"]).cpu().numpy()
+
+
+def test_gpu_cell_jacobian_matches_central_differences(torch_cuda):
+    """dC_l/dtheta against fourth-order central differences (step 1e-4 of each parameter) of the
+    forward chain at solver rtol 1e-9, on backgrounds moved along the exact background tangent.
+
+    Fourth order because the discrete C_l has a fast ripple in the parameters: the FFTLog grid in
+    ln(tau0 - tau) moves with tau0, and the line of sight's discretisation error is periodic in
+    the grid's offset (one cell, 2.4e-3 in ln chi at 4096 points, is a ~2e-3 relative change of
+    omega_c); the exact derivative of the discrete chain contains the ripple's slope, which a
+    second-order quotient of step 1e-4 misses by ~4e-4.
+
+    The background enters as its forward-mode tangent (discoeb_background, checked against the
+    complex-step derivative of the numpy restatement in the CPU tests): a difference quotient of
+    Recfast itself carries the rounding of the reference's cancelling Saha x_H formula (x_e moves
+    by up to ~1e-6 of its scale between two evaluations an ulp apart, ~1e-2 in a quotient of
+    step 1e-4 in the He recombination era), which C_l, unlike P(k), feels.  The start and switch
+    times are held, as forward-mode AD through the reference holds them; everything else, the
+    solve included, is differenced."""
+    from discoeb_b200.background import _DIFF_FIELDS, background_from_buffer, native_background
+    from discoeb_b200.cmb import compute_Cell_jacobian
+    from discoeb_b200.gradients import ODE_DIRECTIONS, THETA_NAMES, param_dots, theta_to_params
+    from discoeb_b200.perturbations import approximation_switch_times, determine_starting_time, k_sampling
+    from discoeb_b200 import cmb
+    solver = dict(rtol=1e-9, atol=1e-12, max_steps=400000)
+    C, J, param = compute_Cell_jacobian(THETA, **SMALL, **solver)
+    assert C.shape == (SMALL["ellmax"] + 1,) and J.shape == (8, SMALL["ellmax"] + 1)
+    assert np.isfinite(J).all()
+    assert np.all(J[THETA_NAMES.index("ln10As")] == 0.0)
+    p = theta_to_params(THETA)
+    pd = param_dots(THETA, ODE_DIRECTIONS)
+    buf, bd = native_background(p, 1024, pd)
+    bg = background_from_buffer(p, buf, 1024)
+    kmodes = k_sampling(bg, 1e-4, 1.0, SMALL["nmodes"], "camb")
+    tau_out = bg["tau_of_a_spline"].evaluate(cmb.cmb_aexp_out())
+    fixed = dict(tau_start=0.99 * np.minimum(tau_out.min(), determine_starting_time(param=bg, k=kmodes)),
+                 switch_tau=approximation_switch_times(bg, kmodes))
+    l = slice(2, None)
+    # the same chain at the same background: the jvp and forward kernels differ in compiled rounding
+    np.testing.assert_allclose(C[l], _chain(bg, kmodes, solver, fixed)[l], rtol=1e-7)
+    worst = {}
+    for i, name in enumerate(THETA_NAMES):
+        if name == "ln10As":
+            continue
+        eps = 1e-4 * abs(THETA[name])
+        fd = 0.0
+        for sgn, wgt in ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0)):
+            if name == "n_s":
+                b = dict(bg)
+                b["n_s"] = bg["n_s"] + sgn * eps
+            else:
+                di = ODE_DIRECTIONS.index(name)
+                ps = dict(p)
+                for f in _DIFF_FIELDS:
+                    ps[f] = p[f] + sgn * eps * pd[di][f]
+                b = background_from_buffer(ps, buf + sgn * eps * bd[di], 1024)
+            fd = fd + wgt * _chain(b, kmodes, solver, fixed) / eps
+        # dC_l/dtheta oscillates in l and crosses zero: deviations against the direction's largest
+        worst[name] = float(np.abs(J[i][l] - fd[l]).max() / np.abs(fd[l]).max())
+    print("max |J - fd| / max |fd| per direction:", worst)
+    assert max(worst.values()) < 2e-5, worst
+
+
+def test_gpu_cell_jacobian_does_not_depend_on_the_difference_step(torch_cuda):
+    """The stages after the solve are smooth along the exact tangent: their fourth-order
+    differences with steps 1e-4 and 3e-4 (relative) agree far below the solver tolerance (a
+    source point whose approximation regime, evaluated from its own time and scale factor as in
+    the reference's compute_time_derivatives, changes inside the wider stencil leaves ~1e-6)."""
+    from discoeb_b200.cmb import compute_Cell_jacobian
+    C1, J1, _ = compute_Cell_jacobian(THETA, rel_step=1e-4, **SMALL)
+    C2, J2, _ = compute_Cell_jacobian(THETA, rel_step=3e-4, **SMALL)
+    np.testing.assert_array_equal(C1, C2)
+    l = slice(2, None)
+    dev = [float(np.abs(J1[i][l] - J2[i][l]).max() / max(np.abs(J1[i][l]).max(), 1e-300)) for i in range(8)]
+    print("step dependence per direction:", dev)
+    assert max(dev) <= 1e-5, dev

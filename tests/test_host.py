@@ -88,6 +88,20 @@ def test_fma_rate_entry_rejects_bad_arguments_before_any_launch():
     assert flops.value == -1.0
 
 
+def test_jvp_entries_reject_missing_outputs_before_any_launch():
+    lib = _abi.lib()
+    host = _abi.DiscoebCosmo()
+    host.lmaxg, host.lmaxgp, host.lmaxr, host.lmaxnu, host.nqmax = 11, 11, 11, 8, 3
+    ctrl = _abi.DiscoebControl(1e-4, 1e-4, 0.25, 0.8, 0.0, 20.0, 0.3, 2048, _abi.METHOD_RODAS5_STRUCTURED, 0, 0)
+    fake = 4096  # never dereferenced: the argument checks return first
+    for entry in (lib.discoeb_jvp, lib.discoeb_jvp_full):
+        args = [fake, ctypes.byref(host), 1, None, fake, 6, ctypes.byref(ctrl), 8, fake, fake, fake, fake, fake, 4,
+                fake, fake, fake, None, fake, fake, None]
+        assert entry(*args) == -1  # no derivative output
+        args[5] = 0
+        assert entry(*args) == -1  # no direction
+
+
 def test_struct_layout_matches_header():
     # the ctypes mirror must have the C layout: compile a tiny probe of offsetof/sizeof
     import tempfile
