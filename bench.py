@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -352,6 +353,69 @@ def run_cmb(args, rank, world, local):
         }), flush=True)
 
 
+def run_cmb_grad(args, rank, world, local):
+    """C_l^TT and dC_l/dtheta (8 parameters) of one cosmology through cmb.compute_Cell_jacobian:
+    background with six forward-mode tangents, one discoeb_jvp_full launch (states and their
+    tangents at every output time), then the sources, line of sight and C_l at the base point and
+    at four points along each tangent.  DISCO-Notebook cosmology; the reference's
+    compute_Cell_spectrum_from_cosmo_params defaults, or with ``--cmb-large`` photon and
+    polarisation l_max 50, 2000 modes over [5e-5, 0.5] and 2000 source times.  Wall-clock per
+    call (host and device, results back on the host), next to the forward chain's."""
+    import torch
+
+    from discoeb_b200 import cmb
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    h = 0.67742
+    theta = {"omega_c": (0.3099 - 0.0488911) * h * h, "omega_b": 0.0488911 * h * h, "h": h, "n_s": 0.96822,
+             "ln10As": math.log(2.1064e-9 * 1e10), "w0": -0.99, "wa": 0.0, "m_nu": 0.06}
+    if args.cmb_large:
+        opts = dict(nmodes=2000, kmin=5e-5, kmax=0.5, lmaxg=50, lmaxgp=50, lmaxr=17, lmaxnu=17, nqmax=5,
+                    aexp_out=cmb.cmb_aexp_out(200, 400, 800, 600))
+        name = "cmb_tt_grad_disco_notebook_lmax50_k2000_tau2000_l2500"
+    else:
+        opts = {}
+        name = "cmb_tt_grad_disco_notebook_k128_l2500"
+    from discoeb_b200.gradients import theta_to_params
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, out
+
+    fwd = lambda: cmb.compute_Cell_spectrum_from_cosmo_params(theta_to_params(theta), device=device, **opts)  # noqa
+    grad = lambda: cmb.compute_Cell_jacobian(theta, device=device, **opts)  # noqa
+    for _ in range(args.warmup):
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            fwd()
+            grad()
+    tf, tg = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore")
+                tf.append(timed(fwd)[0])
+                dt, (C, J, _) = timed(grad)
+                tg.append(dt)
+    if rank == 0:
+        ms = 1e3 * statistics.mean(tg)
+        print(json.dumps({
+            "metric": "C_l^TT and dC_l/dtheta (8 parameters) of one cosmology", "value": 1e3 / ms,
+            "unit": "spectra+gradients/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "dtype": "f64", "data": "synthetic (DISCO-Notebook cosmology)",
+            "config": {"workload": name, "gradient_of": "C_l w.r.t. omega_c, omega_b, h, n_s, ln10As, w0, wa, m_nu",
+                       **{k: (v if not isinstance(v, np.ndarray) else int(v.shape[0])) for k, v in opts.items()}},
+            "e2e": {"value": 1e3 / ms, "unit": "spectra+gradients/s", "ms_per_cosmology": ms},
+            "forward_only_ms": 1e3 * statistics.mean(tf),
+            "finite": bool(np.isfinite(C).all() and np.isfinite(J).all()),
+            "clocks": clk.summary(),
+        }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -359,7 +423,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pk_lcdm_mnu_k512_z4")
-    ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward", "cmb", "batch"])
+    ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward", "cmb", "cmb-grad", "batch"])
+    ap.add_argument("--cmb-large", action="store_true", help="cmb-grad: l_max 50, 2000 modes, 2000 source times")
     ap.add_argument("--n-cosmo", type=int, default=64, help="cosmologies per launch in --mode batch")
     ap.add_argument("--grad", action="store_true", help="--mode batch: forward + gradient (discoeb_jvp)")
     ap.add_argument("--host-backend", default="native", choices=["native", "device"],
@@ -379,6 +444,9 @@ def main():
         return
     if args.mode == "cmb":
         run_cmb(args, rank, world, local)
+        return
+    if args.mode == "cmb-grad":
+        run_cmb_grad(args, rank, world, local)
         return
     if args.mode == "batch":
         run_batch(args, rank, world, local)

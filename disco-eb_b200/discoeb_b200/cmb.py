@@ -245,7 +245,7 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
                            num_thermo=num_thermo, de_guard_eps=de_guard_eps, device=device, full_state=True,
                            buffers=(buf, bdots), **L)
     prob.launch()
-    y, ydot = prob.states()
+    y = prob.state()
 
     def spectrum(param, states, n_s):
         src = compute_sources(param=param, yout=states, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
@@ -261,13 +261,15 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     stencil = ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0))
     for di, name in enumerate(ODE_DIRECTIONS):
         h = rel_step * max(abs(float(theta[name])), 1e-2)
+        ydot = prob.state_tangent(di)
         acc = np.zeros(ellmax + 1)
         for m, wgt in stencil:
             ps = dict(p)
             for f in _DIFF_FIELDS:
                 ps[f] = p[f] + m * h * pdots[di][f]
             bgs = background_from_buffer(ps, buf + m * h * bdots[di], num_thermo)
-            acc += wgt * spectrum(bgs, y + (m * h) * ydot[di], bg["n_s"])[2]
+            acc += wgt * spectrum(bgs, torch.add(y, ydot, alpha=m * h), bg["n_s"])[2]
+        del ydot
         J[THETA_NAMES.index(name)] = acc / h
     h = rel_step * max(abs(float(bg["n_s"])), 1e-2)
     acc = np.zeros(ellmax + 1)

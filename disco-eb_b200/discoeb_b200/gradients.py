@@ -18,7 +18,8 @@ Here the same forward-mode derivative is assembled from two exact pieces:
 
 The start times of the modes (a numerical choice) and the approximation switch times are held
 fixed.  n_s and A_s enter P(k) only through the primordial spectrum and are differentiated
-analytically.
+analytically.  A ``full_state`` JacobianProblem (``discoeb_jvp_full``) gives the whole states and
+their tangents at every output time instead, the input of ``cmb.compute_Cell_jacobian``.
 """
 from __future__ import annotations
 
@@ -302,16 +303,27 @@ class JacobianProblem:
         if rc != 0:
             raise RuntimeError(f"discoeb_jvp failed with code {rc}")
 
-    def states(self, on_failure="raise"):
-        """(y[K, nout, n], y_dot[6, K, nout, n]) as device tensors in the caller's k order (a
-        ``full_state`` problem): the RSA-projected states at the output times and their
-        derivatives along ODE_DIRECTIONS (output times moving with the parameters)."""
+    def state(self, on_failure="raise"):
+        """y[K, nout, n]: the RSA-projected states at the output times, a device tensor in the
+        caller's k order (a ``full_state`` problem)."""
         if not self.full_state:
-            raise ValueError("states() needs a JacobianProblem made with full_state=True")
+            raise ValueError("state() needs a JacobianProblem made with full_state=True")
         stat = self.d_stat.cpu().numpy()[:, self.inv]
         _check_status(stat[0], stat[1], self.kmodes, on_failure)
-        inv = self.torch.as_tensor(self.inv, device=self.device)
-        return self.d_out[inv], self.d_outd[:, inv]
+        return self.d_out[self.torch.as_tensor(self.inv, device=self.device)]
+
+    def state_tangent(self, direction):
+        """d y / d theta_d [K, nout, n] along ODE_DIRECTIONS[direction] (output times moving
+        with the parameters), a device tensor in the caller's k order; one direction at a time,
+        so that a caller of large problems holds one reordered copy."""
+        if not self.full_state:
+            raise ValueError("state_tangent() needs a JacobianProblem made with full_state=True")
+        return self.d_outd[direction][self.torch.as_tensor(self.inv, device=self.device)]
+
+    def states(self, on_failure="raise"):
+        """(y[K, nout, n], y_dot[6, K, nout, n]): state() and every state_tangent()."""
+        y = self.state(on_failure)
+        return y, self.torch.stack([self.state_tangent(d) for d in range(len(self.dirs))])
 
     def result(self, on_failure="raise"):
         """(P[K, nout], J[8, K, nout], status[K], nsteps[K]) in the caller's k order."""
