@@ -218,11 +218,14 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     The background and its six parameter tangents come from discoeb_background (forward mode,
     Recfast steps held), the perturbation states at every output time and their tangents from one
     discoeb_jvp_full launch (forward mode, accepted steps held).  The stages after the solve
-    (sources, line of sight, C_l) involve no adaptive choice: along each direction their
-    derivative is the fourth-order central difference of the same device stages with every input
-    (states, output times, background tables and scalars) moved by -2h, -h, h, 2h times its exact
-    tangent, h = ``rel_step`` max(|theta_d|, 0.01): the error is O(h^4) of a smooth function plus
-    their rounding (a few 1e-12 of C_l at low l, where the FFTLog sum cancels) over h.  n_s enters
+    (sources, line of sight, C_l) involve no adaptive choice, so along each direction they are
+    differenced along the exact tangents of their inputs, h = ``rel_step`` max(|theta_d|, 0.01):
+    the sources by a central difference with states, output times, background tables and scalars
+    moved by +-h times their tangents (the sources are smooth in them: O(h^2)), then the line of
+    sight and C_l by a fourth-order central difference along the first-order path (sources, output
+    times and tau0 moved by -2h..2h times their tangents; fourth order because the discrete C_l
+    ripples as the FFTLog grid moves with tau0): O(h^4) plus rounding (a few 1e-12 of C_l at low
+    l, where the FFTLog sum cancels) over h.  n_s enters
     through the primordial weight of C_l alone (a fourth-order difference of compute_Cell); C_l
     does not depend on A_s (D_l carries it).  The k
     sampling, start times and approximation switch times are held at the base point (the camb
@@ -247,29 +250,46 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     prob.launch()
     y = prob.state()
 
-    def spectrum(param, states, n_s):
-        src = compute_sources(param=param, yout=states, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
-                              device=device, **L)
-        tau = param["tau_of_a_spline"].evaluate(aexp_out)
-        tau0 = float(param["tau_of_a_spline"].evaluate(1.0))
-        th, kk = compute_theta_ell(ellmax, kmodes, tau, src["S"], tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
-                                   device=device)
-        return th, kk, compute_Cell(th, kk, n_s, param["k_p"], device=device).cpu().numpy()
+    def sources(param, states):
+        return compute_sources(param=param, yout=states, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
+                               device=device, **L)["S"]
 
-    th, kk, cell = spectrum(bg, y, bg["n_s"])
+    def times(param):
+        return param["tau_of_a_spline"].evaluate(aexp_out), float(param["tau_of_a_spline"].evaluate(1.0))
+
+    def los_cell(S, tau, tau0):
+        th, kk = compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                   device=device)
+        return th, kk, compute_Cell(th, kk, bg["n_s"], bg["k_p"], device=device).cpu().numpy()
+
+    S0 = sources(bg, y)
+    tau_b, tau0_b = times(bg)
+    th, kk, cell = los_cell(S0, tau_b, tau0_b)
     J = np.zeros((len(THETA_NAMES), ellmax + 1))
     stencil = ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0))
     for di, name in enumerate(ODE_DIRECTIONS):
         h = rel_step * max(abs(float(theta[name])), 1e-2)
         ydot = prob.state_tangent(di)
-        acc = np.zeros(ellmax + 1)
-        for m, wgt in stencil:
+        # the tangents of the line of sight's inputs: sources by a central difference (smooth in
+        # their inputs), output times and tau0 exactly (linear in the background tables)
+        side = []
+        for sgn in (1.0, -1.0):
             ps = dict(p)
             for f in _DIFF_FIELDS:
-                ps[f] = p[f] + m * h * pdots[di][f]
-            bgs = background_from_buffer(ps, buf + m * h * bdots[di], num_thermo)
-            acc += wgt * spectrum(bgs, torch.add(y, ydot, alpha=m * h), bg["n_s"])[2]
+                ps[f] = p[f] + sgn * h * pdots[di][f]
+            bgs = background_from_buffer(ps, buf + sgn * h * bdots[di], num_thermo)
+            side.append((sources(bgs, torch.add(y, ydot, alpha=sgn * h)), *times(bgs)))
         del ydot
+        S_dot = (side[0][0] - side[1][0]) / (2 * h)
+        tau_dot = (side[0][1] - side[1][1]) / (2 * h)
+        tau0_dot = (side[0][2] - side[1][2]) / (2 * h)
+        del side
+        # the line of sight and C_l along that first-order path (the derivative at the base point
+        # depends on the path's slope only): fourth order, the discrete C_l ripples in tau0
+        acc = np.zeros(ellmax + 1)
+        for m, wgt in stencil:
+            acc += wgt * los_cell(torch.add(S0, S_dot, alpha=m * h), tau_b + m * h * tau_dot,
+                                  tau0_b + m * h * tau0_dot)[2]
         J[THETA_NAMES.index(name)] = acc / h
     h = rel_step * max(abs(float(bg["n_s"])), 1e-2)
     acc = np.zeros(ellmax + 1)
