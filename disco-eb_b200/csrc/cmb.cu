@@ -359,23 +359,8 @@ __global__ void mcoef_kernel(int n_ell, int n_freq, int n_fft, const double* __r
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)n_ell * n_freq) return;
-    const double dl = g[1];
     const int l = (int)(t / n_freq), q = (int)(t - (long long)l * n_freq);
-    const double eta = 2.0 * M_PI * q / (n_fft * dl);
-    const Cx p = cx(kBias, eta);
-    const Cx a1 = cx((1.0 + l + p.re) / 2.0, p.im / 2.0), a2 = cx((2.0 + l - p.re) / 2.0, -p.im / 2.0);
-    const Cx lc = cx((p.re - 1.0) * M_LN2 + 0.5 * log(M_PI), p.im * M_LN2) + lngamma_c(a1) - lngamma_c(a2);
-    double* b = B + (size_t)l * (2 * (size_t)n_freq) + 2 * q;
-    if (lc.re == -INFINITY) {
-        b[0] = 0.0;
-        b[1] = 0.0;
-        return;
-    }
-    const double mag = exp(lc.re);
-    double sn, cs;
-    sincos(lc.im, &sn, &cs);
-    b[0] = mag * cs;
-    b[1] = -mag * sn;
+    fftlog_mcoef(l, q, n_fft, kBias, g[1], 0.0, B + (size_t)l * (2 * (size_t)n_freq) + 2 * q, nullptr);
 }
 
 // C_l = trapezoid over ln k of (k/k_p)^(n_s-1) Theta_l(k)^2, written as sum_i w_i Theta_il^2 with
@@ -383,6 +368,15 @@ __global__ void mcoef_kernel(int n_ell, int n_freq, int n_fft, const double* __r
 // consecutive l (one coalesced 256-byte row segment per mode) and its 8 warps stride over the
 // modes; the weights of a chunk of modes are computed once per block into shared memory.
 constexpr int kCellChunk = 1024;
+
+// trapezoid weight in ln k of mode i times the primordial factor (k_i/k_p)^(n_s-1)
+__device__ inline double cell_weight(int i, int n_modes, const double* __restrict__ kmodes, double n_s, double k_p)
+{
+    const double lk = log(kmodes[i]);
+    const double lo = i > 0 ? log(kmodes[i - 1]) : lk;
+    const double hi = i + 1 < n_modes ? log(kmodes[i + 1]) : lk;
+    return pow(kmodes[i] / k_p, n_s - 1.0) * (0.5 * (hi - lo));
+}
 
 __global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __restrict__ kmodes, int n_ell,
                                                    const double* __restrict__ theta, double n_s, double k_p,
@@ -396,13 +390,7 @@ __global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __
     for (int c0 = 0; c0 < n_modes; c0 += kCellChunk) {
         const int cn = min(kCellChunk, n_modes - c0);
         __syncthreads();
-        for (int j = threadIdx.x; j < cn; j += blockDim.x) {
-            const int i = c0 + j;
-            const double lk = log(kmodes[i]);
-            const double lo = i > 0 ? log(kmodes[i - 1]) : lk;
-            const double hi = i + 1 < n_modes ? log(kmodes[i + 1]) : lk;
-            w[j] = pow(kmodes[i] / k_p, n_s - 1.0) * (0.5 * (hi - lo));
-        }
+        for (int j = threadIdx.x; j < cn; j += blockDim.x) w[j] = cell_weight(c0 + j, n_modes, kmodes, n_s, k_p);
         __syncthreads();
         if (l < n_ell) {
 #pragma unroll 4
@@ -419,6 +407,197 @@ __global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __
         for (int q = 0; q < 8; ++q) sum += part[q][lx];
         cell[l] = sum;
     }
+}
+
+// ------------------------------------------------------------------------------------------
+// tangent of C_l along one direction of the line of sight's inputs (sources S', output times
+// tau', tau0'): forward mode through the resampling, the FFT coefficients and the table M_l(p),
+// folded into C_l = sum_k w_k Theta_kl^2 with Theta = A B^T (A the coefficient rows, B the
+// table): dC_l = 2 sum_j (B_lj H_lj + B'_lj G_lj), G = Omega^T A, H = Omega^T A',
+// Omega_kl = w_k Theta_kl.  The interval indices of the resampling are those of the base point.
+
+// d(lo, dl) of geom_kernel's grid: it moves with tau0 - tau at the last and first knots
+__global__ void geom_dot_kernel(int n_tau, const double* __restrict__ tau, const double* __restrict__ tau_dot,
+                                double tau0, double tau0_dot, int n_fft, double* gd)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double cmin = tau0 - tau[n_tau - 1];
+    const double lo_dot = cmin > 1.0 ? (tau0_dot - tau_dot[n_tau - 1]) / cmin : 0.0;  // else held by fmax
+    const double hi_dot = (tau0_dot - tau_dot[0]) / (tau0 - tau[0]);
+    gd[0] = lo_dot;
+    gd[1] = (hi_dot - lo_dot) / n_fft;
+}
+
+// d ln chi of the knots (lchi_kernel)
+__global__ void lchi_dot_kernel(int n_tau, const double* __restrict__ tau, const double* __restrict__ tau_dot,
+                                double tau0, double tau0_dot, double* lchi_dot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tau) return;
+    const double c = tau0 - tau[n_tau - 1 - t];
+    lchi_dot[t] = c > 1e-10 ? (tau0_dot - tau_dot[n_tau - 1 - t]) / c : 0.0;
+}
+
+// d ln chi_m and d chi_m^-bias of the FFTLog points (fgrid_kernel: ln chi_m = lo + m dl)
+__global__ void fgrid_dot_kernel(int n_fft, const double* __restrict__ gd, const double* __restrict__ fbias,
+                                 double* fx_dot, double* fbias_dot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_fft) return;
+    const double xd = gd[0] + t * gd[1];
+    fx_dot[t] = xd;
+    fbias_dot[t] = -kBias * xd * fbias[t];
+}
+
+// spline_second in dual numbers: knots x + e x', values y + e y' (value stride ys, knot stride 1);
+// the second derivatives' values and derivatives go to S, S_dot (stride ys); cp, cp_dot scratch
+__device__ void spline_second_dual(int n, const double* x, const double* xd, const double* y, const double* yd,
+                                   long long ys, double* S, double* Sd, double* cp, double* cpd)
+{
+    S[0] = Sd[0] = 0.0;
+    S[(long long)(n - 1) * ys] = Sd[(long long)(n - 1) * ys] = 0.0;
+    const int m = n - 2;
+    if (m <= 0) return;
+    auto X = [&](int i) { return Dual(x[i], xd[i]); };
+    auto Y = [&](int i) { return Dual(y[(long long)i * ys], yd[(long long)i * ys]); };
+    Dual dprev(0.0), cprev(0.0);
+    for (int i = 0; i < m; ++i) {
+        const Dual h0 = X(i + 1) - X(i), h1 = X(i + 2) - X(i + 1);
+        const Dual a = h0, bb = 2.0 * (h0 + h1), c = h1;
+        const Dual d = 6.0 * ((Y(i + 2) - Y(i + 1)) / h1 - (Y(i + 1) - Y(i)) / h0);
+        Dual cc, dd;
+        if (i == 0) {
+            cc = c / bb;
+            dd = d / bb;
+        } else {
+            const Dual den = bb - a * cprev;
+            cc = (i < m - 1) ? c / den : Dual(0.0);
+            dd = (d - a * dprev) / den;
+        }
+        cp[i] = cc.v;
+        cpd[i] = cc.d;
+        S[(long long)(i + 1) * ys] = dd.v;
+        Sd[(long long)(i + 1) * ys] = dd.d;
+        cprev = cc;
+        dprev = dd;
+    }
+    for (int i = m - 2; i >= 0; --i) {
+        const long long a1 = (long long)(i + 1) * ys, a2 = (long long)(i + 2) * ys;
+        const Dual r = Dual(S[a1], Sd[a1]) - Dual(cp[i], cpd[i]) * Dual(S[a2], Sd[a2]);
+        S[a1] = r.v;
+        Sd[a1] = r.d;
+    }
+}
+
+__device__ Dual spline_value_dual(Dual x0, Dual x1, Dual y0, Dual y1, Dual S0, Dual S1, Dual xn)
+{
+    const Dual h = x1 - x0, t = (xn - x0) / h, A = 1.0 - t, B = t;
+    return A * y0 + B * y1 + ((A * A * A - A) * S0 + (B * B * B - B) * S1) * (h * h) / 6.0;
+}
+
+// chi_spline_kernel in dual numbers (one thread per row; rows in chi order as there)
+__global__ void chi_spline_dot_kernel(int n_rows, int n_tau, const double* __restrict__ lchi,
+                                      const double* __restrict__ lchi_dot, const double* Srow, const double* Srow_dot,
+                                      double* S2v, double* S2d, double* cpv, double* cpd)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    const size_t last = (size_t)r * n_tau + (n_tau - 1);
+    spline_second_dual(n_tau, lchi, lchi_dot, Srow + last, Srow_dot + last, -1, S2v + last, S2d + last,
+                       cpv + (size_t)r * n_tau, cpd + (size_t)r * n_tau);
+}
+
+// the derivative of chi_eval_kernel's biased source on the FFTLog grid, into F_dot (row pitch)
+__global__ void chi_eval_dot_kernel(int n_rows, int n_tau, const double* __restrict__ lchi,
+                                    const double* __restrict__ lchi_dot, const double* __restrict__ Srow,
+                                    const double* __restrict__ Srow_dot, const double* __restrict__ S2v,
+                                    const double* __restrict__ S2d, int n_fft, const int* __restrict__ fidx,
+                                    const double* __restrict__ fx, const double* __restrict__ fx_dot,
+                                    const double* __restrict__ fbias, const double* __restrict__ fbias_dot,
+                                    long long pitch, double* Fd)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_rows * n_fft) return;
+    const int r = (int)(t / n_fft), m = (int)(t - (long long)r * n_fft);
+    const int i = fidx[m];
+    const size_t base = (size_t)r * n_tau + (n_tau - 1);
+    const Dual v = spline_value_dual(Dual(lchi[i], lchi_dot[i]), Dual(lchi[i + 1], lchi_dot[i + 1]),
+                                     Dual(Srow[base - i], Srow_dot[base - i]),
+                                     Dual(Srow[base - i - 1], Srow_dot[base - i - 1]), Dual(S2v[base - i], S2d[base - i]),
+                                     Dual(S2v[base - i - 1], S2d[base - i - 1]), Dual(fx[m], fx_dot[m])) *
+                   Dual(fbias[m], fbias_dot[m]);
+    Fd[(size_t)r * pitch + m] = v.d;
+}
+
+// the derivative of ck_kernel's coefficients: c = mag e^{i ph} F with ph = -eta (lo + ln k) and
+// eta = 2 pi q / (n_fft dl), so c' = mag e^{i ph} F' + i ph' c; Fd holds F' (the FFT of the
+// derivative rows) and becomes c', C holds the base point's c
+__global__ void ck_dot_kernel(int n_rows, const double* __restrict__ krow, int n_fft, int n_freq,
+                              const double* __restrict__ g, const double* __restrict__ gd, long long pitch,
+                              const double* __restrict__ C, double* Fd)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_rows * n_freq) return;
+    const double lo = g[0], dl = g[1];
+    const int r = (int)(t / n_freq), q = (int)(t - (long long)r * n_freq);
+    const double eta = 2.0 * M_PI * q / (n_fft * dl);
+    const double eta_dot = -eta * gd[1] / dl;
+    const double lk = log(krow[r]);
+    double w = 2.0;
+    if (q == 0 || ((n_fft % 2 == 0) && q == n_freq - 1)) w = 1.0;
+    const double mag = w * exp(-(kBias + 1.0) * lk) / n_fft;
+    double sn, cs;
+    sincos(-eta * (lo + lk), &sn, &cs);
+    const double ph_dot = -(eta_dot * (lo + lk) + eta * gd[0]);
+    const size_t o = (size_t)r * pitch + 2 * q;
+    const double re = Fd[o], im = Fd[o + 1];
+    Fd[o] = mag * (re * cs - im * sn) - ph_dot * C[o + 1];
+    Fd[o + 1] = mag * (re * sn + im * cs) + ph_dot * C[o];
+}
+
+// the derivative of mcoef_kernel's table along the spacing's derivative gd[1]
+__global__ void mcoef_dot_kernel(int n_ell, int n_freq, int n_fft, const double* __restrict__ g,
+                                 const double* __restrict__ gd, double* Bd)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_ell * n_freq) return;
+    const int l = (int)(t / n_freq), q = (int)(t - (long long)l * n_freq);
+    double b[2];
+    fftlog_mcoef(l, q, n_fft, kBias, g[1], gd[1], b, Bd + (size_t)l * (2 * (size_t)n_freq) + 2 * q);
+}
+
+__global__ void cell_weight_kernel(int n_modes, const double* __restrict__ kmodes, double n_s, double k_p, double* w)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_modes) w[i] = cell_weight(i, n_modes, kmodes, n_s, k_p);
+}
+
+// Omega_kl = w_k Theta_kl in place
+__global__ void scale_rows_kernel(int n_rows, int n_cols, const double* __restrict__ w, double* M)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_rows * n_cols) return;
+    M[t] *= w[t / n_cols];
+}
+
+// dC_l = 2 sum_j (B_lj H_lj + Bd_lj G_lj): one block per l, rows of `pitch` doubles
+__global__ void __launch_bounds__(256) cell_dot_kernel(int n_ell, long long pitch, const double* __restrict__ B,
+                                                       const double* __restrict__ H, const double* __restrict__ Bd,
+                                                       const double* __restrict__ G, double* out)
+{
+    __shared__ double part[256];
+    const int l = blockIdx.x;
+    if (l >= n_ell) return;
+    const size_t o = (size_t)l * pitch;
+    double acc = 0.0;
+    for (long long j = threadIdx.x; j < pitch; j += blockDim.x) acc += B[o + j] * H[o + j] + Bd[o + j] * G[o + j];
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[l] = 2.0 * part[0];
 }
 
 // ------------------------------------------------------------------------------------------
@@ -499,6 +678,130 @@ double* noalloc_scratch(int dev)
     return g_noalloc_ptr[dev];
 }
 
+// Steps 1-5 of the line of sight (the body of discoeb_los) for validated arguments: workspace
+// `ws` (256-byte aligned) carved by los_layout, theta [rows, ellmax + 1] written by the GEMM.
+// Intermediates stay in the workspace: the dense rows, ln chi knots, FFTLog points, the
+// coefficient rows c_q k^-(p_q+1) (`fft`) and the table M_l(p_q) (`B`).
+int32_t los_forward(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S,
+                    double tau0, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, char* ws, int64_t workspace_bytes,
+                    double* theta, double* kmodes_out, void* stream)
+{
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int rows = n_k_dense > 0 ? n_k_dense : n_modes;
+    const long long pitch = 2LL * (n_fftlog / 2 + 1);
+    cufftHandle plan;
+    size_t work = 0;
+    std::unique_lock<std::mutex> fft_lock(discoeb_fft::plan_mutex());
+    if (!discoeb_fft::cached_plan(CUFFT_D2Z, n_fftlog, rows, pitch, pitch / 2, &plan, &work)) return DISCOEB_ECUDA;
+    const LosLayout L = los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work);
+    if ((uint64_t)workspace_bytes < L.total) return DISCOEB_EINVAL;
+    auto D = [&](size_t off) { return reinterpret_cast<double*>(ws + off); };
+    const int T = 256;
+    // 1. rows of S on the k grid used for the integral
+    const double* Srow = S;
+    const double* krow = kmodes;
+    log_kernel<<<blocks_for(n_modes, T), T, 0, s>>>(n_modes, kmodes, D(L.lk));
+    if (n_k_dense > 0) {
+        k_spline_log_kernel<<<blocks_for(n_tau, 64), 64, 0, s>>>(n_modes, D(L.lk), n_tau, S, D(L.s2k), D(L.cpk));
+        k_dense_kernel<<<blocks_for((long long)n_k_dense * n_tau, T), T, 0, s>>>(n_modes, D(L.lk), n_tau, S, D(L.s2k),
+                                                                                  n_k_dense, D(L.sd), D(L.kd));
+        Srow = D(L.sd);
+        krow = D(L.kd);
+    } else {
+        cudaMemcpyAsync(D(L.kd), kmodes, sizeof(double) * n_modes, cudaMemcpyDeviceToDevice, s);
+        krow = D(L.kd);
+    }
+    cudaMemcpyAsync(kmodes_out, krow, sizeof(double) * rows, cudaMemcpyDeviceToDevice, s);
+    // 2. the FFTLog grid and the biased source on it
+    geom_kernel<<<1, 32, 0, s>>>(n_tau, tau, tau0, n_fftlog, D(L.geom));
+    lchi_kernel<<<blocks_for(n_tau, T), T, 0, s>>>(n_tau, tau, tau0, D(L.lchi));
+    fgrid_kernel<<<blocks_for(n_fftlog, T), T, 0, s>>>(n_tau, D(L.lchi), n_fftlog, D(L.geom),
+                                                       reinterpret_cast<int*>(ws + L.fidx), D(L.fx), D(L.fbias));
+    chi_spline_kernel<<<blocks_for(rows, 64), 64, 0, s>>>(rows, n_tau, D(L.lchi), Srow, D(L.s2c), D(L.cpc));
+    chi_eval_kernel<<<blocks_for((long long)rows * n_fftlog, T), T, 0, s>>>(
+        rows, n_tau, D(L.lchi), Srow, D(L.s2c), n_fftlog, reinterpret_cast<const int*>(ws + L.fidx), D(L.fx),
+        D(L.fbias), L.pitch, D(L.fft));
+    // 3. rfft of every row, in place (the plan lock is held from the lookup to here, so no other
+    //    call can evict the plan or change its work area in between)
+    cufftSetWorkArea(plan, ws + L.cufft);
+    cufftSetStream(plan, s);
+    const cufftResult fr = cufftExecD2Z(plan, D(L.fft), reinterpret_cast<cufftDoubleComplex*>(D(L.fft)));
+    fft_lock.unlock();
+    if (fr != CUFFT_SUCCESS) return DISCOEB_ECUDA;
+    // 4. ck in place, and the M table
+    ck_kernel<<<blocks_for((long long)rows * L.n_freq, T), T, 0, s>>>(rows, krow, n_fftlog, L.n_freq, D(L.geom),
+                                                                      L.pitch, D(L.fft));
+    mcoef_kernel<<<blocks_for((long long)(ellmax + 1) * L.n_freq, T), T, 0, s>>>(ellmax + 1, L.n_freq, n_fftlog,
+                                                                                 D(L.geom), D(L.B));
+    if (cudaGetLastError() != cudaSuccess) return DISCOEB_ECUDA;
+    // 5. theta[r, l] = sum_j A[r, j] B[l, j] over the interleaved (re, im) pairs: one DGEMM
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
+    std::lock_guard<std::mutex> lock(g_blas_mu);
+    cublasHandle_t h = blas_handle(dev);
+    if (!h) return DISCOEB_ECUDA;
+    cublasSetStream(h, s);
+    cublasSetWorkspace(h, ws + L.cublas, kCublasWorkspace);
+    const double one = 1.0, zero = 0.0;
+    const cublasStatus_t st =
+        cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ellmax + 1, rows, (int)L.pitch, &one, D(L.B), (int)L.pitch, D(L.fft),
+                    (int)L.pitch, &zero, theta, ellmax + 1);
+    cublasSetWorkspace(h, nullptr, 0);
+    if (st != CUBLAS_STATUS_SUCCESS) return DISCOEB_ECUDA;
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+
+// workspace of discoeb_los_cell_jvp: the line of sight's own (los_layout) followed by these
+struct LosJvpLayout {
+    LosLayout base;
+    size_t th, G, H, Bd, Fd, w, kout, kscratch, sdd, s2kd, cpkd, lchid, fxd, fbd, gd, S2v, S2d, cpv, cpd, total;
+};
+
+LosJvpLayout los_jvp_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n_dense, size_t cufft_bytes)
+{
+    LosJvpLayout J;
+    J.base = los_layout(n_modes, n_tau, ellmax, n_fft, n_dense, cufft_bytes);
+    const size_t rows = (size_t)J.base.n_rows, L = (size_t)ellmax + 1, pitch = (size_t)J.base.pitch;
+    size_t o = J.base.total;
+    auto take = [&](size_t doubles) { const size_t at = o; o = align256(o + sizeof(double) * doubles); return at; };
+    J.th = take(rows * L);
+    J.G = take(L * pitch);
+    J.H = take(L * pitch);
+    J.Bd = take(L * pitch);
+    J.Fd = take(rows * pitch);
+    J.w = take(rows);
+    J.kout = take(rows);
+    J.kscratch = take(rows);
+    J.sdd = take(n_dense > 0 ? (size_t)n_dense * n_tau : 0);
+    J.s2kd = take(n_dense > 0 ? (size_t)n_modes * n_tau : 0);
+    J.cpkd = take(n_dense > 0 ? (size_t)n_modes * n_tau : 0);
+    J.lchid = take(n_tau);
+    J.fxd = take(n_fft);
+    J.fbd = take(n_fft);
+    J.gd = take(2);
+    J.S2v = take(rows * n_tau);
+    J.S2d = take(rows * n_tau);
+    J.cpv = take(rows * n_tau);
+    J.cpd = take(rows * n_tau);
+    J.total = o;
+    return J;
+}
+
+bool los_args_ok(int n_modes, int n_tau, int ellmax, int n_fftlog, int n_k_dense)
+{
+    return !(n_modes < 2 || n_tau < 3 || ellmax < 0 || n_fftlog < 2 || n_k_dense < 0 || n_k_dense == 1);
+}
+
+// cuFFT work-area size of the line of sight's batched transform (plan made and cached)
+bool los_fft_work(int n_fftlog, int rows, size_t* work)
+{
+    const long long pitch = 2LL * (n_fftlog / 2 + 1);
+    cufftHandle plan;
+    std::lock_guard<std::mutex> lock(discoeb_fft::plan_mutex());
+    return discoeb_fft::cached_plan(CUFFT_D2Z, n_fftlog, rows, pitch, pitch / 2, &plan, work);
+}
+
 }  // namespace
 
 extern "C" {
@@ -559,70 +862,8 @@ int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
         return DISCOEB_EINVAL;
     if (!kmodes || !tau || !S || !workspace || !theta || !kmodes_out) return DISCOEB_EINVAL;
     if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return DISCOEB_EINVAL;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const int rows = n_k_dense > 0 ? n_k_dense : n_modes;
-    const long long pitch = 2LL * (n_fftlog / 2 + 1);
-    cufftHandle plan;
-    size_t work = 0;
-    std::unique_lock<std::mutex> fft_lock(discoeb_fft::plan_mutex());
-    if (!discoeb_fft::cached_plan(CUFFT_D2Z, n_fftlog, rows, pitch, pitch / 2, &plan, &work)) return DISCOEB_ECUDA;
-    const LosLayout L = los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work);
-    if ((uint64_t)workspace_bytes < L.total) return DISCOEB_EINVAL;
-    char* ws = static_cast<char*>(workspace);
-    auto D = [&](size_t off) { return reinterpret_cast<double*>(ws + off); };
-    const int T = 256;
-    // 1. rows of S on the k grid used for the integral
-    const double* Srow = S;
-    const double* krow = kmodes;
-    log_kernel<<<blocks_for(n_modes, T), T, 0, s>>>(n_modes, kmodes, D(L.lk));
-    if (n_k_dense > 0) {
-        k_spline_log_kernel<<<blocks_for(n_tau, 64), 64, 0, s>>>(n_modes, D(L.lk), n_tau, S, D(L.s2k), D(L.cpk));
-        k_dense_kernel<<<blocks_for((long long)n_k_dense * n_tau, T), T, 0, s>>>(n_modes, D(L.lk), n_tau, S, D(L.s2k),
-                                                                                  n_k_dense, D(L.sd), D(L.kd));
-        Srow = D(L.sd);
-        krow = D(L.kd);
-    } else {
-        cudaMemcpyAsync(D(L.kd), kmodes, sizeof(double) * n_modes, cudaMemcpyDeviceToDevice, s);
-        krow = D(L.kd);
-    }
-    cudaMemcpyAsync(kmodes_out, krow, sizeof(double) * rows, cudaMemcpyDeviceToDevice, s);
-    // 2. the FFTLog grid and the biased source on it
-    geom_kernel<<<1, 32, 0, s>>>(n_tau, tau, tau0, n_fftlog, D(L.geom));
-    lchi_kernel<<<blocks_for(n_tau, T), T, 0, s>>>(n_tau, tau, tau0, D(L.lchi));
-    fgrid_kernel<<<blocks_for(n_fftlog, T), T, 0, s>>>(n_tau, D(L.lchi), n_fftlog, D(L.geom),
-                                                       reinterpret_cast<int*>(ws + L.fidx), D(L.fx), D(L.fbias));
-    chi_spline_kernel<<<blocks_for(rows, 64), 64, 0, s>>>(rows, n_tau, D(L.lchi), Srow, D(L.s2c), D(L.cpc));
-    chi_eval_kernel<<<blocks_for((long long)rows * n_fftlog, T), T, 0, s>>>(
-        rows, n_tau, D(L.lchi), Srow, D(L.s2c), n_fftlog, reinterpret_cast<const int*>(ws + L.fidx), D(L.fx),
-        D(L.fbias), L.pitch, D(L.fft));
-    // 3. rfft of every row, in place (the plan lock is held from the lookup to here, so no other
-    //    call can evict the plan or change its work area in between)
-    cufftSetWorkArea(plan, ws + L.cufft);
-    cufftSetStream(plan, s);
-    const cufftResult fr = cufftExecD2Z(plan, D(L.fft), reinterpret_cast<cufftDoubleComplex*>(D(L.fft)));
-    fft_lock.unlock();
-    if (fr != CUFFT_SUCCESS) return DISCOEB_ECUDA;
-    // 4. ck in place, and the M table
-    ck_kernel<<<blocks_for((long long)rows * L.n_freq, T), T, 0, s>>>(rows, krow, n_fftlog, L.n_freq, D(L.geom),
-                                                                      L.pitch, D(L.fft));
-    mcoef_kernel<<<blocks_for((long long)(ellmax + 1) * L.n_freq, T), T, 0, s>>>(ellmax + 1, L.n_freq, n_fftlog,
-                                                                                 D(L.geom), D(L.B));
-    if (cudaGetLastError() != cudaSuccess) return DISCOEB_ECUDA;
-    // 5. theta[r, l] = sum_j A[r, j] B[l, j] over the interleaved (re, im) pairs: one DGEMM
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
-    std::lock_guard<std::mutex> lock(g_blas_mu);
-    cublasHandle_t h = blas_handle(dev);
-    if (!h) return DISCOEB_ECUDA;
-    cublasSetStream(h, s);
-    cublasSetWorkspace(h, ws + L.cublas, kCublasWorkspace);
-    const double one = 1.0, zero = 0.0;
-    const cublasStatus_t st =
-        cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ellmax + 1, rows, (int)L.pitch, &one, D(L.B), (int)L.pitch, D(L.fft),
-                    (int)L.pitch, &zero, theta, ellmax + 1);
-    cublasSetWorkspace(h, nullptr, 0);
-    if (st != CUBLAS_STATUS_SUCCESS) return DISCOEB_ECUDA;
-    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+    return los_forward(n_modes, kmodes, n_tau, tau, S, tau0, ellmax, n_fftlog, n_k_dense,
+                       static_cast<char*>(workspace), workspace_bytes, theta, kmodes_out, stream);
 }
 
 int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta, double n_s, double k_p,
@@ -631,6 +872,103 @@ int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const
     if (n_modes < 2 || n_ell < 1 || !kmodes || !theta || !cell) return DISCOEB_EINVAL;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     cell_kernel<<<(n_ell + 31) / 32, 256, 0, s>>>(n_modes, kmodes, n_ell, theta, n_s, k_p, cell);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int64_t discoeb_los_cell_jvp_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
+                                             int32_t n_k_dense)
+{
+    if (!los_args_ok(n_modes, n_tau, ellmax, n_fftlog, n_k_dense)) return DISCOEB_EINVAL;
+    size_t work = 0;
+    if (!los_fft_work(n_fftlog, n_k_dense > 0 ? n_k_dense : n_modes, &work)) return DISCOEB_ECUDA;
+    return (int64_t)los_jvp_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work).total;
+}
+
+int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S,
+                             double tau0, int32_t n_dir, const double* tau_dot, const double* S_dot,
+                             const double* tau0_dot, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, double n_s,
+                             double k_p, void* workspace, int64_t workspace_bytes, double* cell, double* cell_dot,
+                             void* stream)
+{
+    if (!los_args_ok(n_modes, n_tau, ellmax, n_fftlog, n_k_dense) || n_dir < 0) return DISCOEB_EINVAL;
+    if (!kmodes || !tau || !S || !workspace || !cell) return DISCOEB_EINVAL;
+    if (n_dir > 0 && (!tau_dot || !S_dot || !tau0_dot || !cell_dot)) return DISCOEB_EINVAL;
+    if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return DISCOEB_EINVAL;
+    const int rows = n_k_dense > 0 ? n_k_dense : n_modes;
+    size_t work = 0;
+    if (!los_fft_work(n_fftlog, rows, &work)) return DISCOEB_ECUDA;
+    const LosJvpLayout J = los_jvp_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work);
+    if ((uint64_t)workspace_bytes < J.total) return DISCOEB_EINVAL;
+    const LosLayout& L = J.base;
+    char* ws = static_cast<char*>(workspace);
+    auto D = [&](size_t off) { return reinterpret_cast<double*>(ws + off); };
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int n_ell = ellmax + 1, T = 256;
+    const long long pitch = L.pitch;
+    // base point: Theta, C_l, Omega = w Theta (in place), G = Omega^T A
+    int rc = los_forward(n_modes, kmodes, n_tau, tau, S, tau0, ellmax, n_fftlog, n_k_dense, ws, (int64_t)L.total,
+                         D(J.th), D(J.kout), stream);
+    if (rc) return rc;
+    cell_kernel<<<(n_ell + 31) / 32, 256, 0, s>>>(rows, D(J.kout), n_ell, D(J.th), n_s, k_p, cell);
+    if (n_dir == 0) return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+    cell_weight_kernel<<<blocks_for(rows, T), T, 0, s>>>(rows, D(J.kout), n_s, k_p, D(J.w));
+    scale_rows_kernel<<<blocks_for((long long)rows * n_ell, T), T, 0, s>>>(rows, n_ell, D(J.w), D(J.th));
+    if (cudaGetLastError() != cudaSuccess) return DISCOEB_ECUDA;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
+    const double one = 1.0, zero = 0.0;
+    auto omega_t_times = [&](const double* A, double* out) {  // out [n_ell, pitch] = Omega^T A
+        std::lock_guard<std::mutex> lock(g_blas_mu);
+        cublasHandle_t h = blas_handle(dev);
+        if (!h) return false;
+        cublasSetStream(h, s);
+        cublasSetWorkspace(h, ws + L.cublas, kCublasWorkspace);
+        const cublasStatus_t st = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, (int)pitch, n_ell, rows, &one, A, (int)pitch,
+                                              D(J.th), n_ell, &zero, out, (int)pitch);
+        cublasSetWorkspace(h, nullptr, 0);
+        return st == CUBLAS_STATUS_SUCCESS;
+    };
+    if (!omega_t_times(D(L.fft), D(J.G))) return DISCOEB_ECUDA;
+    const double* Srow = n_k_dense > 0 ? D(L.sd) : S;
+    for (int d = 0; d < n_dir; ++d) {
+        const double* Sd_in = S_dot + (size_t)d * n_modes * n_tau;
+        const double* td = tau_dot + (size_t)d * n_tau;
+        const double* Srow_dot = Sd_in;
+        if (n_k_dense > 0) {  // the dense-k resampling is linear in S and k is fixed
+            k_spline_log_kernel<<<blocks_for(n_tau, 64), 64, 0, s>>>(n_modes, D(L.lk), n_tau, Sd_in, D(J.s2kd),
+                                                                      D(J.cpkd));
+            k_dense_kernel<<<blocks_for((long long)n_k_dense * n_tau, T), T, 0, s>>>(
+                n_modes, D(L.lk), n_tau, Sd_in, D(J.s2kd), n_k_dense, D(J.sdd), D(J.kscratch));
+            Srow_dot = D(J.sdd);
+        }
+        geom_dot_kernel<<<1, 32, 0, s>>>(n_tau, tau, td, tau0, tau0_dot[d], n_fftlog, D(J.gd));
+        lchi_dot_kernel<<<blocks_for(n_tau, T), T, 0, s>>>(n_tau, tau, td, tau0, tau0_dot[d], D(J.lchid));
+        fgrid_dot_kernel<<<blocks_for(n_fftlog, T), T, 0, s>>>(n_fftlog, D(J.gd), D(L.fbias), D(J.fxd), D(J.fbd));
+        chi_spline_dot_kernel<<<blocks_for(rows, 64), 64, 0, s>>>(rows, n_tau, D(L.lchi), D(J.lchid), Srow, Srow_dot,
+                                                                  D(J.S2v), D(J.S2d), D(J.cpv), D(J.cpd));
+        chi_eval_dot_kernel<<<blocks_for((long long)rows * n_fftlog, T), T, 0, s>>>(
+            rows, n_tau, D(L.lchi), D(J.lchid), Srow, Srow_dot, D(J.S2v), D(J.S2d), n_fftlog,
+            reinterpret_cast<const int*>(ws + L.fidx), D(L.fx), D(J.fxd), D(L.fbias), D(J.fbd), pitch, D(J.Fd));
+        {
+            cufftHandle plan;
+            size_t w2 = 0;
+            std::lock_guard<std::mutex> lock(discoeb_fft::plan_mutex());
+            if (!discoeb_fft::cached_plan(CUFFT_D2Z, n_fftlog, rows, pitch, pitch / 2, &plan, &w2) || w2 > work)
+                return DISCOEB_ECUDA;
+            cufftSetWorkArea(plan, ws + L.cufft);
+            cufftSetStream(plan, s);
+            if (cufftExecD2Z(plan, D(J.Fd), reinterpret_cast<cufftDoubleComplex*>(D(J.Fd))) != CUFFT_SUCCESS)
+                return DISCOEB_ECUDA;
+        }
+        ck_dot_kernel<<<blocks_for((long long)rows * L.n_freq, T), T, 0, s>>>(rows, D(L.kd), n_fftlog, L.n_freq,
+                                                                              D(L.geom), D(J.gd), pitch, D(L.fft),
+                                                                              D(J.Fd));
+        mcoef_dot_kernel<<<blocks_for((long long)n_ell * L.n_freq, T), T, 0, s>>>(n_ell, L.n_freq, n_fftlog, D(L.geom),
+                                                                                  D(J.gd), D(J.Bd));
+        if (cudaGetLastError() != cudaSuccess) return DISCOEB_ECUDA;
+        if (!omega_t_times(D(J.Fd), D(J.H))) return DISCOEB_ECUDA;
+        cell_dot_kernel<<<n_ell, 256, 0, s>>>(n_ell, pitch, D(L.B), D(J.H), D(J.Bd), D(J.G), cell_dot + (size_t)d * n_ell);
+    }
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 

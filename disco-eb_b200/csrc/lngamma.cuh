@@ -5,21 +5,28 @@
 
 #include <cmath>
 
+// host and device (the host build is the CPU test harness of these formulas)
+#if defined(__CUDACC__)
+#define LGF __host__ __device__ inline
+#else
+#define LGF inline
+#endif
+
 namespace dscb {
 namespace cplx {
 
 struct Cx {
     double re, im;
 };
-__device__ inline Cx cx(double r, double i) { return Cx{r, i}; }
-__device__ inline Cx operator+(Cx a, Cx b) { return cx(a.re + b.re, a.im + b.im); }
-__device__ inline Cx operator-(Cx a, Cx b) { return cx(a.re - b.re, a.im - b.im); }
-__device__ inline Cx operator*(Cx a, Cx b) { return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
-__device__ inline Cx cx_log(Cx z) { return cx(log(hypot(z.re, z.im)), atan2(z.im, z.re)); }
+LGF Cx cx(double r, double i) { return Cx{r, i}; }
+LGF Cx operator+(Cx a, Cx b) { return cx(a.re + b.re, a.im + b.im); }
+LGF Cx operator-(Cx a, Cx b) { return cx(a.re - b.re, a.im - b.im); }
+LGF Cx operator*(Cx a, Cx b) { return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+LGF Cx cx_log(Cx z) { return cx(log(hypot(z.re, z.im)), atan2(z.im, z.re)); }
 
 // log Gamma(z) for Re z > 0.5: Lanczos g = 7 with 9 terms (Lanczos, SIAM J. Numer. Anal. B 1
 // (1964) 86; the coefficient set of util.py:26-36)
-__device__ inline Cx lngamma_lanczos(Cx z)
+LGF Cx lngamma_lanczos(Cx z)
 {
     const double c[9] = {0.99999999999980993227684700473478, 676.520368121885098567009190444019,
                          -1259.13921672240287047156078755283, 771.3234287776530788486528258894,
@@ -37,7 +44,7 @@ __device__ inline Cx lngamma_lanczos(Cx z)
 }
 
 // log sin(pi z), stable for large |Im z| (sin(pi z) = (e^{i pi z} - e^{-i pi z}) / 2i)
-__device__ inline Cx log_sin_pi(Cx z)
+LGF Cx log_sin_pi(Cx z)
 {
     const double x = M_PI * z.re, y = M_PI * z.im;
     if (fabs(y) < 20.0) {
@@ -63,7 +70,7 @@ __device__ inline Cx log_sin_pi(Cx z)
     return cx(ay - M_LN2, -s * x + s * M_PI_2) + corr;
 }
 
-__device__ inline Cx lngamma_c(Cx z)
+LGF Cx lngamma_c(Cx z)
 {
     if (z.re <= 0.5) {  // reflection
         const Cx l = lngamma_lanczos(cx(1.0 - z.re, -z.im));
@@ -71,6 +78,84 @@ __device__ inline Cx lngamma_c(Cx z)
         return cx(1.14472988584940017414342735135, 0.0) - ls - l;
     }
     return lngamma_lanczos(z);
+}
+
+LGF Cx operator/(Cx a, Cx b)
+{
+    const double d = b.re * b.re + b.im * b.im;
+    return cx((a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d);
+}
+
+// d/dz of lngamma_lanczos: the exact derivative of the same formula,
+// ln(z' + 7.5) + (z' + 0.5) / (z' + 7.5) - 1 + A'(z') / A(z'), z' = z - 1
+LGF Cx digamma_lanczos(Cx z)
+{
+    const double c[9] = {0.99999999999980993227684700473478, 676.520368121885098567009190444019,
+                         -1259.13921672240287047156078755283, 771.3234287776530788486528258894,
+                         -176.61502916214059906584551354, 12.507343278686904814458936853,
+                         -0.13857109526572011689554707, 9.984369578019570859563e-6, 1.50563273514931155834e-7};
+    z = cx(z.re - 1.0, z.im);
+    Cx A = cx(c[0], 0.0), dA = cx(0.0, 0.0);
+    for (int j = 1; j < 9; ++j) {
+        const Cx inv = cx(1.0, 0.0) / cx(z.re + j, z.im);
+        A = A + cx(c[j] * inv.re, c[j] * inv.im);
+        const Cx inv2 = inv * inv;
+        dA = dA - cx(c[j] * inv2.re, c[j] * inv2.im);
+    }
+    const Cx zh = cx(z.re + 0.5, z.im), zg = cx(z.re + 7.5, z.im);
+    return cx_log(zg) + zh / zg - cx(1.0, 0.0) + dA / A;
+}
+
+// pi cot(pi z), stable for large |Im z|: i pi (E + 1) / (E - 1) with E = exp(2 i pi z) when
+// Im z > 0, i pi (1 + E') / (1 - E') with E' = exp(-2 i pi z) otherwise (|E|, |E'| <= 1)
+LGF Cx pi_cot_pi(Cx z)
+{
+    const double s = z.im > 0 ? 1.0 : -1.0;
+    const double mag = exp(-2.0 * M_PI * fabs(z.im));
+    double sn, cs;
+    sincos(2.0 * M_PI * s * z.re, &sn, &cs);
+    const Cx E = cx(mag * cs, mag * sn);
+    const Cx q = (z.im > 0) ? (E + cx(1.0, 0.0)) / (E - cx(1.0, 0.0)) : (cx(1.0, 0.0) + E) / (cx(1.0, 0.0) - E);
+    return cx(-M_PI * q.im, M_PI * q.re);
+}
+
+// digamma: the derivative of lngamma_c, branch for branch (reflection for Re z <= 0.5:
+// d/dz [ln pi - ln sin(pi z) - lnGamma(1 - z)] = -pi cot(pi z) + psi(1 - z))
+LGF Cx digamma_c(Cx z)
+{
+    if (z.re <= 0.5) return digamma_lanczos(cx(1.0 - z.re, -z.im)) - pi_cot_pi(z);
+    return digamma_lanczos(z);
+}
+
+// One FFTLog kernel coefficient M_l(p), p = bias + i eta, eta = 2 pi q / (n_fft dl), as the pair
+// (Re M, -Im M) that the frequency sum reads, and its derivative along a change dl_dot of the
+// grid spacing (p moves by i eta_dot, eta_dot = -eta dl_dot / dl):
+// ln M = (p - 1) ln 2 + ln(pi)/2 + lnGamma((1 + l + p)/2) - lnGamma((2 + l - p)/2)
+// (cmb.py:636-677); d ln M / dp = ln 2 + psi((1 + l + p)/2)/2 + psi((2 + l - p)/2)/2.  Where the
+// reference's log-Gamma overflows the coefficient is exactly zero, and so is its derivative.
+LGF void fftlog_mcoef(int l, int q, int n_fft, double bias, double dl, double dl_dot, double* b, double* b_dot)
+{
+    const double eta = 2.0 * M_PI * q / (n_fft * dl);
+    const Cx p = cx(bias, eta);
+    const Cx a1 = cx((1.0 + l + p.re) / 2.0, p.im / 2.0), a2 = cx((2.0 + l - p.re) / 2.0, -p.im / 2.0);
+    const Cx lc = cx((p.re - 1.0) * M_LN2 + 0.5 * log(M_PI), p.im * M_LN2) + lngamma_c(a1) - lngamma_c(a2);
+    if (lc.re == -INFINITY) {
+        b[0] = b[1] = 0.0;
+        if (b_dot) b_dot[0] = b_dot[1] = 0.0;
+        return;
+    }
+    const double mag = exp(lc.re);
+    double sn, cs;
+    sincos(lc.im, &sn, &cs);
+    b[0] = mag * cs;
+    b[1] = -mag * sn;
+    if (!b_dot) return;
+    const Cx half = cx(0.5, 0.0);
+    const Cx dlc = cx(M_LN2, 0.0) + half * digamma_c(a1) + half * digamma_c(a2);
+    const double eta_dot = -eta * dl_dot / dl;
+    const Cx Mdot = cx(mag * cs, mag * sn) * dlc * cx(0.0, eta_dot);
+    b_dot[0] = Mdot.re;
+    b_dot[1] = -Mdot.im;
 }
 
 }  // namespace cplx

@@ -181,6 +181,12 @@ def lib():
                                   ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int64, vp, vp, vp]
         L.discoeb_los.restype = ctypes.c_int32
         L.discoeb_cell.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, ctypes.c_double, ctypes.c_double, vp, vp]
+        L.discoeb_los_cell_jvp_workspace_bytes.argtypes = [ctypes.c_int32] * 5
+        L.discoeb_los_cell_jvp_workspace_bytes.restype = ctypes.c_int64
+        L.discoeb_los_cell_jvp.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, vp, ctypes.c_double, ctypes.c_int32,
+                                           vp, vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                           ctypes.c_double, vp, ctypes.c_int64, vp, vp, vp]
+        L.discoeb_los_cell_jvp.restype = ctypes.c_int32
         L.discoeb_cell.restype = ctypes.c_int32
         c32, c64, cd = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
         L.discoeb_power_amplitudes.argtypes = [c32, vp, vp, c32, c32, cd, cd, cd, c32, vp, vp]

@@ -156,6 +156,40 @@ def compute_Cell(theta_ell, kmodes, n_s, k_p, device=None):
     return cell
 
 
+def compute_Cell_tangent(ellmax, kmodes, tau, S, tau0, n_s, k_p, tau_dot, S_dot, tau0_dot, n_fftlog=16384,
+                         n_k_dense=0, device=None):
+    """C_l of the line of sight (compute_theta_ell then compute_Cell) and its derivatives along
+    the input directions (``tau_dot [D, n_tau]``, ``S_dot [D, K, n_tau]``, ``tau0_dot [D]``) in
+    forward mode (discoeb_los_cell_jvp).  Returns ``(cell [ellmax+1], cell_dot [D, ellmax+1])``
+    as device tensors."""
+    torch, device = _device(device)
+    lib = _abi.lib()
+    f64 = dict(dtype=torch.float64, device=device)
+    as_dev = lambda a: (a if isinstance(a, torch.Tensor) else torch.from_numpy(  # noqa: E731
+        np.ascontiguousarray(a, dtype=np.float64))).to(**f64).contiguous()
+    d_k, d_tau, d_S = as_dev(kmodes), as_dev(tau), as_dev(S)
+    d_td, d_Sd = as_dev(tau_dot), as_dev(S_dot)
+    t0d = np.ascontiguousarray(tau0_dot, dtype=np.float64)
+    K, T = d_S.shape
+    nd = int(t0d.shape[0])
+    if d_k.shape[0] != K or d_tau.shape[0] != T or tuple(d_td.shape) != (nd, T) or tuple(d_Sd.shape) != (nd, K, T):
+        raise ValueError("inconsistent shapes for the line-of-sight tangent")
+    nb = lib.discoeb_los_cell_jvp_workspace_bytes(K, T, int(ellmax), int(n_fftlog), int(n_k_dense))
+    if nb < 0:
+        raise ValueError(f"invalid sizes for the line-of-sight tangent (code {nb})")
+    ws = torch.empty(int(nb) // 8 + 32, **f64)
+    aligned = (ws.data_ptr() + 255) // 256 * 256
+    cell = torch.empty(int(ellmax) + 1, **f64)
+    cell_dot = torch.empty((nd, int(ellmax) + 1), **f64)
+    rc = lib.discoeb_los_cell_jvp(K, d_k.data_ptr(), T, d_tau.data_ptr(), d_S.data_ptr(), float(tau0), nd,
+                                  d_td.data_ptr(), d_Sd.data_ptr(), t0d.ctypes.data, int(ellmax), int(n_fftlog),
+                                  int(n_k_dense), float(n_s), float(k_p), aligned, int(nb), cell.data_ptr(),
+                                  cell_dot.data_ptr(), torch.cuda.current_stream(device).cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"discoeb_los_cell_jvp failed with code {rc}")
+    return cell, cell_dot
+
+
 def compute_Dell(Cell, A_s, Tcmb, ellmax=None):
     """D_l = l(l+1) C_l A_s 2 T_cmb^2 1e12 for l >= 2 (the reference's convention, cmb.py:876-927)."""
     C = Cell.detach().cpu().numpy() if hasattr(Cell, "detach") else np.asarray(Cell)
@@ -210,7 +244,7 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
 def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0, n_k_dense=8192, n_fftlog=16384,
                           lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3, num_thermo=1024, rtol=1e-4, atol=1e-4,
                           max_steps=2048, k_sampling_method="camb", aexp_out=None, de_guard_eps=1e-9, device=None,
-                          rel_step=1e-4):
+                          rel_step=1e-4, los="tangent"):
     """C_l^TT and dC_l/dtheta for theta = (omega_c, omega_b, h, n_s, ln10As, w0, wa, m_nu)
     (``gradients.THETA_NAMES``), what ``jax.jacfwd`` of the reference's
     compute_Cell_spectrum_from_cosmo_params (cmb.py:931-1090) gives.
@@ -218,14 +252,15 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     The background and its six parameter tangents come from discoeb_background (forward mode,
     Recfast steps held), the perturbation states at every output time and their tangents from one
     discoeb_jvp_full launch (forward mode, accepted steps held).  The stages after the solve
-    (sources, line of sight, C_l) involve no adaptive choice, so along each direction they are
-    differenced along the exact tangents of their inputs, h = ``rel_step`` max(|theta_d|, 0.01):
-    the sources by a central difference with states, output times, background tables and scalars
-    moved by +-h times their tangents (the sources are smooth in them: O(h^2)), then the line of
-    sight and C_l by a fourth-order central difference along the first-order path (sources, output
-    times and tau0 moved by -2h..2h times their tangents; fourth order because the discrete C_l
-    ripples as the FFTLog grid moves with tau0): O(h^4) plus rounding (a few 1e-12 of C_l at low
-    l, where the FFTLog sum cancels) over h.  n_s enters
+    (sources, line of sight, C_l) involve no adaptive choice.  The sources' tangent along each
+    direction is a central difference with states, output times, background tables and scalars
+    moved by +-h times their exact tangents, h = ``rel_step`` max(|theta_d|, 0.01) (the sources are
+    smooth in them: O(h^2)).  The line of sight and C_l then take that tangent with the output
+    times' and tau0's: ``los="tangent"`` in forward mode (discoeb_los_cell_jvp: the resampling, the
+    FFT coefficients and the table M_l(p) differentiated as the FFTLog grid moves with tau0, one
+    GEMM per direction), ``los="differences"`` by a fourth-order central difference along the
+    first-order path (four lines of sight per direction; fourth order because the discrete C_l
+    ripples as the grid moves: O(h^4) plus rounding, a few 1e-12 of C_l at low l, over h).  n_s enters
     through the primordial weight of C_l alone (a fourth-order difference of compute_Cell); C_l
     does not depend on A_s (D_l carries it).  The k
     sampling, start times and approximation switch times are held at the base point (the camb
@@ -267,6 +302,9 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     th, kk, cell = los_cell(S0, tau_b, tau0_b)
     J = np.zeros((len(THETA_NAMES), ellmax + 1))
     stencil = ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0))
+    if los not in ("tangent", "differences"):
+        raise ValueError(f"los must be 'tangent' or 'differences', not {los!r}")
+    tangents = []
     for di, name in enumerate(ODE_DIRECTIONS):
         h = rel_step * max(abs(float(theta[name])), 1e-2)
         ydot = prob.state_tangent(di)
@@ -284,6 +322,9 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
         tau_dot = (side[0][1] - side[1][1]) / (2 * h)
         tau0_dot = (side[0][2] - side[1][2]) / (2 * h)
         del side
+        if los == "tangent":
+            tangents.append((S_dot, tau_dot, tau0_dot))
+            continue
         # the line of sight and C_l along that first-order path (the derivative at the base point
         # depends on the path's slope only): fourth order, the discrete C_l ripples in tau0
         acc = np.zeros(ellmax + 1)
@@ -291,6 +332,14 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
             acc += wgt * los_cell(torch.add(S0, S_dot, alpha=m * h), tau_b + m * h * tau_dot,
                                   tau0_b + m * h * tau0_dot)[2]
         J[THETA_NAMES.index(name)] = acc / h
+    if los == "tangent":
+        _, cdot = compute_Cell_tangent(ellmax, kmodes, tau_b, S0, tau0_b, bg["n_s"], bg["k_p"],
+                                       np.stack([t[1] for t in tangents]), torch.stack([t[0] for t in tangents]),
+                                       np.array([t[2] for t in tangents]), n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                       device=device)
+        cdot = cdot.cpu().numpy()
+        for di, name in enumerate(ODE_DIRECTIONS):
+            J[THETA_NAMES.index(name)] = cdot[di]
     h = rel_step * max(abs(float(bg["n_s"])), 1e-2)
     acc = np.zeros(ellmax + 1)
     for m, wgt in stencil:

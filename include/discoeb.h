@@ -257,6 +257,24 @@ int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
 int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta, double n_s,
                      double k_p, double* cell, void* stream);
 
+/* C_l of the line of sight (discoeb_los then discoeb_cell, same arguments) and its derivative
+ * along n_dir directions of the inputs, in forward mode through the resampling, the FFT
+ * coefficients and the table M_l(p) (the grid moves with tau0 - tau; the interval indices of the
+ * resampling are the base point's): the C_l part of jax.jacfwd through compute_theta_ell and
+ * compute_Cell (cmb.py:680-873).
+ *   tau_dot [n_dir, n_tau], S_dot [n_dir, n_modes, n_tau]   device
+ *   tau0_dot [n_dir]                                         host
+ *   cell [ellmax + 1], cell_dot [n_dir, ellmax + 1]          device
+ *   workspace: >= discoeb_los_cell_jvp_workspace_bytes(...) bytes, 256-byte aligned
+ * One GEMM for the base point, one shared, one per direction (each the size of discoeb_los's). */
+int64_t discoeb_los_cell_jvp_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
+                                             int32_t n_k_dense);
+int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S,
+                             double tau0, int32_t n_dir, const double* tau_dot, const double* S_dot,
+                             const double* tau0_dot, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, double n_s,
+                             double k_p, void* workspace, int64_t workspace_bytes, double* cell, double* cell_dot,
+                             void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Observables of the linear power spectrum (device arrays, stream-ordered).
  *

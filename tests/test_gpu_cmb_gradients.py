@@ -98,9 +98,10 @@ def test_gpu_cell_jacobian_matches_central_differences(torch_cuda, size):
         # dC_l/dtheta oscillates in l and crosses zero: deviations against the direction's largest
         worst[name] = float(np.abs(J[i][l] - fd[l]).max() / np.abs(fd[l]).max())
     print("max |J - fd| / max |fd| per direction:", worst)
-    # measured: <= 4e-6 on the reduced chain; at the reference's defaults <= 2.4e-6 except wa and
-    # m_nu (2.4e-5, 7.5e-5), the directions C_l is least sensitive to, where the solver's
-    # rounding in the check's quotient weighs most.  Bound: the metric's 1e-4
+    # measured: <= 4e-6 on the reduced chain; at the reference's defaults <= 2.6e-5 except m_nu
+    # (7.1e-5), limited by the check itself: its step-1e-4 quotient misses ~2e-5 of the ripple
+    # (a cell of the 16384-point grid is ~1.2e-3 of omega_c), and in the directions C_l is least
+    # sensitive to the solver's rounding in the quotient weighs most.  Bound: the metric's 1e-4
     assert max(worst.values()) < 1e-4, worst
 
 
@@ -117,3 +118,28 @@ def test_gpu_cell_jacobian_does_not_depend_on_the_difference_step(torch_cuda):
     dev = [float(np.abs(J1[i][l] - J2[i][l]).max() / max(np.abs(J1[i][l]).max(), 1e-300)) for i in range(8)]
     print("step dependence per direction:", dev)
     assert max(dev) <= 1e-5, dev
+
+
+@pytest.mark.parametrize("size", [SMALL, DEFAULT], ids=["small", "reference_defaults"])
+def test_gpu_line_of_sight_tangent_equals_its_differences(torch_cuda, size):
+    """The forward-mode line of sight (discoeb_los_cell_jvp) against fourth-order differences of
+    the same line of sight along the same first-order path: one derivative, two evaluations.
+
+    The differences' truncation error is (omega h)^4 / 30 of the ripple's share of the derivative,
+    omega the ripple's frequency in the parameter (one FFTLog cell per period: at 16384 points a
+    period is ~1.2e-3 of omega_c, so step 1e-4 leaves ~2e-5); at step 2.5e-5 it is 256 times
+    smaller, but the rounding of the line of sight (its FFTLog sum cancels at low l) over the
+    step grows 4 times and takes over in the directions C_l is least sensitive to.  Per direction
+    the better of the two steps is compared (measured: <= 8e-6 at the reference's defaults,
+    <= 1.3e-6 on the reduced chain)."""
+    from discoeb_b200.cmb import compute_Cell_jacobian
+    C1, J1, _ = compute_Cell_jacobian(THETA, los="tangent", **size)
+    l = slice(2, None)
+    devs = []
+    for step in (1e-4, 2.5e-5):
+        C2, J2, _ = compute_Cell_jacobian(THETA, los="differences", rel_step=step, **size)
+        np.testing.assert_array_equal(C1, C2)
+        devs.append([float(np.abs(J1[i][l] - J2[i][l]).max() / max(np.abs(J2[i][l]).max(), 1e-300)) for i in range(8)])
+    print("tangent vs differences (steps 1e-4, 2.5e-5) per direction:", devs)
+    best = [min(a, b) for a, b in zip(*devs)]
+    assert max(best) <= 2e-5, best
