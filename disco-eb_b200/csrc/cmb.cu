@@ -380,7 +380,7 @@ __device__ inline double cell_weight(int i, int n_modes, const double* __restric
 
 __global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __restrict__ kmodes, int n_ell,
                                                    const double* __restrict__ theta, double n_s, double k_p,
-                                                   double* cell)
+                                                   double* cell, bool d_n_s = false)
 {
     __shared__ double w[kCellChunk];
     __shared__ double part[8][32];
@@ -390,7 +390,9 @@ __global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __
     for (int c0 = 0; c0 < n_modes; c0 += kCellChunk) {
         const int cn = min(kCellChunk, n_modes - c0);
         __syncthreads();
-        for (int j = threadIdx.x; j < cn; j += blockDim.x) w[j] = cell_weight(c0 + j, n_modes, kmodes, n_s, k_p);
+        // d_n_s: the weights' derivative in n_s, ln(k_i/k_p) w_i, for d C_l / d n_s
+        for (int j = threadIdx.x; j < cn; j += blockDim.x)
+            w[j] = cell_weight(c0 + j, n_modes, kmodes, n_s, k_p) * (d_n_s ? log(kmodes[c0 + j] / k_p) : 1.0);
         __syncthreads();
         if (l < n_ell) {
 #pragma unroll 4
@@ -888,7 +890,7 @@ int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_ta
                              double tau0, int32_t n_dir, const double* tau_dot, const double* S_dot,
                              const double* tau0_dot, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, double n_s,
                              double k_p, void* workspace, int64_t workspace_bytes, double* cell, double* cell_dot,
-                             void* stream)
+                             double* cell_dns, void* stream)
 {
     if (!los_args_ok(n_modes, n_tau, ellmax, n_fftlog, n_k_dense) || n_dir < 0) return DISCOEB_EINVAL;
     if (!kmodes || !tau || !S || !workspace || !cell) return DISCOEB_EINVAL;
@@ -910,6 +912,7 @@ int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_ta
                          D(J.th), D(J.kout), stream);
     if (rc) return rc;
     cell_kernel<<<(n_ell + 31) / 32, 256, 0, s>>>(rows, D(J.kout), n_ell, D(J.th), n_s, k_p, cell);
+    if (cell_dns) cell_kernel<<<(n_ell + 31) / 32, 256, 0, s>>>(rows, D(J.kout), n_ell, D(J.th), n_s, k_p, cell_dns, true);
     if (n_dir == 0) return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
     cell_weight_kernel<<<blocks_for(rows, T), T, 0, s>>>(rows, D(J.kout), n_s, k_p, D(J.w));
     scale_rows_kernel<<<blocks_for((long long)rows * n_ell, T), T, 0, s>>>(rows, n_ell, D(J.w), D(J.th));

@@ -185,7 +185,7 @@ def lib():
         L.discoeb_los_cell_jvp_workspace_bytes.restype = ctypes.c_int64
         L.discoeb_los_cell_jvp.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, vp, ctypes.c_double, ctypes.c_int32,
                                            vp, vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
-                                           ctypes.c_double, vp, ctypes.c_int64, vp, vp, vp]
+                                           ctypes.c_double, vp, ctypes.c_int64, vp, vp, vp, vp]
         L.discoeb_los_cell_jvp.restype = ctypes.c_int32
         L.discoeb_cell.restype = ctypes.c_int32
         c32, c64, cd = ctypes.c_int32, ctypes.c_int64, ctypes.c_double

@@ -160,8 +160,8 @@ def compute_Cell_tangent(ellmax, kmodes, tau, S, tau0, n_s, k_p, tau_dot, S_dot,
                          n_k_dense=0, device=None):
     """C_l of the line of sight (compute_theta_ell then compute_Cell) and its derivatives along
     the input directions (``tau_dot [D, n_tau]``, ``S_dot [D, K, n_tau]``, ``tau0_dot [D]``) in
-    forward mode (discoeb_los_cell_jvp).  Returns ``(cell [ellmax+1], cell_dot [D, ellmax+1])``
-    as device tensors."""
+    forward mode (discoeb_los_cell_jvp).  Returns ``(cell [ellmax+1], cell_dot [D, ellmax+1],
+    cell_dns [ellmax+1])`` as device tensors, the last d C_l / d n_s."""
     torch, device = _device(device)
     lib = _abi.lib()
     f64 = dict(dtype=torch.float64, device=device)
@@ -180,14 +180,15 @@ def compute_Cell_tangent(ellmax, kmodes, tau, S, tau0, n_s, k_p, tau_dot, S_dot,
     ws = torch.empty(int(nb) // 8 + 32, **f64)
     aligned = (ws.data_ptr() + 255) // 256 * 256
     cell = torch.empty(int(ellmax) + 1, **f64)
-    cell_dot = torch.empty((nd, int(ellmax) + 1), **f64)
+    cell_dot = torch.empty((max(nd, 1), int(ellmax) + 1), **f64)
+    cell_dns = torch.empty(int(ellmax) + 1, **f64)
     rc = lib.discoeb_los_cell_jvp(K, d_k.data_ptr(), T, d_tau.data_ptr(), d_S.data_ptr(), float(tau0), nd,
                                   d_td.data_ptr(), d_Sd.data_ptr(), t0d.ctypes.data, int(ellmax), int(n_fftlog),
                                   int(n_k_dense), float(n_s), float(k_p), aligned, int(nb), cell.data_ptr(),
-                                  cell_dot.data_ptr(), torch.cuda.current_stream(device).cuda_stream)
+                                  cell_dot.data_ptr(), cell_dns.data_ptr(), torch.cuda.current_stream(device).cuda_stream)
     if rc != 0:
         raise RuntimeError(f"discoeb_los_cell_jvp failed with code {rc}")
-    return cell, cell_dot
+    return cell, cell_dot[:nd], cell_dns
 
 
 def compute_Dell(Cell, A_s, Tcmb, ellmax=None):
@@ -261,7 +262,8 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     GEMM per direction), ``los="differences"`` by a fourth-order central difference along the
     first-order path (four lines of sight per direction; fourth order because the discrete C_l
     ripples as the grid moves: O(h^4) plus rounding, a few 1e-12 of C_l at low l, over h).  n_s enters
-    through the primordial weight of C_l alone (a fourth-order difference of compute_Cell); C_l
+    through the primordial weight of C_l alone (in closed form with ``los="tangent"``, by a
+    fourth-order difference of compute_Cell with ``los="differences"``); C_l
     does not depend on A_s (D_l carries it).  The k
     sampling, start times and approximation switch times are held at the base point (the camb
     sampling's dependence on tau_maxvis is not differentiated).
@@ -299,7 +301,8 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
 
     S0 = sources(bg, y)
     tau_b, tau0_b = times(bg)
-    th, kk, cell = los_cell(S0, tau_b, tau0_b)
+    if los == "differences":
+        th, kk, cell = los_cell(S0, tau_b, tau0_b)
     J = np.zeros((len(THETA_NAMES), ellmax + 1))
     stencil = ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0))
     if los not in ("tangent", "differences"):
@@ -333,18 +336,21 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
                                   tau0_b + m * h * tau0_dot)[2]
         J[THETA_NAMES.index(name)] = acc / h
     if los == "tangent":
-        _, cdot = compute_Cell_tangent(ellmax, kmodes, tau_b, S0, tau0_b, bg["n_s"], bg["k_p"],
-                                       np.stack([t[1] for t in tangents]), torch.stack([t[0] for t in tangents]),
-                                       np.array([t[2] for t in tangents]), n_fftlog=n_fftlog, n_k_dense=n_k_dense,
-                                       device=device)
-        cdot = cdot.cpu().numpy()
+        cell, cdot, cdns = compute_Cell_tangent(ellmax, kmodes, tau_b, S0, tau0_b, bg["n_s"], bg["k_p"],
+                                                np.stack([t[1] for t in tangents]),
+                                                torch.stack([t[0] for t in tangents]),
+                                                np.array([t[2] for t in tangents]), n_fftlog=n_fftlog,
+                                                n_k_dense=n_k_dense, device=device)
+        cell, cdot = cell.cpu().numpy(), cdot.cpu().numpy()
         for di, name in enumerate(ODE_DIRECTIONS):
             J[THETA_NAMES.index(name)] = cdot[di]
-    h = rel_step * max(abs(float(bg["n_s"])), 1e-2)
-    acc = np.zeros(ellmax + 1)
-    for m, wgt in stencil:
-        acc += wgt * compute_Cell(th, kk, bg["n_s"] + m * h, bg["k_p"], device=device).cpu().numpy()
-    J[THETA_NAMES.index("n_s")] = acc / h
+        J[THETA_NAMES.index("n_s")] = cdns.cpu().numpy()
+    else:
+        h = rel_step * max(abs(float(bg["n_s"])), 1e-2)
+        acc = np.zeros(ellmax + 1)
+        for m, wgt in stencil:
+            acc += wgt * compute_Cell(th, kk, bg["n_s"] + m * h, bg["k_p"], device=device).cpu().numpy()
+        J[THETA_NAMES.index("n_s")] = acc / h
     param = dict(bg)
     for key, v in (("lmaxg", lmaxg), ("lmaxgp", lmaxgp), ("lmaxr", lmaxr), ("lmaxnu", lmaxnu), ("nqmax", nqmax),
                    ("nout", aexp_out.shape[0]), ("tau_out", bg["tau_of_a_spline"].evaluate(aexp_out))):

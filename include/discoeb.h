@@ -265,6 +265,7 @@ int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const
  *   tau_dot [n_dir, n_tau], S_dot [n_dir, n_modes, n_tau]   device
  *   tau0_dot [n_dir]                                         host
  *   cell [ellmax + 1], cell_dot [n_dir, ellmax + 1]          device
+ *   cell_dns [ellmax + 1]  d C_l / d n_s (the primordial weight's derivative), device, may be NULL
  *   workspace: >= discoeb_los_cell_jvp_workspace_bytes(...) bytes, 256-byte aligned
  * One GEMM for the base point, one shared, one per direction (each the size of discoeb_los's). */
 int64_t discoeb_los_cell_jvp_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
@@ -273,7 +274,7 @@ int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_ta
                              double tau0, int32_t n_dir, const double* tau_dot, const double* S_dot,
                              const double* tau0_dot, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, double n_s,
                              double k_p, void* workspace, int64_t workspace_bytes, double* cell, double* cell_dot,
-                             void* stream);
+                             double* cell_dns, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
  * Observables of the linear power spectrum (device arrays, stream-ordered).
