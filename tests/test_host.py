@@ -102,6 +102,27 @@ def test_jvp_entries_reject_missing_outputs_before_any_launch():
         assert entry(*args) == -1  # no direction
 
 
+def test_line_of_sight_tangent_entry_rejects_bad_arguments_before_any_launch():
+    lib = _abi.lib()
+    f = lib.discoeb_los_cell_jvp
+    fake = 4096  # never dereferenced: the argument checks return first
+    t0d = (ctypes.c_double * 2)(0.0, 0.0)
+    ok = [8, fake, 16, fake, fake, 1.0e4, 2, fake, fake, ctypes.addressof(t0d), 100, 256, 0, 0.96, 0.05, 4096, 1 << 30,
+          fake, fake, None, None]
+    bad = [(0, 1), (2, 2), (10, -1), (11, 1), (12, 1), (15, None), (6, -1)]  # sizes, workspace, n_dir
+    for i, v in bad:
+        args = list(ok)
+        args[i] = v
+        assert f(*args) == -1, (i, v)
+    args = list(ok)
+    args[8] = None  # directions without their source tangents
+    assert f(*args) == -1
+    args = list(ok)
+    args[15] = 4097  # workspace not 256-byte aligned
+    assert f(*args) == -1
+    assert lib.discoeb_los_cell_jvp_workspace_bytes(1, 16, 100, 256, 0) == -1
+
+
 def test_struct_layout_matches_header():
     # the ctypes mirror must have the C layout: compile a tiny probe of offsetof/sizeof
     import tempfile
