@@ -356,3 +356,34 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
                    ("nout", aexp_out.shape[0]), ("tau_out", bg["tau_of_a_spline"].evaluate(aexp_out))):
         param[key] = v
     return cell, J, param
+
+
+def cell_spectrum_function(**options):
+    """A ``torch.autograd.Function`` mapping theta (float64[8], ``gradients.THETA_NAMES`` order)
+    to C_l^TT (float64[ellmax+1]).
+
+    The forward pass runs compute_Cell_jacobian and keeps the Jacobian; the backward pass
+    contracts it with the incoming gradient, so ``torch.autograd`` sees the derivative of the
+    discrete chain (for a likelihood of C_l, or of D_l = l(l+1) C_l A_s 2 T_cmb^2 1e12 built from
+    it with A_s = exp(theta[4]) / 1e10).  ``options`` are those of compute_Cell_jacobian.
+    """
+    import torch
+
+    from .gradients import THETA_NAMES
+
+    class CellSpectrum(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, theta):
+            if theta.shape != (len(THETA_NAMES),):
+                raise ValueError(f"theta must have shape ({len(THETA_NAMES)},) in the order {THETA_NAMES}")
+            th = dict(zip(THETA_NAMES, theta.detach().to("cpu", torch.float64).tolist()))
+            C, J, _ = compute_Cell_jacobian(th, **options)
+            ctx.save_for_backward(torch.from_numpy(J).to(theta.device))
+            return torch.from_numpy(C).to(theta.device)
+
+        @staticmethod
+        def backward(ctx, grad_C):
+            (J,) = ctx.saved_tensors
+            return J @ grad_C.to(J.dtype)
+
+    return CellSpectrum

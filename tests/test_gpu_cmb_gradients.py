@@ -143,3 +143,17 @@ def test_gpu_line_of_sight_tangent_equals_its_differences(torch_cuda, size):
     print("tangent vs differences (steps 1e-4, 2.5e-5) per direction:", devs)
     best = [min(a, b) for a, b in zip(*devs)]
     assert max(best) <= 2e-5, best
+
+
+def test_gpu_cell_autograd_function_contracts_the_jacobian(torch_cuda):
+    torch = torch_cuda
+    from discoeb_b200.cmb import cell_spectrum_function, compute_Cell_jacobian
+    from discoeb_b200.gradients import THETA_NAMES
+    CS = cell_spectrum_function(**SMALL)
+    theta = torch.tensor([THETA[n] for n in THETA_NAMES], dtype=torch.float64, device="cuda", requires_grad=True)
+    C = CS.apply(theta)
+    weights = torch.linspace(0.5, 2.0, C.numel(), dtype=torch.float64, device="cuda")
+    (C * weights).sum().backward()
+    C_ref, J, _ = compute_Cell_jacobian(THETA, **SMALL)
+    np.testing.assert_array_equal(C.detach().cpu().numpy(), C_ref)
+    np.testing.assert_allclose(theta.grad.cpu().numpy(), J @ weights.cpu().numpy(), rtol=1e-12)
