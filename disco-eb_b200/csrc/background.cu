@@ -169,3 +169,33 @@ extern "C" int32_t discoeb_background(const DiscoebCosmoParams* par, const Disco
     for (auto& th : pool) th.join();
     return DISCOEB_SUCCESS;
 }
+
+// Knot second derivatives of the natural cubic spline through (x[i], y[i]), i < n: the Thomas
+// recurrence of the reference's spline_interpolation (spline_interpolation.py:19-75), operation
+// for operation (host code, IEEE double, no contraction), so that host tables built here equal
+// those of the Python restatement bit for bit.
+extern "C" int32_t discoeb_natural_spline_second(int32_t n, const double* x, const double* y, double* S)
+{
+    if (n < 2 || !x || !y || !S) return DISCOEB_EINVAL;
+    S[0] = 0.0;
+    S[n - 1] = 0.0;
+    const int m = n - 2;
+    if (m <= 0) return DISCOEB_SUCCESS;
+    std::vector<double> cp(m), dp(m);
+    for (int i = 0; i < m; ++i) {
+        const double h0 = x[i + 1] - x[i], h1 = x[i + 2] - x[i + 1];
+        const double a = h0, b = 2.0 * (h0 + h1), c = h1;
+        const double d = 6.0 * ((y[i + 2] - y[i + 1]) / h1 - (y[i + 1] - y[i]) / h0);
+        if (i == 0) {
+            cp[0] = c / b;
+            dp[0] = d / b;
+        } else {
+            const double denom = b - a * cp[i - 1];
+            cp[i] = (i < m - 1) ? c / denom : 0.0;
+            dp[i] = (d - a * dp[i - 1]) / denom;
+        }
+    }
+    S[m] = dp[m - 1];
+    for (int i = m - 2; i >= 0; --i) S[i + 1] = dp[i] - cp[i] * S[i + 2];
+    return DISCOEB_SUCCESS;
+}

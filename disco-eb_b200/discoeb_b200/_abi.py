@@ -208,6 +208,8 @@ def lib():
         L.discoeb_background_batch_workspace_bytes.restype = c64
         L.discoeb_background_batch.argtypes = [vp, vp, c32, c32, c32, vp, c64, vp, vp, vp]
         L.discoeb_background_batch.restype = c32
+        L.discoeb_natural_spline_second.argtypes = [c32, vp, vp, vp]
+        L.discoeb_natural_spline_second.restype = c32
         L.discoeb_fma_rate_threads.argtypes = []
         L.discoeb_fma_rate_threads.restype = c64
         L.discoeb_fma_rate.argtypes = [c64, vp, c64, ctypes.POINTER(ctypes.c_double), vp]

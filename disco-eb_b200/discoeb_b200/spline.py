@@ -39,7 +39,14 @@ class spline_interpolation:
         h = x[1:] - x[:-1]
         m = n - 2
         S = np.zeros(n, dtype=np.result_type(x.dtype, y.dtype))
-        if m > 0:
+        if m > 0 and S.dtype == np.float64:
+            # the library's host restatement of the same recurrence (discoeb_natural_spline_second)
+            from . import _abi
+            x, y = np.ascontiguousarray(x), np.ascontiguousarray(y)
+            rc = _abi.lib().discoeb_natural_spline_second(n, x.ctypes.data, y.ctypes.data, S.ctypes.data)
+            if rc != 0:
+                raise ValueError(f"discoeb_natural_spline_second failed with code {rc}")
+        elif m > 0:  # complex-step parameters: the recurrence in numpy's complex arithmetic
             a = h[:-1]
             b = 2.0 * (h[:-1] + h[1:])
             c = h[1:]

@@ -381,6 +381,11 @@ int32_t discoeb_background_batch(const DiscoebCosmoParams* par_dev, const Discoe
                                  int32_t n_cosmo, int32_t n_dir, int32_t num_thermo, void* workspace,
                                  int64_t workspace_bytes, double* out_dev, double* out_dot_dev, void* stream);
 
+/* Knot second derivatives S[n] of the natural cubic spline through (x[i], y[i]) (host memory, host
+ * code): the Thomas recurrence of spline_interpolation.__init__ (spline_interpolation.py:19-75),
+ * operation for operation, for the host layer's tables.  DISCOEB_EINVAL if n < 2. */
+int32_t discoeb_natural_spline_second(int32_t n, const double* x, const double* y, double* S);
+
 /* Measurement utility, no counterpart in the reference: the FP64 fused-multiply-add throughput of
  * the current GPU, the roofline denominator of the solver kernels (their arithmetic is FP64 FMA
  * work).  discoeb_fma_rate_threads() returns the thread count of one launch (4 blocks of 256 per

@@ -123,6 +123,47 @@ def test_line_of_sight_tangent_entry_rejects_bad_arguments_before_any_launch():
     assert lib.discoeb_los_cell_jvp_workspace_bytes(1, 16, 100, 256, 0) == -1
 
 
+def test_native_spline_recurrence_equals_the_reference_recurrence_bitwise():
+    """spline_interpolation's knot second derivatives come from the library's host restatement of
+    the reference's Thomas recurrence (spline_interpolation.py:19-75); the recurrence written out
+    on numpy float64 scalars gives the same bits."""
+    from discoeb_b200.spline import spline_interpolation
+
+    def recurrence(x, y):
+        n = len(y)
+        S = np.zeros(n)
+        m = n - 2
+        if m <= 0:
+            return S
+        h = x[1:] - x[:-1]
+        a, b, c = h[:-1], 2.0 * (h[:-1] + h[1:]), h[1:]
+        d = 6.0 * ((y[2:] - y[1:-1]) / h[1:] - (y[1:-1] - y[:-2]) / h[:-1])
+        cp, dp = np.zeros(m), np.zeros(m)
+        cp[0], dp[0] = c[0] / b[0], d[0] / b[0]
+        for i in range(1, m):
+            den = b[i] - a[i] * cp[i - 1]
+            cp[i] = c[i] / den if i < m - 1 else 0.0
+            dp[i] = (d[i] - a[i] * dp[i - 1]) / den
+        Si = np.zeros(m)
+        Si[m - 1] = dp[m - 1]
+        for i in range(m - 2, -1, -1):
+            Si[i] = dp[i] - cp[i] * Si[i + 1]
+        S[1:-1] = Si
+        return S
+
+    rng = np.random.default_rng(7)
+    for n in (2, 3, 4, 17, 1024):
+        x = np.sort(rng.uniform(-3.0, 10.0, n))
+        y = np.exp(-x) + rng.normal(size=n) * 1e-3
+        np.testing.assert_array_equal(spline_interpolation(x, y).S, recurrence(x, y))
+    # complex (complex-step) data keeps the numpy recurrence, whose real part is the same spline
+    x = np.sort(rng.uniform(0.0, 5.0, 64))
+    y = np.sin(x)
+    Sc = spline_interpolation(x, y + 1e-30j * np.cos(x)).S
+    np.testing.assert_allclose(Sc.real, recurrence(x, y), rtol=1e-12, atol=1e-13)
+    assert _abi.lib().discoeb_natural_spline_second(1, 0, 0, 0) == -1
+
+
 def test_struct_layout_matches_header():
     # the ctypes mirror must have the C layout: compile a tiny probe of offsetof/sizeof
     import tempfile
