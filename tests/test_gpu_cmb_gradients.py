@@ -13,6 +13,7 @@ THETA = dict(omega_c=0.120, omega_b=0.0224, h=0.674, n_s=0.965, ln10As=math.log(
 # reference's pipeline defaults
 SMALL = dict(ellmax=600, nmodes=32, n_k_dense=1024, n_fftlog=4096)
 DEFAULT = dict(ellmax=2500, nmodes=128, n_k_dense=8192, n_fftlog=16384)
+NO_DENSE = dict(ellmax=600, nmodes=32, n_k_dense=0, n_fftlog=4096)  # the modes' own k grid
 
 
 @pytest.fixture(scope="module")
@@ -120,7 +121,7 @@ def test_gpu_cell_jacobian_does_not_depend_on_the_difference_step(torch_cuda):
     assert max(dev) <= 1e-5, dev
 
 
-@pytest.mark.parametrize("size", [SMALL, DEFAULT], ids=["small", "reference_defaults"])
+@pytest.mark.parametrize("size", [SMALL, DEFAULT, NO_DENSE], ids=["small", "reference_defaults", "no_dense_k"])
 def test_gpu_line_of_sight_tangent_equals_its_differences(torch_cuda, size):
     """The forward-mode line of sight (discoeb_los_cell_jvp) against fourth-order differences of
     the same line of sight along the same first-order path: one derivative, two evaluations.
