@@ -273,6 +273,8 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     """
     from .background import _DIFF_FIELDS, background_from_buffer, native_background
     from .gradients import ODE_DIRECTIONS, THETA_NAMES, JacobianProblem, param_dots, theta_to_params
+    if los not in ("tangent", "differences"):
+        raise ValueError(f"los must be 'tangent' or 'differences', not {los!r}")
     torch, device = _device(device)
     L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
     aexp_out = cmb_aexp_out() if aexp_out is None else np.asarray(aexp_out, dtype=np.float64)
@@ -305,8 +307,6 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
         th, kk, cell = los_cell(S0, tau_b, tau0_b)
     J = np.zeros((len(THETA_NAMES), ellmax + 1))
     stencil = ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0))
-    if los not in ("tangent", "differences"):
-        raise ValueError(f"los must be 'tangent' or 'differences', not {los!r}")
     tangents = []
     for di, name in enumerate(ODE_DIRECTIONS):
         h = rel_step * max(abs(float(theta[name])), 1e-2)

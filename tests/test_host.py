@@ -164,6 +164,13 @@ def test_native_spline_recurrence_equals_the_reference_recurrence_bitwise():
     assert _abi.lib().discoeb_natural_spline_second(1, 0, 0, 0) == -1
 
 
+def test_cell_jacobian_rejects_an_unknown_line_of_sight_mode():
+    from discoeb_b200.cmb import compute_Cell_jacobian
+    theta = dict(omega_c=0.12, omega_b=0.0224, h=0.674, n_s=0.965, ln10As=3.04, w0=-0.95, wa=0.0, m_nu=0.06)
+    with pytest.raises(ValueError):
+        compute_Cell_jacobian(theta, los="adjoint")
+
+
 def test_struct_layout_matches_header():
     # the ctypes mirror must have the C layout: compile a tiny probe of offsetof/sizeof
     import tempfile
