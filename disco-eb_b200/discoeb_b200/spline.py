@@ -105,7 +105,7 @@ class spline_interpolation:
         else:
             # number of knots strictly below x_new, minus one (== searchsorted left - 1)
             idx = np.searchsorted(self.x, x_new, side="left") - 1
-        return np.clip(idx, 0, self.n - 2)
+        return np.minimum(np.maximum(idx, 0), self.n - 2)  # clip to [0, n-2] (np.clip's checks cost more)
 
     def _local(self, x_new):
         x_new = np.asarray(x_new)
