@@ -136,9 +136,11 @@ constexpr int kMaxDirsPerBlock = 6;
 // the state at the moving output time is y' + f tau_out', then the RSA projection and the
 // output conversion in dual numbers.  y: the forward state at tau_out[j]; pf: n doubles of
 // scratch; TT.fd / TT.jk are used as scratch.  Full: the RSA-projected state and its tangent
-// (n values per output) are written instead of the 20 output fields.
+// (n values per output) are written instead of the 20 output fields.  Kept out of line: it runs
+// at output times only, and inlined into the tangent loop it lengthens the hot code the seven
+// warps of a block fetch (measured: the gradient kernel 2% slower inlined).
 template <bool Full>
-__device__ void emit_tangent_output(const WarpTeam& tm, const DiscoebCosmo& P, const DiscoebTangent* TN, const Dims& D,
+__device__ __noinline__ void emit_tangent_output(const WarpTeam& tm, const DiscoebCosmo& P, const DiscoebTangent* TN, const Dims& D,
                                     double k, int mode, int dir, int n_modes, int n_out, int j, const double* tau_out,
                                     const double* tau_out_dot, const double* y, int regime, const TanMem& TT,
                                     double* pf, double* y_out20, double* y_out20_dot)
