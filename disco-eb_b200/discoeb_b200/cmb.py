@@ -261,12 +261,11 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     FFT coefficients and the table M_l(p) differentiated as the FFTLog grid moves with tau0, one
     GEMM per direction), ``los="differences"`` by a fourth-order central difference along the
     first-order path (four lines of sight per direction; fourth order because the discrete C_l
-    ripples as the grid moves: O(h^4) plus rounding, a few 1e-12 of C_l at low l, over h).  n_s enters
-    through the primordial weight of C_l alone (in closed form with ``los="tangent"``, by a
-    fourth-order difference of compute_Cell with ``los="differences"``); C_l
-    does not depend on A_s (D_l carries it).  The k
-    sampling, start times and approximation switch times are held at the base point (the camb
-    sampling's dependence on tau_maxvis is not differentiated).
+    ripples as the grid moves: O(h^4) plus rounding, a few 1e-12 of C_l at low l, over h).
+    n_s enters through the primordial weight of C_l alone (in closed form with ``los="tangent"``,
+    by a fourth-order difference of compute_Cell with ``los="differences"``); C_l does not depend
+    on A_s (D_l carries it).  The k sampling, start times and approximation switch times are held
+    at the base point (the camb sampling's dependence on tau_maxvis is not differentiated).
 
     Returns ``(Cell [ellmax+1], J [8, ellmax+1], param)`` (numpy; param as
     compute_Cell_spectrum_from_cosmo_params returns it).
