@@ -260,28 +260,35 @@ class JacobianProblem:
         self.inv[order] = np.arange(K)
         self.dc = DeviceCosmo(bg, de_guard_eps=de_guard_eps, device=device, **L)
         f64 = dict(dtype=torch.float64, device=device)
-        self._keep = []
+        # every input array in one pinned host buffer and one copy (256-byte aligned slices)
+        host_arrays = [kmodes[order], tau_start[order], y0[order], np.stack([d["y0"][order] for d in tans]), sw[order],
+                       tau_out, np.stack([d["tau_out"] for d in tans])]
+        host_arrays += [a for d in tans for (yy, SS) in d["tables"].values() for a in (yy, SS)]
+        offs, o = [], 0
+        for a in host_arrays:
+            offs.append(o)
+            o += (np.asarray(a).size + 31) // 32 * 32
+        self._pinned = torch.empty(o, dtype=torch.float64, pin_memory=True)
+        hp = self._pinned.numpy()
+        for a, at in zip(host_arrays, offs):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            hp[at:at + a.size] = a.ravel()
+        dev = self._pinned.to(device, non_blocking=True)
+        views = [dev[at:at + np.asarray(a).size].view(np.asarray(a).shape) for a, at in zip(host_arrays, offs)]
+        self.d_k, self.d_ts, self.d_y0, self.d_y0d, self.d_sw, self.d_tout, self.d_toutd = views[:7]
+        self._keep = views[7:]  # the tangents' tables, in the order of the DiscoebTangent fields below
         tstructs = []
+        tables = iter(self._keep)
         for d in tans:
             t = _abi.DiscoebTangent()
             for f, v in d["scalars"].items():
                 setattr(t, f, v)
-            for short, (yy, SS) in d["tables"].items():
-                ty = torch.from_numpy(yy).to(device)
-                tS = torch.from_numpy(SS).to(device)
-                self._keep += [ty, tS]
-                setattr(t, short + "_y", ty.data_ptr())
-                setattr(t, short + "_S", tS.data_ptr())
+            for short in d["tables"]:
+                setattr(t, short + "_y", next(tables).data_ptr())
+                setattr(t, short + "_S", next(tables).data_ptr())
             tstructs.append(t)
         tan_arr = (_abi.DiscoebTangent * len(tstructs))(*tstructs)
         self.d_tan = torch.frombuffer(bytearray(bytes(tan_arr)), dtype=torch.uint8).to(device)
-        self.d_k = torch.tensor(kmodes[order], **f64)
-        self.d_ts = torch.tensor(tau_start[order], **f64)
-        self.d_y0 = torch.tensor(y0[order], **f64).contiguous()
-        self.d_y0d = torch.tensor(np.stack([d["y0"][order] for d in tans]), **f64).contiguous()
-        self.d_sw = torch.tensor(sw[order], **f64).contiguous()
-        self.d_tout = torch.tensor(tau_out, **f64)
-        self.d_toutd = torch.tensor(np.stack([d["tau_out"] for d in tans]), **f64).contiguous()
         self.full_state = bool(full_state)
         width = self.n if self.full_state else 20
         self.d_out = torch.empty((K, nout, width), **f64)
