@@ -38,6 +38,107 @@ constexpr double kPad = 2.0;     // padding of the log-chi range (cmb.py:738)
 // ------------------------------------------------------------------------------------------
 // sources
 
+// Scalar parameters the source assembly reads: plain values, or values with their derivative
+// along one parameter direction (DiscoebTangent) for the forward-mode sources.
+template <class T> struct SrcPar {
+    T grhom, Omegam, Omegab, OmegaDE, amnu, w0, wa;
+};
+
+// The source terms and their intermediates at one (mode, output time) from the state y, its
+// time derivative yp and the background row bt[DISCOEB_BG_NFIELDS] (cmb.py:17-633), in the number
+// type T: double for the sources, Dual for their derivative along a direction.  Y(i), YP(i) give
+// the state and its derivative as T; out[DISCOEB_SRC_NFIELDS] (S and S1 are left to isw_kernel).
+template <class T, class FY, class FYP>
+__device__ void assemble_sources(const DiscoebCosmo& P, const SrcPar<T>& sp, const Dims& D, double k, const T* bt,
+                                 FY Y, FYP YP, T* out)
+{
+    const int n = D.n;
+    const T a = bt[DISCOEB_BG_A], aH = bt[DISCOEB_BG_APRIMEOA];
+    const T rhonu = bt[DISCOEB_BG_RHONU], rho_Q = bt[DISCOEB_BG_RHO_Q];
+    const T w_Q = bt[DISCOEB_BG_W_Q];
+    const T opac = bt[DISCOEB_BG_OPAC], opacprime = bt[DISCOEB_BG_OPACPRIME];
+    const T gvis = bt[DISCOEB_BG_GVIS], gvisprime = bt[DISCOEB_BG_GVISPRIME];
+    const T gvispprime = bt[DISCOEB_BG_GVISPPRIME];
+    // massive neutrinos (nu_perturb, nu_perturb_prime: perturbations.py:29-85; the derivative
+    // of the speed is written as the reference writes it)
+    T drhonu = 0.0, dpnu = 0.0, fnu = 0.0, shearnu = 0.0, rnp = 0.0, snp = 0.0;
+    const int nq = D.nq, i0 = D.iq0, i1 = i0 + nq, i2 = i1 + nq;
+    for (int q = 0; q < nq; ++q) {
+        const T aq = a * sp.amnu / P.q[q];
+        const T v = 1.0 / xsqrt(1.0 + aq * aq);
+        const T vp = -0.5 * aq * aH * v * v * v;
+        const double w = P.wq[q];
+        drhonu += w * Y(i0 + q) / v;
+        dpnu += w * Y(i0 + q) * v;
+        fnu += w * Y(i1 + q);
+        shearnu += w * Y(i2 + q) * v;
+        rnp += w * (YP(i0 + q) / v - Y(i0 + q) / (v * v) * vp);
+        snp += w * (YP(i2 + q) * v + Y(i2 + q) * vp);
+    }
+    dpnu = dpnu / 3.0;
+    shearnu = shearnu * (2.0 / 3.0);
+    snp = snp * (2.0 / 3.0);
+    // metric (cmb.py:241-338)
+    const int ig = 7, igp = D.idxgp, ir = D.idxr;
+    const T eta = Y(2), deltac = Y(3), thetac = Y(4), deltab = Y(5), thetab = Y(6);
+    const T deltag = Y(ig), thetag = Y(ig + 1), shearg = 0.5 * Y(ig + 2);
+    const T deltar = Y(ir), thetar = Y(ir + 1), shearr = 0.5 * Y(ir + 2);
+    const T deltaq = Y(n - 2), thetaq = Y(n - 1);
+    const T thetabprime = YP(6), thetagprime = YP(ig + 1), sheargprime = 0.5 * YP(ig + 2);
+    const T shearrprime = 0.5 * YP(ir + 2);
+    const T a2 = a * a;
+    const double k2 = k * k;
+    const T Omegac = sp.Omegam - sp.Omegab;
+    const T rpt = (1.0 + w_Q) * rho_Q * sp.grhom * sp.OmegaDE * thetaq * a2;
+    const T grhoprime =
+        (-sp.grhom * sp.Omegam / a - 2.0 * (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / a2 +
+         sp.grhom * sp.OmegaDE * (-3.0 * (1.0 + sp.w0 + (1.0 - a) * sp.wa) * rho_Q * a2 + 2.0 * rho_Q * a2)) * aH +
+        P.grhor * P.Nmnu * rnp / a2;
+    const T aHprime = grhoprime / (6.0 * aH);
+    const T dgrho = sp.grhom * (Omegac * deltac + sp.Omegab * deltab) / a +
+                    (P.grhog * deltag + P.grhor * (P.Neff * deltar + P.Nmnu * drhonu)) / a2 +
+                    sp.grhom * sp.OmegaDE * deltaq * rho_Q * a2;
+    const T dgtheta = sp.grhom * (Omegac * thetac + sp.Omegab * thetab) / a +
+                      4.0 / 3.0 * (P.grhog * thetag + P.Neff * P.grhor * thetar) / a2 +
+                      P.Nmnu * P.grhor * k * fnu / a2 + rpt;
+    const T dgshear = 4.0 / 3.0 * (P.grhog * shearg + P.Neff * P.grhor * shearr) / a2 +
+                      P.Nmnu * P.grhor * shearnu / a2;
+    const T dgshearprime = 4.0 / 3.0 * (P.grhog * sheargprime + P.Neff * P.grhor * shearrprime) / a2 +
+                           P.Nmnu * P.grhor * snp / a2 - 2.0 * aH * dgshear;
+    const T hprime = (2.0 * k2 * eta + dgrho) / aH;
+    const T etaprime = 0.5 * dgtheta / k2;
+    const T alpha = (hprime + 6.0 * etaprime) / 2.0 / k2;
+    const T alphaprime = -3.0 * dgshear / (2.0 * k2) + eta - 2.0 * aH * alpha;
+    const T alphapprime = -3.0 * dgshearprime / (2.0 * k2) + etaprime - 2.0 * (aHprime * alpha + aH * alphaprime);
+    // polarisation (cmb.py:341-389)
+    const T couplprime = 8.0 * (thetagprime + k2 * alphaprime) / 15.0 -
+                         k * 0.6 * (YP(ig + 3) + YP(igp + 1) + YP(igp + 3));
+    const T pol = Y(ig + 2) + Y(igp) + Y(igp + 2);
+    const T polp = YP(ig + 2) + YP(igp) + YP(igp + 2);
+    const T polpp = couplprime - 0.3 * (opacprime * pol + opac * polp);
+    // sources (cmb.py:456-582); S1 needs d/dtau along the mode, see isw_kernel
+    out[DISCOEB_SRC_S2] = gvis * (0.25 * deltag + 2.0 * alphaprime + pol / 16.0 + (thetabprime + 3.0 / 16.0 * polpp) / k2);
+    out[DISCOEB_SRC_S3] = gvisprime * (alpha + (thetab + 3.0 / 8.0 * polp) / k2);
+    out[DISCOEB_SRC_S4] = gvispprime * 3.0 / 16.0 * pol / k2;
+    out[DISCOEB_SRC_POTENTIAL] = eta + alphaprime;
+    out[DISCOEB_SRC_ALPHA] = alpha;
+    out[DISCOEB_SRC_ALPHAPRIME] = alphaprime;
+    out[DISCOEB_SRC_ALPHAPPRIME] = alphapprime;
+    out[DISCOEB_SRC_HPRIME] = hprime;
+    out[DISCOEB_SRC_ETAPRIME] = etaprime;
+    out[DISCOEB_SRC_APRIMEOAPRIME] = aHprime;
+    out[DISCOEB_SRC_POL] = pol;
+    out[DISCOEB_SRC_POLPRIME] = polp;
+    out[DISCOEB_SRC_POLPPRIME] = polpp;
+    out[DISCOEB_SRC_DRHONU] = drhonu;
+    out[DISCOEB_SRC_DPNU] = dpnu;
+    out[DISCOEB_SRC_FNU] = fnu;
+    out[DISCOEB_SRC_SHEARNU] = shearnu;
+    out[DISCOEB_SRC_RHONUPRIME] = rnp;
+    out[DISCOEB_SRC_SHEARNUPRIME] = snp;
+    out[DISCOEB_SRC_THETABPRIME] = thetabprime;
+}
+
 __global__ void __launch_bounds__(128) sources_kernel(const DiscoebCosmo* __restrict__ cosmo, int n_modes,
                                                       const double* __restrict__ kmodes, int n_tau,
                                                       const double* __restrict__ tau, const double* __restrict__ bt,
@@ -61,94 +162,13 @@ __global__ void __launch_bounds__(128) sources_kernel(const DiscoebCosmo* __rest
     rhs_team(tm, P, D, b, k, t, y, yp, (double*)nullptr);
     tm.sync();
     if (!tm.leader()) return;
-
-    const double a = bt[DISCOEB_BG_A * n_tau + j], aH = bt[DISCOEB_BG_APRIMEOA * n_tau + j];
-    const double rhonu = bt[DISCOEB_BG_RHONU * n_tau + j], rho_Q = bt[DISCOEB_BG_RHO_Q * n_tau + j];
-    const double w_Q = bt[DISCOEB_BG_W_Q * n_tau + j];
-    const double opac = bt[DISCOEB_BG_OPAC * n_tau + j], opacprime = bt[DISCOEB_BG_OPACPRIME * n_tau + j];
-    const double gvis = bt[DISCOEB_BG_GVIS * n_tau + j], gvisprime = bt[DISCOEB_BG_GVISPRIME * n_tau + j];
-    const double gvispprime = bt[DISCOEB_BG_GVISPPRIME * n_tau + j];
-    // massive neutrinos (nu_perturb, nu_perturb_prime: perturbations.py:29-85; the derivative
-    // of the speed is written as the reference writes it)
-    double drhonu = 0.0, dpnu = 0.0, fnu = 0.0, shearnu = 0.0, rnp = 0.0, snp = 0.0;
-    const int nq = D.nq, i0 = D.iq0, i1 = i0 + nq, i2 = i1 + nq;
-    for (int q = 0; q < nq; ++q) {
-        const double aq = a * P.amnu / P.q[q];
-        const double v = 1.0 / sqrt(1.0 + aq * aq);
-        const double vp = -0.5 * aq * aH * v * v * v;
-        const double w = P.wq[q];
-        drhonu += w * y[i0 + q] / v;
-        dpnu += w * y[i0 + q] * v;
-        fnu += w * y[i1 + q];
-        shearnu += w * y[i2 + q] * v;
-        rnp += w * (yp[i0 + q] / v - y[i0 + q] / (v * v) * vp);
-        snp += w * (yp[i2 + q] * v + y[i2 + q] * vp);
-    }
-    dpnu /= 3.0;
-    shearnu *= 2.0 / 3.0;
-    snp *= 2.0 / 3.0;
-    // metric (cmb.py:241-338)
-    const int ig = 7, igp = D.idxgp, ir = D.idxr;
-    const double eta = y[2], deltac = y[3], thetac = y[4], deltab = y[5], thetab = y[6];
-    const double deltag = y[ig], thetag = y[ig + 1], shearg = 0.5 * y[ig + 2];
-    const double deltar = y[ir], thetar = y[ir + 1], shearr = 0.5 * y[ir + 2];
-    const double deltaq = y[n - 2], thetaq = y[n - 1];
-    const double thetabprime = yp[6], thetagprime = yp[ig + 1], sheargprime = 0.5 * yp[ig + 2];
-    const double shearrprime = 0.5 * yp[ir + 2];
-    const double a2 = a * a, k2 = k * k;
-    const double Omegac = P.Omegam - P.Omegab;
-    const double rpt = (1.0 + w_Q) * rho_Q * P.grhom * P.OmegaDE * thetaq * a2;
-    const double grhoprime =
-        (-P.grhom * P.Omegam / a - 2.0 * (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / a2 +
-         P.grhom * P.OmegaDE * (-3.0 * (1.0 + P.w0 + (1.0 - a) * P.wa) * rho_Q * a2 + 2.0 * rho_Q * a2)) * aH +
-        P.grhor * P.Nmnu * rnp / a2;
-    const double aHprime = grhoprime / (6.0 * aH);
-    const double dgrho = P.grhom * (Omegac * deltac + P.Omegab * deltab) / a +
-                         (P.grhog * deltag + P.grhor * (P.Neff * deltar + P.Nmnu * drhonu)) / a2 +
-                         P.grhom * P.OmegaDE * deltaq * rho_Q * a2;
-    const double dgtheta = P.grhom * (Omegac * thetac + P.Omegab * thetab) / a +
-                           4.0 / 3.0 * (P.grhog * thetag + P.Neff * P.grhor * thetar) / a2 +
-                           P.Nmnu * P.grhor * k * fnu / a2 + rpt;
-    const double dgshear = 4.0 / 3.0 * (P.grhog * shearg + P.Neff * P.grhor * shearr) / a2 +
-                           P.Nmnu * P.grhor * shearnu / a2;
-    const double dgshearprime = 4.0 / 3.0 * (P.grhog * sheargprime + P.Neff * P.grhor * shearrprime) / a2 +
-                                P.Nmnu * P.grhor * snp / a2 - 2.0 * aH * dgshear;
-    const double hprime = (2.0 * k2 * eta + dgrho) / aH;
-    const double etaprime = 0.5 * dgtheta / k2;
-    const double alpha = (hprime + 6.0 * etaprime) / 2.0 / k2;
-    const double alphaprime = -3.0 * dgshear / (2.0 * k2) + eta - 2.0 * aH * alpha;
-    const double alphapprime = -3.0 * dgshearprime / (2.0 * k2) + etaprime - 2.0 * (aHprime * alpha + aH * alphaprime);
-    // polarisation (cmb.py:341-389)
-    const double couplprime = 8.0 * (thetagprime + k2 * alphaprime) / 15.0 -
-                              k * 0.6 * (yp[ig + 3] + yp[igp + 1] + yp[igp + 3]);
-    const double pol = y[ig + 2] + y[igp] + y[igp + 2];
-    const double polp = yp[ig + 2] + yp[igp] + yp[igp + 2];
-    const double polpp = couplprime - 0.3 * (opacprime * pol + opac * polp);
-    // sources (cmb.py:456-582); S1 needs d/dtau along the mode, see isw_kernel
-    const double S2 = gvis * (0.25 * deltag + 2.0 * alphaprime + pol / 16.0 + (thetabprime + 3.0 / 16.0 * polpp) / k2);
-    const double S3 = gvisprime * (alpha + (thetab + 3.0 / 8.0 * polp) / k2);
-    const double S4 = gvispprime * 3.0 / 16.0 * pol / k2;
+    double btj[DISCOEB_BG_NFIELDS];
+    for (int f = 0; f < DISCOEB_BG_NFIELDS; ++f) btj[f] = bt[f * n_tau + j];
+    const SrcPar<double> sp{P.grhom, P.Omegam, P.Omegab, P.OmegaDE, P.amnu, P.w0, P.wa};
+    double out[DISCOEB_SRC_NFIELDS];
+    assemble_sources(P, sp, D, k, btj, [&](int i) { return y[i]; }, [&](int i) { return yp[i]; }, out);
     const size_t stride = (size_t)n_points, o = (size_t)warp;
-    fields[DISCOEB_SRC_S2 * stride + o] = S2;
-    fields[DISCOEB_SRC_S3 * stride + o] = S3;
-    fields[DISCOEB_SRC_S4 * stride + o] = S4;
-    fields[DISCOEB_SRC_POTENTIAL * stride + o] = eta + alphaprime;
-    fields[DISCOEB_SRC_ALPHA * stride + o] = alpha;
-    fields[DISCOEB_SRC_ALPHAPRIME * stride + o] = alphaprime;
-    fields[DISCOEB_SRC_ALPHAPPRIME * stride + o] = alphapprime;
-    fields[DISCOEB_SRC_HPRIME * stride + o] = hprime;
-    fields[DISCOEB_SRC_ETAPRIME * stride + o] = etaprime;
-    fields[DISCOEB_SRC_APRIMEOAPRIME * stride + o] = aHprime;
-    fields[DISCOEB_SRC_POL * stride + o] = pol;
-    fields[DISCOEB_SRC_POLPRIME * stride + o] = polp;
-    fields[DISCOEB_SRC_POLPPRIME * stride + o] = polpp;
-    fields[DISCOEB_SRC_DRHONU * stride + o] = drhonu;
-    fields[DISCOEB_SRC_DPNU * stride + o] = dpnu;
-    fields[DISCOEB_SRC_FNU * stride + o] = fnu;
-    fields[DISCOEB_SRC_SHEARNU * stride + o] = shearnu;
-    fields[DISCOEB_SRC_RHONUPRIME * stride + o] = rnp;
-    fields[DISCOEB_SRC_SHEARNUPRIME * stride + o] = snp;
-    fields[DISCOEB_SRC_THETABPRIME * stride + o] = thetabprime;
+    for (int f = DISCOEB_SRC_S2; f < DISCOEB_SRC_NFIELDS; ++f) fields[f * stride + o] = out[f];
 }
 
 // Natural cubic spline second derivatives through (x[i], y[i*ys]) for i < n (the Thomas
@@ -603,6 +623,105 @@ __global__ void __launch_bounds__(256) cell_dot_kernel(int n_ell, long long pitc
 }
 
 // ------------------------------------------------------------------------------------------
+// forward-mode sources: the derivative of S along one parameter direction from the states' and
+// output times' derivatives, the tables' (DiscoebTangent) and the background rows' derivatives
+
+// one warp per (direction, mode, output time): y' and its derivative (the e-part of f at
+// y + e y_dot under the dual background, plus d f / d tau at fixed y times tau_dot), then the
+// assembly in dual numbers; writes the derivatives of S2, S3, S4 and the potential eta + alpha'
+__global__ void __launch_bounds__(128) sources_dot_kernel(
+    const DiscoebCosmo* __restrict__ cosmo, const DiscoebTangent* __restrict__ tangents, int n_dir, int n_modes,
+    const double* __restrict__ kmodes, int n_tau, const double* __restrict__ tau, const double* __restrict__ tau_dot,
+    const double* __restrict__ bt, const double* __restrict__ bt_dot, const double* __restrict__ y_full,
+    const double* __restrict__ y_full_dot, double* fd4)
+{
+    extern __shared__ double smem[];
+    const int wib = threadIdx.x >> 5;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long n_points = (long long)n_modes * n_tau;
+    if (warp >= n_points * n_dir) return;
+    const WarpTeam tm{(int)(threadIdx.x & 31)};
+    const DiscoebCosmo& P = *cosmo;
+    const Dims D = make_dims(P);
+    const int n = D.n;
+    const int d = (int)(warp / n_points);
+    const long long pt = warp - (long long)d * n_points;
+    const int im = (int)(pt / n_tau), j = (int)(pt - (long long)im * n_tau);
+    const DiscoebTangent* TN = tangents + d;
+    const double k = kmodes[im], t = tau[j], tdot = tau_dot[(size_t)d * n_tau + j];
+    const double* y = y_full + (size_t)pt * n;
+    const double* yd = y_full_dot + ((size_t)d * n_points + pt) * n;
+    double* yp = smem + (size_t)wib * 2 * n;
+    double* ypd = yp + n;
+    Bg<double> b;
+    bg_eval(P, y[0], t, k, -1, b);
+    rhs_team(tm, P, D, b, k, t, y, yp, (double*)nullptr);
+    int hint = P.xe_loga.n_knots / 2;
+    Bg<Dual> bd;
+    bg_eval_team(tm, P, Dual(y[0], yd[0]), t, k, -1, bd, hint, TN);
+    rhs_team(tm, P, D, bd, k, t, y, ypd, (double*)nullptr, yd, (const double*)nullptr, 1, 1);
+    tm.sync();
+    for (int i = tm.lane; i < n; i += 32) ypd[i] += dtau_row(D, b, t, i, y) * tdot;
+    tm.sync();
+    if (!tm.leader()) return;
+    Dual btj[DISCOEB_BG_NFIELDS];
+    for (int f = 0; f < DISCOEB_BG_NFIELDS; ++f)
+        btj[f] = Dual(bt[f * n_tau + j], bt_dot[((size_t)d * DISCOEB_BG_NFIELDS + f) * n_tau + j]);
+    const SrcPar<Dual> sp{Dual(P.grhom, TN->grhom), Dual(P.Omegam, TN->Omegam), Dual(P.Omegab, TN->Omegab),
+                          Dual(P.OmegaDE, TN->OmegaDE), Dual(P.amnu, TN->amnu), Dual(P.w0, TN->w0),
+                          Dual(P.wa, TN->wa)};
+    Dual out[DISCOEB_SRC_NFIELDS];
+    assemble_sources(P, sp, D, k, btj, [&](int i) { return Dual(y[i], yd[i]); },
+                     [&](int i) { return Dual(yp[i], ypd[i]); }, out);
+    const size_t stride = (size_t)n_dir * n_points, o = (size_t)d * n_points + pt;
+    fd4[0 * stride + o] = out[DISCOEB_SRC_S2].d;
+    fd4[1 * stride + o] = out[DISCOEB_SRC_S3].d;
+    fd4[2 * stride + o] = out[DISCOEB_SRC_S4].d;
+    fd4[3 * stride + o] = out[DISCOEB_SRC_POTENTIAL].d;
+}
+
+__device__ Dual spline_slope_dual(Dual x0, Dual x1, Dual y0, Dual y1, Dual S0, Dual S1, Dual xn)
+{
+    const Dual h = x1 - x0, dx = xn - x0;
+    const Dual b = (y1 - y0) / h - h * (S1 + 2.0 * S0) / 6.0, c = S0 / 2.0, dd = (S1 - S0) / (6.0 * h);
+    return b + 2.0 * c * dx + 3.0 * dd * dx * dx;
+}
+
+// isw_kernel in dual numbers, one thread per (direction, mode): the spline of the potential along
+// tau with moving knots, its slope at the knots, times exp(-optical depth); S_dot = S1' + S2' +
+// S3' + S4'.  pot: the base point's potential rows [n_modes, n_tau]; scratch 4 n_dir n_modes n_tau
+__global__ void isw_dot_kernel(int n_dir, int n_modes, int n_tau, const double* __restrict__ tau,
+                               const double* __restrict__ tau_dot, const double* __restrict__ bt,
+                               const double* __restrict__ bt_dot, const double* __restrict__ pot,
+                               const double* __restrict__ fd4, double* scratch, double* S_dot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_dir * n_modes) return;
+    const int d = t / n_modes, im = t - d * n_modes;
+    const size_t np = (size_t)n_modes * n_tau, stride = (size_t)n_dir * np;
+    const size_t row = (size_t)im * n_tau, drow = (size_t)d * np + row;
+    const double* pv = pot + row;
+    const double* pd = fd4 + 3 * stride + drow;
+    const double* td = tau_dot + (size_t)d * n_tau;
+    double* Sv = scratch + drow;
+    double* Sd = scratch + stride + drow;
+    double* cpv = scratch + 2 * stride + drow;
+    double* cpd = scratch + 3 * stride + drow;
+    spline_second_dual(n_tau, tau, td, pv, pd, 1, Sv, Sd, cpv, cpd);
+    for (int j = 0; j < n_tau; ++j) {
+        const int i = spline_interval(tau, 1, n_tau, tau[j]);
+        const Dual slope = spline_slope_dual(Dual(tau[i], td[i]), Dual(tau[i + 1], td[i + 1]), Dual(pv[i], pd[i]),
+                                             Dual(pv[i + 1], pd[i + 1]), Dual(Sv[i], Sd[i]),
+                                             Dual(Sv[i + 1], Sd[i + 1]), Dual(tau[j], td[j]));
+        const Dual od(bt[DISCOEB_BG_OPTICAL_DEPTH * n_tau + j],
+                      bt_dot[((size_t)d * DISCOEB_BG_NFIELDS + DISCOEB_BG_OPTICAL_DEPTH) * n_tau + j]);
+        const Dual s1 = xexp(-od) * slope;
+        const size_t o = drow + j;
+        S_dot[o] = s1.d + fd4[o] + fd4[stride + o] + fd4[2 * stride + o];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // workspace layout of discoeb_los (byte offsets, 256-byte aligned)
 
 struct LosLayout {
@@ -972,6 +1091,33 @@ int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_ta
         if (!omega_t_times(D(J.Fd), D(J.H))) return DISCOEB_ECUDA;
         cell_dot_kernel<<<n_ell, 256, 0, s>>>(n_ell, pitch, D(L.B), D(J.H), D(J.Bd), D(J.G), cell_dot + (size_t)d * n_ell);
     }
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int32_t discoeb_sources_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host,
+                            const DiscoebTangent* tangents_dev, int32_t n_dir, int32_t n_modes, const double* kmodes,
+                            int32_t n_tau, const double* tau, const double* tau_dot, const double* bgtab,
+                            const double* bgtab_dot, const double* y_full, const double* y_full_dot,
+                            const double* fields, double* S_dot, double* scratch, void* stream)
+{
+    if (!cosmo_host || !cosmo_dev || !tangents_dev || n_dir < 1 || n_modes < 0 || n_tau < 0) return DISCOEB_EINVAL;
+    if (cosmo_host->use_tca) return DISCOEB_EUNSUPPORTED;
+    if (n_modes == 0 || n_tau == 0) return DISCOEB_SUCCESS;
+    if (n_tau < 3 || !kmodes || !tau || !tau_dot || !bgtab || !bgtab_dot || !y_full || !y_full_dot || !fields ||
+        !S_dot || !scratch)
+        return DISCOEB_EINVAL;
+    const Dims D = make_dims(*cosmo_host);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const long long points = (long long)n_dir * n_modes * n_tau;
+    const int threads = 128;
+    const size_t smem = sizeof(double) * 2 * (size_t)D.n * (threads / 32);
+    double* fd4 = scratch;                       // [4, n_dir, n_modes, n_tau]
+    double* sp = scratch + 4 * (size_t)points;  // [4, n_dir, n_modes, n_tau]
+    sources_dot_kernel<<<blocks_for(points * 32, threads), threads, smem, s>>>(
+        cosmo_dev, tangents_dev, n_dir, n_modes, kmodes, n_tau, tau, tau_dot, bgtab, bgtab_dot, y_full, y_full_dot, fd4);
+    const size_t stride = (size_t)n_modes * n_tau;
+    isw_dot_kernel<<<blocks_for((long long)n_dir * n_modes, 64), 64, 0, s>>>(
+        n_dir, n_modes, n_tau, tau, tau_dot, bgtab, bgtab_dot, fields + DISCOEB_SRC_POTENTIAL * stride, fd4, sp, S_dot);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 

@@ -245,7 +245,7 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
 def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0, n_k_dense=8192, n_fftlog=16384,
                           lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3, num_thermo=1024, rtol=1e-4, atol=1e-4,
                           max_steps=2048, k_sampling_method="camb", aexp_out=None, de_guard_eps=1e-9, device=None,
-                          rel_step=1e-4, los="tangent"):
+                          rel_step=1e-4, los="tangent", sources="tangent"):
     """C_l^TT and dC_l/dtheta for theta = (omega_c, omega_b, h, n_s, ln10As, w0, wa, m_nu)
     (``gradients.THETA_NAMES``), what ``jax.jacfwd`` of the reference's
     compute_Cell_spectrum_from_cosmo_params (cmb.py:931-1090) gives.
@@ -254,9 +254,11 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     Recfast steps held), the perturbation states at every output time and their tangents from one
     discoeb_jvp_full launch (forward mode, accepted steps held).  The stages after the solve
     (sources, line of sight, C_l) involve no adaptive choice.  The sources' tangent along each
-    direction is a central difference with states, output times, background tables and scalars
-    moved by +-h times their exact tangents, h = ``rel_step`` max(|theta_d|, 0.01) (the sources are
-    smooth in them: O(h^2)).  The line of sight and C_l then take that tangent with the output
+    direction: ``sources="tangent"`` in forward mode (discoeb_sources_jvp: y' and the source
+    assembly in dual numbers from the state, output-time and table tangents; only the 1-D
+    background rows, host tables, are differenced, centrally with the background moved by +-h
+    along its exact tangent, h = ``rel_step`` max(|theta_d|, 0.01)), ``sources="differences"`` by a
+    central difference of the whole source stage along the same tangents (O(h^2)).  The line of sight and C_l then take that tangent with the output
     times' and tau0's: ``los="tangent"`` in forward mode (discoeb_los_cell_jvp: the resampling, the
     FFT coefficients and the table M_l(p) differentiated as the FFTLog grid moves with tau0, one
     GEMM per direction), ``los="differences"`` by a fourth-order central difference along the
@@ -274,6 +276,8 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     from .gradients import ODE_DIRECTIONS, THETA_NAMES, JacobianProblem, param_dots, theta_to_params
     if los not in ("tangent", "differences"):
         raise ValueError(f"los must be 'tangent' or 'differences', not {los!r}")
+    if sources not in ("tangent", "differences"):
+        raise ValueError(f"sources must be 'tangent' or 'differences', not {sources!r}")
     torch, device = _device(device)
     L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
     aexp_out = cmb_aexp_out() if aexp_out is None else np.asarray(aexp_out, dtype=np.float64)
@@ -288,7 +292,7 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     prob.launch()
     y = prob.state()
 
-    def sources(param, states):
+    def source_S(param, states):
         return compute_sources(param=param, yout=states, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
                                device=device, **L)["S"]
 
@@ -300,8 +304,19 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
                                    device=device)
         return th, kk, compute_Cell(th, kk, bg["n_s"], bg["k_p"], device=device).cpu().numpy()
 
-    S0 = sources(bg, y)
+    fields0 = compute_sources(param=bg, yout=y, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
+                              device=device, **L)
+    S0 = fields0["S"]
     tau_b, tau0_b = times(bg)
+    if sources == "tangent":
+        lib = _abi.lib()
+        f64 = dict(dtype=torch.float64, device=device)
+        K, T = S0.shape
+        d_k = torch.from_numpy(np.ascontiguousarray(kmodes)).to(device)
+        d_tau = torch.from_numpy(np.ascontiguousarray(tau_b)).to(device)
+        d_bt = torch.from_numpy(background_table(aexp_out, tau_b, bg)).to(device)
+        scratch = torch.empty(8 * K * T, **f64)
+        tan_size = ctypes.sizeof(_abi.DiscoebTangent)
     if los == "differences":
         th, kk, cell = los_cell(S0, tau_b, tau0_b)
     J = np.zeros((len(THETA_NAMES), ellmax + 1))
@@ -318,12 +333,28 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
             for f in _DIFF_FIELDS:
                 ps[f] = p[f] + sgn * h * pdots[di][f]
             bgs = background_from_buffer(ps, buf + sgn * h * bdots[di], num_thermo)
-            side.append((sources(bgs, torch.add(y, ydot, alpha=sgn * h)), *times(bgs)))
-        del ydot
-        S_dot = (side[0][0] - side[1][0]) / (2 * h)
+            tau_s, tau0_s = times(bgs)
+            if sources == "tangent":  # the background rows of the sources, differenced on the host
+                side.append((background_table(aexp_out, tau_s, bgs), tau_s, tau0_s))
+            else:
+                side.append((source_S(bgs, torch.add(y, ydot, alpha=sgn * h)), tau_s, tau0_s))
         tau_dot = (side[0][1] - side[1][1]) / (2 * h)
         tau0_dot = (side[0][2] - side[1][2]) / (2 * h)
-        del side
+        if sources == "tangent":
+            bt_dot = torch.from_numpy(np.ascontiguousarray((side[0][0] - side[1][0]) / (2 * h))).to(device)
+            S_dot = torch.empty((K, T), **f64)
+            d_tau_dot = torch.from_numpy(np.ascontiguousarray(tau_dot)).to(device)
+            rc = lib.discoeb_sources_jvp(prob.dc.struct.data_ptr(), ctypes.byref(prob.dc.host),
+                                         prob.d_tan.data_ptr() + di * tan_size, 1, K, d_k.data_ptr(), T,
+                                         d_tau.data_ptr(), d_tau_dot.data_ptr(),
+                                         d_bt.data_ptr(), bt_dot.data_ptr(), y.data_ptr(), ydot.data_ptr(),
+                                         S0.data_ptr(), S_dot.data_ptr(), scratch.data_ptr(),
+                                         torch.cuda.current_stream(device).cuda_stream)
+            if rc != 0:
+                raise RuntimeError(f"discoeb_sources_jvp failed with code {rc}")
+        else:
+            S_dot = (side[0][0] - side[1][0]) / (2 * h)
+        del ydot, side
         if los == "tangent":
             tangents.append((S_dot, tau_dot, tau0_dot))
             continue

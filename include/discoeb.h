@@ -237,6 +237,21 @@ int32_t discoeb_sources_noalloc(const DiscoebCosmo* cosmo_dev, const DiscoebCosm
                                 const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
                                 const double* y_full, double* fields, void* stream);
 
+/* Forward-mode sources: the derivative of S (fields row DISCOEB_SRC_S) along n_dir parameter
+ * directions, from the derivatives of the states at the (moving) output times, of the output
+ * times, of the background rows and of the tables and scalars (the C_l gradient's sources:
+ * jax.jacfwd through compute_source_function, cmb.py:17-633).
+ *   tangents_dev [n_dir]                   d(parameters, tables)/d(theta_d), as for discoeb_jvp
+ *   tau_dot [n_dir, n_tau], bgtab_dot [n_dir, DISCOEB_BG_NFIELDS, n_tau]
+ *   y_full_dot [n_dir, n_modes, n_tau, nvar]  (discoeb_jvp_full's state tangents)
+ *   fields: discoeb_sources' output at the base point (its potential row is read)
+ *   S_dot [n_dir, n_modes, n_tau] out; scratch: 8 n_dir n_modes n_tau doubles.  Device arrays. */
+int32_t discoeb_sources_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host,
+                            const DiscoebTangent* tangents_dev, int32_t n_dir, int32_t n_modes, const double* kmodes,
+                            int32_t n_tau, const double* tau, const double* tau_dot, const double* bgtab,
+                            const double* bgtab_dot, const double* y_full, const double* y_full_dot,
+                            const double* fields, double* S_dot, double* scratch, void* stream);
+
 /* Workspace bytes of discoeb_los for these sizes (< 0: invalid sizes or a cuFFT error). */
 int64_t discoeb_los_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
                                     int32_t n_k_dense);

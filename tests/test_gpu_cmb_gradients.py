@@ -158,3 +158,17 @@ def test_gpu_cell_autograd_function_contracts_the_jacobian(torch_cuda):
     C_ref, J, _ = compute_Cell_jacobian(THETA, **SMALL)
     np.testing.assert_array_equal(C.detach().cpu().numpy(), C_ref)
     np.testing.assert_allclose(theta.grad.cpu().numpy(), J @ weights.cpu().numpy(), rtol=1e-12)
+
+
+@pytest.mark.parametrize("size", [SMALL, DEFAULT], ids=["small", "reference_defaults"])
+def test_gpu_forward_mode_sources_equal_their_differences(torch_cuda, size):
+    """discoeb_sources_jvp (the sources' derivative in dual numbers) against the central difference
+    of the whole source stage along the same tangents (O(h^2) with h = 1e-4 of each parameter)."""
+    from discoeb_b200.cmb import compute_Cell_jacobian
+    C1, J1, _ = compute_Cell_jacobian(THETA, sources="tangent", **size)
+    C2, J2, _ = compute_Cell_jacobian(THETA, sources="differences", **size)
+    np.testing.assert_array_equal(C1, C2)
+    l = slice(2, None)
+    dev = [float(np.abs(J1[i][l] - J2[i][l]).max() / max(np.abs(J2[i][l]).max(), 1e-300)) for i in range(8)]
+    print("forward-mode vs differenced sources per direction:", dev)
+    assert max(dev) <= 1e-6, dev
