@@ -171,6 +171,18 @@ def test_cell_jacobian_rejects_an_unknown_line_of_sight_mode():
         compute_Cell_jacobian(theta, los="adjoint")
 
 
+def test_sources_tangent_entry_rejects_bad_arguments_before_any_launch():
+    lib = _abi.lib()
+    host = _abi.DiscoebCosmo()
+    host.lmaxg, host.lmaxgp, host.lmaxr, host.lmaxnu, host.nqmax = 11, 11, 11, 8, 3
+    fake = 4096  # never dereferenced: the argument checks return first
+    ok = [fake, ctypes.byref(host), fake, 1, 8, fake, 16, fake, fake, fake, fake, fake, fake, fake, fake, fake, None]
+    for i, v in ((3, 0), (4, -1), (6, 2), (14, None), (15, None), (0, None)):
+        args = list(ok)
+        args[i] = v
+        assert lib.discoeb_sources_jvp(*args) == -1, (i, v)
+
+
 def test_struct_layout_matches_header():
     # the ctypes mirror must have the C layout: compile a tiny probe of offsetof/sizeof
     import tempfile
