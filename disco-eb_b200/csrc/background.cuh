@@ -445,135 +445,143 @@ template <class T> BGF void nu_background(double a, const T& amnu, T& rho, T& p,
 }
 
 // ---------------------------------------------------------------------------------------------
-// Recfast (thermodynamics_recfast.py:124-281): d(x_H, x_He, T_mat)/da.  Y is the state's number
-// type (T, or Fw<T> for the Jacobian); parameters of type T are lifted to Y.
+// Recfast model (replaces thermodynamics_recfast.py:124-281): d(x_H, x_He, T_mat)/da, one
+// function per process, from Seager, Sasselov & Scott (1999, 2000) and Wong, Moss & Scott (2008).
+// Y is the state's number type (T, or Fw<T> for the Jacobian); parameters of type T are lifted
+// to Y.  Branches are taken on value parts.
 template <class T> struct RecCtx {
     const Bg<T>* g;
     RecConst k;
 };
 
+// What the rate equations share at scale factor a: 1 + z, hydrogen and helium number densities
+// [m^-3], radiation and matter temperatures [K], the Hubble rate [1/s] and the ionised fractions
+// (x_e = x_H + f_He x_He electrons per hydrogen nucleus).
+template <class Y> struct Plasma {
+    double zp1, Tr, fHe;
+    Y h, nH, nHe, Tm, Hs, xH, xHe, xe;
+};
+
+template <class Y, class T>
+BGF Plasma<Y> plasma_at(double a, const Y* y, const Params<T>& P, const T& aprime_t)
+{
+    Plasma<Y> s;
+    const double yhe = P.YHe;
+    s.h = lift<Y>(P.H0) / 100.0;
+    s.zp1 = 1.0 / a;
+    s.fHe = yhe / (const_mHe_mH * (1.0 - yhe));
+    // hydrogen nuclei per m^3: rho_b (1 - Y) / m_H, with rho_crit / m_H = const_dens_fac h^2
+    s.nH = const_dens_fac * s.h * s.h * lift<Y>(P.Omegab) * (1.0 - yhe) * pow(s.zp1, 3.0);
+    s.nHe = s.fHe * s.nH;
+    s.Tr = P.Tcmb * s.zp1;
+    s.Tm = re(y[2]) >= 0.0 ? y[2] : -y[2];
+    // conformal a'/a [1/Mpc] -> H(z) [1/s]
+    s.Hs = 1e-5 * lift<Y>(aprime_t) * s.zp1 * const_c * bigH;
+    s.xH = y[0];
+    s.xHe = y[1];
+    s.xe = s.xH + s.fHe * s.xHe;
+    return s;
+}
+
+// Sobolev escape probability (1 - e^-tau) / tau
+template <class Y> BGF Y rec_escape(const Y& tau) { return (1.0 - bexp(-tau)) / tau; }
+
+// Ratio of the rate at which H continuum absorption removes photons from a HeI line to the line's
+// decay rate (Kholupenko, Ivanchik & Varshalovich 2007), with the line's Doppler width at T_m.
+template <class Y>
+BGF Y he_line_broadening(const Plasma<Y>& s, const RecConst& K, double wavenumber, double einstein_a, double sigma_abs)
+{
+    const double c2 = const_c * const_c;
+    const Y vth = bsqrt(2.0 * const_kB * s.Tm / (const_mH * const_mHe_mH * c2));
+    const Y doppler = const_c * wavenumber * vth;
+    const double lc = const_c * wavenumber;
+    return (3.0 * einstein_a * s.fHe * (1.0 - s.xHe) * c2) /
+           (K.sqrt_pi * sigma_abs * 8.0 * kPi * doppler * (1.0 - s.xH) * (lc * lc));
+}
+
+// dx_H/dz: Peebles' effective three-level atom with the Recfast fudge F = 1.105 and the
+// two-Gaussian correction of the Lyman-alpha escape rate.  Zero while x_H > 0.99, the rate
+// without the Peebles factor for 0.985 < x_H <= 0.99.
+template <class Y> BGF Y rec_hydrogen(const Plasma<Y>& s, const RecConst& K)
+{
+    const Y t4 = s.Tm / 1e4;
+    // case-B recombination coefficient (Pequignot, Petitjean & Boisson 1991 fit) [m^3/s]
+    const Y alpha_B = 1e-19 * K.a_PPB * bpow(t4, K.b_PPB) / (1.0 + K.c_PPB * bpow(t4, K.d_PPB));
+    // photo-ionisation rate from n = 2, by detailed balance [1/s]
+    const Y beta_B = alpha_B * bpow(K.CR * s.Tm, 1.5) * bexp(-K.CDB / s.Tm);
+    const double lz = log(s.zp1);
+    const double g1 = (lz - zGauss1) / wGauss1, g2 = (lz - zGauss2) / wGauss2;
+    const double k_fix = 1.0 + AGauss1 * exp(-(g1 * g1)) + AGauss2 * exp(-(g2 * g2));
+    const Y K_alpha = K.CK / s.Hs * k_fix;  // Lyman-alpha redshifting factor lambda^3 / (8 pi H)
+    const Y n_1s = s.nH * (1.0 - s.xH);
+    const Y net = (s.xe * s.xH * s.nH * alpha_B - beta_B * (1.0 - s.xH) * bexp(-K.CL / s.Tm)) / (s.Hs * s.zp1);
+    if (re(s.xH) > 0.99) return 0.0 * s.xH;
+    if (re(s.xH) > 0.985) return net;
+    // Peebles factor, with the case-B coefficient divided by the fudge F
+    const Y decay = 1.0 + K_alpha * Lambda_ * n_1s;
+    return net * (decay / (decay / 1.105 + K_alpha * beta_B * n_1s));
+}
+
+// dx_He/dz through the HeI singlet 2^1P -> 1^1S channel: Verner & Ferland (1996) recombination fit,
+// Sobolev escape plus H continuum absorption (p = 0.36, q = 0.86).
+template <class Y> BGF Y rec_helium_singlet(const Plasma<Y>& s, const RecConst& K)
+{
+    const Y r0 = bsqrt(s.Tm / K.T_0), r1 = bsqrt(s.Tm / K.T_1);
+    const Y alpha_He = K.a_VF / (r0 * bpow(1.0 + r0, 1.0 - K.b_VF) * bpow(1.0 + r1, 1.0 + K.b_VF));
+    const Y beta_He = 4.0 * alpha_He * bpow(K.CR * s.Tm, 1.5) * bexp(-K.CDB_He / s.Tm);
+    const Y n_HeI = s.nHe * (1.0 - s.xHe);
+    const Y K_line = K.CK_He / s.Hs;
+    const Y p_esc = rec_escape(A2P_s * K_line * 3.0 * n_HeI);
+    const Y a_cont = A2P_s / (1.0 + 0.36 * bpow(he_line_broadening(s, K, L_He_2p, A2P_s, sigma_He_2Ps), 0.86));
+    const bool ends = re(s.xHe) < 5e-9 || re(s.xHe) > 0.98;
+    const Y esc_rate = re(s.xH) < 0.9999999 ? A2P_s * p_esc + a_cont : A2P_s * p_esc;
+    const Y K_He = ends ? K_line : 1.0 / (esc_rate * 3.0 * n_HeI);
+    const Y bt = K.Bfact / s.Tm;
+    const Y boltz = bexp(re(bt) < 680.0 ? bt : Y(680.0));  // 2s-2p energy gap factor
+    const Y net = (s.xe * s.xHe * s.nH * alpha_He - beta_He * (1.0 - s.xHe) * bexp(-K.CL_He / s.Tm)) / (s.Hs * s.zp1);
+    const Y k_n = K_He * n_HeI * boltz;
+    return net * (1.0 + k_n * Lambda_He) / (1.0 + k_n * (Lambda_He + beta_He));
+}
+
+// dx_He/dz through the HeI triplet 2^3P -> 1^1S intercombination line (p = 0.66, q = 0.9); omitted
+// at the ends of helium recombination.
+template <class Y> BGF Y rec_helium_triplet(const Plasma<Y>& s, const RecConst& K)
+{
+    if (re(s.xHe) < 5e-9 || re(s.xHe) > 0.98) return 0.0 * s.xHe;
+    const Y r0 = bsqrt(s.Tm / K.T_0), r1 = bsqrt(s.Tm / K.T_1);
+    const Y alpha_t = K.a_trip / (r0 * bpow(1.0 + r0, 1.0 - K.b_trip) * bpow(1.0 + r1, 1.0 + K.b_trip));
+    const Y beta_t = (4.0 / 3.0) * alpha_t * bexp((-const_h * const_c * L_He2St_ion) / (const_kB * s.Tm)) *
+                     bpow(K.CR * s.Tm, 1.5);
+    const Y n_HeI = s.nHe * (1.0 - s.xHe);
+    const Y p_esc = rec_escape(A2P_t * n_HeI * 3.0 / (8.0 * kPi * s.Hs * pow(L_He_2Pt, 3.0)));
+    const Y a_cont = A2P_t / (1.0 + 0.66 * bpow(he_line_broadening(s, K, L_He_2Pt, A2P_t, sigma_He_2Pt), 0.9)) / 3.0;
+    const Y decay = (re(s.xH) > 0.99999 ? A2P_t * p_esc : A2P_t * p_esc + a_cont) * bexp(-K.CL_PSt / s.Tm);
+    const Y c_trip = decay / (beta_t + decay);  // chance that an atom in 2^3P reaches the ground state
+    const Y net = s.xe * s.xHe * s.nH * alpha_t - 3.0 * beta_t * (1.0 - s.xHe) * bexp(-K.hcL2St_kB / s.Tm);
+    return net * c_trip / (s.Hs * s.zp1);
+}
+
+// dT_m/dz: Compton coupling against adiabatic cooling; T_m follows T_rad while the Compton time
+// is below 1e-3 of the Hubble time.
+template <class Y> BGF Y rec_temperature(const Plasma<Y>& s, const RecConst& K)
+{
+    const Y heat = K.CT * pow(s.Tr, 4.0) * s.xe / (1.0 + s.xe + s.fHe);  // inverse Compton time [1/s]
+    const Y t_hubble = 2.0 / (3.0 * s.h * bigH * pow(s.zp1, 1.5));
+    if (re(1.0 / heat) < H_frac * re(t_hubble)) return s.Tm / s.zp1;
+    return heat * (s.Tm - s.Tr) / (s.Hs * s.zp1) + 2.0 * s.Tm / s.zp1;
+}
+
 template <class Y, class T>
 BGF void ionization(double a, const Y* y, const RecCtx<T>& c, const T& aprime_t, Y* f)
 {
-    const RecConst& K = c.k;
-    const Params<T>& P = c.g->p;
-    const double YHe = P.YHe;
-    const double z = 1.0 / a - 1.0;
-    const Y H = lift<Y>(P.H0) / 100.0;
-    const Y HO = H * bigH;
-    const double fu = 1.105;
-    const double mu_H = 1.0 / (1.0 - YHe);
-    const double fHe = YHe / (const_mHe_mH * (1.0 - YHe));
-    const Y Nnow = const_dens_fac * H * H * lift<Y>(P.Omegab) / mu_H;
-    const Y aprime = lift<Y>(aprime_t);
-
-    const Y x_H = y[0];
-    const Y x_He = y[1];
-    const Y x = x_H + fHe * x_He;
-    const Y Tmat = re(y[2]) >= 0.0 ? y[2] : -y[2];
-
-    const Y n = Nnow * pow(1.0 + z, 3.0);
-    const Y n_He = fHe * n;
-    const double Trad = P.Tcmb * (1.0 + z);
-    const double z_term = 1.0 + z;
-    const Y Hz = (1e-5 * aprime) / a * const_c * bigH;
-
-    const Y Tmat_1e4 = Tmat / 1e4;
-    const Y CR_Tmat_15 = bpow(K.CR * Tmat, 1.5);
-    const Y Rdown = 1e-19 * K.a_PPB * bpow(Tmat_1e4, K.b_PPB) / (1.0 + K.c_PPB * bpow(Tmat_1e4, K.d_PPB));
-    const Y Rup = Rdown * CR_Tmat_15 * bexp(-K.CDB / Tmat);
-
-    const Y sq_0 = bsqrt(Tmat / K.T_0);
-    const Y sq_1 = bsqrt(Tmat / K.T_1);
-    const Y sq_0_term = 1.0 + sq_0;
-    const Y sq_1_term = 1.0 + sq_1;
-    const Y Rdown_He = K.a_VF / (sq_0 * bpow(sq_0_term, 1.0 - K.b_VF) * bpow(sq_1_term, 1.0 + K.b_VF));
-    const Y Rup_He = 4.0 * Rdown_He * CR_Tmat_15 * bexp(-K.CDB_He / Tmat);
-
-    const Y bt = K.Bfact / Tmat;
-    const Y He_Boltz = bexp(re(bt) < 680.0 ? bt : Y(680.0));
-
-    const Y Rdown_trip = K.a_trip / (sq_0 * bpow(sq_0_term, 1.0 - K.b_trip) * bpow(sq_1_term, 1.0 + K.b_trip));
-    const Y Rup_trip = Rdown_trip * bexp((-const_h * const_c * L_He2St_ion) / (const_kB * Tmat)) * CR_Tmat_15 *
-                       (4.0 / 3.0);
-
-    const double lz = log(z_term);
-    const double g1 = (lz - zGauss1) / wGauss1, g2 = (lz - zGauss2) / wGauss2;
-    const double K_gaussian = 1.0 + AGauss1 * exp(-(g1 * g1)) + AGauss2 * exp(-(g2 * g2));
-    const Y Kc = K.CK / Hz * K_gaussian;
-
-    const Y one_minus_x_He = 1.0 - x_He;
-    const Y one_minus_x_H = 1.0 - x_H;
-    const Y n_He_1_minus_x_He = n_He * one_minus_x_He;
-
-    const Y tauHe_s = A2P_s * K.CK_He * 3.0 * n_He_1_minus_x_He / Hz;
-    const Y pHe_s = (1.0 - bexp(-tauHe_s)) / tauHe_s;
-
-    const double c2 = const_c * const_c;
-    const Y Doppler_term = bsqrt(2.0 * const_kB * Tmat / (const_mH * const_mHe_mH * c2));
-    const Y Doppler_2p = const_c * L_He_2p * Doppler_term;
-    const Y Doppler_2Pt = const_c * L_He_2Pt * Doppler_term;
-
-    const double cL2p = const_c * L_He_2p, cL2Pt = const_c * L_He_2Pt;
-    const Y gamma_2Ps_term = 3.0 * A2P_s * fHe * one_minus_x_He * c2;
-    const Y gamma_2Ps_denom = K.sqrt_pi * sigma_He_2Ps * 8.0 * kPi * Doppler_2p * one_minus_x_H * (cL2p * cL2p);
-    const Y gamma_2Ps = gamma_2Ps_term / gamma_2Ps_denom;
-    const double pb = 0.36, qb = 0.86;
-    const Y AHcon = A2P_s / (1.0 + pb * bpow(gamma_2Ps, qb));
-
-    const bool K_He_cond1 = (re(x_He) < 5e-9) || (re(x_He) > 0.98);
-    const bool K_He_cond2 = re(x_H) < 0.9999999;
-    const Y K_He = K_He_cond1 ? K.CK_He / Hz
-                              : (K_He_cond2 ? 1.0 / ((A2P_s * pHe_s + AHcon) * 3.0 * n_He_1_minus_x_He)
-                                            : 1.0 / (A2P_s * pHe_s * 3.0 * n_He_1_minus_x_He));
-
-    const Y tauHe_t = A2P_t * n_He_1_minus_x_He * 3.0 / (8.0 * kPi * Hz * pow(L_He_2Pt, 3.0));
-    const Y pHe_t = (1.0 - bexp(-tauHe_t)) / tauHe_t;
-    const Y gamma_2Pt_term = 3.0 * A2P_t * fHe * one_minus_x_He * c2;
-    const Y gamma_2Pt_denom = K.sqrt_pi * sigma_He_2Pt * 8.0 * kPi * Doppler_2Pt * one_minus_x_H * (cL2Pt * cL2Pt);
-    const Y gamma_2Pt = gamma_2Pt_term / gamma_2Pt_denom;
-    const double pb_t = 0.66, qb_t = 0.9;
-    const Y AHcon_t = A2P_t / (1.0 + pb_t * bpow(gamma_2Pt, qb_t)) / 3.0;
-
-    const Y exp_CL_PSt = bexp(-K.CL_PSt / Tmat);
-    Y CfHe_t = re(x_H) > 0.99999 ? A2P_t * pHe_t * exp_CL_PSt : (A2P_t * pHe_t + AHcon_t) * exp_CL_PSt;
-    CfHe_t = CfHe_t / (Rup_trip + CfHe_t);
-
-    const Y timeTh = (1.0 / (K.CT * pow(Trad, 4.0))) * (1.0 + x + fHe) / x;
-    const Y timeH = 2.0 / (3.0 * HO * pow(z_term, 1.5));
-
-    const Y Hz_z_term = Hz * z_term;
-    const Y x_x_H_n_Rdown = x * x_H * n * Rdown;
-    const Y Rup_1_minus_x_H_exp_CL = Rup * one_minus_x_H * bexp(-K.CL / Tmat);
-    const Y rate_diff = x_x_H_n_Rdown - Rup_1_minus_x_H_exp_CL;
-    const Y K_Lambda_n_1_minus_x_H = Kc * Lambda_ * n * one_minus_x_H;
-    const Y denom_term = 1.0 / fu + K_Lambda_n_1_minus_x_H / fu + Kc * Rup * n * one_minus_x_H;
-    Y f0;
-    if (re(x_H) > 0.99) f0 = 0.0 * x_H;
-    else if (re(x_H) > 0.985) f0 = rate_diff / Hz_z_term;
-    else f0 = (rate_diff * (1.0 + K_Lambda_n_1_minus_x_H)) / (Hz_z_term * denom_term);
-
-    const Y x_x_He_n_Rdown_He = x * x_He * n * Rdown_He;
-    const Y Rup_He_term = Rup_He * one_minus_x_He * bexp(-K.CL_He / Tmat);
-    const Y rate_diff_He = x_x_He_n_Rdown_He - Rup_He_term;
-    const Y K_He_LHe = K_He * Lambda_He * n_He_1_minus_x_He * He_Boltz;
-    const Y He_denom_term = 1.0 + K_He * (Lambda_He + Rup_He) * n_He_1_minus_x_He * He_Boltz;
-    const Y f1_main = (rate_diff_He * (1.0 + K_He_LHe)) / (Hz_z_term * He_denom_term);
-    const Y trip_rate_diff = x * x_He * n * Rdown_trip - one_minus_x_He * 3.0 * Rup_trip * bexp(-K.hcL2St_kB / Tmat);
-    const Y trip_contrib = trip_rate_diff * CfHe_t / Hz_z_term;
-    const bool trip_cond = (re(x_He) < 5e-9) || (re(x_He) > 0.98);
-    Y f1;
-    if (re(x_He) < 1e-8) f1 = 0.0 * x_He;
-    else f1 = f1_main + (trip_cond ? 0.0 * x_He : trip_contrib);
-
-    Y f2;
-    if (re(timeTh) < H_frac * re(timeH)) f2 = Tmat / z_term;
-    else f2 = K.CT * pow(Trad, 4.0) * x / (1.0 + x + fHe) * (Tmat - Trad) / Hz_z_term + 2.0 * Tmat / z_term;
-
+    const Plasma<Y> s = plasma_at(a, y, c.g->p, aprime_t);
+    const Y dxH = rec_hydrogen(s, c.k);
+    const Y dxHe = re(s.xHe) < 1e-8 ? 0.0 * s.xHe : rec_helium_singlet(s, c.k) + rec_helium_triplet(s, c.k);
+    const Y dTm = rec_temperature(s, c.k);
     const double dzda = -1.0 / (a * a);
-    f[0] = f0 * dzda;
-    f[1] = f1 * dzda;
-    f[2] = f2 * dzda;
+    f[0] = dxH * dzda;
+    f[1] = dxHe * dzda;
+    f[2] = dTm * dzda;
 }
 
 // Kaps & Rentrop (1979) GRK4A (ode_integrators_stiff.py:157-254): all stages at t0, as the

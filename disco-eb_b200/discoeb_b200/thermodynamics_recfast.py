@@ -93,130 +93,140 @@ def _re(x):
     return np.real(x)
 
 
-def ionization(a, y, param, aprimeoa):
-    """d(x_H, x_He, T_mat)/da (thermodynamics_recfast.py:124-281).
+class _Plasma:
+    """What the three rate equations share at scale factor ``a``: 1 + z, the hydrogen and helium
+    number densities [m^-3], the radiation and matter temperatures [K], the Hubble rate [1/s] and
+    the ionised fractions (x_e = x_H + f_He x_He electrons per hydrogen nucleus).  ``y`` may be
+    complex (complex-step derivatives); branches use its real part."""
 
-    ``y`` may be complex (complex-step Jacobian) and may carry trailing batch axes;
-    comparisons use the real part.  ``aprimeoa`` is the conformal Hubble rate at
-    ``a`` (``get_aprimeoa``), passed in because it only depends on ``a``.
+    __slots__ = ("zp1", "nH", "nHe", "Tr", "Tm", "Hs", "xH", "xHe", "xe", "fHe", "h")
+
+    def __init__(self, a, y, param, aprimeoa):
+        yhe = param["YHe"]
+        self.h = param["H0"] / 100.0
+        self.zp1 = 1.0 / a
+        self.fHe = yhe / (const_mHe_mH * (1.0 - yhe))
+        # hydrogen nuclei per m^3: rho_b (1 - Y) / m_H, with rho_crit / m_H = const_dens_fac h^2
+        self.nH = const_dens_fac * self.h * self.h * param["Omegab"] * (1.0 - yhe) * self.zp1**3
+        self.nHe = self.fHe * self.nH
+        self.Tr = param["Tcmb"] * self.zp1
+        self.Tm = np.where(_re(y[2]) >= 0, y[2], -y[2])
+        # conformal a'/a [1/Mpc] -> H(z) [1/s]
+        self.Hs = 1e-5 * aprimeoa * self.zp1 * const_c * bigH
+        self.xH = y[0]
+        self.xHe = y[1]
+        self.xe = self.xH + self.fHe * self.xHe
+
+
+def _escape(tau):
+    """Sobolev escape probability (1 - e^-tau) / tau of a line of optical depth tau."""
+    return (1.0 - np.exp(-tau)) / tau
+
+
+def _he_line_broadening(s, wavenumber, einstein_a, sigma_abs):
+    """Ratio gamma of the rate at which H continuum absorption removes photons from a HeI line to
+    the line's decay rate (Kholupenko, Ivanchik & Varshalovich 2007; Switzer & Hirata 2008), with
+    the line's thermal Doppler width at T_m."""
+    vth = np.sqrt(2.0 * const_kB * s.Tm / (const_mH * const_mHe_mH * const_c**2))
+    doppler = const_c * wavenumber * vth
+    lam_inv_c = const_c * wavenumber
+    return (3.0 * einstein_a * s.fHe * (1.0 - s.xHe) * const_c**2) / (
+        math.sqrt(math.pi) * sigma_abs * 8.0 * math.pi * doppler * (1.0 - s.xH) * lam_inv_c**2)
+
+
+def _hydrogen_dxdz(s):
+    """dx_H/dz: Peebles' effective three-level atom (Seager, Sasselov & Scott 1999) with the Recfast
+    fudge F = 1.105 and the two-Gaussian correction of the Lyman-alpha escape rate (Wong, Moss &
+    Scott 2008).  Zero while x_H > 0.99, the Saha-limited rate without the Peebles factor for
+    0.985 < x_H <= 0.99."""
+    t4 = s.Tm / 1e4
+    # case-B recombination coefficient, fit of Pequignot, Petitjean & Boisson (1991) [m^3/s]
+    alpha_B = 1e-19 * a_PPB * t4**b_PPB / (1.0 + c_PPB * t4**d_PPB)
+    # photo-ionisation rate from n = 2, by detailed balance [1/s]
+    beta_B = alpha_B * (CR * s.Tm) ** 1.5 * np.exp(-CDB / s.Tm)
+    lnzp1 = math.log(s.zp1)
+    k_fix = 1.0 + AGauss1 * math.exp(-(((lnzp1 - zGauss1) / wGauss1) ** 2)) \
+        + AGauss2 * math.exp(-(((lnzp1 - zGauss2) / wGauss2) ** 2))
+    K_alpha = CK / s.Hs * k_fix          # Lyman-alpha redshifting factor lambda^3 / (8 pi H)
+    n_1s = s.nH * (1.0 - s.xH)           # atoms in the ground state
+    # recombinations minus ionisations out of the ground state, per unit redshift
+    net = (s.xe * s.xH * s.nH * alpha_B - beta_B * (1.0 - s.xH) * np.exp(-CL / s.Tm)) / (s.Hs * s.zp1)
+    # Peebles factor: chance that an atom in n = 2 decays (2s two-photon, or Lyman-alpha escape)
+    # before it is photo-ionised, with the case-B coefficient divided by the fudge F
+    decay = 1.0 + K_alpha * Lambda * n_1s
+    peebles = decay / (decay / 1.105 + K_alpha * beta_B * n_1s)
+    full = net * peebles
+    return np.where(_re(s.xH) > 0.99, 0.0 * s.xH, np.where(_re(s.xH) > 0.985, net, full))
+
+
+def _helium_singlet_dxdz(s):
+    """dx_He/dz through the HeI singlet 2^1P -> 1^1S channel (Seager et al. 2000; Wong et al. 2008):
+    Verner & Ferland (1996) recombination fit, Sobolev escape of the 584 A line plus its removal by
+    H continuum absorption (fit parameters p = 0.36, q = 0.86) once hydrogen starts recombining."""
+    r0 = np.sqrt(s.Tm / T_0)
+    r1 = np.sqrt(s.Tm / T_1)
+    alpha_He = a_VF / (r0 * (1.0 + r0) ** (1.0 - b_VF) * (1.0 + r1) ** (1.0 + b_VF))
+    beta_He = 4.0 * alpha_He * (CR * s.Tm) ** 1.5 * np.exp(-CDB_He / s.Tm)
+    n_HeI = s.nHe * (1.0 - s.xHe)        # neutral helium
+    K_line = CK_He / s.Hs
+    p_esc = _escape(A2P_s * K_line * 3.0 * n_HeI)
+    gamma = _he_line_broadening(s, L_He_2p, A2P_s, sigma_He_2Ps)
+    a_cont = A2P_s / (1.0 + 0.36 * gamma**0.86)
+    # effective K of the line: plain redshifting at the ends of He recombination, else the inverse
+    # escape rate (Sobolev, with the H continuum term while x_H < 0.9999999)
+    ends = (_re(s.xHe) < 5e-9) | (_re(s.xHe) > 0.98)
+    esc_rate = np.where(_re(s.xH) < 0.9999999, A2P_s * p_esc + a_cont, A2P_s * p_esc)
+    K_He = np.where(ends, K_line, 1.0 / (esc_rate * 3.0 * n_HeI))
+    boltz = np.exp(np.where(_re(Bfact / s.Tm) < 680.0, Bfact / s.Tm, 680.0))  # 2s-2p energy gap factor
+    net = (s.xe * s.xHe * s.nH * alpha_He - beta_He * (1.0 - s.xHe) * np.exp(-CL_He / s.Tm)) / (s.Hs * s.zp1)
+    k_n = K_He * n_HeI * boltz
+    return net * (1.0 + k_n * Lambda_He) / (1.0 + k_n * (Lambda_He + beta_He))
+
+
+def _helium_triplet_dxdz(s):
+    """dx_He/dz through the HeI triplet 2^3P -> 1^1S intercombination line (Wong et al. 2008):
+    recombination fit, detailed-balance ionisation from 2^3S, Sobolev escape and H continuum
+    absorption (p = 0.66, q = 0.9).  Omitted at the ends of He recombination."""
+    r0 = np.sqrt(s.Tm / T_0)
+    r1 = np.sqrt(s.Tm / T_1)
+    alpha_t = a_trip / (r0 * (1.0 + r0) ** (1.0 - b_trip) * (1.0 + r1) ** (1.0 + b_trip))
+    beta_t = (4.0 / 3.0) * alpha_t * np.exp(-const_h * const_c * L_He2St_ion / (const_kB * s.Tm)) * (CR * s.Tm) ** 1.5
+    n_HeI = s.nHe * (1.0 - s.xHe)
+    p_esc = _escape(A2P_t * n_HeI * 3.0 / (8.0 * math.pi * s.Hs * L_He_2Pt**3))
+    gamma = _he_line_broadening(s, L_He_2Pt, A2P_t, sigma_He_2Pt)
+    a_cont = A2P_t / (1.0 + 0.66 * gamma**0.9) / 3.0
+    decay = np.where(_re(s.xH) > 0.99999, A2P_t * p_esc, A2P_t * p_esc + a_cont) * np.exp(-CL_PSt / s.Tm)
+    c_trip = decay / (beta_t + decay)    # probability that an atom in 2^3P reaches the ground state
+    net = s.xe * s.xHe * s.nH * alpha_t - 3.0 * beta_t * (1.0 - s.xHe) * np.exp(-const_h_c_L_He_2St_kB / s.Tm)
+    ends = (_re(s.xHe) < 5e-9) | (_re(s.xHe) > 0.98)
+    return np.where(ends, 0.0 * s.xHe, net * c_trip / (s.Hs * s.zp1))
+
+
+def _matter_temperature_dTdz(s):
+    """dT_m/dz: Compton coupling to the radiation against adiabatic cooling; T_m follows T_rad while
+    the Compton time is below 1e-3 of the Hubble time (Seager et al. 1999, eq. 3)."""
+    heat = CT * s.Tr**4 * s.xe / (1.0 + s.xe + s.fHe)   # inverse Compton time [1/s]
+    t_compton = 1.0 / heat
+    t_hubble = 2.0 / (3.0 * s.h * bigH * s.zp1**1.5)
+    coupled = s.Tm / s.zp1
+    free = heat * (s.Tm - s.Tr) / (s.Hs * s.zp1) + 2.0 * s.Tm / s.zp1
+    return np.where(_re(t_compton) < H_frac * t_hubble, coupled, free)
+
+
+def ionization(a, y, param, aprimeoa):
+    """d(x_H, x_He, T_m)/da of the Recfast model (replaces thermodynamics_recfast.py:124-281).
+
+    ``a`` is a real scalar; ``y`` may be complex (complex-step Jacobian) and may carry trailing
+    batch axes; branches use the real part.  ``aprimeoa`` is the conformal Hubble rate at ``a``
+    (``get_aprimeoa``), passed in because it only depends on ``a``.
     """
     with np.errstate(all="ignore"):
-        return _ionization(a, y, param, aprimeoa)
-
-
-def _ionization(a, y, param, aprimeoa):
-    z = 1.0 / a - 1.0
-    H = param["H0"] / 100.0
-    HO = H * bigH
-    fu = 1.105
-    mu_H = 1.0 / (1.0 - param["YHe"])
-    fHe = param["YHe"] / (const_mHe_mH * (1.0 - param["YHe"]))
-    Nnow = const_dens_fac * H * H * param["Omegab"] / mu_H
-
-    x_H = y[0]
-    x_He = y[1]
-    x = x_H + fHe * x_He
-    Tmat = np.where(_re(y[2]) >= 0, y[2], -y[2])
-
-    n = Nnow * (1 + z) ** 3
-    n_He = fHe * n
-    Trad = param["Tcmb"] * (1 + z)
-    z_term = 1 + z
-    Hz = (1e-5 * aprimeoa) / a * const_c * bigH
-
-    Tmat_1e4 = Tmat / 1e4
-    CR_Tmat_15 = (CR * Tmat) ** 1.5
-    Rdown = 1e-19 * a_PPB * Tmat_1e4**b_PPB / (1 + c_PPB * Tmat_1e4**d_PPB)
-    Rup = Rdown * CR_Tmat_15 * np.exp(-CDB / Tmat)
-
-    sq_0 = np.sqrt(Tmat / T_0)
-    sq_1 = np.sqrt(Tmat / T_1)
-    sq_0_term = 1 + sq_0
-    sq_1_term = 1 + sq_1
-    Rdown_He = a_VF / (sq_0 * sq_0_term ** (1 - b_VF) * sq_1_term ** (1 + b_VF))
-    Rup_He = 4 * Rdown_He * CR_Tmat_15 * np.exp(-CDB_He / Tmat)
-
-    bt = Bfact / Tmat
-    He_Boltz = np.exp(np.where(_re(bt) < 680.0, bt, 680.0))
-
-    Rdown_trip = a_trip / (sq_0 * sq_0_term ** (1 - b_trip) * sq_1_term ** (1 + b_trip))
-    Rup_trip = Rdown_trip * np.exp(-const_h * const_c * L_He2St_ion / (const_kB * Tmat)) * CR_Tmat_15 * (4 / 3)
-
-    lz = math.log(z_term)
-    K_gaussian = 1 + AGauss1 * math.exp(-(((lz - zGauss1) / wGauss1) ** 2)) + AGauss2 * math.exp(-(((lz - zGauss2) / wGauss2) ** 2))
-    K = CK / Hz * K_gaussian
-
-    one_minus_x_He = 1 - x_He
-    one_minus_x_H = 1 - x_H
-    n_He_1_minus_x_He = n_He * one_minus_x_He
-
-    tauHe_s = A2P_s * CK_He * 3 * n_He_1_minus_x_He / Hz
-    pHe_s = (1 - np.exp(-tauHe_s)) / tauHe_s
-
-    Doppler_term = np.sqrt(2 * const_kB * Tmat / (const_mH * const_mHe_mH * const_c**2))
-    Doppler_2p = const_c * L_He_2p * Doppler_term
-    Doppler_2Pt = const_c * L_He_2Pt * Doppler_term
-
-    gamma_2Ps_term = 3 * A2P_s * fHe * one_minus_x_He * const_c**2
-    gamma_2Ps_denom = math.sqrt(math.pi) * sigma_He_2Ps * 8 * math.pi * Doppler_2p * one_minus_x_H * (const_c * L_He_2p) ** 2
-    gamma_2Ps = gamma_2Ps_term / gamma_2Ps_denom
-
-    pb = 0.36
-    qb = 0.86
-    AHcon = A2P_s / (1 + pb * (gamma_2Ps**qb))
-
-    K_He_cond1 = (_re(x_He) < 5e-9) | (_re(x_He) > 0.98)
-    K_He_cond2 = _re(x_H) < 0.9999999
-    K_He_default = CK_He / Hz
-    K_He_case1 = 1.0 / ((A2P_s * pHe_s + AHcon) * 3.0 * n_He_1_minus_x_He)
-    K_He_case2 = 1.0 / (A2P_s * pHe_s * 3.0 * n_He_1_minus_x_He)
-    K_He = np.where(K_He_cond1, K_He_default, np.where(K_He_cond2, K_He_case1, K_He_case2))
-
-    tauHe_t = A2P_t * n_He_1_minus_x_He * 3 / (8 * math.pi * Hz * L_He_2Pt**3)
-    pHe_t = (1 - np.exp(-tauHe_t)) / tauHe_t
-    gamma_2Pt_term = 3 * A2P_t * fHe * one_minus_x_He * const_c**2
-    gamma_2Pt_denom = math.sqrt(math.pi) * sigma_He_2Pt * 8 * math.pi * Doppler_2Pt * one_minus_x_H * (const_c * L_He_2Pt) ** 2
-    gamma_2Pt = gamma_2Pt_term / gamma_2Pt_denom
-    pb_t = 0.66
-    qb_t = 0.9
-    AHcon_t = A2P_t / (1 + pb_t * gamma_2Pt**qb_t) / 3
-
-    exp_CL_PSt = np.exp(-CL_PSt / Tmat)
-    CfHe_t_case1 = A2P_t * pHe_t * exp_CL_PSt
-    CfHe_t_case2 = (A2P_t * pHe_t + AHcon_t) * exp_CL_PSt
-    CfHe_t = np.where(_re(x_H) > 0.99999, CfHe_t_case1, CfHe_t_case2)
-    CfHe_t = CfHe_t / (Rup_trip + CfHe_t)
-
-    timeTh = (1 / (CT * Trad**4)) * (1 + x + fHe) / x
-    timeH = 2 / (3 * HO * z_term**1.5)
-
-    Hz_z_term = Hz * z_term
-    x_x_H_n_Rdown = x * x_H * n * Rdown
-    Rup_1_minus_x_H_exp_CL = Rup * one_minus_x_H * np.exp(-CL / Tmat)
-    rate_diff = x_x_H_n_Rdown - Rup_1_minus_x_H_exp_CL
-    K_Lambda_n_1_minus_x_H = K * Lambda * n * one_minus_x_H
-    denom_term = 1 / fu + K_Lambda_n_1_minus_x_H / fu + K * Rup * n * one_minus_x_H
-    f0_case2 = rate_diff / Hz_z_term
-    f0_case3 = (rate_diff * (1 + K_Lambda_n_1_minus_x_H)) / (Hz_z_term * denom_term)
-    f0 = np.where(_re(x_H) > 0.99, 0.0 * x_H, np.where(_re(x_H) > 0.985, f0_case2, f0_case3))
-
-    x_x_He_n_Rdown_He = x * x_He * n * Rdown_He
-    Rup_He_term = Rup_He * one_minus_x_He * np.exp(-CL_He / Tmat)
-    rate_diff_He = x_x_He_n_Rdown_He - Rup_He_term
-    K_He_LHe = K_He * Lambda_He * n_He_1_minus_x_He * He_Boltz
-    He_denom_term = 1 + K_He * (Lambda_He + Rup_He) * n_He_1_minus_x_He * He_Boltz
-    f1_main = (rate_diff_He * (1 + K_He_LHe)) / (Hz_z_term * He_denom_term)
-    trip_rate_diff = x * x_He * n * Rdown_trip - one_minus_x_He * 3 * Rup_trip * np.exp(-const_h_c_L_He_2St_kB / Tmat)
-    trip_contrib = trip_rate_diff * CfHe_t / Hz_z_term
-    trip_cond = (_re(x_He) < 5e-9) | (_re(x_He) > 0.98)
-    f1 = np.where(_re(x_He) < 1e-8, 0.0 * x_He, f1_main + np.where(trip_cond, 0.0 * x_He, trip_contrib))
-
-    f2_case1 = Tmat / z_term
-    f2_case2 = CT * (Trad**4) * x / (1 + x + fHe) * (Tmat - Trad) / Hz_z_term + 2 * Tmat / z_term
-    f2 = np.where(_re(timeTh) < H_frac * timeH, f2_case1, f2_case2)
-
-    dzda = -1.0 / a**2
-    return np.stack([f0 * dzda, f1 * dzda, f2 * dzda])
+        s = _Plasma(a, y, param, aprimeoa)
+        dxH = _hydrogen_dxdz(s)
+        dxHe = np.where(_re(s.xHe) < 1e-8, 0.0 * s.xHe, _helium_singlet_dxdz(s) + _helium_triplet_dxdz(s))
+        dTm = _matter_temperature_dTdz(s)
+        dzda = -1.0 / a**2
+        return np.stack([dxH * dzda, dxHe * dzda, dTm * dzda])
 
 
 # Kaps & Rentrop (1979) GRK4A coefficients (thermodynamics via ode_integrators_stiff.py:176-196)
