@@ -70,7 +70,9 @@ def test_oracle_jacobian_matches_finite_differences():
     n = OP.n
     for j in range(n):
         e = np.zeros(n)
-        h = 1e-6 * max(abs(y[j]), 1e-8)
+        # rows >= 1 are linear in y[1:], so a floor on the step costs no accuracy; without it a
+        # zero entry (theta_c in the synchronous gauge) gets a step at the rounding level
+        h = 1e-6 * max(abs(y[j]), 1e-4)
         e[j] = h
         fd = (OP.rhs(tau, y + e, k) - OP.rhs(tau, y - e, k)) / (2 * h)
         np.testing.assert_allclose(J[:, j], fd, rtol=1e-5, atol=1e-6 * np.abs(J).max())
