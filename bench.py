@@ -54,11 +54,11 @@ def _env_int(name, default):
         return default
 
 
-def _background(w):
+def _background(w, backend="native"):
     from discoeb_b200.background import evolve_background
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
-        return evolve_background(param=w["param"])
+        return evolve_background(param=w["param"], backend=backend)
 
 
 def _sample_modes(w, count):
@@ -67,19 +67,79 @@ def _sample_modes(w, count):
     return k[idx]
 
 
-def _shifted_backgrounds(w):
-    """Backgrounds at theta +- 1e-4 |theta_i| along the 6 solver directions (central differences)."""
+def _shifted_backgrounds(w, backend="native", replay=None):
+    """Backgrounds at theta +- 1e-4 |theta_i| along the 6 solver directions (central differences);
+    ``replay``: a base point's Recfast trace, repeated (its step sequence held fixed)."""
     from discoeb_b200.background import evolve_background
     from discoeb_b200.gradients import ODE_DIRECTIONS, theta_to_params
     out = []
     for name in ODE_DIRECTIONS:
         for sgn in (1, -1):
             th = dict(w["theta"])
-            th[name] += sgn * 1e-4 * max(abs(th[name]), 1e-3)
+            th[name] += sgn * _fd_step(th, name)
             with warnings.catch_warnings():
                 warnings.simplefilter("ignore")
-                out.append(evolve_background(param=theta_to_params(th)))
+                out.append(evolve_background(param=theta_to_params(th), backend=backend, replay=replay))
     return out
+
+
+def _fd_step(theta, name):
+    return 1e-4 * max(abs(theta[name]), 1e-3)
+
+
+def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13):
+    """Max relative error of the GPU's P(k) and dP/dtheta against the oracle (the CPU restatement,
+    converged: rtol 1e-10), on modes spread over the workload's k range.
+
+    P: |P_gpu / P_oracle - 1| over n_p modes at every output.  J: for each solver direction and
+    output, max_k |J_gpu - J_fd| / max_k |J_fd| over n_j modes, J_fd the oracle's central
+    difference of step 1e-4 |theta_i| with the start times, the approximation switch times and
+    the Recfast step sequence held at the base point (the derivative forward-mode AD through the
+    reference defines).  n_s and ln10As are analytic and not checked here."""
+    from discoeb_b200.background import evolve_background
+    from discoeb_b200.gradients import ODE_DIRECTIONS, THETA_NAMES, theta_to_params
+    from discoeb_b200.perturbations import approximation_switch_times, determine_starting_time, get_power
+    from oracle import pyoracle as O
+    L = {k: w[k] for k in ("lmaxg", "lmaxgp", "lmaxr", "lmaxnu", "nqmax")}
+    aout = np.asarray(w["aexp_out"], dtype=np.float64)
+    t_start = time.perf_counter()
+
+    def fixed_times(b, ks):
+        tout = b["tau_of_a_spline"].evaluate(aout)
+        return 0.99 * np.minimum(tout.min(), determine_starting_time(param=b, k=ks)), approximation_switch_times(b, ks)
+
+    def power(b, ks, ts, sw):
+        y, st = O.output_fields_fixed(b, ks, aout, ts, sw, rtol=rtol, atol=atol, **L)
+        if (st != 0).any():
+            raise RuntimeError("oracle solve failed in the accuracy check")
+        return get_power(k=ks[:, None], y=y, idx=4, param=b)
+
+    ip = np.unique(np.linspace(0, len(kmodes) - 1, n_p).round().astype(int))
+    ts, sw = fixed_times(bg, kmodes[ip])
+    Po = power(bg, kmodes[ip], ts, sw)
+    err_p = float(np.max(np.abs(P[ip] / Po - 1)))
+    if n_j == 0:
+        return {"P": err_p, "modes_P": int(ip.size), "oracle": f"CPU restatement, clip mode, rtol {rtol:g}, atol "
+                f"{atol:g}", "seconds": time.perf_counter() - t_start}
+    ij = np.unique(np.linspace(0, len(kmodes) - 1, n_j).round().astype(int))
+    trace = {}
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        evolve_background(param=theta_to_params(w["theta"]), backend="numpy", trace=trace)
+    shifted = _shifted_backgrounds(w, backend="numpy", replay=trace)
+    ts, sw = fixed_times(bg, kmodes[ij])
+    err_j, per_dir = 0.0, {}
+    for d, name in enumerate(ODE_DIRECTIONS):
+        fd = (power(shifted[2 * d], kmodes[ij], ts, sw) - power(shifted[2 * d + 1], kmodes[ij], ts, sw)) \
+            / (2 * _fd_step(w["theta"], name))
+        e = np.abs(J[THETA_NAMES.index(name)][ij] - fd).max(axis=0) / np.abs(fd).max(axis=0)
+        per_dir[name] = float(e.max())
+        err_j = max(err_j, per_dir[name])
+    return {"P": err_p, "J": err_j, "J_per_direction": per_dir, "modes_P": int(ip.size), "modes_J": int(ij.size),
+            "oracle": f"CPU restatement, clip mode, rtol {rtol:g}, atol {atol:g}; J: central differences, step 1e-4 "
+                      "|theta_i|, start / switch times and Recfast steps held; max_k |dJ| / max_k |J| per direction "
+                      "and output",
+            "seconds": time.perf_counter() - t_start}
 
 
 def run_reference(args, rank, world):
@@ -89,13 +149,14 @@ def run_reference(args, rank, world):
     from discoeb_b200.workloads import workload
     from oracle import pyoracle as O
     w = workload(args.workload)
-    bg = _background(w)
+    # the numpy restatement of the background (no native library in this process)
+    bg = _background(w, backend="numpy")
     L = {k: w[k] for k in ("lmaxg", "lmaxgp", "lmaxr", "lmaxnu", "nqmax")}
     ks = _sample_modes(w, args.ref_sample)
     threads = os.cpu_count() or 1
 
     grad = args.mode == "fwd+grad"
-    bgs = [bg] + (_shifted_backgrounds(w) if grad else [])
+    bgs = [bg] + (_shifted_backgrounds(w, backend="numpy") if grad else [])
 
     def one():
         t = time.perf_counter()
@@ -430,7 +491,8 @@ def main():
     ap.add_argument("--host-backend", default="native", choices=["native", "device"],
                     help="--mode batch: backgrounds on the host (native C++) or in one GPU launch")
     ap.add_argument("--wpb", type=int, default=0, help="warps (modes) per block; 0 = the library default")
-    ap.add_argument("--ref-sample", type=int, default=24)
+    ap.add_argument("--ref-sample", type=int, default=16)
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the oracle accuracy check")
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel-only", action="store_true", help="skip the e2e loop and the FP64 peak (profiling)")
@@ -616,6 +678,18 @@ def main():
                "sample": f"{len(ks)} modes spread over the workload's k range, oracle dense-LU Rodas5{how}, "
                          f"{dt:.1f} s"}
 
+    accuracy = None
+    if rank == 0 and world == 1 and not args.no_accuracy and not args.kernel_only:
+        # the checker: the GPU's results of the timed launches against the converged oracle
+        if grad:
+            P_gpu, J_gpu = prob.result()[:2]
+        else:
+            inv = np.empty_like(order)
+            inv[order] = np.arange(K)
+            P_gpu = pert.get_power(k=kmodes[:, None], y=d_out.cpu().numpy()[inv], idx=4, param=bg)
+            J_gpu = None
+        accuracy = oracle_accuracy(w, bg, kmodes, P_gpu, J_gpu, n_j=8 if grad else 0)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -624,6 +698,8 @@ def main():
             "config": {"workload": args.workload, "mode": args.mode, "num_k": K, "nvar": n, "n_out": nout,
                        "tangent_directions": n_dir, "gradient_of": "P(k) at every output w.r.t. omega_c, omega_b, h, "
                        "n_s, ln10As, w0, wa, m_nu" if grad else None,
+                       "gradient_method": "forward-mode tangents (discoeb_jvp: 6 directions through the solver, "
+                       "n_s and ln10As analytic)" if grad else None,
                        "rtol": w["rtol"], "atol": w["atol"], "method": "rodas5-structured",
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "ms_per_cosmology": ms, "step_attempts_per_mode_sum": step_attempts,
@@ -644,6 +720,8 @@ def main():
             line["forward_only"] = {"value": world * K / (fwd_ms / 1e3), "unit": UNIT, "ms_per_cosmology": fwd_ms}
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if accuracy is not None:
+            line["max_rel_err"] = accuracy
         print(json.dumps(line), flush=True)
     replicas.finish(dist)
 

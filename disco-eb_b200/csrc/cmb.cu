@@ -786,14 +786,19 @@ std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[64] = {};
 
 // device address of g_noalloc_scratch on the current device, looked up once per device (on the
-// first no-allocation call made with that device current)
+// first no-allocation call made with that device current) and kept for the life of the process:
+// a device reset (cudaDeviceReset) unloads the module, after which the kept address is stale, so
+// the no-allocation entry is not for processes that reset a device they have used it on
 double* noalloc_scratch(int dev)
 {
     if (dev < 0 || dev >= 64) return nullptr;
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
         void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();  // clear the error: it belongs to this call, not to the next one
+            return nullptr;
+        }
         g_noalloc_ptr[dev] = static_cast<double*>(p);
     }
     return g_noalloc_ptr[dev];
@@ -939,6 +944,7 @@ int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const long long points = (long long)n_modes * n_tau;
     const int threads = 128;
+    if (points * 32 / threads >= 0x7fffffffLL) return DISCOEB_EINVAL;  // one warp per point must fit the grid
     const size_t smem = sizeof(double) * (size_t)D.n * (threads / 32);
     sources_kernel<<<blocks_for(points * 32, threads), threads, smem, s>>>(cosmo_dev, n_modes, kmodes, n_tau, tau,
                                                                             bgtab, y_full, fields);
@@ -1110,6 +1116,9 @@ int32_t discoeb_sources_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* c
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const long long points = (long long)n_dir * n_modes * n_tau;
     const int threads = 128;
+    // isw_dot_kernel indexes (direction, mode) pairs with an int, and one warp per point must fit
+    // the grid: larger problems are refused rather than truncated
+    if ((long long)n_dir * n_modes > 0x7fffffffLL || points * 32 / threads >= 0x7fffffffLL) return DISCOEB_EINVAL;
     const size_t smem = sizeof(double) * 2 * (size_t)D.n * (threads / 32);
     double* fd4 = scratch;                       // [4, n_dir, n_modes, n_tau]
     double* sp = scratch + 4 * (size_t)points;  // [4, n_dir, n_modes, n_tau]

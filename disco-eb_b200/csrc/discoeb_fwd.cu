@@ -190,7 +190,9 @@ __device__ __noinline__ void emit_tangent_output(const WarpTeam& tm, const Disco
 // the block's abort flag is set, or the poll budget runs out, after which it sets the abort
 // flag itself); returns true when the target was reached.  No wait can last forever.
 constexpr long long kMaxPolls = 1LL << 24;  // ~2 s with the back-off below; a step takes < 1 ms
-__device__ bool wait_at_least(const WarpTeam& tm, volatile int* flag, int target, volatile int* abort_flag)
+__device__ long long poll_budget(const DiscoebControl& c) { return c.max_polls > 0 ? (long long)c.max_polls : kMaxPolls; }
+__device__ bool wait_at_least(const WarpTeam& tm, volatile int* flag, int target, volatile int* abort_flag,
+                              long long max_polls)
 {
     int ok = 0;
     if (tm.leader()) {
@@ -198,7 +200,7 @@ __device__ bool wait_at_least(const WarpTeam& tm, volatile int* flag, int target
         while (true) {
             if (*flag >= target) { ok = 1; break; }
             if (*abort_flag) break;
-            if (++polls > kMaxPolls) { *abort_flag = 1; break; }
+            if (++polls > max_polls) { *abort_flag = 1; break; }
             __nanosleep(100);
         }
         __threadfence_block();
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
         int m = 0;
         auto accept = [&](double t, double h, double tnext, int regime) -> bool {
             const int sl = m & 1;
-            if (m >= 2 && !wait_at_least(tm, vf + 2 + sl, nd * (m / 2), vf + 6)) return false;
+            if (m >= 2 && !wait_at_least(tm, vf + 2 + sl, nd * (m / 2), vf + 6, poll_budget(ctrl))) return false;
             double* dst = slot0 + sl * rec;
             for (int i = tm.lane; i < mem_doubles; i += 32) dst[i] = fmem[i];
             if (tm.leader()) {
@@ -355,6 +357,7 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     for (int i = tm.lane; i < n; i += 32) TT.yd[i] = y0_dot[((size_t)dir * n_modes + mode) * n + i];
     tm.sync();
     int hint = P->xe_loga.n_knots / 2, iout = 0;
+    const long long budget = poll_budget(ctrl);
     for (int m = 0;; ++m) {
         const int sl = m & 1;
         // the next step, unless the forward has finished with fewer steps
@@ -365,7 +368,7 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
                 if (vf[sl] == m + 1) { have = 1; break; }
                 if (vf[4] && vf[5] <= m) break;
                 if (vf[6]) break;
-                if (++polls > kMaxPolls) { vf[6] = 1; break; }
+                if (++polls > budget) { vf[6] = 1; break; }
                 __nanosleep(100);
             }
             __threadfence_block();

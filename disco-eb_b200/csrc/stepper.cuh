@@ -821,9 +821,16 @@ DDV SolveResult solve_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, c
             const double e = M.K[7 * n + i] / (C.atol + C.rtol * sc) * w6[q];
             sumsq += e * e;
         }
+        // non-finite candidate entries count 1, non-finite entries of the step start (state or
+        // Jacobian column d f/d a: a NaN or an infinity in an input table) count 1024
         double lf = 0.0;
-        for (int i = tm.lane; i < n; i += tm.nl) lf += xfinite(M.u[i] + M.K[7 * n + i]) ? 0.0 : 1.0;
-        const bool finite = ok && tm.sum(lf) == 0.0;
+        for (int i = tm.lane; i < n; i += tm.nl) {
+            lf += xfinite(M.u[i] + M.K[7 * n + i]) ? 0.0 : 1.0;
+            lf += (xfinite(M.y[i]) && xfinite(M.col0[i])) ? 0.0 : 1024.0;
+        }
+        const double nbad = tm.sum(lf);
+        if (nbad >= 1024.0) { R.status = DISCOEB_NONFINITE; break; }  // no step size can help
+        const bool finite = ok && nbad == 0.0;
         const double err = finite ? sqrt(sumsq / 6.0) : INFINITY;
         const bool keep = err < 1.0;
         double inv = 1.0 / err;

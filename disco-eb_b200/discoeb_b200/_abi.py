@@ -21,7 +21,8 @@ METHOD_RODAS5_DENSE = 1
 METHOD_RODAS5_DENSE_MIXED = 2
 
 STATUS_NAMES = {0: "ok", 1: "max_steps exceeded", 2: "non-finite state", 3: "step size underflow", 4: "singular",
-                5: "cosmology index out of range"}
+                5: "cosmology index out of range",
+                6: "aborted (a cooperating warp gave up waiting)"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -52,7 +53,7 @@ class DiscoebTangent(ctypes.Structure):
 
 class DiscoebControl(ctypes.Structure):
     _fields_ = ([(f, ctypes.c_double) for f in ("rtol", "atol", "pcoeff", "icoeff", "dcoeff", "factormax", "factormin")]
-                + [(f, ctypes.c_int32) for f in ("max_steps", "method", "warps_per_block", "reserved")])
+                + [(f, ctypes.c_int32) for f in ("max_steps", "method", "warps_per_block", "max_polls")])
 
 
 class DiscoebCosmoParams(ctypes.Structure):

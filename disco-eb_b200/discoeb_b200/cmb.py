@@ -62,6 +62,18 @@ def background_table(aexp_out, tau, param):
     return np.ascontiguousarray(np.stack([np.broadcast_to(rows[f], aexp_out.shape) for f in BG_FIELDS]))
 
 
+# points (modes x output times) that discoeb_sources_noalloc's own scratch array holds
+NOALLOC_MAX_POINTS = 1 << 20
+
+
+def noalloc_check(n_modes, n_tau):
+    """Raise ValueError if discoeb_sources_noalloc would refuse these sizes (its scratch array
+    holds NOALLOC_MAX_POINTS points)."""
+    if n_modes * n_tau > NOALLOC_MAX_POINTS:
+        raise ValueError(f"no_alloc: {n_modes} modes x {n_tau} times exceeds the {NOALLOC_MAX_POINTS} points of "
+                         "the library's scratch")
+
+
 def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, de_guard_eps=1e-9,
                     device=None, no_alloc=False):
     """All source fields of compute_source_function and its intermediates (cmb.py:17-633).
@@ -85,8 +97,8 @@ def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmax
     y = y.to(**f64).contiguous()
     if y.shape[:2] != (K, T):
         raise ValueError(f"yout must have shape [{K}, {T}, nvar], got {tuple(y.shape)}")
-    if no_alloc and K * T > (1 << 20):
-        raise ValueError(f"no_alloc: {K} modes x {T} times exceeds the 2^20 points of the library's scratch")
+    if no_alloc:
+        noalloc_check(K, T)
     d_k = torch.from_numpy(kmodes).to(device)
     d_tau = torch.from_numpy(np.ascontiguousarray(tau)).to(device)
     d_bt = torch.from_numpy(background_table(aexp_out, tau, param)).to(device)

@@ -74,7 +74,11 @@ typedef struct {
     int32_t max_steps;
     int32_t method;       /* DISCOEB_METHOD_* */
     int32_t warps_per_block;
-    int32_t reserved;
+    /* Poll budget of every wait between cooperating warps of one mode (discoeb_jvp): a warp that
+     * polls a hand-over counter this many times without progress stops the mode with
+     * DISCOEB_ABORTED instead of waiting on.  <= 0: the library default, 2^24 polls of ~100 ns
+     * (about 2 s; one step takes well under a millisecond). */
+    int32_t max_polls;
 } DiscoebControl;
 
 #define DISCOEB_METHOD_RODAS5_STRUCTURED 0 /* default: banded-chain + rank-3 LU, FP64 */
@@ -84,7 +88,8 @@ typedef struct {
 /* per-mode status codes */
 #define DISCOEB_OK 0
 #define DISCOEB_MAX_STEPS 1
-#define DISCOEB_NONFINITE 2
+#define DISCOEB_NONFINITE 2 /* the state or the Jacobian at a step start is not finite (a NaN or an
+                             * infinity in an input table, say): no step size can help */
 #define DISCOEB_DT_UNDERFLOW 3
 #define DISCOEB_SINGULAR 4
 #define DISCOEB_BAD_INDEX 5 /* mode_cosmo[mode] outside [0, n_cosmo), or that cosmology's l_max / nq
@@ -229,7 +234,9 @@ int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo
  * file-scope device array of 2^20 doubles (8 MiB) that the library holds on every GPU that loads
  * it, until the process exits.  Limit: n_modes * n_tau <= 1048576, else DISCOEB_EINVAL and no
  * work.  The first call on a device looks up the array's device address (cudaGetSymbolAddress,
- * with that device current); make that first call before any stream capture.  Every call shares
+ * with that device current) and keeps it until the process exits; make that first call before any
+ * stream capture, and do not use this entry after resetting a device it has run on
+ * (cudaDeviceReset unloads the array, and the kept address would be stale).  Every call shares
  * the array, so calls that overlap on the GPU (two streams, two host threads) race: serialise
  * them.  Nothing in the array has to start at zero (it is written before it is read).  No
  * counterpart in the reference. */

@@ -256,3 +256,29 @@ def evolve_perturbations(*, param, aexp_out, kmin, kmax, num_k, lmaxg=11, lmaxgp
         for j in range(nout):
             out[i, j] = OP.output_vars(k, proj[i, j])
     return out, kmodes, stats
+
+
+def output_fields_fixed(param, kmodes, aexp_out, tau_start, switch_tau, *, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, rtol,
+                        atol, max_steps=400000, de_guard_eps=1e-9, threads=None):
+    """Output fields [K, nout, 20] of the clip-mode solve with the start times ``tau_start`` [K] and
+    approximation switch times ``switch_tau`` [K, 3] given (held at a base point's values when the
+    parameters move, the convention of forward-mode AD through the reference), and status [K]."""
+    OP = OracleProblem(param, lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax,
+                       de_guard_eps=de_guard_eps)
+    kmodes = np.asarray(kmodes, dtype=np.float64)
+    tau_out = param["tau_of_a_spline"].evaluate(np.atleast_1d(np.asarray(aexp_out, dtype=np.float64)))
+    nout = tau_out.shape[0]
+
+    def run(i):
+        k, t0 = float(kmodes[i]), float(tau_start[i])
+        ys, st = OP.solve([k], t0, OP.ics(t0, k), tau_out, rtol=rtol, atol=atol, max_steps=max_steps,
+                          sw=np.asarray(switch_tau[i], dtype=np.float64))
+        out = np.array([OP.output_vars(k, OP.rsa_project(tau_out[j], k, ys[0, j])) for j in range(nout)])
+        return i, out, st.status
+
+    out = np.zeros((kmodes.shape[0], nout, 20))
+    status = np.zeros(kmodes.shape[0], dtype=np.int32)
+    with ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as ex:
+        for i, o, s in ex.map(run, range(kmodes.shape[0])):
+            out[i], status[i] = o, s
+    return out, status

@@ -183,6 +183,38 @@ def test_sources_tangent_entry_rejects_bad_arguments_before_any_launch():
         assert lib.discoeb_sources_jvp(*args) == -1, (i, v)
 
 
+def test_noalloc_size_limit_is_the_same_in_c_and_python():
+    # the no-allocation sources entry holds 2^20 points in its own array: one point more is refused
+    # by the C entry before any device work (its pointers are never touched), and the Python
+    # pre-check draws the line at the same place
+    from discoeb_b200 import cmb
+    lib = _abi.lib()
+    host = _abi.DiscoebCosmo()
+    assert cmb.NOALLOC_MAX_POINTS == 1 << 20
+    assert lib.discoeb_sources_noalloc(None, ctypes.byref(host), 1025, None, 1024, None, None, None, None, None) == -1
+    assert lib.discoeb_sources_noalloc(None, ctypes.byref(host), 1, None, (1 << 20) + 1, None, None, None, None,
+                                       None) == -1
+    cmb.noalloc_check(1024, 1024)
+    cmb.noalloc_check(1, 1 << 20)
+    with pytest.raises(ValueError):
+        cmb.noalloc_check(1025, 1024)
+    with pytest.raises(ValueError):
+        cmb.noalloc_check(1, (1 << 20) + 1)
+
+
+def test_sources_entries_refuse_grids_beyond_the_launch_limits():
+    # one warp per (direction, mode, time) point: sizes whose grid would not fit are refused before
+    # any launch (the pointers are never dereferenced)
+    lib = _abi.lib()
+    host = _abi.DiscoebCosmo()
+    host.lmaxg, host.lmaxgp, host.lmaxr, host.lmaxnu, host.nqmax = 11, 11, 11, 8, 3
+    fake = 4096
+    big = 1 << 30
+    assert lib.discoeb_sources_jvp(fake, ctypes.byref(host), fake, 8, big, fake, 16, fake, fake, fake, fake, fake,
+                                   fake, fake, fake, fake, None) == -1
+    assert lib.discoeb_sources(fake, ctypes.byref(host), big, fake, 64, fake, fake, fake, fake, fake, None) == -1
+
+
 def test_struct_layout_matches_header():
     # the ctypes mirror must have the C layout: compile a tiny probe of offsetof/sizeof
     import tempfile
