@@ -160,14 +160,20 @@ template <class T> DHD T inv_vq(const DiscoebCosmo& P, const Bg<T>& b, int q)
     return xsqrt(1.0 + aq * aq);
 }
 
-template <class T> DHD T aprimeoa_of(const DiscoebCosmo& P, const Par<T>& par, const DiscoebTangent* tn, T a, T loga)
+// a'/a (get_aprimeoa, background.py:101-123) from the massive-neutrino density rho_nu at a
+template <class T> DHD T aprimeoa_from(const DiscoebCosmo& P, const Par<T>& par, T a, T loga, T rhonu)
 {
-    const int i = spline_index(P.logrhonu_loga, val(loga));
-    T rhonu = xexp(spline_eval_at(P.logrhonu_loga, i, loga, tn ? tn->logrhonu_y : nullptr, tn ? tn->logrhonu_S : nullptr));
     T rho_Q = xexp(-3.0 * (1.0 + par.w0 + par.wa) * loga + 3.0 * (a - 1.0) * par.wa);
     T grho = par.grhom * par.Omegam / a + (P.grhog + P.grhor * (P.Neff + P.Nmnu * rhonu)) / (a * a) +
              par.grhom * par.OmegaDE * rho_Q * a * a + par.grhom * P.Omegak;
     return xsqrt(grho * (1.0 / 3.0));
+}
+
+template <class T> DHD T aprimeoa_of(const DiscoebCosmo& P, const Par<T>& par, const DiscoebTangent* tn, T a, T loga)
+{
+    const int i = spline_index(P.logrhonu_loga, val(loga));
+    T rhonu = xexp(spline_eval_at(P.logrhonu_loga, i, loga, tn ? tn->logrhonu_y : nullptr, tn ? tn->logrhonu_S : nullptr));
+    return aprimeoa_from(P, par, a, loga, rhonu);
 }
 
 // index of a non-uniform spline searched from a hint (the previous index): same result
@@ -676,21 +682,19 @@ namespace dscb {
 
 // ---- RSA output projection (approximations.py:84-176): the fields that replace the
 // photon and massless-neutrino moments at an output time.  Returns true when the RSA
-// condition holds there (evaluated from (tau, a) as the reference does).  y with tangent yd
-// (may be null) and parameter tangent tn (may be null).
-template <class T>
-DHD bool rsa_projection(const DiscoebCosmo& P, const DiscoebTangent* tn, const Dims& D, double tau, double k,
-                        const double* y, const double* yd, T out[4])
+// condition holds there (evaluated from (tau, a) as the reference does).  rsa_fields takes the
+// state through Y(i) and the table values at a (rho_nu, x_e, dx_e/dln a, c_s^2 a); rsa_projection
+// reads them from the tables, with the state's tangent yd (may be null) and the parameter tangent
+// tn (may be null).
+template <class T, class YF>
+DHD bool rsa_fields(const DiscoebCosmo& P, const Par<T>& par, const Dims& D, double tau, double k, const YF& Y,
+                    const T& a, const T& loga, const T& rhonu, const T& xe, const T& dxe_dloga, const T& cs2a,
+                    T out[4])
 {
-    const Par<T> par = make_par<T>(P, tn);
-    auto Y = [&](int i) { return seed_t<T>(y[i], yd ? yd[i] : 0.0); };
-    const T a = Y(0), loga = xlog(a), eta = Y(2), deltab = Y(5), thetab = Y(6);
-    const T aH = aprimeoa_of(P, par, tn, a, loga);
-    const int ix = spline_index(P.xe_loga, val(loga));
-    const T xe = spline_eval_at(P.xe_loga, ix, loga, tn ? tn->xe_y : nullptr, tn ? tn->xe_S : nullptr);
-    const T xeprime = spline_deriv_at(P.xe_loga, ix, loga, tn ? tn->xe_y : nullptr, tn ? tn->xe_S : nullptr) * aH;
-    const int ic = spline_index(P.cs2a_loga, val(loga));
-    const T cs2 = spline_eval_at(P.cs2a_loga, ic, loga, tn ? tn->cs2a_y : nullptr, tn ? tn->cs2a_S : nullptr) / a;
+    const T eta = Y(2), deltab = Y(5), thetab = Y(6);
+    const T aH = aprimeoa_from(P, par, a, loga, rhonu);
+    const T xeprime = dxe_dloga * aH;
+    const T cs2 = cs2a / a;
     const T opac = xe * par.akthom / (a * a);
     const T tau_c = rcp(xmaxc(opac, 1e-30));
     const T tau_c_prime = tau_c * (2.0 * aH - xeprime / xmaxc(xe, 1e-30));
@@ -716,6 +720,24 @@ DHD bool rsa_projection(const DiscoebCosmo& P, const DiscoebTangent* tn, const D
     return P.use_rsa && (tcr / (tau > 1e-30 ? tau : 1e-30) > P.rsa_tau_c_over_tau) && (tau * k > P.rsa_tau_over_tau_k);
 }
 
+template <class T>
+DHD bool rsa_projection(const DiscoebCosmo& P, const DiscoebTangent* tn, const Dims& D, double tau, double k,
+                        const double* y, const double* yd, T out[4])
+{
+    const Par<T> par = make_par<T>(P, tn);
+    auto Y = [&](int i) { return seed_t<T>(y[i], yd ? yd[i] : 0.0); };
+    const T a = Y(0), loga = xlog(a);
+    const int ir = spline_index(P.logrhonu_loga, val(loga));
+    const T rhonu = xexp(spline_eval_at(P.logrhonu_loga, ir, loga, tn ? tn->logrhonu_y : nullptr,
+                                        tn ? tn->logrhonu_S : nullptr));
+    const int ix = spline_index(P.xe_loga, val(loga));
+    const T xe = spline_eval_at(P.xe_loga, ix, loga, tn ? tn->xe_y : nullptr, tn ? tn->xe_S : nullptr);
+    const T dxe = spline_deriv_at(P.xe_loga, ix, loga, tn ? tn->xe_y : nullptr, tn ? tn->xe_S : nullptr);
+    const int ic = spline_index(P.cs2a_loga, val(loga));
+    const T cs2a = spline_eval_at(P.cs2a_loga, ic, loga, tn ? tn->cs2a_y : nullptr, tn ? tn->cs2a_S : nullptr);
+    return rsa_fields(P, par, D, tau, k, Y, a, loga, rhonu, xe, dxe, cs2a, out);
+}
+
 // is index i one of the moments the RSA projection overwrites?  (value slot or -1 for zero)
 DHD int rsa_slot(const Dims& D, int i)
 {
@@ -728,23 +750,18 @@ DHD int rsa_slot(const Dims& D, int i)
     return -2;  // untouched
 }
 
-// ---- convert_to_output_variables (perturbations.py:528-677), state y with tangent yd ----
-template <class T>
-DHD void output_vars(const DiscoebCosmo& P, const DiscoebTangent* tn, const Dims& D, double k, const double* y,
-                     const double* yd, T* o)
+// ---- convert_to_output_variables (perturbations.py:528-677) ----
+// output_fields takes the state through Y(i) and the table values rho_nu, p_nu at a;
+// output_vars reads them from the tables, with the state's tangent yd and parameter tangent tn
+// (either may be null).
+template <class T, class YF>
+DHD void output_fields(const DiscoebCosmo& P, const Par<T>& par, const Dims& D, double k, const YF& Y, const T& a,
+                       const T& loga, const T& rhonu, const T& pnu, T* o)
 {
-    const Par<T> par = make_par<T>(P, tn);
-    auto Y = [&](int i) { return seed_t<T>(y[i], yd ? yd[i] : 0.0); };
     const T Omegac = par.Omegam - par.Omegab;
     const int n = D.n, nq = D.nq, iq0 = D.iq0, iq1 = iq0 + nq;
-    const T a = Y(0), eta = Y(2), deltac = Y(3), thetac = Y(4), deltab = Y(5), thetab = Y(6);
+    const T eta = Y(2), deltac = Y(3), thetac = Y(4), deltab = Y(5), thetab = Y(6);
     const T deltag = Y(7), thetag = Y(8), deltar = Y(D.idxr), thetar = Y(D.idxr + 1);
-    const T loga = xlog(a);
-    const int inu = spline_index(P.logrhonu_loga, val(loga));
-    const T rhonu = xexp(spline_eval_at(P.logrhonu_loga, inu, loga, tn ? tn->logrhonu_y : nullptr,
-                                        tn ? tn->logrhonu_S : nullptr));
-    const int ip = spline_index(P.logpnu_loga, val(loga));
-    const T pnu = xexp(spline_eval_at(P.logpnu_loga, ip, loga, tn ? tn->logpnu_y : nullptr, tn ? tn->logpnu_S : nullptr));
     T drhonu = 0.0, fnu = 0.0;
     for (int q = 0; q < nq; ++q) {
         const T aq = a * par.amnu * (1.0 / P.q[q]);
@@ -783,6 +800,22 @@ DHD void output_vars(const DiscoebCosmo& P, const DiscoebTangent* tn, const Dims
     o[8] = deltac; o[9] = thetac * iaH; o[10] = deltab; o[11] = thetab * iaH;
     o[12] = deltag; o[13] = thetag * iaH; o[14] = deltar; o[15] = thetar * iaH;
     o[16] = deltanu; o[17] = thetanu * iaH; o[18] = deltaq; o[19] = thetaq * iaH;
+}
+
+
+template <class T>
+DHD void output_vars(const DiscoebCosmo& P, const DiscoebTangent* tn, const Dims& D, double k, const double* y,
+                     const double* yd, T* o)
+{
+    const Par<T> par = make_par<T>(P, tn);
+    auto Y = [&](int i) { return seed_t<T>(y[i], yd ? yd[i] : 0.0); };
+    const T a = Y(0), loga = xlog(a);
+    const int inu = spline_index(P.logrhonu_loga, val(loga));
+    const T rhonu = xexp(spline_eval_at(P.logrhonu_loga, inu, loga, tn ? tn->logrhonu_y : nullptr,
+                                        tn ? tn->logrhonu_S : nullptr));
+    const int ip = spline_index(P.logpnu_loga, val(loga));
+    const T pnu = xexp(spline_eval_at(P.logpnu_loga, ip, loga, tn ? tn->logpnu_y : nullptr, tn ? tn->logpnu_S : nullptr));
+    output_fields(P, par, D, k, Y, a, loga, rhonu, pnu, o);
 }
 
 }  // namespace dscb

@@ -140,28 +140,20 @@ DHD double comp(double x, int c) { return c == 0 ? x : 0.0; }
 DHD double comp(const Dual& x, int c) { return c == 0 ? x.v : (c == 1 ? x.d : 0.0); }
 DHD double comp(const HDual& x, int c) { return c == 0 ? x.v.v : (c == 1 ? x.v.d : (c == 2 ? x.d.v : x.d.d)); }
 
-// ---- RHS f(tau, y) (all entries), T = double or Dual in a ----
-// The metric functionals and the 15 "special" rows are computed in straight-line code by every
-// lane (no divergence, no reductions); the hierarchy rows are spread over the lanes as one
-// uniform class.  Same equations as model_synchronous (perturbations.py:88-525).
-// S is the type of the state entries: T when the state carries derivative parts (yd, yk), or
-// double for a plain state under a dual background, where the products of coefficients and state
-// entries then cost the dual-times-double form.
-template <class TM, class T, class S = T>
-DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau,
-                  const double* y, double* f, double* dfda, const double* yd = nullptr, const double* yk = nullptr,
-                  int fcomp = 0, int dcomp = 1)
+// ---- the 15 special rows and the metric functionals ----
+// Rows a, a h', eta, CDM, baryons, photon l <= 2, massless l <= 2 and dark energy (sp, in the
+// order of special_row) and the three functionals g = (h', eta', polter) through which the
+// hierarchy rows couple, in straight-line code (every lane of a team computes them; no
+// divergence, no reductions).  Y(j) gives state entry j (type S); ivl / vl are 1/v and v of
+// momentum bin tm.lane, read through tm.bcast when tm.full().  Same equations as
+// model_synchronous (perturbations.py:88-525).
+template <class TM, class T, class S, class YF>
+DHD void special_part(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau,
+                      YF Y, const T ivl, const T vl, T sp[15], T& g0, T& g1, T& g2)
 {
-    auto Y = [&](int j) { return state_at<S>(y, yd, yk, j); };
     const int n = D.n, nq = D.nq, iq0 = D.iq0, idxr = D.idxr;
     const double k2 = k * k;
     const T Omegac = b.par.Omegam - b.par.Omegab;
-    // 1/v of momentum bin q on lane q
-    T ivl = 1.0;
-    if (tm.full() && tm.lane < nq) ivl = inv_vq(P, b, tm.lane);
-    const T vl = rcp(ivl);
-    // d ln f0 / d ln q of bin q on lane q
-    const double dll = (tm.full() && tm.lane < nq) ? dlfdlq_of(P.q[tm.lane]) : 0.0;
     T drho = 0.0, dp = 0.0, fnu = 0.0;
 #pragma unroll
     for (int q = 0; q < DISCOEB_MAX_NQ; ++q) {
@@ -212,7 +204,6 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
     const T polter = hier_photons ? T(y9 + Y(D.idxgp) + Y(D.idxgp + 2)) : T(0.0);
     const T alpha = (H + 6.0 * E) * (0.5 / k2);
     // special rows
-    T sp[15];
     sp[0] = b.aH * b.a;
     sp[1] = -(dgrho + 3.0 * dgpres) * b.a;
     sp[2] = E;
@@ -239,6 +230,33 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
                  9.0 * b.opw * (cs2Q - b.ca2_Q) * b.aH * b.aH * (1.0 / k2) * thetaq;
         sp[14] = -(1.0 - 3.0 * cs2Q) * b.aH * thetaq + cs2Q * b.iopw * k2 * deltaq;
     }
+    g0 = H;
+    g1 = E;
+    g2 = polter;
+}
+
+// ---- RHS f(tau, y) (all entries), T = double or Dual in a ----
+// The metric functionals and the 15 "special" rows are computed in straight-line code by every
+// lane (no divergence, no reductions); the hierarchy rows are spread over the lanes as one
+// uniform class.  Same equations as model_synchronous (perturbations.py:88-525).
+// S is the type of the state entries: T when the state carries derivative parts (yd, yk), or
+// double for a plain state under a dual background, where the products of coefficients and state
+// entries then cost the dual-times-double form.
+template <class TM, class T, class S = T>
+DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau,
+                  const double* y, double* f, double* dfda, const double* yd = nullptr, const double* yk = nullptr,
+                  int fcomp = 0, int dcomp = 1)
+{
+    auto Y = [&](int j) { return state_at<S>(y, yd, yk, j); };
+    const int nq = D.nq;
+    // 1/v of momentum bin q on lane q
+    T ivl = 1.0;
+    if (tm.full() && tm.lane < nq) ivl = inv_vq(P, b, tm.lane);
+    const T vl = rcp(ivl);
+    // d ln f0 / d ln q of bin q on lane q
+    const double dll = (tm.full() && tm.lane < nq) ? dlfdlq_of(P.q[tm.lane]) : 0.0;
+    T sp[15], g0, g1, g2;
+    special_part<TM, T, S>(tm, P, D, b, k, tau, Y, ivl, vl, sp, g0, g1, g2);
     if (tm.leader()) {
 #pragma unroll
         for (int ss = 0; ss < 15; ++ss) {
@@ -247,7 +265,6 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
             if (dfda) dfda[i] = comp(sp[ss], dcomp);
         }
     }
-    const T g0 = H, g1 = E, g2 = polter;
     const int nh = n_hier_rows(D);
     // every lane runs the same number of iterations: the shuffle in the loop needs all lanes
     for (int h0 = 0; h0 < nh; h0 += tm.nl) {
@@ -448,9 +465,11 @@ template <class TM> DDV void solve_A(const TM& tm, const Dims& D, const ModeMem&
 }
 
 // Assemble and factor W at (t, y) for step size h.  Needs M.col0 (d f/d a) already set.
+// ukeep (may be null): receives the coupling columns U (3 n doubles) before the factorisation
+// replaces them by A^{-1} U (the transposed solves of the adjoint need U itself).
 template <class TM>
 DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<double>& b, double k, double tau,
-                  double h, const ModeMem& M)
+                  double h, const ModeMem& M, double* ukeep = nullptr)
 {
     const int n = D.n;
     const double gh = kR5.gamma * h;
@@ -513,6 +532,8 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
         M.sc[SC_F1U + 2] = u[2];
     }
     tm.sync();
+    if (ukeep)
+        for (int i = tm.lane; i < 3 * n; i += tm.nl) ukeep[i] = M.Z[i];
     bool ok = true;
     const int nc = n_chains(D);
     for (int c = tm.lane; c < nc; c += tm.nl) ok = factor_chain(M.A, chain_of(D, c)) && ok;
@@ -711,7 +732,8 @@ DDV void tangent_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
 // M.K[7] the error estimate.  Returns false on a non-finite factorisation.
 template <class TM>
 DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
-                     const ModeMem& M, int& hint, const DiscoebTangent* tn = nullptr, const TanMem* TT = nullptr)
+                     const ModeMem& M, int& hint, const DiscoebTangent* tn = nullptr, const TanMem* TT = nullptr,
+                     double* ukeep = nullptr)
 {
     const int n = D.n;
     // Jacobian column d f/d a and f(y) in one dual pass
@@ -721,7 +743,7 @@ DDV bool rodas5_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double 
     const Bg<double> b = bg_value(bd);
     for (int i = tm.lane; i < n; i += tm.nl) M.dT[i] = dtau_row(D, b, t, i, M.y);
     tm.sync();
-    const bool ok = factor_W(tm, P, D, b, k, t, h, M);
+    const bool ok = factor_W(tm, P, D, b, k, t, h, M, ukeep);
     // tangent, once per step: the background at the step start with its derivative along the
     // direction, and d/de of the Jacobian column d f / d a (see tangent_stage)
     Bg<Dual> bj;

@@ -71,4 +71,5 @@ def shim(tmp_path_factory):
     S.shim_solve_mode_tangent_records.argtypes = [CP, ctypes.c_void_p, CT, ctypes.c_double, ctypes.c_double, dp, dp,
                                                   dp, ctypes.c_int, dp, dp, ip]
     S.shim_output_tangent.argtypes = [CP, ctypes.c_void_p, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp, dp, dp]
+    S.shim_projected_output_tangent.argtypes = [CP, ctypes.c_void_p, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp]
     return S

@@ -199,3 +199,29 @@ int shim_solve_mode_tangent_records(const DiscoebCosmo* P, const DiscoebTangent*
     return R.status;
 }
 }
+
+// the 20 output fields at an output time and their tangents, after the RSA projection (the
+// arithmetic of the output stage of the forward and tangent kernels): state y with tangent yd
+// (the tangent at the moving output time), parameter tangent tn (may be null)
+extern "C" void shim_projected_output_tangent(const DiscoebCosmo* P, const DiscoebTangent* tn, double k, double tau,
+                                              const double* y, const double* yd, double* o, double* od)
+{
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    Dual fld[4];
+    const bool rsa = rsa_projection<Dual>(*P, tn, D, tau, k, y, yd, fld);
+    std::vector<double> yp(n), ypd(n);
+    for (int i = 0; i < n; ++i) {
+        double v = y[i], vd = yd[i];
+        if (rsa) {
+            const int s = rsa_slot(D, i);
+            if (s >= 0) { v = fld[s].v; vd = fld[s].d; }
+            else if (s == -1) { v = 0.0; vd = 0.0; }
+        }
+        yp[i] = v;
+        ypd[i] = vd;
+    }
+    Dual out[20];
+    output_vars<Dual>(*P, tn, D, k, yp.data(), ypd.data(), out);
+    for (int q = 0; q < 20; ++q) { o[q] = out[q].v; od[q] = out[q].d; }
+}

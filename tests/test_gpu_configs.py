@@ -149,9 +149,9 @@ def test_gpu_jacobian_equals_cpu_build_of_the_tangent_code(torch_cuda, shim):
                 f, col0 = np.zeros(n), np.zeros(n)
                 shim.shim_rhs(ctypes.byref(C), tau_out[j], p(yo[j]), k, -1, p(f), p(col0))
                 ydm = ydo[j] + f * tan["tau_out"][j]  # the state's tangent at the moving output time
-                o, od, r, rd = np.zeros(20), np.zeros(20), np.zeros(4), np.zeros(4)
-                shim.shim_output_tangent(ctypes.byref(C), ctypes.byref(tn), k, tau_out[j], p(yo[j]), p(ydm), p(o),
-                                         p(od), p(r), p(rd))
+                o, od = np.zeros(20), np.zeros(20)
+                shim.shim_projected_output_tangent(ctypes.byref(C), ctypes.byref(tn), k, tau_out[j], p(yo[j]),
+                                                   p(ydm), p(o), p(od))
                 np.testing.assert_allclose(o[4], y_gpu[i, j, 4], rtol=1e-6)
                 scale = np.abs(yd_gpu[d, :, j, 4]).max()
                 assert abs(od[4] - yd_gpu[d, i, j, 4]) <= 1e-6 * scale, (d, i, j, od[4], yd_gpu[d, i, j, 4])
