@@ -22,7 +22,8 @@ METHOD_RODAS5_DENSE_MIXED = 2
 
 STATUS_NAMES = {0: "ok", 1: "max_steps exceeded", 2: "non-finite state", 3: "step size underflow", 4: "singular",
                 5: "cosmology index out of range",
-                6: "aborted (a cooperating warp gave up waiting)"}
+                6: "aborted (a cooperating warp gave up waiting)",
+                7: "step record full (raise step_capacity)"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -167,6 +168,20 @@ def lib():
                                   ctypes.POINTER(DiscoebControl), ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_int32,
                                   vp, vp, vp, vp, vp, vp, vp]
         L.discoeb_jvp.restype = ctypes.c_int32
+        i32, i64 = ctypes.c_int32, ctypes.c_int64
+        CPp, CTp = ctypes.POINTER(DiscoebCosmo), ctypes.POINTER(DiscoebControl)
+        L.discoeb_step_record_doubles.argtypes = [i32, i32, i32]
+        L.discoeb_step_record_doubles.restype = i64
+        L.discoeb_fwd_record.argtypes = [vp, CPp, i32, CTp, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, i32, i32, vp, vp,
+                                         vp]
+        L.discoeb_fwd_record.restype = i32
+        L.discoeb_bwd_workspace_bytes.argtypes = [CPp, i32, i32]
+        L.discoeb_bwd_workspace_bytes.restype = i64
+        L.discoeb_bwd.argtypes = [vp, CPp, i32, vp, i32, vp, vp, vp, i32, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp,
+                                  i32, vp, i64, vp, vp]
+        L.discoeb_bwd.restype = i32
+        L.discoeb_bwd_contract.argtypes = [vp, i32, vp, i32, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp]
+        L.discoeb_bwd_contract.restype = i32
         L.discoeb_jvp_full.argtypes = L.discoeb_jvp.argtypes
         L.discoeb_jvp_full.restype = ctypes.c_int32
         L.discoeb_rhs.restype = ctypes.c_int32

@@ -368,16 +368,41 @@ def power_spectrum_jacobian(theta, *, on_failure="raise", return_stats=False, **
     return prob.kmodes, P, J
 
 
-def power_spectrum_function(**options):
+def power_spectrum_function(gradient="forward", **options):
     """A ``torch.autograd.Function`` mapping theta (float64[8], THETA_NAMES order) to
     P(k, a_out) (float64[K, nout]).
 
-    The forward pass runs ``discoeb_jvp`` (P and its full Jacobian in one launch) and keeps the
-    Jacobian; the backward pass contracts it with the incoming gradient, so ``torch.autograd``
-    (grad, vjp, jacrev, jacfwd through it) sees the exact discrete derivative.  ``options``
-    are those of JacobianProblem (k range, output scale factors, l_max, tolerances).
+    gradient="forward": the forward pass runs ``discoeb_jvp`` (P and its full Jacobian in one
+    launch) and keeps the Jacobian; the backward pass contracts it with the incoming gradient.
+    gradient="adjoint": the forward pass records the solve (``discoeb_fwd_record``), the backward
+    pass runs the discrete adjoint (``discoeb_bwd``): one reverse sweep per mode for any incoming
+    gradient.  Either way ``torch.autograd`` sees the exact derivative of the discrete solution.
+    ``options`` are those of JacobianProblem (k range, output scale factors, l_max, tolerances).
     """
     import torch
+
+    if gradient == "adjoint":
+        class PowerSpectrumAdjoint(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, theta):
+                if theta.shape != (len(THETA_NAMES),):
+                    raise ValueError(f"theta must have shape ({len(THETA_NAMES)},) in the order {THETA_NAMES}")
+                th = dict(zip(THETA_NAMES, theta.detach().to("cpu", torch.float64).tolist()))
+                prob = AdjointProblem(th, **options)
+                prob.launch_forward()
+                ctx.prob = prob
+                return torch.from_numpy(prob.forward_power()[0][0]).to(theta.device)
+
+            @staticmethod
+            def backward(ctx, grad_P):
+                prob = ctx.prob
+                prob.launch_backward(grad_P)
+                g = prob.gradient(grad_P.detach().to("cpu", torch.float64).numpy())[0]
+                return torch.from_numpy(g).to(grad_P.device)
+
+        return PowerSpectrumAdjoint
+    if gradient != "forward":
+        raise ValueError(f"gradient must be 'forward' or 'adjoint', not {gradient!r}")
 
     class PowerSpectrum(torch.autograd.Function):
         @staticmethod
@@ -511,3 +536,150 @@ class JacobianBatch:
             J[c, THETA_NAMES.index("n_s")] = P[c] * np.log(k / bg["k_p"])
             J[c, THETA_NAMES.index("ln10As")] = P[c]
         return P, J, stat[0].reshape(C, K), stat[1].reshape(C, K)
+
+
+class _ReverseMode:
+    """Reverse-mode gradients (discrete adjoint) for the modes of a JacobianProblem or a
+    JacobianBatch: ``launch_forward`` solves and records the accepted steps (discoeb_fwd_record),
+    ``launch_backward(grad_P)`` runs the reverse sweep from the cotangent of P(k) (discoeb_bwd)
+    and contracts the cotangents with the parameter tangents the prologue computed
+    (discoeb_bwd_contract); ``gradient`` returns dL/dtheta [C, 8] for L = sum grad_P * P.  One
+    reverse sweep per mode whatever the number of parameters (the reference's jax.grad through
+    diffeqsolve with DirectAdjoint, perturbations.py:904-925).
+
+    ``step_capacity``: accepted steps a mode's record holds (a mode that needs more stops with
+    DISCOEB_RECORD_FULL); ``checkpoint_every``: the record keeps every n-th step's start state
+    (the reverse sweep recomputes the steps in between: memory against a second forward pass).
+    """
+
+    def _reverse_init(self, step_capacity, checkpoint_every):
+        torch, dev = self.torch, self.device
+        M = self._C * self.K
+        rec = int(self.lib.discoeb_step_record_doubles(self.n, int(step_capacity), int(checkpoint_every)))
+        if rec <= 0:
+            raise ValueError("invalid step_capacity / checkpoint_every")
+        self.step_capacity, self.checkpoint_every = int(step_capacity), int(checkpoint_every)
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.d_rec = torch.empty((M, rec), **f64)
+        self.d_nacc = torch.empty(M, dtype=torch.int32, device=dev)
+        self.d_fstat = torch.empty((2, M), dtype=torch.int32, device=dev)
+        self.d_bstat = torch.empty(M, dtype=torch.int32, device=dev)
+        self.d_ybar = torch.zeros((M, self.nout, 20), **f64)
+        self.d_y0bar = torch.empty((M, self.n), **f64)
+        self.d_toutbar = torch.empty((M, self.nout), **f64)
+        self.d_pbar = torch.empty((M, 8), **f64)
+        self.tstride = max(bg[key].n for bg in self._bgs for key, _ in _TABLES)
+        self.d_tbar = torch.zeros((self._C, 8, self.tstride), **f64)
+        ws = int(self.lib.discoeb_bwd_workspace_bytes(ctypes.byref(self._host), M, self.checkpoint_every))
+        self.d_ws = torch.empty(max(ws // 8, 1), **f64)
+        self.d_thbar = torch.empty((self._C, len(ODE_DIRECTIONS)), **f64)
+        # primordial amplitude of every mode in launch order: P = amp * delta^2
+        k = np.tile(self.kmodes, self._C)
+        amp = np.concatenate([2 * np.pi**2 * bg["A_s"] * (self.kmodes / bg["k_p"]) ** (bg["n_s"] - 1)
+                              * self.kmodes**-3 for bg in self._bgs])
+        order = np.empty_like(self.inv)
+        order[self.inv] = np.arange(k.size)
+        self.d_amp = torch.from_numpy(np.ascontiguousarray(amp[order])).to(dev)
+
+    def launch_forward(self):
+        stream = self.torch.cuda.current_stream(self.device).cuda_stream
+        M = self._C * self.K
+        rc = self.lib.discoeb_fwd_record(self._cosmos_ptr, ctypes.byref(self._host), self._C, ctypes.byref(self.ctrl),
+                                         M, self._mc_ptr, self.d_k.data_ptr(), self.d_ts.data_ptr(),
+                                         self.d_y0.data_ptr(), self.d_sw.data_ptr(), self.nout,
+                                         self.d_tout.data_ptr(), self.d_out.data_ptr(), self.d_fstat[0].data_ptr(),
+                                         self.d_fstat[1].data_ptr(), self.step_capacity, self.checkpoint_every,
+                                         self.d_rec.data_ptr(), self.d_nacc.data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_fwd_record failed with code {rc}")
+
+    def forward_power(self, on_failure="raise"):
+        """(P [C, K, nout], status [C, K], nsteps [C, K]) of the recorded forward, caller order."""
+        C, K, nout, inv = self._C, self.K, self.nout, self.inv
+        y = self.d_out.cpu().numpy()[inv].reshape(C, K, nout, 20)
+        stat = self.d_fstat.cpu().numpy()[:, inv]
+        _check_status(stat[0], stat[1], np.tile(self.kmodes, C), on_failure)
+        amp = np.stack([2 * np.pi**2 * bg["A_s"] * (self.kmodes / bg["k_p"]) ** (bg["n_s"] - 1) * self.kmodes**-3
+                        for bg in self._bgs])
+        P = amp[:, :, None] * y[..., self.idx] ** 2
+        return P, stat[0].reshape(C, K), stat[1].reshape(C, K)
+
+    def launch_backward(self, grad_P):
+        """Reverse sweep from grad_P [C, K, nout] (or [K, nout] for one cosmology; numpy or a
+        device tensor, the caller's k order)."""
+        torch = self.torch
+        g = torch.as_tensor(grad_P, dtype=torch.float64).to(self.device).reshape(self._C * self.K, self.nout)
+        g = g[torch.as_tensor(np.argsort(self.inv), device=self.device)]  # launch order
+        delta = self.d_out[:, :, self.idx]
+        self.d_ybar.zero_()
+        self.d_ybar[:, :, self.idx] = 2.0 * g * self.d_amp[:, None] * delta  # dL/d delta of L = sum g * amp delta^2
+        self.d_tbar.zero_()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        M = self._C * self.K
+        rc = self.lib.discoeb_bwd(self._cosmos_ptr, ctypes.byref(self._host), self._C, self._mc_ptr, M,
+                                  self.d_k.data_ptr(), self.d_ts.data_ptr(), self.d_sw.data_ptr(), self.nout,
+                                  self.d_tout.data_ptr(), self.step_capacity, self.checkpoint_every,
+                                  self.d_rec.data_ptr(), self.d_nacc.data_ptr(), self.d_fstat[0].data_ptr(),
+                                  self.d_ybar.data_ptr(), self.d_y0bar.data_ptr(), self.d_toutbar.data_ptr(),
+                                  self.d_pbar.data_ptr(), self.d_tbar.data_ptr(), self.tstride,
+                                  self.d_ws.data_ptr(), self.d_ws.numel() * 8, self.d_bstat.data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_bwd failed with code {rc}")
+        rc = self.lib.discoeb_bwd_contract(self._cosmos_ptr, self._C, self._mc_ptr, M, self.n, self.nout,
+                                           self.d_tan.data_ptr(), len(ODE_DIRECTIONS), self.d_y0d.data_ptr(),
+                                           self.d_toutd.data_ptr(), self.d_y0bar.data_ptr(), self.d_toutbar.data_ptr(),
+                                           self.d_pbar.data_ptr(), self.d_tbar.data_ptr(), self.tstride,
+                                           self.d_thbar.data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_bwd_contract failed with code {rc}")
+
+    def gradient(self, grad_P, on_failure="raise"):
+        """dL/dtheta [C, 8] (THETA_NAMES order) of L = sum grad_P * P after launch_backward(grad_P):
+        the six solver directions from the reverse sweep, n_s and ln10As in closed form."""
+        st = self.d_bstat.cpu().numpy()[self.inv]
+        _check_status(st, np.zeros_like(st), np.tile(self.kmodes, self._C), on_failure)
+        th = self.d_thbar.cpu().numpy()
+        P = self.forward_power(on_failure="ignore")[0]
+        g = np.asarray(grad_P, dtype=np.float64).reshape(P.shape)
+        out = np.zeros((self._C, len(THETA_NAMES)))
+        for di, name in enumerate(ODE_DIRECTIONS):
+            out[:, THETA_NAMES.index(name)] = th[:, di]
+        for c, bg in enumerate(self._bgs):
+            out[c, THETA_NAMES.index("n_s")] = np.sum(g[c] * P[c] * np.log(self.kmodes / bg["k_p"])[:, None])
+            out[c, THETA_NAMES.index("ln10As")] = np.sum(g[c] * P[c])
+        return out
+
+
+class AdjointProblem(JacobianProblem, _ReverseMode):
+    """P(k) of one cosmology with reverse-mode gradients of scalar losses (the discrete adjoint):
+    the prologue and options of JacobianProblem, plus ``step_capacity`` and ``checkpoint_every``
+    (see _ReverseMode)."""
+
+    def __init__(self, theta, *, step_capacity=8192, checkpoint_every=16, **options):
+        JacobianProblem.__init__(self, theta, **options)
+        self._C, self._bgs, self._host, self._mc_ptr = 1, [self.bg], self.dc.host, None
+        self._cosmos_ptr = self.dc.struct.data_ptr()
+        self._reverse_init(step_capacity, checkpoint_every)
+
+
+class AdjointBatch(JacobianBatch, _ReverseMode):
+    """AdjointProblem for many cosmologies in one forward and one reverse launch (the options of
+    JacobianBatch, plus ``step_capacity`` and ``checkpoint_every``)."""
+
+    def __init__(self, thetas, *, step_capacity=8192, checkpoint_every=16, **options):
+        JacobianBatch.__init__(self, thetas, **options)
+        self.n = nvar_of(**{k: options.get(k, d) for k, d in (("lmaxg", 12), ("lmaxgp", 12), ("lmaxr", 17),
+                                                              ("lmaxnu", 17), ("nqmax", 5))})
+        self._C, self._bgs, self._host = self.C, self.bgs, self.dcs[0].host
+        self._mc_ptr, self._cosmos_ptr = self.d_mc.data_ptr(), self.d_cosmos.data_ptr()
+        self._reverse_init(step_capacity, checkpoint_every)
+
+
+def power_spectrum_gradient(theta, grad_P, **options):
+    """(k, P [K, nout], dL/dtheta [8]) for the scalar loss L = sum grad_P * P(k, a_out) by one
+    forward and one reverse sweep (AdjointProblem; options as JacobianProblem)."""
+    prob = AdjointProblem(theta, **options)
+    prob.launch_forward()
+    P = prob.forward_power()[0][0]
+    prob.launch_backward(np.asarray(grad_P, dtype=np.float64).reshape(P.shape))
+    return prob.kmodes, P, prob.gradient(grad_P)[0]

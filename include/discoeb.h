@@ -95,6 +95,7 @@ typedef struct {
 #define DISCOEB_BAD_INDEX 5 /* mode_cosmo[mode] outside [0, n_cosmo), or that cosmology's l_max / nq
                               * differ from cosmos[0]'s: the mode was not solved */
 #define DISCOEB_ABORTED 6   /* the solve stopped because a cooperating warp of the same mode gave up */
+#define DISCOEB_RECORD_FULL 7 /* discoeb_fwd_record: the mode took more accepted steps than its record holds */
 
 /* return codes of the entry points */
 #define DISCOEB_SUCCESS 0
@@ -163,6 +164,66 @@ int32_t discoeb_jvp_full(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cos
                          const double* y0, const double* y0_dot, const double* switch_tau, int32_t n_out,
                          const double* tau_out, const double* tau_out_dot, double* y_full, double* y_full_dot,
                          int32_t* status, int32_t* nsteps, void* stream);
+
+/* ---- Discrete adjoint (reverse mode) ----
+ * Replaces reverse-mode differentiation (jax.grad / jax.vjp) through diffeqsolve(...,
+ * adjoint=DirectAdjoint()) (src/discoeb/perturbations.py:904-925, :1059-1083): the exact
+ * vector-Jacobian product of the discrete Rodas5 solution with its accepted step sequence held
+ * fixed (the transpose of what discoeb_jvp computes), in one reverse sweep per mode whatever the
+ * number of parameters.  Two launches: discoeb_fwd_record solves forward and records the accepted
+ * steps (their end times, and the start state of every checkpoint_every-th step); discoeb_bwd
+ * runs the reverse sweep from the cotangent of the output fields, recomputing each segment of
+ * checkpoint_every steps from its checkpoint.  Start times and approximation switch times are
+ * held fixed, as forward-mode AD through the reference leaves them.
+ *
+ * Doubles of one mode's record: step_capacity step end times plus
+ * ceil(step_capacity / checkpoint_every) checkpoint states of nvar doubles. */
+int64_t discoeb_step_record_doubles(int32_t nvar, int32_t step_capacity, int32_t checkpoint_every);
+
+/* discoeb_fwd (same arguments; y_out20 may be NULL, whole states are not written) that also writes
+ * records [n_modes, discoeb_step_record_doubles(...)] and n_accepted [n_modes] (device).  A mode
+ * that takes more than step_capacity accepted steps stops with status DISCOEB_RECORD_FULL. */
+int32_t discoeb_fwd_record(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                           const DiscoebControl* ctrl, int32_t n_modes, const int32_t* mode_cosmo,
+                           const double* kmodes, const double* tau_start, const double* y0,
+                           const double* switch_tau, int32_t n_out, const double* tau_out, double* y_out20,
+                           int32_t* status, int32_t* nsteps, int32_t step_capacity, int32_t checkpoint_every,
+                           double* records, int32_t* n_accepted, void* stream);
+
+/* Device workspace of discoeb_bwd: one segment of checkpoint_every states per mode. */
+int64_t discoeb_bwd_workspace_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_modes, int32_t checkpoint_every);
+
+/* Reverse sweep of a recorded solve (the same cosmos, modes, start and switch times, output times,
+ * records, n_accepted and the forward's status; device arrays):
+ *   y_out20_bar [n_modes, n_out, 20]  cotangent of the output fields
+ *   y0_bar [n_modes, nvar]            cotangent of the initial states
+ *   tau_out_bar [n_modes, n_out]      cotangent of the output times (through y' = f at each one)
+ *   par_bar [n_modes, 8]              cotangents of grhom, Omegam, Omegab, OmegaDE, amnu, w0, wa, H0
+ *                                     (DiscoebTangent's scalar order)
+ *   table_bar [n_cosmo, 8, table_stride]  ADDED to (the caller zeroes it): cotangents of the knot
+ *                                     values xe_y, xe_S, cs2a_y, cs2a_S, logrhonu_y, logrhonu_S,
+ *                                     logpnu_y, logpnu_S (DiscoebTangent's table order), summed
+ *                                     over each cosmology's modes (atomically: equal to rounding
+ *                                     between runs); table_stride >= every table's knot count
+ *   workspace                         >= discoeb_bwd_workspace_bytes(...) bytes
+ *   status [n_modes]                  DISCOEB_OK, or the forward's status (NaN outputs) */
+int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                    const int32_t* mode_cosmo, int32_t n_modes, const double* kmodes, const double* tau_start,
+                    const double* switch_tau, int32_t n_out, const double* tau_out, int32_t step_capacity,
+                    int32_t checkpoint_every, const double* records, const int32_t* n_accepted,
+                    const int32_t* fwd_status, const double* y_out20_bar, double* y0_bar, double* tau_out_bar,
+                    double* par_bar, double* table_bar, int32_t table_stride, void* workspace, int64_t workspace_bytes,
+                    int32_t* status, void* stream);
+
+/* theta_bar [n_cosmo, n_dir] = the cotangents of discoeb_bwd contracted with n_dir parameter
+ * tangents (tangents_dev [n_cosmo, n_dir], y0_dot [n_dir, n_modes, nvar], tau_out_dot
+ * [n_cosmo, n_dir, n_out], the arrays discoeb_jvp takes): the gradient of a scalar loss with
+ * respect to those parameters, summed over each cosmology's modes (device arrays). */
+int32_t discoeb_bwd_contract(const DiscoebCosmo* cosmos_dev, int32_t n_cosmo, const int32_t* mode_cosmo,
+                             int32_t n_modes, int32_t nvar, int32_t n_out, const DiscoebTangent* tangents_dev,
+                             int32_t n_dir, const double* y0_dot, const double* tau_out_dot, const double* y0_bar,
+                             const double* tau_out_bar, const double* par_bar, const double* table_bar,
+                             int32_t table_stride, double* theta_bar, void* stream);
 
 /* RHS f(tau_i, y_i; k_i) of n_points states (compute_time_derivatives):
  *   y, f [n_points, nvar]; tau, kmodes [n_points]; regime < 0: approximation switches
