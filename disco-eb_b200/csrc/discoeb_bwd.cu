@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(32) bwd_kernel(
     const double* __restrict__ tau_out, int cap, int every, long long rec_doubles, const double* __restrict__ records,
     const int32_t* __restrict__ n_acc, const int32_t* __restrict__ fwd_status, double* seg,
     const double* __restrict__ ybar20, int mem_doubles, int adj_doubles, double* y0_bar, double* tau_out_bar,
-    double* par_bar, double* table_bar, int tstride, int32_t* status)
+    double* par_bar, double* table_bar, int tstride, int table_per_mode, int32_t* status)
 {
     extern __shared__ double smem[];
     const WarpTeam tm{(int)(threadIdx.x & 31)};
@@ -156,8 +156,8 @@ __global__ void __launch_bounds__(32) bwd_kernel(
     const double* rec = records + (size_t)mode * rec_doubles;
     bwd_mode(tm, *P, D, kmodes[mode], tau_start[mode], sw + 3 * mode, n_out, tau_out + (size_t)ci * n_out, rec,
              rec + cap, every, n_acc[mode], seg + (size_t)mode * every * n, ybar20 + (size_t)mode * n_out * 20, M, A,
-             y0_bar + (size_t)mode * n, tau_out_bar + (size_t)mode * n_out, table_bar + (size_t)ci * 8 * tstride,
-             tstride);
+             y0_bar + (size_t)mode * n, tau_out_bar + (size_t)mode * n_out,
+             table_bar + (size_t)(table_per_mode ? mode : ci) * 8 * tstride, tstride);
     for (int q = tm.lane; q < 8; q += 32) par_bar[(size_t)mode * 8 + q] = A.pb[X_GRHOM + q];
     if (tm.leader()) status[mode] = DISCOEB_OK;
 }
@@ -203,6 +203,46 @@ __global__ void __launch_bounds__(256) contract_kernel(
         __syncthreads();
     }
     if (threadIdx.x == 0) theta_bar[blockIdx.x] = red[0];
+}
+
+// theta_bar[m, d] for each mode on its own (its table cotangents in rows [m, 8, tstride]): one
+// warp per (mode, direction)
+__global__ void __launch_bounds__(128) contract_mode_kernel(
+    const DiscoebCosmo* __restrict__ cosmos, int n_cosmo, const int32_t* __restrict__ mode_cosmo, int n_modes, int n,
+    int n_out, const DiscoebTangent* __restrict__ tangents, int n_dir, const double* __restrict__ y0_dot,
+    const double* __restrict__ tau_out_dot, const double* __restrict__ y0_bar, const double* __restrict__ tau_out_bar,
+    const double* __restrict__ par_bar, const double* __restrict__ table_bar, int tstride, double* theta_bar)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (long long)n_modes * n_dir) return;
+    const int m = (int)(w / n_dir), d = (int)(w - (long long)m * n_dir);
+    const int c = mode_cosmo ? mode_cosmo[m] : 0;
+    if (c < 0 || c >= n_cosmo) {
+        if (lane == 0) theta_bar[w] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    const DiscoebTangent& tn = tangents[(size_t)c * n_dir + d];
+    double acc = 0.0;
+    const double* yb = y0_bar + (size_t)m * n;
+    const double* yd = y0_dot + ((size_t)d * n_modes + m) * n;
+    for (int i = lane; i < n; i += 32) acc += yb[i] * yd[i];
+    const double* td = tau_out_dot + ((size_t)c * n_dir + d) * n_out;
+    for (int j = lane; j < n_out; j += 32) acc += tau_out_bar[(size_t)m * n_out + j] * td[j];
+    const double sc[8] = {tn.grhom, tn.Omegam, tn.Omegab, tn.OmegaDE, tn.amnu, tn.w0, tn.wa, tn.H0};
+    if (lane < 8) acc += par_bar[(size_t)m * 8 + lane] * sc[lane];
+    const DiscoebCosmo& P = cosmos[c];
+    const double* rows[8] = {tn.xe_y, tn.xe_S, tn.cs2a_y, tn.cs2a_S, tn.logrhonu_y, tn.logrhonu_S, tn.logpnu_y,
+                             tn.logpnu_S};
+    const int nk[4] = {P.xe_loga.n_knots, P.cs2a_loga.n_knots, P.logrhonu_loga.n_knots, P.logpnu_loga.n_knots};
+    for (int r = 0; r < 8; ++r) {
+        if (!rows[r]) continue;
+        const int kk = nk[r >> 1] < tstride ? nk[r >> 1] : tstride;
+        const double* tb = table_bar + ((size_t)m * 8 + r) * tstride;
+        for (int i = lane; i < kk; i += 32) acc += tb[i] * rows[r][i];
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) theta_bar[w] = acc;
 }
 
 int validate_cosmo_b(const DiscoebCosmo* c)
@@ -269,8 +309,8 @@ int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
                     const double* switch_tau, int32_t n_out, const double* tau_out, int32_t step_capacity,
                     int32_t checkpoint_every, const double* records, const int32_t* n_accepted,
                     const int32_t* fwd_status, const double* y_out20_bar, double* y0_bar, double* tau_out_bar,
-                    double* par_bar, double* table_bar, int32_t table_stride, void* workspace, int64_t workspace_bytes,
-                    int32_t* status, void* stream)
+                    double* par_bar, double* table_bar, int32_t table_stride, int32_t table_per_mode, void* workspace,
+                    int64_t workspace_bytes, int32_t* status, void* stream)
 {
     int rc = validate_cosmo_b(cosmo0_host);
     if (rc) return rc;
@@ -299,7 +339,7 @@ int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
     bwd_kernel<<<n_modes, 32, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
         cosmos_dev, n_cosmo, mode_cosmo, n_modes, kmodes, tau_start, switch_tau, n_out, tau_out, step_capacity,
         checkpoint_every, rec, records, n_accepted, fwd_status, static_cast<double*>(workspace), y_out20_bar, mem, adj,
-        y0_bar, tau_out_bar, par_bar, table_bar, table_stride, status);
+        y0_bar, tau_out_bar, par_bar, table_bar, table_stride, table_per_mode ? 1 : 0, status);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 
@@ -307,12 +347,21 @@ int32_t discoeb_bwd_contract(const DiscoebCosmo* cosmos_dev, int32_t n_cosmo, co
                              int32_t n_modes, int32_t nvar, int32_t n_out, const DiscoebTangent* tangents_dev,
                              int32_t n_dir, const double* y0_dot, const double* tau_out_dot, const double* y0_bar,
                              const double* tau_out_bar, const double* par_bar, const double* table_bar,
-                             int32_t table_stride, double* theta_bar, void* stream)
+                             int32_t table_stride, int32_t per_mode, double* theta_bar, void* stream)
 {
     if (!cosmos_dev || n_cosmo < 1 || n_modes < 0 || nvar < 1 || n_out < 1 || !tangents_dev || n_dir < 1 || !y0_dot ||
         !tau_out_dot || !y0_bar || !tau_out_bar || !par_bar || !table_bar || table_stride < 1 || !theta_bar)
         return DISCOEB_EINVAL;
     if ((long long)n_cosmo * n_dir > 0x7fffffffLL) return DISCOEB_EINVAL;
+    if (per_mode) {
+        const long long threads = (long long)n_modes * n_dir * 32;
+        if (threads / 128 >= 0x7fffffffLL) return DISCOEB_EINVAL;
+        if (n_modes == 0) return DISCOEB_SUCCESS;
+        contract_mode_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+            cosmos_dev, n_cosmo, mode_cosmo, n_modes, nvar, n_out, tangents_dev, n_dir, y0_dot, tau_out_dot, y0_bar,
+            tau_out_bar, par_bar, table_bar, table_stride, theta_bar);
+        return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+    }
     contract_kernel<<<n_cosmo * n_dir, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         cosmos_dev, n_cosmo, mode_cosmo, n_modes, nvar, n_out, tangents_dev, n_dir, y0_dot, tau_out_dot, y0_bar,
         tau_out_bar, par_bar, table_bar, table_stride, theta_bar);

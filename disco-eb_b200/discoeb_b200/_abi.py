@@ -178,9 +178,10 @@ def lib():
         L.discoeb_bwd_workspace_bytes.argtypes = [CPp, i32, i32]
         L.discoeb_bwd_workspace_bytes.restype = i64
         L.discoeb_bwd.argtypes = [vp, CPp, i32, vp, i32, vp, vp, vp, i32, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp,
-                                  i32, vp, i64, vp, vp]
+                                  i32, i32, vp, i64, vp, vp]
         L.discoeb_bwd.restype = i32
-        L.discoeb_bwd_contract.argtypes = [vp, i32, vp, i32, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp]
+        L.discoeb_bwd_contract.argtypes = [vp, i32, vp, i32, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, i32, i32, vp,
+                                           vp]
         L.discoeb_bwd_contract.restype = i32
         L.discoeb_jvp_full.argtypes = L.discoeb_jvp.argtypes
         L.discoeb_jvp_full.restype = ctypes.c_int32

@@ -621,17 +621,64 @@ class _ReverseMode:
                                   self.d_tout.data_ptr(), self.step_capacity, self.checkpoint_every,
                                   self.d_rec.data_ptr(), self.d_nacc.data_ptr(), self.d_fstat[0].data_ptr(),
                                   self.d_ybar.data_ptr(), self.d_y0bar.data_ptr(), self.d_toutbar.data_ptr(),
-                                  self.d_pbar.data_ptr(), self.d_tbar.data_ptr(), self.tstride,
+                                  self.d_pbar.data_ptr(), self.d_tbar.data_ptr(), self.tstride, 0,
                                   self.d_ws.data_ptr(), self.d_ws.numel() * 8, self.d_bstat.data_ptr(), stream)
         if rc != 0:
             raise RuntimeError(f"discoeb_bwd failed with code {rc}")
         rc = self.lib.discoeb_bwd_contract(self._cosmos_ptr, self._C, self._mc_ptr, M, self.n, self.nout,
                                            self.d_tan.data_ptr(), len(ODE_DIRECTIONS), self.d_y0d.data_ptr(),
                                            self.d_toutd.data_ptr(), self.d_y0bar.data_ptr(), self.d_toutbar.data_ptr(),
-                                           self.d_pbar.data_ptr(), self.d_tbar.data_ptr(), self.tstride,
+                                           self.d_pbar.data_ptr(), self.d_tbar.data_ptr(), self.tstride, 0,
                                            self.d_thbar.data_ptr(), stream)
         if rc != 0:
             raise RuntimeError(f"discoeb_bwd_contract failed with code {rc}")
+
+    def launch_jacobian_rows(self, out_index=-1):
+        """Reverse sweeps whose cotangent is each mode's own P at output out_index: every mode's
+        row of dP(k, z)/dtheta in one launch (the per-mode table cotangents are kept apart)."""
+        torch = self.torch
+        M = self._C * self.K
+        if getattr(self, "d_tbar_mode", None) is None:
+            f64 = dict(dtype=torch.float64, device=self.device)
+            self.d_tbar_mode = torch.zeros((M, 8, self.tstride), **f64)
+            self.d_thbar_mode = torch.empty((M, len(ODE_DIRECTIONS)), **f64)
+        j = out_index % self.nout
+        self.d_ybar.zero_()
+        self.d_ybar[:, j, self.idx] = 2.0 * self.d_amp * self.d_out[:, j, self.idx]
+        self.d_tbar_mode.zero_()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        rc = self.lib.discoeb_bwd(self._cosmos_ptr, ctypes.byref(self._host), self._C, self._mc_ptr, M,
+                                  self.d_k.data_ptr(), self.d_ts.data_ptr(), self.d_sw.data_ptr(), self.nout,
+                                  self.d_tout.data_ptr(), self.step_capacity, self.checkpoint_every,
+                                  self.d_rec.data_ptr(), self.d_nacc.data_ptr(), self.d_fstat[0].data_ptr(),
+                                  self.d_ybar.data_ptr(), self.d_y0bar.data_ptr(), self.d_toutbar.data_ptr(),
+                                  self.d_pbar.data_ptr(), self.d_tbar_mode.data_ptr(), self.tstride, 1,
+                                  self.d_ws.data_ptr(), self.d_ws.numel() * 8, self.d_bstat.data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_bwd failed with code {rc}")
+        rc = self.lib.discoeb_bwd_contract(self._cosmos_ptr, self._C, self._mc_ptr, M, self.n, self.nout,
+                                           self.d_tan.data_ptr(), len(ODE_DIRECTIONS), self.d_y0d.data_ptr(),
+                                           self.d_toutd.data_ptr(), self.d_y0bar.data_ptr(), self.d_toutbar.data_ptr(),
+                                           self.d_pbar.data_ptr(), self.d_tbar_mode.data_ptr(), self.tstride, 1,
+                                           self.d_thbar_mode.data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_bwd_contract failed with code {rc}")
+        self._rows_out = j
+
+    def jacobian_rows(self, on_failure="raise"):
+        """J [C, 8, K]: dP(k, z)/dtheta at the output of the last launch_jacobian_rows (THETA_NAMES
+        order, caller's k order; n_s and ln10As in closed form)."""
+        st = self.d_bstat.cpu().numpy()[self.inv]
+        _check_status(st, np.zeros_like(st), np.tile(self.kmodes, self._C), on_failure)
+        rows = self.d_thbar_mode.cpu().numpy()[self.inv].reshape(self._C, self.K, len(ODE_DIRECTIONS))
+        P = self.forward_power(on_failure="ignore")[0][:, :, self._rows_out]
+        J = np.zeros((self._C, len(THETA_NAMES), self.K))
+        for di, name in enumerate(ODE_DIRECTIONS):
+            J[:, THETA_NAMES.index(name)] = rows[:, :, di]
+        for c, bg in enumerate(self._bgs):
+            J[c, THETA_NAMES.index("n_s")] = P[c] * np.log(self.kmodes / bg["k_p"])
+            J[c, THETA_NAMES.index("ln10As")] = P[c]
+        return J
 
     def gradient(self, grad_P, on_failure="raise"):
         """dL/dtheta [C, 8] (THETA_NAMES order) of L = sum grad_P * P after launch_backward(grad_P):

@@ -205,6 +205,8 @@ int64_t discoeb_bwd_workspace_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_m
  *                                     logpnu_y, logpnu_S (DiscoebTangent's table order), summed
  *                                     over each cosmology's modes (atomically: equal to rounding
  *                                     between runs); table_stride >= every table's knot count
+ *   table_per_mode                    nonzero: table_bar is [n_modes, 8, table_stride], one block
+ *                                     of rows per mode (the per-mode gradients of a Jacobian row) 
  *   workspace                         >= discoeb_bwd_workspace_bytes(...) bytes
  *   status [n_modes]                  DISCOEB_OK, or the forward's status (NaN outputs) */
 int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
@@ -212,18 +214,20 @@ int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
                     const double* switch_tau, int32_t n_out, const double* tau_out, int32_t step_capacity,
                     int32_t checkpoint_every, const double* records, const int32_t* n_accepted,
                     const int32_t* fwd_status, const double* y_out20_bar, double* y0_bar, double* tau_out_bar,
-                    double* par_bar, double* table_bar, int32_t table_stride, void* workspace, int64_t workspace_bytes,
-                    int32_t* status, void* stream);
+                    double* par_bar, double* table_bar, int32_t table_stride, int32_t table_per_mode, void* workspace,
+                    int64_t workspace_bytes, int32_t* status, void* stream);
 
 /* theta_bar [n_cosmo, n_dir] = the cotangents of discoeb_bwd contracted with n_dir parameter
  * tangents (tangents_dev [n_cosmo, n_dir], y0_dot [n_dir, n_modes, nvar], tau_out_dot
  * [n_cosmo, n_dir, n_out], the arrays discoeb_jvp takes): the gradient of a scalar loss with
- * respect to those parameters, summed over each cosmology's modes (device arrays). */
+ * respect to those parameters, summed over each cosmology's modes (device arrays).  per_mode
+ * nonzero (table_bar per mode, as discoeb_bwd's table_per_mode): theta_bar [n_modes, n_dir], each
+ * mode's own gradient (a row of dP(k)/dtheta when the cotangent is that mode's output). */
 int32_t discoeb_bwd_contract(const DiscoebCosmo* cosmos_dev, int32_t n_cosmo, const int32_t* mode_cosmo,
                              int32_t n_modes, int32_t nvar, int32_t n_out, const DiscoebTangent* tangents_dev,
                              int32_t n_dir, const double* y0_dot, const double* tau_out_dot, const double* y0_bar,
                              const double* tau_out_bar, const double* par_bar, const double* table_bar,
-                             int32_t table_stride, double* theta_bar, void* stream);
+                             int32_t table_stride, int32_t per_mode, double* theta_bar, void* stream);
 
 /* RHS f(tau_i, y_i; k_i) of n_points states (compute_time_derivatives):
  *   y, f [n_points, nvar]; tau, kmodes [n_points]; regime < 0: approximation switches

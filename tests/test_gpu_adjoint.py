@@ -43,6 +43,22 @@ def test_gpu_adjoint_equals_contracted_forward_jacobian(torch_cuda, every):
     np.testing.assert_allclose(g, expect, rtol=1e-8, atol=1e-12 * np.abs(expect).max())
 
 
+def test_gpu_adjoint_jacobian_rows_equal_forward_jacobian(torch_cuda):
+    # one reverse sweep per mode with that mode's P(k, z = 0) as the cotangent: the whole
+    # Jacobian dP(k, z=0)/dtheta (the gradient configuration) row by row
+    from discoeb_b200.gradients import AdjointProblem, JacobianProblem
+    kw = dict(aexp_out=A4, kmin=1e-4, kmax=10.0, num_k=24, rtol=1e-5, atol=1e-8, **L143)
+    jp = JacobianProblem(THETA, **kw)
+    jp.launch()
+    P, J, _, _ = jp.result()
+    ap = AdjointProblem(THETA, **kw)
+    ap.launch_forward()
+    ap.launch_jacobian_rows(out_index=-1)
+    Ja = ap.jacobian_rows()[0]
+    scale = np.abs(J[:, :, -1]).max(axis=1, keepdims=True)
+    np.testing.assert_array_less(np.abs(Ja - J[:, :, -1]), 1e-8 * scale + 1e-300)
+
+
 def test_gpu_adjoint_matches_central_differences(torch_cuda):
     """dL/dtheta of L = sum w P against central differences of step 1e-4 |theta_i| of the whole
     pipeline at rtol 1e-10, with the start times, switch times and Recfast steps held at the base
