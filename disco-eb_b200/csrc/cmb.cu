@@ -120,6 +120,9 @@ __device__ void assemble_sources(const DiscoebCosmo& P, const SrcPar<T>& sp, con
     out[DISCOEB_SRC_S2] = gvis * (0.25 * deltag + 2.0 * alphaprime + pol / 16.0 + (thetabprime + 3.0 / 16.0 * polpp) / k2);
     out[DISCOEB_SRC_S3] = gvisprime * (alpha + (thetab + 3.0 / 8.0 * polp) / k2);
     out[DISCOEB_SRC_S4] = gvispprime * 3.0 / 16.0 * pol / k2;
+    // E-mode polarisation source (3/4) g Pi of Zaldarriaga & Seljak (1997), whose Pi is a quarter
+    // of pol (the reference's temperature terms Pi / 16, 3 Pi'' / 16 are theirs with that Pi)
+    out[DISCOEB_SRC_E] = gvis * 3.0 / 16.0 * pol;
     out[DISCOEB_SRC_POTENTIAL] = eta + alphaprime;
     out[DISCOEB_SRC_ALPHA] = alpha;
     out[DISCOEB_SRC_ALPHAPRIME] = alphaprime;
@@ -400,7 +403,8 @@ __device__ inline double cell_weight(int i, int n_modes, const double* __restric
 
 __global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __restrict__ kmodes, int n_ell,
                                                    const double* __restrict__ theta, double n_s, double k_p,
-                                                   double* cell, bool d_n_s = false)
+                                                   double* cell, bool d_n_s = false,
+                                                   const double* __restrict__ theta_b = nullptr)
 {
     __shared__ double w[kCellChunk];
     __shared__ double part[8][32];
@@ -418,7 +422,8 @@ __global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __
 #pragma unroll 4
             for (int j = wy; j < cn; j += 8) {
                 const double th = theta[(size_t)(c0 + j) * n_ell + l];
-                acc += w[j] * (th * th);
+                const double tb = theta_b ? theta_b[(size_t)(c0 + j) * n_ell + l] : th;  // cross spectrum
+                acc += w[j] * (th * tb);
             }
         }
     }
@@ -429,6 +434,54 @@ __global__ void __launch_bounds__(256) cell_kernel(int n_modes, const double* __
         for (int q = 0; q < 8; ++q) sum += part[q][lx];
         cell[l] = sum;
     }
+}
+
+// ------------------------------------------------------------------------------------------
+// E-mode line of sight: Theta_E,l(k) = sqrt((l+2)!/(l-2)!) int S_E(k, tau) j_l(x) / x^2 dtau,
+// x = k (tau0 - tau) (Zaldarriaga & Seljak 1997).  Below kELSwitch: the FFTLog integral of
+// S_E / chi^2 (chi held >= 1 Mpc: S_E ~ 0 today, where 1/chi^2 diverges) times the factor / k^2.
+// From kELSwitch on, where that integral's absolute FFTLog error times l^2 / k^2 would swamp the
+// signal: j_l / x^2 = [j_{l-2} / (2l-1) + j_l (1/(2l-1) + 1/(2l+3)) + j_{l+2} / (2l+3)] / (2l+1)
+// (from j_{l-1} + j_{l+1} = (2l+1) j_l / x), i.e. the FFTLog integrals of S_E itself at l - 2, l,
+// l + 2 with positive weights (no cancellation).  Below l = 4 the recurrence would need
+// l - 2 < 2, outside the FFTLog's convergence strip at bias -1.1.
+constexpr int kELSwitch = 8;
+
+__device__ __forceinline__ double e_factor(int l)
+{
+    return l >= 2 ? sqrt((l + 2.0) * (l + 1.0) * l * (l - 1.0)) : 0.0;
+}
+
+__global__ void e_source_kernel(int n_modes, int n_tau, const double* __restrict__ tau, double tau0,
+                                const double* __restrict__ S, double* out)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_modes * n_tau) return;
+    const int j = (int)(t % n_tau);
+    const double chi = fmax(tau0 - tau[j], 1.0);
+    out[t] = S[t] / (chi * chi);
+}
+
+// theta[r, l] for l < nlo from the direct integrals th_lo [rows, nlo]
+__global__ void e_low_kernel(int rows, int n_ell, int nlo, const double* __restrict__ k,
+                             const double* __restrict__ th_lo, double* theta)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)rows * nlo) return;
+    const int r = (int)(t / nlo), l = (int)(t - (long long)r * nlo);
+    theta[(size_t)r * n_ell + l] = th_lo[t] * e_factor(l) / (k[r] * k[r]);
+}
+
+// theta[r, l] for nlo <= l < n_ell from the integrals of S_E th [rows, n_ell + 2] by the recurrence
+__global__ void e_high_kernel(int rows, int n_ell, int nlo, const double* __restrict__ th, double* theta)
+{
+    const int span = n_ell - nlo;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (span <= 0 || t >= (long long)rows * span) return;
+    const int r = (int)(t / span), l = nlo + (int)(t - (long long)r * span);
+    const double* row = th + (size_t)r * (n_ell + 2);
+    const double a = 2.0 * l + 1.0, cm = 1.0 / (a * (2.0 * l - 1.0)), cp = 1.0 / (a * (2.0 * l + 3.0));
+    theta[(size_t)r * n_ell + l] = e_factor(l) * (cm * row[l - 2] + (cm + cp) * row[l] + cp * row[l + 2]);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -999,6 +1052,62 @@ int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const
     if (n_modes < 2 || n_ell < 1 || !kmodes || !theta || !cell) return DISCOEB_EINVAL;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     cell_kernel<<<(n_ell + 31) / 32, 256, 0, s>>>(n_modes, kmodes, n_ell, theta, n_s, k_p, cell);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int32_t discoeb_cell_cross(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta_a,
+                           const double* theta_b, double n_s, double k_p, double* cell, void* stream)
+{
+    if (n_modes < 2 || n_ell < 1 || !kmodes || !theta_a || !theta_b || !cell) return DISCOEB_EINVAL;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    cell_kernel<<<(n_ell + 31) / 32, 256, 0, s>>>(n_modes, kmodes, n_ell, theta_a, n_s, k_p, cell, false, theta_b);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+static int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
+
+int64_t discoeb_los_e_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
+                                      int32_t n_k_dense)
+{
+    if (ellmax < 0 || ellmax > 0x7ffffff0) return DISCOEB_EINVAL;
+    const int64_t b = discoeb_los_workspace_bytes(n_modes, n_tau, ellmax + 2, n_fftlog, n_k_dense);
+    if (b < 0) return b;
+    const int64_t rows = n_k_dense > 0 ? n_k_dense : n_modes;
+    return align256((int64_t)n_modes * n_tau * 8) + align256(rows * (ellmax + 3) * 8) + b;
+}
+
+int32_t discoeb_los_e(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S_E,
+                      double tau0, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, void* workspace,
+                      int64_t workspace_bytes, double* theta, double* kmodes_out, void* stream)
+{
+    if (n_modes < 2 || n_tau < 3 || ellmax < 0 || n_fftlog < 2 || n_k_dense < 0 || n_k_dense == 1)
+        return DISCOEB_EINVAL;
+    if (!kmodes || !tau || !S_E || !workspace || !theta || !kmodes_out) return DISCOEB_EINVAL;
+    if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return DISCOEB_EINVAL;
+    const int64_t need = discoeb_los_e_workspace_bytes(n_modes, n_tau, ellmax, n_fftlog, n_k_dense);
+    if (need < 0) return (int32_t)need;
+    if (workspace_bytes < need) return DISCOEB_EINVAL;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int rows = n_k_dense > 0 ? n_k_dense : n_modes;
+    const int n_ell = ellmax + 1, nlo = n_ell < kELSwitch ? n_ell : kELSwitch;
+    char* ws = static_cast<char*>(workspace);
+    double* Sx = reinterpret_cast<double*>(ws);
+    const int64_t o1 = align256((int64_t)n_modes * n_tau * 8);
+    double* th = reinterpret_cast<double*>(ws + o1);
+    const int64_t o2 = o1 + align256((int64_t)rows * (ellmax + 3) * 8);
+    const long long pts = (long long)n_modes * n_tau;
+    // l < nlo: S_E / chi^2
+    e_source_kernel<<<blocks_for(pts, 256), 256, 0, s>>>(n_modes, n_tau, tau, tau0, S_E, Sx);
+    int32_t rc = los_forward(n_modes, kmodes, n_tau, tau, Sx, tau0, nlo - 1, n_fftlog, n_k_dense, ws + o2,
+                             workspace_bytes - o2, th, kmodes_out, stream);
+    if (rc != DISCOEB_SUCCESS) return rc;
+    e_low_kernel<<<blocks_for((long long)rows * nlo, 256), 256, 0, s>>>(rows, n_ell, nlo, kmodes_out, th, theta);
+    if (n_ell > nlo) {  // l >= nlo: S_E at l - 2, l, l + 2
+        rc = los_forward(n_modes, kmodes, n_tau, tau, S_E, tau0, ellmax + 2, n_fftlog, n_k_dense, ws + o2,
+                         workspace_bytes - o2, th, kmodes_out, stream);
+        if (rc != DISCOEB_SUCCESS) return rc;
+        e_high_kernel<<<blocks_for((long long)rows * (n_ell - nlo), 256), 256, 0, s>>>(rows, n_ell, nlo, th, theta);
+    }
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 

@@ -183,6 +183,12 @@ def lib():
         L.discoeb_bwd_contract.argtypes = [vp, i32, vp, i32, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, i32, i32, vp,
                                            vp]
         L.discoeb_bwd_contract.restype = i32
+        L.discoeb_los_e_workspace_bytes.argtypes = [i32, i32, i32, i32, i32]
+        L.discoeb_los_e_workspace_bytes.restype = i64
+        L.discoeb_los_e.argtypes = [i32, vp, i32, vp, vp, ctypes.c_double, i32, i32, i32, vp, i64, vp, vp, vp]
+        L.discoeb_los_e.restype = i32
+        L.discoeb_cell_cross.argtypes = [i32, vp, i32, vp, vp, ctypes.c_double, ctypes.c_double, vp, vp]
+        L.discoeb_cell_cross.restype = i32
         L.discoeb_jvp_full.argtypes = L.discoeb_jvp.argtypes
         L.discoeb_jvp_full.restype = ctypes.c_int32
         L.discoeb_rhs.restype = ctypes.c_int32

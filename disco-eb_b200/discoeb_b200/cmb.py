@@ -24,7 +24,7 @@ BG_FIELDS = ("a", "aprimeoa", "rhonu", "rho_Q", "w_Q", "opac", "opacprime", "gvi
              "optical_depth")
 SRC_FIELDS = ("S", "S1", "S2", "S3", "S4", "potential", "alpha", "alphaprime", "alphapprime", "hprime", "etaprime",
               "aprimeoaprime", "polarization_term", "polarization_termprime", "polarization_termpprime", "drhonu",
-              "dpnu", "fnu", "shearnu", "rho_nu_prime", "shear_nu_prime", "thetabprime")
+              "dpnu", "fnu", "shearnu", "rho_nu_prime", "shear_nu_prime", "thetabprime", "E")
 
 
 def _device(device):
@@ -116,11 +116,16 @@ def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmax
     return {name: fields[i] for i, name in enumerate(SRC_FIELDS)}
 
 
-def compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0, device=None):
+def compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0, device=None, kind="T"):
     """Theta_l(k) by FFTLog line-of-sight integration (cmb.py:680-835).
 
+    ``kind="T"``: the temperature multipoles of the source S (the reference's path); ``kind="E"``:
+    the E-mode multipoles sqrt((l+2)!/(l-2)!) int S_E j_l(x) / x^2 dtau of the E source
+    (``compute_sources(...)["E"]``; discoeb_los_e, no counterpart in the reference).
     Returns ``(theta [K', ellmax+1], kmodes [K'])`` as device tensors (K' = n_k_dense if > 0).
     """
+    if kind not in ("T", "E"):
+        raise ValueError(f"kind must be 'T' or 'E', not {kind!r}")
     torch, device = _device(device)
     lib = _abi.lib()
     f64 = dict(dtype=torch.float64, device=device)
@@ -133,7 +138,9 @@ def compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0,
     K, T = d_S.shape
     if d_k.shape[0] != K or d_tau.shape[0] != T:
         raise ValueError("S must have shape [len(kmodes), len(tau)]")
-    nb = lib.discoeb_los_workspace_bytes(K, T, int(ellmax), int(n_fftlog), int(n_k_dense))
+    size_fn, entry = ((lib.discoeb_los_workspace_bytes, lib.discoeb_los) if kind == "T" else
+                      (lib.discoeb_los_e_workspace_bytes, lib.discoeb_los_e))
+    nb = size_fn(K, T, int(ellmax), int(n_fftlog), int(n_k_dense))
     if nb < 0:
         raise ValueError(f"invalid sizes for the line-of-sight integral (code {nb})")
     ws = torch.empty(int(nb) // 8 + 32, dtype=torch.float64, device=device)
@@ -143,26 +150,34 @@ def compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0,
     stream = torch.cuda.current_stream(device).cuda_stream
     base = ws.data_ptr()
     aligned = (base + 255) // 256 * 256
-    rc = lib.discoeb_los(K, d_k.data_ptr(), T, d_tau.data_ptr(), d_S.data_ptr(), float(tau0), int(ellmax),
-                         int(n_fftlog), int(n_k_dense), aligned, int(nb), theta.data_ptr(), k_out.data_ptr(), stream)
+    rc = entry(K, d_k.data_ptr(), T, d_tau.data_ptr(), d_S.data_ptr(), float(tau0), int(ellmax), int(n_fftlog),
+               int(n_k_dense), aligned, int(nb), theta.data_ptr(), k_out.data_ptr(), stream)
     if rc != 0:
-        raise RuntimeError(f"discoeb_los failed with code {rc}")
+        raise RuntimeError(f"line-of-sight integral ({kind}) failed with code {rc}")
     return theta, k_out
 
 
-def compute_Cell(theta_ell, kmodes, n_s, k_p, device=None):
-    """C_l = int d ln k (k/k_p)^(n_s-1) Theta_l^2, trapezoid (cmb.py:838-873); device tensor."""
+def compute_Cell(theta_ell, kmodes, n_s, k_p, device=None, theta_ell_b=None):
+    """C_l = int d ln k (k/k_p)^(n_s-1) Theta_l^2, trapezoid (cmb.py:838-873); device tensor.
+    ``theta_ell_b``: the cross spectrum int d ln k (k/k_p)^(n_s-1) Theta_l Theta^b_l (C_l^TE from
+    the T and E multipoles; discoeb_cell_cross)."""
     torch, device = _device(device)
     lib = _abi.lib()
     f64 = dict(dtype=torch.float64, device=device)
-    th = theta_ell if isinstance(theta_ell, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(theta_ell))
-    th = th.to(**f64).contiguous()
-    kk = kmodes if isinstance(kmodes, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(kmodes))
-    kk = kk.to(**f64).contiguous()
+    as_dev = lambda a: (a if isinstance(a, torch.Tensor) else torch.from_numpy(  # noqa: E731
+        np.ascontiguousarray(a))).to(**f64).contiguous()
+    th, kk = as_dev(theta_ell), as_dev(kmodes)
     K, L = th.shape
     cell = torch.empty(L, **f64)
-    rc = lib.discoeb_cell(K, kk.data_ptr(), L, th.data_ptr(), float(n_s), float(k_p), cell.data_ptr(),
-                          torch.cuda.current_stream(device).cuda_stream)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    if theta_ell_b is None:
+        rc = lib.discoeb_cell(K, kk.data_ptr(), L, th.data_ptr(), float(n_s), float(k_p), cell.data_ptr(), stream)
+    else:
+        tb = as_dev(theta_ell_b)
+        if tuple(tb.shape) != (K, L):
+            raise ValueError("theta_ell_b must have the shape of theta_ell")
+        rc = lib.discoeb_cell_cross(K, kk.data_ptr(), L, th.data_ptr(), tb.data_ptr(), float(n_s), float(k_p),
+                                    cell.data_ptr(), stream)
     if rc != 0:
         raise RuntimeError(f"discoeb_cell failed with code {rc}")
     return cell
@@ -224,12 +239,17 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
                                             n_fftlog=16384, lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3,
                                             num_thermo=1024, rtol=1e-4, atol=1e-4, max_steps=2048,
                                             k_sampling_method="camb", aexp_out=None, device=None,
-                                            return_intermediates=False):
+                                            return_intermediates=False, spectra=("TT",)):
     """C_l^TT of a cosmology (cmb.py:931-1090): background (host), full perturbation solve,
     sources, FFTLog line of sight and C_l on the GPU, large arrays never leaving the device.
 
-    Returns ``(Cell [ellmax+1] numpy, param)`` like the reference.
+    Returns ``(Cell [ellmax+1] numpy, param)`` like the reference.  ``spectra`` naming more than TT
+    (any of "TT", "TE", "EE"; the reference has temperature only) returns ``({name: Cell}, param)``
+    with the E-mode multipoles from the same solve (compute_theta_ell(kind="E")).
     """
+    spectra = tuple(spectra)
+    if not spectra or any(x not in ("TT", "TE", "EE") for x in spectra):
+        raise ValueError(f"spectra must name TT, TE and/or EE, not {spectra!r}")
     torch, device = _device(device)
     param = evolve_background(param=dict(param_dict), thermo_module="RECFAST", num_thermo=num_thermo)
     aexp_out = cmb_aexp_out() if aexp_out is None else np.asarray(aexp_out, dtype=np.float64)
@@ -241,16 +261,25 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
                     device=device, as_tensor=True, **L)
     src = compute_sources(param=param, yout=y, kmodes=kmodes, aexp_out=aexp_out, device=device, **L)
     tau0 = float(param["tau_of_a_spline"].evaluate(1.0))
-    theta, kk = compute_theta_ell(ellmax, kmodes, tau, src["S"], tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
-                                  device=device)
-    cell = compute_Cell(theta, kk, param["n_s"], param["k_p"], device=device)
+    theta = theta_e = None
+    if "TT" in spectra or "TE" in spectra:
+        theta, kk = compute_theta_ell(ellmax, kmodes, tau, src["S"], tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                      device=device)
+    if "TE" in spectra or "EE" in spectra:
+        theta_e, kk = compute_theta_ell(ellmax, kmodes, tau, src["E"], tau0, n_fftlog=n_fftlog,
+                                        n_k_dense=n_k_dense, device=device, kind="E")
+    cells = {}
+    for name in spectra:
+        a = theta if name[0] == "T" else theta_e
+        b = None if name in ("TT", "EE") else theta_e
+        cells[name] = compute_Cell(a, kk, param["n_s"], param["k_p"], device=device, theta_ell_b=b).cpu().numpy()
     for key, v in (("lmaxg", lmaxg), ("lmaxgp", lmaxgp), ("lmaxr", lmaxr), ("lmaxnu", lmaxnu), ("nqmax", nqmax),
                    ("nout", aexp_out.shape[0]), ("tau_out", tau)):
         param[key] = v
-    out = cell.cpu().numpy()
+    out = cells["TT"] if spectra == ("TT",) else cells
     if return_intermediates:
         return out, param, {"kmodes": kmodes, "aexp_out": aexp_out, "tau": tau, "y": y, "sources": src,
-                            "theta": theta, "kmodes_los": kk}
+                            "theta": theta, "theta_E": theta_e, "kmodes_los": kk}
     return out, param
 
 

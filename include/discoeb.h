@@ -278,7 +278,9 @@ int32_t discoeb_rhs(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_hos
 #define DISCOEB_SRC_RHONUPRIME 19
 #define DISCOEB_SRC_SHEARNUPRIME 20
 #define DISCOEB_SRC_THETABPRIME 21  /* theta_b' of compute_time_derivatives */
-#define DISCOEB_SRC_NFIELDS 22
+#define DISCOEB_SRC_E 22            /* E-mode polarisation source (3/16) g Pi (no counterpart in the
+                                     * reference, which computes temperature only) */
+#define DISCOEB_SRC_NFIELDS 23
 
 /* CMB source function at the output times of a full solve: replaces
  * compute_time_derivatives + extract_perturbations + compute_neutrino_perturbations +
@@ -343,6 +345,25 @@ int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
  * (cmb.py:838-873).  theta [n_modes, n_ell], cell [n_ell], device. */
 int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta, double n_s,
                      double k_p, double* cell, void* stream);
+
+/* E-mode polarisation (no counterpart in the reference, which computes C_l^TT only): the
+ * multipoles Theta_E,l(k) = sqrt((l+2)!/(l-2)!) int S_E(k, tau) j_l(x) / x^2 dtau, x = k(tau0 - tau)
+ * (Zaldarriaga & Seljak 1997), of the source row DISCOEB_SRC_E, by the FFTLog method of
+ * discoeb_los: for l < 8 applied to S_E / chi^2 (chi held >= 1 Mpc), for l >= 8 applied to S_E at
+ * l - 2, l, l + 2 and combined by the spherical Bessel recurrence (j_l / x^2 as a sum of j_(l-2),
+ * j_l, j_(l+2)), which keeps the FFTLog's error from being multiplied by l^2.  Arguments as
+ * discoeb_los; workspace: discoeb_los_e_workspace_bytes(...) bytes, 256-byte aligned.  theta_l = 0
+ * for l < 2. */
+int64_t discoeb_los_e_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
+                                      int32_t n_k_dense);
+int32_t discoeb_los_e(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S_E,
+                      double tau0, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, void* workspace,
+                      int64_t workspace_bytes, double* theta, double* kmodes_out, void* stream);
+
+/* Cross spectrum C_l^AB = trapezoid over ln k of (k/k_p)^(n_s-1) Theta^A_l(k) Theta^B_l(k) (C_l^TE
+ * from the temperature and E-mode multipoles on the same k grid); as discoeb_cell otherwise. */
+int32_t discoeb_cell_cross(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta_a,
+                           const double* theta_b, double n_s, double k_p, double* cell, void* stream);
 
 /* C_l of the line of sight (discoeb_los then discoeb_cell, same arguments) and its derivative
  * along n_dir directions of the inputs, in forward mode through the resampling, the FFT

@@ -12,6 +12,8 @@ each docstring):
   source terms S1..S4, S  cmb.py:392-633
   theta_ell (FFTLog)      cmb.py:680-835 (+ the lngamma of util.py:13-45)
   Cell, Dell              cmb.py:838-927
+  e_source, theta_ell_E   E-mode polarisation (no counterpart in the reference): the source of
+                          Zaldarriaga & Seljak (1997) and its line of sight with j_l(x) / x^2
 
 Index layout of the state (extract_perturbations, cmb.py:17-92): 2 eta, 3/4 delta_c/theta_c,
 5/6 delta_b/theta_b, 7.. photon temperature (lmaxg+1), then polarisation (lmaxgp+1), massless
@@ -23,6 +25,9 @@ from __future__ import annotations
 import math
 
 import numpy as np
+
+# multipole from which the E-mode line of sight uses the Bessel recurrence (theta_ell_E)
+E_L_SWITCH = 8
 
 
 class NaturalSpline:
@@ -228,6 +233,7 @@ def sources(yout, yprime, kmodes, aexp, tau, param, q, w, lmaxg, lmaxgp, lmaxr):
     metric = metric_perturbations(pt, nu, bq, param, kmodes, aexp)
     pol = polarization_terms(pt, metric, vis, yout, yprime, kmodes)
     src = source_terms(pt, metric, vis, pol, kmodes, tau)
+    src["E"] = e_source(vis["gvis"], pol["polarization_term"])
     return {**src, "metric": metric, "pol": pol, "nu": nu, "vis": vis, "bq": bq, "pt": pt}
 
 
@@ -302,9 +308,49 @@ def theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0):
     return th, kmodes
 
 
-def Cell(theta, kmodes, n_s, k_p):
-    """compute_Cell (cmb.py:838-873): trapezoid in ln k of (k/k_p)^(n_s-1) theta^2."""
-    f = (kmodes[:, None] / k_p) ** (n_s - 1) * theta**2
+def e_source(gvis, pol):
+    """E-mode polarisation source (3/4) g Pi of Zaldarriaga & Seljak (1997, ApJ 482, 6), whose
+    Pi is a quarter of the reference's polarisation term pol (F_g2 + G_g0 + G_g2).  No counterpart
+    in the reference, which computes temperature only."""
+    return gvis * 3.0 / 16.0 * pol
+
+
+def e_factor(ell):
+    """sqrt((l+2)!/(l-2)!) for l >= 2, else 0."""
+    ell = np.asarray(ell, dtype=np.float64)
+    return np.where(ell >= 2, np.sqrt(np.maximum((ell + 2) * (ell + 1) * ell * (ell - 1), 0.0)), 0.0)
+
+
+def theta_ell_E(ellmax, kmodes, tau, S_E, tau0, n_fftlog=16384, n_k_dense=0, l_switch=E_L_SWITCH):
+    """E-mode multipoles Theta_E,l(k) = sqrt((l+2)!/(l-2)!) int S_E j_l(x) / x^2 dtau, x = k (tau0 - tau).
+
+    For l < l_switch: theta_ell of S_E / chi^2 (chi held >= 1 Mpc) divided by k^2.  For l >= l_switch,
+    where the FFTLog's absolute error of that integral, multiplied by l^2 / k^2, would swamp the
+    signal: the identity j_l / x^2 = [j_{l-2} / (2l-1) + j_l (1/(2l-1) + 1/(2l+3)) + j_{l+2} / (2l+3)]
+    / (2l+1) (from j_{l-1} + j_{l+1} = (2l+1) j_l / x) turns it into theta_ell of S_E itself at
+    l - 2, l, l + 2."""
+    ell = np.arange(ellmax + 1, dtype=np.float64)
+    F = e_factor(ell)
+    nlo = min(l_switch, ellmax + 1)
+    th_lo, kk = theta_ell(nlo - 1, kmodes, tau, S_E / np.maximum(tau0 - tau, 1.0)[None, :] ** 2, tau0,
+                          n_fftlog=n_fftlog, n_k_dense=n_k_dense)
+    out = np.zeros((th_lo.shape[0], ellmax + 1))
+    out[:, :nlo] = th_lo * F[None, :nlo] / kk[:, None] ** 2
+    if ellmax >= l_switch:
+        th, _ = theta_ell(ellmax + 2, kmodes, tau, S_E, tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense)
+        l = ell[l_switch:]
+        cm = 1.0 / ((2 * l + 1) * (2 * l - 1))
+        c0 = (1.0 / (2 * l - 1) + 1.0 / (2 * l + 3)) / (2 * l + 1)
+        cp = 1.0 / ((2 * l + 1) * (2 * l + 3))
+        li = l.astype(int)
+        out[:, l_switch:] = F[None, l_switch:] * (cm * th[:, li - 2] + c0 * th[:, li] + cp * th[:, li + 2])
+    return out, kk
+
+
+def Cell(theta, kmodes, n_s, k_p, theta_b=None):
+    """compute_Cell (cmb.py:838-873): trapezoid in ln k of (k/k_p)^(n_s-1) theta^2; with theta_b
+    the cross spectrum of theta and theta_b."""
+    f = (kmodes[:, None] / k_p) ** (n_s - 1) * theta * (theta if theta_b is None else theta_b)
     lk = np.log(kmodes)
     return np.sum(0.5 * (f[1:] + f[:-1]) * np.diff(lk)[:, None], axis=0)
 

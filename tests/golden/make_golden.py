@@ -11,6 +11,7 @@ thermal history, 128 camb-sampled modes, 320 output times, lmax 11/11/11/8/3, rt
   background_quantities, neutrino_perturbations, metric_perturbations, polarization_terms,
   source_term_sachs_wolfe, source_term_doppler, source_term_polarization, theta_ell, Cell,
   Dell}.csv and test_benchmark_extract_perturbations.csv
+and the CLASS TT, EE and TE spectra of tests/resources/class_benchmarks/DISCO-Notebook.csv.
 Usage: python tests/golden/make_golden.py /path/to/reference
 """
 import csv
@@ -80,6 +81,14 @@ with open(os.path.join(ref, "tests/resources/camb_benchmarks/DISCO-Notebook.csv"
     cb = np.array([[float(v) for v in r] for r in list(csv.reader(fh))[1:]])  # columns ell, D_ell
 cmb["camb:ell"] = cb[:, 0]
 cmb["camb:D_ell"] = cb[:, 1]
+# the CLASS spectra the reference's test_cmb_vs_class compares with (no reionisation, no lensing;
+# columns ell, D_ell_TT, D_ell_EE, D_ell_TE): TT pins the temperature chain, EE and TE the E-mode
+# polarisation that this build adds
+with open(os.path.join(ref, "tests/resources/class_benchmarks/DISCO-Notebook.csv")) as fh:
+    rows = list(csv.reader(fh))
+head, vals = rows[0], np.array([[float(v) for v in r] for r in rows[1:]])
+for i, name in enumerate(head):
+    cmb[f"class:{name}"] = vals[:, i]
 out2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_cmb_golden.npz")
 np.savez_compressed(out2, **cmb)
 print(out2, os.path.getsize(out2), "bytes")

@@ -87,6 +87,29 @@ def test_fftlog_against_direct_quadrature():
             assert abs(th[ik, l] - v) <= tol * abs(v), (ks[ik], l, th[ik, l], v)
 
 
+def test_e_mode_fftlog_against_direct_quadrature():
+    """The E-mode line of sight (sqrt((l+2)!/(l-2)!) int S j_l(x) / x^2 dtau) against adaptive
+    quadrature with spherical Bessel functions, for a source localised like the visibility
+    function: the direct form below the switch multipole and the recurrence form above it."""
+    sp = pytest.importorskip("scipy.special")
+    si = pytest.importorskip("scipy.integrate")
+    tau0 = 14000.0
+    tau = np.concatenate([np.geomspace(1.0, 200, 40, endpoint=False), np.linspace(200, 400, 200, endpoint=False),
+                          np.geomspace(400, tau0, 80)])
+
+    def src(t):
+        return np.exp(-0.5 * ((t - 280.0) / 15.0) ** 2)
+
+    ks = np.array([2e-3, 0.02])
+    th, kk = C.theta_ell_E(80, ks, tau, np.tile(src(tau), (2, 1)), tau0)
+    for ik, ells in ((0, (2, 3, 6, 12, 20)), (1, (2, 6, 12, 40, 80))):
+        for l in ells:
+            v = si.quad(lambda t: src(t) * sp.spherical_jn(l, ks[ik] * (tau0 - t)) / (ks[ik] * (tau0 - t)) ** 2, 1.0,
+                        tau0, limit=4000, points=[280.0], epsabs=0, epsrel=1e-11)[0]
+            v *= C.e_factor(l)
+            assert abs(th[ik, l] - v) <= 2e-3 * abs(v), (ks[ik], l, th[ik, l], v)
+
+
 def test_full_chain_matches_reference_accuracy_record():
     """compute_Cell_spectrum_from_cosmo_params at the reference's defaults (128 camb-sampled
     modes, 320 output times, rtol = atol = 1e-4, 8192 dense k, 16384 FFTLog points, l <= 2500),
@@ -117,3 +140,14 @@ def test_full_chain_matches_reference_accuracy_record():
     assert rel.mean() < 0.01
     dev = np.abs(rel - camb["camb:disco_relative_error"])
     assert np.median(dev) < 3e-3 and np.percentile(dev, 90) < 1e-2, (np.median(dev), np.percentile(dev, 90))
+    # E-mode polarisation (no counterpart in the reference) from the same states, against the CLASS
+    # EE and TE spectra the reference commits beside the TT it tests against (no reionisation)
+    if "class:ell" in camb:
+        the, _ = C.theta_ell_E(2500, ks, tau, src["E"], float(bg["tau_of_a_spline"].evaluate(1.0)), 16384, 8192)
+        _, DEE = C.Dell(C.Cell(the, kk, bg["n_s"], bg["k_p"]), bg["A_s"], bg["Tcmb"])
+        _, DTE = C.Dell(C.Cell(th, kk, bg["n_s"], bg["k_p"], the), bg["A_s"], bg["Tcmb"])
+        cls = {f: np.interp(ell, camb["class:ell"], camb[f"class:D_ell_{f}"]) for f in ("TT", "EE", "TE")}
+        ree = np.abs(DEE / cls["EE"] - 1)
+        rte = np.abs(DTE - cls["TE"]) / np.sqrt(cls["TT"] * cls["EE"])
+        assert ree.mean() < 0.02 and np.median(ree) < 0.015, (ree.mean(), np.median(ree))
+        assert rte.mean() < 0.01, rte.mean()

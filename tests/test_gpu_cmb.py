@@ -58,7 +58,7 @@ def test_gpu_sources_match_oracle(gpu_states):
             "alphapprime": R["metric"]["alphapprime"], "hprime": R["metric"]["hprime"],
             "polarization_term": R["pol"]["polarization_term"],
             "polarization_termpprime": R["pol"]["polarization_termpprime"],
-            "drhonu": R["nu"]["drhonu"], "shear_nu_prime": R["nu"]["shear_nu_prime"]}
+            "drhonu": R["nu"]["drhonu"], "shear_nu_prime": R["nu"]["shear_nu_prime"], "E": R["E"]}
     for name, ref in want.items():
         _close(src[name].cpu().numpy(), ref, 1e-9)
 
@@ -77,6 +77,22 @@ def test_gpu_theta_ell_and_cell_match_oracle(gpu_states, n_k_dense):
     np.testing.assert_allclose(cl, C.Cell(th.cpu().numpy(), kk_o, bg["n_s"], bg["k_p"]), rtol=1e-12)
 
 
+@pytest.mark.parametrize("n_k_dense", [0, 200])
+def test_gpu_e_mode_theta_ell_and_cross_cell_match_oracle(gpu_states, n_k_dense):
+    from discoeb_b200.cmb import compute_Cell, compute_sources, compute_theta_ell
+    bg, a, tau, ks, y = gpu_states
+    src = compute_sources(param=bg, yout=y, kmodes=ks, aexp_out=a, **L11)
+    tau0 = float(bg["tau_of_a_spline"].evaluate(1.0))
+    th, kk = compute_theta_ell(300, ks, tau, src["S"], tau0, n_fftlog=4096, n_k_dense=n_k_dense)
+    the, kk2 = compute_theta_ell(300, ks, tau, src["E"], tau0, n_fftlog=4096, n_k_dense=n_k_dense, kind="E")
+    the_o, kk_o = C.theta_ell_E(300, ks, tau, src["E"].cpu().numpy(), tau0, n_fftlog=4096, n_k_dense=n_k_dense)
+    np.testing.assert_allclose(kk2.cpu().numpy(), kk_o, rtol=1e-14)
+    _close(the.cpu().numpy(), the_o, 1e-9)
+    cte = compute_Cell(th, kk, bg["n_s"], bg["k_p"], theta_ell_b=the).cpu().numpy()
+    ref = C.Cell(th.cpu().numpy(), kk_o, bg["n_s"], bg["k_p"], the.cpu().numpy())
+    np.testing.assert_allclose(cte, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
 def test_gpu_cmb_spectrum_pipeline(torch_cuda):
     """compute_Cell_spectrum_from_cosmo_params at the reference's defaults: every stage on the
     GPU equals the restated chain applied to the GPU's own states, and D_l is within the
@@ -88,7 +104,9 @@ def test_gpu_cmb_spectrum_pipeline(torch_cuda):
          "Omegak": 0.0, "k_p": 0.05}
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
-        cell, param, mid = compute_Cell_spectrum_from_cosmo_params(p, return_intermediates=True)
+        cells, param, mid = compute_Cell_spectrum_from_cosmo_params(p, return_intermediates=True,
+                                                                    spectra=("TT", "TE", "EE"))
+    cell = cells["TT"]
     ell, D = compute_Dell(cell, param["A_s"], param["Tcmb"])
     g = np.load(os.path.join(GOLDEN, "reference_cmb_golden.npz"))
     Dc = np.interp(ell, g["camb:ell"], g["camb:D_ell"])
@@ -103,3 +121,19 @@ def test_gpu_cmb_spectrum_pipeline(torch_cuda):
     th, kk = C.theta_ell(2500, ks, tau, R["S"], float(param["tau_of_a_spline"].evaluate(1.0)), 16384, 8192)
     cl_o = C.Cell(th, kk, param["n_s"], param["k_p"])
     np.testing.assert_allclose(cell[2:], cl_o[2:], rtol=1e-8)
+    # E-mode polarisation: the restated chain, and the CLASS EE / TE the reference commits (no
+    # reionisation) at the level the reference holds TT against CLASS and CAMB
+    tau0 = float(param["tau_of_a_spline"].evaluate(1.0))
+    the, _ = C.theta_ell_E(2500, ks, tau, R["E"], tau0, 16384, 8192)
+    ee_o = C.Cell(the, kk, param["n_s"], param["k_p"])
+    te_o = C.Cell(th, kk, param["n_s"], param["k_p"], the)
+    np.testing.assert_allclose(cells["EE"][2:], ee_o[2:], rtol=1e-7)
+    sc = np.sqrt(np.abs(cl_o[2:] * ee_o[2:]))
+    assert np.all(np.abs(cells["TE"][2:] - te_o[2:]) <= 1e-7 * sc)
+    cls = {f: np.interp(ell, g["class:ell"], g[f"class:D_ell_{f}"]) for f in ("TT", "EE", "TE")}
+    _, DEE = compute_Dell(cells["EE"], param["A_s"], param["Tcmb"])
+    _, DTE = compute_Dell(cells["TE"], param["A_s"], param["Tcmb"])
+    ree = np.abs(DEE / cls["EE"] - 1)
+    rte = np.abs(DTE - cls["TE"]) / np.sqrt(cls["TT"] * cls["EE"])
+    assert ree.mean() < 0.02 and np.median(ree) < 0.015, (ree.mean(), np.median(ree))
+    assert rte.mean() < 0.01, rte.mean()
