@@ -87,7 +87,7 @@ def _fd_step(theta, name):
     return 1e-4 * max(abs(theta[name]), 1e-3)
 
 
-def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13):
+def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, J_rows=None):
     """Max relative error of the GPU's P(k) and dP/dtheta against the oracle (the CPU restatement,
     converged: rtol 1e-10), on modes spread over the workload's k range.
 
@@ -128,18 +128,24 @@ def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13):
         evolve_background(param=theta_to_params(w["theta"]), backend="numpy", trace=trace)
     shifted = _shifted_backgrounds(w, backend="numpy", replay=trace)
     ts, sw = fixed_times(bg, kmodes[ij])
-    err_j, per_dir = 0.0, {}
+    err_j, per_dir, err_r = 0.0, {}, 0.0
     for d, name in enumerate(ODE_DIRECTIONS):
         fd = (power(shifted[2 * d], kmodes[ij], ts, sw) - power(shifted[2 * d + 1], kmodes[ij], ts, sw)) \
             / (2 * _fd_step(w["theta"], name))
         e = np.abs(J[THETA_NAMES.index(name)][ij] - fd).max(axis=0) / np.abs(fd).max(axis=0)
         per_dir[name] = float(e.max())
         err_j = max(err_j, per_dir[name])
-    return {"P": err_p, "J": err_j, "J_per_direction": per_dir, "modes_P": int(ip.size), "modes_J": int(ij.size),
+        if J_rows is not None:  # the adjoint's rows of dP(k, z=0)/dtheta at the last output
+            r = np.abs(J_rows[THETA_NAMES.index(name)][ij] - fd[:, -1]).max() / np.abs(fd[:, -1]).max()
+            err_r = max(err_r, float(r))
+    out = {"P": err_p, "J": err_j, "J_per_direction": per_dir, "modes_P": int(ip.size), "modes_J": int(ij.size),
             "oracle": f"CPU restatement, clip mode, rtol {rtol:g}, atol {atol:g}; J: central differences, step 1e-4 "
                       "|theta_i|, start / switch times and Recfast steps held; max_k |dJ| / max_k |J| per direction "
                       "and output",
             "seconds": time.perf_counter() - t_start}
+    if J_rows is not None:
+        out["J_adjoint_z0"] = err_r
+    return out
 
 
 def run_reference(args, rank, world):
@@ -492,6 +498,8 @@ def main():
                     help="--mode batch: backgrounds on the host (native C++) or in one GPU launch")
     ap.add_argument("--wpb", type=int, default=0, help="warps (modes) per block; 0 = the library default")
     ap.add_argument("--ref-sample", type=int, default=16)
+    ap.add_argument("--no-adjoint", action="store_true", help="fwd+grad: skip the reverse-mode timing")
+    ap.add_argument("--checkpoint-every", type=int, default=16, help="adjoint: steps between stored states")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the oracle accuracy check")
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -621,6 +629,43 @@ def main():
             fwd_times.append(e0.elapsed_time(e1))
         fwd_ms = replicas.max_over_ranks(statistics.mean(fwd_times), dist, device)
 
+    # ---- reverse mode (discrete adjoint) on the same modes: the recorded forward plus one reverse
+    # sweep per mode whose cotangent is that mode's P(k, z = 0) (every row of dP(k, z=0)/dtheta),
+    # and the gradient of a scalar loss (one reverse sweep per mode, cotangent on every output)
+    adj = None
+    if grad and not args.no_adjoint:
+        from discoeb_b200.gradients import AdjointProblem
+        ap = AdjointProblem(w["theta"], aexp_out=aout, kmodes=kmodes, rtol=w["rtol"], atol=w["atol"],
+                            max_steps=100000, device=device, checkpoint_every=args.checkpoint_every, **L)
+        wts = torch.ones((K, nout), dtype=torch.float64, device=device)
+
+        def timed(fn):
+            ts = []
+            for i in range(args.warmup + args.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                e1.synchronize()
+                if i >= args.warmup:
+                    ts.append(e0.elapsed_time(e1))
+            return replicas.max_over_ranks(statistics.mean(ts), dist, device)
+
+        ap.launch_forward()
+        torch.cuda.synchronize()
+        if (ap.forward_power(on_failure="ignore")[1] != 0).any():
+            raise RuntimeError("the recorded forward solve failed")
+        rec_ms = timed(ap.launch_forward)
+        rows_ms = timed(lambda: ap.launch_jacobian_rows(out_index=-1))
+        loss_ms = timed(lambda: ap.launch_backward(wts))
+        J_rows = ap.jacobian_rows()[0]
+        adj = {"jacobian_rows_z0": {"value": world * K / ((rec_ms + rows_ms) / 1e3), "unit": UNIT,
+                                    "ms_per_cosmology": rec_ms + rows_ms, "forward_record_ms": rec_ms,
+                                    "reverse_ms": rows_ms},
+               "scalar_loss_gradient": {"ms_per_cosmology": rec_ms + loss_ms, "reverse_ms": loss_ms},
+               "checkpoint_every": args.checkpoint_every}
+
     # ---- end to end through the public API (host arrays in, host arrays out) ----
     e2e_ms = []
     for i in range(0 if args.kernel_only else args.warmup + args.steps):
@@ -688,7 +733,8 @@ def main():
             inv[order] = np.arange(K)
             P_gpu = pert.get_power(k=kmodes[:, None], y=d_out.cpu().numpy()[inv], idx=4, param=bg)
             J_gpu = None
-        accuracy = oracle_accuracy(w, bg, kmodes, P_gpu, J_gpu, n_j=8 if grad else 0)
+        accuracy = oracle_accuracy(w, bg, kmodes, P_gpu, J_gpu, n_j=8 if grad else 0,
+                                   J_rows=J_rows if adj is not None else None)
 
     if rank == 0:
         line = {
@@ -722,6 +768,8 @@ def main():
             line["cpu_baseline"] = cpu
         if accuracy is not None:
             line["max_rel_err"] = accuracy
+        if adj is not None:
+            line["adjoint"] = adj
         print(json.dumps(line), flush=True)
     replicas.finish(dist)
 

@@ -38,14 +38,21 @@ def cosmo_params(*, h=0.674, omega_b=0.0224, omega_c=0.120, A_s=2.1e-9, n_s=0.96
 # z in {2, 1, 0.5, 0} as increasing scale factors
 A_OUT_4Z = np.array([1.0 / 3.0, 0.5, 2.0 / 3.0, 1.0])
 
+# w0 of the cosmological-constant workloads.  The reference's dark-energy fluid equations divide by
+# 1 + w (perturbations.py:521-523: NaN at w = -1 exactly), so its LCDM point is taken at
+# w0 = -1 + 1e-6, where they are regular: P(k) equals the w = -1 limit to < 1e-6 (the same step
+# counts), and dP/dw0, dP/dwa include the fluid's clustering response, as the limit does (the
+# solver's guard at w = -1 exactly would hold the fluid's perturbations at zero and drop it).
+W0_LCDM = -1.0 + 1e-6
+
 WORKLOADS = {
     # flat LCDM, massless neutrinos only, P(k, z=0) on 128 log-spaced modes
     "pk_lcdm_massless_k128": dict(
-        cosmo=dict(), theta=dict(m_nu=0.0, w0=-1.0, wa=0.0), kmin=1e-4, kmax=1.0, num_k=128, aexp_out=np.array([1.0]),
+        cosmo=dict(w0=W0_LCDM), theta=dict(m_nu=0.0, w0=W0_LCDM, wa=0.0), kmin=1e-4, kmax=1.0, num_k=128, aexp_out=np.array([1.0]),
         lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=3, nqmax=3, rtol=1e-5, atol=1e-8),
     # + one 0.06 eV neutrino (5 momentum bins, l_max 17): 512 modes to k = 10/Mpc, P(k) at z = 0, 0.5, 1, 2
     "pk_lcdm_mnu_k512_z4": dict(
-        cosmo=dict(m_nu=0.06), theta=dict(m_nu=0.06, w0=-1.0, wa=0.0), kmin=1e-4, kmax=10.0, num_k=512, aexp_out=A_OUT_4Z,
+        cosmo=dict(m_nu=0.06, w0=W0_LCDM), theta=dict(m_nu=0.06, w0=W0_LCDM, wa=0.0), kmin=1e-4, kmax=10.0, num_k=512, aexp_out=A_OUT_4Z,
         lmaxg=12, lmaxgp=12, lmaxr=17, lmaxnu=17, nqmax=5, rtol=1e-5, atol=1e-8),
 }
 

@@ -43,7 +43,7 @@ def _chain(bg, kmodes, solver, fixed, size):
 @pytest.mark.parametrize("size", [SMALL, DEFAULT], ids=["small", "reference_defaults"])
 def test_gpu_cell_jacobian_matches_central_differences(torch_cuda, size):
     """dC_l/dtheta against fourth-order central differences (step 1e-4 of each parameter) of the
-    forward chain at solver rtol 1e-9, on backgrounds moved along the exact background tangent.
+    forward chain at solver rtol 1e-11, on backgrounds moved along the exact background tangent.
 
     Fourth order because the discrete C_l has a fast ripple in the parameters: the FFTLog grid in
     ln(tau0 - tau) moves with tau0, and the line of sight's discretisation error is periodic in
@@ -63,7 +63,10 @@ def test_gpu_cell_jacobian_matches_central_differences(torch_cuda, size):
     from discoeb_b200.gradients import ODE_DIRECTIONS, THETA_NAMES, param_dots, theta_to_params
     from discoeb_b200.perturbations import approximation_switch_times, determine_starting_time, k_sampling
     from discoeb_b200 import cmb
-    solver = dict(rtol=1e-9, atol=1e-12, max_steps=400000)
+    # rtol 1e-11: the quotient re-runs the adaptive solve, whose step sequence can change between
+    # the four points; at 1e-9 that noise, over a step of 1e-4, reached ~2e-4 of the weakest
+    # directions' derivative on some backgrounds
+    solver = dict(rtol=1e-11, atol=1e-14, max_steps=2000000)
     C, J, param = compute_Cell_jacobian(THETA, **size, **solver)
     assert C.shape == (size["ellmax"] + 1,) and J.shape == (8, size["ellmax"] + 1)
     assert np.isfinite(J).all()

@@ -50,12 +50,12 @@ def test_gpu_nonfinite_table_fails_only_its_cosmology(torch_cuda):
         bgs = [evolve_background(param=theta_to_params(t)) for t in thetas]
     ks = np.geomspace(1e-3, 1.0, 5)
     batch = CosmologyBatch(params=bgs, kmodes=ks, aexp_out=np.array([0.5, 1.0]), rtol=1e-5, atol=1e-8, **L65)
-    # DeviceCosmo.tensors hold each table as [x | y | S]: poison the knot values of cosmology 1's
+    # DeviceCosmo.tensors hold each table as rows x, y, S: poison the knot values of cosmology 1's
     # x_e table with NaN and those of cosmology 2's c_s^2 a table with +inf
     n_xe = bgs[1]["xe_of_loga_spline"].n
-    batch.dcs[1].tensors[0][n_xe:2 * n_xe] = float("nan")
+    batch.dcs[1].tensors[0].view(-1)[n_xe:2 * n_xe] = float("nan")
     n_cs = bgs[2]["cs2a_of_loga_spline"].n
-    batch.dcs[2].tensors[1][n_cs:2 * n_cs] = float("inf")
+    batch.dcs[2].tensors[1].view(-1)[n_cs:2 * n_cs] = float("inf")
     batch.launch()
     y, status, nsteps = batch.result(on_failure="ignore")
     assert (status[0] == 0).all() and (status[3] == 0).all(), status
