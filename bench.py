@@ -84,7 +84,15 @@ def _shifted_backgrounds(w, backend="native", replay=None):
 
 
 def _fd_step(theta, name):
-    return 1e-4 * max(abs(theta[name]), 1e-3)
+    """1e-4 |theta_i|, at least 3e-7: at the workloads' w0 = -1 + 1e-6, wa = 0, w(a) crosses -1
+    (where the fluid equations are singular) once wa < -1e-6, so the quotient in wa must stay well
+    inside that distance."""
+    return 1e-4 * max(abs(theta[name]), 3e-3)
+
+
+# the oracle's tolerances for a quotient of step below 1e-5: its noise is the solve's error over
+# the step (at rtol 1e-10 and step 3e-7, ~1e-4 of dP/dwa; ~1.5e-5 at rtol 1e-12)
+_FINE_FD = dict(rtol=1e-12, atol=1e-15)
 
 
 def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, J_rows=None):
@@ -93,9 +101,10 @@ def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, 
 
     P: |P_gpu / P_oracle - 1| over n_p modes at every output.  J: for each solver direction and
     output, max_k |J_gpu - J_fd| / max_k |J_fd| over n_j modes, J_fd the oracle's central
-    difference of step 1e-4 |theta_i| with the start times, the approximation switch times and
-    the Recfast step sequence held at the base point (the derivative forward-mode AD through the
-    reference defines).  n_s and ln10As are analytic and not checked here."""
+    difference of step _fd_step (1e-4 |theta_i|, at least 3e-7) with the start times, the
+    approximation switch times and the Recfast step sequence held at the base point (the
+    derivative forward-mode AD through the reference defines).  n_s and ln10As are analytic and
+    not checked here."""
     from discoeb_b200.background import evolve_background
     from discoeb_b200.gradients import ODE_DIRECTIONS, THETA_NAMES, theta_to_params
     from discoeb_b200.perturbations import approximation_switch_times, determine_starting_time, get_power
@@ -108,8 +117,9 @@ def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, 
         tout = b["tau_of_a_spline"].evaluate(aout)
         return 0.99 * np.minimum(tout.min(), determine_starting_time(param=b, k=ks)), approximation_switch_times(b, ks)
 
-    def power(b, ks, ts, sw):
-        y, st = O.output_fields_fixed(b, ks, aout, ts, sw, rtol=rtol, atol=atol, **L)
+    def power(b, ks, ts, sw, tol=None):
+        tol = tol or dict(rtol=rtol, atol=atol)
+        y, st = O.output_fields_fixed(b, ks, aout, ts, sw, **tol, **L)
         if (st != 0).any():
             raise RuntimeError("oracle solve failed in the accuracy check")
         return get_power(k=ks[:, None], y=y, idx=4, param=b)
@@ -130,8 +140,10 @@ def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, 
     ts, sw = fixed_times(bg, kmodes[ij])
     err_j, per_dir, err_r = 0.0, {}, 0.0
     for d, name in enumerate(ODE_DIRECTIONS):
-        fd = (power(shifted[2 * d], kmodes[ij], ts, sw) - power(shifted[2 * d + 1], kmodes[ij], ts, sw)) \
-            / (2 * _fd_step(w["theta"], name))
+        h = _fd_step(w["theta"], name)
+        tol = _FINE_FD if h < 1e-5 else None
+        fd = (power(shifted[2 * d], kmodes[ij], ts, sw, tol) - power(shifted[2 * d + 1], kmodes[ij], ts, sw, tol)) \
+            / (2 * h)
         e = np.abs(J[THETA_NAMES.index(name)][ij] - fd).max(axis=0) / np.abs(fd).max(axis=0)
         per_dir[name] = float(e.max())
         err_j = max(err_j, per_dir[name])
@@ -140,8 +152,8 @@ def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, 
             err_r = max(err_r, float(r))
     out = {"P": err_p, "J": err_j, "J_per_direction": per_dir, "modes_P": int(ip.size), "modes_J": int(ij.size),
             "oracle": f"CPU restatement, clip mode, rtol {rtol:g}, atol {atol:g}; J: central differences, step 1e-4 "
-                      "|theta_i|, start / switch times and Recfast steps held; max_k |dJ| / max_k |J| per direction "
-                      "and output",
+                      "max(|theta_i|, 3e-3) (rtol 1e-12 / atol 1e-15 where the step is below 1e-5), start / switch "
+                      "times and Recfast steps held; max_k |dJ| / max_k |J| per direction and output",
             "seconds": time.perf_counter() - t_start}
     if J_rows is not None:
         out["J_adjoint_z0"] = err_r

@@ -686,7 +686,7 @@ __global__ void __launch_bounds__(128) sources_dot_kernel(
     const DiscoebCosmo* __restrict__ cosmo, const DiscoebTangent* __restrict__ tangents, int n_dir, int n_modes,
     const double* __restrict__ kmodes, int n_tau, const double* __restrict__ tau, const double* __restrict__ tau_dot,
     const double* __restrict__ bt, const double* __restrict__ bt_dot, const double* __restrict__ y_full,
-    const double* __restrict__ y_full_dot, double* fd4)
+    const double* __restrict__ y_full_dot, double* fd4, double* se_dot)
 {
     extern __shared__ double smem[];
     const int wib = threadIdx.x >> 5;
@@ -731,6 +731,7 @@ __global__ void __launch_bounds__(128) sources_dot_kernel(
     fd4[1 * stride + o] = out[DISCOEB_SRC_S3].d;
     fd4[2 * stride + o] = out[DISCOEB_SRC_S4].d;
     fd4[3 * stride + o] = out[DISCOEB_SRC_POTENTIAL].d;
+    if (se_dot) se_dot[o] = out[DISCOEB_SRC_E].d;  // the E-mode source has no spline part
 }
 
 __device__ Dual spline_slope_dual(Dual x0, Dual x1, Dual y0, Dual y1, Dual S0, Dual S1, Dual xn)
@@ -1064,7 +1065,7 @@ int32_t discoeb_cell_cross(int32_t n_modes, const double* kmodes, int32_t n_ell,
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 
-static int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
+static int64_t e_align(int64_t b) { return (b + 255) / 256 * 256; }
 
 int64_t discoeb_los_e_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,
                                       int32_t n_k_dense)
@@ -1073,7 +1074,7 @@ int64_t discoeb_los_e_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t el
     const int64_t b = discoeb_los_workspace_bytes(n_modes, n_tau, ellmax + 2, n_fftlog, n_k_dense);
     if (b < 0) return b;
     const int64_t rows = n_k_dense > 0 ? n_k_dense : n_modes;
-    return align256((int64_t)n_modes * n_tau * 8) + align256(rows * (ellmax + 3) * 8) + b;
+    return e_align((int64_t)n_modes * n_tau * 8) + e_align(rows * (ellmax + 3) * 8) + b;
 }
 
 int32_t discoeb_los_e(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S_E,
@@ -1092,9 +1093,9 @@ int32_t discoeb_los_e(int32_t n_modes, const double* kmodes, int32_t n_tau, cons
     const int n_ell = ellmax + 1, nlo = n_ell < kELSwitch ? n_ell : kELSwitch;
     char* ws = static_cast<char*>(workspace);
     double* Sx = reinterpret_cast<double*>(ws);
-    const int64_t o1 = align256((int64_t)n_modes * n_tau * 8);
+    const int64_t o1 = e_align((int64_t)n_modes * n_tau * 8);
     double* th = reinterpret_cast<double*>(ws + o1);
-    const int64_t o2 = o1 + align256((int64_t)rows * (ellmax + 3) * 8);
+    const int64_t o2 = o1 + e_align((int64_t)rows * (ellmax + 3) * 8);
     const long long pts = (long long)n_modes * n_tau;
     // l < nlo: S_E / chi^2
     e_source_kernel<<<blocks_for(pts, 256), 256, 0, s>>>(n_modes, n_tau, tau, tau0, S_E, Sx);
@@ -1213,7 +1214,7 @@ int32_t discoeb_sources_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* c
                             const DiscoebTangent* tangents_dev, int32_t n_dir, int32_t n_modes, const double* kmodes,
                             int32_t n_tau, const double* tau, const double* tau_dot, const double* bgtab,
                             const double* bgtab_dot, const double* y_full, const double* y_full_dot,
-                            const double* fields, double* S_dot, double* scratch, void* stream)
+                            const double* fields, double* S_dot, double* scratch, double* SE_dot, void* stream)
 {
     if (!cosmo_host || !cosmo_dev || !tangents_dev || n_dir < 1 || n_modes < 0 || n_tau < 0) return DISCOEB_EINVAL;
     if (cosmo_host->use_tca) return DISCOEB_EUNSUPPORTED;
@@ -1232,7 +1233,8 @@ int32_t discoeb_sources_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* c
     double* fd4 = scratch;                       // [4, n_dir, n_modes, n_tau]
     double* sp = scratch + 4 * (size_t)points;  // [4, n_dir, n_modes, n_tau]
     sources_dot_kernel<<<blocks_for(points * 32, threads), threads, smem, s>>>(
-        cosmo_dev, tangents_dev, n_dir, n_modes, kmodes, n_tau, tau, tau_dot, bgtab, bgtab_dot, y_full, y_full_dot, fd4);
+        cosmo_dev, tangents_dev, n_dir, n_modes, kmodes, n_tau, tau, tau_dot, bgtab, bgtab_dot, y_full, y_full_dot, fd4,
+        SE_dot);
     const size_t stride = (size_t)n_modes * n_tau;
     isw_dot_kernel<<<blocks_for((long long)n_dir * n_modes, 64), 64, 0, s>>>(
         n_dir, n_modes, n_tau, tau, tau_dot, bgtab, bgtab_dot, fields + DISCOEB_SRC_POTENTIAL * stride, fd4, sp, S_dot);

@@ -205,7 +205,7 @@ def lib():
         L.discoeb_los.restype = ctypes.c_int32
         L.discoeb_cell.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, ctypes.c_double, ctypes.c_double, vp, vp]
         L.discoeb_sources_jvp.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), vp, ctypes.c_int32, ctypes.c_int32, vp,
-                                          ctypes.c_int32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+                                          ctypes.c_int32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.discoeb_sources_jvp.restype = ctypes.c_int32
         L.discoeb_los_cell_jvp_workspace_bytes.argtypes = [ctypes.c_int32] * 5
         L.discoeb_los_cell_jvp_workspace_bytes.restype = ctypes.c_int64

@@ -286,7 +286,7 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
 def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0, n_k_dense=8192, n_fftlog=16384,
                           lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3, num_thermo=1024, rtol=1e-4, atol=1e-4,
                           max_steps=2048, k_sampling_method="camb", aexp_out=None, de_guard_eps=1e-9, device=None,
-                          rel_step=1e-4, los="tangent", sources="tangent"):
+                          rel_step=1e-4, los="tangent", sources="tangent", spectra=("TT",)):
     """C_l^TT and dC_l/dtheta for theta = (omega_c, omega_b, h, n_s, ln10As, w0, wa, m_nu)
     (``gradients.THETA_NAMES``), what ``jax.jacfwd`` of the reference's
     compute_Cell_spectrum_from_cosmo_params (cmb.py:931-1090) gives.
@@ -312,7 +312,17 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
 
     Returns ``(Cell [ellmax+1], J [8, ellmax+1], param)`` (numpy; param as
     compute_Cell_spectrum_from_cosmo_params returns it).
+
+    ``spectra`` naming TE or EE (E-mode polarisation, which the reference does not compute) returns
+    ``({name: Cell}, {name: J}, param)``: the E source and its tangent come from the same forward-mode
+    solve and sources (discoeb_sources_jvp's SE_dot), and the E-mode line of sight and the cross and
+    auto C_l along each direction's first-order path by fourth-order differences (as ``los=
+    "differences"`` does for TT).
     """
+    spectra = tuple(spectra)
+    if not spectra or any(x not in ("TT", "TE", "EE") for x in spectra):
+        raise ValueError(f"spectra must name TT, TE and/or EE, not {spectra!r}")
+    pol = "TE" in spectra or "EE" in spectra
     from .background import _DIFF_FIELDS, background_from_buffer, native_background
     from .gradients import ODE_DIRECTIONS, THETA_NAMES, JacobianProblem, param_dots, theta_to_params
     if los not in ("tangent", "differences"):
@@ -334,8 +344,9 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     y = prob.state()
 
     def source_S(param, states):
-        return compute_sources(param=param, yout=states, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
-                               device=device, **L)["S"]
+        f = compute_sources(param=param, yout=states, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
+                            device=device, **L)
+        return (f["S"], f["E"]) if pol else f["S"]
 
     def times(param):
         return param["tau_of_a_spline"].evaluate(aexp_out), float(param["tau_of_a_spline"].evaluate(1.0))
@@ -348,6 +359,20 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     fields0 = compute_sources(param=bg, yout=y, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
                               device=device, **L)
     S0 = fields0["S"]
+    SE0 = fields0["E"]
+
+    def pol_cells(S, SE, tau, tau0):
+        """C_l^TE and C_l^EE (numpy) of the line of sight of (S, S_E)."""
+        out = {}
+        the, kk = compute_theta_ell(ellmax, kmodes, tau, SE, tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                    device=device, kind="E")
+        if "TE" in spectra:
+            tht, _ = compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                       device=device)
+            out["TE"] = compute_Cell(tht, kk, bg["n_s"], bg["k_p"], device=device, theta_ell_b=the)
+        if "EE" in spectra:
+            out["EE"] = compute_Cell(the, kk, bg["n_s"], bg["k_p"], device=device)
+        return out
     tau_b, tau0_b = times(bg)
     if sources == "tangent":
         lib = _abi.lib()
@@ -361,6 +386,7 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     if los == "differences":
         th, kk, cell = los_cell(S0, tau_b, tau0_b)
     J = np.zeros((len(THETA_NAMES), ellmax + 1))
+    Jp = {name: np.zeros((len(THETA_NAMES), ellmax + 1)) for name in ("TE", "EE") if name in spectra}
     stencil = ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0))
     tangents = []
     for di, name in enumerate(ODE_DIRECTIONS):
@@ -381,21 +407,37 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
                 side.append((source_S(bgs, torch.add(y, ydot, alpha=sgn * h)), tau_s, tau0_s))
         tau_dot = (side[0][1] - side[1][1]) / (2 * h)
         tau0_dot = (side[0][2] - side[1][2]) / (2 * h)
+        SE_dot = None
         if sources == "tangent":
             bt_dot = torch.from_numpy(np.ascontiguousarray((side[0][0] - side[1][0]) / (2 * h))).to(device)
             S_dot = torch.empty((K, T), **f64)
+            SE_dot = torch.empty((K, T), **f64) if pol else None
             d_tau_dot = torch.from_numpy(np.ascontiguousarray(tau_dot)).to(device)
             rc = lib.discoeb_sources_jvp(prob.dc.struct.data_ptr(), ctypes.byref(prob.dc.host),
                                          prob.d_tan.data_ptr() + di * tan_size, 1, K, d_k.data_ptr(), T,
                                          d_tau.data_ptr(), d_tau_dot.data_ptr(),
                                          d_bt.data_ptr(), bt_dot.data_ptr(), y.data_ptr(), ydot.data_ptr(),
                                          S0.data_ptr(), S_dot.data_ptr(), scratch.data_ptr(),
+                                         SE_dot.data_ptr() if pol else None,
                                          torch.cuda.current_stream(device).cuda_stream)
             if rc != 0:
                 raise RuntimeError(f"discoeb_sources_jvp failed with code {rc}")
+        elif pol:
+            S_dot = (side[0][0][0] - side[1][0][0]) / (2 * h)
+            SE_dot = (side[0][0][1] - side[1][0][1]) / (2 * h)
         else:
             S_dot = (side[0][0] - side[1][0]) / (2 * h)
         del ydot, side
+        if pol:  # E-mode line of sight and C_l^TE / C_l^EE along the path, fourth order
+            acc = {sp: 0.0 for sp in Jp}
+            for m, wgt in stencil:
+                pc = pol_cells(torch.add(S0, S_dot, alpha=m * h), torch.add(SE0, SE_dot, alpha=m * h),
+                               tau_b + m * h * tau_dot, tau0_b + m * h * tau0_dot)
+                for sp in Jp:
+                    acc[sp] = acc[sp] + wgt * pc[sp].cpu().numpy()
+            for sp in Jp:
+                Jp[sp][THETA_NAMES.index(name)] = acc[sp] / h
+            del SE_dot
         if los == "tangent":
             tangents.append((S_dot, tau_dot, tau0_dot))
             continue
@@ -426,7 +468,29 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     for key, v in (("lmaxg", lmaxg), ("lmaxgp", lmaxgp), ("lmaxr", lmaxr), ("lmaxnu", lmaxnu), ("nqmax", nqmax),
                    ("nout", aexp_out.shape[0]), ("tau_out", bg["tau_of_a_spline"].evaluate(aexp_out))):
         param[key] = v
-    return cell, J, param
+    if not pol:
+        return cell, J, param
+    cells, jacs = {}, {}
+    if "TT" in spectra:
+        cells["TT"], jacs["TT"] = cell, J
+    # the base point's polarisation spectra, and their n_s row (the primordial weight alone)
+    the, kk = compute_theta_ell(ellmax, kmodes, tau_b, SE0, tau0_b, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                device=device, kind="E")
+    tht = None
+    if "TE" in spectra:
+        tht, _ = compute_theta_ell(ellmax, kmodes, tau_b, S0, tau0_b, n_fftlog=n_fftlog, n_k_dense=n_k_dense,
+                                   device=device)
+    h = rel_step * max(abs(float(bg["n_s"])), 1e-2)
+    for sp in Jp:
+        a, b = (tht, the) if sp == "TE" else (the, None)
+        cells[sp] = compute_Cell(a, kk, bg["n_s"], bg["k_p"], device=device, theta_ell_b=b).cpu().numpy()
+        acc = np.zeros(ellmax + 1)
+        for m, wgt in stencil:
+            acc += wgt * compute_Cell(a, kk, bg["n_s"] + m * h, bg["k_p"], device=device,
+                                      theta_ell_b=b).cpu().numpy()
+        Jp[sp][THETA_NAMES.index("n_s")] = acc / h
+        jacs[sp] = Jp[sp]
+    return {sp: cells[sp] for sp in spectra}, {sp: jacs[sp] for sp in spectra}, param
 
 
 def cell_spectrum_function(**options):

@@ -319,12 +319,14 @@ int32_t discoeb_sources_noalloc(const DiscoebCosmo* cosmo_dev, const DiscoebCosm
  *   tau_dot [n_dir, n_tau], bgtab_dot [n_dir, DISCOEB_BG_NFIELDS, n_tau]
  *   y_full_dot [n_dir, n_modes, n_tau, nvar]  (discoeb_jvp_full's state tangents)
  *   fields: discoeb_sources' output at the base point (its potential row is read)
- *   S_dot [n_dir, n_modes, n_tau] out; scratch: 8 n_dir n_modes n_tau doubles.  Device arrays. */
+ *   S_dot [n_dir, n_modes, n_tau] out; scratch: 8 n_dir n_modes n_tau doubles
+ *   SE_dot [n_dir, n_modes, n_tau] out, may be NULL: the derivative of the E-mode source
+ *   (DISCOEB_SRC_E; no counterpart in the reference).  Device arrays. */
 int32_t discoeb_sources_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host,
                             const DiscoebTangent* tangents_dev, int32_t n_dir, int32_t n_modes, const double* kmodes,
                             int32_t n_tau, const double* tau, const double* tau_dot, const double* bgtab,
                             const double* bgtab_dot, const double* y_full, const double* y_full_dot,
-                            const double* fields, double* S_dot, double* scratch, void* stream);
+                            const double* fields, double* S_dot, double* scratch, double* SE_dot, void* stream);
 
 /* Workspace bytes of discoeb_los for these sizes (< 0: invalid sizes or a cuFFT error). */
 int64_t discoeb_los_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellmax, int32_t n_fftlog,

@@ -275,10 +275,14 @@ def fftlog_coefficients(ells, p):
     return np.exp(lc)
 
 
-def theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0):
+def theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0, abs_sums=False):
     """compute_theta_ell (cmb.py:680-835): optional dense-k spline resampling, spline
     resampling onto a log-chi grid padded by 2 in ln chi, bias -1.1, rfft, analytic
-    power-law Bessel integrals.  Returns (theta [K', ellmax+1], kmodes')."""
+    power-law Bessel integrals.  Returns (theta [K', ellmax+1], kmodes').
+
+    ``abs_sums``: also return the sums of magnitudes that bound the rounding of each multipole
+    (the FFT's, sum |S_f chi^1.1| / n per coefficient, and the sum over coefficients of
+    |c_p M_l(p)|), so that eps times them is the scale of a correctly rounded evaluation's error."""
     if n_k_dense > 0:
         lk = np.log(kmodes)
         lkd = np.linspace(lk[0], lk[-1], n_k_dense)
@@ -305,7 +309,11 @@ def theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0):
         th = th + np.real(ck[:, -1:]) @ np.real(M[:, -1:]).T - np.imag(ck[:, -1:]) @ np.imag(M[:, -1:]).T
     else:
         th = th + 2.0 * (np.real(ck[:, 1:]) @ np.real(M[:, 1:]).T - np.imag(ck[:, 1:]) @ np.imag(M[:, 1:]).T)
-    return th, kmodes
+    if not abs_sums:
+        return th, kmodes
+    w = np.exp(-(bias + 1.0) * np.log(kmodes))[:, None]  # |k^-(p+1)|
+    fft_abs = np.abs(S_f * chi_f[None, :] ** (-bias)).sum(axis=-1, keepdims=True) / n_fftlog * w
+    return th, kmodes, 2.0 * (np.abs(ck) @ np.abs(M).T) + 2.0 * fft_abs * np.abs(M).sum(axis=1)[None, :]
 
 
 def e_source(gvis, pol):
@@ -321,30 +329,35 @@ def e_factor(ell):
     return np.where(ell >= 2, np.sqrt(np.maximum((ell + 2) * (ell + 1) * ell * (ell - 1), 0.0)), 0.0)
 
 
-def theta_ell_E(ellmax, kmodes, tau, S_E, tau0, n_fftlog=16384, n_k_dense=0, l_switch=E_L_SWITCH):
+def theta_ell_E(ellmax, kmodes, tau, S_E, tau0, n_fftlog=16384, n_k_dense=0, l_switch=E_L_SWITCH, abs_sums=False):
     """E-mode multipoles Theta_E,l(k) = sqrt((l+2)!/(l-2)!) int S_E j_l(x) / x^2 dtau, x = k (tau0 - tau).
 
     For l < l_switch: theta_ell of S_E / chi^2 (chi held >= 1 Mpc) divided by k^2.  For l >= l_switch,
     where the FFTLog's absolute error of that integral, multiplied by l^2 / k^2, would swamp the
     signal: the identity j_l / x^2 = [j_{l-2} / (2l-1) + j_l (1/(2l-1) + 1/(2l+3)) + j_{l+2} / (2l+3)]
     / (2l+1) (from j_{l-1} + j_{l+1} = (2l+1) j_l / x) turns it into theta_ell of S_E itself at
-    l - 2, l, l + 2."""
+    l - 2, l, l + 2.  ``abs_sums``: also return theta_ell's sums of magnitudes carried through the
+    same combination (eps times them is the rounding scale of each multipole)."""
     ell = np.arange(ellmax + 1, dtype=np.float64)
     F = e_factor(ell)
     nlo = min(l_switch, ellmax + 1)
-    th_lo, kk = theta_ell(nlo - 1, kmodes, tau, S_E / np.maximum(tau0 - tau, 1.0)[None, :] ** 2, tau0,
-                          n_fftlog=n_fftlog, n_k_dense=n_k_dense)
+    r = theta_ell(nlo - 1, kmodes, tau, S_E / np.maximum(tau0 - tau, 1.0)[None, :] ** 2, tau0,
+                  n_fftlog=n_fftlog, n_k_dense=n_k_dense, abs_sums=abs_sums)
+    th_lo, kk = r[0], r[1]
     out = np.zeros((th_lo.shape[0], ellmax + 1))
-    out[:, :nlo] = th_lo * F[None, :nlo] / kk[:, None] ** 2
+    parts = [(out, th_lo)] + ([(np.zeros_like(out), r[2])] if abs_sums else [])
+    for o, t in parts:
+        o[:, :nlo] = t * F[None, :nlo] / kk[:, None] ** 2
     if ellmax >= l_switch:
-        th, _ = theta_ell(ellmax + 2, kmodes, tau, S_E, tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense)
+        r = theta_ell(ellmax + 2, kmodes, tau, S_E, tau0, n_fftlog=n_fftlog, n_k_dense=n_k_dense, abs_sums=abs_sums)
         l = ell[l_switch:]
         cm = 1.0 / ((2 * l + 1) * (2 * l - 1))
         c0 = (1.0 / (2 * l - 1) + 1.0 / (2 * l + 3)) / (2 * l + 1)
         cp = 1.0 / ((2 * l + 1) * (2 * l + 3))
         li = l.astype(int)
-        out[:, l_switch:] = F[None, l_switch:] * (cm * th[:, li - 2] + c0 * th[:, li] + cp * th[:, li + 2])
-    return out, kk
+        for (o, _), t in zip(parts, r[::2]):
+            o[:, l_switch:] = F[None, l_switch:] * (cm * t[:, li - 2] + c0 * t[:, li] + cp * t[:, li + 2])
+    return (out, kk, parts[1][0]) if abs_sums else (out, kk)
 
 
 def Cell(theta, kmodes, n_s, k_p, theta_b=None):

@@ -151,3 +151,24 @@ def test_full_chain_matches_reference_accuracy_record():
         rte = np.abs(DTE - cls["TE"]) / np.sqrt(cls["TT"] * cls["EE"])
         assert ree.mean() < 0.02 and np.median(ree) < 0.015, (ree.mean(), np.median(ree))
         assert rte.mean() < 0.01, rte.mean()
+
+
+def test_line_of_sight_rounding_scale_bounds_a_reordered_evaluation():
+    """theta_ell(_E)'s ``abs_sums``: the values are unchanged, and eps times the sums of magnitudes
+    bounds how far a differently rounded evaluation of the same sums moves (the FFTLog's inputs
+    perturbed by one ulp here), which is what the GPU comparison allows beyond its relative bar."""
+    tau0 = 14000.0
+    tau = np.concatenate([np.geomspace(1.0, 200, 40, endpoint=False), np.linspace(200, 400, 200, endpoint=False),
+                          np.geomspace(400, tau0, 80)])
+    ks = np.geomspace(1e-4, 0.5, 6)
+    S = np.exp(-0.5 * ((tau[None, :] - 280.0) / 15.0) ** 2) * np.sin(ks[:, None] * tau[None, :] + 0.3)
+    for fn in (C.theta_ell, C.theta_ell_E):
+        a, kk = fn(120, ks, tau, S, tau0, n_fftlog=2048, n_k_dense=40)
+        a2, kk2, mag = fn(120, ks, tau, S, tau0, n_fftlog=2048, n_k_dense=40, abs_sums=True)
+        np.testing.assert_array_equal(a, a2)
+        np.testing.assert_array_equal(kk, kk2)
+        assert np.all(mag >= np.abs(a))
+        rng = np.random.default_rng(1)
+        b, _ = fn(120, ks, tau, S * (1 + np.finfo(float).eps * rng.choice([-1.0, 1.0], S.shape)), tau0,
+                  n_fftlog=2048, n_k_dense=40)
+        assert np.all(np.abs(b - a) <= 32 * np.finfo(float).eps * mag)

@@ -85,9 +85,15 @@ def test_gpu_e_mode_theta_ell_and_cross_cell_match_oracle(gpu_states, n_k_dense)
     tau0 = float(bg["tau_of_a_spline"].evaluate(1.0))
     th, kk = compute_theta_ell(300, ks, tau, src["S"], tau0, n_fftlog=4096, n_k_dense=n_k_dense)
     the, kk2 = compute_theta_ell(300, ks, tau, src["E"], tau0, n_fftlog=4096, n_k_dense=n_k_dense, kind="E")
-    the_o, kk_o = C.theta_ell_E(300, ks, tau, src["E"].cpu().numpy(), tau0, n_fftlog=4096, n_k_dense=n_k_dense)
+    the_o, kk_o, mag = C.theta_ell_E(300, ks, tau, src["E"].cpu().numpy(), tau0, n_fftlog=4096,
+                                     n_k_dense=n_k_dense, abs_sums=True)
     np.testing.assert_allclose(kk2.cpu().numpy(), kk_o, rtol=1e-14)
-    _close(the.cpu().numpy(), the_o, 1e-9)
+    # 1e-9 of each mode's largest multipole, plus the rounding scale of the FFTLog sums: at high k
+    # the recurrence's three terms cancel by ~(k chi)^2 near l = 8, where eps times the sum of
+    # magnitudes reaches ~5e-9 of the row's largest value on the dense k grid
+    got = the.cpu().numpy()
+    bound = 1e-9 * np.abs(the_o).max(axis=-1, keepdims=True) + 32 * np.finfo(float).eps * mag
+    assert np.all(np.abs(got - the_o) <= bound), float((np.abs(got - the_o) / bound).max())
     cte = compute_Cell(th, kk, bg["n_s"], bg["k_p"], theta_ell_b=the).cpu().numpy()
     ref = C.Cell(th.cpu().numpy(), kk_o, bg["n_s"], bg["k_p"], the.cpu().numpy())
     np.testing.assert_allclose(cte, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())

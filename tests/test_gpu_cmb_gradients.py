@@ -175,3 +175,92 @@ def test_gpu_forward_mode_sources_equal_their_differences(torch_cuda, size):
     dev = [float(np.abs(J1[i][l] - J2[i][l]).max() / max(np.abs(J2[i][l]).max(), 1e-300)) for i in range(8)]
     print("forward-mode vs differenced sources per direction:", dev)
     assert max(dev) <= 1e-6, dev
+
+
+def _chain_pol(bg, kmodes, solver, fixed, size):
+    """C_l^TE and C_l^EE of the forward chain on the background dict ``bg`` (as _chain)."""
+    from discoeb_b200 import cmb
+    from discoeb_b200.perturbations import solve_modes
+    a = cmb.cmb_aexp_out()
+    tau = bg["tau_of_a_spline"].evaluate(a)
+    tau0 = float(bg["tau_of_a_spline"].evaluate(1.0))
+    L = dict(lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3)
+    y = solve_modes(param=bg, kmodes=kmodes, tau_out=tau, pcoeff=0.25, icoeff=0.8, dcoeff=0.0, factormax=20.0,
+                    factormin=0.3, return_full=True, as_tensor=True, **fixed, **solver, **L)
+    src = cmb.compute_sources(param=bg, yout=y, kmodes=kmodes, aexp_out=a, **L)
+    kw = dict(n_fftlog=size["n_fftlog"], n_k_dense=size["n_k_dense"])
+    tht, kk = cmb.compute_theta_ell(size["ellmax"], kmodes, tau, src["S"], tau0, **kw)
+    the, _ = cmb.compute_theta_ell(size["ellmax"], kmodes, tau, src["E"], tau0, kind="E", **kw)
+    return {"TE": cmb.compute_Cell(tht, kk, bg["n_s"], bg["k_p"], theta_ell_b=the).cpu().numpy(),
+            "EE": cmb.compute_Cell(the, kk, bg["n_s"], bg["k_p"]).cpu().numpy()}
+
+
+def test_gpu_polarisation_jacobian_matches_central_differences(torch_cuda):
+    """dC_l^TE/dtheta and dC_l^EE/dtheta (the E source's tangent from discoeb_sources_jvp, the
+    E-mode line of sight by fourth-order differences along the path) against fourth-order central
+    differences of the whole chain at solver rtol 1e-11 on the reduced chain, as the TT test does;
+    and the TT block of the same call equals the TT-only call."""
+    from discoeb_b200.background import _DIFF_FIELDS, background_from_buffer, native_background
+    from discoeb_b200.cmb import compute_Cell_jacobian
+    from discoeb_b200.gradients import ODE_DIRECTIONS, THETA_NAMES, param_dots, theta_to_params
+    from discoeb_b200.perturbations import approximation_switch_times, determine_starting_time, k_sampling
+    from discoeb_b200 import cmb
+    solver = dict(rtol=1e-11, atol=1e-14, max_steps=2000000)
+    size = SMALL
+    C, J, _ = compute_Cell_jacobian(THETA, spectra=("TT", "TE", "EE"), **size, **solver)
+    assert set(C) == {"TT", "TE", "EE"}
+    C_tt, J_tt, _ = compute_Cell_jacobian(THETA, **size, **solver)
+    np.testing.assert_array_equal(C["TT"], C_tt)
+    np.testing.assert_array_equal(J["TT"], J_tt)
+    p = theta_to_params(THETA)
+    pd = param_dots(THETA, ODE_DIRECTIONS)
+    buf, bd = native_background(p, 1024, pd)
+    bg = background_from_buffer(p, buf, 1024)
+    kmodes = k_sampling(bg, 1e-4, 1.0, size["nmodes"], "camb")
+    tau_out = bg["tau_of_a_spline"].evaluate(cmb.cmb_aexp_out())
+    fixed = dict(tau_start=0.99 * np.minimum(tau_out.min(), determine_starting_time(param=bg, k=kmodes)),
+                 switch_tau=approximation_switch_times(bg, kmodes))
+    base = _chain_pol(bg, kmodes, solver, fixed, size)
+    l = slice(2, None)
+    for sp in ("TE", "EE"):
+        np.testing.assert_allclose(C[sp][l], base[sp][l], rtol=1e-7, atol=1e-7 * np.abs(base[sp][l]).max())
+        assert np.isfinite(J[sp]).all() and np.all(J[sp][THETA_NAMES.index("ln10As")] == 0.0)
+    worst = {"TE": {}, "EE": {}}
+    for i, name in enumerate(THETA_NAMES):
+        if name == "ln10As":
+            continue
+        eps = 1e-4 * abs(THETA[name])
+        fd = {"TE": 0.0, "EE": 0.0}
+        for sgn, wgt in ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0)):
+            if name == "n_s":
+                b = dict(bg)
+                b["n_s"] = bg["n_s"] + sgn * eps
+            else:
+                di = ODE_DIRECTIONS.index(name)
+                ps = dict(p)
+                for f in _DIFF_FIELDS:
+                    ps[f] = p[f] + sgn * eps * pd[di][f]
+                b = background_from_buffer(ps, buf + sgn * eps * bd[di], 1024)
+            ch = _chain_pol(b, kmodes, solver, fixed, size)
+            for sp in fd:
+                fd[sp] = fd[sp] + wgt * ch[sp] / eps
+        for sp in fd:
+            # TE crosses zero in l: deviations against the direction's largest
+            worst[sp][name] = float(np.abs(J[sp][i][l] - fd[sp][l]).max() / np.abs(fd[sp][l]).max())
+    print("max |J - fd| / max |fd| per direction:", worst)
+    assert max(max(w.values()) for w in worst.values()) < 1e-4, worst
+
+
+def test_gpu_polarisation_forward_mode_sources_equal_their_differences(torch_cuda):
+    """The E source's forward-mode tangent (discoeb_sources_jvp's SE_dot) against the central
+    difference of the whole source stage along the same tangents, through C_l^TE and C_l^EE."""
+    from discoeb_b200.cmb import compute_Cell_jacobian
+    C1, J1, _ = compute_Cell_jacobian(THETA, sources="tangent", spectra=("TE", "EE"), **SMALL)
+    C2, J2, _ = compute_Cell_jacobian(THETA, sources="differences", spectra=("TE", "EE"), **SMALL)
+    l = slice(2, None)
+    for sp in ("TE", "EE"):
+        np.testing.assert_array_equal(C1[sp], C2[sp])
+        dev = [float(np.abs(J1[sp][i][l] - J2[sp][i][l]).max() / max(np.abs(J2[sp][i][l]).max(), 1e-300))
+               for i in range(8)]
+        print(sp, "forward-mode vs differenced sources per direction:", dev)
+        assert max(dev) <= 1e-6, (sp, dev)

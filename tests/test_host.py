@@ -176,7 +176,8 @@ def test_sources_tangent_entry_rejects_bad_arguments_before_any_launch():
     host = _abi.DiscoebCosmo()
     host.lmaxg, host.lmaxgp, host.lmaxr, host.lmaxnu, host.nqmax = 11, 11, 11, 8, 3
     fake = 4096  # never dereferenced: the argument checks return first
-    ok = [fake, ctypes.byref(host), fake, 1, 8, fake, 16, fake, fake, fake, fake, fake, fake, fake, fake, fake, None]
+    ok = [fake, ctypes.byref(host), fake, 1, 8, fake, 16, fake, fake, fake, fake, fake, fake, fake, fake, fake, None,
+          None]
     for i, v in ((3, 0), (4, -1), (6, 2), (14, None), (15, None), (0, None)):
         args = list(ok)
         args[i] = v
@@ -211,7 +212,7 @@ def test_sources_entries_refuse_grids_beyond_the_launch_limits():
     fake = 4096
     big = 1 << 30
     assert lib.discoeb_sources_jvp(fake, ctypes.byref(host), fake, 8, big, fake, 16, fake, fake, fake, fake, fake,
-                                   fake, fake, fake, fake, None) == -1
+                                   fake, fake, fake, fake, None, None) == -1
     assert lib.discoeb_sources(fake, ctypes.byref(host), big, fake, 64, fake, fake, fake, fake, fake, None) == -1
 
 
