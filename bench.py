@@ -95,7 +95,7 @@ def _fd_step(theta, name):
 _FINE_FD = dict(rtol=1e-12, atol=1e-15)
 
 
-def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, J_rows=None):
+def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, J_rows=None, P_other=None):
     """Max relative error of the GPU's P(k) and dP/dtheta against the oracle (the CPU restatement,
     converged: rtol 1e-10), on modes spread over the workload's k range.
 
@@ -128,9 +128,14 @@ def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, 
     ts, sw = fixed_times(bg, kmodes[ip])
     Po = power(bg, kmodes[ip], ts, sw)
     err_p = float(np.max(np.abs(P[ip] / Po - 1)))
+    # other solves of the same modes (the mixed-precision forward) against the same oracle values
+    other = {name: float(np.max(np.abs(Px[ip] / Po - 1))) for name, Px in (P_other or {}).items()}
     if n_j == 0:
-        return {"P": err_p, "modes_P": int(ip.size), "oracle": f"CPU restatement, clip mode, rtol {rtol:g}, atol "
-                f"{atol:g}", "seconds": time.perf_counter() - t_start}
+        out = {"P": err_p, "modes_P": int(ip.size), "oracle": f"CPU restatement, clip mode, rtol {rtol:g}, atol "
+               f"{atol:g}", "seconds": time.perf_counter() - t_start}
+        if other:
+            out["P_other"] = other
+        return out
     ij = np.unique(np.linspace(0, len(kmodes) - 1, n_j).round().astype(int))
     trace = {}
     with warnings.catch_warnings():
@@ -157,6 +162,8 @@ def oracle_accuracy(w, bg, kmodes, P, J, n_p=16, n_j=8, rtol=1e-10, atol=1e-13, 
             "seconds": time.perf_counter() - t_start}
     if J_rows is not None:
         out["J_adjoint_z0"] = err_r
+    if other:
+        out["P_other"] = other
     return out
 
 
@@ -509,6 +516,8 @@ def main():
     ap.add_argument("--host-backend", default="native", choices=["native", "device"],
                     help="--mode batch: backgrounds on the host (native C++) or in one GPU launch")
     ap.add_argument("--wpb", type=int, default=0, help="warps (modes) per block; 0 = the library default")
+    ap.add_argument("--method", default="structured", choices=["structured", "structured-mixed"],
+                    help="--mode forward: FP64 chain factors, or FP32 factors with an FP64 refinement")
     ap.add_argument("--ref-sample", type=int, default=16)
     ap.add_argument("--no-adjoint", action="store_true", help="fwd+grad: skip the reverse-mode timing")
     ap.add_argument("--checkpoint-every", type=int, default=16, help="adjoint: steps between stored states")
@@ -574,16 +583,17 @@ def main():
     d_tout = torch.tensor(tau_out, **f64)
     d_out = torch.empty((K, nout, 20), **f64)
     d_stat = torch.empty((2, K), dtype=torch.int32, device=device)
-    ctrl = _abi.DiscoebControl(w["rtol"], w["atol"], 0.25, 0.80, 0.0, 20.0, 0.3, 100000,
-                               _abi.METHOD_RODAS5_STRUCTURED, args.wpb, 0)
+    methods = {"structured": _abi.METHOD_RODAS5_STRUCTURED, "structured-mixed": _abi.METHOD_RODAS5_STRUCTURED_MIXED}
+    ctrl = _abi.DiscoebControl(w["rtol"], w["atol"], 0.25, 0.80, 0.0, 20.0, 0.3, 100000, methods[args.method],
+                               args.wpb, 0)
     lib = _abi.lib()
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)  # > 126 MB L2
 
-    def forward():
-        rc = lib.discoeb_fwd(dc.struct.data_ptr(), ctypes.byref(dc.host), 1, ctypes.byref(ctrl), K, None,
+    def forward(c=ctrl, out=d_out):
+        rc = lib.discoeb_fwd(dc.struct.data_ptr(), ctypes.byref(dc.host), 1, ctypes.byref(c), K, None,
                              d_k.data_ptr(), d_ts.data_ptr(), d_y0.data_ptr(), d_sw.data_ptr(), nout,
-                             d_tout.data_ptr(), None, d_out.data_ptr(), d_stat[0].data_ptr(), d_stat[1].data_ptr(),
+                             d_tout.data_ptr(), None, out.data_ptr(), d_stat[0].data_ptr(), d_stat[1].data_ptr(),
                              stream.cuda_stream)
         if rc != 0:
             raise RuntimeError(f"discoeb_fwd returned {rc}")
@@ -626,20 +636,32 @@ def main():
     ms = replicas.max_over_ranks(statistics.mean(times_ms), dist, device)
     value = world * K / (ms / 1e3)
 
-    fwd_ms = None
-    if grad:  # the forward solve alone, for comparison (same events and L2 flush)
-        for _ in range(args.warmup):
-            forward()
-        fwd_times = []
-        for i in range(args.steps):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            forward()
-            e1.record(stream)
-            e1.synchronize()
-            fwd_times.append(e0.elapsed_time(e1))
-        fwd_ms = replicas.max_over_ranks(statistics.mean(fwd_times), dist, device)
+    fwd_ms = mixed_ms = None
+    d_out_mixed = None
+    if grad:  # the forward solve alone, for comparison (same events and L2 flush), in FP64 and in the
+        # mixed-precision form (FP32 chain factors, one FP64 refinement per chain solve)
+        ctrl_mixed = _abi.DiscoebControl(w["rtol"], w["atol"], 0.25, 0.80, 0.0, 20.0, 0.3, 100000,
+                                         _abi.METHOD_RODAS5_STRUCTURED_MIXED, args.wpb, 0)
+        d_out_mixed = torch.empty_like(d_out)
+
+        def timed_forward(fn):
+            for _ in range(args.warmup):
+                fn()
+            times = []
+            for i in range(args.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            return replicas.max_over_ranks(statistics.mean(times), dist, device)
+
+        fwd_ms = timed_forward(forward)
+        mixed_ms = timed_forward(lambda: forward(ctrl_mixed, d_out_mixed))
+        if (d_stat[0] != 0).any():
+            raise RuntimeError("the mixed-precision forward solve failed")
 
     # ---- reverse mode (discrete adjoint) on the same modes: the recorded forward plus one reverse
     # sweep per mode whose cotangent is that mode's P(k, z = 0) (every row of dP(k, z=0)/dtheta),
@@ -738,15 +760,20 @@ def main():
     accuracy = None
     if rank == 0 and world == 1 and not args.no_accuracy and not args.kernel_only:
         # the checker: the GPU's results of the timed launches against the converged oracle
+        P_other = None
         if grad:
             P_gpu, J_gpu = prob.result()[:2]
+            inv = np.empty_like(order)
+            inv[order] = np.arange(K)
+            P_other = {"forward_only_mixed": pert.get_power(k=kmodes[:, None], y=d_out_mixed.cpu().numpy()[inv],
+                                                            idx=4, param=bg)}
         else:
             inv = np.empty_like(order)
             inv[order] = np.arange(K)
             P_gpu = pert.get_power(k=kmodes[:, None], y=d_out.cpu().numpy()[inv], idx=4, param=bg)
             J_gpu = None
         accuracy = oracle_accuracy(w, bg, kmodes, P_gpu, J_gpu, n_j=8 if grad else 0,
-                                   J_rows=J_rows if adj is not None else None)
+                                   J_rows=J_rows if adj is not None else None, P_other=P_other)
 
     if rank == 0:
         line = {
@@ -758,7 +785,9 @@ def main():
                        "n_s, ln10As, w0, wa, m_nu" if grad else None,
                        "gradient_method": "forward-mode tangents (discoeb_jvp: 6 directions through the solver, "
                        "n_s and ln10As analytic)" if grad else None,
-                       "rtol": w["rtol"], "atol": w["atol"], "method": "rodas5-structured",
+                       "rtol": w["rtol"], "atol": w["atol"],
+                       "method": "rodas5-structured" + ("-mixed" if args.method == "structured-mixed" and not grad
+                                                        else ""),
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "ms_per_cosmology": ms, "step_attempts_per_mode_sum": step_attempts,
                        "warps_per_block": args.wpb or "default"},
@@ -776,6 +805,9 @@ def main():
         }
         if fwd_ms is not None:
             line["forward_only"] = {"value": world * K / (fwd_ms / 1e3), "unit": UNIT, "ms_per_cosmology": fwd_ms}
+            line["forward_only_mixed"] = {"value": world * K / (mixed_ms / 1e3), "unit": UNIT,
+                                          "ms_per_cosmology": mixed_ms,
+                                          "method": "FP32 chain factors + one FP64 refinement per chain solve"}
         if cpu is not None:
             line["cpu_baseline"] = cpu
         if accuracy is not None:

@@ -56,18 +56,20 @@ __device__ void emit_output(const WarpTeam& tm, const DiscoebCosmo& P, const Dim
     tm.sync();
 }
 
+// TM: WarpTeam (FP64) or WarpTeamMixed (FP32 chain factors, mix_doubles more per warp)
+template <class TM>
 __global__ void __launch_bounds__(256) fwd_structured_kernel(
     const DiscoebCosmo* __restrict__ cosmos, int n_cosmo, const int32_t* __restrict__ mode_cosmo, DiscoebControl ctrl,
     int n_modes,
     const double* __restrict__ kmodes, const double* __restrict__ tau_start, const double* __restrict__ y0,
-    const double* __restrict__ sw, int n_out, const double* __restrict__ tau_out, int mem_doubles, double* y_full,
-    double* y_out20, int32_t* status, int32_t* nsteps)
+    const double* __restrict__ sw, int n_out, const double* __restrict__ tau_out, int mem_doubles, int mix_doubles,
+    double* y_full, double* y_out20, int32_t* status, int32_t* nsteps)
 {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5;
-    const WarpTeam tm{(int)(threadIdx.x & 31)};
+    const TM tm{(int)(threadIdx.x & 31)};
     const int wpb = blockDim.x >> 5;
-    double* base = smem + (size_t)warp * (kCosmoDoubles + mem_doubles);
+    double* base = smem + (size_t)warp * (kCosmoDoubles + mem_doubles + mix_doubles);
     DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(base);
     double* wmem = base + kCosmoDoubles;
     const int total_warps = gridDim.x * wpb;
@@ -98,7 +100,8 @@ __global__ void __launch_bounds__(256) fwd_structured_kernel(
         }
         const Dims D = make_dims(*P);
         const int n = D.n;
-        if (mode_mem_doubles(D) != mem_doubles) {  // every cosmology must have the sizes of the first
+        if (mode_mem_doubles(D) != mem_doubles || (TM::mixed && mixed_mem_doubles(D) != mix_doubles)) {
+            // every cosmology must have the sizes of the first
             fill_nan(mode, 0);
             if (tm.leader()) {
                 status[mode] = DISCOEB_BAD_INDEX;
@@ -107,6 +110,7 @@ __global__ void __launch_bounds__(256) fwd_structured_kernel(
             continue;
         }
         ModeMem M = carve(wmem, D);
+        if constexpr (TM::mixed) carve_mixed(wmem + mem_doubles, D, M);
         const double k = kmodes[mode];
         for (int i = tm.lane; i < n; i += 32) M.y[i] = y0[(size_t)mode * n + i];
         double swm[3] = {sw[3 * mode], sw[3 * mode + 1], sw[3 * mode + 2]};
@@ -496,11 +500,13 @@ int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
     if (n_modes == 0) return DISCOEB_SUCCESS;
     if (!kmodes || !tau_start || !y0 || !switch_tau || !tau_out || !status || !nsteps) return DISCOEB_EINVAL;
     if (!y_full && !y_out20) return DISCOEB_EINVAL;
-    if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED) return DISCOEB_EUNSUPPORTED;
+    const bool mixed = ctrl->method == DISCOEB_METHOD_RODAS5_STRUCTURED_MIXED;
+    if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED && !mixed) return DISCOEB_EUNSUPPORTED;
     if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
     const Dims D = make_dims(*cosmo0_host);
-    const int mem = mode_mem_doubles(D);
-    const size_t per_warp = (size_t)(kCosmoDoubles + mem) * sizeof(double);
+    const int mem = mode_mem_doubles(D), mix = mixed ? mixed_mem_doubles(D) : 0;
+    const size_t per_warp = (size_t)(kCosmoDoubles + mem + mix) * sizeof(double);
+    const auto kernel = mixed ? fwd_structured_kernel<WarpTeamMixed> : fwd_structured_kernel<WarpTeam>;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
     int max_optin = 0, n_sm = 0;
@@ -511,14 +517,12 @@ int32_t discoeb_fwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
     while (wpb > 1 && per_warp * wpb > (size_t)max_optin) --wpb;
     if (per_warp > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
     const size_t smem = per_warp * wpb;
-    if (cudaFuncSetAttribute(fwd_structured_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return DISCOEB_ECUDA;
     int blocks = (n_modes + wpb - 1) / wpb;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    fwd_structured_kernel<<<blocks, 32 * wpb, smem, s>>>(cosmos_dev, n_cosmo, mode_cosmo, *ctrl, n_modes, kmodes,
-                                                          tau_start, y0, switch_tau, n_out, tau_out, mem, y_full,
-                                                          y_out20, status, nsteps);
+    kernel<<<blocks, 32 * wpb, smem, s>>>(cosmos_dev, n_cosmo, mode_cosmo, *ctrl, n_modes, kmodes, tau_start, y0,
+                                          switch_tau, n_out, tau_out, mem, mix, y_full, y_out20, status, nsteps);
     (void)n_sm;
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }

@@ -83,7 +83,18 @@ DHD int mode_mem_doubles(const Dims& D) { return 23 * D.n + 4 * kMaxSlots + 32; 
 
 struct ModeMem {
     double *y, *u, *f, *dT, *col0, *K, *A, *Z, *Gs, *F1s, *sc;
+    // mixed-precision form only (teams with TM::mixed): the chain factors in FP32 (7 n floats;
+    // A then keeps W's band unfactored, in FP64, for the residuals) and n doubles of scratch
+    float* Af = nullptr;
+    double* rs = nullptr;
 };
+// extra doubles per mode of the mixed-precision form, after mode_mem_doubles
+DHD int mixed_mem_doubles(const Dims& D) { return (7 * D.n + 1) / 2 + D.n; }
+DHD void carve_mixed(double* base, const Dims& D, ModeMem& M)
+{
+    M.Af = reinterpret_cast<float*>(base);
+    M.rs = base + (7 * D.n + 1) / 2;
+}
 
 DHD ModeMem carve(double* base, const Dims& D)
 {
@@ -286,22 +297,24 @@ DDV void rhs_team(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<T
 }
 
 // ---- chain LU (no pivoting) and solves ----
-DHD double& bandA(double* A, int i, int m) { return A[7 * i + m + 3]; }
+// E: the element type of the factors (double; float in the mixed-precision form)
+template <class E> DHD E& bandA(E* A, int i, int m) { return A[7 * i + m + 3]; }
+DHD float rcp(float x) { return 1.0f / x; }
 
-DDV bool factor_chain(double* A, const Chain& ch)
+template <class E> DDV bool factor_chain(E* A, const Chain& ch)
 {
     bool ok = true;
     for (int p = 0; p < ch.len; ++p) {
         const int i = ch.start + p * ch.stride;
-        const double piv = bandA(A, i, 0);
-        if (!(fabs(piv) > 0.0) || !xfinite(piv)) ok = false;
-        const double rp = rcp(piv);  // correctly rounded, as 1.0 / piv
+        const E piv = bandA(A, i, 0);
+        if (!(fabs(piv) > E(0)) || !xfinite((double)piv)) ok = false;
+        const E rp = rcp(piv);  // correctly rounded, as 1 / piv
         bandA(A, i, 0) = rp;
         for (int d = 1; d <= ch.kl && p + d < ch.len; ++d) {
             const int r = i + d * ch.stride;
-            const double l = bandA(A, r, -d) * rp;
+            const E l = bandA(A, r, -d) * rp;
             bandA(A, r, -d) = l;
-            if (l != 0.0)
+            if (l != E(0))
                 for (int m = 1; m <= ch.ku && p + m < ch.len; ++m) bandA(A, r, m - d) -= l * bandA(A, i, m);
         }
     }
@@ -311,21 +324,23 @@ DDV bool factor_chain(double* A, const Chain& ch)
 // Forward and back substitution along one chain.  With CH = 4 the sweeps run in chunks of four
 // elements whose loads are issued together before the dependent arithmetic (the loads do not
 // depend on the recurrence), so a chunk costs one shared-memory latency instead of four; CH = 1 is
-// the plain element-by-element sweep.  The arithmetic and its order are the same for both.
-template <int CH> DDV void solve_chain(const double* A, const Chain& ch, double* z)
+// the plain element-by-element sweep.  The arithmetic and its order are the same for both.  E: the
+// element type of the factors and of the arithmetic (float in the mixed-precision form, where z
+// stays double in memory).
+template <int CH, class E = double> DDV void solve_chain(const E* A, const Chain& ch, double* z)
 {
     const int st = ch.stride, len = ch.len;
     if (ch.kl == 1 && ch.ku == 1) {
         // tridiagonal: carry the neighbour in a register
         int i = ch.start;
-        double prev = z[i];
+        E prev = E(z[i]);
         int p = 1;
         for (; CH > 1 && p + 4 <= len; p += 4) {
-            double zz[4], a2[4];
+            E zz[4], a2[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int j = i + (q + 1) * st;
-                zz[q] = z[j];
+                zz[q] = E(z[j]);
                 a2[q] = A[7 * j + 2];
             }
 #pragma unroll
@@ -337,18 +352,18 @@ template <int CH> DDV void solve_chain(const double* A, const Chain& ch, double*
         }
         for (; p < len; ++p) {
             i += st;
-            prev = z[i] - A[7 * i + 2] * prev;
+            prev = E(z[i]) - A[7 * i + 2] * prev;
             z[i] = prev;
         }
-        double next = prev * A[7 * i + 3];
+        E next = prev * A[7 * i + 3];
         z[i] = next;
         p = len - 2;
         for (; CH > 1 && p >= 3; p -= 4) {
-            double zz[4], a4[4], a3[4];
+            E zz[4], a4[4], a3[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int j = i - (q + 1) * st;
-                zz[q] = z[j];
+                zz[q] = E(z[j]);
                 a4[q] = A[7 * j + 4];
                 a3[q] = A[7 * j + 3];
             }
@@ -361,35 +376,35 @@ template <int CH> DDV void solve_chain(const double* A, const Chain& ch, double*
         }
         for (; p >= 0; --p) {
             i -= st;
-            next = (z[i] - A[7 * i + 4] * next) * A[7 * i + 3];
+            next = (E(z[i]) - A[7 * i + 4] * next) * A[7 * i + 3];
             z[i] = next;
         }
         return;
     }
     // pentadiagonal (kl = ku = 2)
     int i = ch.start;
-    double p1 = z[i], p2 = 0.0;
+    E p1 = E(z[i]), p2 = E(0);
     int p = 1;
     if (len > 1) {  // the second element has one sub-diagonal neighbour
         i += st;
-        const double v = z[i] - A[7 * i + 2] * p1;
+        const E v = E(z[i]) - A[7 * i + 2] * p1;
         z[i] = v;
         p2 = p1;
         p1 = v;
         p = 2;
     }
     for (; CH > 1 && p + 4 <= len; p += 4) {
-        double zz[4], a2[4], a1[4];
+        E zz[4], a2[4], a1[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int j = i + (q + 1) * st;
-            zz[q] = z[j];
+            zz[q] = E(z[j]);
             a2[q] = A[7 * j + 2];
             a1[q] = A[7 * j + 1];
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            double v = zz[q] - a2[q] * p1;
+            E v = zz[q] - a2[q] * p1;
             v -= a1[q] * p2;
             z[i + (q + 1) * st] = v;
             p2 = p1;
@@ -399,18 +414,18 @@ template <int CH> DDV void solve_chain(const double* A, const Chain& ch, double*
     }
     for (; p < len; ++p) {
         i += st;
-        double v = z[i] - A[7 * i + 2] * p1;
+        E v = E(z[i]) - A[7 * i + 2] * p1;
         v -= A[7 * i + 1] * p2;
         z[i] = v;
         p2 = p1;
         p1 = v;
     }
-    double n1 = p1 * A[7 * i + 3], n2 = 0.0;
+    E n1 = p1 * A[7 * i + 3], n2 = E(0);
     z[i] = n1;
     p = len - 2;
     if (p >= 0) {  // the last-but-one element has one super-diagonal neighbour
         i -= st;
-        double v = z[i] - A[7 * i + 4] * n1;
+        E v = E(z[i]) - A[7 * i + 4] * n1;
         v *= A[7 * i + 3];
         z[i] = v;
         n2 = n1;
@@ -418,18 +433,18 @@ template <int CH> DDV void solve_chain(const double* A, const Chain& ch, double*
         --p;
     }
     for (; CH > 1 && p >= 3; p -= 4) {
-        double zz[4], a4[4], a5[4], a3[4];
+        E zz[4], a4[4], a5[4], a3[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int j = i - (q + 1) * st;
-            zz[q] = z[j];
+            zz[q] = E(z[j]);
             a4[q] = A[7 * j + 4];
             a5[q] = A[7 * j + 5];
             a3[q] = A[7 * j + 3];
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            double v = zz[q] - a4[q] * n1;
+            E v = zz[q] - a4[q] * n1;
             v -= a5[q] * n2;
             v *= a3[q];
             z[i - (q + 1) * st] = v;
@@ -440,13 +455,33 @@ template <int CH> DDV void solve_chain(const double* A, const Chain& ch, double*
     }
     for (; p >= 0; --p) {
         i -= st;
-        double v = z[i] - A[7 * i + 4] * n1;
+        E v = E(z[i]) - A[7 * i + 4] * n1;
         v -= A[7 * i + 5] * n2;
         v *= A[7 * i + 3];
         z[i] = v;
         n2 = n1;
         n1 = v;
     }
+}
+
+// Mixed precision: A z = r along one chain with the FP32 factors Af and one step of iterative
+// refinement, the residual r - A z0 taken in FP64 with the unfactored band A:
+//   z0 = A32^{-1} r,  z = z0 + A32^{-1} (r - A z0).
+// rs (n doubles, each chain its own entries) holds r, then the residual and its correction.
+DDV void solve_chain_mixed(const double* A, const float* Af, const Chain& ch, double* z, double* rs)
+{
+    const int st = ch.stride, len = ch.len;
+    for (int p = 0; p < len; ++p) rs[ch.start + p * st] = z[ch.start + p * st];
+    solve_chain<1, float>(Af, ch, z);
+    for (int p = 0; p < len; ++p) {
+        const int i = ch.start + p * st;
+        double r = rs[i] - A[7 * i + 3] * z[i];
+        for (int d = 1; d <= ch.kl && p - d >= 0; ++d) r -= A[7 * i + 3 - d] * z[i - d * st];
+        for (int d = 1; d <= ch.ku && p + d < len; ++d) r -= A[7 * i + 3 + d] * z[i + d * st];
+        rs[i] = r;
+    }
+    solve_chain<1, float>(Af, ch, rs);
+    for (int p = 0; p < len; ++p) z[ch.start + p * st] += rs[ch.start + p * st];
 }
 
 // A z = r for rows >= 2 (in place); gh = gamma*h
@@ -459,7 +494,8 @@ template <class TM> DDV void solve_A(const TM& tm, const Dims& D, const ModeMem&
     for (int c = tm.lane; c < nc; c += tm.nl) {
         const Chain ch = chain_of(D, c);
         if (c == 0) z[6] += etac * z[2];
-        solve_chain<TM::chunk>(M.A, ch, z);
+        if constexpr (TM::mixed) solve_chain_mixed(M.A, M.Af, ch, z, M.rs);
+        else solve_chain<TM::chunk>(M.A, ch, z);
     }
     tm.sync();
 }
@@ -536,7 +572,19 @@ DDV bool factor_W(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<d
         for (int i = tm.lane; i < 3 * n; i += tm.nl) ukeep[i] = M.Z[i];
     bool ok = true;
     const int nc = n_chains(D);
-    for (int c = tm.lane; c < nc; c += tm.nl) ok = factor_chain(M.A, chain_of(D, c)) && ok;
+    for (int c = tm.lane; c < nc; c += tm.nl) {
+        const Chain ch = chain_of(D, c);
+        if constexpr (TM::mixed) {  // FP32 factors; A keeps the FP64 band for the residuals
+            for (int p = 0; p < ch.len; ++p)
+                for (int m = 0; m < 7; ++m) {
+                    const int i = ch.start + p * ch.stride;
+                    M.Af[7 * i + m] = (float)M.A[7 * i + m];
+                }
+            ok = factor_chain(M.Af, ch) && ok;
+        } else {
+            ok = factor_chain(M.A, ch) && ok;
+        }
+    }
     tm.sync();
     // Z = A^{-1} U
     for (int r = 0; r < 3; ++r) solve_A(tm, D, M, gh, M.Z + r * n);

@@ -14,6 +14,7 @@ struct WarpTeam {
     static constexpr int nl = 32;
     static constexpr int chunk = 4;         // elements per load batch in the chain substitutions
     static constexpr bool reconverge = true;  // explicit reconvergence after divergent table lookups
+    static constexpr bool mixed = false;      // FP32 chain factors + FP64 refinement (ModeMem::Af)
     __device__ __forceinline__ void sync() const { __syncwarp(); }
     __device__ __forceinline__ double sum(double x) const
     {
@@ -37,6 +38,10 @@ struct WarpTeamSeq : WarpTeam {
     static constexpr int chunk = 1;
     static constexpr bool reconverge = false;
 };
+// The forward-solve warp team of the mixed-precision form (DISCOEB_METHOD_RODAS5_STRUCTURED_MIXED)
+struct WarpTeamMixed : WarpTeam {
+    static constexpr bool mixed = true;
+};
 #endif
 
 struct HostTeam {
@@ -44,12 +49,16 @@ struct HostTeam {
     static constexpr int nl = 1;
     static constexpr int chunk = 4;
     static constexpr bool reconverge = false;
+    static constexpr bool mixed = false;
     DHD void sync() const {}
     DHD double sum(double x) const { return x; }
     DHD bool leader() const { return true; }
     DHD double bcast(double x, int) const { return x; }
     template <class B> DHD DualT<B> bcast(const DualT<B>& x, int) const { return x; }
     DHD bool full() const { return false; }
+};
+struct HostTeamMixed : HostTeam {
+    static constexpr bool mixed = true;
 };
 
 }  // namespace dscb

@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(HERE, LIB_NAME)
 METHOD_RODAS5_STRUCTURED = 0
 METHOD_RODAS5_DENSE = 1
 METHOD_RODAS5_DENSE_MIXED = 2
+METHOD_RODAS5_STRUCTURED_MIXED = 3
 
 STATUS_NAMES = {0: "ok", 1: "max_steps exceeded", 2: "non-finite state", 3: "step size underflow", 4: "singular",
                 5: "cosmology index out of range",

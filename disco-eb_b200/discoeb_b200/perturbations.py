@@ -237,7 +237,7 @@ def _check_status(status, nsteps, kmodes, on_failure):
 def solve_modes(*, param, kmodes, tau_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, rtol, atol, pcoeff, icoeff, dcoeff,
                 factormax, factormin, max_steps, return_full, de_guard_eps=1e-9, device=None, warps_per_block=0,
                 on_failure="raise", sort_modes=True, return_stats=False, tau_start=None, switch_tau=None,
-                as_tensor=False):
+                as_tensor=False, method="structured"):
     """Integrate the given modes of one cosmology to ``tau_out`` on the GPU.
 
     Returns numpy ``y`` (``[K, nout, 20]`` or ``[K, nout, nvar]``); with
@@ -245,7 +245,12 @@ def solve_modes(*, param, kmodes, tau_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, 
     override the start times and approximation switch times derived from ``param`` (to hold
     these numerical choices fixed while parameters move, as forward-mode AD does).
     ``as_tensor``: return ``y`` as a device tensor (the caller's mode order) instead of numpy.
+    ``method``: "structured" (FP64 chain factors) or "structured-mixed" (FP32 chain factors, one
+    FP64 residual refinement of every chain solve).
     """
+    methods = {"structured": _abi.METHOD_RODAS5_STRUCTURED, "structured-mixed": _abi.METHOD_RODAS5_STRUCTURED_MIXED}
+    if method not in methods:
+        raise ValueError(f"method must be one of {sorted(methods)}, not {method!r}")
     import torch
     if device is None:
         if not torch.cuda.is_available():
@@ -286,7 +291,7 @@ def solve_modes(*, param, kmodes, tau_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, 
     d_out20 = None if return_full else torch.empty((K, nout, 20), **f64)
     d_stat = torch.empty((2, K), dtype=torch.int32, device=device)
     ctrl = _abi.DiscoebControl(rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin, int(max_steps),
-                               _abi.METHOD_RODAS5_STRUCTURED, int(warps_per_block), 0)
+                               methods[method], int(warps_per_block), 0)
     stream = torch.cuda.current_stream(device).cuda_stream
     rc = L.discoeb_fwd(dc.struct.data_ptr(), ctypes.byref(dc.host), 1, ctypes.byref(ctrl), K, None,
                        d_k.data_ptr(), d_ts.data_ptr(), d_y0.data_ptr(), d_sw.data_ptr(), nout, d_tout.data_ptr(),

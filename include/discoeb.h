@@ -84,6 +84,9 @@ typedef struct {
 #define DISCOEB_METHOD_RODAS5_STRUCTURED 0 /* default: banded-chain + rank-3 LU, FP64 */
 #define DISCOEB_METHOD_RODAS5_DENSE 1      /* dense partial-pivot LU per mode, FP64 */
 #define DISCOEB_METHOD_RODAS5_DENSE_MIXED 2/* dense FP32 LU + FP64 residual refinement */
+/* the structured form with the chain factors in FP32 and one FP64 residual refinement of every
+ * chain solve (discoeb_fwd only; the gradient and adjoint entries answer DISCOEB_EUNSUPPORTED) */
+#define DISCOEB_METHOD_RODAS5_STRUCTURED_MIXED 3
 
 /* per-mode status codes */
 #define DISCOEB_OK 0

@@ -65,6 +65,8 @@ def shim(tmp_path_factory):
     S.shim_jacobian.argtypes = [CP, ctypes.c_double, dp, ctypes.c_double, ctypes.c_int, dp, dp]
     S.shim_wsolve.argtypes = [CP, ctypes.c_double, dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, dp]
     S.shim_solve_mode.argtypes = [CP, CT, ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_int, dp, dp, ip]
+    S.shim_wsolve_mixed.argtypes = S.shim_wsolve.argtypes
+    S.shim_solve_mode_mixed.argtypes = S.shim_solve_mode.argtypes
     S.shim_solve_mode_tangent.argtypes = [CP, ctypes.c_void_p, CT, ctypes.c_double, ctypes.c_double, dp, dp, dp,
                                           ctypes.c_int, dp, dp, dp, ip, dp, ctypes.c_int]
     S.shim_replay.argtypes = [CP, ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_int, dp, dp]

@@ -8,6 +8,47 @@
 
 using namespace dscb;
 
+template <class Team>
+static int wsolve_impl(const DiscoebCosmo* P, double tau, const double* y, double k, int regime, double h,
+                       const double* r, double* x)
+{
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    std::vector<double> mem(mode_mem_doubles(D) + mixed_mem_doubles(D));
+    ModeMem M = carve(mem.data(), D);
+    if (Team::mixed) carve_mixed(mem.data() + mode_mem_doubles(D), D, M);
+    Team tm;
+    std::memcpy(M.y, y, sizeof(double) * n);
+    Bg<Dual> bd;
+    bg_eval(*P, Dual(y[0], 1.0), tau, k, regime, bd);
+    rhs_team(tm, *P, D, bd, k, tau, M.y, M.f, M.col0);
+    Bg<double> b;
+    bg_eval(*P, y[0], tau, k, regime, b);
+    bool ok = factor_W(tm, *P, D, b, k, tau, h, M);
+    std::memcpy(x, r, sizeof(double) * n);
+    solve_W(tm, D, M, h, x);
+    return ok ? 0 : 1;
+}
+
+template <class Team>
+static int solve_mode_impl(const DiscoebCosmo* P, const DiscoebControl* C, double k, double t0, const double* y0,
+                           const double* sw, int nout, const double* tout, double* yout, int* stats)
+{
+    const Dims D = make_dims(*P);
+    std::vector<double> mem(mode_mem_doubles(D) + mixed_mem_doubles(D));
+    ModeMem M = carve(mem.data(), D);
+    if (Team::mixed) carve_mixed(mem.data() + mode_mem_doubles(D), D, M);
+    std::memcpy(M.y, y0, sizeof(double) * D.n);
+    Team tm;
+    const int n = D.n;
+    auto emit = [&](int j, const double* y, int) { std::memcpy(yout + (size_t)j * n, y, sizeof(double) * n); };
+    SolveResult R = solve_mode(tm, *P, D, *C, k, t0, sw, nout, tout, M, emit);
+    stats[0] = R.status;
+    stats[1] = R.steps;
+    stats[2] = R.accepted;
+    return R.status;
+}
+
 extern "C" {
 
 int shim_nvar(const DiscoebCosmo* P) { return make_dims(*P).n; }
@@ -59,21 +100,14 @@ void shim_jacobian(const DiscoebCosmo* P, double tau, const double* y, double k,
 int shim_wsolve(const DiscoebCosmo* P, double tau, const double* y, double k, int regime, double h, const double* r,
                 double* x)
 {
-    const Dims D = make_dims(*P);
-    const int n = D.n;
-    std::vector<double> mem(mode_mem_doubles(D));
-    ModeMem M = carve(mem.data(), D);
-    HostTeam tm;
-    std::memcpy(M.y, y, sizeof(double) * n);
-    Bg<Dual> bd;
-    bg_eval(*P, Dual(y[0], 1.0), tau, k, regime, bd);
-    rhs_team(tm, *P, D, bd, k, tau, M.y, M.f, M.col0);
-    Bg<double> b;
-    bg_eval(*P, y[0], tau, k, regime, b);
-    bool ok = factor_W(tm, *P, D, b, k, tau, h, M);
-    std::memcpy(x, r, sizeof(double) * n);
-    solve_W(tm, D, M, h, x);
-    return ok ? 0 : 1;
+    return wsolve_impl<HostTeam>(P, tau, y, k, regime, h, r, x);
+}
+
+// the same with FP32 chain factors and one FP64 refinement per chain solve
+int shim_wsolve_mixed(const DiscoebCosmo* P, double tau, const double* y, double k, int regime, double h,
+                      const double* r, double* x)
+{
+    return wsolve_impl<HostTeamMixed>(P, tau, y, k, regime, h, r, x);
 }
 
 // forward + tangent solve: raw state and its tangent at the output times (fixed output times)
@@ -126,18 +160,13 @@ int shim_replay(const DiscoebCosmo* P, double k, double t0, const double* y0, co
 int shim_solve_mode(const DiscoebCosmo* P, const DiscoebControl* C, double k, double t0, const double* y0,
                     const double* sw, int nout, const double* tout, double* yout, int* stats)
 {
-    const Dims D = make_dims(*P);
-    std::vector<double> mem(mode_mem_doubles(D));
-    ModeMem M = carve(mem.data(), D);
-    std::memcpy(M.y, y0, sizeof(double) * D.n);
-    HostTeam tm;
-    const int n = D.n;
-    auto emit = [&](int j, const double* y, int) { std::memcpy(yout + (size_t)j * n, y, sizeof(double) * n); };
-    SolveResult R = solve_mode(tm, *P, D, *C, k, t0, sw, nout, tout, M, emit);
-    stats[0] = R.status;
-    stats[1] = R.steps;
-    stats[2] = R.accepted;
-    return R.status;
+    return solve_mode_impl<HostTeam>(P, C, k, t0, y0, sw, nout, tout, yout, stats);
+}
+
+int shim_solve_mode_mixed(const DiscoebCosmo* P, const DiscoebControl* C, double k, double t0, const double* y0,
+                          const double* sw, int nout, const double* tout, double* yout, int* stats)
+{
+    return solve_mode_impl<HostTeamMixed>(P, C, k, t0, y0, sw, nout, tout, yout, stats);
 }
 
 // the 20 output fields and their tangents (output_vars with dual numbers), and the RSA

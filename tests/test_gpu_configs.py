@@ -161,3 +161,25 @@ def test_gpu_jacobian_equals_cpu_build_of_the_tangent_code(torch_cuda, shim):
                 np.testing.assert_allclose(o[4], y_gpu[i, j, 4], rtol=1e-6)
                 scale = np.abs(yd_gpu[d, :, j, 4]).max()
                 assert abs(od[4] - yd_gpu[d, i, j, 4]) <= 1e-6 * scale, (d, i, j, od[4], yd_gpu[d, i, j, 4])
+
+
+def test_gpu_mixed_precision_forward_within_1em4(torch_cuda):
+    """The mixed-precision form (FP32 chain factors, one FP64 refinement of every chain solve) on
+    the batched massive-neutrino configuration: within the benchmark's 1e-4 of the converged oracle
+    and within the solver tolerance of the FP64 form."""
+    from discoeb_b200.perturbations import get_power, solve_modes
+    bg = background("lcdm_mnu", 256)
+    ks = np.geomspace(1e-4, 10.0, 16)
+    tout = bg["tau_of_a_spline"].evaluate(A4)
+    common = dict(param=dict(bg), kmodes=ks, tau_out=tout, rtol=1e-5, atol=1e-8, pcoeff=0.25, icoeff=0.8,
+                  dcoeff=0.0, factormax=20.0, factormin=0.3, max_steps=100000, return_full=False, return_stats=True,
+                  **L143)
+    ym, st_m, n_m = solve_modes(method="structured-mixed", **common)
+    yd, st_d, n_d = solve_modes(method="structured", **common)
+    assert (st_m == 0).all() and (st_d == 0).all()
+    assert np.all(np.abs(n_m - n_d) <= np.maximum(2, 0.02 * n_d)), (n_m, n_d)
+    Pm = get_power(k=ks[:, None], y=ym, idx=4, param=bg)
+    Pd = get_power(k=ks[:, None], y=yd, idx=4, param=bg)
+    Po = get_power(k=ks[:, None], y=_oracle(bg, ks, A4, L143), idx=4, param=bg)
+    assert np.abs(Pm / Po - 1).max() < 1e-4
+    assert np.abs(Pm / Pd - 1).max() < 1e-5

@@ -85,3 +85,51 @@ def test_adaptive_solve_matches_oracle(shim, setup, k):
     assert abs(stats[1] - st.steps) <= max(2, 0.01 * st.steps)  # same step sequence up to rounding flips
     for v in (0, 2, 3, 5):
         np.testing.assert_allclose(ys[:, v], yo[0][:, v], rtol=1e-6)
+
+
+@pytest.mark.parametrize("k", [1e-4, 0.05, 2.0, 10.0])
+def test_mixed_precision_wsolve_matches_oracle(shim, setup, k):
+    """The mixed-precision W solve (FP32 chain factors, one FP64 refinement of every chain solve)
+    against the dense FP64 solve of the oracle's W, at the bar of the FP64 structured solve."""
+    bg, C, OP, _ = setup
+    n = OP.n
+    rng = np.random.default_rng(2)
+    tout, ys = _states(bg, OP, k)
+    worst = 0.0
+    for tau, ybase in zip(tout, ys):
+        y = ybase * (1 + 0.01 * rng.standard_normal(n))
+        for regime in (-1, 0, 2):
+            Jo, _ = OP.jacobian(tau, y, k, regime)
+            for h in (0.05 * tau, 1e-3 * tau):
+                W = np.eye(n) / (0.19 * h) - Jo
+                r = rng.standard_normal(n)
+                x_o = np.linalg.solve(W, r)
+                x_m, x_d = np.zeros(n), np.zeros(n)
+                assert shim.shim_wsolve_mixed(ctypes.byref(C), tau, ptr(y), k, regime, h, ptr(r), ptr(x_m)) == 0
+                assert shim.shim_wsolve(ctypes.byref(C), tau, ptr(y), k, regime, h, ptr(r), ptr(x_d)) == 0
+                np.testing.assert_allclose(x_m, x_o, rtol=0, atol=1e-10 * np.abs(x_o).max())
+                worst = max(worst, float(np.abs(x_m - x_d).max() / np.abs(x_d).max()))
+    assert worst > 0.0  # the FP32 factors do change the rounding
+    print("mixed vs FP64 structured solve:", worst)
+
+
+@pytest.mark.parametrize("k", [1e-3, 0.1, 10.0])
+def test_mixed_precision_adaptive_solve_matches_fp64(shim, setup, k):
+    bg, C, OP, _ = setup
+    n = OP.n
+    ctrl = _abi.DiscoebControl(1e-5, 1e-8, 0.25, 0.8, 0.0, 20.0, 0.3, 100000, 0, 0, 0)
+    tout = bg["tau_of_a_spline"].evaluate(np.array([1 / 3, 0.5, 2 / 3, 1.0]))
+    ts = 0.99 * min(tout.min(), OP.start_time(k))
+    y0 = OP.ics(ts, k)
+    sw = OP.switch_times(k)
+    ys, ym = np.zeros((4, n)), np.zeros((4, n))
+    st_d, st_m = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+    shim.shim_solve_mode(ctypes.byref(C), ctypes.byref(ctrl), k, ts, ptr(y0), ptr(sw), 4, ptr(tout), ptr(ys), st_d)
+    shim.shim_solve_mode_mixed(ctypes.byref(C), ctypes.byref(ctrl), k, ts, ptr(y0), ptr(sw), 4, ptr(tout), ptr(ym),
+                               st_m)
+    assert st_d[0] == 0 and st_m[0] == 0
+    assert abs(st_m[1] - st_d[1]) <= max(2, 0.01 * st_d[1])
+    # the refined solves differ from the FP64 ones by ~1e-12 (the test above), which the error
+    # control turns into different step sizes: the solutions then agree to well inside rtol
+    for v in (0, 2, 3, 5):
+        np.testing.assert_allclose(ym[:, v], ys[:, v], rtol=1e-6)
