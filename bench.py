@@ -44,6 +44,11 @@ METRIC = "fwd+adjoint k-mode solves/s at ≤1e-4 rel err vs FP64 oracle; ms per 
 # 0.304 MB), scaled by the number of modes: the initial states, their tangents and the outputs grow
 # with it, the tables are shared (so this slightly overstates a full launch)
 DRAM_BYTES_PER_MODE = {"fwd+grad": 1.566e6 / 48, "forward": 0.304e6 / 48}
+# FP64 work per step attempt, counted by ncu on a 48-mode launch of the same kernel (thread-level
+# smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum, a DFMA counted as two flops,
+# over the launch's step attempts): jvp_block_kernel 5.526e9 + 14.086e9 + 2 x 15.101e9 = 4.982e10
+# flops over 19187 attempts.  Scaled by the measured attempts of the timed launch.
+FP64_FLOPS_PER_ATTEMPT = {"fwd+grad": 4.9815e10 / 19187}
 UNIT = "k-mode solves/s"
 
 
@@ -726,6 +731,7 @@ def main():
         d2h += 8 * n_dir * K * nout * 20
 
     # ---- roofline: FP64 work of the structured Rodas5 step against a measured FP64 peak ----
+    # (counted by ncu where a capture exists, FP64_FLOPS_PER_ATTEMPT; else estimated from the code)
     flops_per_step = 850.0 * n + 1650.0  # forward structured step, counted from stepper.cuh
     # one tangent direction's work per step, estimated from the operation mix of tangent_step
     # (stepper.cuh): 8 stages x (two dual RHS passes ~ 4 real RHS passes of ~10 n + 300 flops, one
@@ -736,6 +742,11 @@ def main():
     # forward once per mode, each direction's tangent on every step (counted on every attempt:
     # an upper bound, the tangent runs on accepted steps only)
     work = step_attempts * (flops_per_step + tangent_per_step * n_dir) if grad else step_attempts * flops_per_step
+    flops_source = "estimated from the operation mix of the step code (upper bound: every attempt)"
+    if args.mode in FP64_FLOPS_PER_ATTEMPT and args.workload == "pk_lcdm_mnu_k512_z4" and args.method == "structured":
+        work = step_attempts * FP64_FLOPS_PER_ATTEMPT[args.mode]
+        flops_source = ("ncu FP64 thread instructions (dadd + dmul + 2 dfma) per step attempt of a 48-mode launch "
+                        "of the same kernel, times this launch's step attempts")
     dense_work = step_attempts * dense_per_step * (1 + n_dir)
     achieved = work / (ms / 1e3) / 1e12
     peak = fp64_fma_tflops(torch, device) if rank == 0 and not args.kernel_only else None
@@ -799,6 +810,7 @@ def main():
                          "traffic": DRAM_BYTES_PER_MODE.get(args.mode, 0.0) * K or None,
                          "traffic_source": "ncu capture of 48 modes of the same kernel, scaled by the mode count",
                          "peak_source": "FP64 FMA throughput measured in this run (discoeb_fma_rate)",
+                         "flops_source": flops_source,
                          "fp64_dgemm_tflops": dgemm,
                          "dense_equivalent_tflops": dense_work / (ms / 1e3) / 1e12},
             "clocks": clocks,
