@@ -47,8 +47,9 @@ DRAM_BYTES_PER_MODE = {"fwd+grad": 1.566e6 / 48, "forward": 0.304e6 / 48}
 # FP64 work per step attempt, counted by ncu on a 48-mode launch of the same kernel (thread-level
 # smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum, a DFMA counted as two flops,
 # over the launch's step attempts): jvp_block_kernel 5.526e9 + 14.086e9 + 2 x 15.101e9 = 4.982e10
-# flops over 19187 attempts.  Scaled by the measured attempts of the timed launch.
-FP64_FLOPS_PER_ATTEMPT = {"fwd+grad": 4.9815e10 / 19187}
+# flops over 19187 attempts; fwd_structured_kernel 0.4558e9 + 0.9701e9 + 2 x 1.4198e9 = 4.2655e9 flops over
+# 19187 attempts.  Scaled by the measured attempts of the timed launch.
+FP64_FLOPS_PER_ATTEMPT = {"fwd+grad": 4.9815e10 / 19187, "forward": 4.2655e9 / 19187}
 UNIT = "k-mode solves/s"
 
 

@@ -219,20 +219,27 @@ template <class TM> DDV void hier_stat_reduce(const TM& tm, const Dims& D, HierS
 // lambda . f(y) at background b, up to terms that do not depend on b or y, with the hierarchy rows
 // through h (hier_stat of the same lambda and y); lam0 = false leaves out row 0 (a' = a'/a a).
 // Y(j) gives state entry j as a T.
-template <class T, class YF>
-DHD T functional(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau, const double* lam,
-                 bool lam0, const YF& Y, const HierStat& h)
+// LF(ss) gives lambda at special row ss.
+template <class T, class YF, class LF>
+DHD T functional_l(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau, const LF& L,
+                   bool lam0, const YF& Y, const HierStat& h)
 {
     const HostTeam ht;
     T sp[15], g0, g1, g2;
     special_part<HostTeam, T, T>(ht, P, D, b, k, tau, Y, T(1.0), T(1.0), sp, g0, g1, g2);
     T Q = 0.0;
-    for (int ss = lam0 ? 0 : 1; ss < 15; ++ss) Q = Q + lam[special_row(D, ss)] * sp[ss];
+    for (int ss = lam0 ? 0 : 1; ss < 15; ++ss) Q = Q + L(ss) * sp[ss];
     Q = Q + b.opac * h.aop;
     for (int q = 0; q < D.nq; ++q) Q = Q + rcp(inv_vq(P, b, q)) * h.bq[q];
     Q = Q + g0 * (h.gc[0] + b.opac * h.gop[0]) + g1 * (h.gc[1] + b.opac * h.gop[1]) +
         g2 * (h.gc[2] + b.opac * h.gop[2]);
     return Q;
+}
+template <class T, class YF>
+DHD T functional(const DiscoebCosmo& P, const Dims& D, const Bg<T>& b, double k, double tau, const double* lam,
+                 bool lam0, const YF& Y, const HierStat& h)
+{
+    return functional_l<T>(P, D, b, k, tau, [&](int ss) { return lam[special_row(D, ss)]; }, lam0, Y, h);
 }
 
 // ---- table knot cotangents ----
@@ -262,19 +269,114 @@ DDV void tab_add(TabAcc& acc, int xs, int i, double g, double* tbar, int stride)
     acc.w += g;
 }
 
-// ---- per-warp adjoint workspace ----
-struct AdjMem {
-    double *Uk, *Zt, *Kb, *us, *ub, *yb, *rho, *lam, *pb, *sc;
+// ---- deferred functionals ----
+// The parameter and table-knot cotangents of a reverse step do not feed back into the state
+// cotangents, so their functionals can be evaluated after the step (or by another warp): a
+// record holds what a functional lambda . f(Y; b) needs besides the seed, compactly:
+//   [0] a, [1] tau, [2] regime, [3] unused, [4, 19) lambda on the 15 special rows,
+//   [19, 19 + n_read) Y on the entries the special rows read, then the hierarchy statistics.
+// A step leaves 17 records: its 8 stage functionals (Dual, at the stage states), the 8 terms
+// of W's dependence on y_n through J(y_n) (Dual, at y_n, row 0 left out) and the column-0 term
+// (hyper-dual, at y_n).
+constexpr int kRecPerStep = 17;
+constexpr int kDeferredSeeds = kNX - 1;  // every x input but a
+DHD int hs_doubles() { return (int)(sizeof(HierStat) / sizeof(double)); }
+DHD int drec_doubles(const Dims& D) { return 19 + n_read(D) + hs_doubles(); }
+// inverse of read_index (-1: not read)
+DHD int read_slot(const Dims& D, int j)
+{
+    if (j >= 2 && j <= 10) return j - 2;
+    if (j == D.idxgp) return 9;
+    if (j == D.idxgp + 2) return 10;
+    if (j >= D.idxr && j <= D.idxr + 3) return 11 + (j - D.idxr);
+    if (j == D.n - 2) return 15;
+    if (j == D.n - 1) return 16;
+    if (j >= D.iq0 && j < D.iq0 + 2 * D.nq) return 17 + (j - D.iq0);
+    return -1;
+}
+
+// write record rec (team-parallel): lambda from lam (full length), Y from y (full length), hs
+template <class TM>
+DDV void drec_write(const TM& tm, const Dims& D, double* rec, double a, double tau, int regime, const double* lam,
+                    const double* y, const HierStat& hs)
+{
+    const int nr = n_read(D);
+    if (tm.leader()) {
+        rec[0] = a;
+        rec[1] = tau;
+        rec[2] = (double)regime;
+        rec[3] = 0.0;
+        const double* h = reinterpret_cast<const double*>(&hs);
+        for (int q = 0; q < hs_doubles(); ++q) rec[19 + nr + q] = h[q];
+    }
+    for (int ss = tm.lane; ss < 15; ss += tm.nl) rec[4 + ss] = lam[special_row(D, ss)];
+    for (int r = tm.lane; r < nr; r += tm.nl) rec[19 + r] = y[read_index(D, r)];
+}
+
+// gpart of the functional of record rec (kind 0: stage, 1: W term, 2: column-0 term) seeded in xs
+template <class T>
+DHD double drec_eval(const DiscoebCosmo& P, const Dims& D, double k, const double* rec, int kind, int xs)
+{
+    const double a = rec[0], tau = rec[1];
+    const int regime = (int)rec[2];
+    const TabIdx ti = tab_idx(P, log(a));
+    Bg<T> b;
+    bg_seeded(P, a, tau, k, regime, ti, xs, b);
+    HierStat hs;
+    double* h = reinterpret_cast<double*>(&hs);
+    const int nr = n_read(D);
+    for (int q = 0; q < hs_doubles(); ++q) h[q] = rec[19 + nr + q];
+    auto Y = [&](int j) {
+        const int r = read_slot(D, j);
+        return T(r >= 0 ? rec[19 + r] : nan(""));  // an entry outside the read list would poison the result
+    };
+    auto L = [&](int ss) { return rec[4 + ss]; };
+    return gpart(functional_l<T>(P, D, b, k, tau, L, kind != 1, Y, hs));
+}
+
+// Accumulators of the deferred seeds: parameter cotangents pb[16] (index = seed) and one table
+// accumulator per knot seed.  The lane that evaluates seed xs is the only one touching its entry.
+struct DefAcc {
+    double* pb;
     TabAcc* tab;
 };
-DHD int adj_mem_doubles(const Dims& D) { return 19 * D.n + 16 + 32 + 2 * kNTabSeeds; }
-DHD AdjMem carve_adj(double* base, const Dims& D)
+
+// The 17 records of one step, every deferred seed (lanes take seeds), accumulated into acc
+template <class TM>
+DDV void deferred_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, const double* recs,
+                       const DefAcc& acc, double* tbar, int tstride)
+{
+    const int rd = drec_doubles(D);
+    for (int r = 0; r < kRecPerStep; ++r) {
+        const double* rec = recs + (size_t)r * rd;
+        const int kind = r < 8 ? 0 : (r < 16 ? 1 : 2);
+        const TabIdx ti = tab_idx(P, log(rec[0]));
+        for (int sd = tm.lane; sd < kDeferredSeeds; sd += tm.nl) {
+            const int xs = 1 + sd;
+            const double g = kind == 2 ? drec_eval<HDual>(P, D, k, rec, kind, xs) : drec_eval<Dual>(P, D, k, rec, kind, xs);
+            if (xs < X_KNOT0) acc.pb[xs] += g;
+            else tab_add(acc.tab[xs - X_KNOT0], xs, ti.i[kseed_table(xs)], g, tbar, tstride);
+        }
+    }
+    tm.sync();
+}
+
+// ---- per-warp adjoint workspace ----
+// With own_step_buffers the workspace also holds the step's U columns, Zt and deferred records
+// (the single-team sweep); the warp-split kernel keeps those in its shared step slots.
+struct AdjMem {
+    double *Uk, *Zt, *Kb, *us, *ub, *yb, *rho, *lam, *pb, *sc, *rec;
+    TabAcc* tab;
+};
+DHD int adj_mem_doubles(const Dims& D, bool own_step_buffers = true)
+{
+    return 13 * D.n + 16 + 32 + 2 * kNTabSeeds + (own_step_buffers ? 6 * D.n + kRecPerStep * drec_doubles(D) : 0);
+}
+DHD AdjMem carve_adj(double* base, const Dims& D, bool own_step_buffers = true)
 {
     const int n = D.n;
     AdjMem A;
-    A.Uk = base;          // 3n  U columns at the step start (the factorisation overwrites M.Z)
-    A.Zt = A.Uk + 3 * n;  // 3n  A^{-T} G^T
-    A.Kb = A.Zt + 3 * n;  // 8n  stage cotangents Kbar_s, replaced by rbar_s = W^{-T} Kbar_s in turn
+    A.Kb = base;          // 8n  stage cotangents Kbar_s, replaced by rbar_s = W^{-T} Kbar_s in turn
     A.us = A.Kb + 8 * n;  // n   current stage state
     A.ub = A.us + n;      // n   ubar of the current stage
     A.yb = A.ub + n;      // n   ybar_n being accumulated
@@ -283,6 +385,14 @@ DHD AdjMem carve_adj(double* base, const Dims& D)
     A.pb = A.lam + n;     // 16  parameter cotangents (index = seed)
     A.sc = A.pb + 16;     // 32  scalars
     A.tab = reinterpret_cast<TabAcc*>(A.sc + 32);  // kNTabSeeds accumulators (2 doubles each)
+    double* rest = A.sc + 32 + 2 * kNTabSeeds;
+    if (own_step_buffers) {
+        A.Uk = rest;          // 3n  U columns at the step start (the factorisation overwrites M.Z)
+        A.Zt = A.Uk + 3 * n;  // 3n  A^{-T} G^T
+        A.rec = A.Zt + 3 * n; // the step's deferred records
+    } else {
+        A.Uk = A.Zt = A.rec = nullptr;
+    }
     return A;
 }
 static_assert(sizeof(TabAcc) <= 2 * sizeof(double), "TabAcc must fit two doubles");
@@ -509,14 +619,17 @@ DDV void output_adjoint(const TM& tm, const DiscoebCosmo& P, const Dims& D, doub
 
 // ---- the reverse of one step ----
 // On entry: M holds the step's forward recomputation (rodas5_step from y_n = M.y, with factor_W's
-// U columns in A.Uk) and A.Zt = A^{-T} G^T; A.lam = ybar_{n+1}.  On return A.lam = ybar_n, and the
-// parameter / table cotangents of the step are added to A.pb and the table accumulators.
+// U columns in Uk) and Zt = A^{-T} G^T; A.lam = ybar_{n+1}.  On return A.lam = ybar_n.  This is the
+// part of the step the state cotangents depend on (the chain of the reverse sweep): the seeds of
+// the state entries and of a.  The parameter and table-knot seeds of the step's functionals are
+// left in the 17 records at recs (deferred_step evaluates them).
 template <class TM>
 DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
-                      const ModeMem& M, const AdjMem& A, double* tbar, int tstride, int& hint)
+                      const ModeMem& M, const AdjMem& A, const double* Uk, const double* Zt, double* recs, int& hint)
 {
     const int n = D.n;
     const double ih = 1.0 / h;
+    const int rd = drec_doubles(D);
     // stage cotangents: Kbar_7 = ybar_{n+1}, the others start at zero; ubar_7 = ybar_{n+1}
     for (int i = tm.lane; i < n; i += tm.nl) {
         for (int s = 0; s < 7; ++s) A.Kb[s * n + i] = 0.0;
@@ -530,12 +643,12 @@ DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
     bflags.rsa = (regime & 1) != 0;
     bflags.ufa = !bflags.rsa && (regime & 2) != 0;
     bflags.tca = !bflags.rsa && (regime & 4) != 0;
-    const int nseed = kNX + n_read(D);
+    const int nseed = 1 + n_read(D);  // a and the state entries the functional reads
     for (int s = 7; s >= 0; --s) {
         const double* Ks = M.K + s * n;
         // rbar_s = W^{-T} Kbar_s, in place (Kbar_s is complete: only later stages add to it)
         double* rb = A.Kb + s * n;
-        solve_WT(tm, D, M, A.Uk, A.Zt, h, rb);
+        solve_WT(tm, D, M, Uk, Zt, h, rb);
         // stage state u_s
         for (int i = tm.lane; i < n; i += tm.nl) {
             double v = M.y[i];
@@ -548,8 +661,8 @@ DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
         }
         tm.sync();
         // ubar_s += J(u_s)^T rbar_s: hierarchy rows by the gather, the special rows, the metric
-        // functionals and column 0 by the seeded functional; the parameter and table cotangents of
-        // rbar_s . f(t_s, u_s) from the same functional
+        // functionals and column 0 by the seeded functional (its parameter and table seeds go to
+        // the stage's record)
         const double ts = (s <= 5) ? t + kR5.c[s] * h : t + h;
         Bg<double> bs;
         bg_eval_team(tm, P, A.us[0], ts, k, regime, bs, hint);
@@ -558,6 +671,7 @@ DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
         hier_stat_lane(tm, P, D, bs, k, rb, A.us, hs);
         hier_stat_reduce(tm, D, hs);
         hier_gather(tm, P, D, bs, k, rb, A.ub);
+        drec_write(tm, D, recs + (size_t)s * rd, A.us[0], ts, regime, rb, A.us, hs);
         tm.sync();
         {
             const double loga = log(A.us[0]);
@@ -565,16 +679,14 @@ DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
             for (int base = 0; base < nseed; base += tm.nl) {
                 const int sid = base + tm.lane;
                 if (sid < nseed) {
-                    const int xs = sid < kNX ? sid : -1;
-                    const int yj = sid < kNX ? -1 : read_index(D, sid - kNX);
+                    const int xs = sid == 0 ? X_A : -1;
+                    const int yj = sid == 0 ? -1 : read_index(D, sid - 1);
                     Bg<Dual> bd;
                     bg_seeded(P, A.us[0], ts, k, regime, ti, xs, bd);
                     auto Y = [&](int j) { return Dual(A.us[j], j == yj ? 1.0 : 0.0); };
                     const double g = gpart(functional<Dual>(P, D, bd, k, ts, rb, true, Y, hs));
                     if (xs < 0) A.ub[yj] += g;
-                    else if (xs == X_A) A.ub[0] += g;
-                    else if (xs < X_KNOT0) A.pb[xs] += g;
-                    else tab_add(A.tab[xs - X_KNOT0], xs, ti.i[kseed_table(xs)], g, tbar, tstride);
+                    else A.ub[0] += g;
                 }
                 tm.sync();
             }
@@ -603,28 +715,35 @@ DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
         bg_eval_team(tm, P, M.y[0], t, k, regime, b0, hint);
         const double loga = log(M.y[0]);
         const TabIdx ti = tab_idx(P, loga);
-        // (a) columns >= 1: the a- and x-gradient of sum_s rbar_s . (C(b_n) K_s[1:]) (row 0 left out)
+        // (a) columns >= 1: the a-gradient of sum_s rbar_s . (C(b_n) K_s[1:]) (row 0 left out), one
+        // stage per lane; the x-gradients are deferred (records 8..15)
         for (int s = 0; s < 8; ++s) {
-            const double* Ks = M.K + s * n;
-            const double* rb = A.Kb + s * n;
             HierStat hs;
             hier_stat_zero(hs);
-            hier_stat_lane(tm, P, D, b0, k, rb, Ks, hs);
+            hier_stat_lane(tm, P, D, b0, k, A.Kb + s * n, M.K + s * n, hs);
             hier_stat_reduce(tm, D, hs);
-            for (int xs = tm.lane; xs < kNX; xs += tm.nl) {
-                Bg<Dual> bd;
-                bg_seeded(P, M.y[0], t, k, regime, ti, xs, bd);
-                auto Y = [&](int j) { return Dual(Ks[j], 0.0); };
-                const double g = gpart(functional<Dual>(P, D, bd, k, t, rb, false, Y, hs));
-                if (xs == X_A) A.yb[0] += g;
-                else if (xs < X_KNOT0) A.pb[xs] += g;
-                else tab_add(A.tab[xs - X_KNOT0], xs, ti.i[kseed_table(xs)], g, tbar, tstride);
-            }
-            tm.sync();
+            drec_write(tm, D, recs + (size_t)(8 + s) * rd, M.y[0], t, regime, A.Kb + s * n, M.K + s * n, hs);
         }
+        tm.sync();
+        double ga = 0.0;
+        for (int s = tm.lane; s < 8; s += tm.nl) {
+            const double* rec = recs + (size_t)(8 + s) * rd;
+            HierStat hs;
+            double* hp = reinterpret_cast<double*>(&hs);
+            for (int q = 0; q < hs_doubles(); ++q) hp[q] = rec[19 + n_read(D) + q];
+            Bg<Dual> bd;
+            bg_seeded(P, M.y[0], t, k, regime, ti, X_A, bd);
+            const double* Ks = M.K + s * n;
+            auto Y = [&](int j) { return Dual(Ks[j], 0.0); };
+            ga += gpart(functional<Dual>(P, D, bd, k, t, A.Kb + s * n, false, Y, hs));
+        }
+        ga = tm.sum(ga);
+        if (tm.leader()) A.yb[0] += ga;
+        tm.sync();
         // (b) column 0: rho . (d f / d a)(y_n) with rho = sum_s K_s[0] rbar_s; its gradient in
         // y_n[1:] is C'(a)^T rho (hierarchy rows by the gather in Dual a, the rest by the seeded
-        // functional in hyper-dual numbers), in a and the x inputs the mixed second derivative
+        // functional in hyper-dual numbers), in a the second derivative; the x-gradients (mixed
+        // second derivatives) are deferred (record 16)
         HierStat hs;
         hier_stat_zero(hs);
         hier_stat_lane(tm, P, D, b0, k, A.rho, M.y, hs);
@@ -635,20 +754,19 @@ DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
             bg_eval_team(tm, P, Dual(M.y[0], 1.0), t, k, regime, bda, hh);
             hier_gather(tm, P, D, bda, k, A.rho, A.yb);
         }
+        drec_write(tm, D, recs + (size_t)16 * rd, M.y[0], t, regime, A.rho, M.y, hs);
         tm.sync();
         for (int base = 0; base < nseed; base += tm.nl) {
             const int sid = base + tm.lane;
             if (sid < nseed) {
-                const int xs = sid < kNX ? sid : -1;
-                const int yj = sid < kNX ? -1 : read_index(D, sid - kNX);
+                const int xs = sid == 0 ? X_A : -1;
+                const int yj = sid == 0 ? -1 : read_index(D, sid - 1);
                 Bg<HDual> bh;
                 bg_seeded(P, M.y[0], t, k, regime, ti, xs, bh);
                 auto Y = [&](int j) { return HDual(Dual(M.y[j], 0.0), Dual(j == yj ? 1.0 : 0.0, 0.0)); };
                 const double g = gpart(functional<HDual>(P, D, bh, k, t, A.rho, true, Y, hs));
                 if (xs < 0) A.yb[yj] += g;
-                else if (xs == X_A) A.yb[0] += g;
-                else if (xs < X_KNOT0) A.pb[xs] += g;
-                else tab_add(A.tab[xs - X_KNOT0], xs, ti.i[kseed_table(xs)], g, tbar, tstride);
+                else A.yb[0] += g;
             }
             tm.sync();
         }
@@ -754,7 +872,8 @@ DDV void bwd_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, 
                 tm.sync();
                 --jout;
             }
-            adjoint_step(tm, P, D, k, tm0, h, regime, M, A, tbar, tstride, hint);
+            adjoint_step(tm, P, D, k, tm0, h, regime, M, A, A.Uk, A.Zt, A.rec, hint);
+            deferred_step(tm, P, D, k, A.rec, DefAcc{A.pb, A.tab}, tbar, tstride);
         }
     }
     if (toutbar && tm.leader())

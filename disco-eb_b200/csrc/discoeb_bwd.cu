@@ -1,14 +1,16 @@
 // Discrete adjoint on sm_100a: the recording forward solve, the reverse sweep and the contraction
 // of the cotangents with parameter tangents; C ABI (include/discoeb.h).
 //
-// Layout: one warp per k-mode.  The recording forward is the forward solve whose accept hook
+// Layout: the recording forward is the forward solve (one warp per k-mode) whose accept hook
 // writes each accepted step's end time (8 bytes) and every checkpoint_every-th start state into
-// the caller's record buffer.  The reverse sweep holds its cosmology, the recomputed step (state,
-// stages, factorisation) and the adjoint workspace in shared memory (42 n doubles: one warp per
-// block, four blocks per SM at n = 143), recomputes each segment of checkpoint_every steps from
-// its checkpoint into the caller's workspace, and takes it apart step by step.  Table-knot
-// cotangents are summed over the modes of a cosmology with double-precision atomics (the order of
-// those additions is not fixed, so they agree between runs to rounding, not bit for bit).
+// the caller's record buffer.  The reverse sweep runs one block of four warps per mode (replay of
+// the segments from their checkpoints, recomputation of each step, the state-cotangent chain, the
+// parameter and table seeds; bwd_split_kernel), with the cosmology, two recomputed steps, the
+// critical warp's workspace and two steps' deferred records in shared memory (~103 KB at
+// n = 143: two blocks per SM) and two segment buffers per mode in the caller's workspace.
+// Table-knot cotangents are summed over the modes of a cosmology with double-precision atomics
+// (the order of those additions is not fixed, so they agree between runs to rounding, not bit
+// for bit).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -119,47 +121,247 @@ __global__ void __launch_bounds__(128) fwd_record_kernel(
     }
 }
 
-__global__ void __launch_bounds__(32) bwd_kernel(
+// ---- the reverse sweep, split over four cooperating warps per mode ----
+// Warp roles (one mode per block, steps taken apart last to first, "job" j = step nacc - 1 - j):
+//   0 critical:   the state-cotangent chain of every step (adjoint_step) and the output layer;
+//   1 recompute:  each step's stages, factorisation, U columns and Zt into one of two shared
+//                 step slots, from the step's start state;
+//   2 replay:     each segment of `every` steps re-run from its checkpoint into one of two
+//                 global segment buffers (the start states the recompute warp reads);
+//   3 deferred:   the parameter and table-knot seeds of every step's 17 functionals (records in
+//                 one of two shared record buffers), one seed per lane.
+// Hand-over by counters in shared memory, every wait bounded (a wait that runs out sets the
+// block's abort flag, every warp leaves its loop, the mode reports DISCOEB_ABORTED with NaN
+// results and the launch ends normally).
+constexpr long long kMaxPollsB = 1LL << 24;  // ~2 s with the back-off below; a step takes < 1 ms
+enum { F_REC = 0, F_CRIT = 1, F_DEF = 2, F_SEG = 3, F_SEGUSED = 4, F_ABORT = 5, kNFlags = 8 };
+
+__device__ bool wait_flag(const WarpTeam& tm, volatile int* flags, int which, int target)
+{
+    int ok = 0;
+    if (tm.leader()) {
+        long long polls = 0;
+        while (true) {
+            if (flags[which] >= target) { ok = 1; break; }
+            if (flags[F_ABORT]) break;
+            if (++polls > kMaxPollsB) { flags[F_ABORT] = 1; break; }
+            __nanosleep(100);
+        }
+        __threadfence_block();
+    }
+    return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+__device__ void post_flag(const WarpTeam& tm, volatile int* flags, int which, int value)
+{
+    tm.sync();
+    if (tm.leader()) {
+        __threadfence_block();
+        flags[which] = value;
+    }
+    tm.sync();
+}
+
+DHD int slot_doubles(const Dims& D) { return mode_mem_doubles(D) + 6 * D.n + 4; }
+DHD long long bwd_ws_doubles_per_mode(const Dims& D, int every)
+{
+    return 2LL * every * D.n + mode_mem_doubles(D);
+}
+
+__global__ void __launch_bounds__(128, 2) bwd_split_kernel(
     const DiscoebCosmo* __restrict__ cosmos, int n_cosmo, const int32_t* __restrict__ mode_cosmo, int n_modes,
     const double* __restrict__ kmodes, const double* __restrict__ tau_start, const double* __restrict__ sw, int n_out,
     const double* __restrict__ tau_out, int cap, int every, long long rec_doubles, const double* __restrict__ records,
-    const int32_t* __restrict__ n_acc, const int32_t* __restrict__ fwd_status, double* seg,
-    const double* __restrict__ ybar20, int mem_doubles, int adj_doubles, double* y0_bar, double* tau_out_bar,
-    double* par_bar, double* table_bar, int tstride, int table_per_mode, int32_t* status)
+    const int32_t* __restrict__ n_acc, const int32_t* __restrict__ fwd_status, double* ws,
+    const double* __restrict__ ybar20, int mem_doubles, double* y0_bar, double* tau_out_bar, double* par_bar,
+    double* table_bar, int tstride, int table_per_mode, int32_t* status)
 {
     extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5;
     const WarpTeam tm{(int)(threadIdx.x & 31)};
     const int mode = blockIdx.x;
     if (mode >= n_modes) return;
     DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(smem);
-    double* wmem = smem + kCosmoDoublesB;
+    int* flags = reinterpret_cast<int*>(smem + kCosmoDoublesB);
+    volatile int* vf = flags;
+    double* wmem = smem + kCosmoDoublesB + kNFlags / 2;
     const double qnan = __longlong_as_double(0x7ff8000000000000LL);
     const int ci = mode_cosmo ? mode_cosmo[mode] : 0;
     int st = fwd_status[mode];
     if (ci < 0 || ci >= n_cosmo) st = DISCOEB_BAD_INDEX;
     if (st == DISCOEB_OK) {
-        copy_cosmo_warp(tm, cosmos + ci, P);
-        if (mode_mem_doubles(make_dims(*P)) != mem_doubles || adj_mem_doubles(make_dims(*P)) != adj_doubles)
-            st = DISCOEB_BAD_INDEX;
+        const int* src = reinterpret_cast<const int*>(cosmos + ci);
+        int* dst = reinterpret_cast<int*>(P);
+        for (int i = threadIdx.x; i < (int)(sizeof(DiscoebCosmo) / 4); i += blockDim.x) dst[i] = src[i];
     }
+    if (threadIdx.x < kNFlags) flags[threadIdx.x] = 0;
+    __syncthreads();
+    if (st == DISCOEB_OK && mode_mem_doubles(make_dims(*P)) != mem_doubles) st = DISCOEB_BAD_INDEX;
     const int n = (mem_doubles - 4 * kMaxSlots - 32) / 23;  // state size of the launch (mode_mem_doubles)
-    if (st != DISCOEB_OK) {  // no forward to take apart: report, write NaN
-        for (int i = tm.lane; i < n; i += 32) y0_bar[(size_t)mode * n + i] = qnan;
-        for (int j = tm.lane; j < n_out; j += 32) tau_out_bar[(size_t)mode * n_out + j] = qnan;
-        for (int q = tm.lane; q < 8; q += 32) par_bar[(size_t)mode * 8 + q] = qnan;
-        if (tm.leader()) status[mode] = st;
+    if (st != DISCOEB_OK) {  // no forward to take apart: report, write NaN (the whole block returns)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) y0_bar[(size_t)mode * n + i] = qnan;
+        for (int j = threadIdx.x; j < n_out; j += blockDim.x) tau_out_bar[(size_t)mode * n_out + j] = qnan;
+        for (int q = threadIdx.x; q < 8; q += blockDim.x) par_bar[(size_t)mode * 8 + q] = qnan;
+        if (threadIdx.x == 0) status[mode] = st;
         return;
     }
     const Dims D = make_dims(*P);
-    ModeMem M = carve(wmem, D);
-    AdjMem A = carve_adj(wmem + mem_doubles, D);
+    const double k = kmodes[mode];
+    const double t0 = tau_start[mode];
+    const double* swm = sw + 3 * mode;
+    const double* tout = tau_out + (size_t)ci * n_out;
     const double* rec = records + (size_t)mode * rec_doubles;
-    bwd_mode(tm, *P, D, kmodes[mode], tau_start[mode], sw + 3 * mode, n_out, tau_out + (size_t)ci * n_out, rec,
-             rec + cap, every, n_acc[mode], seg + (size_t)mode * every * n, ybar20 + (size_t)mode * n_out * 20, M, A,
-             y0_bar + (size_t)mode * n, tau_out_bar + (size_t)mode * n_out,
-             table_bar + (size_t)(table_per_mode ? mode : ci) * 8 * tstride, tstride);
-    for (int q = tm.lane; q < 8; q += 32) par_bar[(size_t)mode * 8 + q] = A.pb[X_GRHOM + q];
-    if (tm.leader()) status[mode] = DISCOEB_OK;
+    const double* tlog = rec;
+    const double* ckpt = rec + cap;
+    const int nacc = n_acc[mode];
+    double* tbar = table_bar + (size_t)(table_per_mode ? mode : ci) * 8 * tstride;
+    // shared: critical warp's workspace, two step slots, two record buffers, deferred accumulators
+    AdjMem A = carve_adj(wmem, D, false);
+    double* slots = wmem + adj_mem_doubles(D, false);
+    const int sd = slot_doubles(D);
+    double* recbuf = slots + 2 * sd;
+    const int rb = kRecPerStep * drec_doubles(D);
+    double* dpb = recbuf + 2 * rb;
+    TabAcc* dtab = reinterpret_cast<TabAcc*>(dpb + 16);
+    auto slot_mem = [&](int j, ModeMem& M, double*& Uk, double*& Zt, double*& meta) {
+        double* b = slots + (size_t)(j & 1) * sd;
+        M = carve(b, D);
+        Uk = b + mem_doubles;
+        Zt = Uk + 3 * n;
+        meta = Zt + 3 * n;
+    };
+    // global: two segment buffers and the replay warp's step workspace
+    double* mws = ws + (size_t)mode * bwd_ws_doubles_per_mode(D, every);
+    double* segbuf = mws;
+    const int last_sg = nacc > 0 ? (nacc - 1) / every : -1;
+    int hint = P->xe_loga.n_knots / 2;
+
+    if (warp == 0) {
+        // ---- critical ----
+        for (int i = tm.lane; i < n; i += 32) A.lam[i] = 0.0;
+        for (int q = tm.lane; q < 16; q += 32) A.pb[q] = 0.0;
+        for (int q = tm.lane; q < kNTabSeeds; q += 32) {
+            A.tab[q].cur = -1;
+            A.tab[q].w = 0.0;
+        }
+        tm.sync();
+        int jout = n_out - 1;
+        const double* ob = ybar20 + (size_t)mode * n_out * 20;
+        for (int j = 0; j < nacc; ++j) {
+            if (!wait_flag(tm, vf, F_REC, j + 1)) break;
+            if (!wait_flag(tm, vf, F_DEF, j - 1)) break;
+            ModeMem M;
+            double *Uk, *Zt, *meta;
+            slot_mem(j, M, Uk, Zt, meta);
+            const double tm0 = meta[0], h = meta[1];
+            const int regime = (int)meta[2];
+            while (jout >= 0 && tout[jout] > tm0) {  // outputs emitted at the end of this step
+                for (int i = tm.lane; i < n; i += 32) {
+                    A.us[i] = M.u[i] + M.K[7 * n + i];
+                    A.ub[i] = 0.0;
+                }
+                tm.sync();
+                output_adjoint(tm, *P, D, tout[jout], k, A.us, ob + (size_t)jout * 20, A, A.ub, tbar, tstride);
+                Bg<double> bo;
+                bg_eval_team(tm, *P, A.us[0], tout[jout], k, regime, bo, hint);
+                rhs_team(tm, *P, D, bo, k, tout[jout], A.us, A.yb, (double*)nullptr);
+                tm.sync();
+                double acc = 0.0;
+                for (int i = tm.lane; i < n; i += 32) {
+                    acc += A.ub[i] * A.yb[i];
+                    A.lam[i] += A.ub[i];
+                }
+                const double tb = tm.sum(acc);
+                if (tm.leader()) tau_out_bar[(size_t)mode * n_out + jout] = tb;
+                tm.sync();
+                --jout;
+            }
+            adjoint_step(tm, *P, D, k, tm0, h, regime, M, A, Uk, Zt, recbuf + (size_t)(j & 1) * rb, hint);
+            post_flag(tm, vf, F_CRIT, j + 1);
+        }
+        if (tm.leader())
+            for (; jout >= 0; --jout) tau_out_bar[(size_t)mode * n_out + jout] = 0.0;
+        tm.sync();
+    } else if (warp == 1) {
+        // ---- recompute ----
+        for (int j = 0; j < nacc; ++j) {
+            const int m = nacc - 1 - j;
+            const int sg = m / every, q = last_sg - sg, n0 = sg * every;
+            if (!wait_flag(tm, vf, F_SEG, q + 1)) break;
+            if (!wait_flag(tm, vf, F_CRIT, j - 1)) break;
+            ModeMem M;
+            double *Uk, *Zt, *meta;
+            slot_mem(j, M, Uk, Zt, meta);
+            const double* ym = (m == n0) ? ckpt + (size_t)sg * n : segbuf + ((size_t)(q & 1) * every + (m - n0)) * n;
+            for (int i = tm.lane; i < n; i += 32) M.y[i] = ym[i];
+            tm.sync();
+            const double tm0 = m == 0 ? t0 : tlog[m - 1], h = tlog[m] - tm0;
+            const int regime = regime_at(*P, tm0, swm);
+            rodas5_step(tm, *P, D, k, tm0, h, regime, M, hint, (const DiscoebTangent*)nullptr, (const TanMem*)nullptr,
+                        Uk);
+            make_Zt(tm, D, M, h, Zt);
+            if (tm.leader()) {
+                meta[0] = tm0;
+                meta[1] = h;
+                meta[2] = (double)regime;
+            }
+            post_flag(tm, vf, F_REC, j + 1);
+            if (m == n0) post_flag(tm, vf, F_SEGUSED, q + 1);
+        }
+    } else if (warp == 2) {
+        // ---- replay ----
+        ModeMem M = carve(mws + 2LL * every * n, D);
+        for (int q = 0; q <= last_sg; ++q) {
+            const int sg = last_sg - q, n0 = sg * every, n1 = nacc < n0 + every ? nacc : n0 + every;
+            if (!wait_flag(tm, vf, F_SEGUSED, q - 1)) break;
+            double* buf = segbuf + (size_t)(q & 1) * every * n;
+            const double* ck = ckpt + (size_t)sg * n;
+            for (int i = tm.lane; i < n; i += 32) M.y[i] = ck[i];
+            tm.sync();
+            double t = n0 == 0 ? t0 : tlog[n0 - 1];
+            for (int m = n0; m < n1 - 1; ++m) {
+                const double tn = tlog[m];
+                rodas5_step(tm, *P, D, k, t, tn - t, regime_at(*P, t, swm), M, hint);
+                for (int i = tm.lane; i < n; i += 32) {
+                    const double y1 = M.u[i] + M.K[7 * n + i];
+                    M.y[i] = y1;
+                    buf[(size_t)(m + 1 - n0) * n + i] = y1;
+                }
+                tm.sync();
+                t = tn;
+                if (__shfl_sync(0xffffffffu, vf[F_ABORT], 0)) break;  // warp-uniform
+            }
+            post_flag(tm, vf, F_SEG, q + 1);
+        }
+    } else {
+        // ---- deferred ----
+        for (int q = tm.lane; q < 16; q += 32) dpb[q] = 0.0;
+        for (int q = tm.lane; q < kNTabSeeds; q += 32) {
+            dtab[q].cur = -1;
+            dtab[q].w = 0.0;
+        }
+        tm.sync();
+        for (int j = 0; j < nacc; ++j) {
+            if (!wait_flag(tm, vf, F_CRIT, j + 1)) break;
+            deferred_step(tm, *P, D, k, recbuf + (size_t)(j & 1) * rb, DefAcc{dpb, dtab}, tbar, tstride);
+            post_flag(tm, vf, F_DEF, j + 1);
+        }
+    }
+    __syncthreads();
+    const bool aborted = vf[F_ABORT] != 0;
+    if (warp == 0) {
+        for (int i = tm.lane; i < n; i += 32) y0_bar[(size_t)mode * n + i] = aborted ? qnan : A.lam[i];
+        for (int q = tm.lane; q < 8; q += 32)
+            par_bar[(size_t)mode * 8 + q] = aborted ? qnan : A.pb[X_GRHOM + q] + dpb[X_GRHOM + q];
+        if (aborted)
+            for (int j = tm.lane; j < n_out; j += 32) tau_out_bar[(size_t)mode * n_out + j] = qnan;
+        for (int xs = X_KNOT0 + tm.lane; xs < X_KNOT0 + kNTabSeeds; xs += 32) {
+            if (aborted) break;
+            tab_flush(A.tab[xs - X_KNOT0], xs, tbar, tstride);
+            tab_flush(dtab[xs - X_KNOT0], xs, tbar, tstride);
+        }
+        if (tm.leader()) status[mode] = aborted ? DISCOEB_ABORTED : DISCOEB_OK;
+    }
 }
 
 // theta_bar[c, d] = sum over the modes of cosmology c of ybar0 . y0_dot + taubar . tau_out_dot +
@@ -301,7 +503,8 @@ int32_t discoeb_fwd_record(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* c
 int64_t discoeb_bwd_workspace_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_modes, int32_t checkpoint_every)
 {
     if (!cosmo0_host || n_modes < 0 || checkpoint_every < 1) return DISCOEB_EINVAL;
-    return (int64_t)n_modes * checkpoint_every * make_dims(*cosmo0_host).n * (int64_t)sizeof(double);
+    return (int64_t)n_modes * bwd_ws_doubles_per_mode(make_dims(*cosmo0_host), checkpoint_every) *
+           (int64_t)sizeof(double);
 }
 
 int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
@@ -327,18 +530,22 @@ int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
         table_stride < cosmo0_host->logpnu_loga.n_knots)
         return DISCOEB_EINVAL;
     if (workspace_bytes < discoeb_bwd_workspace_bytes(cosmo0_host, n_modes, checkpoint_every)) return DISCOEB_EINVAL;
-    const int mem = mode_mem_doubles(D), adj = adj_mem_doubles(D);
-    const size_t smem = (size_t)(kCosmoDoublesB + mem + adj) * sizeof(double);
+    const int mem = mode_mem_doubles(D);
+    // cosmology, flags, the critical warp's workspace, two step slots, two record buffers and the
+    // deferred warp's accumulators (16 parameter doubles + kNTabSeeds two-double accumulators)
+    const size_t smem = (size_t)(kCosmoDoublesB + kNFlags / 2 + adj_mem_doubles(D, false) + 2 * slot_doubles(D) +
+                                 2 * kRecPerStep * drec_doubles(D) + 16 + 2 * kNTabSeeds) *
+                        sizeof(double);
     int dev = 0, max_optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (smem > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
-    if (cudaFuncSetAttribute(bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(bwd_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return DISCOEB_ECUDA;
     const long long rec = record_doubles(D.n, step_capacity, checkpoint_every);
-    bwd_kernel<<<n_modes, 32, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+    bwd_split_kernel<<<n_modes, 128, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
         cosmos_dev, n_cosmo, mode_cosmo, n_modes, kmodes, tau_start, switch_tau, n_out, tau_out, step_capacity,
-        checkpoint_every, rec, records, n_accepted, fwd_status, static_cast<double*>(workspace), y_out20_bar, mem, adj,
+        checkpoint_every, rec, records, n_accepted, fwd_status, static_cast<double*>(workspace), y_out20_bar, mem,
         y0_bar, tau_out_bar, par_bar, table_bar, table_stride, table_per_mode ? 1 : 0, status);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }

@@ -42,7 +42,8 @@ int shim_adjoint_step(const DiscoebCosmo* P, const DiscoebTangent* tn, double k,
         A.tab[q].cur = -1;
         A.tab[q].w = 0.0;
     }
-    adjoint_step(tm, *P, D, k, t, h, regime, M, A, tbar, tstride, hint);
+    adjoint_step(tm, *P, D, k, t, h, regime, M, A, A.Uk, A.Zt, A.rec, hint);
+    deferred_step(tm, *P, D, k, A.rec, DefAcc{A.pb, A.tab}, tbar, tstride);
     for (int xs = X_KNOT0; xs < X_KNOT0 + kNTabSeeds; ++xs) tab_flush(A.tab[xs - X_KNOT0], xs, tbar, tstride);
     std::memcpy(lam0, A.lam, sizeof(double) * n);
     for (int q = 0; q < 16; ++q) pbar[q] = A.pb[q];
