@@ -216,6 +216,113 @@ template <class TM> DDV void hier_stat_reduce(const TM& tm, const Dims& D, HierS
     for (int q = 0; q < D.nq; ++q) h.bq[q] = tm.sum(h.bq[q]);
 }
 
+// The hierarchy rows' coefficients at one background, computed once and reused by the statistics
+// and the transposed band product of every cotangent taken at that background: per row i (state
+// index) the values c[3i + m] of (lo, di, up), their opacity derivatives ca and bin-velocity
+// derivatives cq, the coupling coefficients u[r] (uv) with their opacity derivatives (ua), and
+// tr[i] = 1 for a truncation row (its band has no upper neighbour; its upper entries are zero).
+struct HierCoef {
+    double *c, *ca, *cq, *uv, *ua, *tr;
+};
+DHD int hier_coef_doubles(const Dims& D) { return 16 * D.n; }
+DHD HierCoef carve_hier_coef(double* base, const Dims& D)
+{
+    const int n = D.n;
+    return HierCoef{base, base + 3 * n, base + 6 * n, base + 9 * n, base + 12 * n, base + 15 * n};
+}
+
+template <class TM>
+DDV void hier_coef_fill(const TM& tm, const DiscoebCosmo& P, const Dims& D, const Bg<double>& b, double k,
+                        const HierCoef& HC)
+{
+    const int nh = n_hier_rows(D);
+    // the bin velocities and d ln f0 / d ln q on lanes, broadcast (every lane runs the same number
+    // of iterations: the shuffles need all lanes)
+    double vlane = 1.0, dll = 0.0;
+    if (tm.full() && tm.lane < D.nq) {
+        vlane = rcp(inv_vq(P, b, tm.lane));
+        dll = dlfdlq_of(P.q[tm.lane]);
+    }
+    for (int h0 = 0; h0 < nh; h0 += tm.nl) {
+        const int hh = h0 + tm.lane;
+        const bool act = hh < nh;
+        const int i = hier_row(D, act ? hh : 0);
+        const int q = hier_bin(D, i);
+        const double vq = tm.full() ? tm.bcast(vlane, q) : rcp(inv_vq(P, b, q));
+        const double dlq = tm.full() ? tm.bcast(dll, q) : dlfdlq_of(P.q[q]);
+        if (!act) continue;
+        HDual lo, di, up, u[3];
+        int st;
+        bool trunc;
+        hier_coef_parts(P, D, b, k, i, vq, dlq, lo, di, up, u, st, trunc);
+        HC.c[3 * i] = lo.v.v; HC.c[3 * i + 1] = di.v.v; HC.c[3 * i + 2] = trunc ? 0.0 : up.v.v;
+        HC.ca[3 * i] = lo.v.d; HC.ca[3 * i + 1] = di.v.d; HC.ca[3 * i + 2] = trunc ? 0.0 : up.v.d;
+        HC.cq[3 * i] = lo.d.v; HC.cq[3 * i + 1] = di.d.v; HC.cq[3 * i + 2] = trunc ? 0.0 : up.d.v;
+        for (int r = 0; r < 3; ++r) {
+            HC.uv[3 * i + r] = u[r].v.v;
+            HC.ua[3 * i + r] = u[r].v.d;
+        }
+        HC.tr[i] = trunc ? 1.0 : 0.0;
+    }
+    tm.sync();
+}
+
+// hier_stat_lane + hier_stat_reduce from cached coefficients (opac: the background's opacity).
+// The massive-neutrino rows run with a fixed bin per lane, so that each lane keeps its bin's
+// velocity statistic in a register; part: tm.nl doubles of scratch for the per-bin sums.
+template <class TM>
+DDV void hier_stat_cached(const TM& tm, const Dims& D, const HierCoef& HC, double opac, const double* lam,
+                          const double* y, HierStat& h, double* part)
+{
+    hier_stat_zero(h);
+    double aop = 0.0, gc[3] = {0.0, 0.0, 0.0}, gop[3] = {0.0, 0.0, 0.0};
+    auto row = [&](int i, double& bacc) {
+        const double li = lam[i];
+        if (li == 0.0) return;
+        const int st = row_stride(D, i);
+        const double ylo = y[i - st], yi = y[i];
+        const double yup = HC.tr[i] != 0.0 ? 0.0 : y[i + st];
+        aop += li * (HC.ca[3 * i] * ylo + HC.ca[3 * i + 1] * yi + HC.ca[3 * i + 2] * yup);
+        bacc += li * (HC.cq[3 * i] * ylo + HC.cq[3 * i + 1] * yi + HC.cq[3 * i + 2] * yup);
+        for (int r = 0; r < 3; ++r) {
+            gop[r] += li * HC.ua[3 * i + r];
+            gc[r] += li * (HC.uv[3 * i + r] - opac * HC.ua[3 * i + r]);
+        }
+    };
+    const int nq = D.nq;
+    const int nmass = nq * (D.lmaxnu + 1);
+    const int nlight = n_hier_rows(D) - nmass;  // photon and massless-neutrino rows come first
+    double unused = 0.0;
+    for (int hh = tm.lane; hh < nlight; hh += tm.nl) row(hier_row(D, hh), unused);
+    if (nq > 0 && TM::nl >= nq) {
+        const int per = TM::nl / nq;  // lanes per bin
+        const int q = tm.lane % nq;
+        double bacc = 0.0;
+        if (tm.lane < per * nq)
+            for (int l = tm.lane / nq; l <= D.lmaxnu; l += per) row(D.iq0 + l * nq + q, bacc);
+        part[tm.lane] = bacc;
+        tm.sync();
+        for (int qq = 0; qq < nq; ++qq) {
+            double v = 0.0;
+            for (int p = 0; p < per; ++p) v += part[p * nq + qq];
+            h.bq[qq] = v;
+        }
+        tm.sync();
+    } else {
+        for (int m = tm.lane; m < nmass; m += tm.nl) {
+            double bacc = 0.0;
+            row(D.iq0 + m, bacc);
+            h.bq[m % nq] += bacc;
+        }
+        for (int qq = 0; qq < nq; ++qq) h.bq[qq] = tm.sum(h.bq[qq]);
+    }
+    h.aop = tm.sum(aop);
+    for (int r = 0; r < 3; ++r) {
+        h.gc[r] = tm.sum(gc[r]);
+        h.gop[r] = tm.sum(gop[r]);
+    }
+}
+
 // lambda . f(y) at background b, up to terms that do not depend on b or y, with the hierarchy rows
 // through h (hier_stat of the same lambda and y); lam0 = false leaves out row 0 (a' = a'/a a).
 // Y(j) gives state entry j as a T.
@@ -280,6 +387,9 @@ DDV void tab_add(TabAcc& acc, int xs, int i, double g, double* tbar, int stride)
 // (hyper-dual, at y_n).
 constexpr int kRecPerStep = 17;
 constexpr int kDeferredSeeds = kNX - 1;  // every x input but a
+// scalars a step leaves for achain_step (c_s, K_s[0] per stage, W_00, h, the output layer's a term)
+enum { AS_C = 0, AS_K0 = 8, AS_W00 = 16, AS_H = 17, AS_LAM0 = 18, kAScalars = 20 };
+constexpr int kAScratch = 32;  // achain_step's scratch (26 used)
 DHD int hs_doubles() { return (int)(sizeof(HierStat) / sizeof(double)); }
 DHD int drec_doubles(const Dims& D) { return 19 + n_read(D) + hs_doubles(); }
 // inverse of read_index (-1: not read)
@@ -341,36 +451,19 @@ struct DefAcc {
     TabAcc* tab;
 };
 
-// The 17 records of one step, every deferred seed (lanes take seeds), accumulated into acc
-template <class TM>
-DDV void deferred_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, const double* recs,
-                       const DefAcc& acc, double* tbar, int tstride)
-{
-    const int rd = drec_doubles(D);
-    for (int r = 0; r < kRecPerStep; ++r) {
-        const double* rec = recs + (size_t)r * rd;
-        const int kind = r < 8 ? 0 : (r < 16 ? 1 : 2);
-        const TabIdx ti = tab_idx(P, log(rec[0]));
-        for (int sd = tm.lane; sd < kDeferredSeeds; sd += tm.nl) {
-            const int xs = 1 + sd;
-            const double g = kind == 2 ? drec_eval<HDual>(P, D, k, rec, kind, xs) : drec_eval<Dual>(P, D, k, rec, kind, xs);
-            if (xs < X_KNOT0) acc.pb[xs] += g;
-            else tab_add(acc.tab[xs - X_KNOT0], xs, ti.i[kseed_table(xs)], g, tbar, tstride);
-        }
-    }
-    tm.sync();
-}
-
 // ---- per-warp adjoint workspace ----
 // With own_step_buffers the workspace also holds the step's U columns, Zt and deferred records
 // (the single-team sweep); the warp-split kernel keeps those in its shared step slots.
 struct AdjMem {
-    double *Uk, *Zt, *Kb, *us, *ub, *yb, *rho, *lam, *pb, *sc, *rec;
+    double *Uk, *Zt, *Kb, *us, *ub, *yb, *rho, *lam, *pb, *sc, *rec, *as, *scr, *g, *hc;
     TabAcc* tab;
 };
 DHD int adj_mem_doubles(const Dims& D, bool own_step_buffers = true)
 {
-    return 13 * D.n + 16 + 32 + 2 * kNTabSeeds + (own_step_buffers ? 6 * D.n + kRecPerStep * drec_doubles(D) : 0);
+    return 13 * D.n + 16 + 32 + 2 * kNTabSeeds + hier_coef_doubles(D) +
+           (own_step_buffers
+                ? 6 * D.n + kRecPerStep * drec_doubles(D) + kAScalars + kAScratch + kRecPerStep * kDeferredSeeds
+                : 0);
 }
 DHD AdjMem carve_adj(double* base, const Dims& D, bool own_step_buffers = true)
 {
@@ -385,42 +478,52 @@ DHD AdjMem carve_adj(double* base, const Dims& D, bool own_step_buffers = true)
     A.pb = A.lam + n;     // 16  parameter cotangents (index = seed)
     A.sc = A.pb + 16;     // 32  scalars
     A.tab = reinterpret_cast<TabAcc*>(A.sc + 32);  // kNTabSeeds accumulators (2 doubles each)
-    double* rest = A.sc + 32 + 2 * kNTabSeeds;
+    A.hc = A.sc + 32 + 2 * kNTabSeeds;  // cached hierarchy coefficients (HierCoef)
+    double* rest = A.hc + hier_coef_doubles(D);
     if (own_step_buffers) {
         A.Uk = rest;          // 3n  U columns at the step start (the factorisation overwrites M.Z)
         A.Zt = A.Uk + 3 * n;  // 3n  A^{-T} G^T
         A.rec = A.Zt + 3 * n; // the step's deferred records
+        A.as = A.rec + kRecPerStep * drec_doubles(D);  // the step's scalars for achain_step
+        A.scr = A.as + kAScalars;                       // achain_step's scratch
+        A.g = A.scr + kAScratch;                        // deferred_records' staging
     } else {
-        A.Uk = A.Zt = A.rec = nullptr;
+        A.Uk = A.Zt = A.rec = A.as = A.scr = A.g = nullptr;
     }
     return A;
 }
 static_assert(sizeof(TabAcc) <= 2 * sizeof(double), "TabAcc must fit two doubles");
 
 // ---- transposed solves ----
-// A^T z = r for one chain of the factorisation (unit-lower L, upper U with reciprocal pivots)
+// A^T z = r for one chain of the factorisation (unit-lower L, upper U with reciprocal pivots).
+// The last two solved values ride in registers (the sweeps never reload what they just stored).
 DDV void solve_chain_T(const double* A, const Chain& ch, double* z)
 {
     const int st = ch.stride, len = ch.len;
     // U^T w = r: forward
+    double p1 = 0.0, p2 = 0.0;
+#pragma unroll 4
     for (int p = 0; p < len; ++p) {
         const int i = ch.start + p * st;
         double v = z[i];
-        for (int m = 1; m <= ch.ku && p - m >= 0; ++m) {
-            const int im = i - m * st;
-            v -= A[7 * im + 3 + m] * z[im];
-        }
-        z[i] = v * A[7 * i + 3];
+        if (p >= 1) v -= A[7 * (i - st) + 4] * p1;
+        if (ch.ku >= 2 && p >= 2) v -= A[7 * (i - 2 * st) + 5] * p2;
+        v *= A[7 * i + 3];
+        z[i] = v;
+        p2 = p1;
+        p1 = v;
     }
     // L^T z = w: backward
+    double n1 = 0.0, n2 = 0.0;
+#pragma unroll 4
     for (int p = len - 1; p >= 0; --p) {
         const int i = ch.start + p * st;
         double v = z[i];
-        for (int d = 1; d <= ch.kl && p + d < len; ++d) {
-            const int id = i + d * st;
-            v -= A[7 * id + 3 - d] * z[id];
-        }
+        if (p + 1 < len) v -= A[7 * (i + st) + 2] * n1;
+        if (ch.kl >= 2 && p + 2 < len) v -= A[7 * (i + 2 * st) + 1] * n2;
         z[i] = v;
+        n2 = n1;
+        n1 = v;
     }
 }
 
@@ -450,8 +553,11 @@ template <class TM> DDV void make_Zt(const TM& tm, const Dims& D, const ModeMem&
 }
 
 // v = W^{-T} g in place (W = I/(gamma h) - J(y_n) as factored by factor_W; Uk its U columns)
+// c_out (may be null): receives c = sum_{i >= 1} J_i0 v_i (with v_1's row-1 form), so that
+// v_0 = (g_0 + c) / W_00: the only place the a-component enters.
 template <class TM>
-DDV void solve_WT(const TM& tm, const Dims& D, const ModeMem& M, const double* Uk, const double* Zt, double h, double* v)
+DDV void solve_WT(const TM& tm, const Dims& D, const ModeMem& M, const double* Uk, const double* Zt, double h, double* v,
+                  double* c_out = nullptr)
 {
     const int n = D.n, ns = n_slots(D);
     const double gh = kR5.gamma * h;
@@ -493,6 +599,7 @@ DDV void solve_WT(const TM& tm, const Dims& D, const ModeMem& M, const double* U
     if (tm.leader()) {
         v[1] = v1;
         v[0] = (g0 + c0v + M.col0[1] * v1) / M.sc[SC_W00];
+        if (c_out) *c_out = c0v + M.col0[1] * v1;
     }
     tm.sync();
 }
@@ -532,6 +639,31 @@ DDV void hier_gather(const TM& tm, const DiscoebCosmo& P, const Dims& D, const B
             if (m == 1 && trunc) continue;                   // a truncation row has no upper entry
             const T c = m == -1 ? lo : (m == 0 ? di : up);  // row i's entry in column j = i + m st
             acc += apart(c) * li;
+        }
+        out[j] += acc;
+    }
+}
+
+// hier_gather at a background whose coefficients are cached (hier_coef_fill)
+template <class TM>
+DDV void hier_gather_cached(const TM& tm, const Dims& D, const HierCoef& HC, const double* lam, double* out)
+{
+    const int n = D.n;
+    auto is_hier = [&](int i) {
+        return (i >= 10 && i <= 7 + D.lmaxg) || (i >= D.idxgp && i <= D.idxgp + D.lmaxgp) ||
+               (i >= D.idxr + 3 && i <= D.idxr + D.lmaxr) || (i >= D.iq0 && i < n - 2);
+    };
+    for (int j = tm.lane; j < n; j += tm.nl) {
+        if (j < 2) continue;
+        const int stj = row_stride(D, j);
+        double acc = 0.0;
+        for (int m = -1; m <= 1; ++m) {
+            const int i = j - m * stj;
+            if (i < 2 || i >= n || !is_hier(i) || row_stride(D, i) != stj) continue;
+            const double li = lam[i];
+            if (li == 0.0) continue;
+            if (m == 1 && HC.tr[i] != 0.0) continue;  // a truncation row has no upper entry
+            acc += HC.c[3 * i + 1 + m] * li;        // row i's entry in column j = i + m st
         }
         out[j] += acc;
     }
@@ -618,37 +750,95 @@ DDV void output_adjoint(const TM& tm, const DiscoebCosmo& P, const Dims& D, doub
 }
 
 // ---- the reverse of one step ----
+// The a-component of the cotangents forms a chain of its own: rows >= 1 of f are linear in
+// y[1:] with coefficients that depend on a, and a' depends on a only, so no cotangent of
+// y[1:] depends on one of a (W^{-T}'s row 0 is solved last, v_0 = (g_0 + c)/W_00, and every
+// y-derivative of lambda_0 f_0 vanishes).  The reverse step therefore runs in two parts:
+// adjoint_step carries the cotangents of y[1:] (the critical chain) and leaves per step the 17
+// functional records and a few scalars; achain_step then carries the a-component through the
+// same stages as a scalar recurrence, with the a-derivatives of the recorded functionals, and
+// completes the records' lambda_0 for the parameter and table seeds (deferred_records).
+
+// scalars a step leaves for achain_step
+
+template <class T, class S, class F> DHD Bg<T> bg_convert(const Bg<S>& s, const F& cv)
+{
+    Bg<T> b;
+    b.par = Par<T>{cv(s.par.grhom), cv(s.par.Omegam), cv(s.par.Omegab), cv(s.par.OmegaDE), cv(s.par.amnu),
+                   cv(s.par.w0), cv(s.par.wa), cv(s.par.akthom)};
+    b.a = cv(s.a); b.ia = cv(s.ia); b.a2 = cv(s.a2); b.ia2 = cv(s.ia2); b.aH = cv(s.aH); b.iaHG = cv(s.iaHG);
+    b.opac = cv(s.opac); b.po = cv(s.po); b.tauc = cv(s.tauc); b.taucprime = cv(s.taucprime); b.cs2 = cv(s.cs2);
+    b.pb43 = cv(s.pb43); b.rho_Q = cv(s.rho_Q); b.w_Q = cv(s.w_Q); b.opw = cv(s.opw); b.iopw = cv(s.iopw);
+    b.ca2_Q = cv(s.ca2_Q); b.pnu = cv(s.pnu); b.rsa_fac = cv(s.rsa_fac); b.rsa_tcs = cv(s.rsa_tcs);
+    b.aprimeprimeoa = cv(s.aprimeprimeoa);
+    b.itau = s.itau;
+    b.rsa = s.rsa; b.ufa = s.ufa; b.tca = s.tca; b.de_frozen = s.de_frozen;
+    return b;
+}
+
+// The backgrounds at the eight stage states of a recomputed step (M), in the order of the reverse
+// stage loop's use, stored as Bg<double> images at out [8 x bg_image_doubles()]; the stage scale
+// factors are formed exactly as adjoint_step forms u_s[0].
+DHD int bg_image_doubles() { return (int)((sizeof(Bg<double>) + sizeof(double) - 1) / sizeof(double)); }
+template <class TM>
+DDV void stage_backgrounds(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h,
+                           int regime, const ModeMem& M, double* out, int& hint)
+{
+    const int n = D.n;
+    for (int s = 7; s >= 0; --s) {
+        double v = M.y[0];
+        const int sl = s <= 5 ? s : 5;
+        for (int j = 0; j < sl; ++j) v += kR5.a[sl][j] * M.K[j * n];
+        if (s >= 6) v += M.K[5 * n];
+        if (s == 7) v += M.K[6 * n];
+        const double ts = (s <= 5) ? t + kR5.c[s] * h : t + h;
+        Bg<double> bs;
+        bg_eval_team(tm, P, v, ts, k, regime, bs, hint);
+        if (tm.leader()) *reinterpret_cast<Bg<double>*>(out + (size_t)s * bg_image_doubles()) = bs;
+    }
+    tm.sync();
+}
+
 // On entry: M holds the step's forward recomputation (rodas5_step from y_n = M.y, with factor_W's
-// U columns in Uk) and Zt = A^{-T} G^T; A.lam = ybar_{n+1}.  On return A.lam = ybar_n.  This is the
-// part of the step the state cotangents depend on (the chain of the reverse sweep): the seeds of
-// the state entries and of a.  The parameter and table-knot seeds of the step's functionals are
-// left in the 17 records at recs (deferred_step evaluates them).
+// U columns in Uk) and Zt = A^{-T} G^T; A.lam[1:] = ybar_{n+1}[1:].  On return A.lam[1:] =
+// ybar_n[1:] (A.lam[0] = 0: the a-component is achain_step's).  lam0_out: the a-cotangent added at
+// this step's end by the output layer (the caller's), passed on in the step scalars sc.
 template <class TM>
 DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double t, double h, int regime,
-                      const ModeMem& M, const AdjMem& A, const double* Uk, const double* Zt, double* recs, int& hint)
+                      const ModeMem& M, const AdjMem& A, const double* Uk, const double* Zt, double* recs, double* sc,
+                      double lam0_out, int& hint, const double* stage_bg = nullptr)
 {
     const int n = D.n;
     const double ih = 1.0 / h;
     const int rd = drec_doubles(D);
     // stage cotangents: Kbar_7 = ybar_{n+1}, the others start at zero; ubar_7 = ybar_{n+1}
     for (int i = tm.lane; i < n; i += tm.nl) {
+        const double l = i == 0 ? 0.0 : A.lam[i];
         for (int s = 0; s < 7; ++s) A.Kb[s * n + i] = 0.0;
-        A.Kb[7 * n + i] = A.lam[i];
-        A.ub[i] = A.lam[i];
+        A.Kb[7 * n + i] = l;
+        A.ub[i] = l;
         A.yb[i] = 0.0;
         A.rho[i] = 0.0;
+    }
+    if (tm.leader()) {
+        sc[AS_W00] = M.sc[SC_W00];
+        sc[AS_H] = h;
+        sc[AS_LAM0] = lam0_out;
+        for (int s = 0; s < 8; ++s) sc[AS_K0 + s] = M.K[s * n];
     }
     tm.sync();
     Bg<double> bflags;
     bflags.rsa = (regime & 1) != 0;
     bflags.ufa = !bflags.rsa && (regime & 2) != 0;
     bflags.tca = !bflags.rsa && (regime & 4) != 0;
-    const int nseed = 1 + n_read(D);  // a and the state entries the functional reads
+    const int nseed = n_read(D);  // the state entries the special rows and the metric functionals read
     for (int s = 7; s >= 0; --s) {
         const double* Ks = M.K + s * n;
-        // rbar_s = W^{-T} Kbar_s, in place (Kbar_s is complete: only later stages add to it)
+        // rbar_s[1:] = (W^{-T} Kbar_s)[1:], in place (Kbar_s is complete: only later stages add to it)
         double* rb = A.Kb + s * n;
-        solve_WT(tm, D, M, Uk, Zt, h, rb);
+        solve_WT(tm, D, M, Uk, Zt, h, rb, sc + AS_C + s);
+        if (tm.leader()) rb[0] = 0.0;  // the a-component: achain_step
+        tm.sync();
         // stage state u_s
         for (int i = tm.lane; i < n; i += tm.nl) {
             double v = M.y[i];
@@ -660,33 +850,29 @@ DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
             A.rho[i] += Ks[0] * rb[i];
         }
         tm.sync();
-        // ubar_s += J(u_s)^T rbar_s: hierarchy rows by the gather, the special rows, the metric
-        // functionals and column 0 by the seeded functional (its parameter and table seeds go to
-        // the stage's record)
+        // ubar_s[1:] += (J(u_s)^T rbar_s)[1:]: hierarchy rows by the gather, the special rows and
+        // the metric functionals by the functional seeded in the state entries it reads, at the
+        // stage's background (no input of the background is seeded: a plain background in dual
+        // form); its a- and x-seeds are the record's
         const double ts = (s <= 5) ? t + kR5.c[s] * h : t + h;
         Bg<double> bs;
-        bg_eval_team(tm, P, A.us[0], ts, k, regime, bs, hint);
+        if (stage_bg) bs = *reinterpret_cast<const Bg<double>*>(stage_bg + (size_t)s * bg_image_doubles());
+        else bg_eval_team(tm, P, A.us[0], ts, k, regime, bs, hint);
+        const HierCoef HC = carve_hier_coef(A.hc, D);
+        hier_coef_fill(tm, P, D, bs, k, HC);
         HierStat hs;
-        hier_stat_zero(hs);
-        hier_stat_lane(tm, P, D, bs, k, rb, A.us, hs);
-        hier_stat_reduce(tm, D, hs);
-        hier_gather(tm, P, D, bs, k, rb, A.ub);
+        hier_stat_cached(tm, D, HC, bs.opac, rb, A.us, hs, A.sc);
+        hier_gather_cached(tm, D, HC, rb, A.ub);
         drec_write(tm, D, recs + (size_t)s * rd, A.us[0], ts, regime, rb, A.us, hs);
         tm.sync();
         {
-            const double loga = log(A.us[0]);
-            const TabIdx ti = tab_idx(P, loga);
+            const Bg<Dual> bd = bg_convert<Dual>(bs, [](double v) { return Dual(v, 0.0); });
             for (int base = 0; base < nseed; base += tm.nl) {
                 const int sid = base + tm.lane;
                 if (sid < nseed) {
-                    const int xs = sid == 0 ? X_A : -1;
-                    const int yj = sid == 0 ? -1 : read_index(D, sid - 1);
-                    Bg<Dual> bd;
-                    bg_seeded(P, A.us[0], ts, k, regime, ti, xs, bd);
+                    const int yj = read_index(D, sid);
                     auto Y = [&](int j) { return Dual(A.us[j], j == yj ? 1.0 : 0.0); };
-                    const double g = gpart(functional<Dual>(P, D, bd, k, ts, rb, true, Y, hs));
-                    if (xs < 0) A.ub[yj] += g;
-                    else A.ub[0] += g;
+                    A.ub[yj] += gpart(functional<Dual>(P, D, bd, k, ts, rb, true, Y, hs));
                 }
                 tm.sync();
             }
@@ -709,69 +895,149 @@ DDV void adjoint_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double
         }
         tm.sync();
     }
-    // W depends on y_n through J(y_n): the term sum_s rbar_s^T J(y_n) K_s, with rbar_s now in A.Kb
+    // W depends on y_n through J(y_n), i.e. through a = y_n[0] alone: the term sum_s rbar_s^T J(y_n)
+    // K_s contributes to a's cotangent and the inputs' only (records 8..15)
     {
         Bg<double> b0;
         bg_eval_team(tm, P, M.y[0], t, k, regime, b0, hint);
-        const double loga = log(M.y[0]);
-        const TabIdx ti = tab_idx(P, loga);
-        // (a) columns >= 1: the a-gradient of sum_s rbar_s . (C(b_n) K_s[1:]) (row 0 left out), one
-        // stage per lane; the x-gradients are deferred (records 8..15)
+        const HierCoef HC = carve_hier_coef(A.hc, D);
+        hier_coef_fill(tm, P, D, b0, k, HC);
         for (int s = 0; s < 8; ++s) {
             HierStat hs;
-            hier_stat_zero(hs);
-            hier_stat_lane(tm, P, D, b0, k, A.Kb + s * n, M.K + s * n, hs);
-            hier_stat_reduce(tm, D, hs);
+            hier_stat_cached(tm, D, HC, b0.opac, A.Kb + s * n, M.K + s * n, hs, A.sc);
             drec_write(tm, D, recs + (size_t)(8 + s) * rd, M.y[0], t, regime, A.Kb + s * n, M.K + s * n, hs);
         }
         tm.sync();
-        double ga = 0.0;
-        for (int s = tm.lane; s < 8; s += tm.nl) {
-            const double* rec = recs + (size_t)(8 + s) * rd;
-            HierStat hs;
-            double* hp = reinterpret_cast<double*>(&hs);
-            for (int q = 0; q < hs_doubles(); ++q) hp[q] = rec[19 + n_read(D) + q];
-            Bg<Dual> bd;
-            bg_seeded(P, M.y[0], t, k, regime, ti, X_A, bd);
-            const double* Ks = M.K + s * n;
-            auto Y = [&](int j) { return Dual(Ks[j], 0.0); };
-            ga += gpart(functional<Dual>(P, D, bd, k, t, A.Kb + s * n, false, Y, hs));
-        }
-        ga = tm.sum(ga);
-        if (tm.leader()) A.yb[0] += ga;
-        tm.sync();
-        // (b) column 0: rho . (d f / d a)(y_n) with rho = sum_s K_s[0] rbar_s; its gradient in
-        // y_n[1:] is C'(a)^T rho (hierarchy rows by the gather in Dual a, the rest by the seeded
-        // functional in hyper-dual numbers), in a the second derivative; the x-gradients (mixed
-        // second derivatives) are deferred (record 16)
+        // column 0: rho . (d f / d a)(y_n) with rho = sum_s K_s[0] rbar_s; its gradient in y_n[1:] is
+        // C'(a)^T rho (hierarchy rows by the gather in Dual a, the rest by the functional in
+        // hyper-dual numbers seeded in the state entries); a- and x-gradients: record 16
         HierStat hs;
-        hier_stat_zero(hs);
-        hier_stat_lane(tm, P, D, b0, k, A.rho, M.y, hs);
-        hier_stat_reduce(tm, D, hs);
+        hier_stat_cached(tm, D, HC, b0.opac, A.rho, M.y, hs, A.sc);
+        Bg<Dual> bda;
         {
-            Bg<Dual> bda;
             int hh = hint;
             bg_eval_team(tm, P, Dual(M.y[0], 1.0), t, k, regime, bda, hh);
             hier_gather(tm, P, D, bda, k, A.rho, A.yb);
         }
         drec_write(tm, D, recs + (size_t)16 * rd, M.y[0], t, regime, A.rho, M.y, hs);
         tm.sync();
+        const Bg<HDual> bh = bg_convert<HDual>(bda, [](const Dual& v) { return HDual(v, Dual(0.0, 0.0)); });
         for (int base = 0; base < nseed; base += tm.nl) {
             const int sid = base + tm.lane;
             if (sid < nseed) {
-                const int xs = sid == 0 ? X_A : -1;
-                const int yj = sid == 0 ? -1 : read_index(D, sid - 1);
-                Bg<HDual> bh;
-                bg_seeded(P, M.y[0], t, k, regime, ti, xs, bh);
+                const int yj = read_index(D, sid);
                 auto Y = [&](int j) { return HDual(Dual(M.y[j], 0.0), Dual(j == yj ? 1.0 : 0.0, 0.0)); };
-                const double g = gpart(functional<HDual>(P, D, bh, k, t, A.rho, true, Y, hs));
-                if (xs < 0) A.yb[yj] += g;
-                else A.yb[0] += g;
+                A.yb[yj] += gpart(functional<HDual>(P, D, bh, k, t, A.rho, true, Y, hs));
             }
             tm.sync();
         }
     }
-    for (int i = tm.lane; i < n; i += tm.nl) A.lam[i] = A.yb[i];
+    for (int i = tm.lane; i < n; i += tm.nl) A.lam[i] = i == 0 ? 0.0 : A.yb[i];
+    tm.sync();
+}
+
+// d f_0 / d a (T = Dual) or d^2 f_0 / d a^2 (T = HDual) at (a, tau): f_0 = a' = a (a'/a)
+template <class T> DHD double f0_a_derivative(const DiscoebCosmo& P, double a, double tau, double k, int regime)
+{
+    const TabIdx ti = tab_idx(P, log(a));
+    Bg<T> b;
+    bg_seeded(P, a, tau, k, regime, ti, X_A, b);
+    return gpart(b.aH * b.a);
+}
+
+// The a-component of one reverse step (after adjoint_step left recs and sc): lam0 = ybar_{n+1}[0]
+// on entry (before this step's output-layer term, which sc carries), ybar_n[0] on return; the
+// records' lambda_0 (stage records: rbar_s[0]; record 16: rho_0) are filled in.  The recurrence
+// is adjoint_step's on the a-component: rbar_s[0] = (Kbar_s[0] + c_s) / W_00, ubar_s[0] gains
+// rbar_s[0] d f_0/d a + (the a-derivative of the rest of the stage functional), W's a-dependence
+// and the column-0 term add their a-derivatives.
+template <class TM>
+DDV void achain_step(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, double* recs, const double* sc,
+                     double& lam0, double* scratch)
+{
+    const int rd = drec_doubles(D);
+    // scratch: [0, 8) d f_0/d a at the stages, [8, 16) the stage functionals' a-derivatives without
+    // row 0, [16, 24) the W terms' a-derivatives, 24: the column-0 term's without row 0, 25: d^2 f_0 / da^2
+    for (int q = tm.lane; q < 26; q += tm.nl) {
+        double v;
+        if (q < 8) {
+            const double* rec = recs + (size_t)q * rd;
+            v = f0_a_derivative<Dual>(P, rec[0], rec[1], k, (int)rec[2]);
+        } else if (q < 16) {
+            v = drec_eval<Dual>(P, D, k, recs + (size_t)(q - 8) * rd, 1, X_A);  // kind 1: row 0 left out
+        } else if (q < 24) {
+            v = drec_eval<Dual>(P, D, k, recs + (size_t)(q - 8) * rd, 1, X_A);
+        } else if (q == 24) {
+            v = drec_eval<HDual>(P, D, k, recs + (size_t)16 * rd, 1, X_A);
+        } else {
+            const double* rec = recs + (size_t)16 * rd;
+            v = f0_a_derivative<HDual>(P, rec[0], rec[1], k, (int)rec[2]);
+        }
+        scratch[q] = v;
+    }
+    tm.sync();
+    double rb0[8], rho0 = 0.0;
+    double l = lam0 + sc[AS_LAM0];
+    {
+        const double ih = 1.0 / sc[AS_H];
+        double Kb0[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        Kb0[7] = l;
+        double ub0 = l, yb0 = 0.0;
+        for (int s = 7; s >= 0; --s) {
+            const double r = (Kb0[s] + sc[AS_C + s]) / sc[AS_W00];
+            rb0[s] = r;
+            rho0 += sc[AS_K0 + s] * r;
+            ub0 += r * scratch[s] + scratch[8 + s];
+            for (int j = 0; j < s; ++j) Kb0[j] += kR5.C[s][j] * ih * r;
+            if (s <= 5) {
+                yb0 += ub0;
+                for (int j = 0; j < s; ++j) Kb0[j] += kR5.a[s][j] * ub0;
+                ub0 = 0.0;
+            } else {
+                Kb0[s - 1] += ub0;
+            }
+        }
+        for (int s = 0; s < 8; ++s) yb0 += scratch[16 + s];
+        yb0 += rho0 * scratch[25] + scratch[24];
+        l = yb0;
+    }
+    tm.sync();
+    if (tm.leader()) {
+        for (int s = 0; s < 8; ++s) recs[(size_t)s * rd + 4] = rb0[s];  // lambda on special row 0 (= row 0)
+        recs[(size_t)16 * rd + 4] = rho0;
+    }
+    lam0 = l;
+    tm.sync();
+}
+
+// The parameter and table-knot seeds of records [r0, r1) of one step (their lambda_0 filled in):
+// the (record, seed) pairs spread over the lanes, the results staged in g [(r1 - r0) x
+// kDeferredSeeds], then each seed's lane adds its column into acc in record order.
+template <class TM>
+DDV void deferred_records(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, const double* recs, int r0,
+                          int r1, double* g, const DefAcc& acc, double* tbar, int tstride)
+{
+    const int rd = drec_doubles(D);
+    const int npairs = (r1 - r0) * kDeferredSeeds;
+    for (int pq = tm.lane; pq < npairs; pq += tm.nl) {
+        const int r = r0 + pq / kDeferredSeeds, xs = 1 + pq % kDeferredSeeds;
+        const double* rec = recs + (size_t)r * rd;
+        const int kind = r < 8 ? 0 : (r < 16 ? 1 : 2);
+        g[pq] = kind == 2 ? drec_eval<HDual>(P, D, k, rec, kind, xs) : drec_eval<Dual>(P, D, k, rec, kind, xs);
+    }
+    tm.sync();
+    for (int sd = tm.lane; sd < kDeferredSeeds; sd += tm.nl) {
+        const int xs = 1 + sd;
+        for (int r = r0; r < r1; ++r) {
+            const double v = g[(r - r0) * kDeferredSeeds + sd];
+            if (xs < X_KNOT0) {
+                acc.pb[xs] += v;
+            } else {
+                const TabIdx ti = tab_idx(P, log(recs[(size_t)r * rd]));
+                tab_add(acc.tab[xs - X_KNOT0], xs, ti.i[kseed_table(xs)], v, tbar, tstride);
+            }
+        }
+    }
     tm.sync();
 }
 
@@ -815,6 +1081,7 @@ DDV void bwd_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, 
 {
     const int n = D.n;
     int hint = P.xe_loga.n_knots / 2;
+    double lam0 = 0.0;  // the a-component of the running cotangent (achain_step's)
     for (int i = tm.lane; i < n; i += tm.nl) A.lam[i] = 0.0;
     for (int q = tm.lane; q < 16; q += tm.nl) A.pb[q] = 0.0;
     for (int q = tm.lane; q < kNTabSeeds; q += tm.nl) {
@@ -851,6 +1118,7 @@ DDV void bwd_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, 
                         A.Uk);
             make_Zt(tm, D, M, h, A.Zt);
             // outputs emitted at the end of this step
+            double lam0_out = 0.0;
             while (jout >= 0 && tout[jout] > tm0) {
                 for (int i = tm.lane; i < n; i += tm.nl) {
                     A.us[i] = M.u[i] + M.K[7 * n + i];
@@ -865,20 +1133,22 @@ DDV void bwd_mode(const TM& tm, const DiscoebCosmo& P, const Dims& D, double k, 
                 double acc = 0.0;
                 for (int i = tm.lane; i < n; i += tm.nl) {
                     acc += A.ub[i] * A.yb[i];
-                    A.lam[i] += A.ub[i];
+                    if (i > 0) A.lam[i] += A.ub[i];
                 }
                 const double tb = tm.sum(acc);
                 if (tm.leader() && toutbar) toutbar[jout] = tb;
+                lam0_out += A.ub[0];
                 tm.sync();
                 --jout;
             }
-            adjoint_step(tm, P, D, k, tm0, h, regime, M, A, A.Uk, A.Zt, A.rec, hint);
-            deferred_step(tm, P, D, k, A.rec, DefAcc{A.pb, A.tab}, tbar, tstride);
+            adjoint_step(tm, P, D, k, tm0, h, regime, M, A, A.Uk, A.Zt, A.rec, A.as, lam0_out, hint);
+            achain_step(tm, P, D, k, A.rec, A.as, lam0, A.scr);
+            deferred_records(tm, P, D, k, A.rec, 0, kRecPerStep, A.g, DefAcc{A.pb, A.tab}, tbar, tstride);
         }
     }
     if (toutbar && tm.leader())
         for (; jout >= 0; --jout) toutbar[jout] = 0.0;
-    for (int i = tm.lane; i < n; i += tm.nl) y0bar[i] = A.lam[i];
+    for (int i = tm.lane; i < n; i += tm.nl) y0bar[i] = i == 0 ? lam0 : A.lam[i];
     for (int xs = X_KNOT0 + tm.lane; xs < X_KNOT0 + kNTabSeeds; xs += tm.nl) tab_flush(A.tab[xs - X_KNOT0], xs, tbar, tstride);
     tm.sync();
 }

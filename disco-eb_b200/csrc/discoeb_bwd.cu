@@ -3,11 +3,12 @@
 //
 // Layout: the recording forward is the forward solve (one warp per k-mode) whose accept hook
 // writes each accepted step's end time (8 bytes) and every checkpoint_every-th start state into
-// the caller's record buffer.  The reverse sweep runs one block of four warps per mode (replay of
-// the segments from their checkpoints, recomputation of each step, the state-cotangent chain, the
-// parameter and table seeds; bwd_split_kernel), with the cosmology, two recomputed steps, the
-// critical warp's workspace and two steps' deferred records in shared memory (~103 KB at
-// n = 143: two blocks per SM) and two segment buffers per mode in the caller's workspace.
+// the caller's record buffer.  The reverse sweep runs one block of five warps per mode (replay of
+// the segments from their checkpoints, recomputation of each step, the chain of the cotangents of
+// y[1:], the a-component's scalar chain, the parameter and table seeds; bwd_split_kernel), with
+// the cosmology, two recomputed steps, the critical warp's workspace and two steps' functional
+// records in shared memory (~108 KB at n = 143) and two segment buffers per mode in the caller's
+// workspace.
 // Table-knot cotangents are summed over the modes of a cosmology with double-precision atomics
 // (the order of those additions is not fixed, so they agree between runs to rounding, not bit
 // for bit).
@@ -121,20 +122,25 @@ __global__ void __launch_bounds__(128) fwd_record_kernel(
     }
 }
 
-// ---- the reverse sweep, split over four cooperating warps per mode ----
+// ---- the reverse sweep, split over five cooperating warps per mode ----
 // Warp roles (one mode per block, steps taken apart last to first, "job" j = step nacc - 1 - j):
-//   0 critical:   the state-cotangent chain of every step (adjoint_step) and the output layer;
+//   0 critical:   the chain of the cotangents of y[1:] (adjoint_step) and the output layer;
 //   1 recompute:  each step's stages, factorisation, U columns and Zt into one of two shared
 //                 step slots, from the step's start state;
 //   2 replay:     each segment of `every` steps re-run from its checkpoint into one of two
 //                 global segment buffers (the start states the recompute warp reads);
-//   3 deferred:   the parameter and table-knot seeds of every step's 17 functionals (records in
-//                 one of two shared record buffers), one seed per lane.
-// Hand-over by counters in shared memory, every wait bounded (a wait that runs out sets the
-// block's abort flag, every warp leaves its loop, the mode reports DISCOEB_ABORTED with NaN
-// results and the launch ends normally).
+//   3 a-chain:    the a-component of every step (achain_step), then the parameter and table
+//                 seeds of the step's W-term records 8..15;
+//   4 deferred:   the parameter and table seeds of the stage records 0..7 and the column-0
+//                 record 16 (after warp 3 has filled in their lambda_0).
+// Records and step scalars live in one of two shared buffers per job parity.  Hand-over by
+// counters in shared memory, every wait bounded (a wait that runs out sets the block's abort
+// flag, every warp leaves its loop, the mode reports DISCOEB_ABORTED with NaN results and the
+// launch ends normally).
 constexpr long long kMaxPollsB = 1LL << 24;  // ~2 s with the back-off below; a step takes < 1 ms
-enum { F_REC = 0, F_CRIT = 1, F_DEF = 2, F_SEG = 3, F_SEGUSED = 4, F_ABORT = 5, kNFlags = 8 };
+enum { F_REC = 0, F_CRIT = 1, F_ACHAIN = 2, F_DEF1 = 3, F_DEF2 = 4, F_SEG = 5, F_SEGUSED = 6, F_ABORT = 7,
+       kNFlags = 8 };
+constexpr int kBwdWarps = 5;
 
 __device__ bool wait_flag(const WarpTeam& tm, volatile int* flags, int which, int target)
 {
@@ -162,13 +168,25 @@ __device__ void post_flag(const WarpTeam& tm, volatile int* flags, int which, in
     tm.sync();
 }
 
-DHD int slot_doubles(const Dims& D) { return mode_mem_doubles(D) + 6 * D.n + 4; }
+// a step slot: the recomputed step (ModeMem), U columns, Zt, 4 scalars, the 8 stage backgrounds
+DHD int slot_doubles(const Dims& D) { return mode_mem_doubles(D) + 6 * D.n + 4 + 8 * bg_image_doubles(); }
 DHD long long bwd_ws_doubles_per_mode(const Dims& D, int every)
 {
     return 2LL * every * D.n + mode_mem_doubles(D);
 }
+// one job parity's records and step scalars
+DHD int job_buf_doubles(const Dims& D) { return kRecPerStep * drec_doubles(D) + kAScalars; }
+// shared memory of bwd_split_kernel, in doubles after the cosmology and the flags: the critical
+// warp's workspace, two step slots, two job buffers, the a-chain warp's scratch and staging, the
+// deferred warp's staging, two accumulator sets (16 parameter doubles + kNTabSeeds two-double
+// accumulators each) and the a-chain's final value
+DHD int bwd_smem_doubles(const Dims& D)
+{
+    return adj_mem_doubles(D, false) + 2 * slot_doubles(D) + 2 * job_buf_doubles(D) + kAScratch +
+           2 * 8 * kDeferredSeeds + 2 * (16 + 2 * kNTabSeeds) + 2;
+}
 
-__global__ void __launch_bounds__(128, 2) bwd_split_kernel(
+__global__ void __launch_bounds__(32 * kBwdWarps, 1) bwd_split_kernel(
     const DiscoebCosmo* __restrict__ cosmos, int n_cosmo, const int32_t* __restrict__ mode_cosmo, int n_modes,
     const double* __restrict__ kmodes, const double* __restrict__ tau_start, const double* __restrict__ sw, int n_out,
     const double* __restrict__ tau_out, int cap, int every, long long rec_doubles, const double* __restrict__ records,
@@ -215,14 +233,24 @@ __global__ void __launch_bounds__(128, 2) bwd_split_kernel(
     const double* ckpt = rec + cap;
     const int nacc = n_acc[mode];
     double* tbar = table_bar + (size_t)(table_per_mode ? mode : ci) * 8 * tstride;
-    // shared: critical warp's workspace, two step slots, two record buffers, deferred accumulators
+    // shared (bwd_smem_doubles): critical warp's workspace, two step slots, two job buffers (records
+    // + step scalars), the a-chain warp's scratch, staging of both seed warps, their accumulators
     AdjMem A = carve_adj(wmem, D, false);
     double* slots = wmem + adj_mem_doubles(D, false);
     const int sd = slot_doubles(D);
-    double* recbuf = slots + 2 * sd;
-    const int rb = kRecPerStep * drec_doubles(D);
-    double* dpb = recbuf + 2 * rb;
-    TabAcc* dtab = reinterpret_cast<TabAcc*>(dpb + 16);
+    double* jobbuf = slots + 2 * sd;
+    const int jb = job_buf_doubles(D);
+    const int recs_len = kRecPerStep * drec_doubles(D);
+    double* ascr = jobbuf + 2 * jb;
+    double* g1 = ascr + kAScratch;
+    double* g2 = g1 + 8 * kDeferredSeeds;
+    double* pb1 = g2 + 8 * kDeferredSeeds;
+    TabAcc* tab1 = reinterpret_cast<TabAcc*>(pb1 + 16);
+    double* pb2 = pb1 + 16 + 2 * kNTabSeeds;
+    TabAcc* tab2 = reinterpret_cast<TabAcc*>(pb2 + 16);
+    double* lam0_final = pb2 + 16 + 2 * kNTabSeeds;
+    auto job_recs = [&](int j) { return jobbuf + (size_t)(j & 1) * jb; };
+    auto job_sc = [&](int j) { return jobbuf + (size_t)(j & 1) * jb + recs_len; };
     auto slot_mem = [&](int j, ModeMem& M, double*& Uk, double*& Zt, double*& meta) {
         double* b = slots + (size_t)(j & 1) * sd;
         M = carve(b, D);
@@ -249,12 +277,14 @@ __global__ void __launch_bounds__(128, 2) bwd_split_kernel(
         const double* ob = ybar20 + (size_t)mode * n_out * 20;
         for (int j = 0; j < nacc; ++j) {
             if (!wait_flag(tm, vf, F_REC, j + 1)) break;
-            if (!wait_flag(tm, vf, F_DEF, j - 1)) break;
+            // the job buffer of parity j was last read by job j - 2's seed warps
+            if (!wait_flag(tm, vf, F_DEF1, j - 1) || !wait_flag(tm, vf, F_DEF2, j - 1)) break;
             ModeMem M;
             double *Uk, *Zt, *meta;
             slot_mem(j, M, Uk, Zt, meta);
             const double tm0 = meta[0], h = meta[1];
             const int regime = (int)meta[2];
+            double lam0_out = 0.0;  // the output layer's a-cotangent at this step's end (warp 3's chain)
             while (jout >= 0 && tout[jout] > tm0) {  // outputs emitted at the end of this step
                 for (int i = tm.lane; i < n; i += 32) {
                     A.us[i] = M.u[i] + M.K[7 * n + i];
@@ -269,14 +299,15 @@ __global__ void __launch_bounds__(128, 2) bwd_split_kernel(
                 double acc = 0.0;
                 for (int i = tm.lane; i < n; i += 32) {
                     acc += A.ub[i] * A.yb[i];
-                    A.lam[i] += A.ub[i];
+                    if (i > 0) A.lam[i] += A.ub[i];
                 }
                 const double tb = tm.sum(acc);
                 if (tm.leader()) tau_out_bar[(size_t)mode * n_out + jout] = tb;
+                lam0_out += A.ub[0];
                 tm.sync();
                 --jout;
             }
-            adjoint_step(tm, *P, D, k, tm0, h, regime, M, A, Uk, Zt, recbuf + (size_t)(j & 1) * rb, hint);
+            adjoint_step(tm, *P, D, k, tm0, h, regime, M, A, Uk, Zt, job_recs(j), job_sc(j), lam0_out, hint, meta + 4);
             post_flag(tm, vf, F_CRIT, j + 1);
         }
         if (tm.leader())
@@ -300,6 +331,7 @@ __global__ void __launch_bounds__(128, 2) bwd_split_kernel(
             rodas5_step(tm, *P, D, k, tm0, h, regime, M, hint, (const DiscoebTangent*)nullptr, (const TanMem*)nullptr,
                         Uk);
             make_Zt(tm, D, M, h, Zt);
+            stage_backgrounds(tm, *P, D, k, tm0, h, regime, M, meta + 4, hint);
             if (tm.leader()) {
                 meta[0] = tm0;
                 meta[1] = h;
@@ -334,31 +366,50 @@ __global__ void __launch_bounds__(128, 2) bwd_split_kernel(
             post_flag(tm, vf, F_SEG, q + 1);
         }
     } else {
-        // ---- deferred ----
-        for (int q = tm.lane; q < 16; q += 32) dpb[q] = 0.0;
+        // ---- seed warps: 3 (the a-chain, then records 8..15) and 4 (records 0..7 and 16) ----
+        const bool achain = warp == 3;
+        double* pbw = achain ? pb1 : pb2;
+        TabAcc* tabw = achain ? tab1 : tab2;
+        double* gw = achain ? g1 : g2;
+        for (int q = tm.lane; q < 16; q += 32) pbw[q] = 0.0;
         for (int q = tm.lane; q < kNTabSeeds; q += 32) {
-            dtab[q].cur = -1;
-            dtab[q].w = 0.0;
+            tabw[q].cur = -1;
+            tabw[q].w = 0.0;
         }
         tm.sync();
+        double lam0 = 0.0;  // warp 3: the a-component of the running cotangent
         for (int j = 0; j < nacc; ++j) {
             if (!wait_flag(tm, vf, F_CRIT, j + 1)) break;
-            deferred_step(tm, *P, D, k, recbuf + (size_t)(j & 1) * rb, DefAcc{dpb, dtab}, tbar, tstride);
-            post_flag(tm, vf, F_DEF, j + 1);
+            double* recs = job_recs(j);
+            if (achain) {
+                achain_step(tm, *P, D, k, recs, job_sc(j), lam0, ascr);
+                post_flag(tm, vf, F_ACHAIN, j + 1);
+                deferred_records(tm, *P, D, k, recs, 8, 16, gw, DefAcc{pbw, tabw}, tbar, tstride);
+                post_flag(tm, vf, F_DEF1, j + 1);
+            } else {
+                if (!wait_flag(tm, vf, F_ACHAIN, j + 1)) break;
+                deferred_records(tm, *P, D, k, recs, 0, 8, gw, DefAcc{pbw, tabw}, tbar, tstride);
+                deferred_records(tm, *P, D, k, recs, 16, 17, gw, DefAcc{pbw, tabw}, tbar, tstride);
+                post_flag(tm, vf, F_DEF2, j + 1);
+            }
         }
+        if (achain && tm.leader()) *lam0_final = lam0;
+        tm.sync();
     }
     __syncthreads();
     const bool aborted = vf[F_ABORT] != 0;
     if (warp == 0) {
-        for (int i = tm.lane; i < n; i += 32) y0_bar[(size_t)mode * n + i] = aborted ? qnan : A.lam[i];
+        for (int i = tm.lane; i < n; i += 32)
+            y0_bar[(size_t)mode * n + i] = aborted ? qnan : (i == 0 ? *lam0_final : A.lam[i]);
         for (int q = tm.lane; q < 8; q += 32)
-            par_bar[(size_t)mode * 8 + q] = aborted ? qnan : A.pb[X_GRHOM + q] + dpb[X_GRHOM + q];
+            par_bar[(size_t)mode * 8 + q] = aborted ? qnan : A.pb[X_GRHOM + q] + pb1[X_GRHOM + q] + pb2[X_GRHOM + q];
         if (aborted)
             for (int j = tm.lane; j < n_out; j += 32) tau_out_bar[(size_t)mode * n_out + j] = qnan;
         for (int xs = X_KNOT0 + tm.lane; xs < X_KNOT0 + kNTabSeeds; xs += 32) {
             if (aborted) break;
             tab_flush(A.tab[xs - X_KNOT0], xs, tbar, tstride);
-            tab_flush(dtab[xs - X_KNOT0], xs, tbar, tstride);
+            tab_flush(tab1[xs - X_KNOT0], xs, tbar, tstride);
+            tab_flush(tab2[xs - X_KNOT0], xs, tbar, tstride);
         }
         if (tm.leader()) status[mode] = aborted ? DISCOEB_ABORTED : DISCOEB_OK;
     }
@@ -531,11 +582,7 @@ int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
         return DISCOEB_EINVAL;
     if (workspace_bytes < discoeb_bwd_workspace_bytes(cosmo0_host, n_modes, checkpoint_every)) return DISCOEB_EINVAL;
     const int mem = mode_mem_doubles(D);
-    // cosmology, flags, the critical warp's workspace, two step slots, two record buffers and the
-    // deferred warp's accumulators (16 parameter doubles + kNTabSeeds two-double accumulators)
-    const size_t smem = (size_t)(kCosmoDoublesB + kNFlags / 2 + adj_mem_doubles(D, false) + 2 * slot_doubles(D) +
-                                 2 * kRecPerStep * drec_doubles(D) + 16 + 2 * kNTabSeeds) *
-                        sizeof(double);
+    const size_t smem = (size_t)(kCosmoDoublesB + kNFlags / 2 + bwd_smem_doubles(D)) * sizeof(double);
     int dev = 0, max_optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -543,7 +590,7 @@ int32_t discoeb_bwd(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
     if (cudaFuncSetAttribute(bwd_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return DISCOEB_ECUDA;
     const long long rec = record_doubles(D.n, step_capacity, checkpoint_every);
-    bwd_split_kernel<<<n_modes, 128, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+    bwd_split_kernel<<<n_modes, 32 * kBwdWarps, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
         cosmos_dev, n_cosmo, mode_cosmo, n_modes, kmodes, tau_start, switch_tau, n_out, tau_out, step_capacity,
         checkpoint_every, rec, records, n_accepted, fwd_status, static_cast<double*>(workspace), y_out20_bar, mem,
         y0_bar, tau_out_bar, par_bar, table_bar, table_stride, table_per_mode ? 1 : 0, status);

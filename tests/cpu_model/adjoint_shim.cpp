@@ -42,8 +42,11 @@ int shim_adjoint_step(const DiscoebCosmo* P, const DiscoebTangent* tn, double k,
         A.tab[q].cur = -1;
         A.tab[q].w = 0.0;
     }
-    adjoint_step(tm, *P, D, k, t, h, regime, M, A, A.Uk, A.Zt, A.rec, hint);
-    deferred_step(tm, *P, D, k, A.rec, DefAcc{A.pb, A.tab}, tbar, tstride);
+    double l0 = lam1[0];
+    adjoint_step(tm, *P, D, k, t, h, regime, M, A, A.Uk, A.Zt, A.rec, A.as, 0.0, hint);
+    achain_step(tm, *P, D, k, A.rec, A.as, l0, A.scr);
+    deferred_records(tm, *P, D, k, A.rec, 0, kRecPerStep, A.g, DefAcc{A.pb, A.tab}, tbar, tstride);
+    A.lam[0] = l0;
     for (int xs = X_KNOT0; xs < X_KNOT0 + kNTabSeeds; ++xs) tab_flush(A.tab[xs - X_KNOT0], xs, tbar, tstride);
     std::memcpy(lam0, A.lam, sizeof(double) * n);
     for (int q = 0; q < 16; ++q) pbar[q] = A.pb[q];
