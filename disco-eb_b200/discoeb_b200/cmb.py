@@ -283,6 +283,61 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
     return out, param
 
 
+def compute_Cell_sharded(param_dict, *, dist=None, device=None, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0,
+                         n_fftlog=16384, lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3, num_thermo=1024, rtol=1e-4,
+                         atol=1e-4, max_steps=2048, k_sampling_method="camb", aexp_out=None, spectra=("TT",)):
+    """compute_Cell_spectrum_from_cosmo_params on the modes' own k grid (n_k_dense = 0) with the
+    modes spread over the ranks of ``dist`` (a torch.distributed process group, one process per
+    GPU): every rank solves its share of the modes (``replicas.shard``), takes their sources and
+    line of sight (rows of the line of sight are independent on the modes' own grid) and its
+    partial trapezoid sum over ln k of C_l, and the partial sums are added over the ranks
+    (``replicas.sum_over_ranks``; ``device``: where the collective's tensor lives, the rank's GPU
+    with NCCL, None with gloo).  Every rank returns the whole result, ``(Cell, param)`` as
+    compute_Cell_spectrum_from_cosmo_params with ``n_k_dense=0`` (a dict of spectra when
+    ``spectra`` names more than TT).  One process (dist None): the same computation on one GPU."""
+    from . import replicas
+    spectra = tuple(spectra)
+    if not spectra or any(x not in ("TT", "TE", "EE") for x in spectra):
+        raise ValueError(f"spectra must name TT, TE and/or EE, not {spectra!r}")
+    torch, dev = _device(None)
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist is not None else (0, 1)
+    param = evolve_background(param=dict(param_dict), thermo_module="RECFAST", num_thermo=num_thermo)
+    aexp_out = cmb_aexp_out() if aexp_out is None else np.asarray(aexp_out, dtype=np.float64)
+    kmodes = k_sampling(param, kmin, kmax, nmodes, k_sampling_method)
+    idx = replicas.shard(kmodes, rank, world)
+    mine = kmodes[idx]
+    tau = param["tau_of_a_spline"].evaluate(aexp_out)
+    L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
+    # the trapezoid weights in ln k of the whole grid, for this rank's rows
+    dlk = np.diff(np.log(kmodes))
+    wt = np.zeros(kmodes.shape[0])
+    wt[:-1] += 0.5 * dlk
+    wt[1:] += 0.5 * dlk
+    partial = {name: np.zeros(ellmax + 1) for name in spectra}
+    if mine.shape[0] > 0:
+        y = solve_modes(param=param, kmodes=mine, tau_out=tau, rtol=rtol, atol=atol, pcoeff=0.25, icoeff=0.80,
+                        dcoeff=0.0, factormax=20.0, factormin=0.3, max_steps=max_steps, return_full=True,
+                        device=dev, as_tensor=True, **L)
+        src = compute_sources(param=param, yout=y, kmodes=mine, aexp_out=aexp_out, device=dev, **L)
+        tau0 = float(param["tau_of_a_spline"].evaluate(1.0))
+        th = {}
+        if "TT" in spectra or "TE" in spectra:
+            th["T"], _ = compute_theta_ell(ellmax, mine, tau, src["S"], tau0, n_fftlog=n_fftlog, n_k_dense=0,
+                                           device=dev)
+        if "TE" in spectra or "EE" in spectra:
+            th["E"], _ = compute_theta_ell(ellmax, mine, tau, src["E"], tau0, n_fftlog=n_fftlog, n_k_dense=0,
+                                           device=dev, kind="E")
+        f64 = dict(dtype=torch.float64, device=dev)
+        w = torch.as_tensor(wt[idx] * (mine / param["k_p"]) ** (param["n_s"] - 1.0), **f64)
+        for name in spectra:
+            partial[name] = (w[:, None] * th[name[0]] * th[name[1]]).sum(dim=0).cpu().numpy()
+    cells = {name: replicas.sum_over_ranks(partial[name], dist, device) for name in spectra}
+    for key, v in (("lmaxg", lmaxg), ("lmaxgp", lmaxgp), ("lmaxr", lmaxr), ("lmaxnu", lmaxnu), ("nqmax", nqmax),
+                   ("nout", aexp_out.shape[0]), ("tau_out", tau)):
+        param[key] = v
+    return (cells["TT"] if spectra == ("TT",) else cells), param
+
+
 def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0, n_k_dense=8192, n_fftlog=16384,
                           lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3, num_thermo=1024, rtol=1e-4, atol=1e-4,
                           max_steps=2048, k_sampling_method="camb", aexp_out=None, de_guard_eps=1e-9, device=None,

@@ -368,6 +368,30 @@ def power_spectrum_jacobian(theta, *, on_failure="raise", return_stats=False, **
     return prob.kmodes, P, J
 
 
+def power_spectrum_jacobian_sharded(theta, *, dist=None, device=None, on_failure="raise", **options):
+    """power_spectrum_jacobian with one cosmology's modes spread over the ranks of ``dist`` (a
+    torch.distributed process group, one process per GPU; ``replicas.init``): each rank solves its
+    share (``replicas.shard``: longest-first, dealt round-robin) and every rank returns the whole
+    (k, P [K, nout], J [8, K, nout]), gathered with ``replicas.gather_rows`` (``device``: where
+    the collective's tensors live, the rank's GPU with NCCL, None with gloo).  One process (dist
+    None): power_spectrum_jacobian.  Options as power_spectrum_jacobian."""
+    from . import replicas
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist is not None else (0, 1)
+    k = options.pop("kmodes", None)
+    if k is None:
+        kp = theta_to_params(theta)
+        method = options.pop("k_sampling_method", "log")
+        if method == "camb":  # needs tau_maxvis of the background
+            kp = evolve_background(param=kp, num_thermo=options.get("num_thermo", 256))
+        k = k_sampling(kp, options.pop("kmin", 1e-4), options.pop("kmax", 1.0), options.pop("num_k", 64), method)
+    k = np.ascontiguousarray(k, dtype=np.float64)
+    idx = replicas.shard(k, rank, world)
+    _, P, J = power_spectrum_jacobian(theta, kmodes=k[idx], on_failure=on_failure, **options)
+    P_all = replicas.gather_rows(P, idx, k.shape[0], dist, device)
+    J_all = replicas.gather_rows(np.moveaxis(J, 1, 0), idx, k.shape[0], dist, device)
+    return k, P_all, np.moveaxis(J_all, 0, 1)
+
+
 def power_spectrum_function(gradient="forward", **options):
     """A ``torch.autograd.Function`` mapping theta (float64[8], THETA_NAMES order) to
     P(k, a_out) (float64[K, nout]).

@@ -26,8 +26,12 @@ def _rank_main(rank, world, port, out):
     m = replicas.max_over_ranks(1.5 + rank, dist)
     ks = np.geomspace(1e-4, 10.0, 11)
     mine = replicas.shard(ks, r, w)
+    # every rank gets all rows back in the caller's order; partial sums add up
+    rows = np.stack([mine * 1.0, np.sqrt(mine + 1.0)], axis=1)[:, :, None]
+    full = replicas.gather_rows(rows, mine, ks.size, dist)
+    total = replicas.sum_over_ranks(np.array([rank + 1.0, 0.5]), dist)
     replicas.finish(dist)
-    out.put((rank, m, mine.tolist()))
+    out.put((rank, m, mine.tolist(), full.tolist(), total.tolist()))
 
 
 def test_two_gloo_ranks():
@@ -42,8 +46,12 @@ def test_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    assert [m for _, m, _ in res] == [2.5, 2.5]
-    parts = [set(x) for _, _, x in res]
+    assert [r[1] for r in res] == [2.5, 2.5]
+    want = np.stack([np.arange(11.0), np.sqrt(np.arange(11.0) + 1.0)], axis=1)[:, :, None]
+    for r in res:
+        np.testing.assert_array_equal(np.array(r[3]), want)
+        assert r[4] == [3.0, 1.0]
+    parts = [set(r[2]) for r in res]
     assert parts[0].isdisjoint(parts[1]) and parts[0] | parts[1] == set(range(11))
     assert abs(len(parts[0]) - len(parts[1])) <= 1
 
@@ -56,3 +64,5 @@ def test_single_process_needs_no_process_group(monkeypatch):
     assert replicas.max_over_ranks(3.0, dist) == 3.0
     replicas.finish(dist)
     np.testing.assert_array_equal(replicas.shard(np.array([0.1, 1.0, 0.01]), 0, 1), [0, 1, 2])
+    np.testing.assert_array_equal(replicas.gather_rows(np.array([[1.0], [2.0]]), [1, 0], 2, dist), [[2.0], [1.0]])
+    np.testing.assert_array_equal(replicas.sum_over_ranks([1.0, 2.0], dist), [1.0, 2.0])
