@@ -417,11 +417,21 @@ def run_cmb(args, rank, world, local):
         e[4].synchronize()
         return [e[i].elapsed_time(e[i + 1]) for i in range(4)]
 
+    def fused():  # the solve with the source assembly in its output stage (discoeb_fwd_sources)
+        e = [ev() for _ in range(2)]
+        e[0].record(stream)
+        cmb.solve_sources(param=bg, kmodes=ks, aexp_out=a, rtol=1e-4, atol=1e-4, max_steps=2048, device=device, **L)
+        e[1].record(stream)
+        e[1].synchronize()
+        return e[0].elapsed_time(e[1])
+
     for _ in range(args.warmup):
         stages()
+        fused()
     with ClockSampler(local) as clk:
         times = [stages() for _ in range(args.steps)]
     per = np.mean(np.array(times), axis=0)
+    fused_ms = statistics.mean([fused() for _ in range(args.steps)])
     e2e = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -439,6 +449,7 @@ def run_cmb(args, rank, world, local):
             "config": {"workload": "cmb_tt_disco_notebook_k128_l2500", "num_k": 128, "n_tau": 320, "n_k_dense": 8192,
                        "n_fftlog": 16384, "ellmax": 2500},
             "stages_ms": {"full_solve": per[0], "sources": per[1], "line_of_sight": per[2], "cell": per[3]},
+            "fused_solve_and_sources_ms": fused_ms,
             "e2e": {"value": 1.0 / statistics.mean(e2e), "unit": "spectra/s", "ms_per_cosmology":
                     1e3 * statistics.mean(e2e)},
             "clocks": clk.summary(),

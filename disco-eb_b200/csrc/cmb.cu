@@ -174,6 +174,95 @@ __global__ void __launch_bounds__(128) sources_kernel(const DiscoebCosmo* __rest
     for (int f = DISCOEB_SRC_S2; f < DISCOEB_SRC_NFIELDS; ++f) fields[f * stride + o] = out[f];
 }
 
+// The forward solve with the source assembly in its output stage: one warp per mode runs the
+// adaptive solve (solve_mode) and, at each output time, projects the state (RSA), re-evaluates
+// y' there and assembles the sources, exactly as discoeb_fwd followed by sources_kernel do, but
+// without the full states going through HBM.  y_full (may be null) still receives the projected
+// states.  Shared memory per warp: the cosmology and the mode's workspace.
+constexpr int kCosmoDoublesC = (sizeof(DiscoebCosmo) + 7) / 8;
+
+__global__ void __launch_bounds__(32) fwd_sources_kernel(
+    const DiscoebCosmo* __restrict__ cosmo, DiscoebControl ctrl, int n_modes, const double* __restrict__ kmodes,
+    const double* __restrict__ tau_start, const double* __restrict__ y0, const double* __restrict__ sw, int n_tau,
+    const double* __restrict__ tau, const double* __restrict__ bt, int mem_doubles, double* y_full, double* fields,
+    int32_t* status, int32_t* nsteps)
+{
+    extern __shared__ double smem[];
+    const WarpTeam tm{(int)(threadIdx.x & 31)};
+    const int mode = blockIdx.x;
+    if (mode >= n_modes) return;
+    DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(smem);
+    double* wmem = smem + kCosmoDoublesC;
+    {
+        const int* src = reinterpret_cast<const int*>(cosmo);
+        int* dst = reinterpret_cast<int*>(P);
+        for (int i = tm.lane; i < (int)(sizeof(DiscoebCosmo) / 4); i += 32) dst[i] = src[i];
+    }
+    tm.sync();
+    const Dims D = make_dims(*P);
+    const int n = D.n;
+    const size_t stride = (size_t)n_modes * n_tau;
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+    auto fill_nan = [&](int from) {
+        for (int j = from; j < n_tau; ++j) {
+            const size_t o = (size_t)mode * n_tau + j;
+            for (int f = tm.lane; f < DISCOEB_SRC_NFIELDS; f += 32) fields[f * stride + o] = qnan;
+            if (y_full)
+                for (int i = tm.lane; i < n; i += 32) y_full[o * n + i] = qnan;
+        }
+    };
+    if (mode_mem_doubles(D) != mem_doubles) {
+        fill_nan(0);
+        if (tm.leader()) {
+            status[mode] = DISCOEB_BAD_INDEX;
+            nsteps[mode] = 0;
+        }
+        return;
+    }
+    ModeMem M = carve(wmem, D);
+    const double k = kmodes[mode];
+    for (int i = tm.lane; i < n; i += 32) M.y[i] = y0[(size_t)mode * n + i];
+    const double swm[3] = {sw[3 * mode], sw[3 * mode + 1], sw[3 * mode + 2]};
+    tm.sync();
+    const SrcPar<double> sp{P->grhom, P->Omegam, P->Omegab, P->OmegaDE, P->amnu, P->w0, P->wa};
+    auto emit = [&](int j, const double* y, int) {
+        const double t = tau[j];
+        // the projected state into M.f, y' there into M.dT (both are rebuilt at the next step start)
+        double fld[4];
+        const bool rsa = rsa_projection<double>(*P, nullptr, D, t, k, y, nullptr, fld);
+        const size_t o = (size_t)mode * n_tau + j;
+        for (int i = tm.lane; i < n; i += 32) {
+            double v = y[i];
+            if (rsa) {
+                const int sl = rsa_slot(D, i);
+                if (sl >= 0) v = fld[sl];
+                else if (sl == -1) v = 0.0;
+            }
+            M.f[i] = v;
+            if (y_full) y_full[o * n + i] = v;
+        }
+        tm.sync();
+        Bg<double> b;
+        bg_eval(*P, M.f[0], t, k, -1, b);
+        rhs_team(tm, *P, D, b, k, t, M.f, M.dT, (double*)nullptr);
+        tm.sync();
+        if (tm.leader()) {
+            double btj[DISCOEB_BG_NFIELDS];
+            for (int f = 0; f < DISCOEB_BG_NFIELDS; ++f) btj[f] = bt[f * n_tau + j];
+            double out[DISCOEB_SRC_NFIELDS];
+            assemble_sources(*P, sp, D, k, btj, [&](int i) { return M.f[i]; }, [&](int i) { return M.dT[i]; }, out);
+            for (int f = DISCOEB_SRC_S2; f < DISCOEB_SRC_NFIELDS; ++f) fields[f * stride + o] = out[f];
+        }
+        tm.sync();
+    };
+    const SolveResult R = solve_mode(tm, *P, D, ctrl, k, tau_start[mode], swm, n_tau, tau, M, emit);
+    fill_nan(R.outputs);
+    if (tm.leader()) {
+        status[mode] = R.status;
+        nsteps[mode] = R.steps;
+    }
+}
+
 // Natural cubic spline second derivatives through (x[i], y[i*ys]) for i < n (the Thomas
 // recurrence of spline_interpolation.py:19-75), written to S[i*ys]; cp is scratch of n
 // doubles with stride cs.
@@ -1002,6 +1091,38 @@ int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo
     const size_t smem = sizeof(double) * (size_t)D.n * (threads / 32);
     sources_kernel<<<blocks_for(points * 32, threads), threads, smem, s>>>(cosmo_dev, n_modes, kmodes, n_tau, tau,
                                                                             bgtab, y_full, fields);
+    isw_kernel<<<blocks_for(n_modes, 64), 64, 0, s>>>(n_modes, n_tau, tau, bgtab, fields, scratch);
+    return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
+}
+
+int32_t discoeb_fwd_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host,
+                            const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
+                            const double* y0, const double* switch_tau, int32_t n_tau, const double* tau,
+                            const double* bgtab, double* y_full, double* fields, double* scratch, int32_t* status,
+                            int32_t* nsteps, void* stream)
+{
+    if (!cosmo_host || !cosmo_dev || !ctrl || n_modes < 0 || n_tau < 0) return DISCOEB_EINVAL;
+    if (cosmo_host->use_tca) return DISCOEB_EUNSUPPORTED;
+    if (cosmo_host->nqmax < 0 || cosmo_host->nqmax > DISCOEB_MAX_NQ) return DISCOEB_EINVAL;
+    if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED) return DISCOEB_EUNSUPPORTED;
+    if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
+    if (n_modes == 0 || n_tau == 0) return DISCOEB_SUCCESS;
+    if (n_tau < 3 || !kmodes || !tau_start || !y0 || !switch_tau || !tau || !bgtab || !fields || !scratch ||
+        !status || !nsteps)
+        return DISCOEB_EINVAL;
+    if ((long long)n_modes * n_tau > 0x7fffffffLL) return DISCOEB_EINVAL;
+    const Dims D = make_dims(*cosmo_host);
+    const int mem = mode_mem_doubles(D);
+    const size_t smem = (size_t)(kCosmoDoublesC + mem) * sizeof(double);
+    int dev = 0, max_optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
+    if (cudaFuncSetAttribute(fwd_sources_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return DISCOEB_ECUDA;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    fwd_sources_kernel<<<n_modes, 32, smem, s>>>(cosmo_dev, *ctrl, n_modes, kmodes, tau_start, y0, switch_tau, n_tau,
+                                                  tau, bgtab, mem, y_full, fields, status, nsteps);
     isw_kernel<<<blocks_for(n_modes, 64), 64, 0, s>>>(n_modes, n_tau, tau, bgtab, fields, scratch);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }

@@ -199,6 +199,9 @@ def lib():
         L.discoeb_sources_noalloc.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, vp, ctypes.c_int32, vp,
                                               vp, vp, vp, vp]
         L.discoeb_sources_noalloc.restype = ctypes.c_int32
+        L.discoeb_fwd_sources.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), ctypes.POINTER(DiscoebControl),
+                                          ctypes.c_int32, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.discoeb_fwd_sources.restype = ctypes.c_int32
         L.discoeb_los_workspace_bytes.argtypes = [ctypes.c_int32] * 5
         L.discoeb_los_workspace_bytes.restype = ctypes.c_int64
         L.discoeb_los.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, vp, ctypes.c_double, ctypes.c_int32,

@@ -17,7 +17,8 @@ import numpy as np
 
 from . import _abi
 from .background import compute_background_quantities, evolve_background, get_aprimeoa, get_neutrino_momentum_bins
-from .perturbations import DeviceCosmo, solve_modes, k_sampling
+from .perturbations import (DeviceCosmo, _check_status, adiabatic_ics, approximation_switch_times,
+                            determine_starting_time, k_sampling, solve_modes)
 from .spline import spline_interpolation
 
 BG_FIELDS = ("a", "aprimeoa", "rhonu", "rho_Q", "w_Q", "opac", "opacprime", "gvis", "gvisprime", "gvispprime",
@@ -114,6 +115,57 @@ def compute_sources(*, param, yout, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmax
     if rc != 0:
         raise RuntimeError(f"discoeb_sources failed with code {rc}")
     return {name: fields[i] for i, name in enumerate(SRC_FIELDS)}
+
+
+def solve_sources(*, param, kmodes, aexp_out, lmaxg, lmaxgp, lmaxr, lmaxnu, nqmax, rtol, atol, max_steps,
+                  de_guard_eps=1e-9, device=None, return_states=False, on_failure="raise"):
+    """The full perturbation solve and the source assembly in one pass (discoeb_fwd_sources):
+    the same fields as solve_modes(return_full=True) followed by compute_sources, without the full
+    states going through device memory.  The step controller is the reference pipeline's (PID
+    coefficients 0.25 / 0.80 / 0, factors 20 / 0.3).  Returns the dict of source fields (device
+    tensors [K, n_tau], caller's mode order), and with ``return_states`` also the projected states
+    [K, n_tau, nvar]."""
+    torch, device = _device(device)
+    lib = _abi.lib()
+    aexp_out = np.asarray(aexp_out, dtype=np.float64)
+    tau = param["tau_of_a_spline"].evaluate(aexp_out)
+    if np.any(np.diff(tau) <= 0):
+        raise ValueError("aexp_out must map to strictly increasing output times")
+    kmodes = np.ascontiguousarray(kmodes, dtype=np.float64)
+    K, T = kmodes.shape[0], tau.shape[0]
+    L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
+    tau_start = 0.99 * np.minimum(tau.min(), determine_starting_time(param=param, k=kmodes))
+    y0 = adiabatic_ics(tau=tau_start, param=param, kmode=kmodes, **L)
+    sw = approximation_switch_times(param, kmodes)
+    order = np.argsort(-kmodes, kind="stable")  # longest modes first
+    inv_np = np.argsort(order)
+    dc = DeviceCosmo(param, de_guard_eps=de_guard_eps, device=device, **L)
+    f64 = dict(dtype=torch.float64, device=device)
+    as_dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+    d_k, d_ts, d_y0, d_sw = as_dev(kmodes[order]), as_dev(tau_start[order]), as_dev(y0[order]), as_dev(sw[order])
+    d_tau = as_dev(tau)
+    d_bt = as_dev(background_table(aexp_out, tau, param))
+    n = y0.shape[1]
+    d_full = torch.empty((K, T, n), **f64) if return_states else None
+    fields = torch.empty((len(SRC_FIELDS), K, T), **f64)
+    scratch = torch.empty((K, T), **f64)
+    d_stat = torch.empty((2, K), dtype=torch.int32, device=device)
+    ctrl = _abi.DiscoebControl(rtol, atol, 0.25, 0.80, 0.0, 20.0, 0.3, int(max_steps), _abi.METHOD_RODAS5_STRUCTURED,
+                               0, 0)
+    rc = lib.discoeb_fwd_sources(dc.struct.data_ptr(), ctypes.byref(dc.host), ctypes.byref(ctrl), K, d_k.data_ptr(),
+                                 d_ts.data_ptr(), d_y0.data_ptr(), d_sw.data_ptr(), T, d_tau.data_ptr(),
+                                 d_bt.data_ptr(), d_full.data_ptr() if d_full is not None else None,
+                                 fields.data_ptr(), scratch.data_ptr(), d_stat[0].data_ptr(), d_stat[1].data_ptr(),
+                                 torch.cuda.current_stream(device).cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"discoeb_fwd_sources failed with code {rc}")
+    stat = d_stat.cpu().numpy()
+    _check_status(stat[0][inv_np], stat[1][inv_np], kmodes, on_failure)
+    inv = torch.from_numpy(inv_np).to(device)
+    out = {name: fields[i].index_select(0, inv) for i, name in enumerate(SRC_FIELDS)}
+    if return_states:
+        return out, d_full.index_select(0, inv)
+    return out
 
 
 def compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0, device=None, kind="T"):
@@ -239,13 +291,15 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
                                             n_fftlog=16384, lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3,
                                             num_thermo=1024, rtol=1e-4, atol=1e-4, max_steps=2048,
                                             k_sampling_method="camb", aexp_out=None, device=None,
-                                            return_intermediates=False, spectra=("TT",)):
+                                            return_intermediates=False, spectra=("TT",), fused_sources=False):
     """C_l^TT of a cosmology (cmb.py:931-1090): background (host), full perturbation solve,
     sources, FFTLog line of sight and C_l on the GPU, large arrays never leaving the device.
 
     Returns ``(Cell [ellmax+1] numpy, param)`` like the reference.  ``spectra`` naming more than TT
     (any of "TT", "TE", "EE"; the reference has temperature only) returns ``({name: Cell}, param)``
     with the E-mode multipoles from the same solve (compute_theta_ell(kind="E")).
+    ``fused_sources``: the solve and the source assembly in one pass (solve_sources), the full
+    states never written to device memory (the same sources; intermediates then hold no states).
     """
     spectra = tuple(spectra)
     if not spectra or any(x not in ("TT", "TE", "EE") for x in spectra):
@@ -256,10 +310,15 @@ def compute_Cell_spectrum_from_cosmo_params(param_dict, ellmax=2500, nmodes=128,
     kmodes = k_sampling(param, kmin, kmax, nmodes, k_sampling_method)
     tau = param["tau_of_a_spline"].evaluate(aexp_out)
     L = dict(lmaxg=lmaxg, lmaxgp=lmaxgp, lmaxr=lmaxr, lmaxnu=lmaxnu, nqmax=nqmax)
-    y = solve_modes(param=param, kmodes=kmodes, tau_out=tau, rtol=rtol, atol=atol, pcoeff=0.25, icoeff=0.80,
-                    dcoeff=0.0, factormax=20.0, factormin=0.3, max_steps=max_steps, return_full=True,
-                    device=device, as_tensor=True, **L)
-    src = compute_sources(param=param, yout=y, kmodes=kmodes, aexp_out=aexp_out, device=device, **L)
+    if fused_sources:
+        y = None
+        src = solve_sources(param=param, kmodes=kmodes, aexp_out=aexp_out, rtol=rtol, atol=atol, max_steps=max_steps,
+                            device=device, **L)
+    else:
+        y = solve_modes(param=param, kmodes=kmodes, tau_out=tau, rtol=rtol, atol=atol, pcoeff=0.25, icoeff=0.80,
+                        dcoeff=0.0, factormax=20.0, factormin=0.3, max_steps=max_steps, return_full=True,
+                        device=device, as_tensor=True, **L)
+        src = compute_sources(param=param, yout=y, kmodes=kmodes, aexp_out=aexp_out, device=device, **L)
     tau0 = float(param["tau_of_a_spline"].evaluate(1.0))
     theta = theta_e = None
     if "TT" in spectra or "TE" in spectra:

@@ -296,6 +296,22 @@ int32_t discoeb_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo
                         const double* kmodes, int32_t n_tau, const double* tau, const double* bgtab,
                         const double* y_full, double* fields, double* scratch, void* stream);
 
+/* The forward solve of one cosmology's modes with the source assembly done in its output stage:
+ * discoeb_fwd (its arguments for n_cosmo = 1, the output times being the source times tau) and
+ * discoeb_sources in one pass, replacing evolve_perturbations(return_full=True) +
+ * compute_time_derivatives + the source assembly of cmb.py:17-633 without the full states
+ * making the round trip through device memory.  Each mode's warp projects the state at every
+ * output time, re-evaluates y' there and assembles the sources; the ISW term follows as in
+ * discoeb_sources.  y_full [n_modes, n_tau, nvar] (may be NULL) still receives the projected
+ * states; fields, scratch, bgtab as discoeb_sources; status / nsteps per mode as discoeb_fwd
+ * (fields of a failed mode's unreached times are NaN).  The results equal discoeb_fwd followed
+ * by discoeb_sources.  Structured FP64 method only. */
+int32_t discoeb_fwd_sources(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host,
+                            const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
+                            const double* y0, const double* switch_tau, int32_t n_tau, const double* tau,
+                            const double* bgtab, double* y_full, double* fields, double* scratch, int32_t* status,
+                            int32_t* nsteps, void* stream);
+
 /* discoeb_sources for callers that cannot allocate device memory: code running where another
  * framework owns the GPU's memory (XLA preallocates most of it, so an FFI handler that was given
  * no workspace buffer has nothing to pass as scratch and must not cudaMalloc behind the

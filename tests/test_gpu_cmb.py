@@ -143,3 +143,30 @@ def test_gpu_cmb_spectrum_pipeline(torch_cuda):
     rte = np.abs(DTE - cls["TE"]) / np.sqrt(cls["TT"] * cls["EE"])
     assert ree.mean() < 0.02 and np.median(ree) < 0.015, (ree.mean(), np.median(ree))
     assert rte.mean() < 0.01, rte.mean()
+
+
+def test_gpu_fused_solve_and_sources_equal_the_two_stages(gpu_states):
+    """discoeb_fwd_sources (the solve with the source assembly in its output stage) against
+    discoeb_fwd + discoeb_sources on the same modes: the same states and fields to rounding (the
+    same source code, compiled into two kernels: measured 3.5e-11 on the states), and the
+    pipeline's C_l with fused_sources equal to the two-stage one."""
+    import warnings
+    from discoeb_b200.cmb import compute_Cell_spectrum_from_cosmo_params, compute_sources, solve_sources
+    bg, a, tau, ks, y = gpu_states
+    src = compute_sources(param=bg, yout=y, kmodes=ks, aexp_out=a, **L11)
+    for _ in range(2):
+        fused, yf = solve_sources(param=bg, kmodes=ks, aexp_out=a, rtol=1e-4, atol=1e-4, max_steps=4096,
+                                  return_states=True, **L11)
+        _close(yf.cpu().numpy(), y.cpu().numpy(), 1e-9)
+        for name in src:
+            _close(fused[name].cpu().numpy(), src[name].cpu().numpy(), 1e-9)
+    p = {"Omegam": 0.3099, "Omegab": 0.0488911, "H0": 67.742, "n_s": 0.96822, "A_s": 2.1064e-09, "mnu": 0.06,
+         "Tcmb": 2.7255, "YHe": 0.248, "Neff": 2.046, "Nmnu": 1, "w_DE_0": -0.99, "w_DE_a": 0.0, "cs2_DE": 1.0,
+         "Omegak": 0.0, "k_p": 0.05}
+    opts = dict(ellmax=600, nmodes=32, n_k_dense=1024, n_fftlog=4096, spectra=("TT", "EE"))
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        c1, _ = compute_Cell_spectrum_from_cosmo_params(p, **opts)
+        c2, _ = compute_Cell_spectrum_from_cosmo_params(p, fused_sources=True, **opts)
+    for name in opts["spectra"]:
+        np.testing.assert_allclose(c2[name][2:], c1[name][2:], rtol=1e-8, atol=0)

@@ -261,3 +261,21 @@ def test_plain_c_caller_of_the_background_entry():
     assert got.shape == (len(_abi.BGS), 2)
     np.testing.assert_array_equal(got[:, 0], buf[: len(_abi.BGS)])
     np.testing.assert_array_equal(got[:, 1], dots[0][: len(_abi.BGS)])
+
+
+def test_fused_sources_entry_rejects_bad_arguments_before_any_launch():
+    lib = _abi.lib()
+    host = _abi.DiscoebCosmo()
+    host.lmaxg, host.lmaxgp, host.lmaxr, host.lmaxnu, host.nqmax = 11, 11, 11, 8, 3
+    ctrl = _abi.DiscoebControl(1e-4, 1e-4, 0.25, 0.8, 0.0, 20.0, 0.3, 2048, _abi.METHOD_RODAS5_STRUCTURED, 0, 0)
+    fake = 4096  # never dereferenced: the argument checks return first
+    ok = [fake, ctypes.byref(host), ctypes.byref(ctrl), 4, fake, fake, fake, fake, 16, fake, fake, None, fake, fake,
+          fake, fake, None]
+    for i, v in ((0, None), (3, -1), (8, 2), (12, None), (13, None), (14, None), (9, None)):
+        args = list(ok)
+        args[i] = v
+        assert lib.discoeb_fwd_sources(*args) == -1, (i, v)
+    bad = _abi.DiscoebControl(1e-4, 1e-4, 0.25, 0.8, 0.0, 20.0, 0.3, 2048, _abi.METHOD_RODAS5_STRUCTURED_MIXED, 0, 0)
+    args = list(ok)
+    args[2] = ctypes.byref(bad)
+    assert lib.discoeb_fwd_sources(*args) == -3  # DISCOEB_EUNSUPPORTED
