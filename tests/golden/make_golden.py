@@ -83,7 +83,7 @@ cmb["camb:ell"] = cb[:, 0]
 cmb["camb:D_ell"] = cb[:, 1]
 # the CLASS spectra the reference's test_cmb_vs_class compares with (no reionisation, no lensing;
 # columns ell, D_ell_TT, D_ell_EE, D_ell_TE): TT pins the temperature chain, EE and TE the E-mode
-# polarisation that this build adds
+# polarisation spectra, which the reference itself does not compute
 with open(os.path.join(ref, "tests/resources/class_benchmarks/DISCO-Notebook.csv")) as fh:
     rows = list(csv.reader(fh))
 head, vals = rows[0], np.array([[float(v) for v in r] for r in rows[1:]])
