@@ -432,6 +432,30 @@ def run_cmb(args, rank, world, local):
         times = [stages() for _ in range(args.steps)]
     per = np.mean(np.array(times), axis=0)
     fused_ms = statistics.mean([fused() for _ in range(args.steps)])
+    # the line of sight alone with its frequency sum on the int8 tensor cores (the default) and as
+    # an FP64 DGEMM, on the same sources, and the largest relative difference of their C_l^TT
+    y = solve_modes(param=bg, kmodes=ks, tau_out=tau, rtol=1e-4, atol=1e-4, pcoeff=0.25, icoeff=0.8, dcoeff=0.0,
+                    factormax=20.0, factormin=0.3, max_steps=2048, return_full=True, as_tensor=True, device=device,
+                    **L)
+    src_S = cmb.compute_sources(param=bg, yout=y, kmodes=ks, aexp_out=a, device=device, **L)["S"]
+    before = cmb.get_los_contraction()
+
+    def los(kind):
+        cmb.set_los_contraction(kind, 7)
+        e = [ev() for _ in range(2)]
+        e[0].record(stream)
+        th, kk = cmb.compute_theta_ell(2500, ks, tau, src_S, tau0, n_fftlog=16384, n_k_dense=8192, device=device)
+        e[1].record(stream)
+        e[1].synchronize()
+        return e[0].elapsed_time(e[1]), cmb.compute_Cell(th, kk, bg["n_s"], bg["k_p"], device=device).cpu().numpy()
+
+    los("fp64"), los("int8")
+    los_t = {kind: [los(kind) for _ in range(args.steps)] for kind in ("fp64", "int8")}
+    cmb.set_los_contraction(*before)
+    cl64, cl8 = los_t["fp64"][0][1], los_t["int8"][0][1]
+    los_cmp = {"int8_slices7_ms": statistics.mean(t for t, _ in los_t["int8"]),
+               "fp64_dgemm_ms": statistics.mean(t for t, _ in los_t["fp64"]),
+               "cl_tt_max_rel_diff": float(np.max(np.abs(cl8[2:] / cl64[2:] - 1.0)))}
     e2e = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -450,6 +474,7 @@ def run_cmb(args, rank, world, local):
                        "n_fftlog": 16384, "ellmax": 2500},
             "stages_ms": {"full_solve": per[0], "sources": per[1], "line_of_sight": per[2], "cell": per[3]},
             "fused_solve_and_sources_ms": fused_ms,
+            "line_of_sight_contraction": los_cmp,
             "e2e": {"value": 1.0 / statistics.mean(e2e), "unit": "spectra/s", "ms_per_cosmology":
                     1e3 * statistics.mean(e2e)},
             "clocks": clk.summary(),

@@ -18,10 +18,12 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <mutex>
 
+#include "dgemm_i8.cuh"
 #include "discoeb.h"
 #include "fft_plans.cuh"
 #include "lngamma.cuh"
@@ -867,19 +869,32 @@ __global__ void isw_dot_kernel(int n_dir, int n_modes, int n_tau, const double* 
 // ------------------------------------------------------------------------------------------
 // workspace layout of discoeb_los (byte offsets, 256-byte aligned)
 
+// how the frequency sum is contracted: DISCOEB_LOS_FP64 (cuBLAS DGEMM) or DISCOEB_LOS_INT8
+// (discoeb_dgemm_i8 with `slices` digit planes); library-wide, read once per call
+struct LosContraction {
+    int kind, slices;
+};
+std::atomic<int> g_los_kind{DISCOEB_LOS_INT8};
+std::atomic<int> g_los_slices{7};
+
+LosContraction los_contraction() { return {g_los_kind.load(), g_los_slices.load()}; }
+
 struct LosLayout {
-    size_t sd, s2k, lk, cpk, kd, s2c, cpc, lchi, fidx, fx, fbias, geom, fft, B, cufft, cublas, total;
+    size_t sd, s2k, lk, cpk, kd, s2c, cpc, lchi, fidx, fx, fbias, geom, fft, B, cufft, cublas, i8, total;
     long long pitch;
     int n_rows, n_freq;
+    LosContraction con;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 constexpr size_t kCublasWorkspace = 32u << 20;
 
-LosLayout los_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n_dense, size_t cufft_bytes)
+LosLayout los_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n_dense, size_t cufft_bytes,
+                     LosContraction con)
 {
     LosLayout L;
+    L.con = con;
     L.n_rows = n_dense > 0 ? n_dense : n_modes;
     L.n_freq = n_fft / 2 + 1;
     L.pitch = 2LL * L.n_freq;
@@ -901,6 +916,10 @@ LosLayout los_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n_dense,
     L.B = take(sizeof(double) * (size_t)(ellmax + 1) * L.pitch);
     L.cufft = take(cufft_bytes);
     L.cublas = take(kCublasWorkspace);
+    const int64_t i8 = con.kind == DISCOEB_LOS_INT8
+                           ? dgemm_i8::workspace_bytes(L.n_rows, ellmax + 1, (int)L.pitch, con.slices, 0)
+                           : 0;
+    L.i8 = take(i8 > 0 ? (size_t)i8 : 0);
     L.total = o;
     return L;
 }
@@ -962,7 +981,7 @@ int32_t los_forward(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
     size_t work = 0;
     std::unique_lock<std::mutex> fft_lock(discoeb_fft::plan_mutex());
     if (!discoeb_fft::cached_plan(CUFFT_D2Z, n_fftlog, rows, pitch, pitch / 2, &plan, &work)) return DISCOEB_ECUDA;
-    const LosLayout L = los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work);
+    const LosLayout L = los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work, los_contraction());
     if ((uint64_t)workspace_bytes < L.total) return DISCOEB_EINVAL;
     auto D = [&](size_t off) { return reinterpret_cast<double*>(ws + off); };
     const int T = 256;
@@ -1003,7 +1022,11 @@ int32_t los_forward(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
     mcoef_kernel<<<blocks_for((long long)(ellmax + 1) * L.n_freq, T), T, 0, s>>>(ellmax + 1, L.n_freq, n_fftlog,
                                                                                  D(L.geom), D(L.B));
     if (cudaGetLastError() != cudaSuccess) return DISCOEB_ECUDA;
-    // 5. theta[r, l] = sum_j A[r, j] B[l, j] over the interleaved (re, im) pairs: one DGEMM
+    // 5. theta[r, l] = sum_j A[r, j] B[l, j] over the interleaved (re, im) pairs: one product,
+    //    on the int8 tensor cores (digit planes, exact int32 sums) or as a cuBLAS DGEMM
+    if (L.con.kind == DISCOEB_LOS_INT8)
+        return dgemm_i8::run(rows, ellmax + 1, (int)L.pitch, D(L.fft), L.pitch, D(L.B), L.pitch, theta, ellmax + 1,
+                             L.con.slices, 0, ws + L.i8, (int64_t)(L.total - L.i8), stream);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
     std::lock_guard<std::mutex> lock(g_blas_mu);
@@ -1030,7 +1053,7 @@ struct LosJvpLayout {
 LosJvpLayout los_jvp_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n_dense, size_t cufft_bytes)
 {
     LosJvpLayout J;
-    J.base = los_layout(n_modes, n_tau, ellmax, n_fft, n_dense, cufft_bytes);
+    J.base = los_layout(n_modes, n_tau, ellmax, n_fft, n_dense, cufft_bytes, los_contraction());
     const size_t rows = (size_t)J.base.n_rows, L = (size_t)ellmax + 1, pitch = (size_t)J.base.pitch;
     size_t o = J.base.total;
     auto take = [&](size_t doubles) { const size_t at = o; o = align256(o + sizeof(double) * doubles); return at; };
@@ -1153,7 +1176,24 @@ int64_t discoeb_los_workspace_bytes(int32_t n_modes, int32_t n_tau, int32_t ellm
     size_t work = 0;
     std::lock_guard<std::mutex> lock(discoeb_fft::plan_mutex());
     if (!discoeb_fft::cached_plan(CUFFT_D2Z, n_fftlog, rows, pitch, pitch / 2, &plan, &work)) return DISCOEB_ECUDA;
-    return (int64_t)los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work).total;
+    return (int64_t)los_layout(n_modes, n_tau, ellmax, n_fftlog, n_k_dense, work, los_contraction()).total;
+}
+
+int32_t discoeb_set_los_contraction(int32_t kind, int32_t slices)
+{
+    if (kind != DISCOEB_LOS_FP64 && kind != DISCOEB_LOS_INT8) return DISCOEB_EINVAL;
+    if (kind == DISCOEB_LOS_INT8 && (slices < 1 || slices > dgemm_i8::kMaxSlices)) return DISCOEB_EINVAL;
+    g_los_slices.store(kind == DISCOEB_LOS_INT8 ? slices : g_los_slices.load());
+    g_los_kind.store(kind);
+    return DISCOEB_SUCCESS;
+}
+
+int32_t discoeb_get_los_contraction(int32_t* kind, int32_t* slices)
+{
+    if (!kind || !slices) return DISCOEB_EINVAL;
+    *kind = g_los_kind.load();
+    *slices = g_los_slices.load();
+    return DISCOEB_SUCCESS;
 }
 
 int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const double* tau, const double* S,

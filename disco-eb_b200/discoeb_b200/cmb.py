@@ -209,6 +209,54 @@ def compute_theta_ell(ellmax, kmodes, tau, S, tau0, n_fftlog=16384, n_k_dense=0,
     return theta, k_out
 
 
+LOS_CONTRACTIONS = {"fp64": 0, "int8": 1}
+
+
+def set_los_contraction(kind="int8", slices=7):
+    """Choose how the line of sight contracts its frequency sum (library-wide): ``"int8"`` (the
+    default) on the int8 tensor cores with `slices` digit planes per operand (``dgemm_i8``; 7 give
+    ~1e-13 of each row's largest |theta_l(k)|, 8 ~1e-14), or ``"fp64"``, a cuBLAS DGEMM."""
+    if kind not in LOS_CONTRACTIONS:
+        raise ValueError(f"kind must be one of {sorted(LOS_CONTRACTIONS)}, not {kind!r}")
+    rc = _abi.lib().discoeb_set_los_contraction(LOS_CONTRACTIONS[kind], int(slices))
+    if rc != 0:
+        raise ValueError(f"invalid line-of-sight contraction ({kind!r}, slices={slices})")
+
+
+def get_los_contraction():
+    """(kind, slices) of the current line-of-sight contraction."""
+    k, s = ctypes.c_int32(), ctypes.c_int32()
+    _abi.lib().discoeb_get_los_contraction(ctypes.byref(k), ctypes.byref(s))
+    return {v: n for n, v in LOS_CONTRACTIONS.items()}[k.value], s.value
+
+
+def dgemm_i8(A, B, slices=7, split=0, device=None):
+    """C = A B^T in FP64 on the int8 tensor cores (``discoeb_dgemm_i8``: `slices` digit planes per
+    row of each operand, the digit products summed exactly in int32).  A [m, k], B [n, k]: numpy
+    arrays or torch tensors; returns a torch float64 tensor [m, n] on the device."""
+    torch, device = _device(device)
+    lib = _abi.lib()
+    f64 = dict(dtype=torch.float64, device=device)
+    dA = (A if isinstance(A, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(A, dtype=np.float64)))
+    dB = (B if isinstance(B, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(B, dtype=np.float64)))
+    dA, dB = dA.to(**f64).contiguous(), dB.to(**f64).contiguous()
+    if dA.dim() != 2 or dB.dim() != 2 or dA.shape[1] != dB.shape[1]:
+        raise ValueError("A [m, k] and B [n, k] must share k")
+    m, k = dA.shape
+    n = dB.shape[0]
+    nb = lib.discoeb_dgemm_i8_workspace_bytes(m, n, k, int(slices), int(split))
+    if nb < 0:
+        raise ValueError(f"invalid sizes or slice count for dgemm_i8 (code {nb})")
+    ws = torch.empty(int(nb) // 8 + 32, **f64)
+    aligned = (ws.data_ptr() + 255) // 256 * 256
+    C = torch.empty((m, n), **f64)
+    rc = lib.discoeb_dgemm_i8(m, n, k, dA.data_ptr(), k, dB.data_ptr(), k, C.data_ptr(), n, int(slices), int(split),
+                              aligned, int(nb), torch.cuda.current_stream(device).cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"dgemm_i8 failed with code {rc}")
+    return C
+
+
 def compute_Cell(theta_ell, kmodes, n_s, k_p, device=None, theta_ell_b=None):
     """C_l = int d ln k (k/k_p)^(n_s-1) Theta_l^2, trapezoid (cmb.py:838-873); device tensor.
     ``theta_ell_b``: the cross spectrum int d ln k (k/k_p)^(n_s-1) Theta_l Theta^b_l (C_l^TE from

@@ -362,6 +362,33 @@ int32_t discoeb_los(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
                     double tau0, int32_t ellmax, int32_t n_fftlog, int32_t n_k_dense, void* workspace,
                     int64_t workspace_bytes, double* theta, double* kmodes_out, void* stream);
 
+/* How discoeb_los, discoeb_los_e and discoeb_los_cell_jvp contract the frequency sum
+ * theta[k, l] = sum_q c_q(k) M_l(p_q) (cmb.py:809-834, two real einsums there):
+ * DISCOEB_LOS_INT8 (default, slices 7): discoeb_dgemm_i8 below, about 1e-13 of each row's largest
+ * |theta_l(k)| from the FP64 sum; DISCOEB_LOS_FP64: a cuBLAS DGEMM.  A library-wide setting, read
+ * once by each call (and by the *_workspace_bytes queries, whose result depends on it). */
+#define DISCOEB_LOS_FP64 0
+#define DISCOEB_LOS_INT8 1
+int32_t discoeb_set_los_contraction(int32_t kind, int32_t slices);
+int32_t discoeb_get_los_contraction(int32_t* kind, int32_t* slices);
+
+/* FP64 product C = A B^T on the int8 tensor cores (tcgen05.mma kind::i8): the line of sight's
+ * frequency sum (cmb.py:809-834, two real einsums there) without an FP64 GEMM.  Each row of A and
+ * of B is split over one power-of-two scale into `slices` (1..8) signed 8-bit digit planes
+ * (d_0 in [-127, 127], then 7 bits each); the digit products of equal total weight accumulate
+ * exactly in int32 and the slices levels are summed in FP64.  Error per element about
+ * 2^(1 - 7 slices) (max_k |A_ik| sum_k |B_jk| + sum_k |A_ik| max_k |B_jk|) on top of FP64
+ * rounding; a row holding a non-finite value gives NaN products.
+ *   A [m, lda >= k], B [n, ldb >= k], C [m, ldc >= n]: row-major device arrays.
+ *   split: K ranges per output tile (<= 0: chosen from the SM count).
+ *   workspace: >= discoeb_dgemm_i8_workspace_bytes(m, n, k, slices, split) bytes, 256-byte
+ *   aligned (digit planes, scales, partial products).  A kernel whose bounded waits run out
+ *   (never in a correct launch) writes NaN into C. */
+int64_t discoeb_dgemm_i8_workspace_bytes(int32_t m, int32_t n, int32_t k, int32_t slices, int32_t split);
+int32_t discoeb_dgemm_i8(int32_t m, int32_t n, int32_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
+                         double* C, int64_t ldc, int32_t slices, int32_t split, void* workspace,
+                         int64_t workspace_bytes, void* stream);
+
 /* C_l = trapezoid over ln k of (k/k_p)^(n_s-1) Theta_l(k)^2: replaces compute_Cell
  * (cmb.py:838-873).  theta [n_modes, n_ell], cell [n_ell], device. */
 int32_t discoeb_cell(int32_t n_modes, const double* kmodes, int32_t n_ell, const double* theta, double n_s,

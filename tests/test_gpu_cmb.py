@@ -37,6 +37,17 @@ def gpu_states(torch_cuda):
     return bg, a, tau, ks, y
 
 
+@pytest.fixture(params=["int8", "fp64"])
+def contraction(request, torch_cuda):
+    """the line of sight's frequency sum on the int8 tensor cores (default, 7 digit planes) or as an
+    FP64 DGEMM; restored to the default afterwards"""
+    from discoeb_b200.cmb import get_los_contraction, set_los_contraction
+    before = get_los_contraction()
+    set_los_contraction(request.param, 7)
+    yield request.param
+    set_los_contraction(*before)
+
+
 def _close(got, want, rel):
     """Per mode (row), within rel of the row's largest magnitude."""
     scale = np.abs(want).max(axis=-1, keepdims=True) + 1e-300
@@ -64,7 +75,7 @@ def test_gpu_sources_match_oracle(gpu_states):
 
 
 @pytest.mark.parametrize("n_k_dense", [0, 200])
-def test_gpu_theta_ell_and_cell_match_oracle(gpu_states, n_k_dense):
+def test_gpu_theta_ell_and_cell_match_oracle(gpu_states, n_k_dense, contraction):
     from discoeb_b200.cmb import compute_Cell, compute_sources, compute_theta_ell
     bg, a, tau, ks, y = gpu_states
     S = compute_sources(param=bg, yout=y, kmodes=ks, aexp_out=a, **L11)["S"]
@@ -78,7 +89,7 @@ def test_gpu_theta_ell_and_cell_match_oracle(gpu_states, n_k_dense):
 
 
 @pytest.mark.parametrize("n_k_dense", [0, 200])
-def test_gpu_e_mode_theta_ell_and_cross_cell_match_oracle(gpu_states, n_k_dense):
+def test_gpu_e_mode_theta_ell_and_cross_cell_match_oracle(gpu_states, n_k_dense, contraction):
     from discoeb_b200.cmb import compute_Cell, compute_sources, compute_theta_ell
     bg, a, tau, ks, y = gpu_states
     src = compute_sources(param=bg, yout=y, kmodes=ks, aexp_out=a, **L11)
@@ -90,7 +101,8 @@ def test_gpu_e_mode_theta_ell_and_cross_cell_match_oracle(gpu_states, n_k_dense)
     np.testing.assert_allclose(kk2.cpu().numpy(), kk_o, rtol=1e-14)
     # 1e-9 of each mode's largest multipole, plus the rounding scale of the FFTLog sums: at high k
     # the recurrence's three terms cancel by ~(k chi)^2 near l = 8, where eps times the sum of
-    # magnitudes reaches ~5e-9 of the row's largest value on the dense k grid
+    # magnitudes reaches ~5e-9 of the row's largest value on the dense k grid (the int8 contraction
+    # with 7 digit planes uses 0.35 of this bound there, the FP64 one 0.20)
     got = the.cpu().numpy()
     bound = 1e-9 * np.abs(the_o).max(axis=-1, keepdims=True) + 32 * np.finfo(float).eps * mag
     assert np.all(np.abs(got - the_o) <= bound), float((np.abs(got - the_o) / bound).max())
