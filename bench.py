@@ -481,6 +481,80 @@ def run_cmb(args, rank, world, local):
         }), flush=True)
 
 
+def run_los_gemm(args, rank, world, local):
+    """The line of sight's frequency sum alone: theta = A B^T with A [m, k] the FFTLog coefficient
+    rows, B [n, k] the M_l(p) table (default sizes: 8192 dense modes, l <= 2500, 16384 FFTLog points,
+    so k = 2 x 8193 interleaved (re, im) pairs), synthetic operands with the same decay over the
+    frequencies.  Times discoeb_dgemm_i8 (the whole call: splitting, tensor-core product,
+    reduction), the cuBLAS DGEMM it replaces, and cuBLASLt's int8 GEMM (torch._int_mm) as the
+    measured int8 tensor rate of this GPU."""
+    import torch
+
+    from discoeb_b200 import _abi
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    lib = _abi.lib()
+    m, n, k, sl = args.gemm_m, args.gemm_n, args.gemm_k, args.slices
+    g = torch.Generator(device=device)
+    g.manual_seed(1234)
+    q = torch.arange(k, device=device, dtype=torch.float64)
+    A = torch.randn(m, k, dtype=torch.float64, device=device, generator=g) * torch.exp(-q / 3000.0)
+    B = torch.randn(n, k, dtype=torch.float64, device=device, generator=g) * (1.0 + q) ** -0.8
+    C = torch.empty(m, n, dtype=torch.float64, device=device)
+    nb = lib.discoeb_dgemm_i8_workspace_bytes(m, n, k, sl, 0)
+    ws = torch.empty(nb // 8 + 32, dtype=torch.float64, device=device)
+    al = (ws.data_ptr() + 255) // 256 * 256
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)  # 256 MB > L2
+
+    def timed(fn):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    i8 = lambda: lib.discoeb_dgemm_i8(m, n, k, A.data_ptr(), k, B.data_ptr(), k, C.data_ptr(), n, sl, 0, al, nb,  # noqa
+                                      stream.cuda_stream)
+    f64 = lambda: torch.mm(A, B.T)  # noqa: E731
+    ai = torch.randint(-127, 128, (8192, 16384), dtype=torch.int8, device=device)
+    bi = torch.randint(-127, 128, (16384, 8192), dtype=torch.int8, device=device)
+    imm = lambda: torch._int_mm(ai, bi)  # noqa: E731
+    for _ in range(args.warmup):
+        i8(), f64(), imm()
+    with ClockSampler(local) as clk:
+        t8 = [timed(i8) for _ in range(args.steps)]
+    t64 = [timed(f64) for _ in range(args.steps)]
+    tim = [timed(imm) for _ in range(args.steps)]
+    ref = torch.mm(A, B.T)
+    i8()
+    torch.cuda.synchronize()
+    rowmax = ref.abs().max(dim=1).values
+    err = float(((C - ref).abs().max(dim=1).values / rowmax).max())
+    # what the tensor cores execute: slices (slices + 1) / 2 digit-plane products over the padded tiles
+    pad = lambda x, t: (x + t - 1) // t * t  # noqa: E731
+    ops = 2.0 * sl * (sl + 1) / 2 * pad(m, 256) * pad(n, 256) * pad(k, 128)
+    peak = 2.0 * 8192 * 16384 * 8192 / (min(tim) * 1e-3) / 1e12
+    ms = statistics.mean(t8)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "line-of-sight frequency sum theta = A B^T (FP64 result)", "value": 1e3 / ms,
+            "unit": "contractions/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f64 result from int8 digit planes", "data": "synthetic",
+            "config": {"workload": f"los_contraction_m{m}_n{n}_k{k}", "slices": sl, "l2": "flushed (256 MB write)"},
+            "dgemm_i8_ms": ms, "cublas_dgemm_ms": statistics.mean(t64), "speedup_vs_dgemm": statistics.mean(t64) / ms,
+            "max_err_over_rowmax": err,
+            "roofline": {"bound": "tensor", "achieved": ops / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TOPS (int8)",
+                         "frac": ops / (ms * 1e-3) / 1e12 / peak,
+                         "peak_source": "cuBLASLt int8 GEMM 8192 x 16384 x 8192 (torch._int_mm), best of the run",
+                         "achieved_source": "whole dgemm_i8 call (splitting and reduction included)"},
+            "clocks": clk.summary(),
+        }), flush=True)
+
+
 def run_cmb_grad(args, rank, world, local):
     """C_l^TT and dC_l/dtheta (8 parameters) of one cosmology through cmb.compute_Cell_jacobian:
     background with six forward-mode tangents, one discoeb_jvp_full launch (states and their
@@ -551,7 +625,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pk_lcdm_mnu_k512_z4")
-    ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward", "cmb", "cmb-grad", "batch"])
+    ap.add_argument("--mode", default="fwd+grad", choices=["fwd+grad", "forward", "cmb", "cmb-grad", "batch",
+                                                          "los-gemm"])
+    ap.add_argument("--gemm-m", type=int, default=8192, help="--mode los-gemm: rows of A (dense modes)")
+    ap.add_argument("--gemm-n", type=int, default=2501, help="--mode los-gemm: rows of B (multipoles)")
+    ap.add_argument("--gemm-k", type=int, default=16386, help="--mode los-gemm: contraction length")
+    ap.add_argument("--slices", type=int, default=7, help="--mode los-gemm: digit planes per operand")
     ap.add_argument("--cmb-large", action="store_true", help="cmb-grad: l_max 50, 2000 modes, 2000 source times")
     ap.add_argument("--n-cosmo", type=int, default=64, help="cosmologies per launch in --mode batch")
     ap.add_argument("--grad", action="store_true", help="--mode batch: forward + gradient (discoeb_jvp)")
@@ -580,6 +659,9 @@ def main():
         return
     if args.mode == "cmb-grad":
         run_cmb_grad(args, rank, world, local)
+        return
+    if args.mode == "los-gemm":
+        run_los_gemm(args, rank, world, local)
         return
     if args.mode == "batch":
         run_batch(args, rank, world, local)
