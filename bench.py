@@ -386,6 +386,7 @@ def run_cmb(args, rank, world, local):
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
+    cmb.set_los_contraction(args.los_contraction, 7)
     p = {"Omegam": 0.3099, "Omegab": 0.0488911, "H0": 67.742, "n_s": 0.96822, "A_s": 2.1064e-09, "mnu": 0.06,
          "Tcmb": 2.7255, "YHe": 0.248, "Neff": 2.046, "Nmnu": 1, "w_DE_0": -0.99, "w_DE_a": 0.0, "cs2_DE": 1.0,
          "Omegak": 0.0, "k_p": 0.05}
@@ -517,8 +518,8 @@ def run_los_gemm(args, rank, world, local):
         e1.synchronize()
         return e0.elapsed_time(e1)
 
-    i8 = lambda: lib.discoeb_dgemm_i8(m, n, k, A.data_ptr(), k, B.data_ptr(), k, C.data_ptr(), n, sl, 0, al, nb,  # noqa
-                                      stream.cuda_stream)
+    i8 = lambda: lib.discoeb_dgemm_i8(m, n, k, A.data_ptr(), k, 0, B.data_ptr(), k, 0, C.data_ptr(), n, sl, 0, al,  # noqa
+                                      nb, stream.cuda_stream)
     f64 = lambda: torch.mm(A, B.T)  # noqa: E731
     ai = torch.randint(-127, 128, (8192, 16384), dtype=torch.int8, device=device)
     bi = torch.randint(-127, 128, (16384, 8192), dtype=torch.int8, device=device)
@@ -569,6 +570,7 @@ def run_cmb_grad(args, rank, world, local):
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
+    cmb.set_los_contraction(args.los_contraction, 7)
     h = 0.67742
     theta = {"omega_c": (0.3099 - 0.0488911) * h * h, "omega_b": 0.0488911 * h * h, "h": h, "n_s": 0.96822,
              "ln10As": math.log(2.1064e-9 * 1e10), "w0": -0.99, "wa": 0.0, "m_nu": 0.06}
@@ -610,6 +612,7 @@ def run_cmb_grad(args, rank, world, local):
             "unit": "spectra+gradients/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "dtype": "f64", "data": "synthetic (DISCO-Notebook cosmology)",
             "config": {"workload": name, "gradient_of": "C_l w.r.t. omega_c, omega_b, h, n_s, ln10As, w0, wa, m_nu",
+                       "los_contraction": args.los_contraction,
                        **{k: (v if not isinstance(v, np.ndarray) else int(v.shape[0])) for k, v in opts.items()}},
             "e2e": {"value": 1e3 / ms, "unit": "spectra+gradients/s", "ms_per_cosmology": ms},
             "forward_only_ms": 1e3 * statistics.mean(tf),
@@ -631,6 +634,9 @@ def main():
     ap.add_argument("--gemm-n", type=int, default=2501, help="--mode los-gemm: rows of B (multipoles)")
     ap.add_argument("--gemm-k", type=int, default=16386, help="--mode los-gemm: contraction length")
     ap.add_argument("--slices", type=int, default=7, help="--mode los-gemm: digit planes per operand")
+    ap.add_argument("--los-contraction", default="int8", choices=["int8", "fp64"],
+                    help="--mode cmb / cmb-grad: the line of sight's frequency sum on the int8 tensor cores "
+                         "(7 digit planes) or as an FP64 DGEMM")
     ap.add_argument("--cmb-large", action="store_true", help="cmb-grad: l_max 50, 2000 modes, 2000 source times")
     ap.add_argument("--n-cosmo", type=int, default=64, help="cosmologies per launch in --mode batch")
     ap.add_argument("--grad", action="store_true", help="--mode batch: forward + gradient (discoeb_jvp)")

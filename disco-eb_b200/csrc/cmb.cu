@@ -1025,8 +1025,8 @@ int32_t los_forward(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
     // 5. theta[r, l] = sum_j A[r, j] B[l, j] over the interleaved (re, im) pairs: one product,
     //    on the int8 tensor cores (digit planes, exact int32 sums) or as a cuBLAS DGEMM
     if (L.con.kind == DISCOEB_LOS_INT8)
-        return dgemm_i8::run(rows, ellmax + 1, (int)L.pitch, D(L.fft), L.pitch, D(L.B), L.pitch, theta, ellmax + 1,
-                             L.con.slices, 0, ws + L.i8, (int64_t)(L.total - L.i8), stream);
+        return dgemm_i8::run(rows, ellmax + 1, (int)L.pitch, D(L.fft), L.pitch, false, D(L.B), L.pitch, false, theta,
+                             ellmax + 1, L.con.slices, 0, ws + L.i8, (int64_t)(L.total - L.i8), stream);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
     std::lock_guard<std::mutex> lock(g_blas_mu);
@@ -1047,7 +1047,7 @@ int32_t los_forward(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
 // workspace of discoeb_los_cell_jvp: the line of sight's own (los_layout) followed by these
 struct LosJvpLayout {
     LosLayout base;
-    size_t th, G, H, Bd, Fd, w, kout, kscratch, sdd, s2kd, cpkd, lchid, fxd, fbd, gd, S2v, S2d, cpv, cpd, total;
+    size_t th, G, H, Bd, Fd, w, kout, kscratch, sdd, s2kd, cpkd, lchid, fxd, fbd, gd, S2v, S2d, cpv, cpd, i8t, total;
 };
 
 LosJvpLayout los_jvp_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n_dense, size_t cufft_bytes)
@@ -1076,6 +1076,11 @@ LosJvpLayout los_jvp_layout(int n_modes, int n_tau, int ellmax, int n_fft, int n
     J.S2d = take(rows * n_tau);
     J.cpv = take(rows * n_tau);
     J.cpd = take(rows * n_tau);
+    // the int8 form of Omega^T A ([L, pitch] over the modes): its own digit planes and level sums
+    const int64_t i8t = J.base.con.kind == DISCOEB_LOS_INT8
+                            ? dgemm_i8::workspace_bytes((int)L, (int)pitch, (int)rows, J.base.con.slices, 0)
+                            : 0;
+    J.i8t = take(i8t > 0 ? (size_t)i8t / sizeof(double) + 1 : 0);
     J.total = o;
     return J;
 }
@@ -1317,6 +1322,9 @@ int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_ta
     if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
     const double one = 1.0, zero = 0.0;
     auto omega_t_times = [&](const double* A, double* out) {  // out [n_ell, pitch] = Omega^T A
+        if (L.con.kind == DISCOEB_LOS_INT8)  // both operands K-major over the modes
+            return dgemm_i8::run(n_ell, (int)pitch, rows, D(J.th), n_ell, true, A, pitch, true, out, pitch,
+                                 L.con.slices, 0, ws + J.i8t, (int64_t)(J.total - J.i8t), stream) == DISCOEB_SUCCESS;
         std::lock_guard<std::mutex> lock(g_blas_mu);
         cublasHandle_t h = blas_handle(dev);
         if (!h) return false;

@@ -244,13 +244,46 @@ __global__ void row_scale_kernel(int rows, int k, const double* __restrict__ X, 
     }
 }
 
+// The same for a transposed operand (element (r, j) at X[j * ld + r]): a block per 32 rows, lane =
+// row, the 8 warps striding over K, so every load instruction reads 32 consecutive doubles
+__global__ void row_scale_t_kernel(int rows, int rows_pad, int k, const double* __restrict__ X, long long ld,
+                                   int* __restrict__ e, double* __restrict__ scale)
+{
+    __shared__ double red[8][32];
+    __shared__ int bad[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int r = blockIdx.x * 32 + lane;
+    double mx = 0.0;
+    int nonfinite = 0;
+    if (r < rows)
+        for (int j = w; j < k; j += 8) {
+            const double a = fabs(X[(size_t)j * ld + r]);
+            nonfinite |= !isfinite(a);
+            mx = fmax(mx, a);
+        }
+    red[w][lane] = mx;
+    bad[w][lane] = nonfinite;
+    __syncthreads();
+    if (w == 0 && r < rows_pad) {
+        for (int i = 1; i < 8; ++i) {
+            mx = fmax(mx, red[i][lane]);
+            nonfinite |= bad[i][lane];
+        }
+        int ex = 0;
+        if (!nonfinite && mx > 0.0) frexp(mx * (128.0 / 127.0) * (1.0 + 0x1p-40), &ex);
+        e[r] = nonfinite ? 0 : ex;
+        scale[r] = nonfinite ? __longlong_as_double(0x7ff8000000000000ll) : (mx > 0.0 ? ldexp(1.0, ex - 7) : 0.0);
+    }
+}
+
 // One thread per (padded row, 16 consecutive K elements): its `slices` digits, each plane's 16
 // bytes stored at the row's place in the 8 x 16-byte core matrix of its stage block.  Thread
 // order = (row within the core matrix, 16-byte chunk, 8-row group, stage, tile), so a warp writes
 // 512 contiguous bytes per plane.
-__global__ void slice_kernel(int rows, int k, const double* __restrict__ X, long long ld, const int* __restrict__ e,
-                             const double* __restrict__ scale, int kst, long long n_units, int slices, size_t plane,
-                             uint8_t* __restrict__ D)
+// (element (r, j) at X[r * ld + j], or at X[j * ld + r] for a transposed operand).
+__global__ void slice_kernel(int rows, int k, const double* __restrict__ X, long long ld, bool trans,
+                             const int* __restrict__ e, const double* __restrict__ scale, int kst, long long n_units,
+                             int slices, size_t plane, uint8_t* __restrict__ D)
 {
     const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n_units) return;
@@ -264,7 +297,9 @@ __global__ void slice_kernel(int rows, int k, const double* __restrict__ X, long
     const bool live = row < rows && isfinite(scale[row]) && scale[row] != 0.0;
     const int sh = 7 - (live ? e[row] : 0);
 #pragma unroll
-    for (int j = 0; j < 16; ++j) x[j] = (live && k0 + j < k) ? ldexp(X[(size_t)row * ld + k0 + j], sh) : 0.0;
+    for (int j = 0; j < 16; ++j)
+        x[j] = (live && k0 + j < k) ? ldexp(trans ? X[(size_t)(k0 + j) * ld + row] : X[(size_t)row * ld + k0 + j], sh)
+                                    : 0.0;
     uint8_t* dst = D + ((size_t)rb * kst + kc) * TILE + g * 1024 + c * 128 + rr * 16;
     for (int s = 0; s < slices; ++s) {
         uint32_t w[4] = {0u, 0u, 0u, 0u};
@@ -470,11 +505,12 @@ int64_t workspace_bytes(int m, int n, int k, int slices, int split)
     return (int64_t)g.total;
 }
 
-int32_t run(int m, int n, int k, const double* A, int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc,
-            int slices, int split, char* ws, int64_t ws_bytes, void* stream)
+int32_t run(int m, int n, int k, const double* A, int64_t lda, bool trans_a, const double* B, int64_t ldb,
+            bool trans_b, double* C, int64_t ldc, int slices, int split, char* ws, int64_t ws_bytes, void* stream)
 {
     Geo g;
-    if (!geometry(m, n, k, slices, split, g) || !A || !B || !C || !ws || lda < k || ldb < k || ldc < n)
+    if (!geometry(m, n, k, slices, split, g) || !A || !B || !C || !ws || lda < (trans_a ? m : k) ||
+        ldb < (trans_b ? n : k) || ldc < n)
         return DISCOEB_EINVAL;
     if (ws_bytes < (int64_t)g.total || (reinterpret_cast<uintptr_t>(ws) & 255u)) return DISCOEB_EINVAL;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -498,11 +534,19 @@ int32_t run(int m, int n, int k, const double* A, int64_t lda, const double* B, 
     uint8_t* db = reinterpret_cast<uint8_t*>(ws + g.db);
     int* levels = reinterpret_cast<int*>(ws + g.part);
     cudaMemsetAsync(err, 0, sizeof(int), s);
-    row_scale_kernel<<<g.mt * BM, 256, 0, s>>>(m, k, A, lda, ea, sa);
-    row_scale_kernel<<<g.nt * BN, 256, 0, s>>>(n, k, B, ldb, eb, sb);
+    if (trans_a)
+        row_scale_t_kernel<<<g.mt * BM / 32, 256, 0, s>>>(m, g.mt * BM, k, A, lda, ea, sa);
+    else
+        row_scale_kernel<<<g.mt * BM, 256, 0, s>>>(m, k, A, lda, ea, sa);
+    if (trans_b)
+        row_scale_t_kernel<<<g.nt * BN / 32, 256, 0, s>>>(n, g.nt * BN, k, B, ldb, eb, sb);
+    else
+        row_scale_kernel<<<g.nt * BN, 256, 0, s>>>(n, k, B, ldb, eb, sb);
     const long long ua = (long long)g.mt * BM * g.kst * (BKB / 16), ub = (long long)g.nt * BN * g.kst * (BKB / 16);
-    slice_kernel<<<(unsigned)((ua + 255) / 256), 256, 0, s>>>(m, k, A, lda, ea, sa, g.kst, ua, slices, g.a_plane, da);
-    slice_kernel<<<(unsigned)((ub + 255) / 256), 256, 0, s>>>(n, k, B, ldb, eb, sb, g.kst, ub, slices, g.b_plane, db);
+    slice_kernel<<<(unsigned)((ua + 255) / 256), 256, 0, s>>>(m, k, A, lda, trans_a, ea, sa, g.kst, ua, slices,
+                                                              g.a_plane, da);
+    slice_kernel<<<(unsigned)((ub + 255) / 256), 256, 0, s>>>(n, k, B, ldb, trans_b, eb, sb, g.kst, ub, slices,
+                                                              g.b_plane, db);
     gemm_kernel<<<(unsigned)(g.mt * g.nt * g.split), THREADS, SMEM_BYTES, s>>>(
         g.mt, g.nt, g.kst, g.split, slices, g.a_plane, g.b_plane, da, db, levels, g.ldp, err);
     const long long mn = (long long)m * n;
@@ -520,12 +564,13 @@ int64_t discoeb_dgemm_i8_workspace_bytes(int32_t m, int32_t n, int32_t k, int32_
     return dgemm_i8::workspace_bytes(m, n, k, slices, split);
 }
 
-int32_t discoeb_dgemm_i8(int32_t m, int32_t n, int32_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
-                         double* C, int64_t ldc, int32_t slices, int32_t split, void* workspace,
-                         int64_t workspace_bytes, void* stream)
+int32_t discoeb_dgemm_i8(int32_t m, int32_t n, int32_t k, const double* A, int64_t lda, int32_t trans_a,
+                         const double* B, int64_t ldb, int32_t trans_b, double* C, int64_t ldc, int32_t slices,
+                         int32_t split, void* workspace, int64_t workspace_bytes, void* stream)
 {
-    return dgemm_i8::run(m, n, k, A, lda, B, ldb, C, ldc, slices, split, static_cast<char*>(workspace),
-                         workspace_bytes, stream);
+    if ((trans_a != 0 && trans_a != 1) || (trans_b != 0 && trans_b != 1)) return DISCOEB_EINVAL;
+    return dgemm_i8::run(m, n, k, A, lda, trans_a != 0, B, ldb, trans_b != 0, C, ldc, slices, split,
+                         static_cast<char*>(workspace), workspace_bytes, stream);
 }
 
 }  // extern "C"

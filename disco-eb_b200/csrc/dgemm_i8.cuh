@@ -19,11 +19,11 @@ constexpr int kMaxSlices = 8;
 // (split <= 0: chosen by the library); < 0 for invalid sizes.
 int64_t workspace_bytes(int m, int n, int k, int slices, int split);
 
-// C[i * ldc + j] = sum_k A[i * lda + k] B[j * ldb + k] (row-major, K contiguous, device
-// pointers).  Workspace: >= workspace_bytes(m, n, k, slices, split) bytes, 256-byte aligned.
-// Returns a DISCOEB_* status.  `err_flag`: optional device int set non-zero by a kernel whose
-// bounded waits ran out (never in a correct launch).
-int32_t run(int m, int n, int k, const double* A, int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc,
-            int slices, int split, char* ws, int64_t ws_bytes, void* stream);
+// C[i * ldc + j] = sum_k op(A)[i, k] op(B)[j, k] with op(A)[i, k] = A[i * lda + k], or A[k * lda + i]
+// when trans_a (A stored [k, m]), the same for B (device pointers).  Workspace:
+// >= workspace_bytes(m, n, k, slices, split) bytes, 256-byte aligned.  Returns a DISCOEB_* status;
+// a kernel whose bounded waits ran out (never in a correct launch) makes C NaN.
+int32_t run(int m, int n, int k, const double* A, int64_t lda, bool trans_a, const double* B, int64_t ldb,
+            bool trans_b, double* C, int64_t ldc, int slices, int split, char* ws, int64_t ws_bytes, void* stream);
 
 }  // namespace dgemm_i8

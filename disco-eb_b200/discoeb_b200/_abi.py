@@ -213,9 +213,9 @@ def lib():
         L.discoeb_get_los_contraction.restype = ctypes.c_int32
         L.discoeb_dgemm_i8_workspace_bytes.argtypes = [ctypes.c_int32] * 5
         L.discoeb_dgemm_i8_workspace_bytes.restype = ctypes.c_int64
-        L.discoeb_dgemm_i8.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int64, vp,
-                                       ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, vp,
-                                       ctypes.c_int64, vp]
+        L.discoeb_dgemm_i8.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int64,
+                                       ctypes.c_int32, vp, ctypes.c_int64, ctypes.c_int32, vp, ctypes.c_int64,
+                                       ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int64, vp]
         L.discoeb_dgemm_i8.restype = ctypes.c_int32
         L.discoeb_cell.argtypes = [ctypes.c_int32, vp, ctypes.c_int32, vp, ctypes.c_double, ctypes.c_double, vp, vp]
         L.discoeb_sources_jvp.argtypes = [vp, ctypes.POINTER(DiscoebCosmo), vp, ctypes.c_int32, ctypes.c_int32, vp,

@@ -230,28 +230,32 @@ def get_los_contraction():
     return {v: n for n, v in LOS_CONTRACTIONS.items()}[k.value], s.value
 
 
-def dgemm_i8(A, B, slices=7, split=0, device=None):
-    """C = A B^T in FP64 on the int8 tensor cores (``discoeb_dgemm_i8``: `slices` digit planes per
-    row of each operand, the digit products summed exactly in int32).  A [m, k], B [n, k]: numpy
-    arrays or torch tensors; returns a torch float64 tensor [m, n] on the device."""
+def dgemm_i8(A, B, slices=7, split=0, device=None, trans_a=False, trans_b=False):
+    """C = op(A) op(B)^T in FP64 on the int8 tensor cores (``discoeb_dgemm_i8``: `slices` digit
+    planes per row of each operand, the digit products summed exactly in int32).  op(A) = A [m, k],
+    or A^T when ``trans_a`` (A [k, m]); op(B) = B [n, k], or B^T when ``trans_b``.  numpy arrays or
+    torch tensors; returns a torch float64 tensor [m, n] on the device."""
     torch, device = _device(device)
     lib = _abi.lib()
     f64 = dict(dtype=torch.float64, device=device)
     dA = (A if isinstance(A, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(A, dtype=np.float64)))
     dB = (B if isinstance(B, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(B, dtype=np.float64)))
     dA, dB = dA.to(**f64).contiguous(), dB.to(**f64).contiguous()
-    if dA.dim() != 2 or dB.dim() != 2 or dA.shape[1] != dB.shape[1]:
-        raise ValueError("A [m, k] and B [n, k] must share k")
-    m, k = dA.shape
-    n = dB.shape[0]
+    if dA.dim() != 2 or dB.dim() != 2:
+        raise ValueError("A and B must be matrices")
+    (k, m) = dA.shape if trans_a else dA.shape[::-1]
+    (kb, n) = dB.shape if trans_b else dB.shape[::-1]
+    if k != kb:
+        raise ValueError("op(A) [m, k] and op(B) [n, k] must share k")
     nb = lib.discoeb_dgemm_i8_workspace_bytes(m, n, k, int(slices), int(split))
     if nb < 0:
         raise ValueError(f"invalid sizes or slice count for dgemm_i8 (code {nb})")
     ws = torch.empty(int(nb) // 8 + 32, **f64)
     aligned = (ws.data_ptr() + 255) // 256 * 256
     C = torch.empty((m, n), **f64)
-    rc = lib.discoeb_dgemm_i8(m, n, k, dA.data_ptr(), k, dB.data_ptr(), k, C.data_ptr(), n, int(slices), int(split),
-                              aligned, int(nb), torch.cuda.current_stream(device).cuda_stream)
+    rc = lib.discoeb_dgemm_i8(m, n, k, dA.data_ptr(), dA.shape[1], int(trans_a), dB.data_ptr(), dB.shape[1],
+                              int(trans_b), C.data_ptr(), n, int(slices), int(split), aligned, int(nb),
+                              torch.cuda.current_stream(device).cuda_stream)
     if rc != 0:
         raise RuntimeError(f"dgemm_i8 failed with code {rc}")
     return C

@@ -379,15 +379,16 @@ int32_t discoeb_get_los_contraction(int32_t* kind, int32_t* slices);
  * exactly in int32 and the slices levels are summed in FP64.  Error per element about
  * 2^(1 - 7 slices) (max_k |A_ik| sum_k |B_jk| + sum_k |A_ik| max_k |B_jk|) on top of FP64
  * rounding; a row holding a non-finite value gives NaN products.
- *   A [m, lda >= k], B [n, ldb >= k], C [m, ldc >= n]: row-major device arrays.
- *   split: K ranges per output tile (<= 0: chosen from the SM count).
+ *   C [m, ldc >= n] row-major; op(A)[i, q] = A[i * lda + q] (trans_a = 0, A [m, lda >= k]) or
+ *   A[q * lda + i] (trans_a = 1, A [k, lda >= m]); B likewise with n: C = op(A) op(B)^T.
+ *   Device arrays.  split: K ranges per output tile (<= 0: chosen from the SM count).
  *   workspace: >= discoeb_dgemm_i8_workspace_bytes(m, n, k, slices, split) bytes, 256-byte
- *   aligned (digit planes, scales, partial products).  A kernel whose bounded waits run out
- *   (never in a correct launch) writes NaN into C. */
+ *   aligned (digit planes, scales, level sums).  A kernel whose bounded waits run out (never in a
+ *   correct launch) writes NaN into C. */
 int64_t discoeb_dgemm_i8_workspace_bytes(int32_t m, int32_t n, int32_t k, int32_t slices, int32_t split);
-int32_t discoeb_dgemm_i8(int32_t m, int32_t n, int32_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
-                         double* C, int64_t ldc, int32_t slices, int32_t split, void* workspace,
-                         int64_t workspace_bytes, void* stream);
+int32_t discoeb_dgemm_i8(int32_t m, int32_t n, int32_t k, const double* A, int64_t lda, int32_t trans_a,
+                         const double* B, int64_t ldb, int32_t trans_b, double* C, int64_t ldc, int32_t slices,
+                         int32_t split, void* workspace, int64_t workspace_bytes, void* stream);
 
 /* C_l = trapezoid over ln k of (k/k_p)^(n_s-1) Theta_l(k)^2: replaces compute_Cell
  * (cmb.py:838-873).  theta [n_modes, n_ell], cell [n_ell], device. */

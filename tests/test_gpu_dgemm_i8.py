@@ -95,4 +95,19 @@ def test_gpu_dgemm_i8_arguments(torch_cuda):
     assert lib.discoeb_dgemm_i8_workspace_bytes(4, 4, 4, 7, 0) > 0
     # a workspace one byte short is rejected before any launch
     nb = lib.discoeb_dgemm_i8_workspace_bytes(4, 4, 4, 7, 1)
-    assert lib.discoeb_dgemm_i8(4, 4, 4, 0, 4, 0, 4, 0, 4, 7, 1, 256, nb, None) != 0
+    assert lib.discoeb_dgemm_i8(4, 4, 4, 0, 4, 0, 0, 4, 0, 0, 4, 7, 1, 256, nb, None) != 0
+    assert lib.discoeb_dgemm_i8(4, 4, 4, 0, 4, 2, 0, 4, 0, 0, 4, 7, 1, 256, nb, None) != 0
+
+
+@pytest.mark.parametrize("trans_a,trans_b", [(True, False), (False, True), (True, True)])
+def test_gpu_dgemm_i8_transposed_operands(torch_cuda, trans_a, trans_b):
+    """operands stored K-major over their other index (the forward-mode line of sight contracts
+    over the modes: G = Omega^T A)"""
+    from discoeb_b200.cmb import dgemm_i8
+    rng = np.random.default_rng(11)
+    m, n, k = 300, 520, 777
+    A = rng.standard_normal((m, k)) * np.exp(rng.uniform(-5, 5, m))[:, None]
+    B = rng.standard_normal((n, k)) * np.exp(rng.uniform(-5, 5, n))[:, None]
+    C = dgemm_i8(A.T.copy() if trans_a else A, B.T.copy() if trans_b else B, slices=7, trans_a=trans_a,
+                 trans_b=trans_b).cpu().numpy()
+    assert np.all(np.abs(C - A @ B.T) <= _bound(A, B, 7))
