@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -436,14 +437,16 @@ __global__ void chi_eval_kernel(int n_rows, int n_tau, const double* __restrict_
                                 const double* __restrict__ fx, const double* __restrict__ fbias, long long pitch,
                                 double* F)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)n_rows * n_fft) return;
-    const int r = (int)(t / n_fft), m = (int)(t - (long long)r * n_fft);
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_fft) return;
     const int i = fidx[m];
-    const size_t base = (size_t)r * n_tau + (n_tau - 1);
-    const double y0 = Srow[base - i], y1 = Srow[base - i - 1];
-    const double s0 = S2c[base - i], s1 = S2c[base - i - 1];
-    F[(size_t)r * pitch + m] = spline_value(lchi[i], lchi[i + 1], y0, y1, s0, s1, fx[m]) * fbias[m];
+    const double x = fx[m], fb = fbias[m], l0 = lchi[i], l1 = lchi[i + 1];
+    for (int r = blockIdx.y; r < n_rows; r += gridDim.y) {
+        const size_t base = (size_t)r * n_tau + (n_tau - 1);
+        const double y0 = Srow[base - i], y1 = Srow[base - i - 1];
+        const double s0 = S2c[base - i], s1 = S2c[base - i - 1];
+        F[(size_t)r * pitch + m] = spline_value(l0, l1, y0, y1, s0, s1, x) * fb;
+    }
 }
 
 // c_n k^-(p_n+1) with the rfft normalisation and the interval phase, times the weight of the
@@ -451,30 +454,64 @@ __global__ void chi_eval_kernel(int n_rows, int n_tau, const double* __restrict_
 __global__ void ck_kernel(int n_rows, const double* __restrict__ krow, int n_fft, int n_freq,
                           const double* __restrict__ g, long long pitch, double* F)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)n_rows * n_freq) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_freq) return;
     const double lo = g[0], dl = g[1];
-    const int r = (int)(t / n_freq), q = (int)(t - (long long)r * n_freq);
     const double eta = 2.0 * M_PI * q / (n_fft * dl);
-    const double lk = log(krow[r]);
-    double w = 2.0;
-    if (q == 0 || ((n_fft % 2 == 0) && q == n_freq - 1)) w = 1.0;
-    const double mag = w * exp(-(kBias + 1.0) * lk) / n_fft;
-    double sn, cs;
-    sincos(-eta * (lo + lk), &sn, &cs);
-    double* c = F + (size_t)r * pitch + 2 * q;
-    const double re = c[0], im = c[1];
-    c[0] = mag * (re * cs - im * sn);
-    c[1] = mag * (re * sn + im * cs);
+    const double w = (q == 0 || ((n_fft % 2 == 0) && q == n_freq - 1)) ? 1.0 : 2.0;
+    for (int r = blockIdx.y; r < n_rows; r += gridDim.y) {
+        const double lk = log(krow[r]);
+        const double mag = w * exp(-(kBias + 1.0) * lk) / n_fft;
+        double sn, cs;
+        sincos(-eta * (lo + lk), &sn, &cs);
+        double* c = F + (size_t)r * pitch + 2 * q;
+        const double re = c[0], im = c[1];
+        c[0] = mag * (re * cs - im * sn);
+        c[1] = mag * (re * sn + im * cs);
+    }
 }
 
 // B[l, 2q] = Re M_l(p_q), B[l, 2q + 1] = -Im M_l(p_q) (cmb.py:636-677)
-__global__ void mcoef_kernel(int n_ell, int n_freq, int n_fft, const double* __restrict__ g, double* B)
+// One thread per (frequency, run of kMcoefRun multipoles of one parity): log-Gamma at the run's
+// first l, the recurrence in l + 2 after it (fftlog_mcoef_run).  Threads with consecutive
+// frequencies write consecutive 16-byte (re, im) pairs of a row.  gd / Bd (may be null): the
+// table's derivative along the spacing's derivative gd[1].
+constexpr int kMcoefRun = 16;
+
+__global__ void mcoef_kernel(int n_ell, int n_freq, int n_fft, const double* __restrict__ g,
+                             const double* __restrict__ gd, double* B, double* Bd)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)n_ell * n_freq) return;
-    const int l = (int)(t / n_freq), q = (int)(t - (long long)l * n_freq);
-    fftlog_mcoef(l, q, n_fft, kBias, g[1], 0.0, B + (size_t)l * (2 * (size_t)n_freq) + 2 * q, nullptr);
+    const long long runs = 2LL * ((n_ell + 2 * kMcoefRun - 1) / (2 * kMcoefRun));
+    if (t >= runs * n_freq) return;
+    const int q = (int)(t % n_freq);
+    const long long r = t / n_freq;
+    const int l0 = (int)(r & 1) + 2 * kMcoefRun * (int)(r >> 1);
+    if (l0 >= n_ell) return;
+    const int count = min(kMcoefRun, (n_ell - 1 - l0) / 2 + 1);
+    const size_t o = (size_t)l0 * (2 * (size_t)n_freq) + 2 * q;
+    const long long step = 4LL * n_freq;
+    double* Bo = B ? B + o : nullptr;
+    double* Bdo = Bd ? Bd + o : nullptr;
+    const double dl_dot = gd ? gd[1] : 0.0;
+    if (l0 < 2) {
+        // l = 0, 1: the log-Gamma of (1 + l + p)/2 takes its reflection branch, which overflows to
+        // M = 0 at large eta as the reference's does; evaluated directly, the run starts at l0 + 2
+        double b[2], bd[2];
+        fftlog_mcoef(l0, q, n_fft, kBias, g[1], dl_dot, b, Bdo ? bd : nullptr);
+        if (Bo) Bo[0] = b[0], Bo[1] = b[1];
+        if (Bdo) Bdo[0] = bd[0], Bdo[1] = bd[1];
+        if (count > 1)
+            fftlog_mcoef_run(l0 + 2, count - 1, q, n_fft, kBias, g[1], dl_dot, step, Bo ? Bo + step : nullptr,
+                             Bdo ? Bdo + step : nullptr);
+        return;
+    }
+    fftlog_mcoef_run(l0, count, q, n_fft, kBias, g[1], dl_dot, step, Bo, Bdo);
+}
+
+long long mcoef_threads(int n_ell, int n_freq)
+{
+    return 2LL * ((n_ell + 2 * kMcoefRun - 1) / (2 * kMcoefRun)) * n_freq;
 }
 
 // C_l = trapezoid over ln k of (k/k_p)^(n_s-1) Theta_l(k)^2, written as sum_i w_i Theta_il^2 with
@@ -682,17 +719,20 @@ __global__ void chi_eval_dot_kernel(int n_rows, int n_tau, const double* __restr
                                     const double* __restrict__ fbias, const double* __restrict__ fbias_dot,
                                     long long pitch, double* Fd)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)n_rows * n_fft) return;
-    const int r = (int)(t / n_fft), m = (int)(t - (long long)r * n_fft);
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_fft) return;
     const int i = fidx[m];
-    const size_t base = (size_t)r * n_tau + (n_tau - 1);
-    const Dual v = spline_value_dual(Dual(lchi[i], lchi_dot[i]), Dual(lchi[i + 1], lchi_dot[i + 1]),
-                                     Dual(Srow[base - i], Srow_dot[base - i]),
-                                     Dual(Srow[base - i - 1], Srow_dot[base - i - 1]), Dual(S2v[base - i], S2d[base - i]),
-                                     Dual(S2v[base - i - 1], S2d[base - i - 1]), Dual(fx[m], fx_dot[m])) *
-                   Dual(fbias[m], fbias_dot[m]);
-    Fd[(size_t)r * pitch + m] = v.d;
+    const Dual l0(lchi[i], lchi_dot[i]), l1(lchi[i + 1], lchi_dot[i + 1]), x(fx[m], fx_dot[m]);
+    const Dual fb(fbias[m], fbias_dot[m]);
+    for (int r = blockIdx.y; r < n_rows; r += gridDim.y) {
+        const size_t base = (size_t)r * n_tau + (n_tau - 1);
+        const Dual v = spline_value_dual(l0, l1, Dual(Srow[base - i], Srow_dot[base - i]),
+                                         Dual(Srow[base - i - 1], Srow_dot[base - i - 1]),
+                                         Dual(S2v[base - i], S2d[base - i]), Dual(S2v[base - i - 1], S2d[base - i - 1]),
+                                         x) *
+                       fb;
+        Fd[(size_t)r * pitch + m] = v.d;
+    }
 }
 
 // the derivative of ck_kernel's coefficients: c = mag e^{i ph} F with ph = -eta (lo + ln k) and
@@ -702,34 +742,23 @@ __global__ void ck_dot_kernel(int n_rows, const double* __restrict__ krow, int n
                               const double* __restrict__ g, const double* __restrict__ gd, long long pitch,
                               const double* __restrict__ C, double* Fd)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)n_rows * n_freq) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_freq) return;
     const double lo = g[0], dl = g[1];
-    const int r = (int)(t / n_freq), q = (int)(t - (long long)r * n_freq);
     const double eta = 2.0 * M_PI * q / (n_fft * dl);
     const double eta_dot = -eta * gd[1] / dl;
-    const double lk = log(krow[r]);
-    double w = 2.0;
-    if (q == 0 || ((n_fft % 2 == 0) && q == n_freq - 1)) w = 1.0;
-    const double mag = w * exp(-(kBias + 1.0) * lk) / n_fft;
-    double sn, cs;
-    sincos(-eta * (lo + lk), &sn, &cs);
-    const double ph_dot = -(eta_dot * (lo + lk) + eta * gd[0]);
-    const size_t o = (size_t)r * pitch + 2 * q;
-    const double re = Fd[o], im = Fd[o + 1];
-    Fd[o] = mag * (re * cs - im * sn) - ph_dot * C[o + 1];
-    Fd[o + 1] = mag * (re * sn + im * cs) + ph_dot * C[o];
-}
-
-// the derivative of mcoef_kernel's table along the spacing's derivative gd[1]
-__global__ void mcoef_dot_kernel(int n_ell, int n_freq, int n_fft, const double* __restrict__ g,
-                                 const double* __restrict__ gd, double* Bd)
-{
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)n_ell * n_freq) return;
-    const int l = (int)(t / n_freq), q = (int)(t - (long long)l * n_freq);
-    double b[2];
-    fftlog_mcoef(l, q, n_fft, kBias, g[1], gd[1], b, Bd + (size_t)l * (2 * (size_t)n_freq) + 2 * q);
+    const double w = (q == 0 || ((n_fft % 2 == 0) && q == n_freq - 1)) ? 1.0 : 2.0;
+    for (int r = blockIdx.y; r < n_rows; r += gridDim.y) {
+        const double lk = log(krow[r]);
+        const double mag = w * exp(-(kBias + 1.0) * lk) / n_fft;
+        double sn, cs;
+        sincos(-eta * (lo + lk), &sn, &cs);
+        const double ph_dot = -(eta_dot * (lo + lk) + eta * gd[0]);
+        const size_t o = (size_t)r * pitch + 2 * q;
+        const double re = Fd[o], im = Fd[o + 1];
+        Fd[o] = mag * (re * cs - im * sn) - ph_dot * C[o + 1];
+        Fd[o + 1] = mag * (re * sn + im * cs) + ph_dot * C[o];
+    }
 }
 
 __global__ void cell_weight_kernel(int n_modes, const double* __restrict__ kmodes, double n_s, double k_p, double* w)
@@ -936,6 +965,13 @@ cublasHandle_t blas_handle(int dev)
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+// grid of the row kernels: columns over x (coalesced), rows over y (each block strides over rows
+// when there are more than 65535)
+inline dim3 row_grid(int n_rows, int n_cols, int threads)
+{
+    return dim3(blocks_for(n_cols, threads), (unsigned)std::max(1, std::min(n_rows, 65535)));
+}
+
 // Scratch of discoeb_sources_noalloc, for callers that cannot allocate device memory: one
 // file-scope device array (8 MiB) that every GPU loading the library holds until exit, so the
 // call itself allocates nothing.  It holds the per-mode spline recurrence of the ISW term, which
@@ -1006,7 +1042,7 @@ int32_t los_forward(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
     fgrid_kernel<<<blocks_for(n_fftlog, T), T, 0, s>>>(n_tau, D(L.lchi), n_fftlog, D(L.geom),
                                                        reinterpret_cast<int*>(ws + L.fidx), D(L.fx), D(L.fbias));
     chi_spline_kernel<<<blocks_for(rows, 64), 64, 0, s>>>(rows, n_tau, D(L.lchi), Srow, D(L.s2c), D(L.cpc));
-    chi_eval_kernel<<<blocks_for((long long)rows * n_fftlog, T), T, 0, s>>>(
+    chi_eval_kernel<<<row_grid(rows, n_fftlog, T), T, 0, s>>>(
         rows, n_tau, D(L.lchi), Srow, D(L.s2c), n_fftlog, reinterpret_cast<const int*>(ws + L.fidx), D(L.fx),
         D(L.fbias), L.pitch, D(L.fft));
     // 3. rfft of every row, in place (the plan lock is held from the lookup to here, so no other
@@ -1017,10 +1053,10 @@ int32_t los_forward(int32_t n_modes, const double* kmodes, int32_t n_tau, const 
     fft_lock.unlock();
     if (fr != CUFFT_SUCCESS) return DISCOEB_ECUDA;
     // 4. ck in place, and the M table
-    ck_kernel<<<blocks_for((long long)rows * L.n_freq, T), T, 0, s>>>(rows, krow, n_fftlog, L.n_freq, D(L.geom),
+    ck_kernel<<<row_grid(rows, L.n_freq, T), T, 0, s>>>(rows, krow, n_fftlog, L.n_freq, D(L.geom),
                                                                       L.pitch, D(L.fft));
-    mcoef_kernel<<<blocks_for((long long)(ellmax + 1) * L.n_freq, T), T, 0, s>>>(ellmax + 1, L.n_freq, n_fftlog,
-                                                                                 D(L.geom), D(L.B));
+    mcoef_kernel<<<blocks_for(mcoef_threads(ellmax + 1, L.n_freq), T), T, 0, s>>>(ellmax + 1, L.n_freq, n_fftlog,
+                                                                                 D(L.geom), nullptr, D(L.B), nullptr);
     if (cudaGetLastError() != cudaSuccess) return DISCOEB_ECUDA;
     // 5. theta[r, l] = sum_j A[r, j] B[l, j] over the interleaved (re, im) pairs: one product,
     //    on the int8 tensor cores (digit planes, exact int32 sums) or as a cuBLAS DGEMM
@@ -1353,7 +1389,7 @@ int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_ta
         fgrid_dot_kernel<<<blocks_for(n_fftlog, T), T, 0, s>>>(n_fftlog, D(J.gd), D(L.fbias), D(J.fxd), D(J.fbd));
         chi_spline_dot_kernel<<<blocks_for(rows, 64), 64, 0, s>>>(rows, n_tau, D(L.lchi), D(J.lchid), Srow, Srow_dot,
                                                                   D(J.S2v), D(J.S2d), D(J.cpv), D(J.cpd));
-        chi_eval_dot_kernel<<<blocks_for((long long)rows * n_fftlog, T), T, 0, s>>>(
+        chi_eval_dot_kernel<<<row_grid(rows, n_fftlog, T), T, 0, s>>>(
             rows, n_tau, D(L.lchi), D(J.lchid), Srow, Srow_dot, D(J.S2v), D(J.S2d), n_fftlog,
             reinterpret_cast<const int*>(ws + L.fidx), D(L.fx), D(J.fxd), D(L.fbias), D(J.fbd), pitch, D(J.Fd));
         {
@@ -1367,11 +1403,11 @@ int32_t discoeb_los_cell_jvp(int32_t n_modes, const double* kmodes, int32_t n_ta
             if (cufftExecD2Z(plan, D(J.Fd), reinterpret_cast<cufftDoubleComplex*>(D(J.Fd))) != CUFFT_SUCCESS)
                 return DISCOEB_ECUDA;
         }
-        ck_dot_kernel<<<blocks_for((long long)rows * L.n_freq, T), T, 0, s>>>(rows, D(L.kd), n_fftlog, L.n_freq,
+        ck_dot_kernel<<<row_grid(rows, L.n_freq, T), T, 0, s>>>(rows, D(L.kd), n_fftlog, L.n_freq,
                                                                               D(L.geom), D(J.gd), pitch, D(L.fft),
                                                                               D(J.Fd));
-        mcoef_dot_kernel<<<blocks_for((long long)n_ell * L.n_freq, T), T, 0, s>>>(n_ell, L.n_freq, n_fftlog, D(L.geom),
-                                                                                  D(J.gd), D(J.Bd));
+        mcoef_kernel<<<blocks_for(mcoef_threads(n_ell, L.n_freq), T), T, 0, s>>>(n_ell, L.n_freq, n_fftlog, D(L.geom),
+                                                                                 D(J.gd), nullptr, D(J.Bd));
         if (cudaGetLastError() != cudaSuccess) return DISCOEB_ECUDA;
         if (!omega_t_times(D(J.Fd), D(J.H))) return DISCOEB_ECUDA;
         cell_dot_kernel<<<n_ell, 256, 0, s>>>(n_ell, pitch, D(L.B), D(J.H), D(J.Bd), D(J.G), cell_dot + (size_t)d * n_ell);

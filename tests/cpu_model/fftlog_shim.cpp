@@ -27,4 +27,10 @@ void shim_mcoef(int l, int q, int n_fft, double bias, double dl, double dl_dot, 
     fftlog_mcoef(l, q, n_fft, bias, dl, dl_dot, b, b_dot);
 }
 
+void shim_mcoef_run(int l0, int count, int q, int n_fft, double bias, double dl, double dl_dot, double* b,
+                    double* b_dot)
+{
+    fftlog_mcoef_run(l0, count, q, n_fft, bias, dl, dl_dot, 2, b, b_dot);
+}
+
 }  // extern "C"

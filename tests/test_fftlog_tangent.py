@@ -21,6 +21,7 @@ def lib(tmp_path_factory):
     L.shim_lngamma.argtypes = [d, d, dp]
     L.shim_digamma.argtypes = [d, d, dp]
     L.shim_mcoef.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, d, d, d, dp, dp]
+    L.shim_mcoef_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, d, d, d, dp, dp]
     return L
 
 
@@ -68,3 +69,29 @@ def test_mcoef_tangent_is_the_derivative_of_the_coefficient(lib):
                     continue
                 noise = 4e-16 * (big + 10.0) * np.abs(b).max() / h
                 assert np.abs(bd - fd).max() <= 1e-7 * scale + noise, (dl, l, q, bd, fd, noise)
+
+
+def test_mcoef_recurrence_in_l_matches_the_direct_evaluation(lib):
+    """the table kernel evaluates log-Gamma at every 16th l of a parity and steps
+    M_{l+2} = M_l (1 + l + p)/(2 + l - p) (and d ln M/dp by psi(z + 1) = psi(z) + 1/z) in between.
+    Agreement to the direct evaluation's own rounding: its phase is the difference of two
+    log-Gammas of size ~|z ln z| (~1e4 at the largest frequencies), so eps times those moves M by
+    up to ~1e-12 of |M| there, in the reference's direct evaluation as well"""
+    dp = ctypes.POINTER(ctypes.c_double)
+    n_fft, bias, count = 16384, -1.1, 16
+    for dl in (8.2e-4, 2.4e-3):
+        for l0 in (2, 3, 34, 1001, 2466):
+            for q in (0, 1, 17, 900, 4000, 8192):
+                run, run_d = np.zeros(2 * count), np.zeros(2 * count)
+                lib.shim_mcoef_run(l0, count, q, n_fft, bias, dl, 0.7, run.ctypes.data_as(dp), run_d.ctypes.data_as(dp))
+                eta = 2 * np.pi * q / (n_fft * dl)
+                for i in range(count):
+                    l = l0 + 2 * i
+                    b, bd = np.zeros(2), np.zeros(2)
+                    lib.shim_mcoef(l, q, n_fft, bias, dl, 0.7, b.ctypes.data_as(dp), bd.ctypes.data_as(dp))
+                    big = sum(abs(_call(lib.shim_lngamma, a.real, a.imag)) for a in
+                              (complex((1 + l + bias) / 2, eta / 2), complex((2 + l - bias) / 2, -eta / 2)))
+                    tol = (1e-13 + 4e-16 * big) * np.abs(b).max()
+                    assert np.abs(run[2 * i:2 * i + 2] - b).max() <= tol, (dl, l0, q, i)
+                    assert np.abs(run_d[2 * i:2 * i + 2] - bd).max() <= (1e-12 + 4e-16 * big) * np.abs(bd).max() + \
+                        tol * (0.7 / dl) * eta, (dl, l0, q, i)
