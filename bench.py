@@ -358,7 +358,8 @@ def run_batch(args, rank, world, local):
     ok = status == 0
     if rank == 0:
         print(json.dumps({
-            "metric": ("fwd+adjoint" if args.grad else "forward") + " k-mode solves/s, many cosmologies per launch",
+            "metric": ("fwd+grad (forward-mode tangents)" if args.grad else "forward") +
+                      " k-mode solves/s, many cosmologies per launch",
             "value": world * ok.size / (ms / 1e3),
             "unit": "k-mode solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "dtype": "f64",
