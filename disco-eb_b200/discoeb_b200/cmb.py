@@ -507,7 +507,14 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
                            num_thermo=num_thermo, de_guard_eps=de_guard_eps, device=device, full_state=True,
                            buffers=(buf, bdots), **L)
     prob.launch()
-    y = prob.state()
+    if sources == "tangent":
+        # the source stages run on the launch's row order (modes by descending k): the full states
+        # and their tangents are read where the launch wrote them (no reordering copy of the
+        # [K, nout, n] arrays, 7 GB per direction at l_max 50 and 2000 x 2000), and only the
+        # [K, n_tau] source rows are put back into the caller's order
+        y, k_rows, inv_rows = prob.launch_states()
+    else:
+        y, k_rows, inv_rows = prob.state(), kmodes, None
 
     def source_S(param, states):
         f = compute_sources(param=param, yout=states, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
@@ -522,10 +529,11 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
                                    device=device)
         return th, kk, compute_Cell(th, kk, bg["n_s"], bg["k_p"], device=device).cpu().numpy()
 
-    fields0 = compute_sources(param=bg, yout=y, kmodes=kmodes, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
+    fields0 = compute_sources(param=bg, yout=y, kmodes=k_rows, aexp_out=aexp_out, de_guard_eps=de_guard_eps,
                               device=device, **L)
-    S0 = fields0["S"]
-    SE0 = fields0["E"]
+    S0_rows = fields0["S"]  # the row order of y: the launch's (sources="tangent") or the caller's
+    S0 = fields0["S"] if inv_rows is None else fields0["S"][inv_rows]
+    SE0 = fields0["E"] if inv_rows is None else fields0["E"][inv_rows]
 
     def pol_cells(S, SE, tau, tau0):
         """C_l^TE and C_l^EE (numpy) of the line of sight of (S, S_E)."""
@@ -544,7 +552,7 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
         lib = _abi.lib()
         f64 = dict(dtype=torch.float64, device=device)
         K, T = S0.shape
-        d_k = torch.from_numpy(np.ascontiguousarray(kmodes)).to(device)
+        d_k = torch.from_numpy(np.ascontiguousarray(k_rows)).to(device)
         d_tau = torch.from_numpy(np.ascontiguousarray(tau_b)).to(device)
         d_bt = torch.from_numpy(background_table(aexp_out, tau_b, bg)).to(device)
         scratch = torch.empty(8 * K * T, **f64)
@@ -557,7 +565,7 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
     tangents = []
     for di, name in enumerate(ODE_DIRECTIONS):
         h = rel_step * max(abs(float(theta[name])), 1e-2)
-        ydot = prob.state_tangent(di)
+        ydot = prob.launch_state_tangent(di) if sources == "tangent" else prob.state_tangent(di)
         # the tangents of the line of sight's inputs: sources by a central difference (smooth in
         # their inputs), output times and tau0 exactly (linear in the background tables)
         side = []
@@ -583,11 +591,13 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
                                          prob.d_tan.data_ptr() + di * tan_size, 1, K, d_k.data_ptr(), T,
                                          d_tau.data_ptr(), d_tau_dot.data_ptr(),
                                          d_bt.data_ptr(), bt_dot.data_ptr(), y.data_ptr(), ydot.data_ptr(),
-                                         S0.data_ptr(), S_dot.data_ptr(), scratch.data_ptr(),
+                                         S0_rows.data_ptr(), S_dot.data_ptr(), scratch.data_ptr(),
                                          SE_dot.data_ptr() if pol else None,
                                          torch.cuda.current_stream(device).cuda_stream)
             if rc != 0:
                 raise RuntimeError(f"discoeb_sources_jvp failed with code {rc}")
+            S_dot = S_dot[inv_rows]
+            SE_dot = SE_dot[inv_rows] if pol else None
         elif pol:
             S_dot = (side[0][0][0] - side[1][0][0]) / (2 * h)
             SE_dot = (side[0][0][1] - side[1][0][1]) / (2 * h)

@@ -256,6 +256,7 @@ class JacobianProblem:
         self.dirs = ODE_DIRECTIONS
         # longest modes (largest k) first so that the tail of the launch is short
         order = np.argsort(-kmodes, kind="stable")
+        self.order = order
         self.inv = np.empty_like(order)
         self.inv[order] = np.arange(K)
         self.dc = DeviceCosmo(bg, de_guard_eps=de_guard_eps, device=device, **L)
@@ -318,6 +319,23 @@ class JacobianProblem:
         stat = self.d_stat.cpu().numpy()[:, self.inv]
         _check_status(stat[0], stat[1], self.kmodes, on_failure)
         return self.d_out[self.torch.as_tensor(self.inv, device=self.device)]
+
+    def launch_states(self, on_failure="raise"):
+        """(y [K, nout, n], kmodes [K], inv): the states as the launch holds them (modes by
+        descending k), without state()'s reordering copy, the launch's k of each row, and the row
+        of each of the caller's modes (a device index tensor).  launch_state_tangent() gives the
+        tangents in the same row order (views, no copy)."""
+        if not self.full_state:
+            raise ValueError("launch_states() needs a JacobianProblem made with full_state=True")
+        stat = self.d_stat.cpu().numpy()[:, self.inv]
+        _check_status(stat[0], stat[1], self.kmodes, on_failure)
+        return self.d_out, self.kmodes[self.order], self.torch.as_tensor(self.inv, device=self.device)
+
+    def launch_state_tangent(self, direction):
+        """d y / d theta_d [K, nout, n] in the launch's row order (a view of the launch's output)."""
+        if not self.full_state:
+            raise ValueError("launch_state_tangent() needs a JacobianProblem made with full_state=True")
+        return self.d_outd[direction]
 
     def state_tangent(self, direction):
         """d y / d theta_d [K, nout, n] along ODE_DIRECTIONS[direction] (output times moving
