@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     DiscoebControl ctrl, int n_modes, const double* __restrict__ kmodes, const double* __restrict__ tau_start,
     const double* __restrict__ y0, const double* __restrict__ y0_dot, const double* __restrict__ sw, int n_out,
     const double* __restrict__ tau_out, const double* __restrict__ tau_out_dot, int mem_doubles, int tan_doubles,
-    double* y_out20, double* y_out20_dot, int32_t* status, int32_t* nsteps)
+    double* rec_glob, double* y_out20, double* y_out20_dot, int32_t* status, int32_t* nsteps)
 {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5;
@@ -258,15 +258,18 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     tau_out += (size_t)ci * n_out;
     tau_out_dot += (size_t)ci * n_dir * n_out;
     // shared layout: cosmology, tangents, forward workspace, two step records (+4 scalars
-    // each: t, h, t_next, regime), per tangent warp its workspace + 3 n doubles, flags
+    // each: t, h, t_next, regime), per tangent warp its workspace + 3 n doubles, flags.  With
+    // rec_glob the two records are the block's own part of that global array instead (for states
+    // whose records would leave room for fewer tangent warps): the forward writes them, the
+    // tangent warps of the same block read them after the same counters and block-scope fences
     DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(smem);
     DiscoebTangent* TNs = reinterpret_cast<DiscoebTangent*>(smem + kCosmoDoubles);
     double* fmem = smem + kCosmoDoubles + dpb * kTanDoubles;
-    double* slot0 = fmem + mem_doubles;
     const int rec = mem_doubles + 4;
+    double* slot0 = rec_glob ? rec_glob + (size_t)blockIdx.x * 2 * rec : fmem + mem_doubles;
     const int n0 = (mem_doubles - 4 * kMaxSlots - 32) / 23;  // state size (mode_mem_doubles)
     const int per_tan = tan_doubles + 3 * n0;
-    double* twork = slot0 + 2 * rec;
+    double* twork = rec_glob ? fmem + mem_doubles : slot0 + 2 * rec;
     int* flags = reinterpret_cast<int*>(twork + (size_t)dpb * per_tan);
     // flags: [0,1] published count per slot (step m + 1), [2,3] consumptions per slot,
     //        [4] forward finished, [5] published steps in total, [6] abort
@@ -432,13 +435,59 @@ int validate_cosmo(const DiscoebCosmo* c)
     return DISCOEB_SUCCESS;
 }
 
+// Directions per block of discoeb_jvp: as many as fit in shared memory (at most
+// kMaxDirsPerBlock; the forward is solved once per block).  With the two step records in shared
+// memory (dpb, smem), or in a global workspace (dpb_glob, smem_glob), which is worth its
+// records_bytes only when it lets more directions share a block (larger states, e.g. l_max 50).
+struct JvpPlan {
+    int dpb, dpb_glob, mem, tmem;
+    size_t smem, smem_glob;
+    int64_t records_bytes;
+};
+
+JvpPlan jvp_plan(const DiscoebCosmo& c0, int n_dir, int n_modes)
+{
+    JvpPlan p{};
+    const Dims D = make_dims(c0);
+    p.mem = mode_mem_doubles(D);
+    p.tmem = tan_mem_doubles(D);
+    int dev = 0, max_optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        p.dpb = -1;
+        return p;
+    }
+    auto bytes = [&](int d, bool glob) {
+        return (size_t)(kCosmoDoubles + d * kTanDoubles + (glob ? 1 : 3) * p.mem + (glob ? 0 : 8) +
+                        d * (p.tmem + 3 * D.n)) *
+                   sizeof(double) +
+               8 * sizeof(int);
+    };
+    const int want = n_dir < kMaxDirsPerBlock ? n_dir : kMaxDirsPerBlock;
+    auto fit = [&](bool glob) {
+        int d = want;
+        while (d > 1 && bytes(d, glob) > (size_t)max_optin) --d;
+        return bytes(d, glob) <= (size_t)max_optin ? d : 0;
+    };
+    p.dpb = fit(false);
+    p.dpb_glob = fit(true);
+    p.smem = bytes(p.dpb > 0 ? p.dpb : 1, false);
+    p.smem_glob = bytes(p.dpb_glob > 0 ? p.dpb_glob : 1, true);
+    if (p.dpb_glob > p.dpb) {
+        const long long blocks = (long long)n_modes * ((n_dir + p.dpb_glob - 1) / p.dpb_glob);
+        p.records_bytes = blocks * 2LL * (p.mem + 4) * (int64_t)sizeof(double);
+    }
+    return p;
+}
+
 template <bool Full>
 int32_t launch_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
                    const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev, int32_t n_dir,
                    const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
                    const double* y0, const double* y0_dot, const double* switch_tau, int32_t n_out,
                    const double* tau_out, const double* tau_out_dot, double* y_out, double* y_out_dot,
-                   int32_t* status, int32_t* nsteps, void* stream)
+                   int32_t* status, int32_t* nsteps, double* records, int64_t records_bytes, void* stream)
 {
     int rc = validate_cosmo(cosmo0_host);
     if (rc) return rc;
@@ -450,21 +499,14 @@ int32_t launch_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_ho
         return DISCOEB_EINVAL;
     if (ctrl->method != DISCOEB_METHOD_RODAS5_STRUCTURED) return DISCOEB_EUNSUPPORTED;
     if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
-    const Dims D = make_dims(*cosmo0_host);
-    const int mem = mode_mem_doubles(D), tmem = tan_mem_doubles(D);
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return DISCOEB_ECUDA;
-    int max_optin = 0;
-    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    // directions per block: as many as fit (at most kMaxDirsPerBlock), the forward is shared
-    auto block_bytes = [&](int d) {
-        return (size_t)(kCosmoDoubles + d * kTanDoubles + 3 * mem + 8 + d * (tmem + 3 * D.n)) * sizeof(double) +
-               8 * sizeof(int);
-    };
-    int dpb = n_dir < kMaxDirsPerBlock ? n_dir : kMaxDirsPerBlock;
-    while (dpb > 1 && block_bytes(dpb) > (size_t)max_optin) --dpb;
-    if (block_bytes(dpb) > (size_t)max_optin) return DISCOEB_EUNSUPPORTED;
-    const size_t smem = block_bytes(dpb);
+    const JvpPlan plan = jvp_plan(*cosmo0_host, n_dir, n_modes);
+    if (plan.dpb < 0) return DISCOEB_ECUDA;
+    // the global records are used when the caller passes room for them (discoeb_jvp_records_bytes)
+    const bool glob = plan.records_bytes > 0 && records && records_bytes >= plan.records_bytes;
+    if (!glob && plan.dpb == 0) return DISCOEB_EUNSUPPORTED;
+    const int dpb = glob ? plan.dpb_glob : plan.dpb;
+    const size_t smem = glob ? plan.smem_glob : plan.smem;
+    const int mem = plan.mem, tmem = plan.tmem;
     if (cudaFuncSetAttribute(jvp_block_kernel<Full>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return DISCOEB_ECUDA;
@@ -472,7 +514,8 @@ int32_t launch_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_ho
     if (blocks > 0x7fffffffLL) return DISCOEB_EINVAL;
     jvp_block_kernel<Full><<<(unsigned)blocks, 32 * (1 + dpb), smem, reinterpret_cast<cudaStream_t>(stream)>>>(
         cosmos_dev, n_cosmo, mode_cosmo, tangents_dev, n_dir, dpb, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot,
-        switch_tau, n_out, tau_out, tau_out_dot, mem, tmem, y_out, y_out_dot, status, nsteps);
+        switch_tau, n_out, tau_out, tau_out_dot, mem, tmem, glob ? records : nullptr, y_out, y_out_dot, status,
+        nsteps);
     return cudaGetLastError() == cudaSuccess ? DISCOEB_SUCCESS : DISCOEB_ECUDA;
 }
 
@@ -536,7 +579,7 @@ int32_t discoeb_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_h
 {
     return launch_jvp<false>(cosmos_dev, cosmo0_host, n_cosmo, mode_cosmo, tangents_dev, n_dir, ctrl, n_modes, kmodes,
                              tau_start, y0, y0_dot, switch_tau, n_out, tau_out, tau_out_dot, y_out20, y_out20_dot,
-                             status, nsteps, stream);
+                             status, nsteps, nullptr, 0, stream);
 }
 
 int32_t discoeb_jvp_full(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
@@ -548,7 +591,33 @@ int32_t discoeb_jvp_full(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cos
 {
     return launch_jvp<true>(cosmos_dev, cosmo0_host, n_cosmo, mode_cosmo, tangents_dev, n_dir, ctrl, n_modes, kmodes,
                             tau_start, y0, y0_dot, switch_tau, n_out, tau_out, tau_out_dot, y_full, y_full_dot,
-                            status, nsteps, stream);
+                            status, nsteps, nullptr, 0, stream);
+}
+
+int64_t discoeb_jvp_records_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_dir, int32_t n_modes)
+{
+    if (validate_cosmo(cosmo0_host) || n_dir < 1 || n_modes < 0) return DISCOEB_EINVAL;
+    const JvpPlan plan = jvp_plan(*cosmo0_host, n_dir, n_modes);
+    return plan.dpb < 0 ? (int64_t)DISCOEB_ECUDA : plan.records_bytes;
+}
+
+int32_t discoeb_jvp_records(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                            const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev, int32_t n_dir,
+                            const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
+                            const double* y0, const double* y0_dot, const double* switch_tau, int32_t n_out,
+                            const double* tau_out, const double* tau_out_dot, double* y_out, double* y_out_dot,
+                            int32_t* status, int32_t* nsteps, int32_t full, void* records, int64_t records_bytes,
+                            void* stream)
+{
+    if (full != 0 && full != 1) return DISCOEB_EINVAL;
+    double* rec = static_cast<double*>(records);
+    if (full)
+        return launch_jvp<true>(cosmos_dev, cosmo0_host, n_cosmo, mode_cosmo, tangents_dev, n_dir, ctrl, n_modes,
+                                kmodes, tau_start, y0, y0_dot, switch_tau, n_out, tau_out, tau_out_dot, y_out,
+                                y_out_dot, status, nsteps, rec, records_bytes, stream);
+    return launch_jvp<false>(cosmos_dev, cosmo0_host, n_cosmo, mode_cosmo, tangents_dev, n_dir, ctrl, n_modes, kmodes,
+                             tau_start, y0, y0_dot, switch_tau, n_out, tau_out, tau_out_dot, y_out, y_out_dot, status,
+                             nsteps, rec, records_bytes, stream);
 }
 
 int32_t discoeb_rhs(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host, int32_t n_points,

@@ -298,16 +298,27 @@ class JacobianProblem:
         self.ctrl = _abi.DiscoebControl(rtol, atol, pcoeff, icoeff, dcoeff, factormax, factormin, int(max_steps),
                                         _abi.METHOD_RODAS5_STRUCTURED, int(warps_per_block), 0)
 
-    def launch(self):
+    def launch(self, records=True):
+        """Run the launch.  ``records=False`` keeps the step records in shared memory even where a
+        global workspace would let more directions share a block."""
         stream = self.torch.cuda.current_stream(self.device).cuda_stream
-        entry = self.lib.discoeb_jvp_full if self.full_state else self.lib.discoeb_jvp
-        rc = entry(self.dc.struct.data_ptr(), ctypes.byref(self.dc.host), 1, None,
-                                  self.d_tan.data_ptr(), len(self.dirs), ctypes.byref(self.ctrl), self.K,
-                                  self.d_k.data_ptr(),
-                                  self.d_ts.data_ptr(), self.d_y0.data_ptr(), self.d_y0d.data_ptr(),
-                                  self.d_sw.data_ptr(), self.nout, self.d_tout.data_ptr(), self.d_toutd.data_ptr(),
-                                  self.d_out.data_ptr(), self.d_outd.data_ptr(), self.d_stat[0].data_ptr(),
-                                  self.d_stat[1].data_ptr(), stream)
+        args = (self.dc.struct.data_ptr(), ctypes.byref(self.dc.host), 1, None, self.d_tan.data_ptr(), len(self.dirs),
+                ctypes.byref(self.ctrl), self.K, self.d_k.data_ptr(), self.d_ts.data_ptr(), self.d_y0.data_ptr(),
+                self.d_y0d.data_ptr(), self.d_sw.data_ptr(), self.nout, self.d_tout.data_ptr(),
+                self.d_toutd.data_ptr(), self.d_out.data_ptr(), self.d_outd.data_ptr(), self.d_stat[0].data_ptr(),
+                self.d_stat[1].data_ptr())
+        # large states (l_max 50): the step records in a global workspace let all directions share a
+        # block (discoeb_jvp_records); otherwise they stay in shared memory
+        nb = self.lib.discoeb_jvp_records_bytes(ctypes.byref(self.dc.host), len(self.dirs), self.K)
+        if nb < 0:
+            raise RuntimeError(f"discoeb_jvp_records_bytes failed with code {nb}")
+        if nb > 0 and records:
+            if getattr(self, "_records", None) is None or self._records.numel() * 8 < nb:
+                self._records = self.torch.empty(int(nb) // 8 + 1, dtype=self.torch.float64, device=self.device)
+            rc = self.lib.discoeb_jvp_records(*args, int(self.full_state), self._records.data_ptr(), int(nb), stream)
+        else:
+            entry = self.lib.discoeb_jvp_full if self.full_state else self.lib.discoeb_jvp
+            rc = entry(*args, stream)
         if rc != 0:
             raise RuntimeError(f"discoeb_jvp failed with code {rc}")
 

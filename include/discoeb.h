@@ -168,6 +168,23 @@ int32_t discoeb_jvp_full(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cos
                          const double* tau_out, const double* tau_out_dot, double* y_full, double* y_full_dot,
                          int32_t* status, int32_t* nsteps, void* stream);
 
+/* discoeb_jvp (full = 0) or discoeb_jvp_full (full = 1) with a caller workspace for the step
+ * records that the forward warp of a block hands to its tangent warps.  The plain entries keep
+ * them in shared memory, which for large states (l_max 50: n = 219) leaves room for only three
+ * tangent warps per block, so the forward runs twice per mode and an SM holds three tangent
+ * warps; with the records in global memory all six directions share one block.
+ * discoeb_jvp_records_bytes: the workspace size (0: the records fit with every direction in one
+ * block, nothing to gain; < 0: error).  records: >= that many bytes of device memory, 16-byte
+ * aligned, or NULL / too small for the shared-memory form.  Other arguments as discoeb_jvp. */
+int64_t discoeb_jvp_records_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_dir, int32_t n_modes);
+int32_t discoeb_jvp_records(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
+                            const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev, int32_t n_dir,
+                            const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,
+                            const double* y0, const double* y0_dot, const double* switch_tau, int32_t n_out,
+                            const double* tau_out, const double* tau_out_dot, double* y_out, double* y_out_dot,
+                            int32_t* status, int32_t* nsteps, int32_t full, void* records, int64_t records_bytes,
+                            void* stream);
+
 /* ---- Discrete adjoint (reverse mode) ----
  * Replaces reverse-mode differentiation (jax.grad / jax.vjp) through diffeqsolve(...,
  * adjoint=DirectAdjoint()) (src/discoeb/perturbations.py:904-925, :1059-1083): the exact

@@ -104,3 +104,25 @@ def test_gpu_autograd_function_contracts_the_jacobian(torch_cuda):
     np.testing.assert_allclose(P.detach().cpu().numpy(), P_ref, rtol=1e-12)
     expect = np.einsum("dkn,kn->d", J, weights.cpu().numpy())
     np.testing.assert_allclose(theta.grad.cpu().numpy(), expect, rtol=1e-12)
+
+
+def test_gpu_jvp_records_in_global_memory_equal_the_shared_form(torch_cuda):
+    """l_max 50 (n = 219): the shared-memory step records leave room for three tangent warps per
+    block, so discoeb_jvp_records keeps them in a global workspace and runs all six directions in
+    one block; same code on the same steps, so the same states and tangents as the plain entry
+    (which splits the directions over two blocks, each with its own forward)"""
+    import ctypes
+    from discoeb_b200.gradients import JacobianProblem
+    L50 = dict(lmaxg=50, lmaxgp=50, lmaxr=17, lmaxnu=17, nqmax=5)
+    prob = JacobianProblem(THETA, aexp_out=np.array([0.2, 0.5, 1.0]), kmodes=np.geomspace(1e-3, 0.3, 5), rtol=1e-5,
+                           atol=1e-8, full_state=True, **L50)
+    assert prob.lib.discoeb_jvp_records_bytes(ctypes.byref(prob.dc.host), 6, prob.K) > 0
+    prob.launch(records=False)
+    y, yd = prob.d_out.clone(), prob.d_outd.clone()
+    prob.launch()
+    np.testing.assert_array_equal(prob.d_out.cpu().numpy(), y.cpu().numpy())
+    np.testing.assert_array_equal(prob.d_outd.cpu().numpy(), yd.cpu().numpy())
+    assert np.isfinite(yd.cpu().numpy()).all()
+    # n = 143 gains nothing: every direction already shares the block
+    p143 = JacobianProblem(THETA, aexp_out=A4, kmodes=np.geomspace(1e-3, 0.3, 5), rtol=1e-5, atol=1e-8, **L143)
+    assert p143.lib.discoeb_jvp_records_bytes(ctypes.byref(p143.dc.host), 6, p143.K) == 0
