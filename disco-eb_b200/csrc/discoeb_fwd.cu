@@ -259,17 +259,23 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     tau_out_dot += (size_t)ci * n_dir * n_out;
     // shared layout: cosmology, tangents, forward workspace, two step records (+4 scalars
     // each: t, h, t_next, regime), per tangent warp its workspace + 3 n doubles, flags.  With
-    // rec_glob the two records are the block's own part of that global array instead (for states
-    // whose records would leave room for fewer tangent warps): the forward writes them, the
-    // tangent warps of the same block read them after the same counters and block-scope fences
+    // rec_glob (for states whose records would leave room for fewer tangent warps) there is one
+    // record, split: its first 13 n doubles (state, stage vectors) in the block's own part of that
+    // global array, the factorisation of W (10 n + 224 doubles, re-read by every stage's solve)
+    // and the scalars in shared memory; the forward runs one step ahead instead of two
     DiscoebCosmo* P = reinterpret_cast<DiscoebCosmo*>(smem);
     DiscoebTangent* TNs = reinterpret_cast<DiscoebTangent*>(smem + kCosmoDoubles);
     double* fmem = smem + kCosmoDoubles + dpb * kTanDoubles;
     const int rec = mem_doubles + 4;
-    double* slot0 = rec_glob ? rec_glob + (size_t)blockIdx.x * 2 * rec : fmem + mem_doubles;
     const int n0 = (mem_doubles - 4 * kMaxSlots - 32) / 23;  // state size (mode_mem_doubles)
+    const bool split = rec_glob != nullptr;
+    const int ns = split ? 1 : 2;                // record slots
+    const int gpart = split ? 13 * n0 : 0;       // doubles of a record in global memory
+    const int spart = rec - gpart;               // doubles of a record in shared memory
+    double* gslot = split ? rec_glob + (size_t)blockIdx.x * gpart : nullptr;
+    double* slot0 = fmem + mem_doubles;
     const int per_tan = tan_doubles + 3 * n0;
-    double* twork = rec_glob ? fmem + mem_doubles : slot0 + 2 * rec;
+    double* twork = slot0 + ns * spart;
     int* flags = reinterpret_cast<int*>(twork + (size_t)dpb * per_tan);
     // flags: [0,1] published count per slot (step m + 1), [2,3] consumptions per slot,
     //        [4] forward finished, [5] published steps in total, [6] abort
@@ -318,15 +324,16 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
         tm.sync();
         int m = 0;
         auto accept = [&](double t, double h, double tnext, int regime) -> bool {
-            const int sl = m & 1;
-            if (m >= 2 && !wait_at_least(tm, vf + 2 + sl, nd * (m / 2), vf + 6, poll_budget(ctrl))) return false;
-            double* dst = slot0 + sl * rec;
-            for (int i = tm.lane; i < mem_doubles; i += 32) dst[i] = fmem[i];
+            const int sl = m % ns;
+            if (m >= ns && !wait_at_least(tm, vf + 2 + sl, nd * (m / ns), vf + 6, poll_budget(ctrl))) return false;
+            double* dst = slot0 + sl * spart;
+            for (int i = tm.lane; i < gpart; i += 32) gslot[i] = fmem[i];
+            for (int i = tm.lane; i < mem_doubles - gpart; i += 32) dst[i] = fmem[gpart + i];
             if (tm.leader()) {
-                dst[mem_doubles] = t;
-                dst[mem_doubles + 1] = h;
-                dst[mem_doubles + 2] = tnext;
-                dst[mem_doubles + 3] = (double)regime;
+                dst[spart - 4] = t;
+                dst[spart - 3] = h;
+                dst[spart - 2] = tnext;
+                dst[spart - 1] = (double)regime;
             }
             tm.sync();
             if (tm.leader()) {
@@ -366,7 +373,7 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     int hint = P->xe_loga.n_knots / 2, iout = 0;
     const long long budget = poll_budget(ctrl);
     for (int m = 0;; ++m) {
-        const int sl = m & 1;
+        const int sl = m % ns;
         // the next step, unless the forward has finished with fewer steps
         int have = 0;
         if (tm.leader()) {
@@ -381,11 +388,11 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
             __threadfence_block();
         }
         if (!__shfl_sync(0xffffffffu, have, 0)) break;
-        const double* r = slot0 + sl * rec;
-        ModeMem Mr = carve(const_cast<double*>(r), D);
+        const double* r = slot0 + sl * spart;
+        ModeMem Mr = split ? carve_split(gslot, const_cast<double*>(r), D) : carve(const_cast<double*>(r), D);
         Mr.u = ubuf;
-        const double t = r[mem_doubles], h = r[mem_doubles + 1], tnext = r[mem_doubles + 2];
-        const int regime = (int)r[mem_doubles + 3];
+        const double t = r[spart - 4], h = r[spart - 3], tnext = r[spart - 2];
+        const int regime = (int)r[spart - 1];
         tangent_step(tm, *P, D, k, t, h, regime, Mr, TT, TN, hint);
         for (int i = tm.lane; i < n; i += 32) yend[i] = ubuf[i] + Mr.K[7 * n + i];
         tm.sync();
@@ -458,10 +465,11 @@ JvpPlan jvp_plan(const DiscoebCosmo& c0, int n_dir, int n_modes)
         p.dpb = -1;
         return p;
     }
+    // shared doubles: cosmology, tangents, forward workspace, the records' shared parts (two
+    // whole records, or one record's factorisation and scalars), the tangent warps' workspaces
     auto bytes = [&](int d, bool glob) {
-        return (size_t)(kCosmoDoubles + d * kTanDoubles + (glob ? 1 : 3) * p.mem + (glob ? 0 : 8) +
-                        d * (p.tmem + 3 * D.n)) *
-                   sizeof(double) +
+        const size_t recs = glob ? (size_t)(p.mem + 4 - 13 * D.n) : 2 * (size_t)(p.mem + 4);
+        return (size_t)(kCosmoDoubles + d * kTanDoubles + p.mem + recs + d * (p.tmem + 3 * D.n)) * sizeof(double) +
                8 * sizeof(int);
     };
     const int want = n_dir < kMaxDirsPerBlock ? n_dir : kMaxDirsPerBlock;
@@ -476,7 +484,7 @@ JvpPlan jvp_plan(const DiscoebCosmo& c0, int n_dir, int n_modes)
     p.smem_glob = bytes(p.dpb_glob > 0 ? p.dpb_glob : 1, true);
     if (p.dpb_glob > p.dpb) {
         const long long blocks = (long long)n_modes * ((n_dir + p.dpb_glob - 1) / p.dpb_glob);
-        p.records_bytes = blocks * 2LL * (p.mem + 4) * (int64_t)sizeof(double);
+        p.records_bytes = blocks * 13LL * D.n * (int64_t)sizeof(double);
     }
     return p;
 }

@@ -113,6 +113,18 @@ DHD ModeMem carve(double* base, const Dims& D)
     m.sc = m.F1s + kMaxSlots;  // 32 scalars
     return m;
 }
+// the same fields with the first 13 n (y .. K) at g and the rest (A .. sc) at f
+DHD ModeMem carve_split(double* g, double* f, const Dims& D)
+{
+    const int n = D.n;
+    ModeMem m = carve(g, D);
+    m.A = f;
+    m.Z = m.A + 7 * n;
+    m.Gs = m.Z + 3 * n;
+    m.F1s = m.Gs + 3 * kMaxSlots;
+    m.sc = m.F1s + kMaxSlots;
+    return m;
+}
 // scalar slots
 enum { SC_W00 = 0, SC_ETAC = 1, SC_CINV = 2, SC_F1Z = 11, SC_F1U = 14 };
 
