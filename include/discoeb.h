@@ -170,9 +170,11 @@ int32_t discoeb_jvp_full(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cos
 
 /* discoeb_jvp (full = 0) or discoeb_jvp_full (full = 1) with a caller workspace for the step
  * records that the forward warp of a block hands to its tangent warps.  The plain entries keep
- * them in shared memory, which for large states (l_max 50: n = 219) leaves room for only three
- * tangent warps per block, so the forward runs twice per mode and an SM holds three tangent
- * warps; with the records in global memory all six directions share one block.
+ * two whole records in shared memory, which for large states (l_max 50: n = 219) leaves room for
+ * only three tangent warps per block, so the forward runs twice per mode and an SM holds three
+ * tangent warps.  Here one record is kept, its state and stage vectors (13 n doubles per block) in
+ * the workspace and the factorisation of W in shared memory, and all six directions share a block
+ * (same results bit for bit).
  * discoeb_jvp_records_bytes: the workspace size (0: the records fit with every direction in one
  * block, nothing to gain; < 0: error).  records: >= that many bytes of device memory, 16-byte
  * aligned, or NULL / too small for the shared-memory form.  Other arguments as discoeb_jvp. */
