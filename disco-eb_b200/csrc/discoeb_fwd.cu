@@ -221,7 +221,7 @@ __device__ bool wait_at_least(const WarpTeam& tm, volatile int* flag, int target
 // consumed), every wait bounded (wait_at_least); if a wait gives up, the whole block stops and
 // reports DISCOEB_ABORTED.  The step sequence is the forward's only, so the tangent is the
 // derivative of the discrete solution with the accepted steps held fixed.
-template <bool Full>
+template <bool Full, bool Split>
 __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     const DiscoebCosmo* __restrict__ cosmos, int n_cosmo, const int32_t* __restrict__ mode_cosmo,
     const DiscoebTangent* __restrict__ tangents, int n_dir, int dpb,
@@ -268,11 +268,10 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
     double* fmem = smem + kCosmoDoubles + dpb * kTanDoubles;
     const int rec = mem_doubles + 4;
     const int n0 = (mem_doubles - 4 * kMaxSlots - 32) / 23;  // state size (mode_mem_doubles)
-    const bool split = rec_glob != nullptr;
-    const int ns = split ? 1 : 2;                // record slots
-    const int gpart = split ? 13 * n0 : 0;       // doubles of a record in global memory
+    constexpr int ns = Split ? 1 : 2;            // record slots
+    const int gpart = Split ? 13 * n0 : 0;       // doubles of a record in global memory
     const int spart = rec - gpart;               // doubles of a record in shared memory
-    double* gslot = split ? rec_glob + (size_t)blockIdx.x * gpart : nullptr;
+    double* gslot = Split ? rec_glob + (size_t)blockIdx.x * gpart : nullptr;
     double* slot0 = fmem + mem_doubles;
     const int per_tan = tan_doubles + 3 * n0;
     double* twork = slot0 + ns * spart;
@@ -327,7 +326,8 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
             const int sl = m % ns;
             if (m >= ns && !wait_at_least(tm, vf + 2 + sl, nd * (m / ns), vf + 6, poll_budget(ctrl))) return false;
             double* dst = slot0 + sl * spart;
-            for (int i = tm.lane; i < gpart; i += 32) gslot[i] = fmem[i];
+            if (Split)
+                for (int i = tm.lane; i < gpart; i += 32) gslot[i] = fmem[i];
             for (int i = tm.lane; i < mem_doubles - gpart; i += 32) dst[i] = fmem[gpart + i];
             if (tm.leader()) {
                 dst[spart - 4] = t;
@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(32 * (1 + kMaxDirsPerBlock)) jvp_block_kernel(
         }
         if (!__shfl_sync(0xffffffffu, have, 0)) break;
         const double* r = slot0 + sl * spart;
-        ModeMem Mr = split ? carve_split(gslot, const_cast<double*>(r), D) : carve(const_cast<double*>(r), D);
+        ModeMem Mr = Split ? carve_split(gslot, const_cast<double*>(r), D) : carve(const_cast<double*>(r), D);
         Mr.u = ubuf;
         const double t = r[spart - 4], h = r[spart - 3], tnext = r[spart - 2];
         const int regime = (int)r[spart - 1];
@@ -515,12 +515,12 @@ int32_t launch_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_ho
     const int dpb = glob ? plan.dpb_glob : plan.dpb;
     const size_t smem = glob ? plan.smem_glob : plan.smem;
     const int mem = plan.mem, tmem = plan.tmem;
-    if (cudaFuncSetAttribute(jvp_block_kernel<Full>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    auto kernel = glob ? jvp_block_kernel<Full, true> : jvp_block_kernel<Full, false>;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return DISCOEB_ECUDA;
     const long long blocks = (long long)n_modes * ((n_dir + dpb - 1) / dpb);
     if (blocks > 0x7fffffffLL) return DISCOEB_EINVAL;
-    jvp_block_kernel<Full><<<(unsigned)blocks, 32 * (1 + dpb), smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+    kernel<<<(unsigned)blocks, 32 * (1 + dpb), smem, reinterpret_cast<cudaStream_t>(stream)>>>(
         cosmos_dev, n_cosmo, mode_cosmo, tangents_dev, n_dir, dpb, *ctrl, n_modes, kmodes, tau_start, y0, y0_dot,
         switch_tau, n_out, tau_out, tau_out_dot, mem, tmem, glob ? records : nullptr, y_out, y_out_dot, status,
         nsteps);
