@@ -635,6 +635,9 @@ def main():
     ap.add_argument("--gemm-n", type=int, default=2501, help="--mode los-gemm: rows of B (multipoles)")
     ap.add_argument("--gemm-k", type=int, default=16386, help="--mode los-gemm: contraction length")
     ap.add_argument("--slices", type=int, default=7, help="--mode los-gemm: digit planes per operand")
+    ap.add_argument("--jvp-records", default="auto", choices=["auto", "always", "never"],
+                    help="fwd+grad: where the gradient kernel keeps its step records (auto: the split record "
+                         "only where it lets more directions share a block)")
     ap.add_argument("--los-contraction", default="int8", choices=["int8", "fp64"],
                     help="--mode cmb / cmb-grad: the line of sight's frequency sum on the int8 tensor cores "
                          "(7 digit planes) or as an FP64 DGEMM")
@@ -735,7 +738,8 @@ def main():
         prob = JacobianProblem(w["theta"], aexp_out=aout, kmodes=kmodes, rtol=w["rtol"], atol=w["atol"],
                                max_steps=100000, device=device, warps_per_block=args.wpb, **L)
         n_dir = len(prob.dirs)
-        solve, stat_of = prob.launch, (lambda: prob.d_stat)
+        rec_opt = {"auto": True, "always": "always", "never": False}[args.jvp_records]
+        solve, stat_of = (lambda: prob.launch(records=rec_opt)), (lambda: prob.d_stat)
     else:
         n_dir = 0
         solve, stat_of = forward, (lambda: d_stat)
@@ -922,6 +926,7 @@ def main():
                        "n_s, ln10As, w0, wa, m_nu" if grad else None,
                        "gradient_method": "forward-mode tangents (discoeb_jvp: 6 directions through the solver, "
                        "n_s and ln10As analytic)" if grad else None,
+                       "jvp_records": args.jvp_records if grad else None,
                        "rtol": w["rtol"], "atol": w["atol"],
                        "method": "rodas5-structured" + ("-mixed" if args.method == "structured-mixed" and not grad
                                                         else ""),

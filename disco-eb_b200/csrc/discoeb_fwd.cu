@@ -449,7 +449,8 @@ int validate_cosmo(const DiscoebCosmo* c)
 struct JvpPlan {
     int dpb, dpb_glob, mem, tmem;
     size_t smem, smem_glob;
-    int64_t records_bytes;
+    int64_t records_bytes;  // recommended: the split form's workspace where it adds directions, else 0
+    int64_t split_bytes;    // the split form's workspace (a caller may ask for it anyway)
 };
 
 JvpPlan jvp_plan(const DiscoebCosmo& c0, int n_dir, int n_modes)
@@ -482,10 +483,11 @@ JvpPlan jvp_plan(const DiscoebCosmo& c0, int n_dir, int n_modes)
     p.dpb_glob = fit(true);
     p.smem = bytes(p.dpb > 0 ? p.dpb : 1, false);
     p.smem_glob = bytes(p.dpb_glob > 0 ? p.dpb_glob : 1, true);
-    if (p.dpb_glob > p.dpb) {
+    if (p.dpb_glob > 0) {
         const long long blocks = (long long)n_modes * ((n_dir + p.dpb_glob - 1) / p.dpb_glob);
-        p.records_bytes = blocks * 13LL * D.n * (int64_t)sizeof(double);
+        p.split_bytes = blocks * 13LL * D.n * (int64_t)sizeof(double);
     }
+    if (p.dpb_glob > p.dpb) p.records_bytes = p.split_bytes;
     return p;
 }
 
@@ -509,8 +511,9 @@ int32_t launch_jvp(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_ho
     if (!(ctrl->rtol > 0.0) || !(ctrl->atol >= 0.0) || ctrl->max_steps < 1) return DISCOEB_EINVAL;
     const JvpPlan plan = jvp_plan(*cosmo0_host, n_dir, n_modes);
     if (plan.dpb < 0) return DISCOEB_ECUDA;
-    // the global records are used when the caller passes room for them (discoeb_jvp_records_bytes)
-    const bool glob = plan.records_bytes > 0 && records && records_bytes >= plan.records_bytes;
+    // the split record is used when the caller passes room for it (discoeb_jvp_records_bytes
+    // recommends it where it lets more directions share a block; a caller may pass it anyway)
+    const bool glob = plan.dpb_glob >= plan.dpb && plan.split_bytes > 0 && records && records_bytes >= plan.split_bytes;
     if (!glob && plan.dpb == 0) return DISCOEB_EUNSUPPORTED;
     const int dpb = glob ? plan.dpb_glob : plan.dpb;
     const size_t smem = glob ? plan.smem_glob : plan.smem;
@@ -607,6 +610,13 @@ int64_t discoeb_jvp_records_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_dir
     if (validate_cosmo(cosmo0_host) || n_dir < 1 || n_modes < 0) return DISCOEB_EINVAL;
     const JvpPlan plan = jvp_plan(*cosmo0_host, n_dir, n_modes);
     return plan.dpb < 0 ? (int64_t)DISCOEB_ECUDA : plan.records_bytes;
+}
+
+int64_t discoeb_jvp_split_records_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_dir, int32_t n_modes)
+{
+    if (validate_cosmo(cosmo0_host) || n_dir < 1 || n_modes < 0) return DISCOEB_EINVAL;
+    const JvpPlan plan = jvp_plan(*cosmo0_host, n_dir, n_modes);
+    return plan.dpb < 0 ? (int64_t)DISCOEB_ECUDA : plan.split_bytes;
 }
 
 int32_t discoeb_jvp_records(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,

@@ -194,6 +194,8 @@ def lib():
         L.discoeb_jvp_full.restype = ctypes.c_int32
         L.discoeb_jvp_records_bytes.argtypes = [ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, ctypes.c_int32]
         L.discoeb_jvp_records_bytes.restype = ctypes.c_int64
+        L.discoeb_jvp_split_records_bytes.argtypes = [ctypes.POINTER(DiscoebCosmo), ctypes.c_int32, ctypes.c_int32]
+        L.discoeb_jvp_split_records_bytes.restype = ctypes.c_int64
         L.discoeb_jvp_records.argtypes = L.discoeb_jvp.argtypes[:-1] + [ctypes.c_int32, vp, ctypes.c_int64, vp]
         L.discoeb_jvp_records.restype = ctypes.c_int32
         L.discoeb_rhs.restype = ctypes.c_int32

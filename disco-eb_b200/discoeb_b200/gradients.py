@@ -300,7 +300,9 @@ class JacobianProblem:
 
     def launch(self, records=True):
         """Run the launch.  ``records=False`` keeps the step records in shared memory even where a
-        global workspace would let more directions share a block."""
+        global workspace would let more directions share a block; ``records="always"`` uses the
+        split record (factorisation in shared memory, state and stages in a global workspace) also
+        where every direction already shares the block."""
         stream = self.torch.cuda.current_stream(self.device).cuda_stream
         args = (self.dc.struct.data_ptr(), ctypes.byref(self.dc.host), 1, None, self.d_tan.data_ptr(), len(self.dirs),
                 ctypes.byref(self.ctrl), self.K, self.d_k.data_ptr(), self.d_ts.data_ptr(), self.d_y0.data_ptr(),
@@ -309,7 +311,9 @@ class JacobianProblem:
                 self.d_stat[1].data_ptr())
         # large states (l_max 50): the step records in a global workspace let all directions share a
         # block (discoeb_jvp_records); otherwise they stay in shared memory
-        nb = self.lib.discoeb_jvp_records_bytes(ctypes.byref(self.dc.host), len(self.dirs), self.K)
+        size_fn = (self.lib.discoeb_jvp_split_records_bytes if records == "always" else
+                   self.lib.discoeb_jvp_records_bytes)
+        nb = size_fn(ctypes.byref(self.dc.host), len(self.dirs), self.K)
         if nb < 0:
             raise RuntimeError(f"discoeb_jvp_records_bytes failed with code {nb}")
         if nb > 0 and records:

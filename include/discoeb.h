@@ -179,6 +179,9 @@ int32_t discoeb_jvp_full(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cos
  * block, nothing to gain; < 0: error).  records: >= that many bytes of device memory, 16-byte
  * aligned, or NULL / too small for the shared-memory form.  Other arguments as discoeb_jvp. */
 int64_t discoeb_jvp_records_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_dir, int32_t n_modes);
+/* The split form's workspace whether or not it adds directions per block (a caller that passes
+ * this much gets the split form also where the records would fit in shared memory). */
+int64_t discoeb_jvp_split_records_bytes(const DiscoebCosmo* cosmo0_host, int32_t n_dir, int32_t n_modes);
 int32_t discoeb_jvp_records(const DiscoebCosmo* cosmos_dev, const DiscoebCosmo* cosmo0_host, int32_t n_cosmo,
                             const int32_t* mode_cosmo, const DiscoebTangent* tangents_dev, int32_t n_dir,
                             const DiscoebControl* ctrl, int32_t n_modes, const double* kmodes, const double* tau_start,

@@ -279,3 +279,35 @@ def test_fused_sources_entry_rejects_bad_arguments_before_any_launch():
     args = list(ok)
     args[2] = ctypes.byref(bad)
     assert lib.discoeb_fwd_sources(*args) == -3  # DISCOEB_EUNSUPPORTED
+
+
+def test_int8_contraction_workspace_and_arguments_on_the_host():
+    """discoeb_dgemm_i8's workspace arithmetic and argument checks (host code, no launch): digit
+    planes of 256-row tiles x 128-byte K stages, the K ranges chosen for >= 4 waves of CTAs (148
+    SMs assumed without a device), int32 level sums per K range and level"""
+    lib = _abi.lib()
+    tile = 256 * 128
+
+    def planes(m, n, k, s):
+        mt, nt, kst = -(-m // 256), -(-n // 256), -(-k // 128)
+        return mt, nt, kst, s * (mt + nt) * kst * tile
+
+    for (m, n, k, s, split) in [(8192, 2501, 16386, 7, 2), (300, 260, 1000, 1, 1), (513, 300, 2000, 6, 3)]:
+        mt, nt, kst, pl = planes(m, n, k, s)
+        got = lib.discoeb_dgemm_i8_workspace_bytes(m, n, k, s, split)
+        levels = split * s * mt * 256 * nt * 256 * 4
+        assert pl + levels <= got <= pl + levels + 8 * 256 + 8 * 12 * (mt + nt) * 256, (m, n, k, got)
+    # the line-of-sight size without a split given: 320 tiles -> 2 K ranges (640 CTAs >= 4 x 148)
+    assert lib.discoeb_dgemm_i8_workspace_bytes(8192, 2501, 16386, 7, 0) == \
+        lib.discoeb_dgemm_i8_workspace_bytes(8192, 2501, 16386, 7, 2)
+    for bad in [(0, 4, 4, 7, 0), (4, 0, 4, 7, 0), (4, 4, 0, 7, 0), (4, 4, 4, 0, 0), (4, 4, 4, 9, 0)]:
+        assert lib.discoeb_dgemm_i8_workspace_bytes(*bad) < 0, bad
+    nb = lib.discoeb_dgemm_i8_workspace_bytes(4, 4, 4, 7, 1)
+    # null operands, a bad transpose flag, leading dimensions below the row length, a short or
+    # unaligned workspace: all refused before any launch
+    assert lib.discoeb_dgemm_i8(4, 4, 4, None, 4, 0, None, 4, 0, None, 4, 7, 1, 256, nb, None) != 0
+    assert lib.discoeb_dgemm_i8(4, 4, 4, 256, 4, 2, 256, 4, 0, 256, 4, 7, 1, 256, nb, None) != 0
+    assert lib.discoeb_dgemm_i8(4, 4, 4, 256, 3, 0, 256, 4, 0, 256, 4, 7, 1, 256, nb, None) != 0
+    assert lib.discoeb_dgemm_i8(4, 4, 4, 256, 4, 0, 256, 4, 0, 256, 4, 7, 1, 256, nb - 1, None) != 0
+    assert lib.discoeb_dgemm_i8(4, 4, 4, 256, 4, 0, 256, 4, 0, 256, 4, 7, 1, 264, nb, None) != 0
+    assert lib.discoeb_set_los_contraction(2, 7) != 0 and lib.discoeb_set_los_contraction(1, 9) != 0
