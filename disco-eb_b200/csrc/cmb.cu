@@ -812,46 +812,53 @@ __global__ void __launch_bounds__(128) sources_dot_kernel(
     const int wib = threadIdx.x >> 5;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long n_points = (long long)n_modes * n_tau;
-    if (warp >= n_points * n_dir) return;
+    if (warp >= n_points) return;
     const WarpTeam tm{(int)(threadIdx.x & 31)};
     const DiscoebCosmo& P = *cosmo;
     const Dims D = make_dims(P);
     const int n = D.n;
-    const int d = (int)(warp / n_points);
-    const long long pt = warp - (long long)d * n_points;
+    const long long pt = warp;
     const int im = (int)(pt / n_tau), j = (int)(pt - (long long)im * n_tau);
-    const DiscoebTangent* TN = tangents + d;
-    const double k = kmodes[im], t = tau[j], tdot = tau_dot[(size_t)d * n_tau + j];
+    const double k = kmodes[im], t = tau[j];
     const double* y = y_full + (size_t)pt * n;
-    const double* yd = y_full_dot + ((size_t)d * n_points + pt) * n;
     double* yp = smem + (size_t)wib * 2 * n;
     double* ypd = yp + n;
+    // the base point's y' once per point, then each direction's derivative part
     Bg<double> b;
     bg_eval(P, y[0], t, k, -1, b);
     rhs_team(tm, P, D, b, k, t, y, yp, (double*)nullptr);
     int hint = P.xe_loga.n_knots / 2;
-    Bg<Dual> bd;
-    bg_eval_team(tm, P, Dual(y[0], yd[0]), t, k, -1, bd, hint, TN);
-    rhs_team(tm, P, D, bd, k, t, y, ypd, (double*)nullptr, yd, (const double*)nullptr, 1, 1);
-    tm.sync();
-    for (int i = tm.lane; i < n; i += 32) ypd[i] += dtau_row(D, b, t, i, y) * tdot;
-    tm.sync();
-    if (!tm.leader()) return;
-    Dual btj[DISCOEB_BG_NFIELDS];
-    for (int f = 0; f < DISCOEB_BG_NFIELDS; ++f)
-        btj[f] = Dual(bt[f * n_tau + j], bt_dot[((size_t)d * DISCOEB_BG_NFIELDS + f) * n_tau + j]);
-    const SrcPar<Dual> sp{Dual(P.grhom, TN->grhom), Dual(P.Omegam, TN->Omegam), Dual(P.Omegab, TN->Omegab),
-                          Dual(P.OmegaDE, TN->OmegaDE), Dual(P.amnu, TN->amnu), Dual(P.w0, TN->w0),
-                          Dual(P.wa, TN->wa)};
-    Dual out[DISCOEB_SRC_NFIELDS];
-    assemble_sources(P, sp, D, k, btj, [&](int i) { return Dual(y[i], yd[i]); },
-                     [&](int i) { return Dual(yp[i], ypd[i]); }, out);
-    const size_t stride = (size_t)n_dir * n_points, o = (size_t)d * n_points + pt;
-    fd4[0 * stride + o] = out[DISCOEB_SRC_S2].d;
-    fd4[1 * stride + o] = out[DISCOEB_SRC_S3].d;
-    fd4[2 * stride + o] = out[DISCOEB_SRC_S4].d;
-    fd4[3 * stride + o] = out[DISCOEB_SRC_POTENTIAL].d;
-    if (se_dot) se_dot[o] = out[DISCOEB_SRC_E].d;  // the E-mode source has no spline part
+    const size_t stride = (size_t)n_dir * n_points;
+    for (int d = 0; d < n_dir; ++d) {
+        const DiscoebTangent* TN = tangents + d;
+        const double tdot = tau_dot[(size_t)d * n_tau + j];
+        const double* yd = y_full_dot + ((size_t)d * n_points + pt) * n;
+        Bg<Dual> bd;
+        bg_eval_team(tm, P, Dual(y[0], yd[0]), t, k, -1, bd, hint, TN);
+        rhs_team(tm, P, D, bd, k, t, y, ypd, (double*)nullptr, yd, (const double*)nullptr, 1, 1);
+        tm.sync();
+        for (int i = tm.lane; i < n; i += 32) ypd[i] += dtau_row(D, b, t, i, y) * tdot;
+        tm.sync();
+        if (tm.leader()) {
+            Dual btj[DISCOEB_BG_NFIELDS];
+            for (int f = 0; f < DISCOEB_BG_NFIELDS; ++f)
+                btj[f] = Dual(bt[f * n_tau + j], bt_dot[((size_t)d * DISCOEB_BG_NFIELDS + f) * n_tau + j]);
+            const SrcPar<Dual> sp{Dual(P.grhom, TN->grhom), Dual(P.Omegam, TN->Omegam),
+                                  Dual(P.Omegab, TN->Omegab), Dual(P.OmegaDE, TN->OmegaDE),
+                                  Dual(P.amnu, TN->amnu),   Dual(P.w0, TN->w0),
+                                  Dual(P.wa, TN->wa)};
+            Dual out[DISCOEB_SRC_NFIELDS];
+            assemble_sources(P, sp, D, k, btj, [&](int i) { return Dual(y[i], yd[i]); },
+                             [&](int i) { return Dual(yp[i], ypd[i]); }, out);
+            const size_t o = (size_t)d * n_points + pt;
+            fd4[0 * stride + o] = out[DISCOEB_SRC_S2].d;
+            fd4[1 * stride + o] = out[DISCOEB_SRC_S3].d;
+            fd4[2 * stride + o] = out[DISCOEB_SRC_S4].d;
+            fd4[3 * stride + o] = out[DISCOEB_SRC_POTENTIAL].d;
+            if (se_dot) se_dot[o] = out[DISCOEB_SRC_E].d;  // the E-mode source has no spline part
+        }
+        tm.sync();  // the next direction overwrites ypd
+    }
 }
 
 __device__ Dual spline_slope_dual(Dual x0, Dual x1, Dual y0, Dual y1, Dual S0, Dual S1, Dual xn)
@@ -1430,14 +1437,15 @@ int32_t discoeb_sources_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* c
     const Dims D = make_dims(*cosmo_host);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const long long points = (long long)n_dir * n_modes * n_tau;
+    const long long warps = (long long)n_modes * n_tau;  // one warp per (mode, time), every direction
     const int threads = 128;
     // isw_dot_kernel indexes (direction, mode) pairs with an int, and one warp per point must fit
     // the grid: larger problems are refused rather than truncated
-    if ((long long)n_dir * n_modes > 0x7fffffffLL || points * 32 / threads >= 0x7fffffffLL) return DISCOEB_EINVAL;
+    if ((long long)n_dir * n_modes > 0x7fffffffLL || warps * 32 / threads >= 0x7fffffffLL) return DISCOEB_EINVAL;
     const size_t smem = sizeof(double) * 2 * (size_t)D.n * (threads / 32);
     double* fd4 = scratch;                       // [4, n_dir, n_modes, n_tau]
     double* sp = scratch + 4 * (size_t)points;  // [4, n_dir, n_modes, n_tau]
-    sources_dot_kernel<<<blocks_for(points * 32, threads), threads, smem, s>>>(
+    sources_dot_kernel<<<blocks_for(warps * 32, threads), threads, smem, s>>>(
         cosmo_dev, tangents_dev, n_dir, n_modes, kmodes, n_tau, tau, tau_dot, bgtab, bgtab_dot, y_full, y_full_dot, fd4,
         SE_dot);
     const size_t stride = (size_t)n_modes * n_tau;

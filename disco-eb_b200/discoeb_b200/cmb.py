@@ -555,19 +555,17 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
         d_k = torch.from_numpy(np.ascontiguousarray(k_rows)).to(device)
         d_tau = torch.from_numpy(np.ascontiguousarray(tau_b)).to(device)
         d_bt = torch.from_numpy(background_table(aexp_out, tau_b, bg)).to(device)
-        scratch = torch.empty(8 * K * T, **f64)
-        tan_size = ctypes.sizeof(_abi.DiscoebTangent)
     if los == "differences":
         th, kk, cell = los_cell(S0, tau_b, tau0_b)
     J = np.zeros((len(THETA_NAMES), ellmax + 1))
     Jp = {name: np.zeros((len(THETA_NAMES), ellmax + 1)) for name in ("TE", "EE") if name in spectra}
     stencil = ((2.0, -1.0 / 12.0), (1.0, 8.0 / 12.0), (-1.0, -8.0 / 12.0), (-2.0, 1.0 / 12.0))
     tangents = []
-    for di, name in enumerate(ODE_DIRECTIONS):
+
+    def side_tables(di, name):
+        """the direction's step h and the backgrounds moved by +-h along its exact tangent: their
+        output times, tau0 and (sources="tangent") background rows, or (differences) sources"""
         h = rel_step * max(abs(float(theta[name])), 1e-2)
-        ydot = prob.launch_state_tangent(di) if sources == "tangent" else prob.state_tangent(di)
-        # the tangents of the line of sight's inputs: sources by a central difference (smooth in
-        # their inputs), output times and tau0 exactly (linear in the background tables)
         side = []
         for sgn in (1.0, -1.0):
             ps = dict(p)
@@ -578,32 +576,49 @@ def compute_Cell_jacobian(theta, *, ellmax=2500, nmodes=128, kmin=1e-4, kmax=1.0
             if sources == "tangent":  # the background rows of the sources, differenced on the host
                 side.append((background_table(aexp_out, tau_s, bgs), tau_s, tau0_s))
             else:
+                ydot = prob.state_tangent(di)
                 side.append((source_S(bgs, torch.add(y, ydot, alpha=sgn * h)), tau_s, tau0_s))
+                del ydot
+        return h, side
+
+    if sources == "tangent":
+        # every direction's source tangents in one discoeb_sources_jvp call: one warp per (mode,
+        # time) evaluates the base point's y' once and each direction's derivative after it
+        ND = len(ODE_DIRECTIONS)
+        sides = [side_tables(di, name) for di, name in enumerate(ODE_DIRECTIONS)]
+        tau_dots = np.stack([(sd[0][1] - sd[1][1]) / (2 * h) for h, sd in sides])
+        bt_dots = np.stack([(sd[0][0] - sd[1][0]) / (2 * h) for h, sd in sides])
+        d_tau_dot = torch.from_numpy(np.ascontiguousarray(tau_dots)).to(device)
+        d_bt_dot = torch.from_numpy(np.ascontiguousarray(bt_dots)).to(device)
+        S_dot_all = torch.empty((ND, K, T), **f64)
+        SE_dot_all = torch.empty((ND, K, T), **f64) if pol else None
+        scratch = torch.empty(8 * ND * K * T, **f64)
+        rc = lib.discoeb_sources_jvp(prob.dc.struct.data_ptr(), ctypes.byref(prob.dc.host), prob.d_tan.data_ptr(), ND,
+                                     K, d_k.data_ptr(), T, d_tau.data_ptr(), d_tau_dot.data_ptr(), d_bt.data_ptr(),
+                                     d_bt_dot.data_ptr(), y.data_ptr(), prob.d_outd.data_ptr(), S0_rows.data_ptr(),
+                                     S_dot_all.data_ptr(), scratch.data_ptr(),
+                                     SE_dot_all.data_ptr() if pol else None,
+                                     torch.cuda.current_stream(device).cuda_stream)
+        if rc != 0:
+            raise RuntimeError(f"discoeb_sources_jvp failed with code {rc}")
+        del scratch
+    for di, name in enumerate(ODE_DIRECTIONS):
+        if sources == "tangent":
+            h, side = sides[di]
+        else:
+            h, side = side_tables(di, name)
         tau_dot = (side[0][1] - side[1][1]) / (2 * h)
         tau0_dot = (side[0][2] - side[1][2]) / (2 * h)
         SE_dot = None
         if sources == "tangent":
-            bt_dot = torch.from_numpy(np.ascontiguousarray((side[0][0] - side[1][0]) / (2 * h))).to(device)
-            S_dot = torch.empty((K, T), **f64)
-            SE_dot = torch.empty((K, T), **f64) if pol else None
-            d_tau_dot = torch.from_numpy(np.ascontiguousarray(tau_dot)).to(device)
-            rc = lib.discoeb_sources_jvp(prob.dc.struct.data_ptr(), ctypes.byref(prob.dc.host),
-                                         prob.d_tan.data_ptr() + di * tan_size, 1, K, d_k.data_ptr(), T,
-                                         d_tau.data_ptr(), d_tau_dot.data_ptr(),
-                                         d_bt.data_ptr(), bt_dot.data_ptr(), y.data_ptr(), ydot.data_ptr(),
-                                         S0_rows.data_ptr(), S_dot.data_ptr(), scratch.data_ptr(),
-                                         SE_dot.data_ptr() if pol else None,
-                                         torch.cuda.current_stream(device).cuda_stream)
-            if rc != 0:
-                raise RuntimeError(f"discoeb_sources_jvp failed with code {rc}")
-            S_dot = S_dot[inv_rows]
-            SE_dot = SE_dot[inv_rows] if pol else None
+            S_dot = S_dot_all[di][inv_rows]
+            SE_dot = SE_dot_all[di][inv_rows] if pol else None
         elif pol:
             S_dot = (side[0][0][0] - side[1][0][0]) / (2 * h)
             SE_dot = (side[0][0][1] - side[1][0][1]) / (2 * h)
         else:
             S_dot = (side[0][0] - side[1][0]) / (2 * h)
-        del ydot, side
+        del side
         if pol:  # E-mode line of sight and C_l^TE / C_l^EE along the path, fourth order
             acc = {sp: 0.0 for sp in Jp}
             for m, wgt in stencil:

@@ -264,3 +264,56 @@ def test_gpu_polarisation_forward_mode_sources_equal_their_differences(torch_cud
                for i in range(8)]
         print(sp, "forward-mode vs differenced sources per direction:", dev)
         assert max(dev) <= 1e-6, (sp, dev)
+
+
+def test_gpu_sources_jvp_batched_directions_equal_single_calls(torch_cuda):
+    """discoeb_sources_jvp with all six directions in one call (one warp per mode and time, the
+    base point's y' once) gives the same source tangents, bit for bit, as one call per direction"""
+    import ctypes
+
+    import torch
+    from discoeb_b200 import _abi
+    from discoeb_b200.cmb import background_table, cmb_aexp_out, compute_sources
+    from discoeb_b200.gradients import JacobianProblem
+    L = dict(lmaxg=11, lmaxgp=11, lmaxr=11, lmaxnu=8, nqmax=3)
+    theta = dict(omega_c=0.120, omega_b=0.0224, h=0.674, n_s=0.965, ln10As=math.log(21.0), w0=-0.95, wa=0.05,
+                 m_nu=0.06)
+    a = cmb_aexp_out()
+    ks = np.geomspace(1e-3, 0.2, 6)
+    prob = JacobianProblem(theta, aexp_out=a, kmodes=ks, rtol=1e-4, atol=1e-4, full_state=True, num_thermo=1024, **L)
+    prob.launch()
+    y, k_rows, _ = prob.launch_states()
+    bg = prob.bg
+    tau = bg["tau_of_a_spline"].evaluate(a)
+    dev = y.device
+    f = compute_sources(param=bg, yout=y, kmodes=k_rows, aexp_out=a, device=dev, **L)
+    K, T = f["S"].shape
+    rng = np.random.default_rng(5)
+    tau_dot = torch.from_numpy(rng.standard_normal((6, T)) * 1e-2).to(dev)
+    bt = torch.from_numpy(background_table(a, tau, bg)).to(dev)
+    bt_dot = torch.from_numpy(rng.standard_normal((6,) + tuple(bt.shape)) * 1e-3 * np.abs(bt.cpu().numpy())).to(dev)
+    d_k = torch.from_numpy(np.ascontiguousarray(k_rows)).to(dev)
+    d_tau = torch.from_numpy(np.ascontiguousarray(tau)).to(dev)
+    lib = _abi.lib()
+    tan_size = ctypes.sizeof(_abi.DiscoebTangent)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def call(d0, nd):
+        S = torch.empty((nd, K, T), dtype=torch.float64, device=dev)
+        SE = torch.empty((nd, K, T), dtype=torch.float64, device=dev)
+        scratch = torch.empty(8 * nd * K * T, dtype=torch.float64, device=dev)
+        rc = lib.discoeb_sources_jvp(prob.dc.struct.data_ptr(), ctypes.byref(prob.dc.host),
+                                     prob.d_tan.data_ptr() + d0 * tan_size, nd, K, d_k.data_ptr(), T, d_tau.data_ptr(),
+                                     tau_dot[d0:d0 + nd].contiguous().data_ptr(), bt.data_ptr(),
+                                     bt_dot[d0:d0 + nd].contiguous().data_ptr(), y.data_ptr(),
+                                     prob.d_outd[d0:d0 + nd].contiguous().data_ptr(), f["S"].data_ptr(), S.data_ptr(),
+                                     scratch.data_ptr(), SE.data_ptr(), stream)
+        assert rc == 0
+        return S.cpu().numpy(), SE.cpu().numpy()
+
+    S6, SE6 = call(0, 6)
+    for d in range(6):
+        S1, SE1 = call(d, 1)
+        np.testing.assert_array_equal(S6[d], S1[0])
+        np.testing.assert_array_equal(SE6[d], SE1[0])
+    assert np.isfinite(S6).all() and np.abs(S6).max() > 0
