@@ -362,7 +362,10 @@ int32_t discoeb_sources_noalloc(const DiscoebCosmo* cosmo_dev, const DiscoebCosm
  *   fields: discoeb_sources' output at the base point (its potential row is read)
  *   S_dot [n_dir, n_modes, n_tau] out; scratch: 8 n_dir n_modes n_tau doubles
  *   SE_dot [n_dir, n_modes, n_tau] out, may be NULL: the derivative of the E-mode source
- *   (DISCOEB_SRC_E; no counterpart in the reference).  Device arrays. */
+ *   (DISCOEB_SRC_E; no counterpart in the reference).  Device arrays.
+ * One warp per (mode, time) evaluates the base point's y' once and every direction after it, so
+ * one call with all directions costs less than one call per direction (same results bit for
+ * bit). */
 int32_t discoeb_sources_jvp(const DiscoebCosmo* cosmo_dev, const DiscoebCosmo* cosmo_host,
                             const DiscoebTangent* tangents_dev, int32_t n_dir, int32_t n_modes, const double* kmodes,
                             int32_t n_tau, const double* tau, const double* tau_dot, const double* bgtab,
